@@ -1,0 +1,58 @@
+"""Build the sm_100a shared library liberf_b200.so in-tree with nvcc.
+
+    python -m erf_b200.build            # incremental
+    python -m erf_b200.build --force    # rebuild everything
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "liberf_b200.so")
+SOURCES = ["kernels.cu", "api.cu"]
+HEADERS = ["common.cuh", "kernels.cuh"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xptxas", "-v"]
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "erf_b200.h")]
+    objs = []
+    for s in SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(OBJ, s.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _stale(obj, [src] + hdrs):
+            cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+            out = subprocess.run(cmd, capture_output=True, text=True)
+            log = os.path.join(OBJ, s + ".log")
+            with open(log, "w") as fh:
+                fh.write(" ".join(cmd) + "\n" + out.stdout + out.stderr)
+            if out.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {s}:\n{out.stderr[-4000:]}")
+            if verbose:
+                sys.stderr.write(out.stderr)
+    if force or _stale(LIB, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        if out.returncode != 0:
+            raise RuntimeError("link failed:\n" + out.stderr[-4000:])
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,510 @@
+// api.cu -- host side of the C-ABI: context, device buffers, the multirate RK3
+// step sequence (MRISplitIntegrator::advance, TimeIntegration/ERF_MRI.H:187-369)
+// and its CUDA-graph replay.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace erfb {
+__global__ void k_step_begin(Params P, const double* cons, const double* uo, const double* vo, const double* wo,
+                             StateBuf S, double* un, double* vn, double* wn, StageAux A, double* mut);
+__global__ void k_tau(Params P, const double* cons, const double* u, const double* v, const double* w,
+                      const double* mut, double* t11, double* t22, double* t33, double* t12, double* t13, double* t23);
+__global__ void k_slow_cell(Params P, StateBuf S, StageAux A, const double* mut, double* Fcons, double* avx,
+                            double* avy, double* avz);
+__global__ void k_plane_avg(Params P, const double* cons, const double* prim, double* avg);
+__global__ void k_slow_mom(Params P, StateBuf S, StageAux A, const double* u, const double* v, const double* w,
+                           const double* t11, const double* t22, const double* t33, const double* t12,
+                           const double* t13, const double* t23, const double* pavg, double* Fmx, double* Fmy,
+                           double* Fmz);
+__global__ void k_fast_h(Params P, int step, int nrk, double dtau, double facinv, StateBuf Sprev, int prev_rt,
+                         StateBuf Sst, StageAux A, const double* Fmx, const double* Fmy, const double* lag_in,
+                         double* lag_out, double* avx, double* avy, double* outx, double* outy);
+__global__ void k_fast_col(Params P, int step, double dtau, double facinv, double D, double beta_1, double beta_2,
+                           StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux A, const double* Fcons,
+                           const double* Fmz, const double* newx, const double* newy, double* avz, double* out_cons,
+                           double* out_mz, double* sc_soln, double* sc_cb, double* sc_tr0, double* sc_tr1);
+__global__ void k_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
+                       StageAux Acur, StageAux Anext, int make_next, const double* mut, const double* avx,
+                       const double* avy, const double* avz, double* un, double* vn, double* wn);
+__global__ void k_kessler(Params P, double* cons, double dtn, double dz);
+__global__ void k_base_state(int nz, double dz, double g, double rdOcp, const double* th_cc, const double* qv_cc,
+                             double th_s, double qv_s, double p_s, double* rho0, double* p0o, double* pi0o,
+                             double* th0o);
+__global__ void k_pack(Geo g, erf_b200_fab f, int kind, int ncomp, double* dst);
+__global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const double* src, int tang_lo_zero,
+                         int tang_hi_zero);
+}  // namespace erfb
+
+using namespace erfb;
+
+struct erf_b200_ctx {
+    erf_b200_config cfg;
+    Params P;
+    Geo g;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    StateBuf S[4];            // [0],[1] alternate old/new, [2] second stage buffer, [3] fast sum
+    double* vel[2][3];        // alternating old/new face velocities
+    double *Fcons, *Fmx, *Fmy, *Fmz;
+    double *avx, *avy, *avz;
+    double* lag[2];
+    StageAux aux[2];
+    double* mut;
+    double *t11, *t22, *t33, *t12, *t13, *t23;
+    double* pavg;
+    double *sc_soln, *sc_cb, *sc_tr0, *sc_tr1;
+    double *r0, *p0, *pi0, *th0;
+    double *h_stage;          // device staging buffers for the host-array entry point
+    int* status;
+    bool base_set = false;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int lag_parity_per_step = 0;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+    if (e == cudaSuccess) return ERF_B200_OK;
+    return e == cudaErrorMemoryAllocation ? ERF_B200_ENOMEM : ERF_B200_ECUDA;
+}
+#define CK(x)                                   \
+    do {                                        \
+        cudaError_t e_ = (x);                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_); \
+    } while (0)
+
+int dalloc(erf_b200_ctx* c, double** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(e);
+    cudaMemsetAsync(q, 0, n * sizeof(double), c->stream);
+    c->allocs.push_back(q);
+    c->bytes += n * sizeof(double);
+    *p = (double*)q;
+    return ERF_B200_OK;
+}
+
+bool adv_supported(int t) {
+    return t == ERF_ADV_CENTERED_2ND || t == ERF_ADV_UPWIND_3RD || t == ERF_ADV_CENTERED_4TH ||
+           t == ERF_ADV_UPWIND_5TH || t == ERF_ADV_CENTERED_6TH || t == ERF_ADV_WENO_3 || t == ERF_ADV_WENO_5;
+}
+
+int validate(const erf_b200_config* c) {
+    if (!c) return ERF_B200_EINVAL;
+    if (c->nx < 4 || c->ny < 4 || c->nz < 4) return ERF_B200_ECONFIG;
+    if (!(c->dx > 0 && c->dy > 0 && c->dz > 0 && c->dt > 0)) return ERF_B200_ECONFIG;
+    if (c->mri_ratio < 2 || (c->mri_ratio % 2) != 0) return ERF_B200_ECONFIG;
+    if (c->zlo_bc != ERF_BC_NO_SLIP_WALL && c->zlo_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
+    if (c->zhi_bc != ERF_BC_NO_SLIP_WALL && c->zhi_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
+    // the vertical momentum stencils reduce order near walls only for the
+    // Upwind/Centered family (ERF_AdvectionSrcForMom_N.H:225-265)
+    if (!adv_supported(c->dycore_horiz_adv) || !adv_supported(c->dycore_vert_adv)) return ERF_B200_ECONFIG;
+    if (c->dycore_horiz_adv == ERF_ADV_WENO_3 || c->dycore_horiz_adv == ERF_ADV_WENO_5) return ERF_B200_ECONFIG;
+    if (c->dycore_vert_adv == ERF_ADV_WENO_3 || c->dycore_vert_adv == ERF_ADV_WENO_5) return ERF_B200_ECONFIG;
+    if (c->dycore_horiz_adv == ERF_ADV_CENTERED_2ND && c->dycore_vert_adv == ERF_ADV_CENTERED_2ND) return ERF_B200_ECONFIG;
+    if (!adv_supported(c->dryscal_horiz_adv) || !adv_supported(c->dryscal_vert_adv)) return ERF_B200_ECONFIG;
+    if (!adv_supported(c->moistscal_horiz_adv) || !adv_supported(c->moistscal_vert_adv)) return ERF_B200_ECONFIG;
+    if (c->les_type != ERF_LES_NONE && c->les_type != ERF_LES_SMAGORINSKY) return ERF_B200_ECONFIG;
+    if (c->molec_diff_type < 0 || c->molec_diff_type > 2) return ERF_B200_ECONFIG;
+    if (c->moisture == ERF_MOIST_NONE) {
+        if (c->ncomp != 5) return ERF_B200_ECONFIG;
+    } else if (c->moisture == ERF_MOIST_KESSLER) {
+        if (c->ncomp != 8) return ERF_B200_ECONFIG;
+    } else if (c->moisture == ERF_MOIST_KESSLER_NORAIN) {
+        if (c->ncomp != 7 || c->buoyancy_type != 1) return ERF_B200_ECONFIG;
+    } else {
+        return ERF_B200_ECONFIG;
+    }
+    if (c->buoyancy_type != 1 && c->buoyancy_type != 2 && c->buoyancy_type != 3) return ERF_B200_ECONFIG;
+    if (c->precision != ERF_PREC_FP64) return ERF_B200_ECONFIG;
+    return ERF_B200_OK;
+}
+
+void make_params(erf_b200_ctx* c) {
+    const erf_b200_config& f = c->cfg;
+    Geo& g = c->g;
+    g.nx = f.nx; g.ny = f.ny; g.nz = f.nz;
+    g.sk = (int64_t)f.nx * f.ny;
+    g.ncell = g.sk * f.nz;
+    g.nzf = g.sk * (f.nz + 1);
+    g.dxi = 1.0 / f.dx; g.dyi = 1.0 / f.dy; g.dzi = 1.0 / f.dz;
+    g.zlo_noslip = f.zlo_bc == ERF_BC_NO_SLIP_WALL;
+    g.zhi_noslip = f.zhi_bc == ERF_BC_NO_SLIP_WALL;
+    Params& P = c->P;
+    P.g = g;
+    P.ncomp = f.ncomp; P.nprim = f.ncomp - 1;
+    P.moist = f.moisture != ERF_MOIST_NONE;
+    P.kessler_rain = f.moisture == ERF_MOIST_KESSLER;
+    P.use_turb = f.les_type != ERF_LES_NONE;
+    P.use_diff = (f.molec_diff_type != ERF_MOLEC_NONE) || P.use_turb;
+    P.use_consA = f.molec_diff_type == ERF_MOLEC_CONSTANT_ALPHA;
+    P.les = f.les_type;
+    // Smagorinsky length scale in the reference's order
+    // (ERF_ComputeTurbulentViscosity.cpp:95-97), with map factors 1
+    double cellVolMsf = 1.0 / (g.dxi * 1.0 * g.dyi * 1.0 * g.dzi);
+    double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
+    P.CsDeltaSqr = f.Cs * f.Cs * DeltaMsf * DeltaMsf;
+    P.invPr = 1.0 / f.Pr_t;
+    P.invSc = 1.0 / f.Sc_t;
+    P.alphaT_eff = P.use_consA ? f.alpha_T : f.rho0_trans * f.alpha_T;
+    P.alphaC_eff = P.use_consA ? f.alpha_C : f.rho0_trans * f.alpha_C;
+    P.mu_eff = P.use_consA ? 2.0 * f.dynamic_viscosity / f.rho0_trans : 2.0 * f.dynamic_viscosity;
+    P.gravity = f.gravity;
+    P.rdOcp = R_d / f.c_p;
+    P.c_p = f.c_p;
+    P.c_v = f.c_p - R_d;
+    P.halfg = std::abs(0.5 * -f.gravity);
+    P.buoy_type = f.buoyancy_type;
+    P.coriolis = f.use_coriolis;
+    P.cf = f.coriolis_factor; P.sinphi = f.sinphi; P.cosphi = f.cosphi;
+    P.geo0 = f.abl_geo_forcing[0]; P.geo1 = f.abl_geo_forcing[1]; P.geo2 = f.abl_geo_forcing[2];
+    P.dyc_h = f.dycore_horiz_adv; P.dyc_v = f.dycore_vert_adv;
+    P.dry_h = f.dryscal_horiz_adv; P.dry_v = f.dryscal_vert_adv;
+    P.moi_h = f.moistscal_horiz_adv; P.moi_v = f.moistscal_vert_adv;
+    P.f_dyc_h = f.dycore_horiz_upw_frac; P.f_dyc_v = f.dycore_vert_upw_frac;
+    P.f_dry_h = f.dryscal_horiz_upw_frac; P.f_dry_v = f.dryscal_vert_upw_frac;
+    P.f_moi_h = f.moistscal_horiz_upw_frac; P.f_moi_v = f.moistscal_vert_upw_frac;
+    P.r0 = c->r0; P.p0 = c->p0; P.pi0 = c->pi0;
+    P.status = c->status;
+}
+
+dim3 cell_block() { return dim3(32, 4, 1); }
+dim3 cell_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.nz); }
+dim3 col_block() { return dim3(32, 4, 1); }
+dim3 col_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, 1); }
+
+// Substep schedule of MRISplitIntegrator::advance (ERF_MRI.H:255-282)
+void stage_schedule(const erf_b200_config& f, int nrk, int& nsub, double& dtau, double& slow_dt) {
+    double dt = f.dt;
+    double sub_dt = dt / f.mri_ratio;
+    if (nrk == 0) {
+        if (f.force_stage1_single_substep) { nsub = 1; dtau = dt / 3.0; }
+        else { nsub = f.mri_ratio / 3; dtau = sub_dt; }
+        slow_dt = dt / 3.0;
+    } else if (nrk == 1) {
+        nsub = f.mri_ratio / 2; dtau = sub_dt; slow_dt = dt / 2.0;
+    } else {
+        nsub = f.mri_ratio; dtau = sub_dt; slow_dt = dt;
+    }
+}
+
+int substeps_per_step(const erf_b200_config& f) {
+    int tot = 0;
+    for (int nrk = 0; nrk < 3; ++nrk) { int n; double a, b; stage_schedule(f, nrk, n, a, b); tot += n; }
+    return tot;
+}
+
+// Enqueue one full step with parity p (state slot p is the old state).
+void enqueue_step(erf_b200_ctx* c, int p) {
+    const Params& P = c->P;
+    const Geo& g = c->g;
+    cudaStream_t st = c->stream;
+    StateBuf OLD = c->S[p], N0 = c->S[1 - p], N1 = c->S[2], SUM = c->S[3];
+    double** Vold = c->vel[p];
+    double** Vnew = c->vel[1 - p];
+    dim3 cb = cell_block(), cg = cell_grid(g), kb = col_block(), kg = col_grid(g);
+
+    k_step_begin<<<cg, cb, 0, st>>>(P, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
+                                    c->aux[0], c->mut);
+    StateBuf stage[3] = {OLD, N0, N1};
+    StateBuf outs[3] = {N0, N1, N0};
+    int a = 0;
+    int lp = (p * c->lag_parity_per_step) & 1;
+    const double beta_s = 0.1;
+    const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
+    for (int nrk = 0; nrk < 3; ++nrk) {
+        StateBuf Sst = stage[nrk], Snew = outs[nrk];
+        StageAux Acur = c->aux[a], Anext = c->aux[1 - a];
+        int nsub; double dtau, slow_dt;
+        stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
+        if (P.use_diff)
+            k_tau<<<cg, cb, 0, st>>>(P, Sst.cons, Vnew[0], Vnew[1], Vnew[2], c->mut, c->t11, c->t22, c->t33,
+                                     c->t12, c->t13, c->t23);
+        k_slow_cell<<<cg, cb, 0, st>>>(P, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz);
+        if (P.moist && P.buoy_type == 2)
+            k_plane_avg<<<g.nz, 256, 0, st>>>(P, Sst.cons, Acur.prim, c->pavg);
+        k_slow_mom<<<cg, cb, 0, st>>>(P, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33, c->t12,
+                                      c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz);
+        double facinv = 1.0 / (double)nsub;
+        double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
+        for (int ks = 0; ks < nsub; ++ks) {
+            StateBuf Sprev = (ks == 0) ? OLD : SUM;
+            int prt = ks > 0;
+            k_fast_h<<<cg, cb, 0, st>>>(P, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, c->Fmx, c->Fmy, c->lag[lp],
+                                        c->lag[1 - lp], c->avx, c->avy, SUM.mx, SUM.my);
+            lp ^= 1;
+            k_fast_col<<<kg, kb, 0, st>>>(P, ks, dtau, facinv, D, beta_1, beta_2, Sprev, prt, Sst, Acur, c->Fcons,
+                                          c->Fmz, SUM.mx, SUM.my, c->avz, SUM.cons, SUM.mz, c->sc_soln, c->sc_cb,
+                                          c->sc_tr0, c->sc_tr1);
+        }
+        k_post<<<cg, cb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut, c->avx,
+                                  c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2]);
+        a = 1 - a;
+    }
+    if (P.moist) k_kessler<<<kg, kb, 0, st>>>(P, N0.cons, c->cfg.dt, c->cfg.dz);
+}
+
+int build_graphs(erf_b200_ctx* c) {
+    for (int p = 0; p < 2; ++p) {
+        if (c->graph[p]) continue;
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(c, p);
+        CK(cudaStreamEndCapture(c->stream, &gr));
+        cudaError_t e = cudaGraphInstantiate(&c->graph[p], gr, 0);
+        cudaGraphDestroy(gr);
+        CK(e);
+    }
+    return ERF_B200_OK;
+}
+
+bool fab_ok(const erf_b200_fab* f, int kind, const Geo& g, int ncomp) {
+    if (!f || !f->p) return false;
+    int hx = g.nx - 1 + (kind == 1), hy = g.ny - 1 + (kind == 2), hz = g.nz - 1 + (kind == 3);
+    if (f->lo[0] > 0 || f->lo[1] > 0 || f->lo[2] > 0) return false;
+    if (f->hi[0] < hx || f->hi[1] < hy || f->hi[2] < hz) return false;
+    if (f->ncomp < ncomp) return false;
+    return true;
+}
+
+int pack(erf_b200_ctx* c, const erf_b200_fab* f, int kind, int ncomp, double* dst) {
+    const Geo& g = c->g;
+    dim3 b(32, 4, 1), gr((g.nx + 31) / 32, (g.ny + 3) / 4, kind == 3 ? g.nz + 1 : g.nz);
+    k_pack<<<gr, b, 0, c->stream>>>(g, *f, kind, ncomp, dst);
+    return cuda_fail(cudaGetLastError());
+}
+int unpack(erf_b200_ctx* c, const erf_b200_fab* f, int kind, int ncomp, const double* src) {
+    const Geo& g = c->g;
+    int nxb = f->hi[0] - f->lo[0] + 1, nyb = f->hi[1] - f->lo[1] + 1, nzb = f->hi[2] - f->lo[2] + 1;
+    dim3 b(32, 4, 1), gr((nxb + 31) / 32, (nyb + 3) / 4, nzb);
+    k_unpack<<<gr, b, 0, c->stream>>>(g, *f, kind, ncomp, src, g.zlo_noslip, g.zhi_noslip);
+    return cuda_fail(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+int erf_b200_config_defaults(erf_b200_config* cfg) {
+    if (!cfg) return ERF_B200_EINVAL;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->nx = cfg->ny = cfg->nz = 16;
+    cfg->dx = cfg->dy = cfg->dz = 1.0;
+    cfg->zlo_bc = cfg->zhi_bc = ERF_BC_SLIP_WALL;
+    cfg->dt = 1.0;
+    cfg->mri_ratio = 6;
+    cfg->force_stage1_single_substep = 1;
+    cfg->ncomp = 5;
+    cfg->dycore_horiz_adv = cfg->dycore_vert_adv = ERF_ADV_UPWIND_3RD;
+    cfg->dryscal_horiz_adv = cfg->dryscal_vert_adv = ERF_ADV_UPWIND_3RD;
+    cfg->moistscal_horiz_adv = cfg->moistscal_vert_adv = ERF_ADV_WENO_3;
+    cfg->dycore_horiz_upw_frac = cfg->dycore_vert_upw_frac = 1.0;
+    cfg->dryscal_horiz_upw_frac = cfg->dryscal_vert_upw_frac = 1.0;
+    cfg->moistscal_horiz_upw_frac = cfg->moistscal_vert_upw_frac = 1.0;
+    cfg->molec_diff_type = ERF_MOLEC_CONSTANT;
+    cfg->rho0_trans = 1.0;
+    cfg->Pr_t = 1.0 / 3.0;
+    cfg->Sc_t = 1.0;
+    cfg->Ck = 0.1;
+    cfg->Ce = 0.93;
+    cfg->sigma_k = 0.5;
+    cfg->theta_ref = 300.0;
+    cfg->c_p = Cp_d;
+    cfg->buoyancy_type = 1;
+    return ERF_B200_OK;
+}
+
+int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream) {
+    if (!out) return ERF_B200_EINVAL;
+    *out = nullptr;
+    int v = validate(cfg);
+    if (v != ERF_B200_OK) return v;
+    erf_b200_ctx* c = new (std::nothrow) erf_b200_ctx();
+    if (!c) return ERF_B200_ENOMEM;
+    c->cfg = *cfg;
+    cudaGetDevice(&c->device);
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return ERF_B200_ECUDA; }
+        c->own_stream = true;
+    }
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    const int64_t NZF = (int64_t)cfg->nx * cfg->ny * (cfg->nz + 1);
+    const int nc = cfg->ncomp;
+    int rc = ERF_B200_OK;
+    auto A = [&](double** p, size_t n) { if (rc == ERF_B200_OK) rc = dalloc(c, p, n); };
+    for (int s = 0; s < 4; ++s) {
+        A(&c->S[s].cons, nc * N); A(&c->S[s].mx, N); A(&c->S[s].my, N); A(&c->S[s].mz, NZF);
+    }
+    for (int p = 0; p < 2; ++p) { A(&c->vel[p][0], N); A(&c->vel[p][1], N); A(&c->vel[p][2], NZF); }
+    A(&c->Fcons, 2 * N); A(&c->Fmx, N); A(&c->Fmy, N); A(&c->Fmz, NZF);
+    A(&c->avx, N); A(&c->avy, N); A(&c->avz, NZF);
+    A(&c->lag[0], N); A(&c->lag[1], N);
+    for (int p = 0; p < 2; ++p) { A(&c->aux[p].prim, (nc - 1) * N); A(&c->aux[p].pi, N); A(&c->aux[p].pp, N); }
+    A(&c->mut, N);
+    A(&c->t11, N); A(&c->t22, N); A(&c->t33, N); A(&c->t12, N); A(&c->t13, NZF); A(&c->t23, NZF);
+    A(&c->pavg, 5 * cfg->nz);
+    A(&c->sc_soln, N); A(&c->sc_cb, N); A(&c->sc_tr0, N); A(&c->sc_tr1, N);
+    A(&c->r0, cfg->nz + 2); A(&c->p0, cfg->nz + 2); A(&c->pi0, cfg->nz + 2); A(&c->th0, cfg->nz + 2);
+    if (rc == ERF_B200_OK) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, sizeof(int)) != cudaSuccess) rc = ERF_B200_ENOMEM;
+        else { c->allocs.push_back(q); c->status = (int*)q; cudaMemsetAsync(q, 0, sizeof(int), c->stream); }
+    }
+    if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
+    make_params(c);
+    c->lag_parity_per_step = substeps_per_step(c->cfg) & 1;
+    rc = build_graphs(c);
+    if (rc == ERF_B200_OK) rc = cuda_fail(cudaStreamSynchronize(c->stream));
+    if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
+    *out = c;
+    return ERF_B200_OK;
+}
+
+int erf_b200_destroy(erf_b200_ctx* c) {
+    if (!c) return ERF_B200_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int p = 0; p < 2; ++p) if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
+    for (void* q : c->allocs) cudaFree(q);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ERF_B200_OK;
+}
+
+int erf_b200_set_stream(erf_b200_ctx* c, void* stream) {
+    if (!c) return ERF_B200_EINVAL;
+    if (!stream) return ERF_B200_EINVAL;
+    cudaStreamSynchronize(c->stream);
+    if (c->own_stream) { cudaStreamDestroy(c->stream); c->own_stream = false; }
+    c->stream = (cudaStream_t)stream;
+    return ERF_B200_OK;
+}
+
+int erf_b200_get_status(erf_b200_ctx* c) {
+    if (!c) return ERF_B200_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    int h = 0;
+    CK(cudaMemcpy(&h, c->status, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemset(c->status, 0, sizeof(int)));
+    if (h & ST_NAN) return ERF_B200_ENAN;
+    if (h & ST_BADSTATE) return ERF_B200_EBADSTATE;
+    return ERF_B200_OK;
+}
+
+int erf_b200_scratch_bytes(const erf_b200_ctx* c, size_t* bytes) {
+    if (!c || !bytes) return ERF_B200_EINVAL;
+    *bytes = c->bytes;
+    return ERF_B200_OK;
+}
+
+int erf_b200_make_base_state(erf_b200_ctx* c, const double* theta_cc, const double* qv_cc, double theta_sfc,
+                             double qv_sfc, double p_sfc, double* rho0, double* p0, double* pi0, double* th0) {
+    if (!c || !theta_cc || !qv_cc || !rho0 || !p0 || !pi0 || !th0) return ERF_B200_EINVAL;
+    k_base_state<<<1, 1, 0, c->stream>>>(c->cfg.nz, c->cfg.dz, c->cfg.gravity, R_d / c->cfg.c_p, theta_cc, qv_cc,
+                                         theta_sfc, qv_sfc, p_sfc, rho0, p0, pi0, th0);
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_set_base_state(erf_b200_ctx* c, const double* rho0, const double* p0, const double* pi0,
+                            const double* th0) {
+    if (!c || !rho0 || !p0 || !pi0 || !th0) return ERF_B200_EINVAL;
+    size_t b = (c->cfg.nz + 2) * sizeof(double);
+    CK(cudaMemcpyAsync(c->r0, rho0, b, cudaMemcpyDefault, c->stream));
+    CK(cudaMemcpyAsync(c->p0, p0, b, cudaMemcpyDefault, c->stream));
+    CK(cudaMemcpyAsync(c->pi0, pi0, b, cudaMemcpyDefault, c->stream));
+    CK(cudaMemcpyAsync(c->th0, th0, b, cudaMemcpyDefault, c->stream));
+    c->base_set = true;
+    return ERF_B200_OK;
+}
+
+int erf_b200_advance(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                     const erf_b200_fab* yvel, const erf_b200_fab* zvel, int nsteps) {
+    if (!c || nsteps < 0) return ERF_B200_EINVAL;
+    if (!c->base_set) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
+        return ERF_B200_EINVAL;
+    int rc;
+    if ((rc = pack(c, cons, 0, c->cfg.ncomp, c->S[0].cons))) return rc;
+    if ((rc = pack(c, xvel, 1, 1, c->vel[0][0]))) return rc;
+    if ((rc = pack(c, yvel, 2, 1, c->vel[0][1]))) return rc;
+    if ((rc = pack(c, zvel, 3, 1, c->vel[0][2]))) return rc;
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph[s & 1], c->stream));
+    int p = nsteps & 1;
+    if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[p].cons))) return rc;
+    if ((rc = unpack(c, xvel, 1, 1, c->vel[p][0]))) return rc;
+    if ((rc = unpack(c, yvel, 2, 1, c->vel[p][1]))) return rc;
+    if ((rc = unpack(c, zvel, 3, 1, c->vel[p][2]))) return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_advance_host(erf_b200_ctx* c, double* cons, double* u, double* v, double* w, int nsteps) {
+    if (!c || !cons || !u || !v || !w) return ERF_B200_EINVAL;
+    const erf_b200_config& f = c->cfg;
+    const int64_t nc = f.ncomp, nx = f.nx, ny = f.ny, nz = f.nz;
+    const int64_t ncons = nc * nx * ny * nz, nu = (nx + 1) * ny * nz, nv = nx * (ny + 1) * nz, nw = nx * ny * (nz + 1);
+    if (!c->h_stage) {
+        int rc = dalloc(c, &c->h_stage, ncons + nu + nv + nw);
+        if (rc) return rc;
+    }
+    double* dc = c->h_stage;
+    double* du = dc + ncons;
+    double* dv = du + nu;
+    double* dw = dv + nv;
+    CK(cudaMemcpyAsync(dc, cons, ncons * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(du, u, nu * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dv, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dw, w, nw * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    auto mk = [&](double* p, int hx, int hy, int hz, int ncomp) {
+        erf_b200_fab fb;
+        fb.p = p; fb.lo[0] = fb.lo[1] = fb.lo[2] = 0; fb.hi[0] = hx; fb.hi[1] = hy; fb.hi[2] = hz;
+        fb.jstride = hx + 1; fb.kstride = (int64_t)(hx + 1) * (hy + 1); fb.nstride = fb.kstride * (hz + 1);
+        fb.ncomp = ncomp;
+        return fb;
+    };
+    erf_b200_fab fc = mk(dc, nx - 1, ny - 1, nz - 1, nc), fu = mk(du, nx, ny - 1, nz - 1, 1),
+                 fv = mk(dv, nx - 1, ny, nz - 1, 1), fw = mk(dw, nx - 1, ny - 1, nz, 1);
+    int rc = erf_b200_advance(c, &fc, &fu, &fv, &fw, nsteps);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(cons, dc, ncons * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(u, du, nu * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(v, dv, nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(w, dw, nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ERF_B200_OK;
+}
+
+// Per-pass entry points that are not yet exposed separately from the fused
+// step return ERF_B200_EINVAL.
+int erf_b200_turbulent_viscosity(erf_b200_ctx*, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
+                                 const erf_b200_fab*) { return ERF_B200_EINVAL; }
+int erf_b200_slow_rhs_pre(erf_b200_ctx*, int, double, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
+                          const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*) { return ERF_B200_EINVAL; }
+int erf_b200_make_fast_coeffs(erf_b200_ctx*, const erf_b200_fab*, const erf_b200_fab*, double) { return ERF_B200_EINVAL; }
+int erf_b200_fast_rhs_N(erf_b200_ctx*, int, int, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
+                        const erf_b200_fab*, const erf_b200_fab*, double, double) { return ERF_B200_EINVAL; }
+int erf_b200_slow_rhs_post(erf_b200_ctx*, int, double, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
+                           const erf_b200_fab*, const erf_b200_fab*) { return ERF_B200_EINVAL; }
+int erf_b200_kessler_advance(erf_b200_ctx* c, const erf_b200_fab* cons, double dt) {
+    if (!c || !c->P.moist) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab_ok(cons, 0, g, c->cfg.ncomp)) return ERF_B200_EINVAL;
+    int rc;
+    if ((rc = pack(c, cons, 0, c->cfg.ncomp, c->S[2].cons))) return rc;
+    k_kessler<<<col_grid(g), col_block(), 0, c->stream>>>(c->P, c->S[2].cons, dt, c->cfg.dz);
+    if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[2].cons))) return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
+}  // extern "C"

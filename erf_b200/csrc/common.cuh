@@ -1,0 +1,217 @@
+// common.cuh -- device-side constants, equation of state, face interpolants
+// and periodic/wall index helpers shared by the dycore kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/erf_b200.h"
+
+namespace erfb {
+
+// Physical constants (reference: Source/ERF_Constants.H:10-30, 66-87)
+constexpr double R_d = 287.0;
+constexpr double R_v = 461.505;
+constexpr double Cp_d = 1004.5;
+constexpr double p_0 = 1.0e5;
+constexpr double Gamma_ = 1.4;
+constexpr double ip_0 = 1. / p_0;
+constexpr double iR_d = 1. / R_d;
+constexpr double iGamma = 1. / Gamma_;
+constexpr double L_v = 2.5e6;
+constexpr double lcond = 2.501e6;
+constexpr double Rd_on_Rv = R_d / R_v;
+
+// Status bits written by kernels (OR-ed into ctx->status)
+constexpr int ST_BADSTATE = 1;
+constexpr int ST_NAN = 2;
+
+// ---------------------------------------------------------------------------
+// Equation of state (reference: Source/Utils/ERF_EOS.H:42-151).  Same
+// association of the operands as the reference so FP64 results agree to ulps.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double eos_p(double rt, double qv) {
+    return p_0 * pow(R_d * rt * (1.0 + (R_v / R_d) * qv) * ip_0, Gamma_);
+}
+__device__ __forceinline__ double eos_exner(double rt, double rdOcp) {
+    return pow(R_d * rt * (1.0 + R_v / R_d * 0.0) * ip_0, Gamma_ * rdOcp);
+}
+__device__ __forceinline__ double eos_T(double rho, double rt, double qv) {
+    double p_loc = p_0 * pow(R_d * rt * (1.0 + R_v / R_d * qv) * ip_0, Gamma_);
+    return p_loc / (R_d * rho * (1.0 + R_v / R_d * qv));
+}
+__device__ __forceinline__ double eos_rho_given_theta_p(double theta, double p, double rdOcp, double qv) {
+    return pow(p_0, rdOcp) * pow(p, iGamma) / (R_d * theta * (1.0 + R_v / R_d * qv));
+}
+__device__ __forceinline__ double eos_exner_p(double P, double rdOcp) { return pow(P * ip_0, rdOcp); }
+__device__ __forceinline__ double eos_rt_given_p(double p) {
+    return pow(p * pow(p_0, Gamma_ - 1), iGamma) * iR_d / (1.0 + R_v / R_d * 0.0);
+}
+
+// ---------------------------------------------------------------------------
+// Face interpolants (reference: Source/Utils/ERF_Interpolation_UPW.H:9-611,
+// ERF_Interpolation_WENO.H:9-259).  s[0..5] = phi at offsets -3..+2 from the
+// face's high-side cell; upw is the advecting momentum on the face.
+// ---------------------------------------------------------------------------
+template <int TYPE>
+struct Interp;
+
+template <>
+struct Interp<ERF_ADV_CENTERED_2ND> {
+    static constexpr int W = 1;
+    __device__ static __forceinline__ double eval(const double* s, double, double) { return 0.5 * (s[3] + s[2]); }
+};
+template <>
+struct Interp<ERF_ADV_UPWIND_3RD> {
+    static constexpr int W = 2;
+    __device__ static __forceinline__ double eval(const double* s, double upw, double frac) {
+        if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+        upw *= frac;
+        double a1 = s[3] + s[2], d1 = s[3] - s[2], a2 = s[4] + s[1], d2 = s[4] - s[1];
+        return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2 + upw * (1.0 / 12.0) * (d2 - 3.0 * d1);
+    }
+};
+template <>
+struct Interp<ERF_ADV_CENTERED_4TH> {
+    static constexpr int W = 2;
+    __device__ static __forceinline__ double eval(const double* s, double, double) {
+        double a1 = s[3] + s[2], a2 = s[4] + s[1];
+        return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2;
+    }
+};
+template <>
+struct Interp<ERF_ADV_UPWIND_5TH> {
+    static constexpr int W = 3;
+    __device__ static __forceinline__ double eval(const double* s, double upw, double frac) {
+        if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+        upw *= frac;
+        double a1 = s[3] + s[2], a2 = s[4] + s[1], a3 = s[5] + s[0];
+        double d1 = s[3] - s[2], d2 = s[4] - s[1], d3 = s[5] - s[0];
+        return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3 - upw * (1.0 / 60.0) * (d3 - 5.0 * d2 + 10.0 * d1);
+    }
+};
+template <>
+struct Interp<ERF_ADV_CENTERED_6TH> {
+    static constexpr int W = 3;
+    __device__ static __forceinline__ double eval(const double* s, double, double) {
+        double a1 = s[3] + s[2], a2 = s[4] + s[1], a3 = s[5] + s[0];
+        return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3;
+    }
+};
+template <>
+struct Interp<ERF_ADV_WENO_3> {
+    static constexpr int W = 2;
+    __device__ static __forceinline__ double ev(double a, double b, double c) {
+        const double eps = 1.0e-6;
+        double b1 = (b - a) * (b - a), b2 = (c - b) * (c - b);
+        double w1 = (1.0 / 3.0) / ((eps + b1) * (eps + b1));
+        double w2 = (2.0 / 3.0) / ((eps + b2) * (eps + b2));
+        double ws = w1 + w2;
+        double v1 = -a + 3.0 * b, v2 = b + c;
+        return (w1 * v1 + w2 * v2) / (2.0 * ws);
+    }
+    __device__ static __forceinline__ double eval(const double* s, double upw, double) {
+        const double tol = 1.0e-12;
+        if (upw > tol) return ev(s[1], s[2], s[3]);
+        if (upw < -tol) return ev(s[4], s[3], s[2]);
+        return 0.5 * (s[3] + s[2]);
+    }
+};
+template <>
+struct Interp<ERF_ADV_WENO_5> {
+    static constexpr int W = 3;
+    __device__ static __forceinline__ double ev(double a, double b, double c, double d, double e) {
+        const double c1 = 13.0 / 12.0, eps = 1.0e-6;
+        double b1 = c1 * (a - 2.0 * b + c) * (a - 2.0 * b + c) + 0.25 * (a - 4.0 * b + 3.0 * c) * (a - 4.0 * b + 3.0 * c);
+        double b2 = c1 * (b - 2.0 * c + d) * (b - 2.0 * c + d) + 0.25 * (b - d) * (b - d);
+        double b3 = c1 * (c - 2.0 * d + e) * (c - 2.0 * d + e) + 0.25 * (3.0 * c - 4.0 * d + e) * (3.0 * c - 4.0 * d + e);
+        double w1 = (1.0 / 10.0) / ((eps + b1) * (eps + b1));
+        double w2 = (3.0 / 5.0) / ((eps + b2) * (eps + b2));
+        double w3 = (3.0 / 10.0) / ((eps + b3) * (eps + b3));
+        double ws = w1 + w2 + w3;
+        double v1 = 2.0 * a - 7.0 * b + 11.0 * c;
+        double v2 = -b + 5.0 * c + 2.0 * d;
+        double v3 = 2.0 * c + 5.0 * d - e;
+        return (w1 * v1 + w2 * v2 + w3 * v3) / (6.0 * ws);
+    }
+    __device__ static __forceinline__ double eval(const double* s, double upw, double) {
+        const double tol = 1.0e-12;
+        if (upw > tol) return ev(s[0], s[1], s[2], s[3], s[4]);
+        if (upw < -tol) return ev(s[5], s[4], s[3], s[2], s[1]);
+        return 0.5 * (s[3] + s[2]);
+    }
+};
+
+// Runtime dispatch over the supported interpolant codes
+__device__ __forceinline__ double interp_rt(int type, const double* s, double upw, double frac) {
+    switch (type) {
+    case ERF_ADV_CENTERED_2ND: return Interp<ERF_ADV_CENTERED_2ND>::eval(s, upw, frac);
+    case ERF_ADV_UPWIND_3RD: return Interp<ERF_ADV_UPWIND_3RD>::eval(s, upw, frac);
+    case ERF_ADV_CENTERED_4TH: return Interp<ERF_ADV_CENTERED_4TH>::eval(s, upw, frac);
+    case ERF_ADV_UPWIND_5TH: return Interp<ERF_ADV_UPWIND_5TH>::eval(s, upw, frac);
+    case ERF_ADV_CENTERED_6TH: return Interp<ERF_ADV_CENTERED_6TH>::eval(s, upw, frac);
+    case ERF_ADV_WENO_3: return Interp<ERF_ADV_WENO_3>::eval(s, upw, frac);
+    case ERF_ADV_WENO_5: return Interp<ERF_ADV_WENO_5>::eval(s, upw, frac);
+    default: return 0.0;
+    }
+}
+__host__ __device__ __forceinline__ int stencil_width(int type) {
+    switch (type) {
+    case ERF_ADV_CENTERED_2ND: return 1;
+    case ERF_ADV_UPWIND_3RD: case ERF_ADV_CENTERED_4TH: case ERF_ADV_WENO_3: return 2;
+    default: return 3;
+    }
+}
+
+// Wall-reduced vertical interpolant for w (UPWINDALL, reference
+// ERF_Interpolation_UPW.H:528-611); s entries outside the scheme's width are
+// ignored.
+__device__ __forceinline__ double interp_all(int type, const double* s, double upw, double frac) {
+    if (type == ERF_ADV_CENTERED_2ND) return 0.5 * (s[3] + s[2]);
+    bool wide = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH);
+    double sm3 = wide ? s[0] : 0., sp2 = wide ? s[5] : 0.;
+    if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+    upw *= frac;
+    double a1 = s[3] + s[2], a2 = s[4] + s[1], d1 = s[3] - s[2], d2 = s[4] - s[1];
+    double a3 = sp2 + sm3, d3 = sp2 - sm3;
+    if (type == ERF_ADV_UPWIND_3RD) return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2 + upw * (1.0 / 12.0) * (d2 - 3.0 * d1);
+    if (type == ERF_ADV_CENTERED_4TH) return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2;
+    if (type == ERF_ADV_UPWIND_5TH) return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3 - upw * (1.0 / 60.0) * (d3 - 5.0 * d2 + 10.0 * d1);
+    return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3;
+}
+
+// ---------------------------------------------------------------------------
+// Saturation over water: Flatau et al. (1992) Table 4 polynomials in Horner
+// form, as in the reference's Source/Utils/ERF_Microphysics_Utils.H:52-160.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double esatw(double t) {
+    double dtt = fmin(t - 273.16, 70.);
+    return 6.11239921 + dtt * (0.443987641 + dtt * (0.142986287e-1 + dtt * (0.264847430e-3 + dtt * (0.302950461e-5 + dtt * (0.206739458e-7 + dtt * (0.640689451e-10 + dtt * (-0.952447341e-13 + -0.976195544e-15 * dtt)))))));
+}
+__device__ __forceinline__ double dtesatw(double t) {
+    double dtt = t - 273.16;
+    if (dtt >= 70.) return 0.0;
+    return 0.443956472 + dtt * (0.285976452e-1 + dtt * (0.794747212e-3 + dtt * (0.121167162e-4 + dtt * (0.103167413e-6 + dtt * (0.385208005e-9 + dtt * (-0.604119582e-12 + dtt * (-0.792933209e-14 + -0.599634321e-17 * dtt)))))));
+}
+
+// ---------------------------------------------------------------------------
+// Geometry and array views.  Internal arrays hold the valid region only:
+// cells and x/y faces are nx*ny*nz (periodic faces: face nx == face 0),
+// z faces nx*ny*(nz+1).  Lateral neighbours wrap; vertical neighbours follow
+// the wall conditions.
+// ---------------------------------------------------------------------------
+struct Geo {
+    int nx, ny, nz;
+    int64_t sk;        // nx*ny
+    int64_t ncell;     // nx*ny*nz
+    int64_t nzf;       // nx*ny*(nz+1)
+    double dxi, dyi, dzi;
+    int zlo_noslip, zhi_noslip;
+};
+
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+__device__ __forceinline__ int clampk(int k, int nz) { return k < 0 ? 0 : (k >= nz ? nz - 1 : k); }
+__device__ __forceinline__ int64_t cidx(const Geo& g, int i, int j, int k) {
+    return (int64_t)i + (int64_t)g.nx * j + g.sk * k;
+}
+
+}  // namespace erfb

@@ -1,0 +1,168 @@
+"""Python host binding of the C-ABI (include/erf_b200.h) through ctypes.
+
+The product path is liberf_b200.so; there is no CPU fallback: constructing a
+Dycore without the built library or without a CUDA device raises.  Device
+memory for the Python-level entry points comes from torch tensors (plumbing
+only); all arithmetic runs in the library's kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import config as C
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liberf_b200.so")
+_lib = None
+
+ERRORS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "EBADSTATE", 5: "ENAN", 6: "EPIVOT",
+          7: "ETIMEOUT", 8: "ECONFIG"}
+
+EXPORTS = [
+    "erf_b200_config_defaults", "erf_b200_create", "erf_b200_destroy", "erf_b200_set_stream",
+    "erf_b200_get_status", "erf_b200_scratch_bytes", "erf_b200_make_base_state", "erf_b200_set_base_state",
+    "erf_b200_advance", "erf_b200_advance_host", "erf_b200_turbulent_viscosity", "erf_b200_slow_rhs_pre",
+    "erf_b200_make_fast_coeffs", "erf_b200_fast_rhs_N", "erf_b200_slow_rhs_post", "erf_b200_kessler_advance",
+]
+
+
+class ErfFab(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_void_p), ("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3),
+                ("jstride", ctypes.c_int64), ("kstride", ctypes.c_int64), ("nstride", ctypes.c_int64),
+                ("ncomp", ctypes.c_int)]
+
+
+class ErfError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what} failed: {ERRORS.get(code, code)}")
+        self.code = code
+
+
+def load_library():
+    """Load liberf_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m erf_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, i = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int
+    L.erf_b200_config_defaults.argtypes = [vp]
+    L.erf_b200_create.argtypes = [ctypes.POINTER(vp), vp, vp]
+    L.erf_b200_destroy.argtypes = [vp]
+    L.erf_b200_set_stream.argtypes = [vp, vp]
+    L.erf_b200_get_status.argtypes = [vp]
+    L.erf_b200_scratch_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.erf_b200_make_base_state.argtypes = [vp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           dp, dp, dp, dp]
+    L.erf_b200_set_base_state.argtypes = [vp, dp, dp, dp, dp]
+    fabp = ctypes.POINTER(ErfFab)
+    L.erf_b200_advance.argtypes = [vp, fabp, fabp, fabp, fabp, i]
+    L.erf_b200_advance_host.argtypes = [vp, dp, dp, dp, dp, i]
+    L.erf_b200_kessler_advance.argtypes = [vp, fabp, ctypes.c_double]
+    for name in EXPORTS:
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise ErfError(rc, what)
+
+
+def dense_fab(t, kind: int, nx: int, ny: int, nz: int, ncomp: int = 1) -> ErfFab:
+    """Array4 view of a dense contiguous device tensor (valid region only)."""
+    hx = nx - 1 + (kind == 1)
+    hy = ny - 1 + (kind == 2)
+    hz = nz - 1 + (kind == 3)
+    f = ErfFab()
+    f.p = t.data_ptr()
+    f.lo[0] = f.lo[1] = f.lo[2] = 0
+    f.hi[0], f.hi[1], f.hi[2] = hx, hy, hz
+    f.jstride = hx + 1
+    f.kstride = (hx + 1) * (hy + 1)
+    f.nstride = f.kstride * (hz + 1)
+    f.ncomp = ncomp
+    return f
+
+
+class Dycore:
+    """One dycore context on the current CUDA device."""
+
+    def __init__(self, cfg: C.ErfConfig, stream=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("erf_b200 needs a CUDA device")
+        self.lib = load_library()
+        self.cfg = cfg.copy()
+        self._ctx = ctypes.c_void_p()
+        s = ctypes.c_void_p(stream) if stream is not None else ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _check(self.lib.erf_b200_create(ctypes.byref(self._ctx), ctypes.byref(self.cfg), s), "erf_b200_create")
+        self.base = None
+
+    def close(self):
+        if self._ctx:
+            self.lib.erf_b200_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    def status(self) -> int:
+        return self.lib.erf_b200_get_status(self._ctx)
+
+    def scratch_bytes(self) -> int:
+        n = ctypes.c_size_t()
+        _check(self.lib.erf_b200_scratch_bytes(self._ctx, ctypes.byref(n)), "scratch_bytes")
+        return n.value
+
+    def make_base_state(self, case):
+        """FP64 hydrostatic base state computed on the GPU; returns 4 numpy arrays (nz+2)."""
+        import torch
+        nz = self.cfg.nz
+        th = torch.tensor(np.asarray(case.theta_cc, dtype=np.float64), device="cuda")
+        qv = torch.tensor(np.asarray(case.qv_cc, dtype=np.float64), device="cuda")
+        out = [torch.zeros(nz + 2, dtype=torch.float64, device="cuda") for _ in range(4)]
+        torch.cuda.synchronize()
+        _check(self.lib.erf_b200_make_base_state(self._ctx, th.data_ptr(), qv.data_ptr(), case.theta_sfc,
+                                                 case.qv_sfc, case.p_sfc, *[o.data_ptr() for o in out]),
+               "make_base_state")
+        torch.cuda.synchronize()
+        return [o.cpu().numpy() for o in out]
+
+    def set_base_state(self, base):
+        import torch
+        self._base_dev = [torch.tensor(np.asarray(b, dtype=np.float64), device="cuda") for b in base]
+        torch.cuda.synchronize()
+        _check(self.lib.erf_b200_set_base_state(self._ctx, *[b.data_ptr() for b in self._base_dev]),
+               "set_base_state")
+        _check(self.lib.erf_b200_get_status(self._ctx), "set_base_state sync")
+        self.base = base
+
+    def advance_host(self, cons, u, v, w, nsteps: int):
+        """Advance dense host arrays; returns new arrays (host buffers in, host buffers out)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in (cons, u, v, w)]
+        _check(self.lib.erf_b200_advance_host(self._ctx, *[a.ctypes.data for a in arrs], int(nsteps)),
+               "advance_host")
+        return tuple(arrs)
+
+    def advance(self, cons_t, u_t, v_t, w_t, nsteps: int):
+        """Advance dense device tensors in place (asynchronous on the context stream)."""
+        c = self.cfg
+        fc = dense_fab(cons_t, 0, c.nx, c.ny, c.nz, c.ncomp)
+        fu = dense_fab(u_t, 1, c.nx, c.ny, c.nz)
+        fv = dense_fab(v_t, 2, c.nx, c.ny, c.nz)
+        fw = dense_fab(w_t, 3, c.nx, c.ny, c.nz)
+        _check(self.lib.erf_b200_advance(self._ctx, ctypes.byref(fc), ctypes.byref(fu), ctypes.byref(fv),
+                                         ctypes.byref(fw), int(nsteps)), "advance")

@@ -1,0 +1,277 @@
+/*
+ * erf_b200.h -- C-ABI of the B200-native multirate RK3 dycore.
+ *
+ * The reference (ERF) exposes this hot path as free functions on AMReX
+ * MultiFab/Array4 objects, wired into MRISplitIntegrator through std::function
+ * hooks (Source/TimeIntegration/ERF_MRI.H:137-180, installed by
+ * Source/TimeIntegration/ERF_advance_dycore.cpp:285-302).  This header replaces
+ * those signatures with plain pointers, sizes and POD structs so that an
+ * AMReX-based caller can hand over fab.dataPtr() plus the box and strides
+ * zero-copy, and any other host language can bind it through its FFI.
+ *
+ * Conventions
+ *   - Every array is an erf_b200_fab: a device pointer to FP64 data in Array4
+ *     order (i fastest), the index box [lo, hi] the pointer covers (valid
+ *     region plus whatever ghost cells the caller allocated), and strides.
+ *     p[(i-lo.x) + (j-lo.y)*jstride + (k-lo.z)*kstride + n*nstride].
+ *   - Cell-centred data use cell indices 0..n-1; x-face data use face indices
+ *     0..nx (nodal in x), and likewise for y and z.
+ *   - All calls are asynchronous on the stream given to erf_b200_create (or
+ *     the stream passed per call where a call takes one).  Only
+ *     erf_b200_get_status synchronises.
+ *   - Every function returns an int status: ERF_B200_OK (0) or one of the
+ *     ERF_B200_E* codes below.  Nothing in the library aborts or exits.
+ */
+#ifndef ERF_B200_H
+#define ERF_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------------------
+ * Status codes
+ * ------------------------------------------------------------------------- */
+#define ERF_B200_OK               0
+#define ERF_B200_EINVAL           1   /* bad argument / unsupported option      */
+#define ERF_B200_ECUDA            2   /* a CUDA runtime call failed             */
+#define ERF_B200_ENOMEM           3   /* device allocation failed               */
+#define ERF_B200_EBADSTATE        4   /* non-positive rho*theta or rho seen     */
+#define ERF_B200_ENAN             5   /* NaN/Inf detected in the state          */
+#define ERF_B200_EPIVOT           6   /* vertical tridiagonal pivot ~ 0         */
+#define ERF_B200_ETIMEOUT         7   /* a bounded device wait ran out          */
+#define ERF_B200_ECONFIG          8   /* configuration rejected                 */
+
+/* ----------------------------------------------------------------------------
+ * Enumerations: numeric values match the reference's enums so that a caller
+ * can pass its own SolverChoice fields straight through.
+ * ------------------------------------------------------------------------- */
+/* AdvType (Source/ERF_IndexDefines.H): Centered_2nd=101 ... */
+#define ERF_ADV_CENTERED_2ND 101
+#define ERF_ADV_UPWIND_3RD   102
+#define ERF_ADV_CENTERED_4TH 103
+#define ERF_ADV_UPWIND_5TH   104
+#define ERF_ADV_CENTERED_6TH 105
+#define ERF_ADV_WENO_3       106
+#define ERF_ADV_WENO_3Z      107
+#define ERF_ADV_WENO_5       108
+#define ERF_ADV_WENO_5Z      109
+#define ERF_ADV_WENO_3MZQ    110
+#define ERF_ADV_WENO_7       111
+#define ERF_ADV_WENO_7Z      112
+
+/* LESType (Source/DataStructs/ERF_TurbStruct.H) */
+#define ERF_LES_NONE         0
+#define ERF_LES_SMAGORINSKY  1
+#define ERF_LES_DEARDORFF    2
+
+/* MolecDiffType (Source/DataStructs/ERF_DiffStruct.H) */
+#define ERF_MOLEC_NONE           0
+#define ERF_MOLEC_CONSTANT       1
+#define ERF_MOLEC_CONSTANT_ALPHA 2
+
+/* MoistureType subset */
+#define ERF_MOIST_NONE            0
+#define ERF_MOIST_KESSLER         1
+#define ERF_MOIST_KESSLER_NORAIN  2
+
+/* ERF_BC (Source/ERF_IndexDefines.H): vertical boundary kinds supported */
+#define ERF_BC_NO_SLIP_WALL  5
+#define ERF_BC_SLIP_WALL     6
+#define ERF_BC_PERIODIC      7
+
+/* Arithmetic of the bulk dycore */
+#define ERF_PREC_FP64        0   /* plain FP64 form                          */
+#define ERF_PREC_MIXED       1   /* FP32 bulk on perturbations, FP64 state   */
+
+/* Cell-centred component layout (Source/ERF_IndexDefines.H:36-48) */
+#define ERF_RHO_COMP        0
+#define ERF_RHOTHETA_COMP   1
+#define ERF_RHOKE_COMP      2
+#define ERF_RHOQKE_COMP     3
+#define ERF_RHOSCALAR_COMP  4
+#define ERF_RHOQ1_COMP      5
+
+/* ----------------------------------------------------------------------------
+ * Array4-style view
+ * ------------------------------------------------------------------------- */
+typedef struct erf_b200_fab {
+    double*  p;        /* device pointer to element (lo.x, lo.y, lo.z, 0)    */
+    int      lo[3];    /* inclusive index bounds covered by p               */
+    int      hi[3];
+    int64_t  jstride;  /* elements between j and j+1                        */
+    int64_t  kstride;  /* elements between k and k+1                        */
+    int64_t  nstride;  /* elements between components                       */
+    int      ncomp;
+} erf_b200_fab;
+
+/* ----------------------------------------------------------------------------
+ * Configuration: the SolverChoice / AdvChoice / DiffChoice / TurbChoice keys
+ * that the hot path reads (Source/DataStructs/ERF_DataStruct.H:80-580,
+ * ERF_AdvStruct.H:26-186, ERF_TurbStruct.H:29-210, ERF_DiffStruct.H:26-32),
+ * plus the grid and the fixed time step.  POD, passed by pointer.
+ * ------------------------------------------------------------------------- */
+typedef struct erf_b200_config {
+    /* grid: one box covering the domain, periodic in x and y */
+    int    nx, ny, nz;
+    double dx, dy, dz;
+    int    zlo_bc, zhi_bc;            /* ERF_BC_NO_SLIP_WALL / ERF_BC_SLIP_WALL */
+
+    /* time stepping: fixed_dt, fixed_mri_dt_ratio, force_stage1_single_substep */
+    double dt;
+    int    mri_ratio;                 /* even, >= 2                          */
+    int    force_stage1_single_substep;
+
+    /* state layout: NDRY(4) + NSCALARS(1) + n_qstate */
+    int    ncomp;
+    int    moisture;                  /* ERF_MOIST_*                         */
+
+    /* advection (AdvChoice) */
+    int    dycore_horiz_adv, dycore_vert_adv;
+    int    dryscal_horiz_adv, dryscal_vert_adv;
+    int    moistscal_horiz_adv, moistscal_vert_adv;
+    double dycore_horiz_upw_frac, dycore_vert_upw_frac;
+    double dryscal_horiz_upw_frac, dryscal_vert_upw_frac;
+    double moistscal_horiz_upw_frac, moistscal_vert_upw_frac;
+
+    /* diffusion (DiffChoice) and LES closure (TurbChoice) */
+    int    molec_diff_type;
+    double alpha_T, alpha_C, dynamic_viscosity, rho0_trans;
+    int    les_type;
+    double Cs, Pr_t, Sc_t, Ck, Ce, Ce_wall, sigma_k, theta_ref;
+
+    /* forcing */
+    double gravity;                   /* 9.81 with use_gravity, else 0       */
+    double c_p;                       /* 1004.5 default                      */
+    int    buoyancy_type;             /* 1 dry rho', 2 T'-based (moist)      */
+    int    use_coriolis;
+    double coriolis_factor, sinphi, cosphi;
+    double abl_geo_forcing[3];
+
+    /* arithmetic of the bulk (ERF_PREC_*) */
+    int    precision;
+    int    reserved[7];
+} erf_b200_config;
+
+/* Opaque context: owns all integrator scratch (S_sum, S_scratch, F_slow,
+ * primitive variables, fast coefficients, eddy viscosity, stress, ...). */
+typedef struct erf_b200_ctx erf_b200_ctx;
+
+/* ----------------------------------------------------------------------------
+ * Life cycle
+ * ------------------------------------------------------------------------- */
+
+/* Fill *cfg with the reference defaults (SolverChoice defaults; dycore and dry
+ * scalars Upwind_3rd, moist scalars WENO3, Implicit substepping, c_p 1004.5). */
+int erf_b200_config_defaults(erf_b200_config* cfg);
+
+/* Create a context on the current CUDA device; all scratch is allocated here
+ * and never inside a step.  `stream` is a cudaStream_t (NULL = legacy default). */
+int erf_b200_create(erf_b200_ctx** ctx, const erf_b200_config* cfg, void* stream);
+int erf_b200_destroy(erf_b200_ctx* ctx);
+int erf_b200_set_stream(erf_b200_ctx* ctx, void* stream);
+
+/* Synchronise the context's stream and return (and clear) the sticky device
+ * status word: ERF_B200_OK, ERF_B200_EBADSTATE, ERF_B200_ENAN, ... */
+int erf_b200_get_status(erf_b200_ctx* ctx);
+
+/* Bytes of device memory the context holds (scratch only). */
+int erf_b200_scratch_bytes(const erf_b200_ctx* ctx, size_t* bytes);
+
+/* ----------------------------------------------------------------------------
+ * Base state (BaseState::r0_comp, p0_comp, pi0_comp, th0_comp)
+ * ------------------------------------------------------------------------- */
+
+/* Hydrostatic base state from a sounding, computed on the GPU in FP64.
+ * Replaces InputSoundingData::calc_rho_p (DataStructs/ERF_InputSoundingData.H:176-256,
+ * Newton iterations of Utils/ERF_HSE_utils.H:34-72) followed by
+ * ERF::erf_enforce_hse (Initialization/ERF_init1d.cpp:152-260).
+ * theta_cc/qv_cc: nz device values at cell centres; theta_sfc/qv_sfc/p_sfc at z=0.
+ * Writes rho0, p0, pi0, th0 (nz+2 device values each, index k+1 for cell k,
+ * so the k=-1 and k=nz ghosts are included). */
+int erf_b200_make_base_state(erf_b200_ctx* ctx,
+                             const double* theta_cc, const double* qv_cc,
+                             double theta_sfc, double qv_sfc, double p_sfc,
+                             double* rho0, double* p0, double* pi0, double* th0);
+
+/* Install the base state the dycore uses (same nz+2 layout as above). */
+int erf_b200_set_base_state(erf_b200_ctx* ctx, const double* rho0,
+                            const double* p0, const double* pi0, const double* th0);
+
+/* ----------------------------------------------------------------------------
+ * Full step: replaces ERF::advance_dycore + MRISplitIntegrator::advance +
+ * ERF::advance_microphysics (TimeIntegration/ERF_Advance.cpp:165-174,
+ * ERF_advance_dycore.cpp:37-305, ERF_MRI.H:187-369, ERF_advance_microphysics.cpp).
+ * cons (ncomp comps), xvel, yvel, zvel are read at the start and overwritten
+ * with the state after `nsteps` steps; ghost cells of the caller's fabs are
+ * filled (periodic laterally, wall conditions vertically) on return.  The step
+ * sequence is captured once into a CUDA graph and replayed.
+ * ------------------------------------------------------------------------- */
+int erf_b200_advance(erf_b200_ctx* ctx,
+                     const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                     const erf_b200_fab* yvel, const erf_b200_fab* zvel,
+                     int nsteps);
+
+/* Same as erf_b200_advance with host buffers: copies in, advances, copies out.
+ * Host arrays are dense valid-region arrays (no ghosts), i fastest:
+ * cons[ncomp][nz][ny][nx], u[nz][ny][nx+1], v[nz][ny+1][nx], w[nz+1][ny][nx]. */
+int erf_b200_advance_host(erf_b200_ctx* ctx, double* cons, double* u,
+                          double* v, double* w, int nsteps);
+
+/* ----------------------------------------------------------------------------
+ * Per-pass entry points with the roles and argument order of the reference
+ * functions, for callers that keep their own integrator.  State vectors are
+ * passed as arrays of 4 fabs {cons, xmom, ymom, zmom} (IntVars order).
+ * ------------------------------------------------------------------------- */
+
+/* ComputeStrain_N + ComputeTurbulentViscosityLES (Smagorinsky / Deardorff):
+ * Diffusion/ERF_ComputeStrain_N.cpp:28-229,
+ * Diffusion/ERF_ComputeTurbulentViscosity.cpp:32-433.  Reads velocities and
+ * cons, writes the eddy viscosity held in the context. */
+int erf_b200_turbulent_viscosity(erf_b200_ctx* ctx, const erf_b200_fab* xvel,
+                                 const erf_b200_fab* yvel, const erf_b200_fab* zvel,
+                                 const erf_b200_fab* cons);
+
+/* erf_slow_rhs_pre (TimeIntegration/ERF_slow_rhs_pre.cpp:67-774, declared in
+ * ERF_TI_slow_headers.H:54-110) including make_mom_sources/make_buoyancy and
+ * erf_make_tau_terms.  S_rhs[4] out; S_data[4] stage state in; S_scratch[4]
+ * receives the stage mass fluxes as average momenta; xvel/yvel/zvel the stage
+ * velocities. */
+int erf_b200_slow_rhs_pre(erf_b200_ctx* ctx, int nrk, double slow_dt,
+                          const erf_b200_fab* S_rhs, const erf_b200_fab* S_data,
+                          const erf_b200_fab* S_scratch,
+                          const erf_b200_fab* xvel, const erf_b200_fab* yvel,
+                          const erf_b200_fab* zvel);
+
+/* make_fast_coeffs (TimeIntegration/ERF_make_fast_coeffs.cpp:27-294):
+ * fast_coeffs has 5 comps on z-faces: A, 1/B', C, P, Q. */
+int erf_b200_make_fast_coeffs(erf_b200_ctx* ctx, const erf_b200_fab* fast_coeffs,
+                              const erf_b200_fab* S_stage, double dtau);
+
+/* erf_fast_rhs_N (TimeIntegration/ERF_fast_rhs_N.cpp:36-614): one acoustic
+ * substep.  S_prev is S_old at step 0 and S_data afterwards (may alias). */
+int erf_b200_fast_rhs_N(erf_b200_ctx* ctx, int step, int nrk,
+                        const erf_b200_fab* S_slow_rhs, const erf_b200_fab* S_prev,
+                        const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
+                        const erf_b200_fab* S_scratch,
+                        double dtau, double facinv);
+
+/* erf_slow_rhs_post (TimeIntegration/ERF_slow_rhs_post.cpp:49-559). */
+int erf_b200_slow_rhs_post(erf_b200_ctx* ctx, int nrk, double slow_dt,
+                           const erf_b200_fab* S_rhs, const erf_b200_fab* S_old,
+                           const erf_b200_fab* S_new, const erf_b200_fab* S_data,
+                           const erf_b200_fab* S_scratch);
+
+/* Kessler::AdvanceKessler with Copy_State_to_Micro / Copy_Micro_to_State
+ * (Microphysics/Kessler/ERF_Kessler.cpp:11-185, ERF_Init_Kessler.cpp:64-99,
+ * ERF_Update_Kessler.cpp:14-40), in place on cons. */
+int erf_b200_kessler_advance(erf_b200_ctx* ctx, const erf_b200_fab* cons, double dt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ERF_B200_H */

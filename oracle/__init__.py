@@ -1,0 +1,79 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU FP64 oracle.
+
+The oracle (oracle/erf_oracle.cpp) restates the reference's dycore step on the
+CPU.  Only tests/, the smoke check and bench.py's CPU-baseline leg may load it;
+the product (erf_b200/) never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liberf_oracle.so")
+_lib = None
+
+
+def build(quiet: bool = True) -> str:
+    out = subprocess.run(["make", "-C", _HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.oracle_advance.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_int]
+        L.oracle_advance.restype = ctypes.c_int
+        L.oracle_make_base_state.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, dp, dp, dp, dp]
+        L.oracle_make_base_state.restype = ctypes.c_int
+        L.oracle_interp.argtypes = [ctypes.c_int, dp, ctypes.c_double, ctypes.c_double]
+        L.oracle_interp.restype = ctypes.c_double
+        L.oracle_qsatw.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.oracle_qsatw.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_base_state(cfg, case):
+    nz = cfg.nz
+    out = [np.zeros(nz + 2) for _ in range(4)]
+    th = np.ascontiguousarray(case.theta_cc, dtype=np.float64)
+    qv = np.ascontiguousarray(case.qv_cc, dtype=np.float64)
+    lib().oracle_make_base_state(ctypes.byref(cfg), _p(th), _p(qv), case.theta_sfc, case.qv_sfc,
+                                 case.p_sfc, *[_p(a) for a in out])
+    return out
+
+
+def advance(cfg, base, cons, u, v, w, nsteps):
+    """Advance copies of the dense state arrays by nsteps; returns new arrays."""
+    cons, u, v, w = (np.ascontiguousarray(a, dtype=np.float64).copy() for a in (cons, u, v, w))
+    r0, p0, pi0, th0 = (np.ascontiguousarray(a, dtype=np.float64) for a in base)
+    rc = lib().oracle_advance(ctypes.byref(cfg), _p(r0), _p(p0), _p(pi0), _p(th0),
+                              _p(cons), _p(u), _p(v), _p(w), int(nsteps))
+    if rc != 0:
+        raise RuntimeError("oracle_advance failed: %d" % rc)
+    return cons, u, v, w
+
+
+def interp(kind: int, s6, upw: float, frac: float = 1.0) -> float:
+    s = np.ascontiguousarray(s6, dtype=np.float64)
+    return lib().oracle_interp(int(kind), _p(s), float(upw), float(frac))
+
+
+def qsatw(t: float, p_hpa: float) -> float:
+    return lib().oracle_qsatw(float(t), float(p_hpa))

@@ -1,0 +1,1360 @@
+// ============================================================================
+// erf_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU FP64 restatement of the reference's multirate RK3 dycore step (ERF,
+// Source/TimeIntegration/ERF_MRI.H:187-369 and the functions it calls), used as
+// the correctness oracle for the CUDA implementation in erf_b200/.  Nothing in
+// the product links, imports or executes this file; only tests/, the smoke
+// check and bench.py's CPU-baseline leg load the shared library built from it.
+//
+// Why a restatement: the reference is an AMReX application and AMReX (a git
+// submodule, empty in the checkout) plus MPI are absent, so the reference's
+// sources cannot be compiled here.  This file follows the reference's loops,
+// box extents, ghost-cell fills and operation order line by line, each routine
+// citing the reference file:line it restates.  Its own pin is the set of
+// reference gold plotfiles checked in tests/test_oracle_gold.py.
+//
+// Scope (what the C-ABI product supports): one box covering the domain,
+// periodic in x and y, SlipWall / NoSlipWall at the bottom and top, no terrain,
+// map factors 1, implicit acoustic substepping, Smagorinsky or no LES closure,
+// Constant / ConstantAlpha / no molecular diffusion, dry buoyancy type 1 or
+// moist type 2, Coriolis and geostrophic forcing, Kessler microphysics.
+//
+// Layout of the arrays exchanged through the C entry points: dense valid
+// regions, i fastest:  cons[ncomp][nz][ny][nx], u[nz][ny][nx+1],
+// v[nz][ny+1][nx], w[nz+1][ny][nx]; base state arrays have nz+2 entries
+// (index k+1 for cell k).
+// ============================================================================
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <memory>
+
+#include "../include/erf_b200.h"
+
+namespace {
+
+// ----------------------------------------------------------------------------
+// Physical constants (Source/ERF_Constants.H:10-30, 66-87)
+// ----------------------------------------------------------------------------
+constexpr double R_d = 287.0;
+constexpr double R_v = 461.505;
+constexpr double Cp_d = 1004.5;
+constexpr double p_0 = 1.0e5;
+constexpr double Gamma_ = 1.4;
+constexpr double CONST_GRAV = 9.81;
+constexpr double ip_0 = 1. / p_0;
+constexpr double iR_d = 1. / R_d;
+constexpr double iGamma = 1. / Gamma_;
+constexpr double L_v = 2.5e6;
+constexpr double lcond = 2.501e6;
+constexpr double Rd_on_Rv = R_d / R_v;
+constexpr double qcw0 = 1.e-3;
+constexpr double alphaelq = 1.e-3;
+
+// ----------------------------------------------------------------------------
+// Equation of state (Source/Utils/ERF_EOS.H:42-151)
+// ----------------------------------------------------------------------------
+inline double getPgivenRTh(double rt, double qv = 0.) {
+    return p_0 * std::pow(R_d * rt * (1.0 + (R_v / R_d) * qv) * ip_0, Gamma_);
+}
+inline double getExnergivenRTh(double rt, double rdOcp, double qv = 0.0) {
+    return std::pow(R_d * rt * (1.0 + R_v / R_d * qv) * ip_0, Gamma_ * rdOcp);
+}
+inline double getExnergivenP(double P, double rdOcp) { return std::pow(P * ip_0, rdOcp); }
+inline double getRhoThetagivenP(double p, double qv = 0.0) {
+    return std::pow(p * std::pow(p_0, Gamma_ - 1), iGamma) * iR_d / (1.0 + R_v / R_d * qv);
+}
+inline double getTgivenRandRTh(double rho, double rt, double qv = 0.0) {
+    double p_loc = p_0 * std::pow(R_d * rt * (1.0 + R_v / R_d * qv) * ip_0, Gamma_);
+    return p_loc / (R_d * rho * (1.0 + R_v / R_d * qv));
+}
+inline double getRhogivenThetaPress(double theta, double p, double rdOcp, double qv = 0.0) {
+    return std::pow(p_0, rdOcp) * std::pow(p, iGamma) / (R_d * theta * (1.0 + R_v / R_d * qv));
+}
+
+// ----------------------------------------------------------------------------
+// Saturation vapour pressure over water: Flatau et al. (1992), Table 4
+// polynomials, as used by Source/Utils/ERF_Microphysics_Utils.H:52-160.
+// ----------------------------------------------------------------------------
+inline double esatw(double t) {
+    const double a[9] = {6.11239921, 0.443987641, 0.142986287e-1, 0.264847430e-3,
+                         0.302950461e-5, 0.206739458e-7, 0.640689451e-10,
+                         -0.952447341e-13, -0.976195544e-15};
+    double dtt = std::min(t - 273.16, 70.);
+    return a[0] + dtt * (a[1] + dtt * (a[2] + dtt * (a[3] + dtt * (a[4] + dtt * (a[5] + dtt * (a[6] + dtt * (a[7] + a[8] * dtt)))))));
+}
+inline double dtesatw(double t) {
+    const double a[9] = {0.443956472, 0.285976452e-1, 0.794747212e-3, 0.121167162e-4,
+                         0.103167413e-6, 0.385208005e-9, -0.604119582e-12,
+                         -0.792933209e-14, -0.599634321e-17};
+    double dtt = t - 273.16;
+    if (dtt >= 70.) return 0.0;
+    return a[0] + dtt * (a[1] + dtt * (a[2] + dtt * (a[3] + dtt * (a[4] + dtt * (a[5] + dtt * (a[6] + dtt * (a[7] + a[8] * dtt)))))));
+}
+inline double qsatw(double t, double p) {
+    double es = esatw(t);
+    return Rd_on_Rv * es / std::max(es, p - es);
+}
+inline double dtqsatw(double t, double p) { return Rd_on_Rv * dtesatw(t) / p; }
+
+// ----------------------------------------------------------------------------
+// A FAB: box [lo,hi] (inclusive), ncomp components, i fastest.
+// ----------------------------------------------------------------------------
+struct Fab {
+    int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1}, nc = 0;
+    long sj = 0, sk = 0, sn = 0;
+    std::vector<double> d;
+    Fab() = default;
+    Fab(const int l[3], const int h[3], int n, double v = 0.0) { define(l, h, n, v); }
+    void define(const int l[3], const int h[3], int n, double v = 0.0) {
+        for (int a = 0; a < 3; ++a) { lo[a] = l[a]; hi[a] = h[a]; }
+        nc = n;
+        sj = hi[0] - lo[0] + 1;
+        sk = sj * (hi[1] - lo[1] + 1);
+        sn = sk * (hi[2] - lo[2] + 1);
+        d.assign((size_t)sn * nc, v);
+    }
+    inline double& operator()(int i, int j, int k, int n = 0) {
+        return d[(i - lo[0]) + (j - lo[1]) * sj + (k - lo[2]) * sk + n * sn];
+    }
+    inline double operator()(int i, int j, int k, int n = 0) const {
+        return d[(i - lo[0]) + (j - lo[1]) * sj + (k - lo[2]) * sk + n * sn];
+    }
+    void copy_from(const Fab& o) { d = o.d; }
+};
+
+struct Bx { int lo[3], hi[3]; };
+
+template <class F>
+inline void loop(const Bx& b, F&& f) {
+#pragma omp parallel for schedule(static)
+    for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+        for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) f(i, j, k);
+}
+template <class F>
+inline void loop_serial(const Bx& b, F&& f) {
+    for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+        for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) f(i, j, k);
+}
+
+// Index types: 0 cell, 1 x-face, 2 y-face, 3 z-face
+enum { CC = 0, XF = 1, YF = 2, ZF = 3 };
+
+struct Oracle {
+    erf_b200_config c;
+    int nx, ny, nz, ncomp, nprim;
+    int ngc = 4, ngv = 3;
+    double dxInv[3];
+    double rdOcp;
+    bool use_moisture, kessler_rain;
+    bool use_diff, use_turb, use_consA;
+    bool zlo_noslip, zhi_noslip;
+    // base state, index k+1 for cell k
+    std::vector<double> r0, p0, pi0, th0;
+
+    Oracle(const erf_b200_config& cfg) : c(cfg) {
+        nx = c.nx; ny = c.ny; nz = c.nz; ncomp = c.ncomp; nprim = ncomp - 1;
+        dxInv[0] = 1.0 / c.dx; dxInv[1] = 1.0 / c.dy; dxInv[2] = 1.0 / c.dz;
+        rdOcp = R_d / c.c_p;
+        use_moisture = (c.moisture != ERF_MOIST_NONE);
+        kessler_rain = (c.moisture == ERF_MOIST_KESSLER);
+        use_diff = (c.molec_diff_type != ERF_MOLEC_NONE) || (c.les_type != ERF_LES_NONE);
+        use_turb = (c.les_type != ERF_LES_NONE);
+        use_consA = (c.molec_diff_type == ERF_MOLEC_CONSTANT_ALPHA);
+        zlo_noslip = (c.zlo_bc == ERF_BC_NO_SLIP_WALL);
+        zhi_noslip = (c.zhi_bc == ERF_BC_NO_SLIP_WALL);
+        r0.assign(nz + 2, 0.); p0.assign(nz + 2, 0.); pi0.assign(nz + 2, 0.); th0.assign(nz + 2, 0.);
+    }
+
+    // ------------------------------------------------------------------ boxes
+    Bx valid(int t) const {
+        Bx b{{0, 0, 0}, {nx - 1, ny - 1, nz - 1}};
+        if (t == XF) b.hi[0] = nx;
+        if (t == YF) b.hi[1] = ny;
+        if (t == ZF) b.hi[2] = nz;
+        return b;
+    }
+    void alloc(Fab& f, int t, int ng, int n) const {
+        Bx b = valid(t);
+        int l[3], h[3];
+        for (int a = 0; a < 3; ++a) { l[a] = b.lo[a] - ng; h[a] = b.hi[a] + ng; }
+        f.define(l, h, n, 0.0);
+    }
+    static Bx grow(Bx b, int gx, int gy, int gz) {
+        b.lo[0] -= gx; b.hi[0] += gx; b.lo[1] -= gy; b.hi[1] += gy; b.lo[2] -= gz; b.hi[2] += gz;
+        return b;
+    }
+
+    // ------------------------------------------------------------------
+    // FillBoundary with x/y periodicity: every ghost cell whose periodic
+    // image lies in the valid region receives a copy of it, all components.
+    // ------------------------------------------------------------------
+    void fill_periodic(Fab& f, int t) const {
+        Bx v = valid(t);
+        int px = nx, py = ny;
+        for (int n = 0; n < f.nc; ++n)
+            for (int k = f.lo[2]; k <= f.hi[2]; ++k) {
+                if (k < v.lo[2] || k > v.hi[2]) continue;
+                for (int j = f.lo[1]; j <= f.hi[1]; ++j)
+                    for (int i = f.lo[0]; i <= f.hi[0]; ++i) {
+                        bool in = (i >= v.lo[0] && i <= v.hi[0] && j >= v.lo[1] && j <= v.hi[1]);
+                        if (in) continue;
+                        int is = i, js = j;
+                        while (is < v.lo[0]) is += px;
+                        while (is > v.hi[0]) is -= px;
+                        while (js < v.lo[1]) js += py;
+                        while (js > v.hi[1]) js -= py;
+                        f(i, j, k, n) = f(is, js, k, n);
+                    }
+            }
+    }
+
+    // ERFPhysBCFunct_cons (BoundaryConditions/ERF_PhysBCFunct.cpp:16-75 and
+    // ERF_BoundaryConditions_cons.cpp:286-400): FillBoundary, then the vertical
+    // foextrap of components [icomp, icomp+ncomp) on the box grown by ng.
+    void physbcs_cons(Fab& cons, int icomp, int ncmp, int ng) const {
+        fill_periodic(cons, CC);
+        Bx b = grow(valid(CC), ng, ng, ng);
+        for (int n = icomp; n < icomp + ncmp; ++n)
+            for (int k = b.lo[2]; k <= b.hi[2]; ++k) {
+                if (k >= 0 && k <= nz - 1) continue;
+                int ks = (k < 0) ? 0 : nz - 1;
+                for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+                    for (int i = b.lo[0]; i <= b.hi[0]; ++i) cons(i, j, k, n) = cons(i, j, ks, n);
+            }
+    }
+    // ERFPhysBCFunct_u / _v (ERF_BoundaryConditions_xvel.cpp:155-230): tangential
+    // velocity below/above the walls: ext_dir (no-slip, value 0) or foextrap.
+    void physbcs_tangential(Fab& f, int t, int ng) const {
+        fill_periodic(f, t);
+        Bx b = grow(valid(t), ng, ng, ng);
+        for (int k = b.lo[2]; k <= b.hi[2]; ++k) {
+            if (k >= 0 && k <= nz - 1) continue;
+            bool lo = (k < 0);
+            bool noslip = lo ? zlo_noslip : zhi_noslip;
+            int ks = lo ? 0 : nz - 1;
+            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+                for (int i = b.lo[0]; i <= b.hi[0]; ++i) f(i, j, k) = noslip ? 0.0 : f(i, j, ks);
+        }
+    }
+    // ERFPhysBCFunct_w (ERF_BoundaryConditions_zvel.cpp:151-227): w = 0 on the
+    // bottom and top faces (ext_dir for both wall kinds).
+    void physbcs_w(Fab& w, int ng) const {
+        fill_periodic(w, ZF);
+        Bx b = grow(valid(ZF), ng, ng, 0);
+        for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) { w(i, j, 0) = 0.0; w(i, j, nz) = 0.0; }
+    }
+
+    // Utils/ERF_MomentumToVelocity.cpp:25-96 (valid faces only)
+    void mom_to_vel(Fab& u, Fab& v, Fab& w, const Fab& cons, const Fab& mx, const Fab& my, const Fab& mz) const {
+        loop(valid(XF), [&](int i, int j, int k) { u(i, j, k) = mx(i, j, k) * 2.0 / (cons(i, j, k, 0) + cons(i - 1, j, k, 0)); });
+        loop(valid(YF), [&](int i, int j, int k) { v(i, j, k) = my(i, j, k) * 2.0 / (cons(i, j, k, 0) + cons(i, j - 1, k, 0)); });
+        loop(valid(ZF), [&](int i, int j, int k) { w(i, j, k) = mz(i, j, k) * 2.0 / (cons(i, j, k, 0) + cons(i, j, k - 1, 0)); });
+    }
+    // Utils/ERF_VelocityToMomentum.cpp:28-100 on faces grown by (1,1,1)/(1,1,1)/(1,1,0)
+    void vel_to_mom(const Fab& u, const Fab& v, const Fab& w, const Fab& cons, Fab& mx, Fab& my, Fab& mz) const {
+        loop(grow(valid(XF), 1, 1, 1), [&](int i, int j, int k) { mx(i, j, k) = u(i, j, k) * 0.5 * (cons(i, j, k, 0) + cons(i - 1, j, k, 0)); });
+        loop(grow(valid(YF), 1, 1, 1), [&](int i, int j, int k) { my(i, j, k) = v(i, j, k) * 0.5 * (cons(i, j, k, 0) + cons(i, j - 1, k, 0)); });
+        loop(grow(valid(ZF), 1, 1, 0), [&](int i, int j, int k) { mz(i, j, k) = w(i, j, k) * 0.5 * (cons(i, j, k, 0) + cons(i, j, k - 1, 0)); });
+    }
+
+    struct State { Fab cons, mx, my, mz; };
+    struct Vel { Fab u, v, w; };
+
+    void alloc_state(State& s) const {
+        alloc(s.cons, CC, ngc, ncomp); alloc(s.mx, XF, ngv, 1); alloc(s.my, YF, ngv, 1); alloc(s.mz, ZF, ngv, 1);
+    }
+    void alloc_vel(Vel& v) const { alloc(v.u, XF, ngv, 1); alloc(v.v, YF, ngv, 1); alloc(v.w, ZF, ngv, 1); }
+    static void copy_state(State& d, const State& s) {
+        d.cons.copy_from(s.cons); d.mx.copy_from(s.mx); d.my.copy_from(s.my); d.mz.copy_from(s.mz);
+    }
+
+    // FillIntermediatePatch (BoundaryConditions/ERF_FillIntermediatePatch.cpp:32-261), level 0
+    void fill_intermediate(State& S, Vel& V, int ng_cons, int ng_vel, bool cons_only, int icomp, int ncmp) const {
+        if (!cons_only) mom_to_vel(V.u, V.v, V.w, S.cons, S.mx, S.my, S.mz);
+        physbcs_cons(S.cons, icomp, ncmp, ng_cons);
+        if (!cons_only) {
+            physbcs_tangential(V.u, XF, ng_vel);
+            physbcs_tangential(V.v, YF, ng_vel);
+            physbcs_w(V.w, ng_vel);
+            vel_to_mom(V.u, V.v, V.w, S.cons, S.mx, S.my, S.mz);
+        }
+        fill_periodic(S.cons, CC); fill_periodic(S.mx, XF); fill_periodic(S.my, YF); fill_periodic(S.mz, ZF);
+    }
+
+    // apply_bcs (TimeIntegration/ERF_TI_utils.H:53-150)
+    void apply_bcs(State& S, Vel& V, int ng_cons, int ng_vel, bool fast_only, bool synced) const {
+        int scomp, ncmp, ngu;
+        if (!synced) {
+            ngu = std::max(ng_cons, ng_vel + 1);
+            fill_intermediate(S, V, ngu, 0, true, 0, 1);
+        }
+        if (synced) {
+            scomp = 0; ncmp = fast_only ? 2 : ncomp;
+            ngu = std::max(ng_cons, ng_vel + 1);
+        } else {
+            scomp = 1; ncmp = fast_only ? 1 : ncomp - 1;
+            ngu = ng_cons;
+        }
+        fill_intermediate(S, V, ngu, ng_vel, false, scomp, ncmp);
+    }
+
+    // cons_to_prim (TimeIntegration/ERF_TI_utils.H:4-45)
+    void cons_to_prim(const Fab& cons, int ng, Fab& prim, Fab& pi_stage) const {
+        loop(grow(valid(CC), ng, ng, ng), [&](int i, int j, int k) {
+            double rho = cons(i, j, k, 0);
+            prim(i, j, k, 0) = cons(i, j, k, 1) / rho;
+            for (int n = 1; n < nprim; ++n) prim(i, j, k, n) = cons(i, j, k, 1 + n) / rho;
+        });
+        loop(grow(valid(CC), 1, 1, 1), [&](int i, int j, int k) { pi_stage(i, j, k) = getExnergivenRTh(cons(i, j, k, 1), rdOcp); });
+    }
+
+    // ------------------------------------------------------------------
+    // Face interpolants (Source/Utils/ERF_Interpolation_UPW.H, _WENO.H).
+    // s[0..5] = phi(-3..+2) relative to the face's high-side cell.
+    // ------------------------------------------------------------------
+    static double interp(int type, const double s[6], double upw, double upw_frac) {
+        const double sm3 = s[0], sm2 = s[1], sm1 = s[2], s0 = s[3], sp1 = s[4], sp2 = s[5];
+        const double tol = 1.0e-12, eps = 1.0e-6;
+        switch (type) {
+        case ERF_ADV_CENTERED_2ND: return 0.5 * (s0 + sm1);
+        case ERF_ADV_UPWIND_3RD: {
+            if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+            upw *= upw_frac;
+            double a1 = s0 + sm1, d1 = s0 - sm1, a2 = sp1 + sm2, d2 = sp1 - sm2;
+            return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2 + upw * (1.0 / 12.0) * (d2 - 3.0 * d1);
+        }
+        case ERF_ADV_CENTERED_4TH: {
+            double a1 = s0 + sm1, a2 = sp1 + sm2;
+            return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2;
+        }
+        case ERF_ADV_UPWIND_5TH: {
+            if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+            upw *= upw_frac;
+            double a1 = s0 + sm1, a2 = sp1 + sm2, a3 = sp2 + sm3;
+            double d1 = s0 - sm1, d2 = sp1 - sm2, d3 = sp2 - sm3;
+            return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3 - upw * (1.0 / 60.0) * (d3 - 5.0 * d2 + 10.0 * d1);
+        }
+        case ERF_ADV_CENTERED_6TH: {
+            double a1 = s0 + sm1, a2 = sp1 + sm2, a3 = sp2 + sm3;
+            return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3;
+        }
+        case ERF_ADV_WENO_3: {
+            auto ev = [&](double a, double b, double cc) {
+                double b1 = (b - a) * (b - a), b2 = (cc - b) * (cc - b);
+                double w1 = (1.0 / 3.0) / ((eps + b1) * (eps + b1));
+                double w2 = (2.0 / 3.0) / ((eps + b2) * (eps + b2));
+                double ws = w1 + w2;
+                double v1 = -a + 3.0 * b, v2 = b + cc;
+                return (w1 * v1 + w2 * v2) / (2.0 * ws);
+            };
+            if (upw > tol) return ev(sm2, sm1, s0);
+            if (upw < -tol) return ev(sp1, s0, sm1);
+            return 0.5 * (s0 + sm1);
+        }
+        case ERF_ADV_WENO_5: {
+            auto ev = [&](double a, double b, double cc, double dd, double e) {
+                const double c1 = 13.0 / 12.0;
+                double b1 = c1 * (a - 2.0 * b + cc) * (a - 2.0 * b + cc) + 0.25 * (a - 4.0 * b + 3.0 * cc) * (a - 4.0 * b + 3.0 * cc);
+                double b2 = c1 * (b - 2.0 * cc + dd) * (b - 2.0 * cc + dd) + 0.25 * (b - dd) * (b - dd);
+                double b3 = c1 * (cc - 2.0 * dd + e) * (cc - 2.0 * dd + e) + 0.25 * (3.0 * cc - 4.0 * dd + e) * (3.0 * cc - 4.0 * dd + e);
+                double w1 = (1.0 / 10.0) / ((eps + b1) * (eps + b1));
+                double w2 = (3.0 / 5.0) / ((eps + b2) * (eps + b2));
+                double w3 = (3.0 / 10.0) / ((eps + b3) * (eps + b3));
+                double ws = w1 + w2 + w3;
+                double v1 = 2.0 * a - 7.0 * b + 11.0 * cc;
+                double v2 = -b + 5.0 * cc + 2.0 * dd;
+                double v3 = 2.0 * cc + 5.0 * dd - e;
+                return (w1 * v1 + w2 * v2 + w3 * v3) / (6.0 * ws);
+            };
+            if (upw > tol) return ev(sm3, sm2, sm1, s0, sp1);
+            if (upw < -tol) return ev(sp2, sp1, s0, sm1, sm2);
+            return 0.5 * (s0 + sm1);
+        }
+        default: return NAN;
+        }
+    }
+    // UPWINDALL (ERF_Interpolation_UPW.H:528-611): wall-reduced vertical stencils
+    static double interp_all(int type, const double s[6], double upw, double upw_frac) {
+        if (type == ERF_ADV_CENTERED_2ND) return 0.5 * (s[3] + s[2]);
+        double ss[6] = {s[0], s[1], s[2], s[3], s[4], s[5]};
+        if (!(type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH)) { ss[0] = 0.; ss[5] = 0.; }
+        if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+        upw *= upw_frac;
+        double a1 = ss[3] + ss[2], a2 = ss[4] + ss[1], d1 = ss[3] - ss[2], d2 = ss[4] - ss[1];
+        double a3 = ss[5] + ss[0], d3 = ss[5] - ss[0];
+        if (type == ERF_ADV_UPWIND_3RD) return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2 + upw * (1.0 / 12.0) * (d2 - 3.0 * d1);
+        if (type == ERF_ADV_CENTERED_4TH) return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2;
+        if (type == ERF_ADV_UPWIND_5TH) return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3 - upw * (1.0 / 60.0) * (d3 - 5.0 * d2 + 10.0 * d1);
+        if (type == ERF_ADV_CENTERED_6TH) return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3;
+        return 0.;
+    }
+    static int stencil_width(int type) {
+        switch (type) {
+        case ERF_ADV_CENTERED_2ND: return 1;
+        case ERF_ADV_UPWIND_3RD: case ERF_ADV_CENTERED_4TH: case ERF_ADV_WENO_3: return 2;
+        default: return 3;
+        }
+    }
+    // gather phi(i-3..i+2) along direction dir at component n, only touching
+    // entries the scheme reads (others are zero)
+    static void gather(const Fab& f, int dir, int i, int j, int k, int n, int type, double s[6]) {
+        int w = stencil_width(type);
+        for (int m = 0; m < 6; ++m) {
+            int off = m - 3;
+            bool used = (off >= -w && off <= w - 1);
+            if (!used) { s[m] = 0.; continue; }
+            int ii = i + (dir == 0 ? off : 0), jj = j + (dir == 1 ? off : 0), kk = k + (dir == 2 ? off : 0);
+            s[m] = f(ii, jj, kk, n);
+        }
+    }
+
+    // ------------------------------------------------------------------
+    // ComputeStrain_N (Diffusion/ERF_ComputeStrain_N.cpp:28-229), no map
+    // factors, lateral directions periodic, z walls per config.
+    // ------------------------------------------------------------------
+    void compute_strain(const Bx& bxcc, Bx tbxxy, Bx tbxxz, Bx tbxyz, const Fab& u, const Fab& v, const Fab& w,
+                        Fab& s11, Fab& s22, Fab& s33, Fab& s12, Fab& s13, Fab& s23) const {
+        const double* di = dxInv;
+        bool zl_dir = zlo_noslip && tbxxz.lo[2] == 0;
+        bool zh_dir = zhi_noslip && tbxxz.hi[2] == nz;
+        if (zl_dir) {
+            Bx p = tbxxz; p.hi[2] = p.lo[2];
+            loop(p, [&](int i, int j, int k) {
+                s13(i, j, k) = 0.5 * ((-(8. / 3.) * u(i, j, k - 1) + 3. * u(i, j, k) - (1. / 3.) * u(i, j, k + 1)) * di[2] + (w(i, j, k) - w(i - 1, j, k)) * di[0]);
+            });
+            Bx q = tbxyz; q.hi[2] = q.lo[2];
+            loop(q, [&](int i, int j, int k) {
+                s23(i, j, k) = 0.5 * ((-(8. / 3.) * v(i, j, k - 1) + 3. * v(i, j, k) - (1. / 3.) * v(i, j, k + 1)) * di[2] + (w(i, j, k) - w(i, j - 1, k)) * di[1]);
+            });
+            tbxxz.lo[2] += 1; tbxyz.lo[2] += 1;
+        }
+        if (zh_dir) {
+            Bx p = tbxxz; p.lo[2] = p.hi[2];
+            loop(p, [&](int i, int j, int k) {
+                s13(i, j, k) = 0.5 * (-(-(8. / 3.) * u(i, j, k) + 3. * u(i, j, k - 1) - (1. / 3.) * u(i, j, k - 2)) * di[2] + (w(i, j, k) - w(i - 1, j, k)) * di[0]);
+            });
+            Bx q = tbxyz; q.lo[2] = q.hi[2];
+            loop(q, [&](int i, int j, int k) {
+                s23(i, j, k) = 0.5 * (-(-(8. / 3.) * v(i, j, k) + 3. * v(i, j, k - 1) - (1. / 3.) * v(i, j, k - 2)) * di[2] + (w(i, j, k) - w(i, j - 1, k)) * di[1]);
+            });
+            tbxxz.hi[2] -= 1; tbxyz.hi[2] -= 1;
+        }
+        loop(bxcc, [&](int i, int j, int k) {
+            s11(i, j, k) = (u(i + 1, j, k) - u(i, j, k)) * di[0];
+            s22(i, j, k) = (v(i, j + 1, k) - v(i, j, k)) * di[1];
+            s33(i, j, k) = (w(i, j, k + 1) - w(i, j, k)) * di[2];
+        });
+        loop(tbxxy, [&](int i, int j, int k) { s12(i, j, k) = 0.5 * ((u(i, j, k) - u(i, j - 1, k)) * di[1] + (v(i, j, k) - v(i - 1, j, k)) * di[0]); });
+        loop(tbxxz, [&](int i, int j, int k) { s13(i, j, k) = 0.5 * ((u(i, j, k) - u(i, j, k - 1)) * di[2] + (w(i, j, k) - w(i - 1, j, k)) * di[0]); });
+        loop(tbxyz, [&](int i, int j, int k) { s23(i, j, k) = 0.5 * ((v(i, j, k) - v(i, j, k - 1)) * di[2] + (w(i, j, k) - w(i, j - 1, k)) * di[1]); });
+    }
+
+    // edge FABs with one lateral ghost layer
+    void alloc_edges(Fab& s12, Fab& s13, Fab& s23) const {
+        int l12[3] = {-2, -2, 0}, h12[3] = {nx + 2, ny + 2, nz - 1};
+        int l13[3] = {-2, -2, 0}, h13[3] = {nx + 2, ny + 1, nz};
+        int l23[3] = {-2, -2, 0}, h23[3] = {nx + 1, ny + 2, nz};
+        s12.define(l12, h12, 1); s13.define(l13, h13, 1); s23.define(l23, h23, 1);
+    }
+    void alloc_cc1(Fab& f, int n = 1) const {
+        int l[3] = {-2, -2, -1}, h[3] = {nx + 1, ny + 1, nz};
+        f.define(l, h, n);
+    }
+
+    // ComputeSmnSmn (Diffusion/ERF_EddyViscosity.H:31-83), no MOST
+    static double smnsmn(int i, int j, int k, const Fab& t11, const Fab& t22, const Fab& t33, const Fab& t12, const Fab& t13, const Fab& t23) {
+        double s11 = t11(i, j, k), s22 = t22(i, j, k), s33 = t33(i, j, k);
+        double s12 = 0.25 * (t12(i, j, k) + t12(i, j + 1, k) + t12(i + 1, j, k) + t12(i + 1, j + 1, k));
+        double s13 = 0.25 * (t13(i, j, k) + t13(i, j, k + 1) + t13(i + 1, j, k) + t13(i + 1, j, k + 1));
+        double s23 = 0.25 * (t23(i, j, k) + t23(i, j, k + 1) + t23(i, j + 1, k) + t23(i, j + 1, k + 1));
+        return s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + 2.0 * s23 * s23;
+    }
+
+    // Step-start strain + ComputeTurbulentViscosityLES (Smagorinsky) with the
+    // lateral/periodic/vertical ghost treatment of
+    // Diffusion/ERF_ComputeTurbulentViscosity.cpp:54-127, 230-432.
+    // mu_t holds EddyDiff::Mom_h (== Mom_v for LES), ghost 1.
+    void turbulent_viscosity(const Vel& V, const Fab& cons, Fab& mut) const {
+        Fab t11, t22, t33, t12, t13, t23;
+        alloc_cc1(t11); alloc_cc1(t22); alloc_cc1(t33); alloc_edges(t12, t13, t23);
+        Bx bxcc = grow(valid(CC), 1, 1, 0);
+        Bx txy = grow(Bx{{0, 0, 0}, {nx, ny, nz - 1}}, 1, 1, 0);
+        Bx txz = grow(Bx{{0, 0, 0}, {nx, ny - 1, nz}}, 1, 1, 0);
+        Bx tyz = grow(Bx{{0, 0, 0}, {nx - 1, ny, nz}}, 1, 1, 0);
+        compute_strain(bxcc, txy, txz, tyz, V.u, V.v, V.w, t11, t22, t33, t12, t13, t23);
+        double Cs = c.Cs;
+        loop(valid(CC), [&](int i, int j, int k) {
+            double S = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23);
+            double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dxInv[2]);
+            double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
+            double CsDeltaSqrMsf = Cs * Cs * DeltaMsf * DeltaMsf;
+            mut(i, j, k) = CsDeltaSqrMsf * cons(i, j, k, 0) * std::sqrt(2.0 * S);
+        });
+        // FillBoundary (periodic) then top/bottom extrapolation
+        fill_periodic(mut, CC);
+        for (int j = -1; j <= ny; ++j)
+            for (int i = -1; i <= nx; ++i) { mut(i, j, -1) = mut(i, j, 0); mut(i, j, nz) = mut(i, j, nz - 1); }
+    }
+
+    // Eddy diffusivity of a primitive component (EddyDiff mapping,
+    // ERF_ComputeTurbulentViscosity.cpp:323-366): Theta: 1/Pr_t, scalars and
+    // moisture: 1/Sc_t.
+    double eddy_factor(int prim_index) const {
+        if (prim_index == 0) return 1.0 / c.Pr_t;
+        return 1.0 / c.Sc_t;
+    }
+    double alpha_eff(int prim_index) const {
+        // DiffusionSrcForState_N.cpp:100-165
+        if (c.molec_diff_type == ERF_MOLEC_NONE) {
+            // rhoAlpha_T/C are still rho0_trans*alpha (0 unless set)
+        }
+        bool consA = use_consA;
+        if (prim_index == 0) return consA ? c.alpha_T : c.rho0_trans * c.alpha_T;
+        if (prim_index == 1 || prim_index == 2) return 0.0; // KE, QKE
+        return consA ? c.alpha_C : c.rho0_trans * c.alpha_C;
+    }
+
+    // DiffusionSrcForState_N (Diffusion/ERF_DiffusionSrcForState_N.cpp:39-667),
+    // foextrap scalars at walls, no MOST: adds -div(flux) to rhs comps
+    void diffusion_state(int start_comp, int ncmp, const Fab& cell_data, const Fab& prim, Fab& rhs, const Fab& mut) const {
+        for (int n = 0; n < ncmp; ++n) {
+            int q = start_comp + n, pidx = q - 1;
+            double ae = alpha_eff(pidx);
+            double fac = eddy_factor(pidx);
+            Fab fx, fy, fz;
+            alloc(fx, XF, 0, 1); alloc(fy, YF, 0, 1); alloc(fz, ZF, 0, 1);
+            auto mu = [&](int i, int j, int k) { return mut(i, j, k) * fac; };
+            loop(valid(XF), [&](int i, int j, int k) {
+                double rA = use_consA ? 0.5 * (cell_data(i, j, k, 0) + cell_data(i - 1, j, k, 0)) * ae : ae;
+                if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i - 1, j, k));
+                fx(i, j, k) = -rA * (prim(i, j, k, pidx) - prim(i - 1, j, k, pidx)) * dxInv[0] * 1.0;
+            });
+            loop(valid(YF), [&](int i, int j, int k) {
+                double rA = use_consA ? 0.5 * (cell_data(i, j, k, 0) + cell_data(i, j - 1, k, 0)) * ae : ae;
+                if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j - 1, k));
+                fy(i, j, k) = -rA * (prim(i, j, k, pidx) - prim(i, j - 1, k, pidx)) * dxInv[1] * 1.0;
+            });
+            loop(valid(ZF), [&](int i, int j, int k) {
+                double rA = use_consA ? 0.5 * (cell_data(i, j, k, 0) + cell_data(i, j, k - 1, 0)) * ae : ae;
+                if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j, k - 1));
+                fz(i, j, k) = -rA * (prim(i, j, k, pidx) - prim(i, j, k - 1, pidx)) * dxInv[2];
+            });
+            loop(valid(CC), [&](int i, int j, int k) {
+                rhs(i, j, k, q) -= (fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] * 1.0 + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] * 1.0 + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2];
+            });
+        }
+    }
+
+    // AdvectionSrcForScalars (Advection/ERF_AdvectionSrcForState.cpp:119-370 and
+    // ERF_AdvectionSrcForScalars.H): assigns rhs comps
+    void advect_scalars(int icomp, int ncmp, const Fab& ax, const Fab& ay, const Fab& az, const Fab& prim, Fab& rhs,
+                        int htype, int vtype, double hfrac, double vfrac) const {
+        for (int n = 0; n < ncmp; ++n) {
+            int q = icomp + n, pidx = q - 1;
+            Fab fx, fy, fz;
+            alloc(fx, XF, 0, 1); alloc(fy, YF, 0, 1); alloc(fz, ZF, 0, 1);
+            loop(valid(XF), [&](int i, int j, int k) {
+                double s[6]; gather(prim, 0, i, j, k, pidx, htype, s);
+                fx(i, j, k) = ax(i, j, k) * interp(htype, s, ax(i, j, k), hfrac);
+            });
+            loop(valid(YF), [&](int i, int j, int k) {
+                double s[6]; gather(prim, 1, i, j, k, pidx, htype, s);
+                fy(i, j, k) = ay(i, j, k) * interp(htype, s, ay(i, j, k), hfrac);
+            });
+            loop(valid(ZF), [&](int i, int j, int k) {
+                double s[6]; gather(prim, 2, i, j, k, pidx, vtype, s);
+                fz(i, j, k) = az(i, j, k) * interp(vtype, s, az(i, j, k), vfrac);
+            });
+            loop(valid(CC), [&](int i, int j, int k) {
+                double invdetJ = 1.;
+                double mfsq = 1.0;
+                rhs(i, j, k, q) = -invdetJ * mfsq * ((fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2]);
+            });
+        }
+    }
+
+    // ------------------------------------------------------------------
+    // Everything the integrator keeps across stages.
+    // ------------------------------------------------------------------
+    State S_old, S_new, S_sum, S_scr, F_slow;
+    Vel Vnew;
+    Fab prim, pi_stage, mut, fast_coeffs;
+    Fab xsrc, ysrc, zsrc;
+
+    void init_storage() {
+        alloc_state(S_old); alloc_state(S_new); alloc_state(S_sum); alloc_state(S_scr); alloc_state(F_slow);
+        alloc_vel(Vnew);
+        alloc(prim, CC, ngc, nprim);
+        alloc(pi_stage, CC, ngc, 1);
+        alloc_cc1(mut);
+        alloc(fast_coeffs, ZF, 0, 5);
+        alloc(xsrc, XF, 1, 1); alloc(ysrc, YF, 1, 1); alloc(zsrc, ZF, 1, 1);
+    }
+
+    // make_mom_sources + make_buoyancy (SourceTerms/ERF_make_mom_sources.cpp:40-315,
+    // SourceTerms/ERF_make_buoyancy.cpp:31-380) on stage data
+    void make_mom_sources(const State& S, const Fab& prm) {
+        std::fill(xsrc.d.begin(), xsrc.d.end(), 0.0);
+        std::fill(ysrc.d.begin(), ysrc.d.end(), 0.0);
+        std::fill(zsrc.d.begin(), zsrc.d.end(), 0.0);
+        const Fab& cd = S.cons;
+        double g2 = -c.gravity;
+        Bx tbz_b = valid(ZF); tbz_b.lo[2] = 1; tbz_b.hi[2] = nz - 1;
+        if (!use_moisture) {
+            if (c.buoyancy_type == 1) {
+                loop(tbz_b, [&](int i, int j, int k) {
+                    zsrc(i, j, k) = g2 * 0.5 * ((cd(i, j, k, 0) - r0[k + 1]) + (cd(i, j, k - 1, 0) - r0[k]));
+                });
+            } else {
+                // dry types 2/3 (T' based) use the base state p0
+                loop(tbz_b, [&](int i, int j, int k) {
+                    auto T0 = [&](int kk) { double rt0 = getRhoThetagivenP(p0[kk + 1]); return (rt0 / r0[kk + 1]) / std::pow(p_0 / p0[kk + 1], rdOcp); };
+                    double t0_hi = T0(k), t_hi = getTgivenRandRTh(cd(i, j, k, 0), cd(i, j, k, 1));
+                    double t0_lo = T0(k - 1), t_lo = getTgivenRandRTh(cd(i, j, k - 1, 0), cd(i, j, k - 1, 1));
+                    double qplus = (t_hi - t0_hi) / t0_hi, qminus = (t_lo - t0_lo) / t0_lo;
+                    double r0_q_avg = 0.5 * (r0[k + 1] * qplus + r0[k] * qminus);
+                    zsrc(i, j, k) = -r0_q_avg * g2;
+                });
+            }
+        } else if (c.buoyancy_type == 1) {
+            int nq = ncomp - ERF_RHOQ1_COMP;
+            loop(tbz_b, [&](int i, int j, int k) {
+                double hi = cd(i, j, k, 0) + cd(i, j, k, 5) + cd(i, j, k, 6) - r0[k + 1];
+                double lo = cd(i, j, k - 1, 0) + cd(i, j, k - 1, 5) + cd(i, j, k - 1, 6) - r0[k];
+                for (int qo = 2; qo < nq; ++qo) { hi += cd(i, j, k, 5 + qo); lo += cd(i, j, k - 1, 5 + qo); }
+                zsrc(i, j, k) = g2 * 0.5 * (hi + lo);
+            });
+        } else {
+            // buoyancy type 2: horizontal plane averages of rho, theta, qv, qc, qp
+            int nq = ncomp - ERF_RHOQ1_COMP;
+            std::vector<double> rho_d(nz, 0.), th_d(nz, 0.), qv_d(nz, 0.), qc_d(nz, 0.), qp_d(nz, 0.);
+            double denom = 1.0 / (double)(nx * ny);
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        rho_d[k] += cd(i, j, k, 0) * denom;
+                        th_d[k] += prm(i, j, k, 0) * denom;
+                        if (nq >= 1) qv_d[k] += prm(i, j, k, 4) * denom;
+                        if (nq >= 2) qc_d[k] += prm(i, j, k, 5) * denom;
+                        if (nq >= 3) qp_d[k] += prm(i, j, k, 6) * denom;
+                    }
+            loop(tbz_b, [&](int i, int j, int k) {
+                double tp1 = getTgivenRandRTh(rho_d[k], rho_d[k] * th_d[k], qv_d[k]);
+                double tm1 = getTgivenRandRTh(rho_d[k - 1], rho_d[k - 1] * th_d[k - 1], qv_d[k - 1]);
+                double tp3 = getTgivenRandRTh(cd(i, j, k, 0), cd(i, j, k, 1), cd(i, j, k, 5) / cd(i, j, k, 0));
+                double tm3 = getTgivenRandRTh(cd(i, j, k - 1, 0), cd(i, j, k - 1, 1), cd(i, j, k - 1, 5) / cd(i, j, k - 1, 0));
+                double qvp = nq >= 1 ? prm(i, j, k, 4) : 0.0, qvm = nq >= 1 ? prm(i, j, k - 1, 4) : 0.0;
+                double qcp = nq >= 2 ? prm(i, j, k, 5) : 0.0, qcm = nq >= 2 ? prm(i, j, k - 1, 5) : 0.0;
+                double qpp = nq >= 3 ? prm(i, j, k, 6) : 0.0, qpm = nq >= 3 ? prm(i, j, k - 1, 6) : 0.0;
+                double qplus = 0.61 * (qvp - qv_d[k]) - (qcp - qc_d[k] + qpp - qp_d[k]) + (tp3 - tp1) / tp1 * (1.0 + 0.61 * qv_d[k] - qc_d[k] - qp_d[k]);
+                double qminus = 0.61 * (qvm - qv_d[k - 1]) - (qcm - qc_d[k - 1] + qpm - qp_d[k - 1]) + (tm3 - tm1) / tm1 * (1.0 + 0.61 * qv_d[k - 1] - qc_d[k - 1] - qp_d[k - 1]);
+                double qavg = 0.5 * (qplus + qminus);
+                double r0avg = 0.5 * (rho_d[k] + rho_d[k - 1]);
+                zsrc(i, j, k) = -qavg * r0avg * g2;
+            });
+        }
+        const Fab &ru = S.mx, &rv = S.my, &rw = S.mz;
+        Bx tbx = valid(XF), tby = valid(YF), tbz = valid(ZF);
+        tbz.hi[2] = nz - 1;
+        if (c.use_coriolis) {
+            double cf = c.coriolis_factor, sp = c.sinphi, cp = c.cosphi;
+            loop(tbx, [&](int i, int j, int k) {
+                double rvl = 0.25 * (rv(i, j + 1, k) + rv(i, j, k) + rv(i - 1, j + 1, k) + rv(i - 1, j, k));
+                double rwl = 0.25 * (rw(i, j, k + 1) + rw(i, j, k) + rw(i, j - 1, k + 1) + rw(i, j - 1, k));
+                xsrc(i, j, k) += cf * (rvl * sp - rwl * cp);
+            });
+            loop(tby, [&](int i, int j, int k) {
+                double rul = 0.25 * (ru(i + 1, j, k) + ru(i, j, k) + ru(i + 1, j - 1, k) + ru(i, j - 1, k));
+                ysrc(i, j, k) += -cf * rul * sp;
+            });
+            loop(tbz, [&](int i, int j, int k) {
+                double rul = 0.25 * (ru(i + 1, j, k) + ru(i, j, k) + ru(i + 1, j, k - 1) + ru(i, j, k - 1));
+                zsrc(i, j, k) += cf * rul * cp;
+            });
+        }
+        loop(tbx, [&](int i, int j, int k) { xsrc(i, j, k) += 0.5 * (cd(i, j, k, 0) + cd(i - 1, j, k, 0)) * c.abl_geo_forcing[0]; });
+        loop(tby, [&](int i, int j, int k) { ysrc(i, j, k) += 0.5 * (cd(i, j, k, 0) + cd(i, j - 1, k, 0)) * c.abl_geo_forcing[1]; });
+        loop(tbz, [&](int i, int j, int k) { zsrc(i, j, k) += 0.5 * (cd(i, j, k, 0) + cd(i, j, k - 1, 0)) * c.abl_geo_forcing[2]; });
+    }
+
+    // erf_make_tau_terms (TimeIntegration/ERF_make_tau_terms.cpp:320-424), no terrain
+    void make_tau(const Vel& V, const State& S, Fab& t11, Fab& t22, Fab& t33, Fab& t12, Fab& t13, Fab& t23) const {
+        Fab er; alloc_cc1(er);
+        Fab s11, s22, s33, s12, s13, s23;
+        alloc_cc1(s11); alloc_cc1(s22); alloc_cc1(s33); alloc_edges(s12, s13, s23);
+        Bx bxcc = grow(valid(CC), 1, 1, 0);
+        Bx txy = grow(Bx{{0, 0, 0}, {nx, ny, nz - 1}}, 1, 1, 0);
+        Bx txz = grow(Bx{{0, 0, 0}, {nx, ny - 1, nz}}, 1, 1, 0);
+        Bx tyz = grow(Bx{{0, 0, 0}, {nx - 1, ny, nz}}, 1, 1, 0);
+        const Fab &u = V.u, &v = V.v, &w = V.w;
+        loop(bxcc, [&](int i, int j, int k) {
+            er(i, j, k) = (u(i + 1, j, k) - u(i, j, k)) * dxInv[0] + (v(i, j + 1, k) - v(i, j, k)) * dxInv[1] + (w(i, j, k + 1) - w(i, j, k)) * dxInv[2];
+        });
+        compute_strain(bxcc, txy, txz, tyz, u, v, w, s11, s22, s33, s12, s13, s23);
+        double mu_eff = use_consA ? 2.0 * c.dynamic_viscosity / c.rho0_trans : 2.0 * c.dynamic_viscosity;
+        const double OneThird = 1. / 3.;
+        Bx exy = Bx{{0, 0, 0}, {nx, ny, nz - 1}}, exz = Bx{{0, 0, 0}, {nx, ny - 1, nz}}, eyz = Bx{{0, 0, 0}, {nx - 1, ny, nz}};
+        const Fab& cd = S.cons;
+        // ComputeStress{Cons,Var}Visc_N (Diffusion/ERF_ComputeStress_N.cpp:23-189)
+        loop(bxcc, [&](int i, int j, int k) {
+            double m11, m33;
+            double base = use_consA ? cd(i, j, k, 0) * mu_eff : mu_eff;
+            if (use_turb) { m11 = base + 2.0 * mut(i, j, k); m33 = base + 2.0 * mut(i, j, k); }
+            else { m11 = base; m33 = base; }
+            t11(i, j, k) = -m11 * (s11(i, j, k) - OneThird * er(i, j, k));
+            t22(i, j, k) = -m11 * (s22(i, j, k) - OneThird * er(i, j, k));
+            t33(i, j, k) = -m33 * (s33(i, j, k) - OneThird * er(i, j, k));
+        });
+        loop(exy, [&](int i, int j, int k) {
+            double m = use_consA ? 0.25 * (cd(i - 1, j, k, 0) + cd(i, j, k, 0) + cd(i - 1, j - 1, k, 0) + cd(i, j - 1, k, 0)) * mu_eff : mu_eff;
+            if (use_turb) m += 2.0 * (0.25 * (mut(i - 1, j, k) + mut(i, j, k) + mut(i - 1, j - 1, k) + mut(i, j - 1, k)));
+            t12(i, j, k) = s12(i, j, k) * -m;
+        });
+        loop(exz, [&](int i, int j, int k) {
+            double m = use_consA ? 0.25 * (cd(i - 1, j, k, 0) + cd(i, j, k, 0) + cd(i - 1, j, k - 1, 0) + cd(i, j, k - 1, 0)) * mu_eff : mu_eff;
+            if (use_turb) m += 2.0 * (0.25 * (mut(i - 1, j, k) + mut(i, j, k) + mut(i - 1, j, k - 1) + mut(i, j, k - 1)));
+            t13(i, j, k) = s13(i, j, k) * -m;
+        });
+        loop(eyz, [&](int i, int j, int k) {
+            double m = use_consA ? 0.25 * (cd(i, j - 1, k, 0) + cd(i, j, k, 0) + cd(i, j - 1, k - 1, 0) + cd(i, j, k - 1, 0)) * mu_eff : mu_eff;
+            if (use_turb) m += 2.0 * (0.25 * (mut(i, j - 1, k) + mut(i, j, k) + mut(i, j - 1, k - 1) + mut(i, j, k - 1)));
+            t23(i, j, k) = s23(i, j, k) * -m;
+        });
+    }
+
+    // erf_slow_rhs_pre (TimeIntegration/ERF_slow_rhs_pre.cpp:67-774), no terrain,
+    // no anelastic, no mono advection, periodic laterally.
+    void slow_rhs_pre(int nrk, double dt, State& R, const State& S, State& Scr, const Vel& V) {
+        (void)nrk; (void)dt;
+        make_mom_sources(S, prim);
+        Fab t11, t22, t33, t12, t13, t23;
+        if (use_diff) {
+            alloc_cc1(t11); alloc_cc1(t22); alloc_cc1(t33); alloc_edges(t12, t13, t23);
+            make_tau(V, S, t11, t22, t33, t12, t13, t23);
+        }
+        std::fill(R.mz.d.begin(), R.mz.d.end(), 0.0);
+        const Fab& cd = S.cons;
+        // p' on the tile grown by one (z clipped at 0)
+        Fab pp; alloc_cc1(pp);
+        Bx gbx = grow(valid(CC), 1, 1, 1); gbx.lo[2] = 0;
+        loop(gbx, [&](int i, int j, int k) {
+            double qv = use_moisture ? cd(i, j, k, ERF_RHOQ1_COMP) / cd(i, j, k, 0) : 0.0;
+            pp(i, j, k) = getPgivenRTh(cd(i, j, k, 1), qv) - p0[k + 1];
+        });
+        // Omega = rho_w (no terrain), on z-faces grown by one laterally
+        // AdvectionSrcForRho (Advection/ERF_AdvectionSrcForState.cpp:30-93)
+        Fab fx, fy, fz;
+        alloc(fx, XF, 0, 1); alloc(fy, YF, 0, 1); alloc(fz, ZF, 0, 1);
+        loop(valid(XF), [&](int i, int j, int k) { fx(i, j, k) = 1.0 * S.mx(i, j, k) / 1.0; Scr.mx(i, j, k) = fx(i, j, k); });
+        loop(valid(YF), [&](int i, int j, int k) { fy(i, j, k) = 1.0 * S.my(i, j, k) / 1.0; Scr.my(i, j, k) = fy(i, j, k); });
+        loop(valid(ZF), [&](int i, int j, int k) { fz(i, j, k) = 1.0 * S.mz(i, j, k) / 1.0; Scr.mz(i, j, k) = fz(i, j, k); });
+        loop(valid(CC), [&](int i, int j, int k) {
+            R.cons(i, j, k, 0) = -1.0 / 1.0 * ((fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2]);
+        });
+        advect_scalars(1, 1, Scr.mx, Scr.my, Scr.mz, prim, R.cons, c.dryscal_horiz_adv, c.dryscal_vert_adv,
+                       c.dryscal_horiz_upw_frac, c.dryscal_vert_upw_frac);
+        if (use_diff) diffusion_state(1, 1, cd, prim, R.cons, mut);
+        // cc_src is zero for the supported configurations
+
+        // AdvectionSrcForMom (Advection/ERF_AdvectionSrcForMom.cpp:41-204,
+        // ERF_AdvectionSrcForMom_N.H:17-407)
+        const Fab &ru = S.mx, &rv = S.my, &rw = S.mz, &u = V.u, &v = V.v, &w = V.w;
+        int ht = c.dycore_horiz_adv, vt = c.dycore_vert_adv;
+        double hf = c.dycore_horiz_upw_frac, vf = c.dycore_vert_upw_frac;
+        bool c2 = (ht == ERF_ADV_CENTERED_2ND && vt == ERF_ADV_CENTERED_2ND);
+        auto iX = [&](const Fab& f, int i, int j, int k, double upw) { double s[6]; gather(f, 0, i, j, k, 0, ht, s); return interp(ht, s, upw, hf); };
+        auto iY = [&](const Fab& f, int i, int j, int k, double upw) { double s[6]; gather(f, 1, i, j, k, 0, ht, s); return interp(ht, s, upw, hf); };
+        auto iZ = [&](const Fab& f, int i, int j, int k, double upw) { double s[6]; gather(f, 2, i, j, k, 0, vt, s); return interp(vt, s, upw, vf); };
+        Bx tbx = valid(XF), tby = valid(YF), tbz = valid(ZF);
+        tbz.lo[2] = 1; tbz.hi[2] = nz - 1;
+        int lo_z_face = 0, hi_z_face = nz;
+        loop(tbx, [&](int i, int j, int k) {
+            double src;
+            if (c2) {
+                double xh = 0.25 * (ru(i, j, k) * 1.0 + ru(i + 1, j, k) * 1.0) * (u(i + 1, j, k) + u(i, j, k));
+                double xl = 0.25 * (ru(i, j, k) * 1.0 + ru(i - 1, j, k) * 1.0) * (u(i - 1, j, k) + u(i, j, k));
+                double yh = 0.25 * (rv(i, j + 1, k) * 1.0 + rv(i - 1, j + 1, k) * 1.0) * (u(i, j + 1, k) + u(i, j, k));
+                double yl = 0.25 * (rv(i, j, k) * 1.0 + rv(i - 1, j, k) * 1.0) * (u(i, j - 1, k) + u(i, j, k));
+                double zh = 0.25 * (rw(i, j, k + 1) + rw(i - 1, j, k + 1)) * (u(i, j, k + 1) + u(i, j, k));
+                double zl = 0.25 * (rw(i, j, k) + rw(i - 1, j, k)) * (u(i, j, k - 1) + u(i, j, k));
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+            } else {
+                double a, xh, xl, yh, yl, zh, zl;
+                a = 0.5 * (ru(i + 1, j, k) * 1.0 + ru(i, j, k) * 1.0); xh = a * iX(u, i + 1, j, k, a);
+                a = 0.5 * (ru(i - 1, j, k) * 1.0 + ru(i, j, k) * 1.0); xl = a * iX(u, i, j, k, a);
+                a = 0.5 * (rv(i, j + 1, k) * 1.0 + rv(i - 1, j + 1, k) * 1.0); yh = a * iY(u, i, j + 1, k, a);
+                a = 0.5 * (rv(i, j, k) * 1.0 + rv(i - 1, j, k) * 1.0); yl = a * iY(u, i, j, k, a);
+                a = 0.5 * (rw(i, j, k + 1) + rw(i - 1, j, k + 1)); zh = a * iZ(u, i, j, k + 1, a);
+                a = 0.5 * (rw(i, j, k) + rw(i - 1, j, k)); zl = a * iZ(u, i, j, k, a);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+            }
+            R.mx(i, j, k) = -src;
+        });
+        loop(tby, [&](int i, int j, int k) {
+            double src;
+            if (c2) {
+                double xh = 0.25 * (ru(i + 1, j, k) * 1.0 + ru(i + 1, j - 1, k) * 1.0) * (v(i + 1, j, k) + v(i, j, k));
+                double xl = 0.25 * (ru(i, j, k) * 1.0 + ru(i, j - 1, k) * 1.0) * (v(i - 1, j, k) + v(i, j, k));
+                double yh = 0.25 * (rv(i, j + 1, k) * 1.0 + rv(i, j, k) * 1.0) * (v(i, j + 1, k) + v(i, j, k));
+                double yl = 0.25 * (rv(i, j, k) * 1.0 + rv(i, j - 1, k) * 1.0) * (v(i, j - 1, k) + v(i, j, k));
+                double zh = 0.25 * (rw(i, j, k + 1) + rw(i, j - 1, k + 1)) * (v(i, j, k + 1) + v(i, j, k));
+                double zl = 0.25 * (rw(i, j, k) + rw(i, j - 1, k)) * (v(i, j, k - 1) + v(i, j, k));
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+            } else {
+                double a, xh, xl, yh, yl, zh, zl;
+                a = 0.5 * (ru(i + 1, j, k) * 1.0 + ru(i + 1, j - 1, k) * 1.0); xh = a * iX(v, i + 1, j, k, a);
+                a = 0.5 * (ru(i, j, k) * 1.0 + ru(i, j - 1, k) * 1.0); xl = a * iX(v, i, j, k, a);
+                a = 0.5 * (rv(i, j, k) * 1.0 + rv(i, j + 1, k) * 1.0); yh = a * iY(v, i, j + 1, k, a);
+                a = 0.5 * (rv(i, j, k) * 1.0 + rv(i, j - 1, k) * 1.0); yl = a * iY(v, i, j, k, a);
+                a = 0.5 * (rw(i, j, k + 1) + rw(i, j - 1, k + 1)); zh = a * iZ(v, i, j, k + 1, a);
+                a = 0.5 * (rw(i, j, k) + rw(i, j - 1, k)); zl = a * iZ(v, i, j, k, a);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+            }
+            R.my(i, j, k) = -src;
+        });
+        loop(tbz, [&](int i, int j, int k) {
+            double src;
+            if (c2) {
+                double xh = 0.25 * (ru(i + 1, j, k) + ru(i + 1, j, k - 1)) * 1.0 * (w(i + 1, j, k) + w(i, j, k));
+                double xl = 0.25 * (ru(i, j, k) + ru(i, j, k - 1)) * 1.0 * (w(i - 1, j, k) + w(i, j, k));
+                double yh = 0.25 * (rv(i, j + 1, k) + rv(i, j + 1, k - 1)) * 1.0 * (w(i, j + 1, k) + w(i, j, k));
+                double yl = 0.25 * (rv(i, j, k) + rv(i, j, k - 1)) * 1.0 * (w(i, j - 1, k) + w(i, j, k));
+                double zl = 0.25 * (rw(i, j, k) + rw(i, j, k - 1)) * (w(i, j, k) + w(i, j, k - 1));
+                double zh = (k == hi_z_face) ? rw(i, j, k) * w(i, j, k) : 0.25 * (rw(i, j, k) + rw(i, j, k + 1)) * (w(i, j, k) + w(i, j, k + 1));
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+            } else {
+                double a, xh, xl, yh, yl, zh, zl, ih, il;
+                a = 0.5 * (ru(i + 1, j, k) + ru(i + 1, j, k - 1)) * 1.0; xh = a * iX(w, i + 1, j, k, a);
+                a = 0.5 * (ru(i, j, k) + ru(i, j, k - 1)) * 1.0; xl = a * iX(w, i, j, k, a);
+                a = 0.5 * (rv(i, j + 1, k) + rv(i, j + 1, k - 1)) * 1.0; yh = a * iY(w, i, j + 1, k, a);
+                a = 0.5 * (rv(i, j, k) + rv(i, j, k - 1)) * 1.0; yl = a * iY(w, i, j, k, a);
+                auto iZall = [&](int kk, double upw, double frac, int type) { double s[6]; gather(w, 2, i, j, kk, 0, (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH) ? ERF_ADV_UPWIND_5TH : (type == ERF_ADV_CENTERED_2ND ? ERF_ADV_CENTERED_2ND : ERF_ADV_UPWIND_3RD), s); return interp_all(type, s, upw, frac); };
+                if (k == hi_z_face) { zh = rw(i, j, k) * w(i, j, k); }
+                else {
+                    a = 0.5 * (rw(i, j, k) + rw(i, j, k + 1));
+                    if (k == hi_z_face - 1) ih = iZall(k + 1, a, 0, ERF_ADV_CENTERED_2ND);
+                    else if (k == hi_z_face - 2 || k == lo_z_face + 1) {
+                        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) ih = iZall(k + 1, a, 0, ERF_ADV_CENTERED_4TH);
+                        else ih = iZall(k + 1, a, vf, vt);
+                    } else ih = iZ(w, i, j, k + 1, a);
+                    zh = a * ih;
+                }
+                if (k == lo_z_face) { zl = rw(i, j, k) * w(i, j, k); }
+                else {
+                    a = 0.5 * (rw(i, j, k) + rw(i, j, k - 1));
+                    if (k == lo_z_face + 1) il = iZall(k, a, 0, ERF_ADV_CENTERED_2ND);
+                    else if (k == lo_z_face + 2 || k == hi_z_face - 1) {
+                        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) il = iZall(k, a, 0, ERF_ADV_CENTERED_4TH);
+                        else il = iZall(k, a, vf, vt);
+                    } else il = iZ(w, i, j, k, a);
+                    zl = a * il;
+                }
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+            }
+            R.mz(i, j, k) = -src;
+        });
+        if (use_diff) {
+            // DiffusionSrcForMom_N (Diffusion/ERF_DiffusionSrcForMom_N.cpp:25-67)
+            loop(tbx, [&](int i, int j, int k) {
+                R.mx(i, j, k) -= ((t11(i, j, k) - t11(i - 1, j, k)) * dxInv[0] * 1.0 + (t12(i, j + 1, k) - t12(i, j, k)) * dxInv[1] * 1.0 + (t13(i, j, k + 1) - t13(i, j, k)) * dxInv[2]);
+            });
+            loop(tby, [&](int i, int j, int k) {
+                R.my(i, j, k) -= ((t12(i + 1, j, k) - t12(i, j, k)) * dxInv[0] * 1.0 + (t22(i, j, k) - t22(i, j - 1, k)) * dxInv[1] * 1.0 + (t23(i, j, k + 1) - t23(i, j, k)) * dxInv[2]);
+            });
+            loop(tbz, [&](int i, int j, int k) {
+                R.mz(i, j, k) -= ((t13(i + 1, j, k) - t13(i, j, k)) * dxInv[0] * 1.0 + (t23(i, j + 1, k) - t23(i, j, k)) * dxInv[1] * 1.0 + (t33(i, j, k) - t33(i, j, k - 1)) * dxInv[2]);
+            });
+        }
+        // pressure gradient and momentum sources (ERF_slow_rhs_pre.cpp:594-744)
+        loop(tbx, [&](int i, int j, int k) {
+            double gpx = dxInv[0] * (pp(i, j, k) - pp(i - 1, j, k));
+            gpx *= 1.0;
+            double q = 0.0;
+            if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i - 1, j, k, 4) + prim(i, j, k, 5) + prim(i - 1, j, k, 5));
+            R.mx(i, j, k) += (-gpx - 0.0) / (1.0 + q) + xsrc(i, j, k);
+        });
+        loop(tby, [&](int i, int j, int k) {
+            double gpy = dxInv[1] * (pp(i, j, k) - pp(i, j - 1, k));
+            gpy *= 1.0;
+            double q = 0.0;
+            if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i, j - 1, k, 4) + prim(i, j, k, 5) + prim(i, j - 1, k, 5));
+            R.my(i, j, k) += (-gpy - 0.0) / (1.0 + q) + ysrc(i, j, k);
+        });
+        loop(tbz, [&](int i, int j, int k) {
+            double gpz = dxInv[2] * (pp(i, j, k) - pp(i, j, k - 1)) / 1.0;
+            double q = 0.0;
+            if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i, j, k - 1, 4) + prim(i, j, k, 5) + prim(i, j, k - 1, 5));
+            R.mz(i, j, k) += (zsrc(i, j, k) - gpz - 0.0) / (1.0 + q);
+        });
+    }
+
+    // make_fast_coeffs (TimeIntegration/ERF_make_fast_coeffs.cpp:27-294), no terrain
+    void make_fast_coeffs(const State& Sst, double dtau, double beta_s) {
+        double beta_2 = 0.5 * (1.0 + beta_s);
+        double c_v = c.c_p - R_d;
+        double dzi = dxInv[2];
+        double halfg = std::abs(0.5 * -c.gravity);
+        Fab& fc = fast_coeffs;
+        Bx b = valid(CC); b.lo[2] = 1; b.hi[2] = nz - 1;
+        loop(b, [&](int i, int j, int k) {
+            double rhobar_lo = r0[k], rhobar_hi = r0[k + 1], pibar_lo = pi0[k], pibar_hi = pi0[k + 1];
+            double pi_c = 0.5 * (pi_stage(i, j, k - 1) + pi_stage(i, j, k));
+            double cP = -Gamma_ * R_d * dzi + halfg * R_d * rhobar_hi / (c_v * pibar_hi * Sst.cons(i, j, k, 1));
+            cP *= pi_c;
+            double cQ = Gamma_ * R_d * dzi + halfg * R_d * rhobar_lo / (c_v * pibar_lo * Sst.cons(i, j, k - 1, 1));
+            cQ *= pi_c;
+            fc(i, j, k, 3) = cP; fc(i, j, k, 4) = cQ;
+            if (use_moisture) {
+                double q = 0.5 * (prim(i, j, k, 4) + prim(i, j, k - 1, 4) + prim(i, j, k, 5) + prim(i, j, k - 1, 5));
+                cP /= (1.0 + q); cQ /= (1.0 + q);
+            }
+            double tlo = 0.5 * (prim(i, j, k - 2, 0) + prim(i, j, k - 1, 0));
+            double tmid = 0.5 * (prim(i, j, k - 1, 0) + prim(i, j, k, 0));
+            double thi = 0.5 * (prim(i, j, k, 0) + prim(i, j, k + 1, 0));
+            double D = dtau * dtau * beta_2 * beta_2 * dzi;
+            fc(i, j, k, 0) = D * (halfg - cQ * tlo);
+            fc(i, j, k, 2) = D * (-halfg + cP * thi);
+            fc(i, j, k, 1) = 1.0 + D * (cQ - cP) * tmid;
+        });
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                fc(i, j, 0, 0) = 0.0; fc(i, j, 0, 1) = 1.0; fc(i, j, 0, 2) = 0.0;
+                fc(i, j, nz, 0) = 0.0; fc(i, j, nz, 1) = 1.0; fc(i, j, nz, 2) = 0.0;
+                double bet = fc(i, j, 0, 1);
+                for (int k = 1; k <= nz; ++k) {
+                    double gam = fc(i, j, k - 1, 2) / bet;
+                    bet = fc(i, j, k, 1) - fc(i, j, k, 0) * gam;
+                    fc(i, j, k, 1) = bet;
+                }
+            }
+        loop(b, [&](int i, int j, int k) { fc(i, j, k, 1) = 1.0 / fc(i, j, k, 1); });
+    }
+
+    // erf_fast_rhs_N (TimeIntegration/ERF_fast_rhs_N.cpp:36-614), implicit
+    void fast_rhs_N(int step, int nrk, const State& Rs, const State& Sprev_in, const State& Sst, State& Sd, State& Scr,
+                    double dtau, double beta_s, double facinv) {
+        // S_prev may alias S_data: work from a snapshot of the previous values
+        State Sprev; alloc_state(Sprev); copy_state(Sprev, Sprev_in);
+        double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s), beta_d = 0.1;
+        double dxi = dxInv[0], dyi = dxInv[1], dzi = dxInv[2];
+        Fab drt, drw, extrap, trhs, tcx, tcy;
+        alloc(drt, CC, 1, 1); alloc(drw, ZF, 1, 1); alloc(extrap, CC, 1, 1); alloc(trhs, CC, 0, 2);
+        alloc(tcx, XF, 0, 1); alloc(tcy, YF, 0, 1);
+        Fab& lag = Scr.cons;
+        loop(grow(valid(CC), 1, 1, 1), [&](int i, int j, int k) {
+            drt(i, j, k) = Sprev.cons(i, j, k, 1) - Sst.cons(i, j, k, 1);
+            if (step == 0) extrap(i, j, k) = drt(i, j, k);
+            else extrap(i, j, k) = drt(i, j, k) + beta_d * (drt(i, j, k) - lag(i, j, k, 1));
+            lag(i, j, k, 1) = drt(i, j, k);
+        });
+        loop(grow(valid(ZF), 1, 1, 0), [&](int i, int j, int k) { drw(i, j, k) = Sprev.mz(i, j, k) - Sst.mz(i, j, k); });
+        Fab& ax = Scr.mx; Fab& ay = Scr.my; Fab& az = Scr.mz;
+        if (nrk == 0 && step == 0) {
+            loop(valid(XF), [&](int i, int j, int k) {
+                double nd = Sprev.mx(i, j, k) - Sst.mx(i, j, k) + dtau * Rs.mx(i, j, k);
+                ax(i, j, k) += facinv * nd; tcx(i, j, k) = Sst.mx(i, j, k) + nd;
+            });
+            loop(valid(YF), [&](int i, int j, int k) {
+                double nd = Sprev.my(i, j, k) - Sst.my(i, j, k) + dtau * Rs.my(i, j, k);
+                ay(i, j, k) += facinv * nd; tcy(i, j, k) = Sst.my(i, j, k) + nd;
+            });
+        } else {
+            loop(valid(XF), [&](int i, int j, int k) {
+                double gpx = (extrap(i, j, k) - extrap(i - 1, j, k)) * dxi;
+                gpx *= 1.0;
+                if (use_moisture) {
+                    double q = 0.5 * (prim(i, j, k, 4) + prim(i - 1, j, k, 4) + prim(i, j, k, 5) + prim(i - 1, j, k, 5));
+                    gpx /= (1.0 + q);
+                }
+                double pi_c = 0.5 * (pi_stage(i - 1, j, k) + pi_stage(i, j, k));
+                double f = -Gamma_ * R_d * pi_c * gpx;
+                double nd = Sprev.mx(i, j, k) - Sst.mx(i, j, k) + dtau * f + dtau * Rs.mx(i, j, k);
+                ax(i, j, k) += facinv * nd; tcx(i, j, k) = Sst.mx(i, j, k) + nd;
+            });
+            loop(valid(YF), [&](int i, int j, int k) {
+                double gpy = (extrap(i, j, k) - extrap(i, j - 1, k)) * dyi;
+                gpy *= 1.0;
+                if (use_moisture) {
+                    double q = 0.5 * (prim(i, j, k, 4) + prim(i, j - 1, k, 4) + prim(i, j, k, 5) + prim(i, j - 1, k, 5));
+                    gpy /= (1.0 + q);
+                }
+                double pi_c = 0.5 * (pi_stage(i, j - 1, k) + pi_stage(i, j, k));
+                double f = -Gamma_ * R_d * pi_c * gpy;
+                double nd = Sprev.my(i, j, k) - Sst.my(i, j, k) + dtau * f + dtau * Rs.my(i, j, k);
+                ay(i, j, k) += facinv * nd; tcy(i, j, k) = Sst.my(i, j, k) + nd;
+            });
+        }
+        // horizontal fluxes of rho and rho*theta
+        loop(valid(CC), [&](int i, int j, int k) {
+            double xl = (tcx(i, j, k) - Sst.mx(i, j, k)) / 1.0, xh = (tcx(i + 1, j, k) - Sst.mx(i + 1, j, k)) / 1.0;
+            double yl = (tcy(i, j, k) - Sst.my(i, j, k)) / 1.0, yh = (tcy(i, j + 1, k) - Sst.my(i, j + 1, k)) / 1.0;
+            double mfsq = 1.0;
+            trhs(i, j, k, 0) = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
+            trhs(i, j, k, 1) = ((xh * (prim(i, j, k, 0) + prim(i + 1, j, k, 0)) - xl * (prim(i, j, k, 0) + prim(i - 1, j, k, 0))) * dxi * mfsq +
+                                (yh * (prim(i, j, k, 0) + prim(i, j + 1, k, 0)) - yl * (prim(i, j, k, 0) + prim(i, j - 1, k, 0))) * dyi * mfsq) * 0.5;
+        });
+        double halfg = std::abs(0.5 * -c.gravity);
+        Fab RHS, soln; alloc(RHS, ZF, 0, 1); alloc(soln, ZF, 0, 1);
+        Bx bs = valid(CC); bs.lo[2] = 1; bs.hi[2] = nz - 1;
+        const Fab& fc = fast_coeffs;
+        loop(bs, [&](int i, int j, int k) {
+            double cP = fc(i, j, k, 3), cQ = fc(i, j, k, 4);
+            if (use_moisture) {
+                double q = 0.5 * (prim(i, j, k, 4) + prim(i, j, k - 1, 4) + prim(i, j, k, 5) + prim(i, j, k - 1, 5));
+                cP /= (1.0 + q); cQ /= (1.0 + q);
+            }
+            double tlo = 0.5 * (prim(i, j, k - 2, 0) + prim(i, j, k - 1, 0));
+            double tmid = 0.5 * (prim(i, j, k - 1, 0) + prim(i, j, k, 0));
+            double thi = 0.5 * (prim(i, j, k, 0) + prim(i, j, k + 1, 0));
+            double Okp1 = Sprev.mz(i, j, k + 1) - Sst.mz(i, j, k + 1);
+            double Ok = Sprev.mz(i, j, k) - Sst.mz(i, j, k);
+            double Okm1 = Sprev.mz(i, j, k - 1) - Sst.mz(i, j, k - 1);
+            double odk = Sprev.cons(i, j, k, 0) - Sst.cons(i, j, k, 0);
+            double odkm1 = Sprev.cons(i, j, k - 1, 0) - Sst.cons(i, j, k - 1, 0);
+            double R0 = cP * drt(i, j, k) + cQ * drt(i, j, k - 1) - halfg * (odk + odkm1);
+            double R1 = halfg * (-Rs.cons(i, j, k, 0) - Rs.cons(i, j, k - 1, 0) + trhs(i, j, k, 0) + trhs(i, j, k - 1, 0)) +
+                        (cP * (Rs.cons(i, j, k, 1) - trhs(i, j, k, 1)) + cQ * (Rs.cons(i, j, k - 1, 1) - trhs(i, j, k - 1, 1)));
+            R1 += beta_1 * dzi * ((Okp1 - Okm1) * halfg - (Okp1 * thi - Ok * tmid) * cP - (Ok * tmid - Okm1 * tlo) * cQ);
+            RHS(i, j, k) = Ok + dtau * (Rs.mz(i, j, k) + R0 + dtau * beta_2 * R1);
+        });
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                RHS(i, j, 0) = Sprev.mz(i, j, 0) - Sst.mz(i, j, 0) + dtau * Rs.mz(i, j, 0);
+                RHS(i, j, nz) = Sprev.mz(i, j, nz) - Sst.mz(i, j, nz) + dtau * Rs.mz(i, j, nz);
+            }
+#pragma omp parallel for
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                soln(i, j, 0) = RHS(i, j, 0) * fc(i, j, 0, 1);
+                Sd.mz(i, j, 0) = Sst.mz(i, j, 0) + soln(i, j, 0);
+                for (int k = 1; k <= nz; ++k) soln(i, j, k) = (RHS(i, j, k) - fc(i, j, k, 0) * soln(i, j, k - 1)) * fc(i, j, k, 1);
+                Sd.mz(i, j, nz) = Sst.mz(i, j, nz) + soln(i, j, nz);
+                for (int k = nz - 1; k >= 0; --k) {
+                    soln(i, j, k) -= (fc(i, j, k, 2) * fc(i, j, k, 1)) * soln(i, j, k + 1);
+                    Sd.mz(i, j, k) = Sst.mz(i, j, k) + soln(i, j, k);
+                }
+            }
+        loop(valid(CC), [&](int i, int j, int k) {
+            double zl = beta_2 * soln(i, j, k) + beta_1 * drw(i, j, k);
+            double zh = beta_2 * soln(i, j, k + 1) + beta_1 * drw(i, j, k + 1);
+            az(i, j, k) += facinv * zl / (1.0 * 1.0);
+            if (k == nz - 1) az(i, j, k + 1) += facinv * zh / (1.0 * 1.0);
+            trhs(i, j, k, 0) += dzi * (zh - zl);
+            trhs(i, j, k, 1) += 0.5 * dzi * (zh * (prim(i, j, k, 0) + prim(i, j, k + 1, 0)) - zl * (prim(i, j, k, 0) + prim(i, j, k - 1, 0)));
+        });
+        loop(valid(CC), [&](int i, int j, int k) {
+            Sd.cons(i, j, k, 0) = Sprev.cons(i, j, k, 0) + dtau * (Rs.cons(i, j, k, 0) - trhs(i, j, k, 0));
+            Sd.cons(i, j, k, 1) = Sprev.cons(i, j, k, 1) + dtau * (Rs.cons(i, j, k, 1) - trhs(i, j, k, 1));
+        });
+        loop(valid(XF), [&](int i, int j, int k) { Sd.mx(i, j, k) = tcx(i, j, k); });
+        loop(valid(YF), [&](int i, int j, int k) { Sd.my(i, j, k) = tcy(i, j, k); });
+    }
+
+    // erf_slow_rhs_post (TimeIntegration/ERF_slow_rhs_post.cpp:49-559)
+    void slow_rhs_post(int nrk, double dt, State& R, const State& Sold, State& Snew, State& Sd, State& Scr) {
+        (void)nrk;
+        int nsv = ncomp - 2;
+        loop(valid(CC), [&](int i, int j, int k) { for (int n = 2; n < 2 + nsv; ++n) Sd.cons(i, j, k, n) = Snew.cons(i, j, k, n); });
+        // valid slow variables: RhoScalar always; moisture if present
+        auto do_var = [&](int start, int num_adv, int htype, int vtype, double hf, double vf) {
+            advect_scalars(start, num_adv, Scr.mx, Scr.my, Scr.mz, prim, R.cons, htype, vtype, hf, vf);
+            if (use_diff) diffusion_state(start, num_adv, Snew.cons, prim, R.cons, mut);
+        };
+        do_var(ERF_RHOSCALAR_COMP, 1, c.dryscal_horiz_adv, c.dryscal_vert_adv, c.dryscal_horiz_upw_frac, c.dryscal_vert_upw_frac);
+        int nq = ncomp - ERF_RHOQ1_COMP;
+        if (use_moisture && nq > 0)
+            do_var(ERF_RHOQ1_COMP, nq, c.moistscal_horiz_adv, c.moistscal_vert_adv, c.moistscal_horiz_upw_frac, c.moistscal_vert_upw_frac);
+        loop(valid(CC), [&](int i, int j, int k) {
+            int n = ERF_RHOSCALAR_COMP;
+            Sd.cons(i, j, k, n) = Sold.cons(i, j, k, n) + dt * R.cons(i, j, k, n);
+            if (use_moisture)
+                for (int m = ERF_RHOQ1_COMP; m < ncomp; ++m) {
+                    Sd.cons(i, j, k, m) = Sold.cons(i, j, k, m) + dt * R.cons(i, j, k, m);
+                    Sd.cons(i, j, k, m) = std::max(Sd.cons(i, j, k, m), 0.0);
+                }
+        });
+        loop(valid(CC), [&](int i, int j, int k) { for (int n = 0; n < ncomp; ++n) Snew.cons(i, j, k, n) = Sd.cons(i, j, k, n); });
+        loop(valid(XF), [&](int i, int j, int k) { Snew.mx(i, j, k) = Sd.mx(i, j, k); });
+        loop(valid(YF), [&](int i, int j, int k) { Snew.my(i, j, k) = Sd.my(i, j, k); });
+        loop(valid(ZF), [&](int i, int j, int k) { Snew.mz(i, j, k) = Sd.mz(i, j, k); });
+    }
+
+    // Kessler (Microphysics/Kessler/ERF_Kessler.cpp:11-185 with
+    // ERF_Init_Kessler.cpp:64-99 and ERF_Update_Kessler.cpp:14-40)
+    void kessler(Fab& cons, double dtn) {
+        Fab rho, th, qv, qc, qp, tabs, pres, fz;
+        alloc(rho, CC, 0, 1); alloc(th, CC, 0, 1); alloc(qv, CC, 0, 1); alloc(qc, CC, 0, 1); alloc(qp, CC, 0, 1);
+        alloc(tabs, CC, 0, 1); alloc(pres, CC, 0, 1); alloc(fz, ZF, 0, 1);
+        loop(valid(CC), [&](int i, int j, int k) {
+            rho(i, j, k) = cons(i, j, k, 0);
+            th(i, j, k) = cons(i, j, k, 1) / cons(i, j, k, 0);
+            qv(i, j, k) = cons(i, j, k, 5) / cons(i, j, k, 0);
+            qc(i, j, k) = cons(i, j, k, 6) / cons(i, j, k, 0);
+            qp(i, j, k) = (ncomp > 7) ? cons(i, j, k, 7) / cons(i, j, k, 0) : 0.0;
+            tabs(i, j, k) = getTgivenRandRTh(cons(i, j, k, 0), cons(i, j, k, 1), qv(i, j, k));
+            pres(i, j, k) = getPgivenRTh(cons(i, j, k, 1), qv(i, j, k)) / 100.;
+        });
+        double fac_cond = lcond / c.c_p;
+        double dz = c.dz;
+        if (kessler_rain) {
+            loop(valid(ZF), [&](int i, int j, int k) {
+                double ra, qa;
+                if (k == 0) { ra = rho(i, j, k); qa = qp(i, j, k); }
+                else if (k == nz) { ra = rho(i, j, k - 1); qa = qp(i, j, k - 1); }
+                else { ra = 0.5 * (rho(i, j, k - 1) + rho(i, j, k)); qa = 0.5 * (qp(i, j, k - 1) + qp(i, j, k)); }
+                qa = std::max(0.0, qa);
+                double Vt = 36.34 * std::pow(ra * 0.001 * qa, 0.1346) * std::pow(ra / 1.16, -0.5);
+                fz(i, j, k) = ra * Vt * qa;
+            });
+            // the reference zeroes tiny fluxes from inside the cell loop; doing it
+            // once beforehand gives the same values
+            loop(valid(ZF), [&](int i, int j, int k) { if (std::fabs(fz(i, j, k)) < 1e-14) fz(i, j, k) = 0.0; });
+            loop(valid(CC), [&](int i, int j, int k) {
+                qv(i, j, k) = std::max(0.0, qv(i, j, k));
+                qc(i, j, k) = std::max(0.0, qc(i, j, k));
+                qp(i, j, k) = std::max(0.0, qp(i, j, k));
+                double p = pres(i, j, k);
+                double qs = qsatw(tabs(i, j, k), p), dqs = dtqsatw(tabs(i, j, k), p);
+                if (qs <= 0.0) qs = 0.0;
+                double d_c2r = 0.0, d_r2v = 0.0, d_v2c = 0.0, d_c2v = 0.0;
+                double fac = 1.0 + (L_v / Cp_d) * dqs;
+                if (qv(i, j, k) > qs) d_v2c = std::min(qv(i, j, k), (qv(i, j, k) - qs) / (1.0 + fac));
+                if (qv(i, j, k) < qs && qc(i, j, k) > 0.0) d_c2v = std::min(qc(i, j, k), (qs - qv(i, j, k)) / (1.0 + fac));
+                if (qp(i, j, k) > 0.0 && qv(i, j, k) < qs) {
+                    double C = 1.6 + 124.9 * std::pow(0.001 * rho(i, j, k) * qp(i, j, k), 0.2046);
+                    d_r2v = 1.0 / (0.001 * rho(i, j, k)) * (1.0 - qv(i, j, k) / qs) * C * std::pow(0.001 * rho(i, j, k) * qp(i, j, k), 0.525) /
+                            (5.4e5 + 2.55e6 / (p * qs)) * dtn;
+                    d_r2v = std::min(qp(i, j, k), d_r2v);
+                }
+                if (qc(i, j, k) > 0.0) {
+                    double qcc = qc(i, j, k);
+                    double auto_r = (qcc > qcw0) ? alphaelq : 0.0;
+                    double accrr = 2.2 * std::pow(qp(i, j, k), 0.875);
+                    d_c2r = dtn * (accrr * qcc + auto_r * (qcc - qcw0));
+                    d_c2r = std::min(d_c2r, qc(i, j, k));
+                }
+                double dq_sed = dtn * 1.0 * (1.0 / rho(i, j, k)) * (fz(i, j, k + 1) - fz(i, j, k)) / dz;
+                if (std::fabs(dq_sed) < 1e-14) dq_sed = 0.0;
+                qv(i, j, k) += -d_v2c + d_c2v + d_r2v;
+                qc(i, j, k) += d_v2c - d_c2v - d_c2r;
+                qp(i, j, k) += dq_sed + d_c2r - d_r2v;
+                double tot = th(i, j, k) / tabs(i, j, k);
+                th(i, j, k) += tot * fac_cond * (d_v2c - d_c2v - d_r2v);
+                qv(i, j, k) = std::max(0.0, qv(i, j, k));
+                qc(i, j, k) = std::max(0.0, qc(i, j, k));
+                qp(i, j, k) = std::max(0.0, qp(i, j, k));
+            });
+        } else {
+            loop(valid(CC), [&](int i, int j, int k) {
+                qc(i, j, k) = std::max(0.0, qc(i, j, k));
+                double p = pres(i, j, k);
+                double qs = qsatw(tabs(i, j, k), p), dqs = dtqsatw(tabs(i, j, k), p);
+                double d_v2c = 0.0, d_c2v = 0.0;
+                double fac = 1.0 + (L_v / Cp_d) * dqs;
+                if (qv(i, j, k) > qs) d_v2c = std::min(qv(i, j, k), (qv(i, j, k) - qs) / (1.0 + fac));
+                if (qv(i, j, k) < qs && qc(i, j, k) > 0.0) d_c2v = std::min(qc(i, j, k), (qs - qv(i, j, k)) / (1.0 + fac));
+                qv(i, j, k) += -d_v2c + d_c2v;
+                qc(i, j, k) += d_v2c - d_c2v;
+                double tot = th(i, j, k) / tabs(i, j, k);
+                th(i, j, k) += tot * fac_cond * (d_v2c - d_c2v);
+                qv(i, j, k) = std::max(0.0, qv(i, j, k));
+                qc(i, j, k) = std::max(0.0, qc(i, j, k));
+            });
+        }
+        loop(valid(CC), [&](int i, int j, int k) {
+            cons(i, j, k, 1) = rho(i, j, k) * th(i, j, k);
+            cons(i, j, k, 5) = rho(i, j, k) * qv(i, j, k);
+            cons(i, j, k, 6) = rho(i, j, k) * qc(i, j, k);
+            if (ncomp > 7) cons(i, j, k, 7) = rho(i, j, k) * qp(i, j, k);
+        });
+        fill_periodic(cons, CC);
+    }
+
+    // ------------------------------------------------------------------
+    // One full time step: ERF::Advance (TimeIntegration/ERF_Advance.cpp:19-233)
+    // -> advance_dycore (ERF_advance_dycore.cpp:37-305) -> MRISplitIntegrator::
+    // advance (ERF_MRI.H:187-369) -> advance_microphysics.
+    // Persistent state: cons and face velocities (valid + ghosts).
+    // ------------------------------------------------------------------
+    Fab cons_state;
+    Vel vel_state;
+
+    void step(double dt) {
+        const double beta_s = 0.1;
+        // FillPatch of the old state (ghost cells of cons and velocities)
+        Fab& Sc = cons_state;
+        physbcs_cons(Sc, 0, ncomp, ngc);
+        physbcs_tangential(vel_state.u, XF, ngv);
+        physbcs_tangential(vel_state.v, YF, ngv);
+        physbcs_w(vel_state.w, ngv);
+        // S_old = {cons, V2M(old velocities)}
+        S_old.cons.copy_from(Sc);
+        // turbulent viscosity from the old velocities (strain + Smagorinsky)
+        if (use_turb) turbulent_viscosity(vel_state, S_old.cons, mut);
+        vel_to_mom(vel_state.u, vel_state.v, vel_state.w, S_old.cons, S_old.mx, S_old.my, S_old.mz);
+        Vnew.u.copy_from(vel_state.u); Vnew.v.copy_from(vel_state.v); Vnew.w.copy_from(vel_state.w);
+        apply_bcs(S_old, Vnew, ngc, ngv, false, true);
+        cons_to_prim(S_old.cons, ngc, prim, pi_stage);
+
+        // MRISplitIntegrator::advance
+        copy_state(S_new, S_old);
+        int ratio = c.mri_ratio;
+        double sub_dt = dt / ratio;
+        for (int nrk = 0; nrk < 3; ++nrk) {
+            int nsub; double dtau;
+            if (nrk == 0) {
+                if (c.force_stage1_single_substep) { nsub = 1; dtau = dt / 3.0; }
+                else { nsub = ratio / 3; dtau = sub_dt; }
+            } else if (nrk == 1) { nsub = ratio / 2; dtau = sub_dt; }
+            else { nsub = ratio; dtau = sub_dt; }
+            double slow_dt = (nrk == 0 ? dt / 3.0 : (nrk == 1 ? dt / 2.0 : dt));
+            if (nrk > 0) cons_to_prim(S_new.cons, ngc, prim, pi_stage);
+            slow_rhs_pre(nrk, slow_dt, F_slow, S_new, S_scr, Vnew);
+            double inv_fac = 1.0 / (double)nsub;
+            for (int ks = 0; ks < nsub; ++ks) {
+                if (ks == 0) make_fast_coeffs(S_new, dtau, beta_s);
+                fast_rhs_N(ks, nrk, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);
+                apply_bcs(S_sum, Vnew, 1, 1, true, false);
+            }
+            slow_rhs_post(nrk, slow_dt, F_slow, S_old, S_new, S_sum, S_scr);
+            apply_bcs(S_new, Vnew, ngc, ngv, false, false);
+        }
+        // new state: cons of S_new, velocities from the last post_update
+        Sc.copy_from(S_new.cons);
+        vel_state.u.copy_from(Vnew.u); vel_state.v.copy_from(Vnew.v); vel_state.w.copy_from(Vnew.w);
+        if (use_moisture) kessler(Sc, dt);
+    }
+
+    // ------------------------------------------------------------------
+    // Hydrostatic base state: InputSoundingData::calc_rho_p
+    // (DataStructs/ERF_InputSoundingData.H:176-256) with Newton_Raphson_hse
+    // (Utils/ERF_HSE_utils.H:34-72) at cell centres, then erf_enforce_hse
+    // (Initialization/ERF_init1d.cpp:152-260).
+    // ------------------------------------------------------------------
+    void make_base_state(const double* th_cc, const double* qv_cc, double th_s, double qv_s, double p_s,
+                         double* rho_o, double* p_o, double* pi_o, double* th_o) const {
+        const double tol = 1.0e-12;
+        std::vector<double> z(nz + 1), th(nz + 1), qv(nz + 1), pm(nz + 1), rd(nz + 1);
+        z[0] = 0.; th[0] = th_s; qv[0] = qv_s;
+        for (int k = 0; k < nz; ++k) { z[k + 1] = (k + 0.5) * c.dz; th[k + 1] = th_cc[k]; qv[k + 1] = qv_cc[k]; }
+        double g = c.gravity;
+        pm[0] = p_s;
+        rd[0] = getRhogivenThetaPress(th[0], p_s, R_d / Cp_d, qv[0]);
+        for (int k = 1; k <= nz; ++k) {
+            double dz = z[k] - z[k - 1];
+            double rlo = rd[k - 1] * (1. + qv[k - 1]);
+            double C = -pm[k - 1] + 0.5 * rlo * g * dz;
+            pm[k] = pm[k - 1];
+            rd[k] = getRhogivenThetaPress(th[k], pm[k], R_d / Cp_d, qv[k]);
+            double rhi = rd[k] * (1. + qv[k]);
+            double F = pm[k] + 0.5 * rhi * g * dz + C;
+            if (std::abs(F) > tol) {
+                int iter = 0;
+                double eps = 1.0e-6, ieps = 1.0e6;
+                do {
+                    double hi = getRhogivenThetaPress(th[k], pm[k] + eps, R_d / Cp_d, qv[k]);
+                    double lo = getRhogivenThetaPress(th[k], pm[k] - eps, R_d / Cp_d, qv[k]);
+                    double dFdp = 1.0 + 0.25 * ieps * (hi - lo) * g * dz;
+                    pm[k] -= F / dFdp;
+                    rd[k] = getRhogivenThetaPress(th[k], pm[k], R_d / Cp_d, qv[k]);
+                    double rt = rd[k] * (1. + qv[k]);
+                    F = pm[k] + 0.5 * rt * g * dz + C;
+                    ++iter;
+                } while (std::abs(F) > tol && iter < 30);
+            }
+        }
+        // rho0 at cell centres (dry density), ghosts by foextrap
+        for (int k = 0; k < nz; ++k) rho_o[k + 1] = rd[k + 1];
+        rho_o[0] = rho_o[1]; rho_o[nz + 1] = rho_o[nz];
+        // erf_enforce_hse
+        double hz = 0.5 * c.dz;
+        p_o[1] = p_0 - hz * rho_o[1] * g;
+        pi_o[1] = getExnergivenP(p_o[1], rdOcp);
+        th_o[1] = getRhoThetagivenP(p_o[1]) / rho_o[1];
+        p_o[0] = p_0 + hz * rho_o[1] * g;
+        pi_o[0] = getExnergivenP(p_o[0], rdOcp);
+        th_o[0] = getRhoThetagivenP(p_o[0]) / rho_o[0];
+        for (int k = 1; k <= nz; ++k) {
+            int kk = k + 1;  // k == nz is the top ghost cell
+            double di = 0.5 * (rho_o[kk] + rho_o[kk - 1]);
+            p_o[kk] = p_o[kk - 1] - c.dz * di * g;
+            pi_o[kk] = getExnergivenP(p_o[kk], rdOcp);
+            th_o[kk] = getRhoThetagivenP(p_o[kk]) / rho_o[kk];
+        }
+    }
+};
+
+// dense valid-region <-> Fab
+void load_cc(Fab& f, const double* a, int nx, int ny, int nz, int nc) {
+    for (int n = 0; n < nc; ++n)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) f(i, j, k, n) = a[(((size_t)n * nz + k) * ny + j) * nx + i];
+}
+void store_cc(const Fab& f, double* a, int nx, int ny, int nz, int nc) {
+    for (int n = 0; n < nc; ++n)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) a[(((size_t)n * nz + k) * ny + j) * nx + i] = f(i, j, k, n);
+}
+void load_box(Fab& f, const double* a, int mx, int my, int mz) {
+    for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; ++j)
+            for (int i = 0; i < mx; ++i) f(i, j, k) = a[((size_t)k * my + j) * mx + i];
+}
+void store_box(const Fab& f, double* a, int mx, int my, int mz) {
+    for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; ++j)
+            for (int i = 0; i < mx; ++i) a[((size_t)k * my + j) * mx + i] = f(i, j, k);
+}
+
+}  // namespace
+
+// ============================================================================
+// C entry points for the test harness (ctypes)
+// ============================================================================
+extern "C" {
+
+int oracle_make_base_state(const erf_b200_config* cfg, const double* th_cc, const double* qv_cc, double th_s,
+                           double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0) {
+    Oracle o(*cfg);
+    o.make_base_state(th_cc, qv_cc, th_s, qv_s, p_s, rho0, p0, pi0, th0);
+    return 0;
+}
+
+// Advance `nsteps` full steps.  base: rho0,p0,pi0,th0 each nz+2.
+int oracle_advance(const erf_b200_config* cfg, const double* rho0, const double* p0, const double* pi0,
+                   const double* th0, double* cons, double* u, double* v, double* w, int nsteps) {
+    std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
+    for (int k = 0; k < nz + 2; ++k) { o->r0[k] = rho0[k]; o->p0[k] = p0[k]; o->pi0[k] = pi0[k]; o->th0[k] = th0[k]; }
+    o->init_storage();
+    o->alloc(o->cons_state, CC, o->ngc, o->ncomp);
+    o->alloc_vel(o->vel_state);
+    load_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    load_box(o->vel_state.u, u, nx + 1, ny, nz);
+    load_box(o->vel_state.v, v, nx, ny + 1, nz);
+    load_box(o->vel_state.w, w, nx, ny, nz + 1);
+    for (int s = 0; s < nsteps; ++s) o->step(cfg->dt);
+    store_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    store_box(o->vel_state.u, u, nx + 1, ny, nz);
+    store_box(o->vel_state.v, v, nx, ny + 1, nz);
+    store_box(o->vel_state.w, w, nx, ny, nz + 1);
+    return 0;
+}
+
+// Interpolant known-answer hook: evaluates one face interpolant.
+double oracle_interp(int type, const double* s6, double upw, double frac) { return Oracle::interp(type, s6, upw, frac); }
+
+// Saturation mixing ratio over water (hPa input), for known-answer tests.
+double oracle_qsatw(double t, double p_hpa) { return qsatw(t, p_hpa); }
+
+}  // extern "C"
