@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Benchmark of the multirate RK3 dycore step: cell-RK3-steps/s on B200.
+
+Workload (default): the moist warm-bubble case, 128 x 128 x 80 cells,
+Kessler microphysics, Upwind_5th dycore, WENO5 scalars, buoyancy type 2,
+dt = 2 s with 6 acoustic substeps per RK3 stage 3 (10 substeps per step),
+plain FP64 arithmetic.  A "step" is one full RK3 step of the whole domain
+including all acoustic substeps and the Kessler pass.  Inputs are synthetic
+and seeded (erf_b200/cases.py); the device working set (~0.9 GB) is larger
+than the 126 MB L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line is printed by rank 0.  Under torchrun each rank advances its
+own replica of the workload (the path does not shard: replicas only) and the
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from erf_b200 import cases  # noqa: E402
+
+METRIC = "cell-RK3-steps/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Algorithmic bytes per cell for each kernel slot: every array the pass must
+# read or write, counted once, at 8 bytes (FP64).  The derivation per slot is
+# in DESIGN.md ("Kernels and their rooflines").
+# ---------------------------------------------------------------------------
+def algorithmic_values_per_cell(cfg):
+    moist = cfg.moisture != 0
+    nq = cfg.ncomp - 5
+    diff = cfg.les_type != 0 or cfg.molec_diff_type != 0
+    return {
+        # reads cons(ncomp) + u,v,w; writes 3 momenta, 3 velocities, prim (ncomp-1), pi, p'
+        "step_begin": cfg.ncomp + 3 + 3 + 3 + (cfg.ncomp - 1) + 2 + (1 if cfg.les_type == 1 else 0),
+        "stress": 4 + (1 if diff else 0) + 6,
+        # reads 3 momenta, theta, (rho, mu for diffusion); writes rhs rho, rho-theta, 3 avg momenta
+        "slow_cell": 3 + 1 + (2 if diff else 0) + 2 + 3,
+        "plane_avg": 5 if moist else 2,
+        # reads 3 momenta, 3 velocities, rho, p', (moisture 2), (6 stresses); writes 3 rhs
+        "slow_mom": 3 + 3 + 1 + 1 + (2 if moist else 0) + (6 if diff else 0) + 3,
+        # reads prev 2 mom + rho-theta (+rho), stage 2 mom + rho-theta, 2 rhs, lag, pi, (q 2),
+        # avg 2; writes avg 2, new 2 mom, lag
+        "fast_horizontal": 3 + 3 + 2 + 1 + 1 + (2 if moist else 0) + 2 + 2 + 2 + 1,
+        # reads prev rho, rho-theta, w-mom; stage rho, rho-theta, 3 mom; new 2 mom; theta; pi;
+        # (q 2); rhs rho, rho-theta, w; avg w; writes rho, rho-theta, w-mom, avg w
+        "fast_column": 3 + 5 + 2 + 1 + 1 + (2 if moist else 0) + 3 + 1 + 4,
+        # reads scalars prim (1+nq), 3 avg mom, old scalars (1+nq), sum rho, rho-theta, 3 mom;
+        # writes new cons (ncomp), 3 mom, 3 vel, next prim (ncomp-1), pi, p'
+        "slow_post": (1 + nq) * 2 + 3 + 5 + cfg.ncomp + 6 + (cfg.ncomp - 1) + 2,
+        # reads rho, rho-theta, 3 moisture; writes rho-theta, 3 moisture
+        "kessler": (5 + 4) if moist else 0,
+    }
+
+
+def sample_clocks(stop, out):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except Exception:
+        return
+    dev = os.environ.get("LOCAL_RANK", "0")
+    try:
+        while not stop.is_set():
+            line = p.stdout.readline()
+            if not line:
+                break
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[0] == dev:
+                out.append(f)
+    finally:
+        p.terminate()
+        try:
+            p.wait(timeout=2)
+        except Exception:
+            p.kill()
+
+
+def summarize_clocks(samples):
+    if not samples:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    sm = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
+    mx = [float(s[2]) for s in samples if s[2].replace(".", "").isdigit()]
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = []
+    for q, nm in enumerate(names):
+        if any(s[5 + q].lower().startswith("active") for s in samples):
+            reasons.append(nm)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons, "samples": len(samples)}
+
+
+def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
+    """Time the FP64 CPU oracle on a bounded sample of the workload."""
+    import oracle
+    case = case_fn(nx=nx, ny=ny, nz=nz)
+    base = oracle.make_base_state(case.cfg, case)
+    cons, u, v, w = case.build_state(base[0])
+    oracle.advance(case.cfg, base, cons, u, v, w, 1)  # warm the library / page in
+    t0 = time.perf_counter()
+    oracle.advance(case.cfg, base, cons, u, v, w, nsteps)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return nx * ny * nz * nsteps / dt, dt, cores
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU FP64 oracle (a restatement of the reference's own
+    CPU path; the reference itself cannot be built here) on the host cores."""
+    if rank != 0:
+        return 0
+    case_fn = cases.CASES[args.case]
+    full = case_fn()
+    # each step is a bounded sample: a 64 x 64 column block of the same case
+    nx, ny, nz = min(64, full.cfg.nx), min(64, full.cfg.ny), full.cfg.nz
+    import oracle
+    case = case_fn(nx=nx, ny=ny, nz=nz)
+    base = oracle.make_base_state(case.cfg, case)
+    cons, u, v, w = case.build_state(base[0])
+    st = (cons, u, v, w)
+    for _ in range(args.warmup):
+        st = oracle.advance(case.cfg, base, *st, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = oracle.advance(case.cfg, base, *st, 1)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = nx * ny * nz * args.steps / dt
+    sample = f"{args.steps} steps of a {nx}x{ny}x{nz} block of the {args.case} case per run, FP64, OpenMP"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.case} {full.cfg.nx}x{full.cfg.ny}x{full.cfg.nz} (sampled {nx}x{ny}x{nz})",
+                   "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--case", default="moist_bubble", choices=sorted(cases.CASES))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from erf_b200 import Dycore
+    case = cases.CASES[args.case]()
+    cfg = case.cfg
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    dy = Dycore(cfg, stream=stream.cuda_stream)
+    base = dy.make_base_state(case)
+    dy.set_base_state(base)
+    cons, u, v, w = case.build_state(base[0])
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (cons, u, v, w)]
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # ---- warm-up (graph already instantiated at create)
+    dy.advance(*dev, args.warmup)
+    barrier()
+
+    # ---- timed region 1: device-resident state, CUDA graph replay
+    clock_samples, stop = [], threading.Event()
+    th = threading.Thread(target=sample_clocks, args=(stop, clock_samples), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dy.advance(*dev, args.steps)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    stop.set()
+    th.join(timeout=5)
+    ms = max_over_ranks(ms)
+    st = dy.status()
+    n_cells = cfg.nx * cfg.ny * cfg.nz
+    value = world * n_cells * args.steps / (ms * 1e-3)
+
+    # ---- timed region 2: same K steps, eager launches with per-kernel events
+    barrier()
+    prof = dy.advance_profiled(*dev, args.steps)
+    barrier()
+
+    # ---- timed region 3: end to end through the host-buffer entry point,
+    #      pinned host memory in and out every step
+    host = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (cons, u, v, w)]
+    h2d = sum(t.numel() * 8 for t in host)
+    dy.lib.erf_b200_advance_host(dy.ctx, *[t.data_ptr() for t in host], 1)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rc = dy.lib.erf_b200_advance_host(dy.ctx, *[t.data_ptr() for t in host], 1)
+        if rc:
+            raise RuntimeError(f"advance_host rc={rc}")
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * n_cells * args.steps / e2e_s
+
+    peaks, peak_kind = load_peaks()
+    hbm = float(peaks["hbm_gbs"])
+    vals = algorithmic_values_per_cell(cfg)
+    kern = {}
+    for name, (kms, cnt) in prof.items():
+        if cnt == 0:
+            continue
+        per_launch_ms = kms / cnt
+        nb = vals.get(name, 0) * 8 * n_cells
+        if name == "plane_avg":
+            nb = vals[name] * 8 * n_cells
+        kern[name] = {"launches": cnt, "total_ms": kms, "ms_per_launch": per_launch_ms,
+                      "algo_bytes": nb, "gbs": nb / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else None}
+    dominant = max(kern, key=lambda k: kern[k]["total_ms"])
+    dk = kern[dominant]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            traffic = json.load(fh).get(args.case, {}).get(dominant)
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm, "unit": "GB/s",
+                "frac": dk["gbs"] / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                "algo_bytes_per_launch": dk["algo_bytes"], "ms_per_launch": dk["ms_per_launch"]}
+    step_bytes = sum(vals[k] * 8 * n_cells * (kern[k]["launches"] / args.steps) for k in kern)
+    roof_cells = hbm * 1e9 / (step_bytes / n_cells)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        bx, by = min(64, cfg.nx), min(64, cfg.ny)
+        v_cpu, t_cpu, cores = cpu_baseline_run(cases.CASES[args.case], bx, by, cfg.nz, 2)
+        cpu = {"value": v_cpu, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+               "sample": f"2 steps of a {bx}x{by}x{cfg.nz} block of the {args.case} case "
+                         f"({t_cpu:.1f} s, FP64 oracle, OpenMP)"}
+
+    launches = dy.kernels_per_step() * args.steps
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.case} {cfg.nx}x{cfg.ny}x{cfg.nz}, Kessler, Upwind_5th dycore, "
+                                   f"WENO5 scalars, dt={cfg.dt} s, {cfg.mri_ratio} substeps/RK stage 3, FP64 plain",
+                       "cells": n_cells, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "working set > 126 MB L2 (no flush needed)"},
+            "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+            "roofline": roofline,
+            "step_roofline": {"algo_bytes_per_cell_step": step_bytes / n_cells,
+                              "hbm_roof_cell_steps_per_s": roof_cells, "frac": value / world / roof_cells},
+            "kernels": kern,
+            "cpu_baseline": cpu,
+            "clocks": summarize_clocks(clock_samples),
+            "gpu_launches": launches,
+            "status": st,
+        }
+        print(json.dumps(line), flush=True)
+    dy.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -204,8 +204,31 @@ int substeps_per_step(const erf_b200_config& f) {
     return tot;
 }
 
+// Optional per-launch event timing (profiling entry point only).
+struct LaunchTimer {
+    cudaStream_t st;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> slot;
+    size_t used = 0;
+    void mark(int s) {
+        if (used + 2 > ev.size()) {
+            for (int q = 0; q < 64; ++q) { cudaEvent_t e; cudaEventCreate(&e); ev.push_back(e); }
+        }
+        cudaEventRecord(ev[used], st);
+        slot.push_back(s);
+        used += 2;
+    }
+    void done() { cudaEventRecord(ev[used - 1], st); }
+};
+#define TIMED(slotid, launch)                 \
+    do {                                      \
+        if (T) T->mark(slotid);               \
+        launch;                               \
+        if (T) T->done();                     \
+    } while (0)
+
 // Enqueue one full step with parity p (state slot p is the old state).
-void enqueue_step(erf_b200_ctx* c, int p) {
+void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
     const Params& P = c->P;
     const Geo& g = c->g;
     cudaStream_t st = c->stream;
@@ -214,8 +237,8 @@ void enqueue_step(erf_b200_ctx* c, int p) {
     double** Vnew = c->vel[1 - p];
     dim3 cb = cell_block(), cg = cell_grid(g), kb = col_block(), kg = col_grid(g);
 
-    k_step_begin<<<cg, cb, 0, st>>>(P, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
-                                    c->aux[0], c->mut);
+    TIMED(0, (k_step_begin<<<cg, cb, 0, st>>>(P, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1],
+                                              Vnew[2], c->aux[0], c->mut)));
     StateBuf stage[3] = {OLD, N0, N1};
     StateBuf outs[3] = {N0, N1, N0};
     int a = 0;
@@ -228,30 +251,30 @@ void enqueue_step(erf_b200_ctx* c, int p) {
         int nsub; double dtau, slow_dt;
         stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
         if (P.use_diff)
-            k_tau<<<cg, cb, 0, st>>>(P, Sst.cons, Vnew[0], Vnew[1], Vnew[2], c->mut, c->t11, c->t22, c->t33,
-                                     c->t12, c->t13, c->t23);
-        k_slow_cell<<<cg, cb, 0, st>>>(P, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz);
+            TIMED(1, (k_tau<<<cg, cb, 0, st>>>(P, Sst.cons, Vnew[0], Vnew[1], Vnew[2], c->mut, c->t11, c->t22,
+                                               c->t33, c->t12, c->t13, c->t23)));
+        TIMED(2, (k_slow_cell<<<cg, cb, 0, st>>>(P, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz)));
         if (P.moist && P.buoy_type == 2)
-            k_plane_avg<<<g.nz, 256, 0, st>>>(P, Sst.cons, Acur.prim, c->pavg);
-        k_slow_mom<<<cg, cb, 0, st>>>(P, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33, c->t12,
-                                      c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz);
+            TIMED(3, (k_plane_avg<<<g.nz, 256, 0, st>>>(P, Sst.cons, Acur.prim, c->pavg)));
+        TIMED(4, (k_slow_mom<<<cg, cb, 0, st>>>(P, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33,
+                                                c->t12, c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz)));
         double facinv = 1.0 / (double)nsub;
         double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
         for (int ks = 0; ks < nsub; ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
-            k_fast_h<<<cg, cb, 0, st>>>(P, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, c->Fmx, c->Fmy, c->lag[lp],
-                                        c->lag[1 - lp], c->avx, c->avy, SUM.mx, SUM.my);
+            TIMED(5, (k_fast_h<<<cg, cb, 0, st>>>(P, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, c->Fmx, c->Fmy,
+                                                  c->lag[lp], c->lag[1 - lp], c->avx, c->avy, SUM.mx, SUM.my)));
             lp ^= 1;
-            k_fast_col<<<kg, kb, 0, st>>>(P, ks, dtau, facinv, D, beta_1, beta_2, Sprev, prt, Sst, Acur, c->Fcons,
-                                          c->Fmz, SUM.mx, SUM.my, c->avz, SUM.cons, SUM.mz, c->sc_soln, c->sc_cb,
-                                          c->sc_tr0, c->sc_tr1);
+            TIMED(6, (k_fast_col<<<kg, kb, 0, st>>>(P, ks, dtau, facinv, D, beta_1, beta_2, Sprev, prt, Sst, Acur,
+                                                    c->Fcons, c->Fmz, SUM.mx, SUM.my, c->avz, SUM.cons, SUM.mz,
+                                                    c->sc_soln, c->sc_cb, c->sc_tr0, c->sc_tr1)));
         }
-        k_post<<<cg, cb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut, c->avx,
-                                  c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2]);
+        TIMED(7, (k_post<<<cg, cb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut,
+                                            c->avx, c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2])));
         a = 1 - a;
     }
-    if (P.moist) k_kessler<<<kg, kb, 0, st>>>(P, N0.cons, c->cfg.dt, c->cfg.dz);
+    if (P.moist) TIMED(8, (k_kessler<<<kg, kb, 0, st>>>(P, N0.cons, c->cfg.dt, c->cfg.dz)));
 }
 
 int build_graphs(erf_b200_ctx* c) {
@@ -482,6 +505,55 @@ int erf_b200_advance_host(erf_b200_ctx* c, double* cons, double* u, double* v, d
     CK(cudaMemcpyAsync(v, dv, nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(w, dw, nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return ERF_B200_OK;
+}
+
+int erf_b200_advance_profiled(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                              const erf_b200_fab* yvel, const erf_b200_fab* zvel, int nsteps, double* kernel_ms,
+                              int* kernel_launches, int nslots) {
+    if (!c || nsteps < 0 || !kernel_ms || !kernel_launches || nslots < ERF_B200_NUM_KERNEL_SLOTS) return ERF_B200_EINVAL;
+    if (!c->base_set) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
+        return ERF_B200_EINVAL;
+    for (int q = 0; q < nslots; ++q) { kernel_ms[q] = 0.0; kernel_launches[q] = 0; }
+    int rc;
+    if ((rc = pack(c, cons, 0, c->cfg.ncomp, c->S[0].cons))) return rc;
+    if ((rc = pack(c, xvel, 1, 1, c->vel[0][0]))) return rc;
+    if ((rc = pack(c, yvel, 2, 1, c->vel[0][1]))) return rc;
+    if ((rc = pack(c, zvel, 3, 1, c->vel[0][2]))) return rc;
+    LaunchTimer T;
+    T.st = c->stream;
+    for (int s = 0; s < nsteps; ++s) {
+        T.used = 0;
+        T.slot.clear();
+        enqueue_step(c, s & 1, &T);
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t q = 0; q < T.slot.size(); ++q) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, T.ev[2 * q], T.ev[2 * q + 1]);
+            kernel_ms[T.slot[q]] += ms;
+            kernel_launches[T.slot[q]] += 1;
+        }
+    }
+    for (cudaEvent_t e : T.ev) cudaEventDestroy(e);
+    int p = nsteps & 1;
+    if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[p].cons))) return rc;
+    if ((rc = unpack(c, xvel, 1, 1, c->vel[p][0]))) return rc;
+    if ((rc = unpack(c, yvel, 2, 1, c->vel[p][1]))) return rc;
+    if ((rc = unpack(c, zvel, 3, 1, c->vel[p][2]))) return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_kernels_per_step(const erf_b200_ctx* c, int* launches) {
+    if (!c || !launches) return ERF_B200_EINVAL;
+    int n = 1 + (c->P.moist ? 1 : 0);
+    for (int nrk = 0; nrk < 3; ++nrk) {
+        int nsub; double a, b;
+        stage_schedule(c->cfg, nrk, nsub, a, b);
+        n += 3 + (c->P.use_diff ? 1 : 0) + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0) + 2 * nsub;
+    }
+    *launches = n;
     return ERF_B200_OK;
 }
 

@@ -26,7 +26,10 @@ EXPORTS = [
     "erf_b200_get_status", "erf_b200_scratch_bytes", "erf_b200_make_base_state", "erf_b200_set_base_state",
     "erf_b200_advance", "erf_b200_advance_host", "erf_b200_turbulent_viscosity", "erf_b200_slow_rhs_pre",
     "erf_b200_make_fast_coeffs", "erf_b200_fast_rhs_N", "erf_b200_slow_rhs_post", "erf_b200_kessler_advance",
+    "erf_b200_advance_profiled", "erf_b200_kernels_per_step",
 ]
+KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
+                "slow_post", "kessler"]
 
 
 class ErfFab(ctypes.Structure):
@@ -63,6 +66,9 @@ def load_library():
     L.erf_b200_advance.argtypes = [vp, fabp, fabp, fabp, fabp, i]
     L.erf_b200_advance_host.argtypes = [vp, dp, dp, dp, dp, i]
     L.erf_b200_kessler_advance.argtypes = [vp, fabp, ctypes.c_double]
+    L.erf_b200_advance_profiled.argtypes = [vp, fabp, fabp, fabp, fabp, i, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_int), i]
+    L.erf_b200_kernels_per_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -166,3 +172,24 @@ class Dycore:
         fw = dense_fab(w_t, 3, c.nx, c.ny, c.nz)
         _check(self.lib.erf_b200_advance(self._ctx, ctypes.byref(fc), ctypes.byref(fu), ctypes.byref(fv),
                                          ctypes.byref(fw), int(nsteps)), "advance")
+
+    def kernels_per_step(self) -> int:
+        n = ctypes.c_int()
+        _check(self.lib.erf_b200_kernels_per_step(self._ctx, ctypes.byref(n)), "kernels_per_step")
+        return n.value
+
+    def advance_profiled(self, cons_t, u_t, v_t, w_t, nsteps: int):
+        """Eager (graph-less) advance with CUDA events around every kernel.
+
+        Returns {slot name: (total_ms, launches)}."""
+        c = self.cfg
+        fc = dense_fab(cons_t, 0, c.nx, c.ny, c.nz, c.ncomp)
+        fu = dense_fab(u_t, 1, c.nx, c.ny, c.nz)
+        fv = dense_fab(v_t, 2, c.nx, c.ny, c.nz)
+        fw = dense_fab(w_t, 3, c.nx, c.ny, c.nz)
+        n = len(KERNEL_SLOTS)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int * n)()
+        _check(self.lib.erf_b200_advance_profiled(self._ctx, ctypes.byref(fc), ctypes.byref(fu), ctypes.byref(fv),
+                                                  ctypes.byref(fw), int(nsteps), ms, cnt, n), "advance_profiled")
+        return {KERNEL_SLOTS[q]: (ms[q], cnt[q]) for q in range(n)}

@@ -222,6 +222,25 @@ int erf_b200_advance_host(erf_b200_ctx* ctx, double* cons, double* u,
                           double* v, double* w, int nsteps);
 
 /* ----------------------------------------------------------------------------
+ * Instrumentation (no counterpart in the reference, which only has TinyProfiler
+ * regions, Source/TimeIntegration/ERF_MRI.H:189): erf_b200_advance without the
+ * CUDA graph, with a CUDA event pair around every kernel launch.  kernel_ms /
+ * kernel_launches (nslots >= ERF_B200_NUM_KERNEL_SLOTS) receive the summed
+ * device time and launch count per kernel slot:
+ *   0 step_begin, 1 stress, 2 slow_cell, 3 plane_avg, 4 slow_mom,
+ *   5 fast_horizontal, 6 fast_column, 7 slow_post, 8 kessler.
+ * ------------------------------------------------------------------------- */
+#define ERF_B200_NUM_KERNEL_SLOTS 9
+int erf_b200_advance_profiled(erf_b200_ctx* ctx,
+                              const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                              const erf_b200_fab* yvel, const erf_b200_fab* zvel,
+                              int nsteps, double* kernel_ms, int* kernel_launches,
+                              int nslots);
+
+/* Number of kernel launches one step issues (the CUDA graph's node count). */
+int erf_b200_kernels_per_step(const erf_b200_ctx* ctx, int* launches);
+
+/* ----------------------------------------------------------------------------
  * Per-pass entry points with the roles and argument order of the reference
  * functions, for callers that keep their own integrator.  State vectors are
  * passed as arrays of 4 fabs {cons, xmom, ymom, zmom} (IntVars order).

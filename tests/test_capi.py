@@ -1,0 +1,89 @@
+"""The C-ABI library loads and exports every symbol include/erf_b200.h declares,
+and the ctypes mirrors have the C struct layouts (no GPU compute here)."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from erf_b200 import config as C
+from erf_b200 import dycore
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "erf_b200.h")
+
+
+def declared_functions():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^int\s+(erf_b200_\w+)\s*\(", txt, flags=re.M)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(dycore.LIB_PATH):
+        from erf_b200 import build
+        build.build()
+    return ctypes.CDLL(dycore.LIB_PATH)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "erf_b200_advance" in names and "erf_b200_create" in names
+    assert len(names) >= 16
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_lists_every_symbol():
+    assert sorted(dycore.EXPORTS) == declared_functions()
+
+
+def test_struct_layouts_match_c():
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "erf_b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(erf_b200_config), sizeof(erf_b200_fab),
+         offsetof(erf_b200_config, abl_geo_forcing), offsetof(erf_b200_config, precision),
+         offsetof(erf_b200_fab, nstride));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        cpath = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(cpath, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), cpath, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    sc, sf, og, op, on = map(int, out)
+    assert sc == ctypes.sizeof(C.ErfConfig)
+    assert sf == ctypes.sizeof(dycore.ErfFab)
+    assert og == C.ErfConfig.abl_geo_forcing.offset
+    assert op == C.ErfConfig.precision.offset
+    assert on == dycore.ErfFab.nstride.offset
+
+
+def test_config_defaults_match_c(lib):
+    c = C.ErfConfig()
+    lib.erf_b200_config_defaults.argtypes = [ctypes.c_void_p]
+    assert lib.erf_b200_config_defaults(ctypes.byref(c)) == 0
+    d = C.defaults()
+    for name, _ in C.ErfConfig._fields_:
+        if name in ("reserved", "abl_geo_forcing"):
+            continue
+        assert getattr(c, name) == pytest.approx(getattr(d, name)), name
+
+
+def test_create_rejects_bad_config_without_gpu(lib):
+    # validation happens before any CUDA call
+    c = C.defaults()
+    c.mri_ratio = 5
+    ctx = ctypes.c_void_p()
+    lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
+    assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
