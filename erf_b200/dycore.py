@@ -26,7 +26,7 @@ EXPORTS = [
     "erf_b200_get_status", "erf_b200_scratch_bytes", "erf_b200_make_base_state", "erf_b200_set_base_state",
     "erf_b200_advance", "erf_b200_advance_host", "erf_b200_turbulent_viscosity", "erf_b200_slow_rhs_pre",
     "erf_b200_make_fast_coeffs", "erf_b200_fast_rhs_N", "erf_b200_slow_rhs_post", "erf_b200_kessler_advance",
-    "erf_b200_advance_profiled", "erf_b200_kernels_per_step",
+    "erf_b200_advance_profiled", "erf_b200_kernels_per_step", "erf_b200_kessler_advance_noalloc",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler"]
@@ -69,6 +69,7 @@ def load_library():
     L.erf_b200_advance_profiled.argtypes = [vp, fabp, fabp, fabp, fabp, i, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_int), i]
     L.erf_b200_kernels_per_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.erf_b200_kessler_advance_noalloc.argtypes = [vp, fabp, ctypes.c_double, vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _lib = L

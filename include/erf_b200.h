@@ -289,6 +289,28 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* ctx, int nrk, double slow_dt,
  * ERF_Update_Kessler.cpp:14-40), in place on cons. */
 int erf_b200_kessler_advance(erf_b200_ctx* ctx, const erf_b200_fab* cons, double dt);
 
+/* ----------------------------------------------------------------------------
+ * Allocation-free Kessler step.  No counterpart in the reference: it is the
+ * same computation as erf_b200_kessler_advance for callers that cannot
+ * allocate device memory -- a host code whose device memory is all reserved
+ * by its own pool (an AMReX arena, say), or code that runs while a CUDA graph
+ * is being captured on its stream, where cudaMalloc is not allowed.  It takes
+ * no context.  Its scratch is one library-owned device array of
+ * ERF_B200_NOALLOC_MAX_DOUBLES doubles (16 MiB), present on every GPU that
+ * loads the library until the process exits; requests with
+ * ncomp*nx*ny*nz > ERF_B200_NOALLOC_MAX_DOUBLES are rejected with
+ * ERF_B200_EINVAL.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current, so make that first
+ * call before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams, or different host threads on the
+ * same device) race, so serialise them.  Asynchronous on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).
+ * ------------------------------------------------------------------------- */
+#define ERF_B200_NOALLOC_MAX_DOUBLES 2097152
+int erf_b200_kessler_advance_noalloc(const erf_b200_config* cfg,
+                                     const erf_b200_fab* cons, double dt,
+                                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif
