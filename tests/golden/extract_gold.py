@@ -1,0 +1,26 @@
+"""Extract the reference's gold plotfiles used to pin the oracle into .npz
+fixtures (run in a checkout that has the reference tree):
+
+    python tests/golden/extract_gold.py /path/to/ERF
+
+Source: Tests/ERFGoldFiles/<name>/ (AMReX plotfiles written by ERF's CTest
+regression runs, Tests/CTestList.cmake:177).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+from plotfile import read_plotfile  # noqa: E402
+
+TESTS = ["TaylorGreenAdvecting", "TaylorGreenAdvectingDiffusing"]
+
+if __name__ == "__main__":
+    ref = sys.argv[1]
+    for name in TESTS:
+        pf = read_plotfile(os.path.join(ref, "Tests", "ERFGoldFiles", name))
+        out = os.path.join(HERE, f"{name}_gold.npz")
+        np.savez_compressed(out, data=pf["data"], names=np.array(pf["names"]), time=pf["time"])
+        print(out, pf["data"].shape, pf["names"], pf["time"])

@@ -57,3 +57,20 @@ def test_moist_bubble_kessler_weno5(nsteps):
     assert st == 0
     bad = {k: v for k, v in errs.items() if not v <= TOL}
     assert not bad, errs
+
+
+@pytest.mark.parametrize("diffusing", [False, True])
+def test_gpu_reproduces_taylor_green_gold(diffusing):
+    """The CUDA path against the reference's gold plotfile directly."""
+    import os
+    from golden.reference_cases import plot_variables, taylor_green
+    name, cfg, base, state, nsteps = taylor_green(diffusing)
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"{name}_gold.npz"))
+    dy = _dycore(cfg)
+    dy.set_base_state(base)
+    out = dy.advance_host(*state, nsteps)
+    assert dy.status() == 0
+    dy.close()
+    for nm, a, b in zip(gold["names"], plot_variables(out), gold["data"]):
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert err <= 2e-10, (str(nm), err)
