@@ -67,14 +67,17 @@ def algorithmic_values_per_cell(cfg):
         # reads prev 2 mom + rho-theta (+rho), stage 2 mom + rho-theta, 2 rhs, lag, pi, (q 2),
         # avg 2; writes avg 2, new 2 mom, lag
         "fast_horizontal": 3 + 3 + 2 + 1 + 1 + (2 if moist else 0) + 2 + 2 + 2 + 1,
-        # reads prev rho, rho-theta, w-mom; stage rho, rho-theta, 3 mom; new 2 mom; theta; pi;
-        # (q 2); rhs rho, rho-theta, w; avg w; writes rho, rho-theta, w-mom, avg w
-        "fast_column": 3 + 5 + 2 + 1 + 1 + (2 if moist else 0) + 3 + 1 + 4,
+        # reads prev rho, rho-theta, w-mom; stage rho, rho-theta, 3 mom; new 2 mom; theta;
+        # coefficients A, 1/B', C/B', P, Q; rhs rho, rho-theta, w; avg w;
+        # writes rho, rho-theta, w-mom, avg w
+        "fast_column": 3 + 5 + 2 + 1 + 5 + 3 + 1 + 4,
         # reads scalars prim (1+nq), 3 avg mom, old scalars (1+nq), sum rho, rho-theta, 3 mom;
         # writes new cons (ncomp), 3 mom, 3 vel, next prim (ncomp-1), pi, p'
         "slow_post": (1 + nq) * 2 + 3 + 5 + cfg.ncomp + 6 + (cfg.ncomp - 1) + 2,
-        # reads rho, rho-theta, 3 moisture; writes rho-theta, 3 moisture
-        "kessler": (5 + 4) if moist else 0,
+        # reads rho, rho-theta, 3 moisture; writes all ncomp (into the other buffer)
+        "kessler": (5 + cfg.ncomp) if moist else 0,
+        # reads stage rho-theta, theta, pi, (q 2); writes A, 1/B', C/B', P, Q
+        "fast_coeffs": 3 + (2 if moist else 0) + 5,
     }
 
 

@@ -32,6 +32,14 @@ __global__ void k_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, St
                        StageAux Acur, StageAux Anext, int make_next, const double* mut, const double* avx,
                        const double* avy, const double* avz, double* un, double* vn, double* wn);
 __global__ void k_kessler(Params P, double* cons, double dtn, double dz);
+__global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double* cA, double* cInvB, double* cCB,
+                            double* cP, double* cQ);
+__global__ void k_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
+                            int prev_rt, StateBuf Sst, StageAux A, const double* Fcons, const double* Fmz,
+                            const double* newx, const double* newy, const double* cA, const double* cInvB,
+                            const double* cCB, const double* cP, const double* cQ, double* avz, double* out_cons,
+                            double* out_mz);
+__global__ void k_kessler_cells(Params P, const double* cin, double* cout, double dtn, double dz);
 __global__ void k_base_state(int nz, double dz, double g, double rdOcp, const double* th_cc, const double* qv_cc,
                              double th_s, double qv_s, double p_s, double* rho0, double* p0o, double* pi0o,
                              double* th0o);
@@ -61,7 +69,9 @@ struct erf_b200_ctx {
     double* mut;
     double *t11, *t22, *t33, *t12, *t13, *t23;
     double* pavg;
-    double *sc_soln, *sc_cb, *sc_tr0, *sc_tr1;
+    double *cA, *cInvB, *cCB, *cP, *cQ;  // fast coefficients of the current stage
+    int tile_tx = 32, vert_warps = 16, coef_warps = 8;
+    size_t vert_smem = 0, coef_smem = 0;
     double *r0, *p0, *pi0, *th0;
     double *h_stage;          // device staging buffers for the host-array entry point
     int* status;
@@ -239,8 +249,13 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
 
     TIMED(0, (k_step_begin<<<cg, cb, 0, st>>>(P, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1],
                                               Vnew[2], c->aux[0], c->mut)));
-    StateBuf stage[3] = {OLD, N0, N1};
+    // stage outputs alternate between the two scratch states so that the last
+    // one lands in slot 1-p (or in N1 when Kessler moves it to slot 1-p)
     StateBuf outs[3] = {N0, N1, N0};
+    if (P.moist) { outs[0] = N1; outs[1] = N0; outs[2] = N1; }
+    StateBuf stage[3] = {OLD, outs[0], outs[1]};
+    dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
+    dim3 tcb(c->tile_tx, c->coef_warps, 1);
     int a = 0;
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
@@ -260,21 +275,24 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
                                                 c->t12, c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz)));
         double facinv = 1.0 / (double)nsub;
         double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
+        TIMED(9, (k_fast_coef<<<tg, tcb, c->coef_smem, st>>>(P, D, Sst, Acur, c->cA, c->cInvB, c->cCB, c->cP,
+                                                             c->cQ)));
         for (int ks = 0; ks < nsub; ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
             TIMED(5, (k_fast_h<<<cg, cb, 0, st>>>(P, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, c->Fmx, c->Fmy,
                                                   c->lag[lp], c->lag[1 - lp], c->avx, c->avy, SUM.mx, SUM.my)));
             lp ^= 1;
-            TIMED(6, (k_fast_col<<<kg, kb, 0, st>>>(P, ks, dtau, facinv, D, beta_1, beta_2, Sprev, prt, Sst, Acur,
-                                                    c->Fcons, c->Fmz, SUM.mx, SUM.my, c->avz, SUM.cons, SUM.mz,
-                                                    c->sc_soln, c->sc_cb, c->sc_tr0, c->sc_tr1)));
+            TIMED(6, (k_fast_vert<<<tg, tb, c->vert_smem, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, prt, Sst,
+                                                                Acur, c->Fcons, c->Fmz, SUM.mx, SUM.my, c->cA,
+                                                                c->cInvB, c->cCB, c->cP, c->cQ, c->avz, SUM.cons,
+                                                                SUM.mz)));
         }
         TIMED(7, (k_post<<<cg, cb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut,
                                             c->avx, c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2])));
         a = 1 - a;
     }
-    if (P.moist) TIMED(8, (k_kessler<<<kg, kb, 0, st>>>(P, N0.cons, c->cfg.dt, c->cfg.dz)));
+    if (P.moist) TIMED(8, (k_kessler_cells<<<cg, cb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
 }
 
 int build_graphs(erf_b200_ctx* c) {
@@ -378,7 +396,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     A(&c->mut, N);
     A(&c->t11, N); A(&c->t22, N); A(&c->t33, N); A(&c->t12, N); A(&c->t13, NZF); A(&c->t23, NZF);
     A(&c->pavg, 5 * cfg->nz);
-    A(&c->sc_soln, N); A(&c->sc_cb, N); A(&c->sc_tr0, N); A(&c->sc_tr1, N);
+    A(&c->cA, NZF); A(&c->cInvB, NZF); A(&c->cCB, NZF); A(&c->cP, NZF); A(&c->cQ, NZF);
     A(&c->r0, cfg->nz + 2); A(&c->p0, cfg->nz + 2); A(&c->pi0, cfg->nz + 2); A(&c->th0, cfg->nz + 2);
     if (rc == ERF_B200_OK) {
         void* q = nullptr;
@@ -388,6 +406,24 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     make_params(c);
     c->lag_parity_per_step = substeps_per_step(c->cfg) & 1;
+    // shared-memory tiles of the vertical kernels: TX columns x all levels
+    {
+        const size_t max_smem = 227 * 1024;
+        int nz = cfg->nz;
+        c->tile_tx = 32;
+        while (c->tile_tx > 4 && (size_t)(7 * nz + 5) * c->tile_tx * sizeof(double) > max_smem) c->tile_tx /= 2;
+        c->vert_smem = (size_t)(7 * nz + 5) * c->tile_tx * sizeof(double);
+        c->coef_smem = (size_t)3 * (nz + 1) * c->tile_tx * sizeof(double);
+        if (c->vert_smem > max_smem) rc = ERF_B200_ECONFIG;
+        c->vert_warps = c->tile_tx == 32 ? 16 : 32;
+        c->coef_warps = c->tile_tx == 32 ? 8 : 16;
+        if (rc == ERF_B200_OK) {
+            if (cudaFuncSetAttribute(k_fast_vert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->vert_smem) != cudaSuccess ||
+                cudaFuncSetAttribute(k_fast_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->coef_smem) != cudaSuccess)
+                rc = ERF_B200_ECUDA;
+        }
+        if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
+    }
     rc = build_graphs(c);
     if (rc == ERF_B200_OK) rc = cuda_fail(cudaStreamSynchronize(c->stream));
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
@@ -551,7 +587,7 @@ int erf_b200_kernels_per_step(const erf_b200_ctx* c, int* launches) {
     for (int nrk = 0; nrk < 3; ++nrk) {
         int nsub; double a, b;
         stage_schedule(c->cfg, nrk, nsub, a, b);
-        n += 3 + (c->P.use_diff ? 1 : 0) + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0) + 2 * nsub;
+        n += 4 + (c->P.use_diff ? 1 : 0) + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0) + 2 * nsub;
     }
     *launches = n;
     return ERF_B200_OK;

@@ -1027,3 +1027,311 @@ __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const doubl
 }
 
 }  // namespace erfb
+
+namespace erfb {
+
+// ---------------------------------------------------------------------------
+// Tile layout shared by the two vertical kernels below: a block owns TX
+// adjacent columns (i = blockIdx.x*TX + threadIdx.x, j = blockIdx.y) and
+// blockDim.y warps split the levels; per-column data live in shared memory as
+// [level][column] so a warp touches consecutive banks.
+// ---------------------------------------------------------------------------
+struct Tile {
+    int i, j, lane, w, nw, tx;
+    bool ok;
+    __device__ Tile(const Geo& g) {
+        tx = blockDim.x; lane = threadIdx.x; w = threadIdx.y; nw = blockDim.y;
+        i = blockIdx.x * tx + lane; j = blockIdx.y;
+        ok = i < g.nx;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Fast coefficients of one RK stage (make_fast_coeffs,
+// TimeIntegration/ERF_make_fast_coeffs.cpp:160-290, no terrain): P and Q
+// (divided by 1+q when moist), A, B, C on interior z-faces, Dirichlet rows at
+// the walls, then the Thomas forward elimination of B.  Stored per face:
+// A, 1/B' (B' at the wall rows, which the reference leaves uninverted),
+// C/B', P, Q.  Levels are computed in parallel; the B' recurrence runs in one
+// warp from shared memory.
+// ---------------------------------------------------------------------------
+__global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double* __restrict__ cA,
+                            double* __restrict__ cInvB, double* __restrict__ cCB, double* __restrict__ cP,
+                            double* __restrict__ cQ) {
+    extern __shared__ double sm[];
+    const Geo& g = P.g;
+    Tile t(g);
+    const int nz = g.nz, TX = t.tx;
+    double* sA = sm;
+    double* sB = sA + (nz + 1) * TX;
+    double* sC = sB + (nz + 1) * TX;
+    const int64_t N = g.ncell;
+    const double dzi = g.dzi, halfg = P.halfg;
+    const double* th = A.prim;
+    if (t.ok) {
+        for (int k = 1 + t.w; k <= nz - 1; k += t.nw) {
+            int64_t c = cidx(g, t.i, t.j, k), cm = c - g.sk;
+            double pi_c = 0.5 * (A.pi[cm] + A.pi[c]);
+            double P_ = -Gamma_ * R_d * dzi + halfg * R_d * P.r0[k + 1] / (P.c_v * P.pi0[k + 1] * Sst.cons[N + c]);
+            P_ *= pi_c;
+            double Q_ = Gamma_ * R_d * dzi + halfg * R_d * P.r0[k] / (P.c_v * P.pi0[k] * Sst.cons[N + cm]);
+            Q_ *= pi_c;
+            if (P.moist) {
+                double q = 0.5 * (th[4 * N + c] + th[4 * N + cm] + th[5 * N + c] + th[5 * N + cm]);
+                P_ /= (1.0 + q);
+                Q_ /= (1.0 + q);
+            }
+            double tlo = 0.5 * (th[cidx(g, t.i, t.j, clampk(k - 2, nz))] + th[cm]);
+            double tmid = 0.5 * (th[cm] + th[c]);
+            double thi = 0.5 * (th[c] + th[cidx(g, t.i, t.j, clampk(k + 1, nz))]);
+            double a = D * (halfg - Q_ * tlo);
+            double cc = D * (-halfg + P_ * thi);
+            double b = 1.0 + D * (Q_ - P_) * tmid;
+            sA[k * TX + t.lane] = a; sB[k * TX + t.lane] = b; sC[k * TX + t.lane] = cc;
+            cA[c] = a; cP[c] = P_; cQ[c] = Q_;
+        }
+        if (t.w == 0) {
+            for (int k : {0, nz}) {
+                sA[k * TX + t.lane] = 0.0; sB[k * TX + t.lane] = 1.0; sC[k * TX + t.lane] = 0.0;
+                int64_t f = cidx(g, t.i, t.j, k);
+                cA[f] = 0.0; cP[f] = 0.0; cQ[f] = 0.0;
+            }
+        }
+    }
+    __syncthreads();
+    if (t.w == 0 && t.ok) {
+        double bet = sB[t.lane];
+        int64_t f0 = cidx(g, t.i, t.j, 0);
+        cInvB[f0] = bet;               // B at the bottom row stays uninverted (== 1)
+        cCB[f0] = sC[t.lane] * bet;
+        for (int k = 1; k <= nz; ++k) {
+            double gam = sC[(k - 1) * TX + t.lane] / bet;
+            bet = sB[k * TX + t.lane] - sA[k * TX + t.lane] * gam;
+            if (!(fabs(bet) > 1e-300)) atomicOr(P.status, ST_BADSTATE);
+            double inv = (k < nz) ? 1.0 / bet : bet;
+            int64_t f = cidx(g, t.i, t.j, k);
+            cInvB[f] = inv;
+            cCB[f] = sC[k * TX + t.lane] * inv;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Acoustic substep, vertical part (erf_fast_rhs_N, ERF_fast_rhs_N.cpp:259-592):
+//   phase 1  horizontal rho / rho*theta fluxes from the new U'', V'' per cell;
+//   phase 2  right-hand side of the implicit w system per face, and
+//            d(rho w) of the previous solution;
+//   phase 3  Thomas forward / back substitution (one warp; FMA only, the
+//            stage's 1/B' and C/B' come from k_fast_coef);
+//   phase 4  vertical fluxes, average z-momentum, rho and rho*theta update.
+// All reads of the previous state happen in phases 1-2, before any write,
+// because the previous and new states may be the same buffers.
+// ---------------------------------------------------------------------------
+__global__ void k_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
+                            int prev_rt, StateBuf Sst, StageAux A, const double* __restrict__ Fcons,
+                            const double* __restrict__ Fmz, const double* __restrict__ newx,
+                            const double* __restrict__ newy, const double* __restrict__ cA,
+                            const double* __restrict__ cInvB, const double* __restrict__ cCB,
+                            const double* __restrict__ cP, const double* __restrict__ cQ, double* __restrict__ avz,
+                            double* out_cons, double* out_mz) {
+    extern __shared__ double sm[];
+    const Geo& g = P.g;
+    Tile t(g);
+    const int nz = g.nz, TX = t.tx, L = t.lane;
+    double* sT0 = sm;
+    double* sT1 = sT0 + nz * TX;
+    double* sR = sT1 + nz * TX;
+    double* sD = sR + (nz + 1) * TX;
+    double* sA = sD + (nz + 1) * TX;
+    double* sI = sA + (nz + 1) * TX;
+    double* sCB = sI + (nz + 1) * TX;
+    const int64_t N = g.ncell;
+    const double dzi = g.dzi, halfg = P.halfg;
+    const double* th = A.prim;
+    const int i = t.i, j = t.j;
+    int ip = 0, im = 0, jp = 0, jm = 0;
+    if (t.ok) { ip = wrap(i + 1, g.nx); im = wrap(i - 1, g.nx); jp = wrap(j + 1, g.ny); jm = wrap(j - 1, g.ny); }
+    auto prev_mz = [&](int k) {
+        int64_t f = cidx(g, i, j, k);
+        double m = Sprev.mz[f];
+        if (prev_rt) {
+            if (k == 0 || k == nz) return 0.0;
+            double rs = Sprev.cons[f] + Sprev.cons[f - g.sk];
+            double wt = (m * 2.0) / rs;
+            m = (wt * 0.5) * rs;
+        }
+        return m;
+    };
+    auto thz = [&](int k) { return th[cidx(g, i, j, clampk(k, nz))]; };
+    // ---- phase 1
+    if (t.ok) {
+        for (int k = t.w; k < nz; k += t.nw) {
+            int64_t c = cidx(g, i, j, k);
+            double xl = (newx[c] - Sst.mx[c]) / 1.0;
+            double xh = (newx[cidx(g, ip, j, k)] - Sst.mx[cidx(g, ip, j, k)]) / 1.0;
+            double yl = (newy[c] - Sst.my[c]) / 1.0;
+            double yh = (newy[cidx(g, i, jp, k)] - Sst.my[cidx(g, i, jp, k)]) / 1.0;
+            double mfsq = 1.0;
+            double tc = th[c];
+            sT0[k * TX + L] = (xh - xl) * g.dxi * mfsq + (yh - yl) * g.dyi * mfsq;
+            sT1[k * TX + L] = ((xh * (tc + th[cidx(g, ip, j, k)]) - xl * (tc + th[cidx(g, im, j, k)])) * g.dxi * mfsq +
+                               (yh * (tc + th[cidx(g, i, jp, k)]) - yl * (tc + th[cidx(g, i, jm, k)])) * g.dyi * mfsq) * 0.5;
+        }
+    }
+    __syncthreads();
+    // ---- phase 2
+    if (t.ok) {
+        for (int k = t.w; k <= nz; k += t.nw) {
+            int64_t f = cidx(g, i, j, k);
+            double Ok = prev_mz(k) - Sst.mz[f];
+            sD[k * TX + L] = Ok;
+            sA[k * TX + L] = cA[f];
+            sI[k * TX + L] = cInvB[f];
+            sCB[k * TX + L] = cCB[f];
+            double rhs;
+            if (k == 0 || k == nz) {
+                rhs = Ok + dtau * Fmz[f];
+            } else {
+                int64_t cm = f - g.sk;
+                double Okp1 = prev_mz(k + 1) - Sst.mz[f + g.sk];
+                double Okm1 = prev_mz(k - 1) - Sst.mz[cm];
+                double cPk = cP[f], cQk = cQ[f];
+                double tlo = 0.5 * (thz(k - 2) + thz(k - 1));
+                double tmid = 0.5 * (thz(k - 1) + thz(k));
+                double thi = 0.5 * (thz(k) + thz(k + 1));
+                double drt_k = Sprev.cons[N + f] - Sst.cons[N + f];
+                double drt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
+                double odk = Sprev.cons[f] - Sst.cons[f];
+                double odkm = Sprev.cons[cm] - Sst.cons[cm];
+                double R0 = cPk * drt_k + cQk * drt_km - halfg * (odk + odkm);
+                double R1 = halfg * (-Fcons[f] - Fcons[cm] + sT0[k * TX + L] + sT0[(k - 1) * TX + L]) +
+                            (cPk * (Fcons[N + f] - sT1[k * TX + L]) + cQk * (Fcons[N + cm] - sT1[(k - 1) * TX + L]));
+                R1 += beta_1 * dzi * ((Okp1 - Okm1) * halfg - (Okp1 * thi - Ok * tmid) * cPk - (Ok * tmid - Okm1 * tlo) * cQk);
+                rhs = Ok + dtau * (Fmz[f] + R0 + dtau * beta_2 * R1);
+            }
+            sR[k * TX + L] = rhs;
+        }
+    }
+    __syncthreads();
+    // ---- phase 3: tridiagonal solve, one warp
+    if (t.w == 0 && t.ok) {
+        double s = sR[L] * sI[L];
+        sR[L] = s;
+        for (int k = 1; k <= nz; ++k) {
+            s = (sR[k * TX + L] - sA[k * TX + L] * s) * sI[k * TX + L];
+            sR[k * TX + L] = s;
+        }
+        for (int k = nz - 1; k >= 0; --k) {
+            s = sR[k * TX + L] - sCB[k * TX + L] * s;
+            sR[k * TX + L] = s;
+        }
+    }
+    __syncthreads();
+    // ---- phase 4
+    if (t.ok) {
+        for (int k = t.w; k < nz; k += t.nw) {
+            int64_t c = cidx(g, i, j, k);
+            double sol = sR[k * TX + L], sol_hi = sR[(k + 1) * TX + L];
+            double zl = beta_2 * sol + beta_1 * sD[k * TX + L];
+            double zh = beta_2 * sol_hi + beta_1 * sD[(k + 1) * TX + L];
+            avz[c] += facinv * zl / (1.0 * 1.0);
+            if (k == nz - 1) avz[c + g.sk] += facinv * zh / (1.0 * 1.0);
+            double tc = th[c];
+            double t0 = sT0[k * TX + L] + dzi * (zh - zl);
+            double t1 = sT1[k * TX + L] + 0.5 * dzi * (zh * (tc + thz(k + 1)) - zl * (tc + thz(k - 1)));
+            double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
+            out_cons[c] = pr + dtau * (Fcons[c] - t0);
+            out_cons[N + c] = prt + dtau * (Fcons[N + c] - t1);
+            double smz = Sst.mz[c];
+            out_mz[c] = smz + sol;
+            if (k == nz - 1) out_mz[c + g.sk] = Sst.mz[c + g.sk] + sol_hi;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Kessler, one thread per cell: the fall fluxes through the cell's bottom and
+// top faces are evaluated from the pre-update neighbours, so cells are
+// independent (same arithmetic as k_kessler).
+// ---------------------------------------------------------------------------
+__global__ void k_kessler_cells(Params P, const double* __restrict__ cin, double* __restrict__ cout, double dtn,
+                                double dz) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_coords(g, i, j, k)) return;
+    const int64_t N = g.ncell;
+    const int nz = g.nz;
+    const bool rain = P.kessler_rain;
+    const bool has_qp = P.ncomp > 7;
+    const double fac_cond = lcond / P.c_p;
+    int64_t c = cidx(g, i, j, k);
+    auto qp_of = [&](int64_t cc) { return has_qp ? cin[7 * N + cc] / cin[cc] : 0.0; };
+    auto flux = [&](double ra, double qa) {
+        qa = fmax(0.0, qa);
+        double Vt = 36.34 * pow(ra * 0.001 * qa, 0.1346) * pow(ra / 1.16, -0.5);
+        double f = ra * Vt * qa;
+        return (fabs(f) < 1e-14) ? 0.0 : f;
+    };
+    double rho = cin[c];
+    double rt = cin[N + c];
+    double theta = rt / rho;
+    double qv = cin[5 * N + c] / rho;
+    double qc = cin[6 * N + c] / rho;
+    double qp = qp_of(c);
+    double tabs = eos_T(rho, rt, qv);
+    double pres = eos_p(rt, qv) / 100.;
+    if (rain) {
+        double fz_lo, fz_hi;
+        if (k == 0) fz_lo = flux(rho, qp);
+        else fz_lo = flux(0.5 * (cin[c - g.sk] + rho), 0.5 * (qp_of(c - g.sk) + qp));
+        if (k == nz - 1) fz_hi = flux(rho, qp);
+        else fz_hi = flux(0.5 * (rho + cin[c + g.sk]), 0.5 * (qp + qp_of(c + g.sk)));
+        qv = fmax(0.0, qv); qc = fmax(0.0, qc); qp = fmax(0.0, qp);
+        double es = esatw(tabs);
+        double qs = Rd_on_Rv * es / fmax(es, pres - es);
+        double dqs = Rd_on_Rv * dtesatw(tabs) / pres;
+        if (qs <= 0.0) qs = 0.0;
+        double d_c2r = 0.0, d_r2v = 0.0, d_v2c = 0.0, d_c2v = 0.0;
+        double fac = 1.0 + (L_v / Cp_d) * dqs;
+        if (qv > qs) d_v2c = fmin(qv, (qv - qs) / (1.0 + fac));
+        if (qv < qs && qc > 0.0) d_c2v = fmin(qc, (qs - qv) / (1.0 + fac));
+        if (qp > 0.0 && qv < qs) {
+            double C = 1.6 + 124.9 * pow(0.001 * rho * qp, 0.2046);
+            d_r2v = 1.0 / (0.001 * rho) * (1.0 - qv / qs) * C * pow(0.001 * rho * qp, 0.525) / (5.4e5 + 2.55e6 / (pres * qs)) * dtn;
+            d_r2v = fmin(qp, d_r2v);
+        }
+        if (qc > 0.0) {
+            double auto_r = (qc > 1.e-3) ? 1.e-3 : 0.0;
+            double accrr = 2.2 * pow(qp, 0.875);
+            d_c2r = dtn * (accrr * qc + auto_r * (qc - 1.e-3));
+            d_c2r = fmin(d_c2r, qc);
+        }
+        double dq_sed = dtn * 1.0 * (1.0 / rho) * (fz_hi - fz_lo) / dz;
+        if (fabs(dq_sed) < 1e-14) dq_sed = 0.0;
+        qv += -d_v2c + d_c2v + d_r2v;
+        qc += d_v2c - d_c2v - d_c2r;
+        qp += dq_sed + d_c2r - d_r2v;
+        theta += theta / tabs * fac_cond * (d_v2c - d_c2v - d_r2v);
+        qv = fmax(0.0, qv); qc = fmax(0.0, qc); qp = fmax(0.0, qp);
+    } else {
+        qc = fmax(0.0, qc);
+        double es = esatw(tabs);
+        double qs = Rd_on_Rv * es / fmax(es, pres - es);
+        double dqs = Rd_on_Rv * dtesatw(tabs) / pres;
+        double d_v2c = 0.0, d_c2v = 0.0;
+        double fac = 1.0 + (L_v / Cp_d) * dqs;
+        if (qv > qs) d_v2c = fmin(qv, (qv - qs) / (1.0 + fac));
+        if (qv < qs && qc > 0.0) d_c2v = fmin(qc, (qs - qv) / (1.0 + fac));
+        qv += -d_v2c + d_c2v;
+        qc += d_v2c - d_c2v;
+        theta += theta / tabs * fac_cond * (d_v2c - d_c2v);
+        qv = fmax(0.0, qv); qc = fmax(0.0, qc);
+    }
+    for (int n = 0; n < P.ncomp; ++n) cout[n * N + c] = cin[n * N + c];
+    cout[N + c] = rho * theta;
+    cout[5 * N + c] = rho * qv;
+    cout[6 * N + c] = rho * qc;
+    if (has_qp) cout[7 * N + c] = rho * qp;
+}
+
+}  // namespace erfb

@@ -29,7 +29,7 @@ EXPORTS = [
     "erf_b200_advance_profiled", "erf_b200_kernels_per_step", "erf_b200_kessler_advance_noalloc",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
-                "slow_post", "kessler"]
+                "slow_post", "kessler", "fast_coeffs"]
 
 
 class ErfFab(ctypes.Structure):

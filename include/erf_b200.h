@@ -228,9 +228,9 @@ int erf_b200_advance_host(erf_b200_ctx* ctx, double* cons, double* u,
  * kernel_launches (nslots >= ERF_B200_NUM_KERNEL_SLOTS) receive the summed
  * device time and launch count per kernel slot:
  *   0 step_begin, 1 stress, 2 slow_cell, 3 plane_avg, 4 slow_mom,
- *   5 fast_horizontal, 6 fast_column, 7 slow_post, 8 kessler.
+ *   5 fast_horizontal, 6 fast_column, 7 slow_post, 8 kessler, 9 fast_coeffs.
  * ------------------------------------------------------------------------- */
-#define ERF_B200_NUM_KERNEL_SLOTS 9
+#define ERF_B200_NUM_KERNEL_SLOTS 10
 int erf_b200_advance_profiled(erf_b200_ctx* ctx,
                               const erf_b200_fab* cons, const erf_b200_fab* xvel,
                               const erf_b200_fab* yvel, const erf_b200_fab* zvel,
