@@ -121,6 +121,22 @@ def summarize_clocks(samples):
             "reasons": reasons, "samples": len(samples)}
 
 
+def max_over_ranks(x, world, device):
+    """Max of a per-rank scalar over all ranks (the timing rule for replicas)."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return x
+
+
+def replica_throughput(world, n_cells, steps, seconds):
+    """Whole-job cell-steps/s: every rank advances its own full replica."""
+    return world * n_cells * steps / seconds
+
+
 def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
     """Time the FP64 CPU oracle on a bounded sample of the workload."""
     import oracle
@@ -213,13 +229,6 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
-
     # ---- warm-up (graph already instantiated at create)
     dy.advance(*dev, args.warmup)
     barrier()
@@ -238,10 +247,10 @@ def main():
     ms = e0.elapsed_time(e1)
     stop.set()
     th.join(timeout=5)
-    ms = max_over_ranks(ms)
+    ms = max_over_ranks(ms, world, "cuda")
     st = dy.status()
     n_cells = cfg.nx * cfg.ny * cfg.nz
-    value = world * n_cells * args.steps / (ms * 1e-3)
+    value = replica_throughput(world, n_cells, args.steps, ms * 1e-3)
 
     # ---- timed region 2: same K steps, eager launches with per-kernel events
     barrier()
@@ -260,8 +269,8 @@ def main():
         if rc:
             raise RuntimeError(f"advance_host rc={rc}")
     barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * n_cells * args.steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+    e2e = replica_throughput(world, n_cells, args.steps, e2e_s)
 
     peaks, peak_kind = load_peaks()
     hbm = float(peaks["hbm_gbs"])

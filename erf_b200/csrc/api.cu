@@ -256,6 +256,8 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
     StateBuf stage[3] = {OLD, outs[0], outs[1]};
     dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
     dim3 tcb(c->tile_tx, c->coef_warps, 1);
+    // scalar-transport tiles: 32 x 8 columns, 8 levels per block
+    dim3 ttb(32, 8, 1), ttg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + 7) / 8);
     int a = 0;
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
@@ -268,11 +270,11 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
         if (P.use_diff)
             TIMED(1, (k_tau<<<cg, cb, 0, st>>>(P, Sst.cons, Vnew[0], Vnew[1], Vnew[2], c->mut, c->t11, c->t22,
                                                c->t33, c->t12, c->t13, c->t23)));
-        TIMED(2, (k_slow_cell<<<cg, cb, 0, st>>>(P, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz)));
+        TIMED(2, (k_slow_cell<<<ttg, ttb, 0, st>>>(P, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz)));
         if (P.moist && P.buoy_type == 2)
             TIMED(3, (k_plane_avg<<<g.nz, 256, 0, st>>>(P, Sst.cons, Acur.prim, c->pavg)));
-        TIMED(4, (k_slow_mom<<<cg, cb, 0, st>>>(P, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33,
-                                                c->t12, c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz)));
+        TIMED(4, (k_slow_mom<<<ttg, ttb, 0, st>>>(P, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33,
+                                                  c->t12, c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz)));
         double facinv = 1.0 / (double)nsub;
         double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
         TIMED(9, (k_fast_coef<<<tg, tcb, c->coef_smem, st>>>(P, D, Sst, Acur, c->cA, c->cInvB, c->cCB, c->cP,
@@ -288,8 +290,8 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
                                                                 c->cInvB, c->cCB, c->cP, c->cQ, c->avz, SUM.cons,
                                                                 SUM.mz)));
         }
-        TIMED(7, (k_post<<<cg, cb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut,
-                                            c->avx, c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2])));
+        TIMED(7, (k_post<<<ttg, ttb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut,
+                                              c->avx, c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2])));
         a = 1 - a;
     }
     if (P.moist) TIMED(8, (k_kessler_cells<<<cg, cb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));

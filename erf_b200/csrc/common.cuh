@@ -100,11 +100,13 @@ struct Interp<ERF_ADV_CENTERED_6TH> {
 template <>
 struct Interp<ERF_ADV_WENO_3> {
     static constexpr int W = 2;
+    // WENO3 (ERF_Interpolation_WENO.H:9-124) with the weights normalised once.
     __device__ static __forceinline__ double ev(double a, double b, double c) {
         const double eps = 1.0e-6;
         double b1 = (b - a) * (b - a), b2 = (c - b) * (c - b);
-        double w1 = (1.0 / 3.0) / ((eps + b1) * (eps + b1));
-        double w2 = (2.0 / 3.0) / ((eps + b2) * (eps + b2));
+        double e1 = (eps + b1) * (eps + b1), e2 = (eps + b2) * (eps + b2);
+        double w1 = (1.0 / 3.0) * e2;
+        double w2 = (2.0 / 3.0) * e1;
         double ws = w1 + w2;
         double v1 = -a + 3.0 * b, v2 = b + c;
         return (w1 * v1 + w2 * v2) / (2.0 * ws);
@@ -119,14 +121,20 @@ struct Interp<ERF_ADV_WENO_3> {
 template <>
 struct Interp<ERF_ADV_WENO_5> {
     static constexpr int W = 3;
+    // Jiang-Shu WENO5 with the reference's smoothness indicators, linear
+    // weights (1/10, 3/5, 3/10) and eps = 1e-6 (ERF_Interpolation_WENO.H:
+    // 129-259).  The non-linear weights g_k / (eps + b_k)^2 are formed as
+    // g_k * prod_{m != k} (eps + b_m)^2, which has the same ratios and needs
+    // one division (the normalisation) instead of four.
     __device__ static __forceinline__ double ev(double a, double b, double c, double d, double e) {
         const double c1 = 13.0 / 12.0, eps = 1.0e-6;
         double b1 = c1 * (a - 2.0 * b + c) * (a - 2.0 * b + c) + 0.25 * (a - 4.0 * b + 3.0 * c) * (a - 4.0 * b + 3.0 * c);
         double b2 = c1 * (b - 2.0 * c + d) * (b - 2.0 * c + d) + 0.25 * (b - d) * (b - d);
         double b3 = c1 * (c - 2.0 * d + e) * (c - 2.0 * d + e) + 0.25 * (3.0 * c - 4.0 * d + e) * (3.0 * c - 4.0 * d + e);
-        double w1 = (1.0 / 10.0) / ((eps + b1) * (eps + b1));
-        double w2 = (3.0 / 5.0) / ((eps + b2) * (eps + b2));
-        double w3 = (3.0 / 10.0) / ((eps + b3) * (eps + b3));
+        double e1 = (eps + b1) * (eps + b1), e2 = (eps + b2) * (eps + b2), e3 = (eps + b3) * (eps + b3);
+        double w1 = (1.0 / 10.0) * (e2 * e3);
+        double w2 = (3.0 / 5.0) * (e1 * e3);
+        double w3 = (3.0 / 10.0) * (e1 * e2);
         double ws = w1 + w2 + w3;
         double v1 = 2.0 * a - 7.0 * b + 11.0 * c;
         double v2 = -b + 5.0 * c + 2.0 * d;

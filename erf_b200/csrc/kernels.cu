@@ -250,32 +250,6 @@ __device__ __forceinline__ double scalar_diff(const Params& P, const double* __r
     return (fxh - fxl) * g.dxi * 1.0 + (fyh - fyl) * g.dyi * 1.0 + (fzh - fzl) * g.dzi;
 }
 
-// ---------------------------------------------------------------------------
-// Slow RHS for rho and rho*theta (erf_slow_rhs_pre cell part,
-// ERF_slow_rhs_pre.cpp:462-526): AdvectionSrcForRho (also initialises the
-// average momenta to the stage mass fluxes, ERF_AdvectionSrcForState.cpp:56-71),
-// AdvectionSrcForScalars for theta, DiffusionSrcForState_N for theta.
-// ---------------------------------------------------------------------------
-__global__ void k_slow_cell(Params P, StateBuf S, StageAux A, const double* __restrict__ mut,
-                            double* __restrict__ Fcons, double* __restrict__ avx, double* __restrict__ avy,
-                            double* __restrict__ avz) {
-    const Geo& g = P.g;
-    int i, j, k;
-    if (!cell_coords(g, i, j, k)) return;
-    int ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
-    int64_t c = cidx(g, i, j, k);
-    avx[c] = S.mx[c];
-    avy[c] = S.my[c];
-    avz[c] = S.mz[c];
-    if (k == g.nz - 1) avz[c + g.sk] = S.mz[c + g.sk];
-    double fr = -1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi + (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi +
-                              (S.mz[c + g.sk] - S.mz[c]) * g.dzi);
-    Fcons[c] = fr;
-    double frt = scalar_adv_tend(P, A.prim, S.mx, S.my, S.mz, P.dry_h, P.dry_v, P.f_dry_h, P.f_dry_v, i, j, k);
-    if (P.use_diff) frt -= scalar_diff(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
-    Fcons[g.ncell + c] = frt;
-}
-
 // Horizontal plane averages of rho, theta, qv, qc, qp for buoyancy type 2
 // (SourceTerms/ERF_make_buoyancy.cpp:212-249): one block per level.
 __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const double* __restrict__ prim,
@@ -337,194 +311,6 @@ __device__ __forceinline__ double gatherz_tang(const Geo& g, const double* f, in
         s[m] = (off >= -w && off <= w - 1) ? tang(f, g, i, j, k + off) : 0.0;
     }
     return interp_rt(type, s, upw, frac);
-}
-
-// ---------------------------------------------------------------------------
-// Slow RHS for the three momenta (erf_slow_rhs_pre face part,
-// ERF_slow_rhs_pre.cpp:556-744): AdvectionSrcForMom (N), DiffusionSrcForMom_N,
-// pressure gradient of p', buoyancy / Coriolis / geostrophic sources
-// (make_mom_sources, make_buoyancy).
-// ---------------------------------------------------------------------------
-__global__ void k_slow_mom(Params P, StateBuf S, StageAux A, const double* __restrict__ u,
-                           const double* __restrict__ v, const double* __restrict__ w,
-                           const double* __restrict__ t11, const double* __restrict__ t22,
-                           const double* __restrict__ t33, const double* __restrict__ t12,
-                           const double* __restrict__ t13, const double* __restrict__ t23,
-                           const double* __restrict__ pavg, double* __restrict__ Fmx, double* __restrict__ Fmy,
-                           double* __restrict__ Fmz) {
-    const Geo& g = P.g;
-    int i, j, k;
-    if (!cell_coords(g, i, j, k)) return;
-    const int64_t N = g.ncell;
-    int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny), ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
-    int64_t c = cidx(g, i, j, k);
-    const double* ru = S.mx;
-    const double* rv = S.my;
-    const double* rw = S.mz;
-    const double* cd = S.cons;
-    const int ht = P.dyc_h, vt = P.dyc_v;
-    const double hf = P.f_dyc_h, vf = P.f_dyc_v;
-    const double* prim = A.prim;
-    const double* pp = A.pp;
-    // ---------------- x-momentum on face i
-    {
-        double a, xh, xl, yh, yl, zh, zl;
-        a = 0.5 * (ru[cidx(g, ip, j, k)] + ru[c]); xh = a * gatherx_interp(g, u, ht, a, hf, ip, j, k);
-        a = 0.5 * (ru[cidx(g, im, j, k)] + ru[c]); xl = a * gatherx_interp(g, u, ht, a, hf, i, j, k);
-        a = 0.5 * (rv[cidx(g, i, jp, k)] + rv[cidx(g, im, jp, k)]); yh = a * gathery_interp(g, u, ht, a, hf, i, jp, k);
-        a = 0.5 * (rv[c] + rv[cidx(g, im, j, k)]); yl = a * gathery_interp(g, u, ht, a, hf, i, j, k);
-        a = 0.5 * (rw[c + g.sk] + rw[cidx(g, im, j, k + 1)]); zh = a * gatherz_tang(g, u, vt, a, vf, i, j, k + 1);
-        a = 0.5 * (rw[c] + rw[cidx(g, im, j, k)]); zl = a * gatherz_tang(g, u, vt, a, vf, i, j, k);
-        double rhs = -((xh - xl) * g.dxi * 1.0 + (yh - yl) * g.dyi * 1.0 + (zh - zl) * g.dzi);
-        if (P.use_diff)
-            rhs -= ((t11[c] - t11[cidx(g, im, j, k)]) * g.dxi * 1.0 + (t12[cidx(g, i, jp, k)] - t12[c]) * g.dyi * 1.0 +
-                    (t13[c + g.sk] - t13[c]) * g.dzi);
-        double gpx = g.dxi * (pp[c] - pp[cidx(g, im, j, k)]);
-        gpx *= 1.0;
-        double q = 0.0;
-        if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + cidx(g, im, j, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, im, j, k)]);
-        double src = 0.0;
-        if (P.coriolis) {
-            double rvl = 0.25 * (rv[cidx(g, i, jp, k)] + rv[c] + rv[cidx(g, im, jp, k)] + rv[cidx(g, im, j, k)]);
-            double rwl = 0.25 * (rw[c + g.sk] + rw[c] + rw[cidx(g, i, jm, k + 1)] + rw[cidx(g, i, jm, k)]);
-            src += P.cf * (rvl * P.sinphi - rwl * P.cosphi);
-        }
-        src += 0.5 * (cd[c] + cd[cidx(g, im, j, k)]) * P.geo0;
-        rhs += (-gpx - 0.0) / (1.0 + q) + src;
-        Fmx[c] = rhs;
-    }
-    // ---------------- y-momentum on face j
-    {
-        double a, xh, xl, yh, yl, zh, zl;
-        a = 0.5 * (ru[cidx(g, ip, j, k)] + ru[cidx(g, ip, jm, k)]); xh = a * gatherx_interp(g, v, ht, a, hf, ip, j, k);
-        a = 0.5 * (ru[c] + ru[cidx(g, i, jm, k)]); xl = a * gatherx_interp(g, v, ht, a, hf, i, j, k);
-        a = 0.5 * (rv[c] + rv[cidx(g, i, jp, k)]); yh = a * gathery_interp(g, v, ht, a, hf, i, jp, k);
-        a = 0.5 * (rv[c] + rv[cidx(g, i, jm, k)]); yl = a * gathery_interp(g, v, ht, a, hf, i, j, k);
-        a = 0.5 * (rw[c + g.sk] + rw[cidx(g, i, jm, k + 1)]); zh = a * gatherz_tang(g, v, vt, a, vf, i, j, k + 1);
-        a = 0.5 * (rw[c] + rw[cidx(g, i, jm, k)]); zl = a * gatherz_tang(g, v, vt, a, vf, i, j, k);
-        double rhs = -((xh - xl) * g.dxi * 1.0 + (yh - yl) * g.dyi * 1.0 + (zh - zl) * g.dzi);
-        if (P.use_diff)
-            rhs -= ((t12[cidx(g, ip, j, k)] - t12[c]) * g.dxi * 1.0 + (t22[c] - t22[cidx(g, i, jm, k)]) * g.dyi * 1.0 +
-                    (t23[c + g.sk] - t23[c]) * g.dzi);
-        double gpy = g.dyi * (pp[c] - pp[cidx(g, i, jm, k)]);
-        gpy *= 1.0;
-        double q = 0.0;
-        if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + cidx(g, i, jm, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, i, jm, k)]);
-        double src = 0.0;
-        if (P.coriolis) {
-            double rul = 0.25 * (ru[cidx(g, ip, j, k)] + ru[c] + ru[cidx(g, ip, jm, k)] + ru[cidx(g, i, jm, k)]);
-            src += -P.cf * rul * P.sinphi;
-        }
-        src += 0.5 * (cd[c] + cd[cidx(g, i, jm, k)]) * P.geo1;
-        rhs += (-gpy - 0.0) / (1.0 + q) + src;
-        Fmy[c] = rhs;
-    }
-    // ---------------- z-momentum on face k (interior faces only)
-    if (k == 0) {
-        Fmz[c] = 0.0;
-    } else {
-        double a, xh, xl, yh, yl, zh, zl;
-        a = 0.5 * (ru[cidx(g, ip, j, k)] + ru[cidx(g, ip, j, k - 1)]) * 1.0; xh = a * gatherx_interp(g, w, ht, a, hf, ip, j, k);
-        a = 0.5 * (ru[c] + ru[cidx(g, i, j, k - 1)]) * 1.0; xl = a * gatherx_interp(g, w, ht, a, hf, i, j, k);
-        a = 0.5 * (rv[cidx(g, i, jp, k)] + rv[cidx(g, i, jp, k - 1)]) * 1.0; yh = a * gathery_interp(g, w, ht, a, hf, i, jp, k);
-        a = 0.5 * (rv[c] + rv[cidx(g, i, j, k - 1)]) * 1.0; yl = a * gathery_interp(g, w, ht, a, hf, i, j, k);
-        const int lo_z_face = 0, hi_z_face = g.nz;
-        auto wz = [&](int kk) { return __ldg(w + cidx(g, i, j, kk)); };
-        auto all = [&](int kk, double upw, double frac, int type) {
-            double s[6];
-            bool wide = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH);
-            s[0] = wide ? wz(kk - 3) : 0.0;
-            s[1] = (type == ERF_ADV_CENTERED_2ND) ? 0.0 : wz(kk - 2);
-            s[2] = wz(kk - 1);
-            s[3] = wz(kk);
-            s[4] = (type == ERF_ADV_CENTERED_2ND) ? 0.0 : wz(kk + 1);
-            s[5] = wide ? wz(kk + 2) : 0.0;
-            return interp_all(type, s, upw, frac);
-        };
-        auto normal = [&](int kk, double upw) {
-            double s[6];
-            int wd = stencil_width(vt);
-            for (int m = 0; m < 6; ++m) {
-                int off = m - 3;
-                s[m] = (off >= -wd && off <= wd - 1) ? wz(kk + off) : 0.0;
-            }
-            return interp_rt(vt, s, upw, vf);
-        };
-        double ih, il;
-        a = 0.5 * (rw[c] + rw[c + g.sk]);
-        if (k == hi_z_face - 1) ih = all(k + 1, a, 0, ERF_ADV_CENTERED_2ND);
-        else if (k == hi_z_face - 2 || k == lo_z_face + 1) {
-            if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) ih = all(k + 1, a, 0, ERF_ADV_CENTERED_4TH);
-            else ih = all(k + 1, a, vf, vt);
-        } else ih = normal(k + 1, a);
-        zh = a * ih;
-        a = 0.5 * (rw[c] + rw[c - g.sk]);
-        if (k == lo_z_face + 1) il = all(k, a, 0, ERF_ADV_CENTERED_2ND);
-        else if (k == lo_z_face + 2 || k == hi_z_face - 1) {
-            if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) il = all(k, a, 0, ERF_ADV_CENTERED_4TH);
-            else il = all(k, a, vf, vt);
-        } else il = normal(k, a);
-        zl = a * il;
-        double rhs = -((xh - xl) * g.dxi * 1.0 + (yh - yl) * g.dyi * 1.0 + (zh - zl) * g.dzi);
-        if (P.use_diff)
-            rhs -= ((t13[cidx(g, ip, j, k)] - t13[c]) * g.dxi * 1.0 + (t23[cidx(g, i, jp, k)] - t23[c]) * g.dyi * 1.0 +
-                    (t33[c] - t33[c - g.sk]) * g.dzi);
-        // buoyancy (make_buoyancy) + Coriolis + geostrophic (make_mom_sources)
-        double b;
-        double g2 = -P.gravity;
-        if (!P.moist) {
-            if (P.buoy_type == 1) {
-                b = g2 * 0.5 * ((cd[c] - P.r0[k + 1]) + (cd[c - g.sk] - P.r0[k]));
-            } else {
-                auto T0 = [&](int kk) {
-                    double rt0 = eos_rt_given_p(P.p0[kk + 1]);
-                    return (rt0 / P.r0[kk + 1]) / pow(p_0 / P.p0[kk + 1], P.rdOcp);
-                };
-                double t0h = T0(k), th_ = eos_T(cd[c], cd[N + c], 0.0);
-                double t0l = T0(k - 1), tl_ = eos_T(cd[c - g.sk], cd[N + c - g.sk], 0.0);
-                double qp_ = (th_ - t0h) / t0h, qm_ = (tl_ - t0l) / t0l;
-                double r0q = 0.5 * (P.r0[k + 1] * qp_ + P.r0[k] * qm_);
-                b = -r0q * g2;
-            }
-        } else if (P.buoy_type == 1) {
-            int nq = P.ncomp - ERF_RHOQ1_COMP;
-            double hi = cd[c] + cd[5 * N + c] + cd[6 * N + c] - P.r0[k + 1];
-            double lo = cd[c - g.sk] + cd[5 * N + c - g.sk] + cd[6 * N + c - g.sk] - P.r0[k];
-            for (int qo = 2; qo < nq; ++qo) { hi += cd[(5 + qo) * N + c]; lo += cd[(5 + qo) * N + c - g.sk]; }
-            b = g2 * 0.5 * (hi + lo);
-        } else {
-            int nq = P.ncomp - ERF_RHOQ1_COMP;
-            const double* rd = pavg;
-            const double* thd = pavg + g.nz;
-            const double* qvd = pavg + 2 * g.nz;
-            const double* qcd = pavg + 3 * g.nz;
-            const double* qpd = pavg + 4 * g.nz;
-            double tp1 = eos_T(rd[k], rd[k] * thd[k], qvd[k]);
-            double tm1 = eos_T(rd[k - 1], rd[k - 1] * thd[k - 1], qvd[k - 1]);
-            double tp3 = eos_T(cd[c], cd[N + c], cd[5 * N + c] / cd[c]);
-            double tm3 = eos_T(cd[c - g.sk], cd[N + c - g.sk], cd[5 * N + c - g.sk] / cd[c - g.sk]);
-            double qvp = nq >= 1 ? prim[4 * N + c] : 0.0, qvm = nq >= 1 ? prim[4 * N + c - g.sk] : 0.0;
-            double qcp = nq >= 2 ? prim[5 * N + c] : 0.0, qcm = nq >= 2 ? prim[5 * N + c - g.sk] : 0.0;
-            double qpp = nq >= 3 ? prim[6 * N + c] : 0.0, qpm = nq >= 3 ? prim[6 * N + c - g.sk] : 0.0;
-            double qplus = 0.61 * (qvp - qvd[k]) - (qcp - qcd[k] + qpp - qpd[k]) + (tp3 - tp1) / tp1 * (1.0 + 0.61 * qvd[k] - qcd[k] - qpd[k]);
-            double qminus = 0.61 * (qvm - qvd[k - 1]) - (qcm - qcd[k - 1] + qpm - qpd[k - 1]) + (tm3 - tm1) / tm1 * (1.0 + 0.61 * qvd[k - 1] - qcd[k - 1] - qpd[k - 1]);
-            double qavg = 0.5 * (qplus + qminus);
-            double r0avg = 0.5 * (rd[k] + rd[k - 1]);
-            b = -qavg * r0avg * g2;
-        }
-        double zsrc = b;
-        if (P.coriolis) {
-            double rul = 0.25 * (ru[cidx(g, ip, j, k)] + ru[c] + ru[cidx(g, ip, j, k - 1)] + ru[c - g.sk]);
-            zsrc += P.cf * rul * P.cosphi;
-        }
-        zsrc += 0.5 * (cd[c] + cd[c - g.sk]) * P.geo2;
-        double gpz = g.dzi * (pp[c] - pp[c - g.sk]) / 1.0;
-        double q = 0.0;
-        if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + c - g.sk] + prim[5 * N + c] + prim[5 * N + c - g.sk]);
-        rhs += (zsrc - gpz - 0.0) / (1.0 + q);
-        Fmz[c] = rhs;
-    }
-    if (k == g.nz - 1) Fmz[c + g.sk] = 0.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -753,77 +539,6 @@ __global__ void k_fast_col(Params P, int step, double dtau, double facinv, doubl
         sol_hi = sol;
         drw_hi = drw_lo;
     }
-}
-
-// ---------------------------------------------------------------------------
-// Slow RHS post + stage finalisation (erf_slow_rhs_post,
-// ERF_slow_rhs_post.cpp:228-531, and post_update = apply_bcs(S_new),
-// ERF_TI_slow_rhs_fun.H:284-288):
-//   * advection (average momenta) and diffusion of the slow scalars
-//     (passive scalar; moisture), S_new = S_old + slow_dt * RHS, clipped;
-//   * rho, rho*theta and the momenta copied from the fast solution, with the
-//     momentum/velocity round trips of the two boundary fills;
-//   * the stage velocities, and (unless last) the next stage's primitive
-//     variables, Exner function and p'.
-// ---------------------------------------------------------------------------
-__global__ void k_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
-                       StageAux Acur, StageAux Anext, int make_next, const double* __restrict__ mut,
-                       const double* __restrict__ avx, const double* __restrict__ avy, const double* __restrict__ avz,
-                       double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn) {
-    const Geo& g = P.g;
-    int i, j, k;
-    if (!cell_coords(g, i, j, k)) return;
-    const int64_t N = g.ncell;
-    int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
-    int64_t c = cidx(g, i, j, k);
-    // slow scalars
-    {
-        int n = ERF_RHOSCALAR_COMP;
-        double r = scalar_adv_tend(P, Acur.prim + (n - 1) * N, avx, avy, avz, P.dry_h, P.dry_v, P.f_dry_h, P.f_dry_v, i, j, k);
-        if (P.use_diff) r -= scalar_diff(P, Sst.cons, Acur.prim + (n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
-        Snew.cons[n * N + c] = Sold.cons[n * N + c] + slow_dt * r;
-    }
-    if (P.moist) {
-        for (int n = ERF_RHOQ1_COMP; n < P.ncomp; ++n) {
-            double r = scalar_adv_tend(P, Acur.prim + (n - 1) * N, avx, avy, avz, P.moi_h, P.moi_v, P.f_moi_h, P.f_moi_v, i, j, k);
-            if (P.use_diff) r -= scalar_diff(P, Sst.cons, Acur.prim + (n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
-            double v_ = Sold.cons[n * N + c] + slow_dt * r;
-            Snew.cons[n * N + c] = fmax(v_, 0.0);
-        }
-    }
-    Snew.cons[c] = Ssum.cons[c];
-    Snew.cons[N + c] = Ssum.cons[N + c];
-    if (Snew.cons != Sst.cons) {
-        Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
-        Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
-    }
-    // momenta: fast-fill round trip, then the post_update round trip
-    double rho = Ssum.cons[c];
-    {
-        double rs = rho + Ssum.cons[cidx(g, im, j, k)];
-        double m = Ssum.mx[c];
-        double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
-        double u2 = (m * 2.0) / rs; m = (u2 * 0.5) * rs;
-        Snew.mx[c] = m; un[c] = u2;
-    }
-    {
-        double rs = rho + Ssum.cons[cidx(g, i, jm, k)];
-        double m = Ssum.my[c];
-        double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
-        double v2 = (m * 2.0) / rs; m = (v2 * 0.5) * rs;
-        Snew.my[c] = m; vn[c] = v2;
-    }
-    if (k == 0) {
-        Snew.mz[c] = 0.0; wn[c] = 0.0;
-    } else {
-        double rs = rho + Ssum.cons[c - g.sk];
-        double m = Ssum.mz[c];
-        double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
-        double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
-        Snew.mz[c] = m; wn[c] = w2;
-    }
-    if (k == g.nz - 1) { Snew.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
-    if (make_next) stage_aux_cell(P, Snew.cons, Anext, c, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -1332,6 +1047,421 @@ __global__ void k_kessler_cells(Params P, const double* __restrict__ cin, double
     cout[5 * N + c] = rho * qv;
     cout[6 * N + c] = rho * qc;
     if (has_qp) cout[7 * N + c] = rho * qp;
+}
+
+}  // namespace erfb
+
+namespace erfb {
+
+// ---------------------------------------------------------------------------
+// Scalar transport on x-y tiles marching up in k.  A block owns TXxTY columns
+// and KZ levels; at each level every thread evaluates the advective flux
+// through its cell's low x and y faces into shared memory (the tile's high
+// edge also evaluates the high faces), and carries the flux through its top
+// face to the next level, so each face flux is evaluated once.
+// Divergence as in AdvectionSrcForScalars (ERF_AdvectionSrcForState.cpp:359-370).
+// ---------------------------------------------------------------------------
+constexpr int TTX = 32, TTY = 8, TKZ = 8;
+
+struct FluxTile {
+    double fx[TTY][TTX + 1];
+    double fy[TTY + 1][TTX];
+};
+
+__device__ __forceinline__ double tile_adv_div(const Geo& g, FluxTile& sh, const double* __restrict__ phi,
+                                               const double* __restrict__ ax, const double* __restrict__ ay,
+                                               const double* __restrict__ az, int th, int tv, double fh, double fv,
+                                               int i, int j, int k, bool ok, bool first, double& fz_carry) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    double fzl = 0.0, fzh = 0.0;
+    if (ok) {
+        sh.fx[ty][tx] = adv_flux_x(g, phi, ax, th, fh, i, j, k);
+        if (tx == TTX - 1 || i == g.nx - 1) sh.fx[ty][tx + 1] = adv_flux_x(g, phi, ax, th, fh, wrap(i + 1, g.nx), j, k);
+        sh.fy[ty][tx] = adv_flux_y(g, phi, ay, th, fh, i, j, k);
+        if (ty == TTY - 1 || j == g.ny - 1) sh.fy[ty + 1][tx] = adv_flux_y(g, phi, ay, th, fh, i, wrap(j + 1, g.ny), k);
+        fzl = first ? adv_flux_z(g, phi, az, tv, fv, i, j, k) : fz_carry;
+        fzh = adv_flux_z(g, phi, az, tv, fv, i, j, k + 1);
+    }
+    __syncthreads();
+    double r = 0.0;
+    if (ok)
+        r = -1.0 * 1.0 * ((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi +
+                          (fzh - fzl) * g.dzi);
+    fz_carry = fzh;
+    __syncthreads();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Slow RHS for rho and rho*theta (erf_slow_rhs_pre cell part,
+// ERF_slow_rhs_pre.cpp:462-526): AdvectionSrcForRho (also initialises the
+// average momenta to the stage mass fluxes, ERF_AdvectionSrcForState.cpp:56-71),
+// AdvectionSrcForScalars for theta, DiffusionSrcForState_N for theta.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TTX * TTY) k_slow_cell(Params P, StateBuf S, StageAux A,
+                                                         const double* __restrict__ mut, double* __restrict__ Fcons,
+                                                         double* __restrict__ avx, double* __restrict__ avy,
+                                                         double* __restrict__ avz) {
+    __shared__ FluxTile sh;
+    const Geo& g = P.g;
+    const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
+    const bool ok = i < g.nx && j < g.ny;
+    const int k0 = blockIdx.z * TKZ, k1 = min(k0 + TKZ, g.nz);
+    const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
+    double carry = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        double frt = tile_adv_div(g, sh, A.prim, S.mx, S.my, S.mz, P.dry_h, P.dry_v, P.f_dry_h, P.f_dry_v, i, j, k, ok,
+                                  k == k0, carry);
+        if (!ok) continue;
+        int64_t c = cidx(g, i, j, k);
+        avx[c] = S.mx[c];
+        avy[c] = S.my[c];
+        avz[c] = S.mz[c];
+        if (k == g.nz - 1) avz[c + g.sk] = S.mz[c + g.sk];
+        Fcons[c] = -1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi + (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi +
+                                 (S.mz[c + g.sk] - S.mz[c]) * g.dzi);
+        if (P.use_diff) frt -= scalar_diff(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
+        Fcons[g.ncell + c] = frt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Slow RHS post + stage finalisation (erf_slow_rhs_post,
+// ERF_slow_rhs_post.cpp:228-531, and post_update = apply_bcs(S_new),
+// ERF_TI_slow_rhs_fun.H:284-288):
+//   * advection (average momenta) and diffusion of the slow scalars
+//     (passive scalar; moisture), S_new = S_old + slow_dt * RHS, clipped;
+//   * rho, rho*theta and the momenta copied from the fast solution, with the
+//     momentum/velocity round trips of the two boundary fills;
+//   * the stage velocities, and (unless last) the next stage's primitive
+//     variables, Exner function and p'.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TTX * TTY) k_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst,
+                                                    StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext,
+                                                    int make_next, const double* __restrict__ mut,
+                                                    const double* __restrict__ avx, const double* __restrict__ avy,
+                                                    const double* __restrict__ avz, double* __restrict__ un,
+                                                    double* __restrict__ vn, double* __restrict__ wn) {
+    __shared__ FluxTile sh;
+    const Geo& g = P.g;
+    const int64_t N = g.ncell;
+    const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
+    const bool ok = i < g.nx && j < g.ny;
+    const int k0 = blockIdx.z * TKZ, k1 = min(k0 + TKZ, g.nz);
+    const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
+    const int nslow = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
+    double carry[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = k0; k < k1; ++k) {
+        double tend[4];
+        for (int q = 0; q < nslow; ++q) {
+            int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
+            bool dry = (q == 0);
+            tend[q] = tile_adv_div(g, sh, Acur.prim + (int64_t)(n - 1) * N, avx, avy, avz, dry ? P.dry_h : P.moi_h,
+                                   dry ? P.dry_v : P.moi_v, dry ? P.f_dry_h : P.f_moi_h, dry ? P.f_dry_v : P.f_moi_v,
+                                   i, j, k, ok, k == k0, carry[q]);
+        }
+        if (!ok) continue;
+        int64_t c = cidx(g, i, j, k);
+        for (int q = 0; q < nslow; ++q) {
+            int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
+            double r = tend[q];
+            if (P.use_diff) r -= scalar_diff(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
+            double v_ = Sold.cons[n * N + c] + slow_dt * r;
+            Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 0.0);
+        }
+        Snew.cons[c] = Ssum.cons[c];
+        Snew.cons[N + c] = Ssum.cons[N + c];
+        Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
+        Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
+        double rho = Ssum.cons[c];
+        {
+            double rs = rho + Ssum.cons[cidx(g, im, j, k)];
+            double m = Ssum.mx[c];
+            double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
+            double u2 = (m * 2.0) / rs; m = (u2 * 0.5) * rs;
+            Snew.mx[c] = m; un[c] = u2;
+        }
+        {
+            double rs = rho + Ssum.cons[cidx(g, i, jm, k)];
+            double m = Ssum.my[c];
+            double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
+            double v2 = (m * 2.0) / rs; m = (v2 * 0.5) * rs;
+            Snew.my[c] = m; vn[c] = v2;
+        }
+        if (k == 0) {
+            Snew.mz[c] = 0.0; wn[c] = 0.0;
+        } else {
+            double rs = rho + Ssum.cons[c - g.sk];
+            double m = Ssum.mz[c];
+            double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
+            double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
+            Snew.mz[c] = m; wn[c] = w2;
+        }
+        if (k == g.nz - 1) { Snew.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
+        if (make_next) stage_aux_cell(P, Snew.cons, Anext, c, k);
+    }
+}
+
+}  // namespace erfb
+
+namespace erfb {
+
+// Momentum fluxes of AdvectionSrcFor{X,Y,Z}Mom_N (ERF_AdvectionSrcForMom_N.H:
+// 17-274).  Each is the flux through the low side of the face's control
+// volume in one direction; the high side is the same function one index up.
+__device__ __forceinline__ double xmom_flux_x(const Params& P, const double* ru, const double* u, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (ru[cidx(g, wrap(i - 1, g.nx), j, k)] + ru[cidx(g, i, j, k)]);
+    return a * gatherx_interp(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
+}
+__device__ __forceinline__ double xmom_flux_y(const Params& P, const double* rv, const double* u, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, wrap(i - 1, g.nx), j, k)]);
+    return a * gathery_interp(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
+}
+__device__ __forceinline__ double xmom_flux_z(const Params& P, const double* rw, const double* u, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (rw[cidx(g, i, j, k)] + rw[cidx(g, wrap(i - 1, g.nx), j, k)]);
+    return a * gatherz_tang(g, u, P.dyc_v, a, P.f_dyc_v, i, j, k);
+}
+__device__ __forceinline__ double ymom_flux_x(const Params& P, const double* ru, const double* v, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (ru[cidx(g, i, j, k)] + ru[cidx(g, i, wrap(j - 1, g.ny), k)]);
+    return a * gatherx_interp(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
+}
+__device__ __forceinline__ double ymom_flux_y(const Params& P, const double* rv, const double* v, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, i, wrap(j - 1, g.ny), k)]);
+    return a * gathery_interp(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
+}
+__device__ __forceinline__ double ymom_flux_z(const Params& P, const double* rw, const double* v, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (rw[cidx(g, i, j, k)] + rw[cidx(g, i, wrap(j - 1, g.ny), k)]);
+    return a * gatherz_tang(g, v, P.dyc_v, a, P.f_dyc_v, i, j, k);
+}
+__device__ __forceinline__ double zmom_flux_x(const Params& P, const double* ru, const double* w, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (ru[cidx(g, i, j, k)] + ru[cidx(g, i, j, k - 1)]) * 1.0;
+    return a * gatherx_interp(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
+}
+__device__ __forceinline__ double zmom_flux_y(const Params& P, const double* rv, const double* w, int i, int j, int k) {
+    const Geo& g = P.g;
+    double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, i, j, k - 1)]) * 1.0;
+    return a * gathery_interp(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
+}
+// Vertical flux of w between faces kk-1 and kk (the "lo" flux of face kk),
+// with the order reduction next to the walls (ERF_AdvectionSrcForMom_N.H:
+// 220-265); for kk == nz it is the "hi" flux of the top interior face,
+// which the reference takes centred.
+__device__ __forceinline__ double zmom_flux_z(const Params& P, const double* rw, const double* w, int i, int j, int kk) {
+    const Geo& g = P.g;
+    const int vt = P.dyc_v, lo_z_face = 0, hi_z_face = g.nz;
+    const double vf = P.f_dyc_v;
+    auto wz = [&](int q) { return __ldg(w + cidx(g, i, j, q)); };
+    auto all = [&](int q, double upw, double frac, int type) {
+        double sv[6];
+        bool wide = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH);
+        sv[0] = wide ? wz(q - 3) : 0.0;
+        sv[1] = (type == ERF_ADV_CENTERED_2ND) ? 0.0 : wz(q - 2);
+        sv[2] = wz(q - 1);
+        sv[3] = wz(q);
+        sv[4] = (type == ERF_ADV_CENTERED_2ND) ? 0.0 : wz(q + 1);
+        sv[5] = wide ? wz(q + 2) : 0.0;
+        return interp_all(type, sv, upw, frac);
+    };
+    auto normal = [&](int q, double upw) {
+        double sv[6];
+        int wd = stencil_width(vt);
+        for (int m = 0; m < 6; ++m) {
+            int off = m - 3;
+            sv[m] = (off >= -wd && off <= wd - 1) ? wz(q + off) : 0.0;
+        }
+        return interp_rt(vt, sv, upw, vf);
+    };
+    double a = 0.5 * (rw[cidx(g, i, j, kk)] + rw[cidx(g, i, j, kk - 1)]);
+    double iv;
+    if (kk == hi_z_face || kk == lo_z_face + 1) iv = all(kk, a, 0, ERF_ADV_CENTERED_2ND);
+    else if (kk == lo_z_face + 2 || kk == hi_z_face - 1) {
+        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) iv = all(kk, a, 0, ERF_ADV_CENTERED_4TH);
+        else iv = all(kk, a, vf, vt);
+    } else iv = normal(kk, a);
+    return a * iv;
+}
+
+// ---------------------------------------------------------------------------
+// Slow RHS for the three momenta (erf_slow_rhs_pre face part,
+// ERF_slow_rhs_pre.cpp:556-744): AdvectionSrcForMom (N), DiffusionSrcForMom_N,
+// pressure gradient of p', buoyancy / Coriolis / geostrophic sources
+// (make_mom_sources, make_buoyancy).  Same x-y tiles marching in k as the
+// scalar transport: every momentum flux is evaluated once.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TTX * TTY) k_slow_mom(Params P, StateBuf S, StageAux A, const double* __restrict__ u,
+                                                        const double* __restrict__ v, const double* __restrict__ w,
+                                                        const double* __restrict__ t11, const double* __restrict__ t22,
+                                                        const double* __restrict__ t33, const double* __restrict__ t12,
+                                                        const double* __restrict__ t13, const double* __restrict__ t23,
+                                                        const double* __restrict__ pavg, double* __restrict__ Fmx,
+                                                        double* __restrict__ Fmy, double* __restrict__ Fmz) {
+    __shared__ FluxTile sh;
+    const Geo& g = P.g;
+    const int64_t N = g.ncell;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * TTX + tx, j = blockIdx.y * TTY + ty;
+    const bool ok = i < g.nx && j < g.ny;
+    const int k0 = blockIdx.z * TKZ, k1 = min(k0 + TKZ, g.nz);
+    const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
+    const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
+    const bool xedge = ok && (tx == TTX - 1 || i == g.nx - 1);
+    const bool yedge = ok && (ty == TTY - 1 || j == g.ny - 1);
+    const double* ru = S.mx;
+    const double* rv = S.my;
+    const double* rw = S.mz;
+    const double* cd = S.cons;
+    const double* prim = A.prim;
+    const double* pp = A.pp;
+    double czu = 0.0, czv = 0.0, czw = 0.0;   // carried vertical fluxes
+    for (int k = k0; k < k1; ++k) {
+        const int64_t c = ok ? cidx(g, i, j, k) : 0;
+        // ---------------- x-momentum on face i
+        double zl = 0.0, zh = 0.0;
+        if (ok) {
+            sh.fx[ty][tx] = xmom_flux_x(P, ru, u, i, j, k);
+            if (xedge) sh.fx[ty][tx + 1] = xmom_flux_x(P, ru, u, ip, j, k);
+            sh.fy[ty][tx] = xmom_flux_y(P, rv, u, i, j, k);
+            if (yedge) sh.fy[ty + 1][tx] = xmom_flux_y(P, rv, u, i, jp, k);
+            zl = (k == k0) ? xmom_flux_z(P, rw, u, i, j, k) : czu;
+            zh = xmom_flux_z(P, rw, u, i, j, k + 1);
+            czu = zh;
+        }
+        __syncthreads();
+        if (ok) {
+            double rhs = -((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi * 1.0 + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi * 1.0 +
+                           (zh - zl) * g.dzi);
+            if (P.use_diff)
+                rhs -= ((t11[c] - t11[cidx(g, im, j, k)]) * g.dxi * 1.0 + (t12[cidx(g, i, jp, k)] - t12[c]) * g.dyi * 1.0 +
+                        (t13[c + g.sk] - t13[c]) * g.dzi);
+            double gpx = g.dxi * (pp[c] - pp[cidx(g, im, j, k)]);
+            gpx *= 1.0;
+            double q = 0.0;
+            if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + cidx(g, im, j, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, im, j, k)]);
+            double src = 0.0;
+            if (P.coriolis) {
+                double rvl = 0.25 * (rv[cidx(g, i, jp, k)] + rv[c] + rv[cidx(g, im, jp, k)] + rv[cidx(g, im, j, k)]);
+                double rwl = 0.25 * (rw[c + g.sk] + rw[c] + rw[cidx(g, i, jm, k + 1)] + rw[cidx(g, i, jm, k)]);
+                src += P.cf * (rvl * P.sinphi - rwl * P.cosphi);
+            }
+            src += 0.5 * (cd[c] + cd[cidx(g, im, j, k)]) * P.geo0;
+            rhs += (-gpx - 0.0) / (1.0 + q) + src;
+            Fmx[c] = rhs;
+        }
+        __syncthreads();
+        // ---------------- y-momentum on face j
+        if (ok) {
+            sh.fx[ty][tx] = ymom_flux_x(P, ru, v, i, j, k);
+            if (xedge) sh.fx[ty][tx + 1] = ymom_flux_x(P, ru, v, ip, j, k);
+            sh.fy[ty][tx] = ymom_flux_y(P, rv, v, i, j, k);
+            if (yedge) sh.fy[ty + 1][tx] = ymom_flux_y(P, rv, v, i, jp, k);
+            zl = (k == k0) ? ymom_flux_z(P, rw, v, i, j, k) : czv;
+            zh = ymom_flux_z(P, rw, v, i, j, k + 1);
+            czv = zh;
+        }
+        __syncthreads();
+        if (ok) {
+            double rhs = -((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi * 1.0 + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi * 1.0 +
+                           (zh - zl) * g.dzi);
+            if (P.use_diff)
+                rhs -= ((t12[cidx(g, ip, j, k)] - t12[c]) * g.dxi * 1.0 + (t22[c] - t22[cidx(g, i, jm, k)]) * g.dyi * 1.0 +
+                        (t23[c + g.sk] - t23[c]) * g.dzi);
+            double gpy = g.dyi * (pp[c] - pp[cidx(g, i, jm, k)]);
+            gpy *= 1.0;
+            double q = 0.0;
+            if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + cidx(g, i, jm, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, i, jm, k)]);
+            double src = 0.0;
+            if (P.coriolis) {
+                double rul = 0.25 * (ru[cidx(g, ip, j, k)] + ru[c] + ru[cidx(g, ip, jm, k)] + ru[cidx(g, i, jm, k)]);
+                src += -P.cf * rul * P.sinphi;
+            }
+            src += 0.5 * (cd[c] + cd[cidx(g, i, jm, k)]) * P.geo1;
+            rhs += (-gpy - 0.0) / (1.0 + q) + src;
+            Fmy[c] = rhs;
+        }
+        __syncthreads();
+        // ---------------- z-momentum on face k (interior faces only)
+        const bool zk = ok && k >= 1;
+        if (zk) {
+            sh.fx[ty][tx] = zmom_flux_x(P, ru, w, i, j, k);
+            if (xedge) sh.fx[ty][tx + 1] = zmom_flux_x(P, ru, w, ip, j, k);
+            sh.fy[ty][tx] = zmom_flux_y(P, rv, w, i, j, k);
+            if (yedge) sh.fy[ty + 1][tx] = zmom_flux_y(P, rv, w, i, jp, k);
+            zl = (k == k0 || k == 1) ? zmom_flux_z(P, rw, w, i, j, k) : czw;
+            zh = zmom_flux_z(P, rw, w, i, j, k + 1);
+            czw = zh;
+        }
+        __syncthreads();
+        if (ok && k == 0) Fmz[c] = 0.0;
+        if (zk) {
+            double rhs = -((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi * 1.0 + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi * 1.0 +
+                           (zh - zl) * g.dzi);
+            if (P.use_diff)
+                rhs -= ((t13[cidx(g, ip, j, k)] - t13[c]) * g.dxi * 1.0 + (t23[cidx(g, i, jp, k)] - t23[c]) * g.dyi * 1.0 +
+                        (t33[c] - t33[c - g.sk]) * g.dzi);
+            double b;
+            double g2 = -P.gravity;
+            if (!P.moist) {
+                if (P.buoy_type == 1) {
+                    b = g2 * 0.5 * ((cd[c] - P.r0[k + 1]) + (cd[c - g.sk] - P.r0[k]));
+                } else {
+                    auto T0 = [&](int kk) {
+                        double rt0 = eos_rt_given_p(P.p0[kk + 1]);
+                        return (rt0 / P.r0[kk + 1]) / pow(p_0 / P.p0[kk + 1], P.rdOcp);
+                    };
+                    double t0h = T0(k), th_ = eos_T(cd[c], cd[N + c], 0.0);
+                    double t0l = T0(k - 1), tl_ = eos_T(cd[c - g.sk], cd[N + c - g.sk], 0.0);
+                    double qp_ = (th_ - t0h) / t0h, qm_ = (tl_ - t0l) / t0l;
+                    double r0q = 0.5 * (P.r0[k + 1] * qp_ + P.r0[k] * qm_);
+                    b = -r0q * g2;
+                }
+            } else if (P.buoy_type == 1) {
+                int nq = P.ncomp - ERF_RHOQ1_COMP;
+                double hi = cd[c] + cd[5 * N + c] + cd[6 * N + c] - P.r0[k + 1];
+                double lo = cd[c - g.sk] + cd[5 * N + c - g.sk] + cd[6 * N + c - g.sk] - P.r0[k];
+                for (int qo = 2; qo < nq; ++qo) { hi += cd[(5 + qo) * N + c]; lo += cd[(5 + qo) * N + c - g.sk]; }
+                b = g2 * 0.5 * (hi + lo);
+            } else {
+                int nq = P.ncomp - ERF_RHOQ1_COMP;
+                const double* rd = pavg;
+                const double* thd = pavg + g.nz;
+                const double* qvd = pavg + 2 * g.nz;
+                const double* qcd = pavg + 3 * g.nz;
+                const double* qpd = pavg + 4 * g.nz;
+                double tp1 = eos_T(rd[k], rd[k] * thd[k], qvd[k]);
+                double tm1 = eos_T(rd[k - 1], rd[k - 1] * thd[k - 1], qvd[k - 1]);
+                double tp3 = eos_T(cd[c], cd[N + c], cd[5 * N + c] / cd[c]);
+                double tm3 = eos_T(cd[c - g.sk], cd[N + c - g.sk], cd[5 * N + c - g.sk] / cd[c - g.sk]);
+                double qvp = nq >= 1 ? prim[4 * N + c] : 0.0, qvm = nq >= 1 ? prim[4 * N + c - g.sk] : 0.0;
+                double qcp = nq >= 2 ? prim[5 * N + c] : 0.0, qcm = nq >= 2 ? prim[5 * N + c - g.sk] : 0.0;
+                double qpp = nq >= 3 ? prim[6 * N + c] : 0.0, qpm = nq >= 3 ? prim[6 * N + c - g.sk] : 0.0;
+                double qplus = 0.61 * (qvp - qvd[k]) - (qcp - qcd[k] + qpp - qpd[k]) + (tp3 - tp1) / tp1 * (1.0 + 0.61 * qvd[k] - qcd[k] - qpd[k]);
+                double qminus = 0.61 * (qvm - qvd[k - 1]) - (qcm - qcd[k - 1] + qpm - qpd[k - 1]) + (tm3 - tm1) / tm1 * (1.0 + 0.61 * qvd[k - 1] - qcd[k - 1] - qpd[k - 1]);
+                double qavg = 0.5 * (qplus + qminus);
+                double r0avg = 0.5 * (rd[k] + rd[k - 1]);
+                b = -qavg * r0avg * g2;
+            }
+            double zsrc = b;
+            if (P.coriolis) {
+                double rul = 0.25 * (ru[cidx(g, ip, j, k)] + ru[c] + ru[cidx(g, ip, j, k - 1)] + ru[c - g.sk]);
+                zsrc += P.cf * rul * P.cosphi;
+            }
+            zsrc += 0.5 * (cd[c] + cd[c - g.sk]) * P.geo2;
+            double gpz = g.dzi * (pp[c] - pp[c - g.sk]) / 1.0;
+            double q = 0.0;
+            if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + c - g.sk] + prim[5 * N + c] + prim[5 * N + c - g.sk]);
+            rhs += (zsrc - gpz - 0.0) / (1.0 + q);
+            Fmz[c] = rhs;
+        }
+        if (ok && k == g.nz - 1) Fmz[c + g.sk] = 0.0;
+        __syncthreads();
+    }
 }
 
 }  // namespace erfb
