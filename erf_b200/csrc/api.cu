@@ -14,13 +14,7 @@ __global__ void k_step_begin(Params P, const double* cons, const double* uo, con
                              StateBuf S, double* un, double* vn, double* wn, StageAux A, double* mut);
 __global__ void k_tau(Params P, const double* cons, const double* u, const double* v, const double* w,
                       const double* mut, double* t11, double* t22, double* t33, double* t12, double* t13, double* t23);
-__global__ void k_slow_cell(Params P, StateBuf S, StageAux A, const double* mut, double* Fcons, double* avx,
-                            double* avy, double* avz);
 __global__ void k_plane_avg(Params P, const double* cons, const double* prim, double* avg);
-__global__ void k_slow_mom(Params P, StateBuf S, StageAux A, const double* u, const double* v, const double* w,
-                           const double* t11, const double* t22, const double* t33, const double* t12,
-                           const double* t13, const double* t23, const double* pavg, double* Fmx, double* Fmy,
-                           double* Fmz);
 __global__ void k_fast_h(Params P, int step, int nrk, double dtau, double facinv, StateBuf Sprev, int prev_rt,
                          StateBuf Sst, StageAux A, const double* Fmx, const double* Fmy, const double* lag_in,
                          double* lag_out, double* avx, double* avy, double* outx, double* outy);
@@ -28,9 +22,6 @@ __global__ void k_fast_col(Params P, int step, double dtau, double facinv, doubl
                            StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux A, const double* Fcons,
                            const double* Fmz, const double* newx, const double* newy, double* avz, double* out_cons,
                            double* out_mz, double* sc_soln, double* sc_cb, double* sc_tr0, double* sc_tr1);
-__global__ void k_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
-                       StageAux Acur, StageAux Anext, int make_next, const double* mut, const double* avx,
-                       const double* avy, const double* avz, double* un, double* vn, double* wn);
 __global__ void k_kessler(Params P, double* cons, double dtn, double dz);
 __global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double* cA, double* cInvB, double* cCB,
                             double* cP, double* cQ);
@@ -49,6 +40,11 @@ __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const doubl
 }  // namespace erfb
 
 using namespace erfb;
+
+// Threads per block of the vertical acoustic kernel (columns x level groups).
+#ifndef ERFB_VERT_THREADS
+#define ERFB_VERT_THREADS 1024
+#endif
 
 struct erf_b200_ctx {
     erf_b200_config cfg;
@@ -70,7 +66,8 @@ struct erf_b200_ctx {
     double *t11, *t22, *t33, *t12, *t13, *t23;
     double* pavg;
     double *cA, *cInvB, *cCB, *cP, *cQ;  // fast coefficients of the current stage
-    int tile_tx = 32, vert_warps = 16, coef_warps = 8;
+    int tile_tx = 32, vert_warps = 32, coef_warps = 8;
+    TiledKz tkz{1, 1, 1};
     size_t vert_smem = 0, coef_smem = 0;
     double *r0, *p0, *pi0, *th0;
     double *h_stage;          // device staging buffers for the host-array entry point
@@ -256,8 +253,6 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
     StateBuf stage[3] = {OLD, outs[0], outs[1]};
     dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
     dim3 tcb(c->tile_tx, c->coef_warps, 1);
-    // scalar-transport tiles: 32 x 8 columns, 8 levels per block
-    dim3 ttb(32, 8, 1), ttg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + 7) / 8);
     int a = 0;
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
@@ -270,11 +265,11 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
         if (P.use_diff)
             TIMED(1, (k_tau<<<cg, cb, 0, st>>>(P, Sst.cons, Vnew[0], Vnew[1], Vnew[2], c->mut, c->t11, c->t22,
                                                c->t33, c->t12, c->t13, c->t23)));
-        TIMED(2, (k_slow_cell<<<ttg, ttb, 0, st>>>(P, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz)));
+        TIMED(2, launch_slow_cell(P, c->tkz, st, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz));
         if (P.moist && P.buoy_type == 2)
             TIMED(3, (k_plane_avg<<<g.nz, 256, 0, st>>>(P, Sst.cons, Acur.prim, c->pavg)));
-        TIMED(4, (k_slow_mom<<<ttg, ttb, 0, st>>>(P, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33,
-                                                  c->t12, c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz)));
+        TIMED(4, launch_slow_mom(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33, c->t12,
+                                 c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz));
         double facinv = 1.0 / (double)nsub;
         double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
         TIMED(9, (k_fast_coef<<<tg, tcb, c->coef_smem, st>>>(P, D, Sst, Acur, c->cA, c->cInvB, c->cCB, c->cP,
@@ -290,8 +285,8 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
                                                                 c->cInvB, c->cCB, c->cP, c->cQ, c->avz, SUM.cons,
                                                                 SUM.mz)));
         }
-        TIMED(7, (k_post<<<ttg, ttb, 0, st>>>(P, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut,
-                                              c->avx, c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2])));
+        TIMED(7, launch_post(P, c->tkz, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut, c->avx,
+                             c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
     }
     if (P.moist) TIMED(8, (k_kessler_cells<<<cg, cb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
@@ -407,6 +402,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     }
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     make_params(c);
+    tiled_setup(c->P, &c->tkz);
     c->lag_parity_per_step = substeps_per_step(c->cfg) & 1;
     // shared-memory tiles of the vertical kernels: TX columns x all levels
     {
@@ -417,7 +413,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         c->vert_smem = (size_t)(7 * nz + 5) * c->tile_tx * sizeof(double);
         c->coef_smem = (size_t)3 * (nz + 1) * c->tile_tx * sizeof(double);
         if (c->vert_smem > max_smem) rc = ERF_B200_ECONFIG;
-        c->vert_warps = c->tile_tx == 32 ? 16 : 32;
+        c->vert_warps = ERFB_VERT_THREADS / c->tile_tx;
         c->coef_warps = c->tile_tx == 32 ? 8 : 16;
         if (rc == ERF_B200_OK) {
             if (cudaFuncSetAttribute(k_fast_vert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->vert_smem) != cudaSuccess ||

@@ -111,11 +111,13 @@ struct Interp<ERF_ADV_WENO_3> {
         double v1 = -a + 3.0 * b, v2 = b + c;
         return (w1 * v1 + w2 * v2) / (2.0 * ws);
     }
+    // The upwind side is selected by operand choice rather than a branch, so
+    // a warp whose faces have mixed signs evaluates the scheme once.
     __device__ static __forceinline__ double eval(const double* s, double upw, double) {
         const double tol = 1.0e-12;
-        if (upw > tol) return ev(s[1], s[2], s[3]);
-        if (upw < -tol) return ev(s[4], s[3], s[2]);
-        return 0.5 * (s[3] + s[2]);
+        const bool pos = upw > tol;
+        double r = ev(pos ? s[1] : s[4], pos ? s[2] : s[3], pos ? s[3] : s[2]);
+        return (upw > tol || upw < -tol) ? r : 0.5 * (s[3] + s[2]);
     }
 };
 template <>
@@ -143,9 +145,9 @@ struct Interp<ERF_ADV_WENO_5> {
     }
     __device__ static __forceinline__ double eval(const double* s, double upw, double) {
         const double tol = 1.0e-12;
-        if (upw > tol) return ev(s[0], s[1], s[2], s[3], s[4]);
-        if (upw < -tol) return ev(s[5], s[4], s[3], s[2], s[1]);
-        return 0.5 * (s[3] + s[2]);
+        const bool pos = upw > tol;
+        double r = ev(pos ? s[0] : s[5], pos ? s[1] : s[4], pos ? s[2] : s[3], pos ? s[3] : s[2], pos ? s[4] : s[1]);
+        return (upw > tol || upw < -tol) ? r : 0.5 * (s[3] + s[2]);
     }
 };
 
@@ -168,6 +170,19 @@ __host__ __device__ __forceinline__ int stencil_width(int type) {
     case ERF_ADV_UPWIND_3RD: case ERF_ADV_CENTERED_4TH: case ERF_ADV_WENO_3: return 2;
     default: return 3;
     }
+}
+
+// Compile-time selection of the interpolant: T >= 0 is a fixed scheme code,
+// T < 0 selects the scheme at run time from `rt`.
+template <int T>
+__device__ __forceinline__ int width_of(int rt) {
+    if constexpr (T < 0) return stencil_width(rt);
+    else return Interp<T>::W;
+}
+template <int T>
+__device__ __forceinline__ double interp_of(int rt, const double* s, double upw, double frac) {
+    if constexpr (T < 0) return interp_rt(rt, s, upw, frac);
+    else return Interp<T>::eval(s, upw, frac);
 }
 
 // Wall-reduced vertical interpolant for w (UPWINDALL, reference

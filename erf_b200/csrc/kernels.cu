@@ -181,38 +181,41 @@ __global__ void k_tau(Params P, const double* __restrict__ cons, const double* _
 // ---------------------------------------------------------------------------
 // Advective flux of primitive component `pc` through the low x/y/z face of
 // cell (i,j,k): mom * interp(phi) (Advection/ERF_AdvectionSrcForScalars.H:7-58).
+template <int T = -1>
 __device__ __forceinline__ double adv_flux_x(const Geo& g, const double* __restrict__ phi, const double* __restrict__ mom,
                                              int type, double frac, int i, int j, int k) {
     double s[6];
-    int w = stencil_width(type);
+    const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, wrap(i + off, g.nx), j, k)) : 0.0;
     }
     double a = __ldg(mom + cidx(g, i, j, k));
-    return a * interp_rt(type, s, a, frac);
+    return a * interp_of<T>(type, s, a, frac);
 }
+template <int T = -1>
 __device__ __forceinline__ double adv_flux_y(const Geo& g, const double* __restrict__ phi, const double* __restrict__ mom,
                                              int type, double frac, int i, int j, int k) {
     double s[6];
-    int w = stencil_width(type);
+    const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, i, wrap(j + off, g.ny), k)) : 0.0;
     }
     double a = __ldg(mom + cidx(g, i, j, k));
-    return a * interp_rt(type, s, a, frac);
+    return a * interp_of<T>(type, s, a, frac);
 }
+template <int T = -1>
 __device__ __forceinline__ double adv_flux_z(const Geo& g, const double* __restrict__ phi, const double* __restrict__ mom,
                                              int type, double frac, int i, int j, int k) {
     double s[6];
-    int w = stencil_width(type);
+    const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? ccz(phi, g, i, j, k + off) : 0.0;
     }
     double a = __ldg(mom + cidx(g, i, j, k));
-    return a * interp_rt(type, s, a, frac);
+    return a * interp_of<T>(type, s, a, frac);
 }
 
 // Advective tendency of one scalar (assigns, like AdvectionSrcForScalars,
@@ -282,35 +285,38 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const dou
 
 // Momentum flux of component `phi` (a face velocity) through a face, with the
 // interpolant selected at run time (ERF_AdvectionSrcForMom_N.H:17-274).
+template <int T = -1>
 __device__ __forceinline__ double gatherx_interp(const Geo& g, const double* f, int type, double upw, double frac,
                                                  int i, int j, int k) {
     double s[6];
-    int w = stencil_width(type);
+    const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? __ldg(f + cidx(g, wrap(i + off, g.nx), j, k)) : 0.0;
     }
-    return interp_rt(type, s, upw, frac);
+    return interp_of<T>(type, s, upw, frac);
 }
+template <int T = -1>
 __device__ __forceinline__ double gathery_interp(const Geo& g, const double* f, int type, double upw, double frac,
                                                  int i, int j, int k) {
     double s[6];
-    int w = stencil_width(type);
+    const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? __ldg(f + cidx(g, i, wrap(j + off, g.ny), k)) : 0.0;
     }
-    return interp_rt(type, s, upw, frac);
+    return interp_of<T>(type, s, upw, frac);
 }
+template <int T = -1>
 __device__ __forceinline__ double gatherz_tang(const Geo& g, const double* f, int type, double upw, double frac,
                                                int i, int j, int k) {
     double s[6];
-    int w = stencil_width(type);
+    const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? tang(f, g, i, j, k + off) : 0.0;
     }
-    return interp_rt(type, s, upw, frac);
+    return interp_of<T>(type, s, upw, frac);
 }
 
 // ---------------------------------------------------------------------------
@@ -842,7 +848,7 @@ __global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double
 // All reads of the previous state happen in phases 1-2, before any write,
 // because the previous and new states may be the same buffers.
 // ---------------------------------------------------------------------------
-__global__ void k_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
+__global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
                             int prev_rt, StateBuf Sst, StageAux A, const double* __restrict__ Fcons,
                             const double* __restrict__ Fmz, const double* __restrict__ newx,
                             const double* __restrict__ newy, const double* __restrict__ cA,
@@ -1054,51 +1060,64 @@ __global__ void k_kessler_cells(Params P, const double* __restrict__ cin, double
 namespace erfb {
 
 // ---------------------------------------------------------------------------
-// Scalar transport on x-y tiles marching up in k.  A block owns TXxTY columns
-// and KZ levels; at each level every thread evaluates the advective flux
-// through its cell's low x and y faces into shared memory (the tile's high
-// edge also evaluates the high faces), and carries the flux through its top
-// face to the next level, so each face flux is evaluated once.
+// Scalar and momentum transport on x-y tiles marching up in k.  A block owns
+// TTX x TTY columns and `kz` consecutive levels.  At each level every thread
+// evaluates the advective flux through its cell's low x and y faces into
+// shared memory (the tile's high edge also evaluates the high faces) and
+// carries the flux through its top face to the next level, so each face flux
+// is evaluated once per block.  All fluxes of one level are staged before a
+// single barrier.  `kz` is chosen on the host so that the whole grid is one
+// wave of resident blocks.
 // Divergence as in AdvectionSrcForScalars (ERF_AdvectionSrcForState.cpp:359-370).
 // ---------------------------------------------------------------------------
-constexpr int TTX = 32, TTY = 8, TKZ = 8;
+// Minimum resident blocks per SM requested from the register allocator for
+// each tiled kernel (trades instruction-level for warp-level parallelism).
+#ifndef ERFB_MINB_CELL
+#define ERFB_MINB_CELL 4
+#endif
+#ifndef ERFB_MINB_MOM
+#define ERFB_MINB_MOM 4
+#endif
+#ifndef ERFB_MINB_POST
+#define ERFB_MINB_POST 4
+#endif
 
 struct FluxTile {
     double fx[TTY][TTX + 1];
     double fy[TTY + 1][TTX];
 };
 
-__device__ __forceinline__ double tile_adv_div(const Geo& g, FluxTile& sh, const double* __restrict__ phi,
-                                               const double* __restrict__ ax, const double* __restrict__ ay,
-                                               const double* __restrict__ az, int th, int tv, double fh, double fv,
-                                               int i, int j, int k, bool ok, bool first, double& fz_carry) {
+// Fluxes of one scalar for cell (i,j,k): x/y into the tile, z through zl/zh
+// (zl is computed only on the block's first level; otherwise it is the
+// carried top flux of the level below).
+template <int TH, int TV>
+__device__ __forceinline__ void tile_put(const Geo& g, FluxTile& t, const double* __restrict__ phi,
+                                         const double* __restrict__ ax, const double* __restrict__ ay,
+                                         const double* __restrict__ az, int th, int tv, double fh, double fv, int i,
+                                         int j, int k, bool first, double& zl, double& zh) {
     const int tx = threadIdx.x, ty = threadIdx.y;
-    double fzl = 0.0, fzh = 0.0;
-    if (ok) {
-        sh.fx[ty][tx] = adv_flux_x(g, phi, ax, th, fh, i, j, k);
-        if (tx == TTX - 1 || i == g.nx - 1) sh.fx[ty][tx + 1] = adv_flux_x(g, phi, ax, th, fh, wrap(i + 1, g.nx), j, k);
-        sh.fy[ty][tx] = adv_flux_y(g, phi, ay, th, fh, i, j, k);
-        if (ty == TTY - 1 || j == g.ny - 1) sh.fy[ty + 1][tx] = adv_flux_y(g, phi, ay, th, fh, i, wrap(j + 1, g.ny), k);
-        fzl = first ? adv_flux_z(g, phi, az, tv, fv, i, j, k) : fz_carry;
-        fzh = adv_flux_z(g, phi, az, tv, fv, i, j, k + 1);
-    }
-    __syncthreads();
-    double r = 0.0;
-    if (ok)
-        r = -1.0 * 1.0 * ((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi +
-                          (fzh - fzl) * g.dzi);
-    fz_carry = fzh;
-    __syncthreads();
-    return r;
+    t.fx[ty][tx] = adv_flux_x<TH>(g, phi, ax, th, fh, i, j, k);
+    if (tx == TTX - 1 || i == g.nx - 1) t.fx[ty][tx + 1] = adv_flux_x<TH>(g, phi, ax, th, fh, wrap(i + 1, g.nx), j, k);
+    t.fy[ty][tx] = adv_flux_y<TH>(g, phi, ay, th, fh, i, j, k);
+    if (ty == TTY - 1 || j == g.ny - 1) t.fy[ty + 1][tx] = adv_flux_y<TH>(g, phi, ay, th, fh, i, wrap(j + 1, g.ny), k);
+    if (first) zl = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k);
+    zh = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k + 1);
+}
+__device__ __forceinline__ double tile_div(const Geo& g, const FluxTile& t, double zl, double zh) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    return -1.0 * 1.0 * ((t.fx[ty][tx + 1] - t.fx[ty][tx]) * g.dxi + (t.fy[ty + 1][tx] - t.fy[ty][tx]) * g.dyi +
+                         (zh - zl) * g.dzi);
 }
 
 // ---------------------------------------------------------------------------
 // Slow RHS for rho and rho*theta (erf_slow_rhs_pre cell part,
 // ERF_slow_rhs_pre.cpp:462-526): AdvectionSrcForRho (also initialises the
 // average momenta to the stage mass fluxes, ERF_AdvectionSrcForState.cpp:56-71),
-// AdvectionSrcForScalars for theta, DiffusionSrcForState_N for theta.
+// AdvectionSrcForScalars for theta with the dycore scheme
+// (ERF_slow_rhs_pre.cpp:139-142, 469-477), DiffusionSrcForState_N for theta.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TTX * TTY) k_slow_cell(Params P, StateBuf S, StageAux A,
+template <int TH, int TV>
+__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params P, int kz, StateBuf S, StageAux A,
                                                          const double* __restrict__ mut, double* __restrict__ Fcons,
                                                          double* __restrict__ avx, double* __restrict__ avy,
                                                          double* __restrict__ avz) {
@@ -1106,22 +1125,28 @@ __global__ void __launch_bounds__(TTX * TTY) k_slow_cell(Params P, StateBuf S, S
     const Geo& g = P.g;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
     const bool ok = i < g.nx && j < g.ny;
-    const int k0 = blockIdx.z * TKZ, k1 = min(k0 + TKZ, g.nz);
+    const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
-    double carry = 0.0;
+    double zl = 0.0, zh = 0.0;
     for (int k = k0; k < k1; ++k) {
-        double frt = tile_adv_div(g, sh, A.prim, S.mx, S.my, S.mz, P.dry_h, P.dry_v, P.f_dry_h, P.f_dry_v, i, j, k, ok,
-                                  k == k0, carry);
-        if (!ok) continue;
-        int64_t c = cidx(g, i, j, k);
-        avx[c] = S.mx[c];
-        avy[c] = S.my[c];
-        avz[c] = S.mz[c];
-        if (k == g.nz - 1) avz[c + g.sk] = S.mz[c + g.sk];
-        Fcons[c] = -1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi + (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi +
-                                 (S.mz[c + g.sk] - S.mz[c]) * g.dzi);
-        if (P.use_diff) frt -= scalar_diff(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
-        Fcons[g.ncell + c] = frt;
+        if (ok)
+            tile_put<TH, TV>(g, sh, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, P.f_dyc_h, P.f_dyc_v, i, j, k,
+                             k == k0, zl, zh);
+        __syncthreads();
+        if (ok) {
+            double frt = tile_div(g, sh, zl, zh);
+            zl = zh;
+            int64_t c = cidx(g, i, j, k);
+            avx[c] = S.mx[c];
+            avy[c] = S.my[c];
+            avz[c] = S.mz[c];
+            if (k == g.nz - 1) avz[c + g.sk] = S.mz[c + g.sk];
+            Fcons[c] = -1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi +
+                                     (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi + (S.mz[c + g.sk] - S.mz[c]) * g.dzi);
+            if (P.use_diff) frt -= scalar_diff(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
+            Fcons[g.ncell + c] = frt;
+        }
+        __syncthreads();
     }
 }
 
@@ -1130,129 +1155,150 @@ __global__ void __launch_bounds__(TTX * TTY) k_slow_cell(Params P, StateBuf S, S
 // ERF_slow_rhs_post.cpp:228-531, and post_update = apply_bcs(S_new),
 // ERF_TI_slow_rhs_fun.H:284-288):
 //   * advection (average momenta) and diffusion of the slow scalars
-//     (passive scalar; moisture), S_new = S_old + slow_dt * RHS, clipped;
+//     (passive scalar with the dry-scalar scheme; moisture with the moist
+//     scheme), S_new = S_old + slow_dt * RHS, moisture clipped at 0;
 //   * rho, rho*theta and the momenta copied from the fast solution, with the
 //     momentum/velocity round trips of the two boundary fills;
 //   * the stage velocities, and (unless last) the next stage's primitive
 //     variables, Exner function and p'.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TTX * TTY) k_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst,
+constexpr int MAX_SLOW = 4;  // passive scalar + up to three moisture species
+template <int DH, int DV, int MH, int MV>
+__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, int kz, double slow_dt, StateBuf Sold, StateBuf Sst,
                                                     StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext,
                                                     int make_next, const double* __restrict__ mut,
                                                     const double* __restrict__ avx, const double* __restrict__ avy,
                                                     const double* __restrict__ avz, double* __restrict__ un,
                                                     double* __restrict__ vn, double* __restrict__ wn) {
-    __shared__ FluxTile sh;
+    __shared__ FluxTile sh[MAX_SLOW];
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
     const bool ok = i < g.nx && j < g.ny;
-    const int k0 = blockIdx.z * TKZ, k1 = min(k0 + TKZ, g.nz);
+    const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
     const int nslow = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
-    double carry[4] = {0.0, 0.0, 0.0, 0.0};
+    double zl[MAX_SLOW], zh[MAX_SLOW];
+#pragma unroll
+    for (int q = 0; q < MAX_SLOW; ++q) zl[q] = zh[q] = 0.0;
     for (int k = k0; k < k1; ++k) {
-        double tend[4];
-        for (int q = 0; q < nslow; ++q) {
-            int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
-            bool dry = (q == 0);
-            tend[q] = tile_adv_div(g, sh, Acur.prim + (int64_t)(n - 1) * N, avx, avy, avz, dry ? P.dry_h : P.moi_h,
-                                   dry ? P.dry_v : P.moi_v, dry ? P.f_dry_h : P.f_moi_h, dry ? P.f_dry_v : P.f_moi_v,
-                                   i, j, k, ok, k == k0, carry[q]);
+        if (ok) {
+#pragma unroll
+            for (int q = 0; q < MAX_SLOW; ++q) {
+                if (q >= nslow) break;
+                if (q == 0)
+                    tile_put<DH, DV>(g, sh[0], Acur.prim + (int64_t)(ERF_RHOSCALAR_COMP - 1) * N, avx, avy, avz,
+                                     P.dry_h, P.dry_v, P.f_dry_h, P.f_dry_v, i, j, k, k == k0, zl[0], zh[0]);
+                else
+                    tile_put<MH, MV>(g, sh[q], Acur.prim + (int64_t)(ERF_RHOQ1_COMP + q - 2) * N, avx, avy, avz,
+                                     P.moi_h, P.moi_v, P.f_moi_h, P.f_moi_v, i, j, k, k == k0, zl[q], zh[q]);
+            }
         }
-        if (!ok) continue;
-        int64_t c = cidx(g, i, j, k);
-        for (int q = 0; q < nslow; ++q) {
-            int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
-            double r = tend[q];
-            if (P.use_diff) r -= scalar_diff(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
-            double v_ = Sold.cons[n * N + c] + slow_dt * r;
-            Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 0.0);
+        __syncthreads();
+        if (ok) {
+            int64_t c = cidx(g, i, j, k);
+#pragma unroll
+            for (int q = 0; q < MAX_SLOW; ++q) {
+                if (q >= nslow) break;
+                int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
+                double r = tile_div(g, sh[q], zl[q], zh[q]);
+                zl[q] = zh[q];
+                if (P.use_diff)
+                    r -= scalar_diff(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
+                double v_ = Sold.cons[n * N + c] + slow_dt * r;
+                Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 0.0);
+            }
+            Snew.cons[c] = Ssum.cons[c];
+            Snew.cons[N + c] = Ssum.cons[N + c];
+            Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
+            Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
+            double rho = Ssum.cons[c];
+            {
+                double rs = rho + Ssum.cons[cidx(g, im, j, k)];
+                double m = Ssum.mx[c];
+                double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
+                double u2 = (m * 2.0) / rs; m = (u2 * 0.5) * rs;
+                Snew.mx[c] = m; un[c] = u2;
+            }
+            {
+                double rs = rho + Ssum.cons[cidx(g, i, jm, k)];
+                double m = Ssum.my[c];
+                double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
+                double v2 = (m * 2.0) / rs; m = (v2 * 0.5) * rs;
+                Snew.my[c] = m; vn[c] = v2;
+            }
+            if (k == 0) {
+                Snew.mz[c] = 0.0; wn[c] = 0.0;
+            } else {
+                double rs = rho + Ssum.cons[c - g.sk];
+                double m = Ssum.mz[c];
+                double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
+                double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
+                Snew.mz[c] = m; wn[c] = w2;
+            }
+            if (k == g.nz - 1) { Snew.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
+            if (make_next) stage_aux_cell(P, Snew.cons, Anext, c, k);
         }
-        Snew.cons[c] = Ssum.cons[c];
-        Snew.cons[N + c] = Ssum.cons[N + c];
-        Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
-        Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
-        double rho = Ssum.cons[c];
-        {
-            double rs = rho + Ssum.cons[cidx(g, im, j, k)];
-            double m = Ssum.mx[c];
-            double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
-            double u2 = (m * 2.0) / rs; m = (u2 * 0.5) * rs;
-            Snew.mx[c] = m; un[c] = u2;
-        }
-        {
-            double rs = rho + Ssum.cons[cidx(g, i, jm, k)];
-            double m = Ssum.my[c];
-            double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
-            double v2 = (m * 2.0) / rs; m = (v2 * 0.5) * rs;
-            Snew.my[c] = m; vn[c] = v2;
-        }
-        if (k == 0) {
-            Snew.mz[c] = 0.0; wn[c] = 0.0;
-        } else {
-            double rs = rho + Ssum.cons[c - g.sk];
-            double m = Ssum.mz[c];
-            double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
-            double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
-            Snew.mz[c] = m; wn[c] = w2;
-        }
-        if (k == g.nz - 1) { Snew.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
-        if (make_next) stage_aux_cell(P, Snew.cons, Anext, c, k);
+        __syncthreads();
     }
 }
-
-}  // namespace erfb
-
-namespace erfb {
 
 // Momentum fluxes of AdvectionSrcFor{X,Y,Z}Mom_N (ERF_AdvectionSrcForMom_N.H:
 // 17-274).  Each is the flux through the low side of the face's control
 // volume in one direction; the high side is the same function one index up.
+template <int HT>
 __device__ __forceinline__ double xmom_flux_x(const Params& P, const double* ru, const double* u, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (ru[cidx(g, wrap(i - 1, g.nx), j, k)] + ru[cidx(g, i, j, k)]);
-    return a * gatherx_interp(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    return a * gatherx_interp<HT>(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
 }
+template <int HT>
 __device__ __forceinline__ double xmom_flux_y(const Params& P, const double* rv, const double* u, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, wrap(i - 1, g.nx), j, k)]);
-    return a * gathery_interp(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    return a * gathery_interp<HT>(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
 }
+template <int VT>
 __device__ __forceinline__ double xmom_flux_z(const Params& P, const double* rw, const double* u, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (rw[cidx(g, i, j, k)] + rw[cidx(g, wrap(i - 1, g.nx), j, k)]);
-    return a * gatherz_tang(g, u, P.dyc_v, a, P.f_dyc_v, i, j, k);
+    return a * gatherz_tang<VT>(g, u, P.dyc_v, a, P.f_dyc_v, i, j, k);
 }
+template <int HT>
 __device__ __forceinline__ double ymom_flux_x(const Params& P, const double* ru, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (ru[cidx(g, i, j, k)] + ru[cidx(g, i, wrap(j - 1, g.ny), k)]);
-    return a * gatherx_interp(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    return a * gatherx_interp<HT>(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
 }
+template <int HT>
 __device__ __forceinline__ double ymom_flux_y(const Params& P, const double* rv, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, i, wrap(j - 1, g.ny), k)]);
-    return a * gathery_interp(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    return a * gathery_interp<HT>(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
 }
+template <int VT>
 __device__ __forceinline__ double ymom_flux_z(const Params& P, const double* rw, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (rw[cidx(g, i, j, k)] + rw[cidx(g, i, wrap(j - 1, g.ny), k)]);
-    return a * gatherz_tang(g, v, P.dyc_v, a, P.f_dyc_v, i, j, k);
+    return a * gatherz_tang<VT>(g, v, P.dyc_v, a, P.f_dyc_v, i, j, k);
 }
+template <int HT>
 __device__ __forceinline__ double zmom_flux_x(const Params& P, const double* ru, const double* w, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (ru[cidx(g, i, j, k)] + ru[cidx(g, i, j, k - 1)]) * 1.0;
-    return a * gatherx_interp(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    return a * gatherx_interp<HT>(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
 }
+template <int HT>
 __device__ __forceinline__ double zmom_flux_y(const Params& P, const double* rv, const double* w, int i, int j, int k) {
     const Geo& g = P.g;
     double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, i, j, k - 1)]) * 1.0;
-    return a * gathery_interp(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    return a * gathery_interp<HT>(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
 }
 // Vertical flux of w between faces kk-1 and kk (the "lo" flux of face kk),
 // with the order reduction next to the walls (ERF_AdvectionSrcForMom_N.H:
 // 220-265); for kk == nz it is the "hi" flux of the top interior face,
 // which the reference takes centred.
+template <int VT>
 __device__ __forceinline__ double zmom_flux_z(const Params& P, const double* rw, const double* w, int i, int j, int kk) {
     const Geo& g = P.g;
     const int vt = P.dyc_v, lo_z_face = 0, hi_z_face = g.nz;
@@ -1271,12 +1317,12 @@ __device__ __forceinline__ double zmom_flux_z(const Params& P, const double* rw,
     };
     auto normal = [&](int q, double upw) {
         double sv[6];
-        int wd = stencil_width(vt);
+        const int wd = width_of<VT>(vt);
         for (int m = 0; m < 6; ++m) {
             int off = m - 3;
             sv[m] = (off >= -wd && off <= wd - 1) ? wz(q + off) : 0.0;
         }
-        return interp_rt(vt, sv, upw, vf);
+        return interp_of<VT>(vt, sv, upw, vf);
     };
     double a = 0.5 * (rw[cidx(g, i, j, kk)] + rw[cidx(g, i, j, kk - 1)]);
     double iv;
@@ -1292,23 +1338,25 @@ __device__ __forceinline__ double zmom_flux_z(const Params& P, const double* rw,
 // Slow RHS for the three momenta (erf_slow_rhs_pre face part,
 // ERF_slow_rhs_pre.cpp:556-744): AdvectionSrcForMom (N), DiffusionSrcForMom_N,
 // pressure gradient of p', buoyancy / Coriolis / geostrophic sources
-// (make_mom_sources, make_buoyancy).  Same x-y tiles marching in k as the
-// scalar transport: every momentum flux is evaluated once.
+// (make_mom_sources, make_buoyancy).  Same tiles as the scalar transport;
+// the three momenta's x/y fluxes of a level are staged before one barrier.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TTX * TTY) k_slow_mom(Params P, StateBuf S, StageAux A, const double* __restrict__ u,
-                                                        const double* __restrict__ v, const double* __restrict__ w,
-                                                        const double* __restrict__ t11, const double* __restrict__ t22,
-                                                        const double* __restrict__ t33, const double* __restrict__ t12,
-                                                        const double* __restrict__ t13, const double* __restrict__ t23,
-                                                        const double* __restrict__ pavg, double* __restrict__ Fmx,
-                                                        double* __restrict__ Fmy, double* __restrict__ Fmz) {
-    __shared__ FluxTile sh;
+template <int HT, int VT>
+__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P, int kz, StateBuf S, StageAux A,
+                                                        const double* __restrict__ u, const double* __restrict__ v,
+                                                        const double* __restrict__ w, const double* __restrict__ t11,
+                                                        const double* __restrict__ t22, const double* __restrict__ t33,
+                                                        const double* __restrict__ t12, const double* __restrict__ t13,
+                                                        const double* __restrict__ t23, const double* __restrict__ pavg,
+                                                        double* __restrict__ Fmx, double* __restrict__ Fmy,
+                                                        double* __restrict__ Fmz) {
+    __shared__ FluxTile sh[3];
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i = blockIdx.x * TTX + tx, j = blockIdx.y * TTY + ty;
     const bool ok = i < g.nx && j < g.ny;
-    const int k0 = blockIdx.z * TKZ, k1 = min(k0 + TKZ, g.nz);
+    const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
     const bool xedge = ok && (tx == TTX - 1 || i == g.nx - 1);
@@ -1319,24 +1367,38 @@ __global__ void __launch_bounds__(TTX * TTY) k_slow_mom(Params P, StateBuf S, St
     const double* cd = S.cons;
     const double* prim = A.prim;
     const double* pp = A.pp;
-    double czu = 0.0, czv = 0.0, czw = 0.0;   // carried vertical fluxes
+    double zlu = 0.0, zhu = 0.0, zlv = 0.0, zhv = 0.0, zlw = 0.0, zhw = 0.0;
     for (int k = k0; k < k1; ++k) {
         const int64_t c = ok ? cidx(g, i, j, k) : 0;
-        // ---------------- x-momentum on face i
-        double zl = 0.0, zh = 0.0;
+        const bool zk = ok && k >= 1;   // z-momentum on interior faces only
         if (ok) {
-            sh.fx[ty][tx] = xmom_flux_x(P, ru, u, i, j, k);
-            if (xedge) sh.fx[ty][tx + 1] = xmom_flux_x(P, ru, u, ip, j, k);
-            sh.fy[ty][tx] = xmom_flux_y(P, rv, u, i, j, k);
-            if (yedge) sh.fy[ty + 1][tx] = xmom_flux_y(P, rv, u, i, jp, k);
-            zl = (k == k0) ? xmom_flux_z(P, rw, u, i, j, k) : czu;
-            zh = xmom_flux_z(P, rw, u, i, j, k + 1);
-            czu = zh;
+            sh[0].fx[ty][tx] = xmom_flux_x<HT>(P, ru, u, i, j, k);
+            if (xedge) sh[0].fx[ty][tx + 1] = xmom_flux_x<HT>(P, ru, u, ip, j, k);
+            sh[0].fy[ty][tx] = xmom_flux_y<HT>(P, rv, u, i, j, k);
+            if (yedge) sh[0].fy[ty + 1][tx] = xmom_flux_y<HT>(P, rv, u, i, jp, k);
+            if (k == k0) zlu = xmom_flux_z<VT>(P, rw, u, i, j, k);
+            zhu = xmom_flux_z<VT>(P, rw, u, i, j, k + 1);
+            sh[1].fx[ty][tx] = ymom_flux_x<HT>(P, ru, v, i, j, k);
+            if (xedge) sh[1].fx[ty][tx + 1] = ymom_flux_x<HT>(P, ru, v, ip, j, k);
+            sh[1].fy[ty][tx] = ymom_flux_y<HT>(P, rv, v, i, j, k);
+            if (yedge) sh[1].fy[ty + 1][tx] = ymom_flux_y<HT>(P, rv, v, i, jp, k);
+            if (k == k0) zlv = ymom_flux_z<VT>(P, rw, v, i, j, k);
+            zhv = ymom_flux_z<VT>(P, rw, v, i, j, k + 1);
+        }
+        if (zk) {
+            sh[2].fx[ty][tx] = zmom_flux_x<HT>(P, ru, w, i, j, k);
+            if (xedge) sh[2].fx[ty][tx + 1] = zmom_flux_x<HT>(P, ru, w, ip, j, k);
+            sh[2].fy[ty][tx] = zmom_flux_y<HT>(P, rv, w, i, j, k);
+            if (yedge) sh[2].fy[ty + 1][tx] = zmom_flux_y<HT>(P, rv, w, i, jp, k);
+            if (k == k0 || k == 1) zlw = zmom_flux_z<VT>(P, rw, w, i, j, k);
+            zhw = zmom_flux_z<VT>(P, rw, w, i, j, k + 1);
         }
         __syncthreads();
+        // ---------------- x-momentum on face i
         if (ok) {
-            double rhs = -((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi * 1.0 + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi * 1.0 +
-                           (zh - zl) * g.dzi);
+            double rhs = -((sh[0].fx[ty][tx + 1] - sh[0].fx[ty][tx]) * g.dxi * 1.0 +
+                           (sh[0].fy[ty + 1][tx] - sh[0].fy[ty][tx]) * g.dyi * 1.0 + (zhu - zlu) * g.dzi);
+            zlu = zhu;
             if (P.use_diff)
                 rhs -= ((t11[c] - t11[cidx(g, im, j, k)]) * g.dxi * 1.0 + (t12[cidx(g, i, jp, k)] - t12[c]) * g.dyi * 1.0 +
                         (t13[c + g.sk] - t13[c]) * g.dzi);
@@ -1354,21 +1416,11 @@ __global__ void __launch_bounds__(TTX * TTY) k_slow_mom(Params P, StateBuf S, St
             rhs += (-gpx - 0.0) / (1.0 + q) + src;
             Fmx[c] = rhs;
         }
-        __syncthreads();
         // ---------------- y-momentum on face j
         if (ok) {
-            sh.fx[ty][tx] = ymom_flux_x(P, ru, v, i, j, k);
-            if (xedge) sh.fx[ty][tx + 1] = ymom_flux_x(P, ru, v, ip, j, k);
-            sh.fy[ty][tx] = ymom_flux_y(P, rv, v, i, j, k);
-            if (yedge) sh.fy[ty + 1][tx] = ymom_flux_y(P, rv, v, i, jp, k);
-            zl = (k == k0) ? ymom_flux_z(P, rw, v, i, j, k) : czv;
-            zh = ymom_flux_z(P, rw, v, i, j, k + 1);
-            czv = zh;
-        }
-        __syncthreads();
-        if (ok) {
-            double rhs = -((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi * 1.0 + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi * 1.0 +
-                           (zh - zl) * g.dzi);
+            double rhs = -((sh[1].fx[ty][tx + 1] - sh[1].fx[ty][tx]) * g.dxi * 1.0 +
+                           (sh[1].fy[ty + 1][tx] - sh[1].fy[ty][tx]) * g.dyi * 1.0 + (zhv - zlv) * g.dzi);
+            zlv = zhv;
             if (P.use_diff)
                 rhs -= ((t12[cidx(g, ip, j, k)] - t12[c]) * g.dxi * 1.0 + (t22[c] - t22[cidx(g, i, jm, k)]) * g.dyi * 1.0 +
                         (t23[c + g.sk] - t23[c]) * g.dzi);
@@ -1385,23 +1437,12 @@ __global__ void __launch_bounds__(TTX * TTY) k_slow_mom(Params P, StateBuf S, St
             rhs += (-gpy - 0.0) / (1.0 + q) + src;
             Fmy[c] = rhs;
         }
-        __syncthreads();
-        // ---------------- z-momentum on face k (interior faces only)
-        const bool zk = ok && k >= 1;
-        if (zk) {
-            sh.fx[ty][tx] = zmom_flux_x(P, ru, w, i, j, k);
-            if (xedge) sh.fx[ty][tx + 1] = zmom_flux_x(P, ru, w, ip, j, k);
-            sh.fy[ty][tx] = zmom_flux_y(P, rv, w, i, j, k);
-            if (yedge) sh.fy[ty + 1][tx] = zmom_flux_y(P, rv, w, i, jp, k);
-            zl = (k == k0 || k == 1) ? zmom_flux_z(P, rw, w, i, j, k) : czw;
-            zh = zmom_flux_z(P, rw, w, i, j, k + 1);
-            czw = zh;
-        }
-        __syncthreads();
+        // ---------------- z-momentum on face k
         if (ok && k == 0) Fmz[c] = 0.0;
         if (zk) {
-            double rhs = -((sh.fx[ty][tx + 1] - sh.fx[ty][tx]) * g.dxi * 1.0 + (sh.fy[ty + 1][tx] - sh.fy[ty][tx]) * g.dyi * 1.0 +
-                           (zh - zl) * g.dzi);
+            double rhs = -((sh[2].fx[ty][tx + 1] - sh[2].fx[ty][tx]) * g.dxi * 1.0 +
+                           (sh[2].fy[ty + 1][tx] - sh[2].fy[ty][tx]) * g.dyi * 1.0 + (zhw - zlw) * g.dzi);
+            zlw = zhw;
             if (P.use_diff)
                 rhs -= ((t13[cidx(g, ip, j, k)] - t13[c]) * g.dxi * 1.0 + (t23[cidx(g, i, jp, k)] - t23[c]) * g.dyi * 1.0 +
                         (t33[c] - t33[c - g.sk]) * g.dzi);
@@ -1462,6 +1503,94 @@ __global__ void __launch_bounds__(TTX * TTY) k_slow_mom(Params P, StateBuf S, St
         if (ok && k == g.nz - 1) Fmz[c + g.sk] = 0.0;
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers for the tiled kernels: scheme dispatch and grid sizing.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Levels per block: minimise waves x (levels + 1), the cost of a block being
+// its levels plus the extra bottom-face flux evaluation.
+template <typename K>
+int pick_kz(K kern, const Geo& g) {
+    int dev = 0, nsm = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, TTX * TTY, 0) != cudaSuccess || per < 1) per = 1;
+    const long cap = (long)per * nsm;
+    const long nxy = (long)((g.nx + TTX - 1) / TTX) * ((g.ny + TTY - 1) / TTY);
+    int best = g.nz;
+    double best_cost = 1e30;
+    for (int zb = 1; zb <= g.nz; ++zb) {
+        int kz = (g.nz + zb - 1) / zb;
+        int zb2 = (g.nz + kz - 1) / kz;
+        long waves = (nxy * zb2 + cap - 1) / cap;
+        double cost = (double)waves * (kz + 1);
+        if (cost < best_cost) { best_cost = cost; best = kz; }
+    }
+    return best;
+}
+
+dim3 tile_grid(const Geo& g, int kz) { return dim3((g.nx + TTX - 1) / TTX, (g.ny + TTY - 1) / TTY, (g.nz + kz - 1) / kz); }
+
+constexpr int U5 = ERF_ADV_UPWIND_5TH, W5 = ERF_ADV_WENO_5;
+
+}  // namespace
+
+using SlowCellK = void (*)(Params, int, StateBuf, StageAux, const double*, double*, double*, double*, double*);
+using SlowMomK = void (*)(Params, int, StateBuf, StageAux, const double*, const double*, const double*, const double*,
+                          const double*, const double*, const double*, const double*, const double*, const double*,
+                          double*, double*, double*);
+using PostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, StateBuf, StageAux, StageAux, int,
+                       const double*, const double*, const double*, const double*, double*, double*, double*);
+
+static SlowCellK slow_cell_kernel(const Params& P) {
+    if (P.dyc_h == U5 && P.dyc_v == U5) return k_slow_cell<U5, U5>;
+    if (P.dyc_h == W5 && P.dyc_v == W5) return k_slow_cell<W5, W5>;
+    return k_slow_cell<-1, -1>;
+}
+static SlowMomK slow_mom_kernel(const Params& P) {
+    if (P.dyc_h == U5 && P.dyc_v == U5) return k_slow_mom<U5, U5>;
+    return k_slow_mom<-1, -1>;
+}
+static PostK post_kernel(const Params& P) {
+    bool dw = P.dry_h == W5 && P.dry_v == W5, du = P.dry_h == U5 && P.dry_v == U5;
+    bool mw = P.moi_h == W5 && P.moi_v == W5, mu = P.moi_h == U5 && P.moi_v == U5;
+    if (!P.moist) {
+        if (dw) return k_post<W5, W5, -1, -1>;
+        if (du) return k_post<U5, U5, -1, -1>;
+    } else {
+        if (dw && mw) return k_post<W5, W5, W5, W5>;
+        if (du && mu) return k_post<U5, U5, U5, U5>;
+        if (du && mw) return k_post<U5, U5, W5, W5>;
+    }
+    return k_post<-1, -1, -1, -1>;
+}
+
+void tiled_setup(const Params& P, TiledKz* t) {
+    t->cell = pick_kz(slow_cell_kernel(P), P.g);
+    t->mom = pick_kz(slow_mom_kernel(P), P.g);
+    t->post = pick_kz(post_kernel(P), P.g);
+}
+
+void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* mut,
+                      double* Fcons, double* avx, double* avy, double* avz) {
+    slow_cell_kernel(P)<<<tile_grid(P.g, t.cell), dim3(TTX, TTY, 1), 0, st>>>(P, t.cell, S, A, mut, Fcons, avx, avy, avz);
+}
+void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* u,
+                     const double* v, const double* w, const double* t11, const double* t22, const double* t33,
+                     const double* t12, const double* t13, const double* t23, const double* pavg, double* Fmx,
+                     double* Fmy, double* Fmz) {
+    slow_mom_kernel(P)<<<tile_grid(P.g, t.mom), dim3(TTX, TTY, 1), 0, st>>>(P, t.mom, S, A, u, v, w, t11, t22, t33,
+                                                                             t12, t13, t23, pavg, Fmx, Fmy, Fmz);
+}
+void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
+                 StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext, int make_next, const double* mut,
+                 const double* avx, const double* avy, const double* avz, double* un, double* vn, double* wn) {
+    post_kernel(P)<<<tile_grid(P.g, t.post), dim3(TTX, TTY, 1), 0, st>>>(P, t.post, slow_dt, Sold, Sst, Ssum, Snew,
+                                                                          Acur, Anext, make_next, mut, avx, avy, avz,
+                                                                          un, vn, wn);
 }
 
 }  // namespace erfb

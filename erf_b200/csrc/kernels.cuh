@@ -42,4 +42,21 @@ struct StageAux {
     double* pp;     // ncell (p - p0)
 };
 
+// x-y tile of the transport kernels (slow_cell, slow_mom, post) and the
+// levels each of their blocks marches through (chosen per context).
+constexpr int TTX = 32, TTY = 8;
+struct TiledKz {
+    int cell, mom, post;
+};
+void tiled_setup(const Params& P, TiledKz* t);
+void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* mut,
+                      double* Fcons, double* avx, double* avy, double* avz);
+void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* u,
+                     const double* v, const double* w, const double* t11, const double* t22, const double* t33,
+                     const double* t12, const double* t13, const double* t23, const double* pavg, double* Fmx,
+                     double* Fmy, double* Fmz);
+void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
+                 StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext, int make_next, const double* mut,
+                 const double* avx, const double* avy, const double* avz, double* un, double* vn, double* wn);
+
 }  // namespace erfb

@@ -759,8 +759,9 @@ struct Oracle {
         loop(valid(CC), [&](int i, int j, int k) {
             R.cons(i, j, k, 0) = -1.0 / 1.0 * ((fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2]);
         });
-        advect_scalars(1, 1, Scr.mx, Scr.my, Scr.mz, prim, R.cons, c.dryscal_horiz_adv, c.dryscal_vert_adv,
-                       c.dryscal_horiz_upw_frac, c.dryscal_vert_upw_frac);
+        // rho*theta is advected with the dycore scheme (ERF_slow_rhs_pre.cpp:139-142, 469-477)
+        advect_scalars(1, 1, Scr.mx, Scr.my, Scr.mz, prim, R.cons, c.dycore_horiz_adv, c.dycore_vert_adv,
+                       c.dycore_horiz_upw_frac, c.dycore_vert_upw_frac);
         if (use_diff) diffusion_state(1, 1, cd, prim, R.cons, mut);
         // cc_src is zero for the supported configurations
 
