@@ -47,38 +47,47 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------
-# Algorithmic bytes per cell for each kernel slot: every array the pass must
-# read or write, counted once, at 8 bytes (FP64).  The derivation per slot is
-# in DESIGN.md ("Kernels and their rooflines").
+# Algorithmic traffic per cell for each kernel slot: every array the pass must
+# read or write, counted once, as (FP64 values, bulk values).  Bulk values are
+# 8 bytes in the plain form and 4 bytes in the mixed form; the prognostic
+# state, velocities and base state are FP64 in both.
 # ---------------------------------------------------------------------------
 def algorithmic_values_per_cell(cfg):
     moist = cfg.moisture != 0
+    m2 = 2 if moist else 0
     nq = cfg.ncomp - 5
     diff = cfg.les_type != 0 or cfg.molec_diff_type != 0
+    les = 1 if cfg.les_type == 1 else 0
+    d = 1 if diff else 0
     return {
-        # reads cons(ncomp) + u,v,w; writes 3 momenta, 3 velocities, prim (ncomp-1), pi, p'
-        "step_begin": cfg.ncomp + 3 + 3 + 3 + (cfg.ncomp - 1) + 2 + (1 if cfg.les_type == 1 else 0),
-        "stress": 4 + (1 if diff else 0) + 6,
-        # reads 3 momenta, theta, (rho, mu for diffusion); writes rhs rho, rho-theta, 3 avg momenta
-        "slow_cell": 3 + 1 + (2 if diff else 0) + 2 + 3,
-        "plane_avg": 5 if moist else 2,
-        # reads 3 momenta, 3 velocities, rho, p', (moisture 2), (6 stresses); writes 3 rhs
-        "slow_mom": 3 + 3 + 1 + 1 + (2 if moist else 0) + (6 if diff else 0) + 3,
-        # reads prev 2 mom + rho-theta (+rho), stage 2 mom + rho-theta, 2 rhs, lag, pi, (q 2),
-        # avg 2; writes avg 2, new 2 mom, lag
-        "fast_horizontal": 3 + 3 + 2 + 1 + 1 + (2 if moist else 0) + 2 + 2 + 2 + 1,
-        # reads prev rho, rho-theta, w-mom; stage rho, rho-theta, 3 mom; new 2 mom; theta;
-        # coefficients A, 1/B', C/B', P, Q; rhs rho, rho-theta, w; avg w;
-        # writes rho, rho-theta, w-mom, avg w
-        "fast_column": 3 + 5 + 2 + 1 + 5 + 3 + 1 + 4,
-        # reads scalars prim (1+nq), 3 avg mom, old scalars (1+nq), sum rho, rho-theta, 3 mom;
-        # writes new cons (ncomp), 3 mom, 3 vel, next prim (ncomp-1), pi, p'
-        "slow_post": (1 + nq) * 2 + 3 + 5 + cfg.ncomp + 6 + (cfg.ncomp - 1) + 2,
+        # reads cons(ncomp) + u,v,w; writes 3 momenta, 3 velocities | prim (ncomp-1), pi, p', (mu_t)
+        "step_begin": (cfg.ncomp + 3 + 3 + 3, (cfg.ncomp - 1) + 2 + les),
+        # reads u,v,w, rho | mu_t; writes 6 stresses
+        "stress": (4, d + 6),
+        # reads 3 momenta, (rho) | theta, (mu_t); writes rhs rho, rho-theta, 3 avg momenta
+        "slow_cell": (3 + d, 1 + d + 2 + 3),
+        # reads rho | theta, (qv, qc, qp)
+        "plane_avg": (1, 4 if moist else 1),
+        # reads 3 momenta, 3 velocities, rho | p', (qv, qc), (6 stresses); writes 3 rhs
+        "slow_mom": (7, 1 + m2 + 6 * d + 3),
+        # reads prev 2 mom, rho-theta, rho; stage 2 mom, rho-theta; writes new 2 mom |
+        # reads 2 rhs, lag, pi, (qv, qc), avg 2; writes avg 2, lag
+        "fast_horizontal": (9, 9 + m2),
+        # reads prev rho, rho-theta, w-mom; stage rho, rho-theta, 3 mom; new 2 mom; writes rho,
+        # rho-theta, w-mom | theta, 5 coefficients, rhs rho, rho-theta, w; avg w read+write
+        "fast_column": (13, 11),
+        # reads old scalars (1+nq), sum rho, rho-theta, 3 mom; writes ncomp, 3 mom, 3 vel |
+        # reads scalar prims (1+nq), 3 avg mom; writes next prim (ncomp-1), pi, p'
+        "slow_post": ((1 + nq) + 5 + cfg.ncomp + 6, (1 + nq) + 3 + (cfg.ncomp - 1) + 2),
         # reads rho, rho-theta, 3 moisture; writes all ncomp (into the other buffer)
-        "kessler": (5 + cfg.ncomp) if moist else 0,
-        # reads stage rho-theta, theta, pi, (q 2); writes A, 1/B', C/B', P, Q
-        "fast_coeffs": 3 + (2 if moist else 0) + 5,
+        "kessler": ((5 + cfg.ncomp) if moist else 0, 0),
+        # reads stage rho-theta | theta, pi, (qv, qc); writes A, 1/B', C/B', P, Q
+        "fast_coeffs": (1, 1 + 1 + m2 + 5),
     }
+
+
+def bytes_per_cell(vals, bulk_bytes):
+    return {k: 8 * a + bulk_bytes * b for k, (a, b) in vals.items()}
 
 
 def sample_clocks(stop, out):
@@ -212,91 +221,136 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    from erf_b200 import Dycore
+    from erf_b200 import Dycore, config as C
     case = cases.CASES[args.case]()
     cfg = case.cfg
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    dy = Dycore(cfg, stream=stream.cuda_stream)
-    base = dy.make_base_state(case)
-    dy.set_base_state(base)
-    cons, u, v, w = case.build_state(base[0])
-    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (cons, u, v, w)]
-    torch.cuda.synchronize()
+    n_cells = cfg.nx * cfg.ny * cfg.nz
+    peaks, peak_kind = load_peaks()
+    hbm = float(peaks["hbm_gbs"])
+    vals = algorithmic_values_per_cell(cfg)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- warm-up (graph already instantiated at create)
-    dy.advance(*dev, args.warmup)
-    barrier()
+    def measure(precision, clocks):
+        """Time one precision form: graph replay (device-resident state),
+        eager per-kernel events, and end to end through the host entry point."""
+        cfg.precision = precision
+        dy = Dycore(cfg, stream=stream.cuda_stream)
+        base = dy.make_base_state(case)
+        dy.set_base_state(base)
+        cons, u, v, w = case.build_state(base[0])
+        dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (cons, u, v, w)]
+        torch.cuda.synchronize()
+        dy.advance(*dev, args.warmup)
+        barrier()
+        # ---- timed region 1: device-resident state, CUDA graph replay
+        stop = threading.Event()
+        th = None
+        if clocks is not None:
+            th = threading.Thread(target=sample_clocks, args=(stop, clocks), daemon=True)
+            th.start()
+            time.sleep(0.3)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dy.advance(*dev, args.steps)
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        stop.set()
+        if th is not None:
+            th.join(timeout=5)
+        ms = max_over_ranks(ms, world, "cuda")
+        st = dy.status()
+        value = replica_throughput(world, n_cells, args.steps, ms * 1e-3)
+        # ---- timed region 2: same K steps, eager launches with per-kernel events
+        barrier()
+        prof = dy.advance_profiled(*dev, args.steps)
+        barrier()
+        # ---- timed region 3: end to end through the host-buffer entry point,
+        #      pinned host memory in and out every step
+        host = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (cons, u, v, w)]
+        h2d = sum(t.numel() * 8 for t in host)
+        dy.lib.erf_b200_advance_host(dy.ctx, *[t.data_ptr() for t in host], 1)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            rc = dy.lib.erf_b200_advance_host(dy.ctx, *[t.data_ptr() for t in host], 1)
+            if rc:
+                raise RuntimeError(f"advance_host rc={rc}")
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+        e2e = replica_throughput(world, n_cells, args.steps, e2e_s)
+        bpc = bytes_per_cell(vals, 4 if precision == C.PREC_MIXED else 8)
+        kern = {}
+        for name, (kms, cnt) in prof.items():
+            if cnt == 0:
+                continue
+            per_launch_ms = kms / cnt
+            nb = bpc.get(name, 0) * n_cells
+            kern[name] = {"launches": cnt, "total_ms": kms, "ms_per_launch": per_launch_ms, "algo_bytes": nb,
+                          "gbs": nb / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else None}
+        dominant = max(kern, key=lambda k: kern[k]["total_ms"])
+        dk = kern[dominant]
+        form = "mixed" if precision == C.PREC_MIXED else "fp64"
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as fh:
+                traffic = json.load(fh).get(f"{args.case}/{form}", {}).get(dominant)
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm, "unit": "GB/s",
+                    "frac": dk["gbs"] / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                    "algo_bytes_per_launch": dk["algo_bytes"], "ms_per_launch": dk["ms_per_launch"]}
+        step_bytes = sum(bpc[k] * n_cells * (kern[k]["launches"] / args.steps) for k in kern)
+        roof_cells = hbm * 1e9 / (step_bytes / n_cells)
+        out = {"value": value, "ms_per_step": ms / args.steps, "status": st,
+               "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+               "roofline": roofline,
+               "step_roofline": {"algo_bytes_per_cell_step": step_bytes / n_cells,
+                                 "hbm_roof_cell_steps_per_s": roof_cells, "frac": value / world / roof_cells},
+               "kernels": kern, "launches": dy.kernels_per_step() * args.steps}
+        dy.close()
+        return out, base, (cons, u, v, w)
 
-    # ---- timed region 1: device-resident state, CUDA graph replay
-    clock_samples, stop = [], threading.Event()
-    th = threading.Thread(target=sample_clocks, args=(stop, clock_samples), daemon=True)
-    th.start()
-    time.sleep(0.3)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    dy.advance(*dev, args.steps)
-    e1.record(stream)
-    barrier()
-    ms = e0.elapsed_time(e1)
-    stop.set()
-    th.join(timeout=5)
-    ms = max_over_ranks(ms, world, "cuda")
-    st = dy.status()
-    n_cells = cfg.nx * cfg.ny * cfg.nz
-    value = replica_throughput(world, n_cells, args.steps, ms * 1e-3)
+    def form_error(base, init, nsteps):
+        """Per-field relative L2 of the mixed form against the plain FP64 form
+        (parity-pinned to the oracle) after nsteps from the same state."""
+        res = {}
+        for prec in (C.PREC_FP64, C.PREC_MIXED):
+            cfg.precision = prec
+            dy = Dycore(cfg, stream=stream.cuda_stream)
+            dy.set_base_state(base)
+            dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in init]
+            dy.advance(*dev, nsteps)
+            torch.cuda.synchronize()
+            res[prec] = [t.cpu().numpy() for t in dev]
+            dy.close()
+        cfg.precision = C.PREC_FP64
+        (c64, u64, v64, w64), (c32, u32, v32, w32) = res[C.PREC_FP64], res[C.PREC_MIXED]
 
-    # ---- timed region 2: same K steps, eager launches with per-kernel events
-    barrier()
-    prof = dy.advance_profiled(*dev, args.steps)
-    barrier()
+        def rl2(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+        err = {"u": rl2(u32, u64), "v": rl2(v32, v64), "w": rl2(w32, w64), "theta": rl2(c32[1] / c32[0], c64[1] / c64[0])}
+        if cfg.moisture != 0:
+            for n, nm in ((5, "qv"), (6, "qc"), (7, "qr")):
+                if n < c64.shape[0]:
+                    err[nm] = rl2(c32[n] / c32[0], c64[n] / c64[0])
+        qv32 = c32[5, 0] / c32[0, 0] if cfg.moisture != 0 else 0.0
+        qv64 = c64[5, 0] / c64[0, 0] if cfg.moisture != 0 else 0.0
+        ps = lambda c, qv: 1.0e5 * (287.0 * c[1, 0] * (1.0 + 461.505 / 287.0 * qv) / 1.0e5) ** 1.4
+        err["p_sfc"] = rl2(ps(c32, qv32), ps(c64, qv64))
+        return err
 
-    # ---- timed region 3: end to end through the host-buffer entry point,
-    #      pinned host memory in and out every step
-    host = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (cons, u, v, w)]
-    h2d = sum(t.numel() * 8 for t in host)
-    dy.lib.erf_b200_advance_host(dy.ctx, *[t.data_ptr() for t in host], 1)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        rc = dy.lib.erf_b200_advance_host(dy.ctx, *[t.data_ptr() for t in host], 1)
-        if rc:
-            raise RuntimeError(f"advance_host rc={rc}")
-    barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
-    e2e = replica_throughput(world, n_cells, args.steps, e2e_s)
-
-    peaks, peak_kind = load_peaks()
-    hbm = float(peaks["hbm_gbs"])
-    vals = algorithmic_values_per_cell(cfg)
-    kern = {}
-    for name, (kms, cnt) in prof.items():
-        if cnt == 0:
-            continue
-        per_launch_ms = kms / cnt
-        nb = vals.get(name, 0) * 8 * n_cells
-        if name == "plane_avg":
-            nb = vals[name] * 8 * n_cells
-        kern[name] = {"launches": cnt, "total_ms": kms, "ms_per_launch": per_launch_ms,
-                      "algo_bytes": nb, "gbs": nb / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else None}
-    dominant = max(kern, key=lambda k: kern[k]["total_ms"])
-    dk = kern[dominant]
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as fh:
-            traffic = json.load(fh).get(args.case, {}).get(dominant)
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm, "unit": "GB/s",
-                "frac": dk["gbs"] / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                "algo_bytes_per_launch": dk["algo_bytes"], "ms_per_launch": dk["ms_per_launch"]}
-    step_bytes = sum(vals[k] * 8 * n_cells * (kern[k]["launches"] / args.steps) for k in kern)
-    roof_cells = hbm * 1e9 / (step_bytes / n_cells)
+    clock_samples = []
+    plain, base, init = measure(C.PREC_FP64, clock_samples)
+    mixed, _, _ = measure(C.PREC_MIXED, None)
+    mixed_err = form_error(base, init, 100) if rank == 0 else None
+    cfg.precision = C.PREC_FP64
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -306,28 +360,32 @@ def main():
                "sample": f"2 steps of a {bx}x{by}x{cfg.nz} block of the {args.case} case "
                          f"({t_cpu:.1f} s, FP64 oracle, OpenMP)"}
 
-    launches = dy.kernels_per_step() * args.steps
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": plain["value"], "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": plain["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.case} {cfg.nx}x{cfg.ny}x{cfg.nz}, Kessler, Upwind_5th dycore, "
-                                   f"WENO5 scalars, dt={cfg.dt} s, {cfg.mri_ratio} substeps/RK stage 3, FP64 plain",
+            "config": {"workload": f"{args.case} {cfg.nx}x{cfg.ny}x{cfg.nz}, "
+                                   f"{'Kessler, ' if cfg.moisture else ''}dt={cfg.dt} s, "
+                                   f"{cfg.mri_ratio} substeps/RK stage 3, FP64 plain form",
                        "cells": n_cells, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "working set > 126 MB L2 (no flush needed)"},
-            "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-            "roofline": roofline,
-            "step_roofline": {"algo_bytes_per_cell_step": step_bytes / n_cells,
-                              "hbm_roof_cell_steps_per_s": roof_cells, "frac": value / world / roof_cells},
-            "kernels": kern,
+            "e2e": plain["e2e"],
+            "roofline": plain["roofline"],
+            "step_roofline": plain["step_roofline"],
+            "kernels": plain["kernels"],
+            "mixed": {"value": mixed["value"], "ms_per_step": mixed["ms_per_step"],
+                      "speedup_vs_fp64": mixed["value"] / plain["value"], "dtype": "f32 bulk / f64 state",
+                      "e2e": mixed["e2e"], "roofline": mixed["roofline"], "step_roofline": mixed["step_roofline"],
+                      "kernels": {k: {"ms_per_launch": v["ms_per_launch"], "gbs": v["gbs"]}
+                                  for k, v in mixed["kernels"].items()},
+                      "rel_l2_vs_fp64_after_100_steps": mixed_err, "status": mixed["status"]},
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clock_samples),
-            "gpu_launches": launches,
-            "status": st,
+            "gpu_launches": plain["launches"],
+            "status": plain["status"],
         }
         print(json.dumps(line), flush=True)
-    dy.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

@@ -10,26 +10,7 @@
 #include "kernels.cuh"
 
 namespace erfb {
-__global__ void k_step_begin(Params P, const double* cons, const double* uo, const double* vo, const double* wo,
-                             StateBuf S, double* un, double* vn, double* wn, StageAux A, double* mut);
-__global__ void k_tau(Params P, const double* cons, const double* u, const double* v, const double* w,
-                      const double* mut, double* t11, double* t22, double* t33, double* t12, double* t13, double* t23);
-__global__ void k_plane_avg(Params P, const double* cons, const double* prim, double* avg);
-__global__ void k_fast_h(Params P, int step, int nrk, double dtau, double facinv, StateBuf Sprev, int prev_rt,
-                         StateBuf Sst, StageAux A, const double* Fmx, const double* Fmy, const double* lag_in,
-                         double* lag_out, double* avx, double* avy, double* outx, double* outy);
-__global__ void k_fast_col(Params P, int step, double dtau, double facinv, double D, double beta_1, double beta_2,
-                           StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux A, const double* Fcons,
-                           const double* Fmz, const double* newx, const double* newy, double* avz, double* out_cons,
-                           double* out_mz, double* sc_soln, double* sc_cb, double* sc_tr0, double* sc_tr1);
 __global__ void k_kessler(Params P, double* cons, double dtn, double dz);
-__global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double* cA, double* cInvB, double* cCB,
-                            double* cP, double* cQ);
-__global__ void k_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
-                            int prev_rt, StateBuf Sst, StageAux A, const double* Fcons, const double* Fmz,
-                            const double* newx, const double* newy, const double* cA, const double* cInvB,
-                            const double* cCB, const double* cP, const double* cQ, double* avz, double* out_cons,
-                            double* out_mz);
 __global__ void k_kessler_cells(Params P, const double* cin, double* cout, double dtn, double dz);
 __global__ void k_base_state(int nz, double dz, double g, double rdOcp, const double* th_cc, const double* qv_cc,
                              double th_s, double qv_s, double p_s, double* rho0, double* p0o, double* pi0o,
@@ -40,6 +21,18 @@ __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const doubl
 }  // namespace erfb
 
 using namespace erfb;
+
+// Bulk arrays of a context (type R: double plain, float mixed).
+template <class R>
+struct Bulk {
+    R *Fcons, *Fmx, *Fmy, *Fmz;   // slow right-hand sides
+    R *avx, *avy, *avz;           // average momenta of the substeps
+    R* lag[2];                    // lagged d(rho theta), ping-pong
+    StageAux<R> aux[2];           // stage primitives, Exner, p'
+    R* mut;                       // eddy viscosity
+    R *t11, *t22, *t33, *t12, *t13, *t23;
+    R *cA, *cInvB, *cCB, *cP, *cQ;  // fast coefficients of the current stage
+};
 
 // Threads per block of the vertical acoustic kernel (columns x level groups).
 #ifndef ERFB_VERT_THREADS
@@ -57,15 +50,11 @@ struct erf_b200_ctx {
     std::vector<void*> allocs;
 
     StateBuf S[4];            // [0],[1] alternate old/new, [2] second stage buffer, [3] fast sum
-    double* vel[2][3];        // alternating old/new face velocities
-    double *Fcons, *Fmx, *Fmy, *Fmz;
-    double *avx, *avy, *avz;
-    double* lag[2];
-    StageAux aux[2];
-    double* mut;
-    double *t11, *t22, *t33, *t12, *t13, *t23;
+    double* vel[2][3];        // alternating old/new face velocities (FP64 prognostic)
     double* pavg;
-    double *cA, *cInvB, *cCB, *cP, *cQ;  // fast coefficients of the current stage
+    Bulk<double> bd;          // bulk arrays of the plain form
+    Bulk<float> bf;           // bulk arrays of the mixed form
+    bool mixed = false;
     int tile_tx = 32, vert_warps = 32, coef_warps = 8;
     TiledKz tkz{1, 1, 1};
     size_t vert_smem = 0, coef_smem = 0;
@@ -90,14 +79,15 @@ int cuda_fail(cudaError_t e) {
         if (e_ != cudaSuccess) return cuda_fail(e_); \
     } while (0)
 
-int dalloc(erf_b200_ctx* c, double** p, size_t n) {
+template <class T>
+int dalloc(erf_b200_ctx* c, T** p, size_t n) {
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, n * sizeof(double));
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
     if (e != cudaSuccess) return cuda_fail(e);
-    cudaMemsetAsync(q, 0, n * sizeof(double), c->stream);
+    cudaMemsetAsync(q, 0, n * sizeof(T), c->stream);
     c->allocs.push_back(q);
-    c->bytes += n * sizeof(double);
-    *p = (double*)q;
+    c->bytes += n * sizeof(T);
+    *p = (T*)q;
     return ERF_B200_OK;
 }
 
@@ -133,7 +123,7 @@ int validate(const erf_b200_config* c) {
         return ERF_B200_ECONFIG;
     }
     if (c->buoyancy_type != 1 && c->buoyancy_type != 2 && c->buoyancy_type != 3) return ERF_B200_ECONFIG;
-    if (c->precision != ERF_PREC_FP64) return ERF_B200_ECONFIG;
+    if (c->precision != ERF_PREC_FP64 && c->precision != ERF_PREC_MIXED) return ERF_B200_ECONFIG;
     return ERF_B200_OK;
 }
 
@@ -235,17 +225,18 @@ struct LaunchTimer {
     } while (0)
 
 // Enqueue one full step with parity p (state slot p is the old state).
-void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
+template <class R>
+void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     const Params& P = c->P;
     const Geo& g = c->g;
     cudaStream_t st = c->stream;
     StateBuf OLD = c->S[p], N0 = c->S[1 - p], N1 = c->S[2], SUM = c->S[3];
     double** Vold = c->vel[p];
     double** Vnew = c->vel[1 - p];
-    dim3 cb = cell_block(), cg = cell_grid(g), kb = col_block(), kg = col_grid(g);
+    dim3 cb = cell_block(), cg = cell_grid(g);
 
-    TIMED(0, (k_step_begin<<<cg, cb, 0, st>>>(P, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1],
-                                              Vnew[2], c->aux[0], c->mut)));
+    TIMED(0, launch_step_begin<R>(P, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
+                                  B.aux[0], B.mut));
     // stage outputs alternate between the two scratch states so that the last
     // one lands in slot 1-p (or in N1 when Kessler moves it to slot 1-p)
     StateBuf outs[3] = {N0, N1, N0};
@@ -259,37 +250,57 @@ void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
     const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
     for (int nrk = 0; nrk < 3; ++nrk) {
         StateBuf Sst = stage[nrk], Snew = outs[nrk];
-        StageAux Acur = c->aux[a], Anext = c->aux[1 - a];
+        StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
         int nsub; double dtau, slow_dt;
         stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
         if (P.use_diff)
-            TIMED(1, (k_tau<<<cg, cb, 0, st>>>(P, Sst.cons, Vnew[0], Vnew[1], Vnew[2], c->mut, c->t11, c->t22,
-                                               c->t33, c->t12, c->t13, c->t23)));
-        TIMED(2, launch_slow_cell(P, c->tkz, st, Sst, Acur, c->mut, c->Fcons, c->avx, c->avy, c->avz));
-        if (P.moist && P.buoy_type == 2)
-            TIMED(3, (k_plane_avg<<<g.nz, 256, 0, st>>>(P, Sst.cons, Acur.prim, c->pavg)));
-        TIMED(4, launch_slow_mom(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], c->t11, c->t22, c->t33, c->t12,
-                                 c->t13, c->t23, c->pavg, c->Fmx, c->Fmy, c->Fmz));
+            TIMED(1, launch_tau<R>(P, st, Sst.cons, Vnew[0], Vnew[1], Vnew[2], B.mut, B.t11, B.t22, B.t33, B.t12,
+                                   B.t13, B.t23));
+        TIMED(2, launch_slow_cell<R>(P, c->tkz, st, Sst, Acur, B.mut, B.Fcons, B.avx, B.avy, B.avz));
+        if (P.moist && P.buoy_type == 2) TIMED(3, launch_plane_avg<R>(P, st, Sst.cons, Acur.prim, c->pavg));
+        TIMED(4, launch_slow_mom<R>(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12,
+                                    B.t13, B.t23, c->pavg, B.Fmx, B.Fmy, B.Fmz));
         double facinv = 1.0 / (double)nsub;
         double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
-        TIMED(9, (k_fast_coef<<<tg, tcb, c->coef_smem, st>>>(P, D, Sst, Acur, c->cA, c->cInvB, c->cCB, c->cP,
-                                                             c->cQ)));
+        TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
         for (int ks = 0; ks < nsub; ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
-            TIMED(5, (k_fast_h<<<cg, cb, 0, st>>>(P, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, c->Fmx, c->Fmy,
-                                                  c->lag[lp], c->lag[1 - lp], c->avx, c->avy, SUM.mx, SUM.my)));
+            TIMED(5, launch_fast_h<R>(P, st, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, B.Fmx, B.Fmy, B.lag[lp],
+                                      B.lag[1 - lp], B.avx, B.avy, SUM.mx, SUM.my));
             lp ^= 1;
-            TIMED(6, (k_fast_vert<<<tg, tb, c->vert_smem, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, prt, Sst,
-                                                                Acur, c->Fcons, c->Fmz, SUM.mx, SUM.my, c->cA,
-                                                                c->cInvB, c->cCB, c->cP, c->cQ, c->avz, SUM.cons,
-                                                                SUM.mz)));
+            TIMED(6, launch_fast_vert<R>(P, st, tg, tb, c->vert_smem, dtau, facinv, beta_1, beta_2, Sprev, prt, Sst,
+                                         Acur, B.Fcons, B.Fmz, SUM.mx, SUM.my, B.cA, B.cInvB, B.cCB, B.cP, B.cQ,
+                                         B.avz, SUM.cons, SUM.mz));
         }
-        TIMED(7, launch_post(P, c->tkz, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, c->mut, c->avx,
-                             c->avy, c->avz, Vnew[0], Vnew[1], Vnew[2]));
+        TIMED(7, launch_post<R>(P, c->tkz, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut,
+                                B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
     }
     if (P.moist) TIMED(8, (k_kessler_cells<<<cg, cb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
+}
+
+void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {
+    if (c->mixed) enqueue_step_t<float>(c, c->bf, p, T);
+    else enqueue_step_t<double>(c, c->bd, p, T);
+}
+
+template <class R>
+int alloc_bulk(erf_b200_ctx* c, Bulk<R>& B) {
+    const erf_b200_config* cfg = &c->cfg;
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    const int64_t NZF = (int64_t)cfg->nx * cfg->ny * (cfg->nz + 1);
+    const int nc = cfg->ncomp;
+    int rc = ERF_B200_OK;
+    auto A = [&](R** p, size_t n) { if (rc == ERF_B200_OK) rc = dalloc(c, p, n); };
+    A(&B.Fcons, 2 * N); A(&B.Fmx, N); A(&B.Fmy, N); A(&B.Fmz, NZF);
+    A(&B.avx, N); A(&B.avy, N); A(&B.avz, NZF);
+    A(&B.lag[0], N); A(&B.lag[1], N);
+    for (int p = 0; p < 2; ++p) { A(&B.aux[p].prim, (nc - 1) * N); A(&B.aux[p].pi, N); A(&B.aux[p].pp, N); }
+    A(&B.mut, N);
+    A(&B.t11, N); A(&B.t22, N); A(&B.t33, N); A(&B.t12, N); A(&B.t13, NZF); A(&B.t23, NZF);
+    A(&B.cA, NZF); A(&B.cInvB, NZF); A(&B.cCB, NZF); A(&B.cP, NZF); A(&B.cQ, NZF);
+    return rc;
 }
 
 int build_graphs(erf_b200_ctx* c) {
@@ -386,14 +397,9 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         A(&c->S[s].cons, nc * N); A(&c->S[s].mx, N); A(&c->S[s].my, N); A(&c->S[s].mz, NZF);
     }
     for (int p = 0; p < 2; ++p) { A(&c->vel[p][0], N); A(&c->vel[p][1], N); A(&c->vel[p][2], NZF); }
-    A(&c->Fcons, 2 * N); A(&c->Fmx, N); A(&c->Fmy, N); A(&c->Fmz, NZF);
-    A(&c->avx, N); A(&c->avy, N); A(&c->avz, NZF);
-    A(&c->lag[0], N); A(&c->lag[1], N);
-    for (int p = 0; p < 2; ++p) { A(&c->aux[p].prim, (nc - 1) * N); A(&c->aux[p].pi, N); A(&c->aux[p].pp, N); }
-    A(&c->mut, N);
-    A(&c->t11, N); A(&c->t22, N); A(&c->t33, N); A(&c->t12, N); A(&c->t13, NZF); A(&c->t23, NZF);
     A(&c->pavg, 5 * cfg->nz);
-    A(&c->cA, NZF); A(&c->cInvB, NZF); A(&c->cCB, NZF); A(&c->cP, NZF); A(&c->cQ, NZF);
+    c->mixed = cfg->precision == ERF_PREC_MIXED;
+    if (rc == ERF_B200_OK) rc = c->mixed ? alloc_bulk(c, c->bf) : alloc_bulk(c, c->bd);
     A(&c->r0, cfg->nz + 2); A(&c->p0, cfg->nz + 2); A(&c->pi0, cfg->nz + 2); A(&c->th0, cfg->nz + 2);
     if (rc == ERF_B200_OK) {
         void* q = nullptr;
@@ -402,22 +408,23 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     }
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     make_params(c);
-    tiled_setup(c->P, &c->tkz);
+    if (c->mixed) tiled_setup<float>(c->P, &c->tkz);
+    else tiled_setup<double>(c->P, &c->tkz);
     c->lag_parity_per_step = substeps_per_step(c->cfg) & 1;
     // shared-memory tiles of the vertical kernels: TX columns x all levels
     {
         const size_t max_smem = 227 * 1024;
         int nz = cfg->nz;
         c->tile_tx = 32;
-        while (c->tile_tx > 4 && (size_t)(7 * nz + 5) * c->tile_tx * sizeof(double) > max_smem) c->tile_tx /= 2;
-        c->vert_smem = (size_t)(7 * nz + 5) * c->tile_tx * sizeof(double);
-        c->coef_smem = (size_t)3 * (nz + 1) * c->tile_tx * sizeof(double);
+        const size_t rs = c->mixed ? sizeof(float) : sizeof(double);
+        while (c->tile_tx > 4 && (size_t)(7 * nz + 5) * c->tile_tx * rs > max_smem) c->tile_tx /= 2;
+        c->vert_smem = (size_t)(7 * nz + 5) * c->tile_tx * rs;
+        c->coef_smem = (size_t)3 * (nz + 1) * c->tile_tx * rs;
         if (c->vert_smem > max_smem) rc = ERF_B200_ECONFIG;
         c->vert_warps = ERFB_VERT_THREADS / c->tile_tx;
         c->coef_warps = c->tile_tx == 32 ? 8 : 16;
         if (rc == ERF_B200_OK) {
-            if (cudaFuncSetAttribute(k_fast_vert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->vert_smem) != cudaSuccess ||
-                cudaFuncSetAttribute(k_fast_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->coef_smem) != cudaSuccess)
+            if ((c->mixed ? vert_setup<float>(c->vert_smem, c->coef_smem) : vert_setup<double>(c->vert_smem, c->coef_smem)) != 0)
                 rc = ERF_B200_ECUDA;
         }
         if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }

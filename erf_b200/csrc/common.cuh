@@ -50,7 +50,8 @@ __device__ __forceinline__ double eos_rt_given_p(double p) {
 // ---------------------------------------------------------------------------
 // Face interpolants (reference: Source/Utils/ERF_Interpolation_UPW.H:9-611,
 // ERF_Interpolation_WENO.H:9-259).  s[0..5] = phi at offsets -3..+2 from the
-// face's high-side cell; upw is the advecting momentum on the face.
+// face's high-side cell; upw is the advecting momentum on the face.  V is
+// the arithmetic type (double for the plain form, float for the mixed form).
 // ---------------------------------------------------------------------------
 template <int TYPE>
 struct Interp;
@@ -58,66 +59,74 @@ struct Interp;
 template <>
 struct Interp<ERF_ADV_CENTERED_2ND> {
     static constexpr int W = 1;
-    __device__ static __forceinline__ double eval(const double* s, double, double) { return 0.5 * (s[3] + s[2]); }
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V, V) { return V(0.5) * (s[3] + s[2]); }
 };
 template <>
 struct Interp<ERF_ADV_UPWIND_3RD> {
     static constexpr int W = 2;
-    __device__ static __forceinline__ double eval(const double* s, double upw, double frac) {
-        if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V upw, V frac) {
+        if (upw != V(0)) upw = (upw > V(0)) ? V(1) : V(-1);
         upw *= frac;
-        double a1 = s[3] + s[2], d1 = s[3] - s[2], a2 = s[4] + s[1], d2 = s[4] - s[1];
-        return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2 + upw * (1.0 / 12.0) * (d2 - 3.0 * d1);
+        V a1 = s[3] + s[2], d1 = s[3] - s[2], a2 = s[4] + s[1], d2 = s[4] - s[1];
+        return V(7.0 / 12.0) * a1 - V(1.0 / 12.0) * a2 + upw * V(1.0 / 12.0) * (d2 - V(3) * d1);
     }
 };
 template <>
 struct Interp<ERF_ADV_CENTERED_4TH> {
     static constexpr int W = 2;
-    __device__ static __forceinline__ double eval(const double* s, double, double) {
-        double a1 = s[3] + s[2], a2 = s[4] + s[1];
-        return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2;
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V, V) {
+        V a1 = s[3] + s[2], a2 = s[4] + s[1];
+        return V(7.0 / 12.0) * a1 - V(1.0 / 12.0) * a2;
     }
 };
 template <>
 struct Interp<ERF_ADV_UPWIND_5TH> {
     static constexpr int W = 3;
-    __device__ static __forceinline__ double eval(const double* s, double upw, double frac) {
-        if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V upw, V frac) {
+        if (upw != V(0)) upw = (upw > V(0)) ? V(1) : V(-1);
         upw *= frac;
-        double a1 = s[3] + s[2], a2 = s[4] + s[1], a3 = s[5] + s[0];
-        double d1 = s[3] - s[2], d2 = s[4] - s[1], d3 = s[5] - s[0];
-        return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3 - upw * (1.0 / 60.0) * (d3 - 5.0 * d2 + 10.0 * d1);
+        V a1 = s[3] + s[2], a2 = s[4] + s[1], a3 = s[5] + s[0];
+        V d1 = s[3] - s[2], d2 = s[4] - s[1], d3 = s[5] - s[0];
+        return V(37.0 / 60.0) * a1 - V(2.0 / 15.0) * a2 + V(1.0 / 60.0) * a3 -
+               upw * V(1.0 / 60.0) * (d3 - V(5) * d2 + V(10) * d1);
     }
 };
 template <>
 struct Interp<ERF_ADV_CENTERED_6TH> {
     static constexpr int W = 3;
-    __device__ static __forceinline__ double eval(const double* s, double, double) {
-        double a1 = s[3] + s[2], a2 = s[4] + s[1], a3 = s[5] + s[0];
-        return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3;
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V, V) {
+        V a1 = s[3] + s[2], a2 = s[4] + s[1], a3 = s[5] + s[0];
+        return V(37.0 / 60.0) * a1 - V(2.0 / 15.0) * a2 + V(1.0 / 60.0) * a3;
     }
 };
 template <>
 struct Interp<ERF_ADV_WENO_3> {
     static constexpr int W = 2;
     // WENO3 (ERF_Interpolation_WENO.H:9-124) with the weights normalised once.
-    __device__ static __forceinline__ double ev(double a, double b, double c) {
-        const double eps = 1.0e-6;
-        double b1 = (b - a) * (b - a), b2 = (c - b) * (c - b);
-        double e1 = (eps + b1) * (eps + b1), e2 = (eps + b2) * (eps + b2);
-        double w1 = (1.0 / 3.0) * e2;
-        double w2 = (2.0 / 3.0) * e1;
-        double ws = w1 + w2;
-        double v1 = -a + 3.0 * b, v2 = b + c;
-        return (w1 * v1 + w2 * v2) / (2.0 * ws);
+    template <class V>
+    __device__ static __forceinline__ V ev(V a, V b, V c) {
+        const V eps = V(1.0e-6);
+        V b1 = (b - a) * (b - a), b2 = (c - b) * (c - b);
+        V e1 = (eps + b1) * (eps + b1), e2 = (eps + b2) * (eps + b2);
+        V w1 = V(1.0 / 3.0) * e2;
+        V w2 = V(2.0 / 3.0) * e1;
+        V ws = w1 + w2;
+        V v1 = -a + V(3) * b, v2 = b + c;
+        return (w1 * v1 + w2 * v2) / (V(2) * ws);
     }
     // The upwind side is selected by operand choice rather than a branch, so
     // a warp whose faces have mixed signs evaluates the scheme once.
-    __device__ static __forceinline__ double eval(const double* s, double upw, double) {
-        const double tol = 1.0e-12;
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V upw, V) {
+        const V tol = V(1.0e-12);
         const bool pos = upw > tol;
-        double r = ev(pos ? s[1] : s[4], pos ? s[2] : s[3], pos ? s[3] : s[2]);
-        return (upw > tol || upw < -tol) ? r : 0.5 * (s[3] + s[2]);
+        V r = ev<V>(pos ? s[1] : s[4], pos ? s[2] : s[3], pos ? s[3] : s[2]);
+        return (upw > tol || upw < -tol) ? r : V(0.5) * (s[3] + s[2]);
     }
 };
 template <>
@@ -128,40 +137,43 @@ struct Interp<ERF_ADV_WENO_5> {
     // 129-259).  The non-linear weights g_k / (eps + b_k)^2 are formed as
     // g_k * prod_{m != k} (eps + b_m)^2, which has the same ratios and needs
     // one division (the normalisation) instead of four.
-    __device__ static __forceinline__ double ev(double a, double b, double c, double d, double e) {
-        const double c1 = 13.0 / 12.0, eps = 1.0e-6;
-        double b1 = c1 * (a - 2.0 * b + c) * (a - 2.0 * b + c) + 0.25 * (a - 4.0 * b + 3.0 * c) * (a - 4.0 * b + 3.0 * c);
-        double b2 = c1 * (b - 2.0 * c + d) * (b - 2.0 * c + d) + 0.25 * (b - d) * (b - d);
-        double b3 = c1 * (c - 2.0 * d + e) * (c - 2.0 * d + e) + 0.25 * (3.0 * c - 4.0 * d + e) * (3.0 * c - 4.0 * d + e);
-        double e1 = (eps + b1) * (eps + b1), e2 = (eps + b2) * (eps + b2), e3 = (eps + b3) * (eps + b3);
-        double w1 = (1.0 / 10.0) * (e2 * e3);
-        double w2 = (3.0 / 5.0) * (e1 * e3);
-        double w3 = (3.0 / 10.0) * (e1 * e2);
-        double ws = w1 + w2 + w3;
-        double v1 = 2.0 * a - 7.0 * b + 11.0 * c;
-        double v2 = -b + 5.0 * c + 2.0 * d;
-        double v3 = 2.0 * c + 5.0 * d - e;
-        return (w1 * v1 + w2 * v2 + w3 * v3) / (6.0 * ws);
+    template <class V>
+    __device__ static __forceinline__ V ev(V a, V b, V c, V d, V e) {
+        const V c1 = V(13.0 / 12.0), eps = V(1.0e-6);
+        V b1 = c1 * (a - V(2) * b + c) * (a - V(2) * b + c) + V(0.25) * (a - V(4) * b + V(3) * c) * (a - V(4) * b + V(3) * c);
+        V b2 = c1 * (b - V(2) * c + d) * (b - V(2) * c + d) + V(0.25) * (b - d) * (b - d);
+        V b3 = c1 * (c - V(2) * d + e) * (c - V(2) * d + e) + V(0.25) * (V(3) * c - V(4) * d + e) * (V(3) * c - V(4) * d + e);
+        V e1 = (eps + b1) * (eps + b1), e2 = (eps + b2) * (eps + b2), e3 = (eps + b3) * (eps + b3);
+        V w1 = V(1.0 / 10.0) * (e2 * e3);
+        V w2 = V(3.0 / 5.0) * (e1 * e3);
+        V w3 = V(3.0 / 10.0) * (e1 * e2);
+        V ws = w1 + w2 + w3;
+        V v1 = V(2) * a - V(7) * b + V(11) * c;
+        V v2 = -b + V(5) * c + V(2) * d;
+        V v3 = V(2) * c + V(5) * d - e;
+        return (w1 * v1 + w2 * v2 + w3 * v3) / (V(6) * ws);
     }
-    __device__ static __forceinline__ double eval(const double* s, double upw, double) {
-        const double tol = 1.0e-12;
+    template <class V>
+    __device__ static __forceinline__ V eval(const V* s, V upw, V) {
+        const V tol = V(1.0e-12);
         const bool pos = upw > tol;
-        double r = ev(pos ? s[0] : s[5], pos ? s[1] : s[4], pos ? s[2] : s[3], pos ? s[3] : s[2], pos ? s[4] : s[1]);
-        return (upw > tol || upw < -tol) ? r : 0.5 * (s[3] + s[2]);
+        V r = ev<V>(pos ? s[0] : s[5], pos ? s[1] : s[4], pos ? s[2] : s[3], pos ? s[3] : s[2], pos ? s[4] : s[1]);
+        return (upw > tol || upw < -tol) ? r : V(0.5) * (s[3] + s[2]);
     }
 };
 
 // Runtime dispatch over the supported interpolant codes
-__device__ __forceinline__ double interp_rt(int type, const double* s, double upw, double frac) {
+template <class V>
+__device__ __forceinline__ V interp_rt(int type, const V* s, V upw, V frac) {
     switch (type) {
-    case ERF_ADV_CENTERED_2ND: return Interp<ERF_ADV_CENTERED_2ND>::eval(s, upw, frac);
-    case ERF_ADV_UPWIND_3RD: return Interp<ERF_ADV_UPWIND_3RD>::eval(s, upw, frac);
-    case ERF_ADV_CENTERED_4TH: return Interp<ERF_ADV_CENTERED_4TH>::eval(s, upw, frac);
-    case ERF_ADV_UPWIND_5TH: return Interp<ERF_ADV_UPWIND_5TH>::eval(s, upw, frac);
-    case ERF_ADV_CENTERED_6TH: return Interp<ERF_ADV_CENTERED_6TH>::eval(s, upw, frac);
-    case ERF_ADV_WENO_3: return Interp<ERF_ADV_WENO_3>::eval(s, upw, frac);
-    case ERF_ADV_WENO_5: return Interp<ERF_ADV_WENO_5>::eval(s, upw, frac);
-    default: return 0.0;
+    case ERF_ADV_CENTERED_2ND: return Interp<ERF_ADV_CENTERED_2ND>::eval<V>(s, upw, frac);
+    case ERF_ADV_UPWIND_3RD: return Interp<ERF_ADV_UPWIND_3RD>::eval<V>(s, upw, frac);
+    case ERF_ADV_CENTERED_4TH: return Interp<ERF_ADV_CENTERED_4TH>::eval<V>(s, upw, frac);
+    case ERF_ADV_UPWIND_5TH: return Interp<ERF_ADV_UPWIND_5TH>::eval<V>(s, upw, frac);
+    case ERF_ADV_CENTERED_6TH: return Interp<ERF_ADV_CENTERED_6TH>::eval<V>(s, upw, frac);
+    case ERF_ADV_WENO_3: return Interp<ERF_ADV_WENO_3>::eval<V>(s, upw, frac);
+    case ERF_ADV_WENO_5: return Interp<ERF_ADV_WENO_5>::eval<V>(s, upw, frac);
+    default: return V(0);
     }
 }
 __host__ __device__ __forceinline__ int stencil_width(int type) {
@@ -179,27 +191,29 @@ __device__ __forceinline__ int width_of(int rt) {
     if constexpr (T < 0) return stencil_width(rt);
     else return Interp<T>::W;
 }
-template <int T>
-__device__ __forceinline__ double interp_of(int rt, const double* s, double upw, double frac) {
-    if constexpr (T < 0) return interp_rt(rt, s, upw, frac);
-    else return Interp<T>::eval(s, upw, frac);
+template <int T, class V>
+__device__ __forceinline__ V interp_of(int rt, const V* s, V upw, V frac) {
+    if constexpr (T < 0) return interp_rt<V>(rt, s, upw, frac);
+    else return Interp<T>::template eval<V>(s, upw, frac);
 }
 
 // Wall-reduced vertical interpolant for w (UPWINDALL, reference
 // ERF_Interpolation_UPW.H:528-611); s entries outside the scheme's width are
 // ignored.
-__device__ __forceinline__ double interp_all(int type, const double* s, double upw, double frac) {
-    if (type == ERF_ADV_CENTERED_2ND) return 0.5 * (s[3] + s[2]);
+template <class V>
+__device__ __forceinline__ V interp_all(int type, const V* s, V upw, V frac) {
+    if (type == ERF_ADV_CENTERED_2ND) return V(0.5) * (s[3] + s[2]);
     bool wide = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH);
-    double sm3 = wide ? s[0] : 0., sp2 = wide ? s[5] : 0.;
-    if (upw != 0.) upw = (upw > 0) ? 1. : -1.;
+    V sm3 = wide ? s[0] : V(0), sp2 = wide ? s[5] : V(0);
+    if (upw != V(0)) upw = (upw > V(0)) ? V(1) : V(-1);
     upw *= frac;
-    double a1 = s[3] + s[2], a2 = s[4] + s[1], d1 = s[3] - s[2], d2 = s[4] - s[1];
-    double a3 = sp2 + sm3, d3 = sp2 - sm3;
-    if (type == ERF_ADV_UPWIND_3RD) return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2 + upw * (1.0 / 12.0) * (d2 - 3.0 * d1);
-    if (type == ERF_ADV_CENTERED_4TH) return (7.0 / 12.0) * a1 - (1.0 / 12.0) * a2;
-    if (type == ERF_ADV_UPWIND_5TH) return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3 - upw * (1.0 / 60.0) * (d3 - 5.0 * d2 + 10.0 * d1);
-    return (37.0 / 60.0) * a1 - (2.0 / 15.0) * a2 + (1.0 / 60.0) * a3;
+    V a1 = s[3] + s[2], a2 = s[4] + s[1], d1 = s[3] - s[2], d2 = s[4] - s[1];
+    V a3 = sp2 + sm3, d3 = sp2 - sm3;
+    if (type == ERF_ADV_UPWIND_3RD) return V(7.0 / 12.0) * a1 - V(1.0 / 12.0) * a2 + upw * V(1.0 / 12.0) * (d2 - V(3) * d1);
+    if (type == ERF_ADV_CENTERED_4TH) return V(7.0 / 12.0) * a1 - V(1.0 / 12.0) * a2;
+    if (type == ERF_ADV_UPWIND_5TH)
+        return V(37.0 / 60.0) * a1 - V(2.0 / 15.0) * a2 + V(1.0 / 60.0) * a3 - upw * V(1.0 / 60.0) * (d3 - V(5) * d2 + V(10) * d1);
+    return V(37.0 / 60.0) * a1 - V(2.0 / 15.0) * a2 + V(1.0 / 60.0) * a3;
 }
 
 // ---------------------------------------------------------------------------

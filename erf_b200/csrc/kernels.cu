@@ -1,4 +1,4 @@
-// kernels.cu -- FP64 dycore kernels for sm_100a.
+// kernels.cu -- dycore kernels for sm_100a.
 //
 // Each kernel fuses one or more of the reference's AMReX ParallelFor passes
 // (file:line cited per kernel).  Lateral neighbours are addressed through
@@ -7,6 +7,13 @@
 // substeps; the reference's momentum<->velocity round trips at every boundary
 // fill (BoundaryConditions/ERF_FillIntermediatePatch.cpp:63-67, 224-236) are
 // applied inline where the filled values are next read.
+//
+// The dycore kernels are templates on R, the type of the bulk arrays (derived
+// fields, slow right-hand sides, average momenta, fast coefficients, stresses)
+// and of the arithmetic on them: R = double is the plain FP64 form, R = float
+// the mixed form.  The prognostic state (conserved variables, momenta,
+// between-step velocities), the base state and the equation of state stay
+// FP64 in both, and every update of the state is accumulated in FP64.
 #include "kernels.cuh"
 
 namespace erfb {
@@ -23,14 +30,16 @@ __device__ __forceinline__ double tang(const double* __restrict__ f, const Geo& 
     return __ldg(f + cidx(g, i, j, k));
 }
 // Cell-centred scalar with foextrap in z.
-__device__ __forceinline__ double ccz(const double* __restrict__ f, const Geo& g, int i, int j, int k) {
+template <class V>
+__device__ __forceinline__ V ccz(const V* __restrict__ f, const Geo& g, int i, int j, int k) {
     return __ldg(f + cidx(g, i, j, clampk(k, g.nz)));
 }
 
 // ---------------------------------------------------------------------------
 // Strain-rate components (Diffusion/ERF_ComputeStrain_N.cpp:28-229) with the
 // one-sided wall stencils at no-slip walls.  Edge (i,j,k) of an xy/xz/yz edge
-// array sits at the low corner of cell (i,j,k).
+// array sits at the low corner of cell (i,j,k).  Velocities are FP64 state;
+// the differences are formed in FP64.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double strain12(const double* u, const double* v, const Geo& g, int i, int j, int k) {
     int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
@@ -64,17 +73,19 @@ __device__ __forceinline__ bool cell_coords(const Geo& g, int& i, int& j, int& k
 }
 
 // Derived stage quantities of one cell: cons_to_prim + pi_stage
-// (TimeIntegration/ERF_TI_utils.H:4-45) and p' (ERF_slow_rhs_pre.cpp:337-358).
-__device__ __forceinline__ void stage_aux_cell(const Params& P, const double* __restrict__ cons, StageAux A,
+// (TimeIntegration/ERF_TI_utils.H:4-45) and p' (ERF_slow_rhs_pre.cpp:337-358),
+// evaluated in FP64 from the FP64 state and stored as R.
+template <class R>
+__device__ __forceinline__ void stage_aux_cell(const Params& P, const double* __restrict__ cons, StageAux<R> A,
                                                int64_t c, int k) {
     const int64_t N = P.g.ncell;
     double rho = cons[c];
     double rt = cons[N + c];
-    A.prim[c] = rt / rho;
-    for (int n = 1; n < P.nprim; ++n) A.prim[n * N + c] = cons[(n + 1) * N + c] / rho;
-    A.pi[c] = eos_exner(rt, P.rdOcp);
+    A.prim[c] = R(rt / rho);
+    for (int n = 1; n < P.nprim; ++n) A.prim[n * N + c] = R(cons[(n + 1) * N + c] / rho);
+    A.pi[c] = R(eos_exner(rt, P.rdOcp));
     double qv = P.moist ? cons[5 * N + c] / rho : 0.0;
-    A.pp[c] = eos_p(rt, qv) - P.p0[k + 1];
+    A.pp[c] = R(eos_p(rt, qv) - P.p0[k + 1]);
     if (!(rt > 0.0) || !(rho > 0.0)) atomicOr(P.status, ST_BADSTATE);
 }
 
@@ -88,10 +99,11 @@ __device__ __forceinline__ void stage_aux_cell(const Params& P, const double* __
 //     (ERF_advance_dycore.cpp:260-276);
 //   * cons_to_prim / pi_stage / p' of the old state.
 // ---------------------------------------------------------------------------
+template <class R>
 __global__ void k_step_begin(Params P, const double* __restrict__ cons, const double* __restrict__ uo,
                              const double* __restrict__ vo, const double* __restrict__ wo, StateBuf S,
                              double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn,
-                             StageAux A, double* __restrict__ mut) {
+                             StageAux<R> A, R* __restrict__ mut) {
     const Geo& g = P.g;
     int i, j, k;
     if (!cell_coords(g, i, j, k)) return;
@@ -116,7 +128,7 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
         S.mz[c] = (w1 * 0.5) * rs; wn[c] = w1;
     }
     if (k == g.nz - 1) { S.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
-    stage_aux_cell(P, cons, A, c, k);
+    stage_aux_cell<R>(P, cons, A, c, k);
 
     if (P.les == ERF_LES_SMAGORINSKY) {
         int ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
@@ -130,132 +142,127 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
         double s23 = 0.25 * (strain23(vo, wo, g, i, j, k) + strain23(vo, wo, g, i, j, k + 1) +
                              strain23(vo, wo, g, i, jp, k) + strain23(vo, wo, g, i, jp, k + 1));
         double S2 = s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + 2.0 * s23 * s23;
-        mut[c] = P.CsDeltaSqr * rho * sqrt(2.0 * S2);
+        mut[c] = R(P.CsDeltaSqr * rho * sqrt(2.0 * S2));
     }
 }
 
 // ---------------------------------------------------------------------------
 // Stress tensor (erf_make_tau_terms, TimeIntegration/ERF_make_tau_terms.cpp:
 // 320-424 with ComputeStress{Cons,Var}Visc_N, Diffusion/ERF_ComputeStress_N.cpp):
-// tau_ii at cell centres, tau_12/13/23 on edges.
+// tau_ii at cell centres, tau_12/13/23 on edges.  Strain in FP64 from the
+// FP64 velocities, viscosity and stress in R.
 // ---------------------------------------------------------------------------
+template <class R>
 __global__ void k_tau(Params P, const double* __restrict__ cons, const double* __restrict__ u,
-                      const double* __restrict__ v, const double* __restrict__ w, const double* __restrict__ mut,
-                      double* __restrict__ t11, double* __restrict__ t22, double* __restrict__ t33,
-                      double* __restrict__ t12, double* __restrict__ t13, double* __restrict__ t23) {
+                      const double* __restrict__ v, const double* __restrict__ w, const R* __restrict__ mut,
+                      R* __restrict__ t11, R* __restrict__ t22, R* __restrict__ t33, R* __restrict__ t12,
+                      R* __restrict__ t13, R* __restrict__ t23) {
     const Geo& g = P.g;
     int i, j, k;
     if (!cell_coords(g, i, j, k)) return;
     int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny), ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
     int64_t c = cidx(g, i, j, k);
-    const double OneThird = 1. / 3.;
-    double s11 = (u[cidx(g, ip, j, k)] - u[c]) * g.dxi;
-    double s22 = (v[cidx(g, i, jp, k)] - v[c]) * g.dyi;
-    double s33 = (w[c + g.sk] - w[c]) * g.dzi;
-    double er = s11 + s22 + s33;
-    double base = P.use_consA ? cons[c] * P.mu_eff : P.mu_eff;
-    double m11 = P.use_turb ? base + 2.0 * mut[c] : base;
+    const R OneThird = R(1. / 3.);
+    R s11 = R((u[cidx(g, ip, j, k)] - u[c]) * g.dxi);
+    R s22 = R((v[cidx(g, i, jp, k)] - v[c]) * g.dyi);
+    R s33 = R((w[c + g.sk] - w[c]) * g.dzi);
+    R er = s11 + s22 + s33;
+    const R mu_eff = R(P.mu_eff);
+    R base = P.use_consA ? R(cons[c]) * mu_eff : mu_eff;
+    R m11 = P.use_turb ? base + R(2) * mut[c] : base;
     t11[c] = -m11 * (s11 - OneThird * er);
     t22[c] = -m11 * (s22 - OneThird * er);
     t33[c] = -m11 * (s33 - OneThird * er);
     auto mu = [&](int ii, int jj, int kk) { return __ldg(mut + cidx(g, ii, jj, clampk(kk, g.nz))); };
-    auto rho = [&](int ii, int jj, int kk) { return __ldg(cons + cidx(g, ii, jj, clampk(kk, g.nz))); };
+    auto rho = [&](int ii, int jj, int kk) { return R(__ldg(cons + cidx(g, ii, jj, clampk(kk, g.nz)))); };
     {
-        double m = P.use_consA ? 0.25 * (rho(im, j, k) + rho(i, j, k) + rho(im, jm, k) + rho(i, jm, k)) * P.mu_eff : P.mu_eff;
-        if (P.use_turb) m = m + 2.0 * (0.25 * (mu(im, j, k) + mu(i, j, k) + mu(im, jm, k) + mu(i, jm, k)));
-        t12[c] = strain12(u, v, g, i, j, k) * -m;
+        R m = P.use_consA ? R(0.25) * (rho(im, j, k) + rho(i, j, k) + rho(im, jm, k) + rho(i, jm, k)) * mu_eff : mu_eff;
+        if (P.use_turb) m = m + R(2) * (R(0.25) * (mu(im, j, k) + mu(i, j, k) + mu(im, jm, k) + mu(i, jm, k)));
+        t12[c] = R(strain12(u, v, g, i, j, k)) * -m;
     }
     for (int kk = k; kk <= (k == g.nz - 1 ? g.nz : k); ++kk) {
         int64_t e = cidx(g, i, j, kk);
-        double m = P.use_consA ? 0.25 * (rho(im, j, kk) + rho(i, j, kk) + rho(im, j, kk - 1) + rho(i, j, kk - 1)) * P.mu_eff : P.mu_eff;
-        if (P.use_turb) m = m + 2.0 * (0.25 * (mu(im, j, kk) + mu(i, j, kk) + mu(im, j, kk - 1) + mu(i, j, kk - 1)));
-        t13[e] = strain13(u, w, g, i, j, kk) * -m;
-        double m2 = P.use_consA ? 0.25 * (rho(i, jm, kk) + rho(i, j, kk) + rho(i, jm, kk - 1) + rho(i, j, kk - 1)) * P.mu_eff : P.mu_eff;
-        if (P.use_turb) m2 = m2 + 2.0 * (0.25 * (mu(i, jm, kk) + mu(i, j, kk) + mu(i, jm, kk - 1) + mu(i, j, kk - 1)));
-        t23[e] = strain23(v, w, g, i, j, kk) * -m2;
+        R m = P.use_consA ? R(0.25) * (rho(im, j, kk) + rho(i, j, kk) + rho(im, j, kk - 1) + rho(i, j, kk - 1)) * mu_eff : mu_eff;
+        if (P.use_turb) m = m + R(2) * (R(0.25) * (mu(im, j, kk) + mu(i, j, kk) + mu(im, j, kk - 1) + mu(i, j, kk - 1)));
+        t13[e] = R(strain13(u, w, g, i, j, kk)) * -m;
+        R m2 = P.use_consA ? R(0.25) * (rho(i, jm, kk) + rho(i, j, kk) + rho(i, jm, kk - 1) + rho(i, j, kk - 1)) * mu_eff : mu_eff;
+        if (P.use_turb) m2 = m2 + R(2) * (R(0.25) * (mu(i, jm, kk) + mu(i, j, kk) + mu(i, jm, kk - 1) + mu(i, j, kk - 1)));
+        t23[e] = R(strain23(v, w, g, i, j, kk)) * -m2;
     }
 }
 
 // ---------------------------------------------------------------------------
 // Scalar flux helpers
 // ---------------------------------------------------------------------------
-// Advective flux of primitive component `pc` through the low x/y/z face of
-// cell (i,j,k): mom * interp(phi) (Advection/ERF_AdvectionSrcForScalars.H:7-58).
-template <int T = -1>
-__device__ __forceinline__ double adv_flux_x(const Geo& g, const double* __restrict__ phi, const double* __restrict__ mom,
-                                             int type, double frac, int i, int j, int k) {
-    double s[6];
+// Advective flux of a primitive scalar phi (type R) through the low x/y/z face
+// of cell (i,j,k): mom * interp(phi) (Advection/ERF_AdvectionSrcForScalars.H:
+// 7-58).  The advecting momentum M is the FP64 stage momentum (rho, theta)
+// or the R average momentum (slow scalars).
+template <int T, class R, class M>
+__device__ __forceinline__ R adv_flux_x(const Geo& g, const R* __restrict__ phi, const M* __restrict__ mom, int type,
+                                        R frac, int i, int j, int k) {
+    R s[6];
     const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, wrap(i + off, g.nx), j, k)) : 0.0;
+        s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, wrap(i + off, g.nx), j, k)) : R(0);
     }
-    double a = __ldg(mom + cidx(g, i, j, k));
-    return a * interp_of<T>(type, s, a, frac);
+    R a = R(__ldg(mom + cidx(g, i, j, k)));
+    return a * interp_of<T, R>(type, s, a, frac);
 }
-template <int T = -1>
-__device__ __forceinline__ double adv_flux_y(const Geo& g, const double* __restrict__ phi, const double* __restrict__ mom,
-                                             int type, double frac, int i, int j, int k) {
-    double s[6];
+template <int T, class R, class M>
+__device__ __forceinline__ R adv_flux_y(const Geo& g, const R* __restrict__ phi, const M* __restrict__ mom, int type,
+                                        R frac, int i, int j, int k) {
+    R s[6];
     const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, i, wrap(j + off, g.ny), k)) : 0.0;
+        s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, i, wrap(j + off, g.ny), k)) : R(0);
     }
-    double a = __ldg(mom + cidx(g, i, j, k));
-    return a * interp_of<T>(type, s, a, frac);
+    R a = R(__ldg(mom + cidx(g, i, j, k)));
+    return a * interp_of<T, R>(type, s, a, frac);
 }
-template <int T = -1>
-__device__ __forceinline__ double adv_flux_z(const Geo& g, const double* __restrict__ phi, const double* __restrict__ mom,
-                                             int type, double frac, int i, int j, int k) {
-    double s[6];
+template <int T, class R, class M>
+__device__ __forceinline__ R adv_flux_z(const Geo& g, const R* __restrict__ phi, const M* __restrict__ mom, int type,
+                                        R frac, int i, int j, int k) {
+    R s[6];
     const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? ccz(phi, g, i, j, k + off) : 0.0;
+        s[m] = (off >= -w && off <= w - 1) ? ccz(phi, g, i, j, k + off) : R(0);
     }
-    double a = __ldg(mom + cidx(g, i, j, k));
-    return a * interp_of<T>(type, s, a, frac);
-}
-
-// Advective tendency of one scalar (assigns, like AdvectionSrcForScalars,
-// Advection/ERF_AdvectionSrcForState.cpp:359-370)
-__device__ __forceinline__ double scalar_adv_tend(const Params& P, const double* phi, const double* ax,
-                                                  const double* ay, const double* az, int th, int tv, double fh,
-                                                  double fv, int i, int j, int k) {
-    const Geo& g = P.g;
-    int ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
-    double fxl = adv_flux_x(g, phi, ax, th, fh, i, j, k), fxh = adv_flux_x(g, phi, ax, th, fh, ip, j, k);
-    double fyl = adv_flux_y(g, phi, ay, th, fh, i, j, k), fyh = adv_flux_y(g, phi, ay, th, fh, i, jp, k);
-    double fzl = adv_flux_z(g, phi, az, tv, fv, i, j, k), fzh = adv_flux_z(g, phi, az, tv, fv, i, j, k + 1);
-    return -1.0 * 1.0 * ((fxh - fxl) * g.dxi + (fyh - fyl) * g.dyi + (fzh - fzl) * g.dzi);
+    R a = R(__ldg(mom + cidx(g, i, j, k)));
+    return a * interp_of<T, R>(type, s, a, frac);
 }
 
 // Diffusive tendency -div(-rhoAlpha grad phi) (Diffusion/ERF_DiffusionSrcForState_N.cpp:
 // 196-667), scalars foextrap at the walls; returns the amount subtracted.
-__device__ __forceinline__ double scalar_diff(const Params& P, const double* __restrict__ rhoarr,
-                                              const double* __restrict__ phi, const double* __restrict__ mut,
-                                              double ae, double fac, int i, int j, int k) {
+template <class R>
+__device__ __forceinline__ R scalar_diff(const Params& P, const double* __restrict__ rhoarr, const R* __restrict__ phi,
+                                         const R* __restrict__ mut, double ae_d, double fac_d, int i, int j, int k) {
     const Geo& g = P.g;
+    const R ae = R(ae_d), fac = R(fac_d);
+    const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi);
     int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny), ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
     auto ph = [&](int ii, int jj, int kk) { return ccz(phi, g, ii, jj, kk); };
     auto rA = [&](int i0, int j0, int k0, int i1, int j1, int k1) {
-        double r = P.use_consA ? 0.5 * (ccz(rhoarr, g, i0, j0, k0) + ccz(rhoarr, g, i1, j1, k1)) * ae : ae;
-        if (P.use_turb) r += 0.5 * (ccz(mut, g, i0, j0, k0) * fac + ccz(mut, g, i1, j1, k1) * fac);
+        R r = P.use_consA ? R(0.5) * (R(ccz(rhoarr, g, i0, j0, k0)) + R(ccz(rhoarr, g, i1, j1, k1))) * ae : ae;
+        if (P.use_turb) r += R(0.5) * (ccz(mut, g, i0, j0, k0) * fac + ccz(mut, g, i1, j1, k1) * fac);
         return r;
     };
-    double fxl = -rA(i, j, k, im, j, k) * (ph(i, j, k) - ph(im, j, k)) * g.dxi * 1.0;
-    double fxh = -rA(ip, j, k, i, j, k) * (ph(ip, j, k) - ph(i, j, k)) * g.dxi * 1.0;
-    double fyl = -rA(i, j, k, i, jm, k) * (ph(i, j, k) - ph(i, jm, k)) * g.dyi * 1.0;
-    double fyh = -rA(i, jp, k, i, j, k) * (ph(i, jp, k) - ph(i, j, k)) * g.dyi * 1.0;
-    double fzl = -rA(i, j, k, i, j, k - 1) * (ph(i, j, k) - ph(i, j, k - 1)) * g.dzi;
-    double fzh = -rA(i, j, k + 1, i, j, k) * (ph(i, j, k + 1) - ph(i, j, k)) * g.dzi;
-    return (fxh - fxl) * g.dxi * 1.0 + (fyh - fyl) * g.dyi * 1.0 + (fzh - fzl) * g.dzi;
+    R fxl = -rA(i, j, k, im, j, k) * (ph(i, j, k) - ph(im, j, k)) * dxi * R(1);
+    R fxh = -rA(ip, j, k, i, j, k) * (ph(ip, j, k) - ph(i, j, k)) * dxi * R(1);
+    R fyl = -rA(i, j, k, i, jm, k) * (ph(i, j, k) - ph(i, jm, k)) * dyi * R(1);
+    R fyh = -rA(i, jp, k, i, j, k) * (ph(i, jp, k) - ph(i, j, k)) * dyi * R(1);
+    R fzl = -rA(i, j, k, i, j, k - 1) * (ph(i, j, k) - ph(i, j, k - 1)) * dzi;
+    R fzh = -rA(i, j, k + 1, i, j, k) * (ph(i, j, k + 1) - ph(i, j, k)) * dzi;
+    return (fxh - fxl) * dxi * R(1) + (fyh - fyl) * dyi * R(1) + (fzh - fzl) * dzi;
 }
 
 // Horizontal plane averages of rho, theta, qv, qc, qp for buoyancy type 2
-// (SourceTerms/ERF_make_buoyancy.cpp:212-249): one block per level.
-__global__ void k_plane_avg(Params P, const double* __restrict__ cons, const double* __restrict__ prim,
+// (SourceTerms/ERF_make_buoyancy.cpp:212-249): one block per level, FP64 sums.
+template <class R>
+__global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* __restrict__ prim,
                             double* __restrict__ avg) {
     const Geo& g = P.g;
     int k = blockIdx.x;
@@ -266,10 +273,10 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const dou
     for (int64_t t = threadIdx.x; t < g.sk; t += blockDim.x) {
         int64_t c = g.sk * k + t;
         acc[0] += cons[c] * denom;
-        acc[1] += prim[c] * denom;
-        if (nq >= 1) acc[2] += prim[4 * N + c] * denom;
-        if (nq >= 2) acc[3] += prim[5 * N + c] * denom;
-        if (nq >= 3) acc[4] += prim[6 * N + c] * denom;
+        acc[1] += double(prim[c]) * denom;
+        if (nq >= 1) acc[2] += double(prim[4 * N + c]) * denom;
+        if (nq >= 2) acc[3] += double(prim[5 * N + c]) * denom;
+        if (nq >= 3) acc[4] += double(prim[6 * N + c]) * denom;
     }
     __shared__ double sh[5][256];
     for (int q = 0; q < 5; ++q) sh[q][threadIdx.x] = acc[q];
@@ -283,40 +290,37 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const dou
         for (int q = 0; q < 5; ++q) avg[q * g.nz + k] = sh[q][0];
 }
 
-// Momentum flux of component `phi` (a face velocity) through a face, with the
-// interpolant selected at run time (ERF_AdvectionSrcForMom_N.H:17-274).
-template <int T = -1>
-__device__ __forceinline__ double gatherx_interp(const Geo& g, const double* f, int type, double upw, double frac,
-                                                 int i, int j, int k) {
-    double s[6];
+// Momentum flux helpers: interpolated face velocity (FP64 state) in R
+// (ERF_AdvectionSrcForMom_N.H:17-274).
+template <int T, class R>
+__device__ __forceinline__ R gatherx_interp(const Geo& g, const double* f, int type, R upw, R frac, int i, int j, int k) {
+    R s[6];
     const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? __ldg(f + cidx(g, wrap(i + off, g.nx), j, k)) : 0.0;
+        s[m] = (off >= -w && off <= w - 1) ? R(__ldg(f + cidx(g, wrap(i + off, g.nx), j, k))) : R(0);
     }
-    return interp_of<T>(type, s, upw, frac);
+    return interp_of<T, R>(type, s, upw, frac);
 }
-template <int T = -1>
-__device__ __forceinline__ double gathery_interp(const Geo& g, const double* f, int type, double upw, double frac,
-                                                 int i, int j, int k) {
-    double s[6];
+template <int T, class R>
+__device__ __forceinline__ R gathery_interp(const Geo& g, const double* f, int type, R upw, R frac, int i, int j, int k) {
+    R s[6];
     const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? __ldg(f + cidx(g, i, wrap(j + off, g.ny), k)) : 0.0;
+        s[m] = (off >= -w && off <= w - 1) ? R(__ldg(f + cidx(g, i, wrap(j + off, g.ny), k))) : R(0);
     }
-    return interp_of<T>(type, s, upw, frac);
+    return interp_of<T, R>(type, s, upw, frac);
 }
-template <int T = -1>
-__device__ __forceinline__ double gatherz_tang(const Geo& g, const double* f, int type, double upw, double frac,
-                                               int i, int j, int k) {
-    double s[6];
+template <int T, class R>
+__device__ __forceinline__ R gatherz_tang(const Geo& g, const double* f, int type, R upw, R frac, int i, int j, int k) {
+    R s[6];
     const int w = width_of<T>(type);
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? tang(f, g, i, j, k + off) : 0.0;
+        s[m] = (off >= -w && off <= w - 1) ? R(tang(f, g, i, j, k + off)) : R(0);
     }
-    return interp_of<T>(type, s, upw, frac);
+    return interp_of<T, R>(type, s, upw, frac);
 }
 
 // ---------------------------------------------------------------------------
@@ -324,25 +328,29 @@ __device__ __forceinline__ double gatherz_tang(const Geo& g, const double* f, in
 // d(rho theta) and its forward extrapolation, explicit U'' / V'' update and
 // the average-momentum accumulation.  For substeps after the first, the
 // previous momenta are first passed through the momentum->velocity->momentum
-// round trip of apply_bcs (ERF_TI_fast_rhs_fun.H:183-189).
+// round trip of apply_bcs (ERF_TI_fast_rhs_fun.H:183-189).  The increments
+// are perturbations about the stage state, formed in FP64 and carried in R;
+// the new momenta are accumulated in FP64.
 // ---------------------------------------------------------------------------
-__global__ void k_fast_h(Params P, int step, int nrk, double dtau, double facinv, StateBuf Sprev, int prev_rt,
-                         StateBuf Sst, StageAux A, const double* __restrict__ Fmx, const double* __restrict__ Fmy,
-                         const double* __restrict__ lag_in, double* __restrict__ lag_out, double* __restrict__ avx,
-                         double* __restrict__ avy, double* __restrict__ outx, double* __restrict__ outy) {
+template <class R>
+__global__ void k_fast_h(Params P, int step, int nrk, double dtau_d, double facinv, StateBuf Sprev, int prev_rt,
+                         StateBuf Sst, StageAux<R> A, const R* __restrict__ Fmx, const R* __restrict__ Fmy,
+                         const R* __restrict__ lag_in, R* __restrict__ lag_out, R* __restrict__ avx,
+                         R* __restrict__ avy, double* __restrict__ outx, double* __restrict__ outy) {
     const Geo& g = P.g;
     int i, j, k;
     if (!cell_coords(g, i, j, k)) return;
     const int64_t N = g.ncell;
+    const R dtau = R(dtau_d);
     int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
     int64_t c = cidx(g, i, j, k), cxm = cidx(g, im, j, k), cym = cidx(g, i, jm, k);
-    const double beta_d = 0.1;
+    const R beta_d = R(0.1);
     auto extrap = [&](int64_t cc) {
-        double drt = Sprev.cons[N + cc] - Sst.cons[N + cc];
+        R drt = R(Sprev.cons[N + cc] - Sst.cons[N + cc]);
         if (step == 0) return drt;
         return drt + beta_d * (drt - lag_in[cc]);
     };
-    double drt_c = Sprev.cons[N + c] - Sst.cons[N + c];
+    R drt_c = R(Sprev.cons[N + c] - Sst.cons[N + c]);
     lag_out[c] = drt_c;
     double px = Sprev.mx[c], py = Sprev.my[c];
     if (prev_rt) {
@@ -353,198 +361,34 @@ __global__ void k_fast_h(Params P, int step, int nrk, double dtau, double facinv
         double vt = (py * 2.0) / rs;
         py = (vt * 0.5) * rs;
     }
-    double ndx, ndy;
+    R ndx, ndy;
     if (nrk == 0 && step == 0) {
-        ndx = px - Sst.mx[c] + dtau * Fmx[c];
-        ndy = py - Sst.my[c] + dtau * Fmy[c];
+        ndx = R(px - Sst.mx[c]) + dtau * Fmx[c];
+        ndy = R(py - Sst.my[c]) + dtau * Fmy[c];
     } else {
-        double ec = extrap(c);
-        double gpx = (ec - extrap(cxm)) * g.dxi;
-        gpx *= 1.0;
-        double gpy = (ec - extrap(cym)) * g.dyi;
-        gpy *= 1.0;
+        R ec = extrap(c);
+        R gpx = (ec - extrap(cxm)) * R(g.dxi);
+        gpx *= R(1);
+        R gpy = (ec - extrap(cym)) * R(g.dyi);
+        gpy *= R(1);
         if (P.moist) {
-            const double* pr = A.prim;
-            double qx = 0.5 * (pr[4 * N + c] + pr[4 * N + cxm] + pr[5 * N + c] + pr[5 * N + cxm]);
-            double qy = 0.5 * (pr[4 * N + c] + pr[4 * N + cym] + pr[5 * N + c] + pr[5 * N + cym]);
-            gpx /= (1.0 + qx);
-            gpy /= (1.0 + qy);
+            const R* pr = A.prim;
+            R qx = R(0.5) * (pr[4 * N + c] + pr[4 * N + cxm] + pr[5 * N + c] + pr[5 * N + cxm]);
+            R qy = R(0.5) * (pr[4 * N + c] + pr[4 * N + cym] + pr[5 * N + c] + pr[5 * N + cym]);
+            gpx /= (R(1) + qx);
+            gpy /= (R(1) + qy);
         }
-        double pix = 0.5 * (A.pi[cxm] + A.pi[c]);
-        double piy = 0.5 * (A.pi[cym] + A.pi[c]);
-        double fx = -Gamma_ * R_d * pix * gpx;
-        double fy = -Gamma_ * R_d * piy * gpy;
-        ndx = px - Sst.mx[c] + dtau * fx + dtau * Fmx[c];
-        ndy = py - Sst.my[c] + dtau * fy + dtau * Fmy[c];
+        R pix = R(0.5) * (A.pi[cxm] + A.pi[c]);
+        R piy = R(0.5) * (A.pi[cym] + A.pi[c]);
+        R fx = R(-Gamma_ * R_d) * pix * gpx;
+        R fy = R(-Gamma_ * R_d) * piy * gpy;
+        ndx = R(px - Sst.mx[c]) + dtau * fx + dtau * Fmx[c];
+        ndy = R(py - Sst.my[c]) + dtau * fy + dtau * Fmy[c];
     }
-    avx[c] += facinv * ndx;
-    avy[c] += facinv * ndy;
-    outx[c] = Sst.mx[c] + ndx;
-    outy[c] = Sst.my[c] + ndy;
-}
-
-// ---------------------------------------------------------------------------
-// Acoustic substep, vertical part: one thread per column.  Fuses
-//   * make_fast_coeffs (ERF_make_fast_coeffs.cpp:160-290): P, Q, A, B, C and
-//     the Thomas forward elimination of B, evaluated from the stage state
-//     (they are constant over a stage, so recomputing them per substep
-//     reproduces the stored values);
-//   * the horizontal rho / rho*theta fluxes from the new U'', V''
-//     (ERF_fast_rhs_N.cpp:328-357);
-//   * the right-hand side of the implicit w system (:374-432);
-//   * the tridiagonal solve (:437-453);
-//   * vertical fluxes, average z-momentum and the rho, rho*theta update
-//     (:518-592).
-// Scratch (per column, face/cell layout): soln, C/B', and the horizontal
-// parts of temp_rhs.
-// ---------------------------------------------------------------------------
-__global__ void k_fast_col(Params P, int step, double dtau, double facinv, double D, double beta_1, double beta_2,
-                           StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux A, const double* __restrict__ Fcons,
-                           const double* __restrict__ Fmz, const double* __restrict__ newx,
-                           const double* __restrict__ newy, double* __restrict__ avz, double* __restrict__ out_cons,
-                           double* __restrict__ out_mz, double* __restrict__ sc_soln, double* __restrict__ sc_cb,
-                           double* __restrict__ sc_tr0, double* __restrict__ sc_tr1) {
-    const Geo& g = P.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.nx || j >= g.ny) return;
-    (void)step;
-    const int64_t N = g.ncell;
-    const int nz = g.nz;
-    int ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny), im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
-    const double* th = A.prim;
-    const double halfg = P.halfg;
-    const double dzi = g.dzi;
-    auto thz = [&](int k) { return th[cidx(g, i, j, clampk(k, nz))]; };
-    // horizontal part of temp_rhs for cell k
-    auto trh = [&](int k, double& t0, double& t1) {
-        int64_t c = cidx(g, i, j, k);
-        double xl = (newx[c] - Sst.mx[c]) / 1.0;
-        double xh = (newx[cidx(g, ip, j, k)] - Sst.mx[cidx(g, ip, j, k)]) / 1.0;
-        double yl = (newy[c] - Sst.my[c]) / 1.0;
-        double yh = (newy[cidx(g, i, jp, k)] - Sst.my[cidx(g, i, jp, k)]) / 1.0;
-        double mfsq = 1.0;
-        double tc = th[c];
-        t0 = (xh - xl) * g.dxi * mfsq + (yh - yl) * g.dyi * mfsq;
-        t1 = ((xh * (tc + th[cidx(g, ip, j, k)]) - xl * (tc + th[cidx(g, im, j, k)])) * g.dxi * mfsq +
-              (yh * (tc + th[cidx(g, i, jp, k)]) - yl * (tc + th[cidx(g, i, jm, k)])) * g.dyi * mfsq) * 0.5;
-    };
-    // previous z-momentum at face k (with the apply_bcs round trip)
-    auto prev_mz = [&](int k) {
-        int64_t f = cidx(g, i, j, k);
-        double m = Sprev.mz[f];
-        if (prev_rt) {
-            if (k == 0 || k == nz) return 0.0;
-            double rs = Sprev.cons[f] + Sprev.cons[f - g.sk];
-            double wt = (m * 2.0) / rs;
-            m = (wt * 0.5) * rs;
-        }
-        return m;
-    };
-    auto qcell = [&](int k) {
-        int64_t c = cidx(g, i, j, k);
-        return P.moist ? (th[4 * N + c] + th[5 * N + c]) : 0.0;
-    };
-    (void)qcell;
-
-    // ---- forward sweep over faces
-    double Om = prev_mz(0) - Sst.mz[cidx(g, i, j, 0)];  // Omega at face k-1 (starts as face 0)
-    double Ok = 0.0;
-    double soln_prev, bet, Cprev;
-    {
-        int64_t f0 = cidx(g, i, j, 0);
-        double rhs0 = prev_mz(0) - Sst.mz[f0] + dtau * Fmz[f0];
-        soln_prev = rhs0 * 1.0;
-        sc_soln[f0] = soln_prev;
-        sc_cb[f0] = 0.0 * 1.0;
-        bet = 1.0;
-        Cprev = 0.0;
-    }
-    // rolling cell data for cells k-1 and k
-    double tr0_lo, tr1_lo;
-    trh(0, tr0_lo, tr1_lo);
-    sc_tr0[cidx(g, i, j, 0)] = tr0_lo;
-    sc_tr1[cidx(g, i, j, 0)] = tr1_lo;
-    Ok = prev_mz(1) - Sst.mz[cidx(g, i, j, 1)];
-    for (int k = 1; k <= nz - 1; ++k) {
-        int64_t c = cidx(g, i, j, k), cm = c - g.sk;
-        double tr0_hi, tr1_hi;
-        trh(k, tr0_hi, tr1_hi);
-        sc_tr0[c] = tr0_hi;
-        sc_tr1[c] = tr1_hi;
-        double Okp1 = prev_mz(k + 1) - Sst.mz[c + g.sk];
-        // coefficients (make_fast_coeffs, no terrain)
-        double pi_c = 0.5 * (A.pi[cm] + A.pi[c]);
-        double cP = -Gamma_ * R_d * dzi + halfg * R_d * P.r0[k + 1] / (P.c_v * P.pi0[k + 1] * Sst.cons[N + c]);
-        cP *= pi_c;
-        double cQ = Gamma_ * R_d * dzi + halfg * R_d * P.r0[k] / (P.c_v * P.pi0[k] * Sst.cons[N + cm]);
-        cQ *= pi_c;
-        if (P.moist) {
-            double q = 0.5 * (th[4 * N + c] + th[4 * N + cm] + th[5 * N + c] + th[5 * N + cm]);
-            cP /= (1.0 + q);
-            cQ /= (1.0 + q);
-        }
-        double tlo = 0.5 * (thz(k - 2) + thz(k - 1));
-        double tmid = 0.5 * (thz(k - 1) + thz(k));
-        double thi = 0.5 * (thz(k) + thz(k + 1));
-        double Acoef = D * (halfg - cQ * tlo);
-        double Ccoef = D * (-halfg + cP * thi);
-        double Bcoef = 1.0 + D * (cQ - cP) * tmid;
-        // right-hand side
-        double drt_k = Sprev.cons[N + c] - Sst.cons[N + c];
-        double drt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
-        double odk = Sprev.cons[c] - Sst.cons[c];
-        double odkm = Sprev.cons[cm] - Sst.cons[cm];
-        double R0 = cP * drt_k + cQ * drt_km - halfg * (odk + odkm);
-        double R1 = halfg * (-Fcons[c] - Fcons[cm] + tr0_hi + tr0_lo) +
-                    (cP * (Fcons[N + c] - tr1_hi) + cQ * (Fcons[N + cm] - tr1_lo));
-        R1 += beta_1 * dzi * ((Okp1 - Om) * halfg - (Okp1 * thi - Ok * tmid) * cP - (Ok * tmid - Om * tlo) * cQ);
-        double rhs = Ok + dtau * (Fmz[c] + R0 + dtau * beta_2 * R1);
-        // Thomas forward elimination
-        double gam = Cprev / bet;
-        bet = Bcoef - Acoef * gam;
-        double invB = 1.0 / bet;
-        double sol = (rhs - Acoef * soln_prev) * invB;
-        sc_soln[c] = sol;
-        sc_cb[c] = Ccoef * invB;
-        if (!(fabs(bet) > 1e-300)) atomicOr(P.status, ST_BADSTATE);
-        soln_prev = sol;
-        Cprev = Ccoef;
-        Om = Ok;
-        Ok = Okp1;
-        tr0_lo = tr0_hi;
-        tr1_lo = tr1_hi;
-    }
-    // top face (A = 0, B = 1, C = 0; B' = 1 is not inverted by the reference)
-    int64_t ftop = cidx(g, i, j, nz);
-    double rhs_top = prev_mz(nz) - Sst.mz[ftop] + dtau * Fmz[ftop];
-    double gam = Cprev / bet;
-    double bet_top = 1.0 - 0.0 * gam;
-    double sol_top = (rhs_top - 0.0 * soln_prev) * bet_top;
-    // ---- back substitution and cell updates, top to bottom
-    double drw_hi = prev_mz(nz) - Sst.mz[ftop];
-    out_mz[ftop] = Sst.mz[ftop] + sol_top;
-    double sol_hi = sol_top;
-    for (int k = nz - 1; k >= 0; --k) {
-        int64_t c = cidx(g, i, j, k);
-        double sol = sc_soln[c];
-        sol -= sc_cb[c] * sol_hi;
-        double pmz = prev_mz(k);
-        double drw_lo = pmz - Sst.mz[c];
-        out_mz[c] = Sst.mz[c] + sol;
-        double zl = beta_2 * sol + beta_1 * drw_lo;
-        double zh = beta_2 * sol_hi + beta_1 * drw_hi;
-        avz[c] += facinv * zl / (1.0 * 1.0);
-        if (k == nz - 1) avz[c + g.sk] += facinv * zh / (1.0 * 1.0);
-        double tc = th[c];
-        double t0 = sc_tr0[c] + dzi * (zh - zl);
-        double t1 = sc_tr1[c] + 0.5 * dzi * (zh * (tc + thz(k + 1)) - zl * (tc + thz(k - 1)));
-        double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
-        out_cons[c] = pr + dtau * (Fcons[c] - t0);
-        out_cons[N + c] = prt + dtau * (Fcons[N + c] - t1);
-        sol_hi = sol;
-        drw_hi = drw_lo;
-    }
+    avx[c] += R(facinv) * ndx;
+    avy[c] += R(facinv) * ndy;
+    outx[c] = Sst.mx[c] + double(ndx);
+    outy[c] = Sst.my[c] + double(ndy);
 }
 
 // ---------------------------------------------------------------------------
@@ -747,9 +591,6 @@ __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const doubl
     }
 }
 
-}  // namespace erfb
-
-namespace erfb {
 
 // ---------------------------------------------------------------------------
 // Tile layout shared by the two vertical kernels below: a block owns TX
@@ -774,62 +615,63 @@ struct Tile {
 // the walls, then the Thomas forward elimination of B.  Stored per face:
 // A, 1/B' (B' at the wall rows, which the reference leaves uninverted),
 // C/B', P, Q.  Levels are computed in parallel; the B' recurrence runs in one
-// warp from shared memory.
+// warp from shared memory.  P and Q use the FP64 base and stage state.
 // ---------------------------------------------------------------------------
-__global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double* __restrict__ cA,
-                            double* __restrict__ cInvB, double* __restrict__ cCB, double* __restrict__ cP,
-                            double* __restrict__ cQ) {
-    extern __shared__ double sm[];
+template <class R>
+__global__ void k_fast_coef(Params P, double D_d, StateBuf Sst, StageAux<R> A, R* __restrict__ cA,
+                            R* __restrict__ cInvB, R* __restrict__ cCB, R* __restrict__ cP, R* __restrict__ cQ) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R* sm = reinterpret_cast<R*>(sm_raw);
     const Geo& g = P.g;
     Tile t(g);
     const int nz = g.nz, TX = t.tx;
-    double* sA = sm;
-    double* sB = sA + (nz + 1) * TX;
-    double* sC = sB + (nz + 1) * TX;
+    R* sA = sm;
+    R* sB = sA + (nz + 1) * TX;
+    R* sC = sB + (nz + 1) * TX;
     const int64_t N = g.ncell;
-    const double dzi = g.dzi, halfg = P.halfg;
-    const double* th = A.prim;
+    const R D = R(D_d), halfg = R(P.halfg);
+    const R* th = A.prim;
     if (t.ok) {
         for (int k = 1 + t.w; k <= nz - 1; k += t.nw) {
             int64_t c = cidx(g, t.i, t.j, k), cm = c - g.sk;
-            double pi_c = 0.5 * (A.pi[cm] + A.pi[c]);
-            double P_ = -Gamma_ * R_d * dzi + halfg * R_d * P.r0[k + 1] / (P.c_v * P.pi0[k + 1] * Sst.cons[N + c]);
+            R pi_c = R(0.5) * (A.pi[cm] + A.pi[c]);
+            R P_ = R(-Gamma_ * R_d * g.dzi + P.halfg * R_d * P.r0[k + 1] / (P.c_v * P.pi0[k + 1] * Sst.cons[N + c]));
             P_ *= pi_c;
-            double Q_ = Gamma_ * R_d * dzi + halfg * R_d * P.r0[k] / (P.c_v * P.pi0[k] * Sst.cons[N + cm]);
+            R Q_ = R(Gamma_ * R_d * g.dzi + P.halfg * R_d * P.r0[k] / (P.c_v * P.pi0[k] * Sst.cons[N + cm]));
             Q_ *= pi_c;
             if (P.moist) {
-                double q = 0.5 * (th[4 * N + c] + th[4 * N + cm] + th[5 * N + c] + th[5 * N + cm]);
-                P_ /= (1.0 + q);
-                Q_ /= (1.0 + q);
+                R q = R(0.5) * (th[4 * N + c] + th[4 * N + cm] + th[5 * N + c] + th[5 * N + cm]);
+                P_ /= (R(1) + q);
+                Q_ /= (R(1) + q);
             }
-            double tlo = 0.5 * (th[cidx(g, t.i, t.j, clampk(k - 2, nz))] + th[cm]);
-            double tmid = 0.5 * (th[cm] + th[c]);
-            double thi = 0.5 * (th[c] + th[cidx(g, t.i, t.j, clampk(k + 1, nz))]);
-            double a = D * (halfg - Q_ * tlo);
-            double cc = D * (-halfg + P_ * thi);
-            double b = 1.0 + D * (Q_ - P_) * tmid;
+            R tlo = R(0.5) * (th[cidx(g, t.i, t.j, clampk(k - 2, nz))] + th[cm]);
+            R tmid = R(0.5) * (th[cm] + th[c]);
+            R thi = R(0.5) * (th[c] + th[cidx(g, t.i, t.j, clampk(k + 1, nz))]);
+            R a = D * (halfg - Q_ * tlo);
+            R cc = D * (-halfg + P_ * thi);
+            R b = R(1) + D * (Q_ - P_) * tmid;
             sA[k * TX + t.lane] = a; sB[k * TX + t.lane] = b; sC[k * TX + t.lane] = cc;
             cA[c] = a; cP[c] = P_; cQ[c] = Q_;
         }
         if (t.w == 0) {
             for (int k : {0, nz}) {
-                sA[k * TX + t.lane] = 0.0; sB[k * TX + t.lane] = 1.0; sC[k * TX + t.lane] = 0.0;
+                sA[k * TX + t.lane] = R(0); sB[k * TX + t.lane] = R(1); sC[k * TX + t.lane] = R(0);
                 int64_t f = cidx(g, t.i, t.j, k);
-                cA[f] = 0.0; cP[f] = 0.0; cQ[f] = 0.0;
+                cA[f] = R(0); cP[f] = R(0); cQ[f] = R(0);
             }
         }
     }
     __syncthreads();
     if (t.w == 0 && t.ok) {
-        double bet = sB[t.lane];
+        R bet = sB[t.lane];
         int64_t f0 = cidx(g, t.i, t.j, 0);
         cInvB[f0] = bet;               // B at the bottom row stays uninverted (== 1)
         cCB[f0] = sC[t.lane] * bet;
         for (int k = 1; k <= nz; ++k) {
-            double gam = sC[(k - 1) * TX + t.lane] / bet;
+            R gam = sC[(k - 1) * TX + t.lane] / bet;
             bet = sB[k * TX + t.lane] - sA[k * TX + t.lane] * gam;
-            if (!(fabs(bet) > 1e-300)) atomicOr(P.status, ST_BADSTATE);
-            double inv = (k < nz) ? 1.0 / bet : bet;
+            if (!(fabs(double(bet)) > 1e-300)) atomicOr(P.status, ST_BADSTATE);
+            R inv = (k < nz) ? R(1) / bet : bet;
             int64_t f = cidx(g, t.i, t.j, k);
             cInvB[f] = inv;
             cCB[f] = sC[k * TX + t.lane] * inv;
@@ -846,29 +688,35 @@ __global__ void k_fast_coef(Params P, double D, StateBuf Sst, StageAux A, double
 //            stage's 1/B' and C/B' come from k_fast_coef);
 //   phase 4  vertical fluxes, average z-momentum, rho and rho*theta update.
 // All reads of the previous state happen in phases 1-2, before any write,
-// because the previous and new states may be the same buffers.
+// because the previous and new states may be the same buffers.  The W''
+// system is solved in R; rho, rho*theta and the z-momentum are accumulated
+// in FP64.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
-                            int prev_rt, StateBuf Sst, StageAux A, const double* __restrict__ Fcons,
-                            const double* __restrict__ Fmz, const double* __restrict__ newx,
-                            const double* __restrict__ newy, const double* __restrict__ cA,
-                            const double* __restrict__ cInvB, const double* __restrict__ cCB,
-                            const double* __restrict__ cP, const double* __restrict__ cQ, double* __restrict__ avz,
-                            double* out_cons, double* out_mz) {
-    extern __shared__ double sm[];
+template <class R>
+__global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, double facinv, double beta_1d,
+                                                    double beta_2d, StateBuf Sprev, int prev_rt, StateBuf Sst,
+                                                    StageAux<R> A, const R* __restrict__ Fcons,
+                                                    const R* __restrict__ Fmz, const double* __restrict__ newx,
+                                                    const double* __restrict__ newy, const R* __restrict__ cA,
+                                                    const R* __restrict__ cInvB, const R* __restrict__ cCB,
+                                                    const R* __restrict__ cP, const R* __restrict__ cQ,
+                                                    R* __restrict__ avz, double* out_cons, double* out_mz) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R* sm = reinterpret_cast<R*>(sm_raw);
     const Geo& g = P.g;
     Tile t(g);
     const int nz = g.nz, TX = t.tx, L = t.lane;
-    double* sT0 = sm;
-    double* sT1 = sT0 + nz * TX;
-    double* sR = sT1 + nz * TX;
-    double* sD = sR + (nz + 1) * TX;
-    double* sA = sD + (nz + 1) * TX;
-    double* sI = sA + (nz + 1) * TX;
-    double* sCB = sI + (nz + 1) * TX;
+    R* sT0 = sm;
+    R* sT1 = sT0 + nz * TX;
+    R* sR = sT1 + nz * TX;
+    R* sD = sR + (nz + 1) * TX;
+    R* sA = sD + (nz + 1) * TX;
+    R* sI = sA + (nz + 1) * TX;
+    R* sCB = sI + (nz + 1) * TX;
     const int64_t N = g.ncell;
-    const double dzi = g.dzi, halfg = P.halfg;
-    const double* th = A.prim;
+    const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi), halfg = R(P.halfg);
+    const R dtau = R(dtau_d), beta_1 = R(beta_1d), beta_2 = R(beta_2d);
+    const R* th = A.prim;
     const int i = t.i, j = t.j;
     int ip = 0, im = 0, jp = 0, jm = 0;
     if (t.ok) { ip = wrap(i + 1, g.nx); im = wrap(i - 1, g.nx); jp = wrap(j + 1, g.ny); jm = wrap(j - 1, g.ny); }
@@ -888,15 +736,15 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau, doubl
     if (t.ok) {
         for (int k = t.w; k < nz; k += t.nw) {
             int64_t c = cidx(g, i, j, k);
-            double xl = (newx[c] - Sst.mx[c]) / 1.0;
-            double xh = (newx[cidx(g, ip, j, k)] - Sst.mx[cidx(g, ip, j, k)]) / 1.0;
-            double yl = (newy[c] - Sst.my[c]) / 1.0;
-            double yh = (newy[cidx(g, i, jp, k)] - Sst.my[cidx(g, i, jp, k)]) / 1.0;
-            double mfsq = 1.0;
-            double tc = th[c];
-            sT0[k * TX + L] = (xh - xl) * g.dxi * mfsq + (yh - yl) * g.dyi * mfsq;
-            sT1[k * TX + L] = ((xh * (tc + th[cidx(g, ip, j, k)]) - xl * (tc + th[cidx(g, im, j, k)])) * g.dxi * mfsq +
-                               (yh * (tc + th[cidx(g, i, jp, k)]) - yl * (tc + th[cidx(g, i, jm, k)])) * g.dyi * mfsq) * 0.5;
+            R xl = R(newx[c] - Sst.mx[c]) / R(1);
+            R xh = R(newx[cidx(g, ip, j, k)] - Sst.mx[cidx(g, ip, j, k)]) / R(1);
+            R yl = R(newy[c] - Sst.my[c]) / R(1);
+            R yh = R(newy[cidx(g, i, jp, k)] - Sst.my[cidx(g, i, jp, k)]) / R(1);
+            R mfsq = R(1);
+            R tc = th[c];
+            sT0[k * TX + L] = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
+            sT1[k * TX + L] = ((xh * (tc + th[cidx(g, ip, j, k)]) - xl * (tc + th[cidx(g, im, j, k)])) * dxi * mfsq +
+                               (yh * (tc + th[cidx(g, i, jp, k)]) - yl * (tc + th[cidx(g, i, jm, k)])) * dyi * mfsq) * R(0.5);
         }
     }
     __syncthreads();
@@ -904,29 +752,29 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau, doubl
     if (t.ok) {
         for (int k = t.w; k <= nz; k += t.nw) {
             int64_t f = cidx(g, i, j, k);
-            double Ok = prev_mz(k) - Sst.mz[f];
+            R Ok = R(prev_mz(k) - Sst.mz[f]);
             sD[k * TX + L] = Ok;
             sA[k * TX + L] = cA[f];
             sI[k * TX + L] = cInvB[f];
             sCB[k * TX + L] = cCB[f];
-            double rhs;
+            R rhs;
             if (k == 0 || k == nz) {
                 rhs = Ok + dtau * Fmz[f];
             } else {
                 int64_t cm = f - g.sk;
-                double Okp1 = prev_mz(k + 1) - Sst.mz[f + g.sk];
-                double Okm1 = prev_mz(k - 1) - Sst.mz[cm];
-                double cPk = cP[f], cQk = cQ[f];
-                double tlo = 0.5 * (thz(k - 2) + thz(k - 1));
-                double tmid = 0.5 * (thz(k - 1) + thz(k));
-                double thi = 0.5 * (thz(k) + thz(k + 1));
-                double drt_k = Sprev.cons[N + f] - Sst.cons[N + f];
-                double drt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
-                double odk = Sprev.cons[f] - Sst.cons[f];
-                double odkm = Sprev.cons[cm] - Sst.cons[cm];
-                double R0 = cPk * drt_k + cQk * drt_km - halfg * (odk + odkm);
-                double R1 = halfg * (-Fcons[f] - Fcons[cm] + sT0[k * TX + L] + sT0[(k - 1) * TX + L]) +
-                            (cPk * (Fcons[N + f] - sT1[k * TX + L]) + cQk * (Fcons[N + cm] - sT1[(k - 1) * TX + L]));
+                R Okp1 = R(prev_mz(k + 1) - Sst.mz[f + g.sk]);
+                R Okm1 = R(prev_mz(k - 1) - Sst.mz[cm]);
+                R cPk = cP[f], cQk = cQ[f];
+                R tlo = R(0.5) * (thz(k - 2) + thz(k - 1));
+                R tmid = R(0.5) * (thz(k - 1) + thz(k));
+                R thi = R(0.5) * (thz(k) + thz(k + 1));
+                R drt_k = R(Sprev.cons[N + f] - Sst.cons[N + f]);
+                R drt_km = R(Sprev.cons[N + cm] - Sst.cons[N + cm]);
+                R odk = R(Sprev.cons[f] - Sst.cons[f]);
+                R odkm = R(Sprev.cons[cm] - Sst.cons[cm]);
+                R R0 = cPk * drt_k + cQk * drt_km - halfg * (odk + odkm);
+                R R1 = halfg * (-Fcons[f] - Fcons[cm] + sT0[k * TX + L] + sT0[(k - 1) * TX + L]) +
+                       (cPk * (Fcons[N + f] - sT1[k * TX + L]) + cQk * (Fcons[N + cm] - sT1[(k - 1) * TX + L]));
                 R1 += beta_1 * dzi * ((Okp1 - Okm1) * halfg - (Okp1 * thi - Ok * tmid) * cPk - (Ok * tmid - Okm1 * tlo) * cQk);
                 rhs = Ok + dtau * (Fmz[f] + R0 + dtau * beta_2 * R1);
             }
@@ -936,7 +784,7 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau, doubl
     __syncthreads();
     // ---- phase 3: tridiagonal solve, one warp
     if (t.w == 0 && t.ok) {
-        double s = sR[L] * sI[L];
+        R s = sR[L] * sI[L];
         sR[L] = s;
         for (int k = 1; k <= nz; ++k) {
             s = (sR[k * TX + L] - sA[k * TX + L] * s) * sI[k * TX + L];
@@ -952,20 +800,20 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau, doubl
     if (t.ok) {
         for (int k = t.w; k < nz; k += t.nw) {
             int64_t c = cidx(g, i, j, k);
-            double sol = sR[k * TX + L], sol_hi = sR[(k + 1) * TX + L];
-            double zl = beta_2 * sol + beta_1 * sD[k * TX + L];
-            double zh = beta_2 * sol_hi + beta_1 * sD[(k + 1) * TX + L];
-            avz[c] += facinv * zl / (1.0 * 1.0);
-            if (k == nz - 1) avz[c + g.sk] += facinv * zh / (1.0 * 1.0);
-            double tc = th[c];
-            double t0 = sT0[k * TX + L] + dzi * (zh - zl);
-            double t1 = sT1[k * TX + L] + 0.5 * dzi * (zh * (tc + thz(k + 1)) - zl * (tc + thz(k - 1)));
+            R sol = sR[k * TX + L], sol_hi = sR[(k + 1) * TX + L];
+            R zl = beta_2 * sol + beta_1 * sD[k * TX + L];
+            R zh = beta_2 * sol_hi + beta_1 * sD[(k + 1) * TX + L];
+            avz[c] += R(facinv) * zl / (R(1) * R(1));
+            if (k == nz - 1) avz[c + g.sk] += R(facinv) * zh / (R(1) * R(1));
+            R tc = th[c];
+            R t0 = sT0[k * TX + L] + dzi * (zh - zl);
+            R t1 = sT1[k * TX + L] + R(0.5) * dzi * (zh * (tc + thz(k + 1)) - zl * (tc + thz(k - 1)));
             double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
-            out_cons[c] = pr + dtau * (Fcons[c] - t0);
-            out_cons[N + c] = prt + dtau * (Fcons[N + c] - t1);
+            out_cons[c] = pr + double(dtau * (Fcons[c] - t0));
+            out_cons[N + c] = prt + double(dtau * (Fcons[N + c] - t1));
             double smz = Sst.mz[c];
-            out_mz[c] = smz + sol;
-            if (k == nz - 1) out_mz[c + g.sk] = Sst.mz[c + g.sk] + sol_hi;
+            out_mz[c] = smz + double(sol);
+            if (k == nz - 1) out_mz[c + g.sk] = Sst.mz[c + g.sk] + double(sol_hi);
         }
     }
 }
@@ -1055,10 +903,6 @@ __global__ void k_kessler_cells(Params P, const double* __restrict__ cin, double
     if (has_qp) cout[7 * N + c] = rho * qp;
 }
 
-}  // namespace erfb
-
-namespace erfb {
-
 // ---------------------------------------------------------------------------
 // Scalar and momentum transport on x-y tiles marching up in k.  A block owns
 // TTX x TTY columns and `kz` consecutive levels.  At each level every thread
@@ -1082,19 +926,20 @@ namespace erfb {
 #define ERFB_MINB_POST 4
 #endif
 
+template <class R>
 struct FluxTile {
-    double fx[TTY][TTX + 1];
-    double fy[TTY + 1][TTX];
+    R fx[TTY][TTX + 1];
+    R fy[TTY + 1][TTX];
 };
 
 // Fluxes of one scalar for cell (i,j,k): x/y into the tile, z through zl/zh
 // (zl is computed only on the block's first level; otherwise it is the
 // carried top flux of the level below).
-template <int TH, int TV>
-__device__ __forceinline__ void tile_put(const Geo& g, FluxTile& t, const double* __restrict__ phi,
-                                         const double* __restrict__ ax, const double* __restrict__ ay,
-                                         const double* __restrict__ az, int th, int tv, double fh, double fv, int i,
-                                         int j, int k, bool first, double& zl, double& zh) {
+template <int TH, int TV, class R, class M>
+__device__ __forceinline__ void tile_put(const Geo& g, FluxTile<R>& t, const R* __restrict__ phi,
+                                         const M* __restrict__ ax, const M* __restrict__ ay,
+                                         const M* __restrict__ az, int th, int tv, R fh, R fv, int i, int j, int k,
+                                         bool first, R& zl, R& zh) {
     const int tx = threadIdx.x, ty = threadIdx.y;
     t.fx[ty][tx] = adv_flux_x<TH>(g, phi, ax, th, fh, i, j, k);
     if (tx == TTX - 1 || i == g.nx - 1) t.fx[ty][tx + 1] = adv_flux_x<TH>(g, phi, ax, th, fh, wrap(i + 1, g.nx), j, k);
@@ -1103,10 +948,11 @@ __device__ __forceinline__ void tile_put(const Geo& g, FluxTile& t, const double
     if (first) zl = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k);
     zh = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k + 1);
 }
-__device__ __forceinline__ double tile_div(const Geo& g, const FluxTile& t, double zl, double zh) {
+template <class R>
+__device__ __forceinline__ R tile_div(const Geo& g, const FluxTile<R>& t, R zl, R zh) {
     const int tx = threadIdx.x, ty = threadIdx.y;
-    return -1.0 * 1.0 * ((t.fx[ty][tx + 1] - t.fx[ty][tx]) * g.dxi + (t.fy[ty + 1][tx] - t.fy[ty][tx]) * g.dyi +
-                         (zh - zl) * g.dzi);
+    return R(-1.0 * 1.0) * ((t.fx[ty][tx + 1] - t.fx[ty][tx]) * R(g.dxi) + (t.fy[ty + 1][tx] - t.fy[ty][tx]) * R(g.dyi) +
+                            (zh - zl) * R(g.dzi));
 }
 
 // ---------------------------------------------------------------------------
@@ -1116,34 +962,34 @@ __device__ __forceinline__ double tile_div(const Geo& g, const FluxTile& t, doub
 // AdvectionSrcForScalars for theta with the dycore scheme
 // (ERF_slow_rhs_pre.cpp:139-142, 469-477), DiffusionSrcForState_N for theta.
 // ---------------------------------------------------------------------------
-template <int TH, int TV>
-__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params P, int kz, StateBuf S, StageAux A,
-                                                         const double* __restrict__ mut, double* __restrict__ Fcons,
-                                                         double* __restrict__ avx, double* __restrict__ avy,
-                                                         double* __restrict__ avz) {
-    __shared__ FluxTile sh;
+template <class R, int TH, int TV>
+__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params P, int kz, StateBuf S, StageAux<R> A,
+                                                                         const R* __restrict__ mut,
+                                                                         R* __restrict__ Fcons, R* __restrict__ avx,
+                                                                         R* __restrict__ avy, R* __restrict__ avz) {
+    __shared__ FluxTile<R> sh;
     const Geo& g = P.g;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
     const bool ok = i < g.nx && j < g.ny;
     const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
-    double zl = 0.0, zh = 0.0;
+    R zl = R(0), zh = R(0);
     for (int k = k0; k < k1; ++k) {
         if (ok)
-            tile_put<TH, TV>(g, sh, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, P.f_dyc_h, P.f_dyc_v, i, j, k,
+            tile_put<TH, TV>(g, sh, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, R(P.f_dyc_h), R(P.f_dyc_v), i, j, k,
                              k == k0, zl, zh);
         __syncthreads();
         if (ok) {
-            double frt = tile_div(g, sh, zl, zh);
+            R frt = tile_div(g, sh, zl, zh);
             zl = zh;
             int64_t c = cidx(g, i, j, k);
-            avx[c] = S.mx[c];
-            avy[c] = S.my[c];
-            avz[c] = S.mz[c];
-            if (k == g.nz - 1) avz[c + g.sk] = S.mz[c + g.sk];
-            Fcons[c] = -1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi +
-                                     (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi + (S.mz[c + g.sk] - S.mz[c]) * g.dzi);
-            if (P.use_diff) frt -= scalar_diff(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
+            avx[c] = R(S.mx[c]);
+            avy[c] = R(S.my[c]);
+            avz[c] = R(S.mz[c]);
+            if (k == g.nz - 1) avz[c + g.sk] = R(S.mz[c + g.sk]);
+            Fcons[c] = R(-1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi +
+                                       (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi + (S.mz[c + g.sk] - S.mz[c]) * g.dzi));
+            if (P.use_diff) frt -= scalar_diff<R>(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
             Fcons[g.ncell + c] = frt;
         }
         __syncthreads();
@@ -1156,21 +1002,23 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
 // ERF_TI_slow_rhs_fun.H:284-288):
 //   * advection (average momenta) and diffusion of the slow scalars
 //     (passive scalar with the dry-scalar scheme; moisture with the moist
-//     scheme), S_new = S_old + slow_dt * RHS, moisture clipped at 0;
+//     scheme), S_new = S_old + slow_dt * RHS (FP64), moisture clipped at 0;
 //   * rho, rho*theta and the momenta copied from the fast solution, with the
 //     momentum/velocity round trips of the two boundary fills;
 //   * the stage velocities, and (unless last) the next stage's primitive
 //     variables, Exner function and p'.
 // ---------------------------------------------------------------------------
 constexpr int MAX_SLOW = 4;  // passive scalar + up to three moisture species
-template <int DH, int DV, int MH, int MV>
-__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, int kz, double slow_dt, StateBuf Sold, StateBuf Sst,
-                                                    StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext,
-                                                    int make_next, const double* __restrict__ mut,
-                                                    const double* __restrict__ avx, const double* __restrict__ avy,
-                                                    const double* __restrict__ avz, double* __restrict__ un,
-                                                    double* __restrict__ vn, double* __restrict__ wn) {
-    __shared__ FluxTile sh[MAX_SLOW];
+template <class R, int DH, int DV, int MH, int MV>
+__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, int kz, double slow_dt, StateBuf Sold,
+                                                                    StateBuf Sst, StateBuf Ssum, StateBuf Snew,
+                                                                    StageAux<R> Acur, StageAux<R> Anext, int make_next,
+                                                                    const R* __restrict__ mut,
+                                                                    const R* __restrict__ avx,
+                                                                    const R* __restrict__ avy,
+                                                                    const R* __restrict__ avz, double* __restrict__ un,
+                                                                    double* __restrict__ vn, double* __restrict__ wn) {
+    __shared__ FluxTile<R> sh[MAX_SLOW];
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
@@ -1178,9 +1026,9 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
     const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
     const int nslow = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
-    double zl[MAX_SLOW], zh[MAX_SLOW];
+    R zl[MAX_SLOW], zh[MAX_SLOW];
 #pragma unroll
-    for (int q = 0; q < MAX_SLOW; ++q) zl[q] = zh[q] = 0.0;
+    for (int q = 0; q < MAX_SLOW; ++q) zl[q] = zh[q] = R(0);
     for (int k = k0; k < k1; ++k) {
         if (ok) {
 #pragma unroll
@@ -1188,10 +1036,10 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
                 if (q >= nslow) break;
                 if (q == 0)
                     tile_put<DH, DV>(g, sh[0], Acur.prim + (int64_t)(ERF_RHOSCALAR_COMP - 1) * N, avx, avy, avz,
-                                     P.dry_h, P.dry_v, P.f_dry_h, P.f_dry_v, i, j, k, k == k0, zl[0], zh[0]);
+                                     P.dry_h, P.dry_v, R(P.f_dry_h), R(P.f_dry_v), i, j, k, k == k0, zl[0], zh[0]);
                 else
                     tile_put<MH, MV>(g, sh[q], Acur.prim + (int64_t)(ERF_RHOQ1_COMP + q - 2) * N, avx, avy, avz,
-                                     P.moi_h, P.moi_v, P.f_moi_h, P.f_moi_v, i, j, k, k == k0, zl[q], zh[q]);
+                                     P.moi_h, P.moi_v, R(P.f_moi_h), R(P.f_moi_v), i, j, k, k == k0, zl[q], zh[q]);
             }
         }
         __syncthreads();
@@ -1201,11 +1049,11 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
             for (int q = 0; q < MAX_SLOW; ++q) {
                 if (q >= nslow) break;
                 int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
-                double r = tile_div(g, sh[q], zl[q], zh[q]);
+                R r = tile_div(g, sh[q], zl[q], zh[q]);
                 zl[q] = zh[q];
                 if (P.use_diff)
-                    r -= scalar_diff(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
-                double v_ = Sold.cons[n * N + c] + slow_dt * r;
+                    r -= scalar_diff<R>(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
+                double v_ = Sold.cons[n * N + c] + slow_dt * double(r);
                 Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 0.0);
             }
             Snew.cons[c] = Ssum.cons[c];
@@ -1237,7 +1085,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
                 Snew.mz[c] = m; wn[c] = w2;
             }
             if (k == g.nz - 1) { Snew.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
-            if (make_next) stage_aux_cell(P, Snew.cons, Anext, c, k);
+            if (make_next) stage_aux_cell<R>(P, Snew.cons, Anext, c, k);
         }
         __syncthreads();
     }
@@ -1246,89 +1094,89 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
 // Momentum fluxes of AdvectionSrcFor{X,Y,Z}Mom_N (ERF_AdvectionSrcForMom_N.H:
 // 17-274).  Each is the flux through the low side of the face's control
 // volume in one direction; the high side is the same function one index up.
-template <int HT>
-__device__ __forceinline__ double xmom_flux_x(const Params& P, const double* ru, const double* u, int i, int j, int k) {
+template <int HT, class R>
+__device__ __forceinline__ R xmom_flux_x(const Params& P, const double* ru, const double* u, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (ru[cidx(g, wrap(i - 1, g.nx), j, k)] + ru[cidx(g, i, j, k)]);
-    return a * gatherx_interp<HT>(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    R a = R(0.5) * (R(ru[cidx(g, wrap(i - 1, g.nx), j, k)]) + R(ru[cidx(g, i, j, k)]));
+    return a * gatherx_interp<HT, R>(g, u, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
 }
-template <int HT>
-__device__ __forceinline__ double xmom_flux_y(const Params& P, const double* rv, const double* u, int i, int j, int k) {
+template <int HT, class R>
+__device__ __forceinline__ R xmom_flux_y(const Params& P, const double* rv, const double* u, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, wrap(i - 1, g.nx), j, k)]);
-    return a * gathery_interp<HT>(g, u, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    R a = R(0.5) * (R(rv[cidx(g, i, j, k)]) + R(rv[cidx(g, wrap(i - 1, g.nx), j, k)]));
+    return a * gathery_interp<HT, R>(g, u, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
 }
-template <int VT>
-__device__ __forceinline__ double xmom_flux_z(const Params& P, const double* rw, const double* u, int i, int j, int k) {
+template <int VT, class R>
+__device__ __forceinline__ R xmom_flux_z(const Params& P, const double* rw, const double* u, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (rw[cidx(g, i, j, k)] + rw[cidx(g, wrap(i - 1, g.nx), j, k)]);
-    return a * gatherz_tang<VT>(g, u, P.dyc_v, a, P.f_dyc_v, i, j, k);
+    R a = R(0.5) * (R(rw[cidx(g, i, j, k)]) + R(rw[cidx(g, wrap(i - 1, g.nx), j, k)]));
+    return a * gatherz_tang<VT, R>(g, u, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
 }
-template <int HT>
-__device__ __forceinline__ double ymom_flux_x(const Params& P, const double* ru, const double* v, int i, int j, int k) {
+template <int HT, class R>
+__device__ __forceinline__ R ymom_flux_x(const Params& P, const double* ru, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (ru[cidx(g, i, j, k)] + ru[cidx(g, i, wrap(j - 1, g.ny), k)]);
-    return a * gatherx_interp<HT>(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    R a = R(0.5) * (R(ru[cidx(g, i, j, k)]) + R(ru[cidx(g, i, wrap(j - 1, g.ny), k)]));
+    return a * gatherx_interp<HT, R>(g, v, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
 }
-template <int HT>
-__device__ __forceinline__ double ymom_flux_y(const Params& P, const double* rv, const double* v, int i, int j, int k) {
+template <int HT, class R>
+__device__ __forceinline__ R ymom_flux_y(const Params& P, const double* rv, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, i, wrap(j - 1, g.ny), k)]);
-    return a * gathery_interp<HT>(g, v, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    R a = R(0.5) * (R(rv[cidx(g, i, j, k)]) + R(rv[cidx(g, i, wrap(j - 1, g.ny), k)]));
+    return a * gathery_interp<HT, R>(g, v, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
 }
-template <int VT>
-__device__ __forceinline__ double ymom_flux_z(const Params& P, const double* rw, const double* v, int i, int j, int k) {
+template <int VT, class R>
+__device__ __forceinline__ R ymom_flux_z(const Params& P, const double* rw, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (rw[cidx(g, i, j, k)] + rw[cidx(g, i, wrap(j - 1, g.ny), k)]);
-    return a * gatherz_tang<VT>(g, v, P.dyc_v, a, P.f_dyc_v, i, j, k);
+    R a = R(0.5) * (R(rw[cidx(g, i, j, k)]) + R(rw[cidx(g, i, wrap(j - 1, g.ny), k)]));
+    return a * gatherz_tang<VT, R>(g, v, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
 }
-template <int HT>
-__device__ __forceinline__ double zmom_flux_x(const Params& P, const double* ru, const double* w, int i, int j, int k) {
+template <int HT, class R>
+__device__ __forceinline__ R zmom_flux_x(const Params& P, const double* ru, const double* w, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (ru[cidx(g, i, j, k)] + ru[cidx(g, i, j, k - 1)]) * 1.0;
-    return a * gatherx_interp<HT>(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    R a = R(0.5) * (R(ru[cidx(g, i, j, k)]) + R(ru[cidx(g, i, j, k - 1)])) * R(1);
+    return a * gatherx_interp<HT, R>(g, w, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
 }
-template <int HT>
-__device__ __forceinline__ double zmom_flux_y(const Params& P, const double* rv, const double* w, int i, int j, int k) {
+template <int HT, class R>
+__device__ __forceinline__ R zmom_flux_y(const Params& P, const double* rv, const double* w, int i, int j, int k) {
     const Geo& g = P.g;
-    double a = 0.5 * (rv[cidx(g, i, j, k)] + rv[cidx(g, i, j, k - 1)]) * 1.0;
-    return a * gathery_interp<HT>(g, w, P.dyc_h, a, P.f_dyc_h, i, j, k);
+    R a = R(0.5) * (R(rv[cidx(g, i, j, k)]) + R(rv[cidx(g, i, j, k - 1)])) * R(1);
+    return a * gathery_interp<HT, R>(g, w, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
 }
 // Vertical flux of w between faces kk-1 and kk (the "lo" flux of face kk),
 // with the order reduction next to the walls (ERF_AdvectionSrcForMom_N.H:
 // 220-265); for kk == nz it is the "hi" flux of the top interior face,
 // which the reference takes centred.
-template <int VT>
-__device__ __forceinline__ double zmom_flux_z(const Params& P, const double* rw, const double* w, int i, int j, int kk) {
+template <int VT, class R>
+__device__ __forceinline__ R zmom_flux_z(const Params& P, const double* rw, const double* w, int i, int j, int kk) {
     const Geo& g = P.g;
     const int vt = P.dyc_v, lo_z_face = 0, hi_z_face = g.nz;
-    const double vf = P.f_dyc_v;
-    auto wz = [&](int q) { return __ldg(w + cidx(g, i, j, q)); };
-    auto all = [&](int q, double upw, double frac, int type) {
-        double sv[6];
+    const R vf = R(P.f_dyc_v);
+    auto wz = [&](int q) { return R(__ldg(w + cidx(g, i, j, q))); };
+    auto all = [&](int q, R upw, R frac, int type) {
+        R sv[6];
         bool wide = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH);
-        sv[0] = wide ? wz(q - 3) : 0.0;
-        sv[1] = (type == ERF_ADV_CENTERED_2ND) ? 0.0 : wz(q - 2);
+        sv[0] = wide ? wz(q - 3) : R(0);
+        sv[1] = (type == ERF_ADV_CENTERED_2ND) ? R(0) : wz(q - 2);
         sv[2] = wz(q - 1);
         sv[3] = wz(q);
-        sv[4] = (type == ERF_ADV_CENTERED_2ND) ? 0.0 : wz(q + 1);
-        sv[5] = wide ? wz(q + 2) : 0.0;
-        return interp_all(type, sv, upw, frac);
+        sv[4] = (type == ERF_ADV_CENTERED_2ND) ? R(0) : wz(q + 1);
+        sv[5] = wide ? wz(q + 2) : R(0);
+        return interp_all<R>(type, sv, upw, frac);
     };
-    auto normal = [&](int q, double upw) {
-        double sv[6];
+    auto normal = [&](int q, R upw) {
+        R sv[6];
         const int wd = width_of<VT>(vt);
         for (int m = 0; m < 6; ++m) {
             int off = m - 3;
-            sv[m] = (off >= -wd && off <= wd - 1) ? wz(q + off) : 0.0;
+            sv[m] = (off >= -wd && off <= wd - 1) ? wz(q + off) : R(0);
         }
-        return interp_of<VT>(vt, sv, upw, vf);
+        return interp_of<VT, R>(vt, sv, upw, vf);
     };
-    double a = 0.5 * (rw[cidx(g, i, j, kk)] + rw[cidx(g, i, j, kk - 1)]);
-    double iv;
-    if (kk == hi_z_face || kk == lo_z_face + 1) iv = all(kk, a, 0, ERF_ADV_CENTERED_2ND);
+    R a = R(0.5) * (R(rw[cidx(g, i, j, kk)]) + R(rw[cidx(g, i, j, kk - 1)]));
+    R iv;
+    if (kk == hi_z_face || kk == lo_z_face + 1) iv = all(kk, a, R(0), ERF_ADV_CENTERED_2ND);
     else if (kk == lo_z_face + 2 || kk == hi_z_face - 1) {
-        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) iv = all(kk, a, 0, ERF_ADV_CENTERED_4TH);
+        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) iv = all(kk, a, R(0), ERF_ADV_CENTERED_4TH);
         else iv = all(kk, a, vf, vt);
     } else iv = normal(kk, a);
     return a * iv;
@@ -1340,17 +1188,23 @@ __device__ __forceinline__ double zmom_flux_z(const Params& P, const double* rw,
 // pressure gradient of p', buoyancy / Coriolis / geostrophic sources
 // (make_mom_sources, make_buoyancy).  Same tiles as the scalar transport;
 // the three momenta's x/y fluxes of a level are staged before one barrier.
+// Buoyancy is evaluated in FP64 from the FP64 state (EOS), the rest in R.
 // ---------------------------------------------------------------------------
-template <int HT, int VT>
-__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P, int kz, StateBuf S, StageAux A,
-                                                        const double* __restrict__ u, const double* __restrict__ v,
-                                                        const double* __restrict__ w, const double* __restrict__ t11,
-                                                        const double* __restrict__ t22, const double* __restrict__ t33,
-                                                        const double* __restrict__ t12, const double* __restrict__ t13,
-                                                        const double* __restrict__ t23, const double* __restrict__ pavg,
-                                                        double* __restrict__ Fmx, double* __restrict__ Fmy,
-                                                        double* __restrict__ Fmz) {
-    __shared__ FluxTile sh[3];
+template <class R, int HT, int VT>
+__global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P, int kz, StateBuf S, StageAux<R> A,
+                                                                       const double* __restrict__ u,
+                                                                       const double* __restrict__ v,
+                                                                       const double* __restrict__ w,
+                                                                       const R* __restrict__ t11,
+                                                                       const R* __restrict__ t22,
+                                                                       const R* __restrict__ t33,
+                                                                       const R* __restrict__ t12,
+                                                                       const R* __restrict__ t13,
+                                                                       const R* __restrict__ t23,
+                                                                       const double* __restrict__ pavg,
+                                                                       R* __restrict__ Fmx, R* __restrict__ Fmy,
+                                                                       R* __restrict__ Fmz) {
+    __shared__ FluxTile<R> sh[3];
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -1361,91 +1215,92 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
     const bool xedge = ok && (tx == TTX - 1 || i == g.nx - 1);
     const bool yedge = ok && (ty == TTY - 1 || j == g.ny - 1);
+    const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi);
     const double* ru = S.mx;
     const double* rv = S.my;
     const double* rw = S.mz;
     const double* cd = S.cons;
-    const double* prim = A.prim;
-    const double* pp = A.pp;
-    double zlu = 0.0, zhu = 0.0, zlv = 0.0, zhv = 0.0, zlw = 0.0, zhw = 0.0;
+    const R* prim = A.prim;
+    const R* pp = A.pp;
+    R zlu = R(0), zhu = R(0), zlv = R(0), zhv = R(0), zlw = R(0), zhw = R(0);
     for (int k = k0; k < k1; ++k) {
         const int64_t c = ok ? cidx(g, i, j, k) : 0;
         const bool zk = ok && k >= 1;   // z-momentum on interior faces only
         if (ok) {
-            sh[0].fx[ty][tx] = xmom_flux_x<HT>(P, ru, u, i, j, k);
-            if (xedge) sh[0].fx[ty][tx + 1] = xmom_flux_x<HT>(P, ru, u, ip, j, k);
-            sh[0].fy[ty][tx] = xmom_flux_y<HT>(P, rv, u, i, j, k);
-            if (yedge) sh[0].fy[ty + 1][tx] = xmom_flux_y<HT>(P, rv, u, i, jp, k);
-            if (k == k0) zlu = xmom_flux_z<VT>(P, rw, u, i, j, k);
-            zhu = xmom_flux_z<VT>(P, rw, u, i, j, k + 1);
-            sh[1].fx[ty][tx] = ymom_flux_x<HT>(P, ru, v, i, j, k);
-            if (xedge) sh[1].fx[ty][tx + 1] = ymom_flux_x<HT>(P, ru, v, ip, j, k);
-            sh[1].fy[ty][tx] = ymom_flux_y<HT>(P, rv, v, i, j, k);
-            if (yedge) sh[1].fy[ty + 1][tx] = ymom_flux_y<HT>(P, rv, v, i, jp, k);
-            if (k == k0) zlv = ymom_flux_z<VT>(P, rw, v, i, j, k);
-            zhv = ymom_flux_z<VT>(P, rw, v, i, j, k + 1);
+            sh[0].fx[ty][tx] = xmom_flux_x<HT, R>(P, ru, u, i, j, k);
+            if (xedge) sh[0].fx[ty][tx + 1] = xmom_flux_x<HT, R>(P, ru, u, ip, j, k);
+            sh[0].fy[ty][tx] = xmom_flux_y<HT, R>(P, rv, u, i, j, k);
+            if (yedge) sh[0].fy[ty + 1][tx] = xmom_flux_y<HT, R>(P, rv, u, i, jp, k);
+            if (k == k0) zlu = xmom_flux_z<VT, R>(P, rw, u, i, j, k);
+            zhu = xmom_flux_z<VT, R>(P, rw, u, i, j, k + 1);
+            sh[1].fx[ty][tx] = ymom_flux_x<HT, R>(P, ru, v, i, j, k);
+            if (xedge) sh[1].fx[ty][tx + 1] = ymom_flux_x<HT, R>(P, ru, v, ip, j, k);
+            sh[1].fy[ty][tx] = ymom_flux_y<HT, R>(P, rv, v, i, j, k);
+            if (yedge) sh[1].fy[ty + 1][tx] = ymom_flux_y<HT, R>(P, rv, v, i, jp, k);
+            if (k == k0) zlv = ymom_flux_z<VT, R>(P, rw, v, i, j, k);
+            zhv = ymom_flux_z<VT, R>(P, rw, v, i, j, k + 1);
         }
         if (zk) {
-            sh[2].fx[ty][tx] = zmom_flux_x<HT>(P, ru, w, i, j, k);
-            if (xedge) sh[2].fx[ty][tx + 1] = zmom_flux_x<HT>(P, ru, w, ip, j, k);
-            sh[2].fy[ty][tx] = zmom_flux_y<HT>(P, rv, w, i, j, k);
-            if (yedge) sh[2].fy[ty + 1][tx] = zmom_flux_y<HT>(P, rv, w, i, jp, k);
-            if (k == k0 || k == 1) zlw = zmom_flux_z<VT>(P, rw, w, i, j, k);
-            zhw = zmom_flux_z<VT>(P, rw, w, i, j, k + 1);
+            sh[2].fx[ty][tx] = zmom_flux_x<HT, R>(P, ru, w, i, j, k);
+            if (xedge) sh[2].fx[ty][tx + 1] = zmom_flux_x<HT, R>(P, ru, w, ip, j, k);
+            sh[2].fy[ty][tx] = zmom_flux_y<HT, R>(P, rv, w, i, j, k);
+            if (yedge) sh[2].fy[ty + 1][tx] = zmom_flux_y<HT, R>(P, rv, w, i, jp, k);
+            if (k == k0 || k == 1) zlw = zmom_flux_z<VT, R>(P, rw, w, i, j, k);
+            zhw = zmom_flux_z<VT, R>(P, rw, w, i, j, k + 1);
         }
         __syncthreads();
         // ---------------- x-momentum on face i
         if (ok) {
-            double rhs = -((sh[0].fx[ty][tx + 1] - sh[0].fx[ty][tx]) * g.dxi * 1.0 +
-                           (sh[0].fy[ty + 1][tx] - sh[0].fy[ty][tx]) * g.dyi * 1.0 + (zhu - zlu) * g.dzi);
+            R rhs = -((sh[0].fx[ty][tx + 1] - sh[0].fx[ty][tx]) * dxi * R(1) +
+                      (sh[0].fy[ty + 1][tx] - sh[0].fy[ty][tx]) * dyi * R(1) + (zhu - zlu) * dzi);
             zlu = zhu;
             if (P.use_diff)
-                rhs -= ((t11[c] - t11[cidx(g, im, j, k)]) * g.dxi * 1.0 + (t12[cidx(g, i, jp, k)] - t12[c]) * g.dyi * 1.0 +
-                        (t13[c + g.sk] - t13[c]) * g.dzi);
-            double gpx = g.dxi * (pp[c] - pp[cidx(g, im, j, k)]);
-            gpx *= 1.0;
-            double q = 0.0;
-            if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + cidx(g, im, j, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, im, j, k)]);
-            double src = 0.0;
+                rhs -= ((t11[c] - t11[cidx(g, im, j, k)]) * dxi * R(1) + (t12[cidx(g, i, jp, k)] - t12[c]) * dyi * R(1) +
+                        (t13[c + g.sk] - t13[c]) * dzi);
+            R gpx = dxi * (pp[c] - pp[cidx(g, im, j, k)]);
+            gpx *= R(1);
+            R q = R(0);
+            if (P.moist) q = R(0.5) * (prim[4 * N + c] + prim[4 * N + cidx(g, im, j, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, im, j, k)]);
+            R src = R(0);
             if (P.coriolis) {
-                double rvl = 0.25 * (rv[cidx(g, i, jp, k)] + rv[c] + rv[cidx(g, im, jp, k)] + rv[cidx(g, im, j, k)]);
-                double rwl = 0.25 * (rw[c + g.sk] + rw[c] + rw[cidx(g, i, jm, k + 1)] + rw[cidx(g, i, jm, k)]);
-                src += P.cf * (rvl * P.sinphi - rwl * P.cosphi);
+                R rvl = R(0.25) * (R(rv[cidx(g, i, jp, k)]) + R(rv[c]) + R(rv[cidx(g, im, jp, k)]) + R(rv[cidx(g, im, j, k)]));
+                R rwl = R(0.25) * (R(rw[c + g.sk]) + R(rw[c]) + R(rw[cidx(g, i, jm, k + 1)]) + R(rw[cidx(g, i, jm, k)]));
+                src += R(P.cf) * (rvl * R(P.sinphi) - rwl * R(P.cosphi));
             }
-            src += 0.5 * (cd[c] + cd[cidx(g, im, j, k)]) * P.geo0;
-            rhs += (-gpx - 0.0) / (1.0 + q) + src;
+            src += R(0.5) * (R(cd[c]) + R(cd[cidx(g, im, j, k)])) * R(P.geo0);
+            rhs += (-gpx - R(0)) / (R(1) + q) + src;
             Fmx[c] = rhs;
         }
         // ---------------- y-momentum on face j
         if (ok) {
-            double rhs = -((sh[1].fx[ty][tx + 1] - sh[1].fx[ty][tx]) * g.dxi * 1.0 +
-                           (sh[1].fy[ty + 1][tx] - sh[1].fy[ty][tx]) * g.dyi * 1.0 + (zhv - zlv) * g.dzi);
+            R rhs = -((sh[1].fx[ty][tx + 1] - sh[1].fx[ty][tx]) * dxi * R(1) +
+                      (sh[1].fy[ty + 1][tx] - sh[1].fy[ty][tx]) * dyi * R(1) + (zhv - zlv) * dzi);
             zlv = zhv;
             if (P.use_diff)
-                rhs -= ((t12[cidx(g, ip, j, k)] - t12[c]) * g.dxi * 1.0 + (t22[c] - t22[cidx(g, i, jm, k)]) * g.dyi * 1.0 +
-                        (t23[c + g.sk] - t23[c]) * g.dzi);
-            double gpy = g.dyi * (pp[c] - pp[cidx(g, i, jm, k)]);
-            gpy *= 1.0;
-            double q = 0.0;
-            if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + cidx(g, i, jm, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, i, jm, k)]);
-            double src = 0.0;
+                rhs -= ((t12[cidx(g, ip, j, k)] - t12[c]) * dxi * R(1) + (t22[c] - t22[cidx(g, i, jm, k)]) * dyi * R(1) +
+                        (t23[c + g.sk] - t23[c]) * dzi);
+            R gpy = dyi * (pp[c] - pp[cidx(g, i, jm, k)]);
+            gpy *= R(1);
+            R q = R(0);
+            if (P.moist) q = R(0.5) * (prim[4 * N + c] + prim[4 * N + cidx(g, i, jm, k)] + prim[5 * N + c] + prim[5 * N + cidx(g, i, jm, k)]);
+            R src = R(0);
             if (P.coriolis) {
-                double rul = 0.25 * (ru[cidx(g, ip, j, k)] + ru[c] + ru[cidx(g, ip, jm, k)] + ru[cidx(g, i, jm, k)]);
-                src += -P.cf * rul * P.sinphi;
+                R rul = R(0.25) * (R(ru[cidx(g, ip, j, k)]) + R(ru[c]) + R(ru[cidx(g, ip, jm, k)]) + R(ru[cidx(g, i, jm, k)]));
+                src += -R(P.cf) * rul * R(P.sinphi);
             }
-            src += 0.5 * (cd[c] + cd[cidx(g, i, jm, k)]) * P.geo1;
-            rhs += (-gpy - 0.0) / (1.0 + q) + src;
+            src += R(0.5) * (R(cd[c]) + R(cd[cidx(g, i, jm, k)])) * R(P.geo1);
+            rhs += (-gpy - R(0)) / (R(1) + q) + src;
             Fmy[c] = rhs;
         }
         // ---------------- z-momentum on face k
-        if (ok && k == 0) Fmz[c] = 0.0;
+        if (ok && k == 0) Fmz[c] = R(0);
         if (zk) {
-            double rhs = -((sh[2].fx[ty][tx + 1] - sh[2].fx[ty][tx]) * g.dxi * 1.0 +
-                           (sh[2].fy[ty + 1][tx] - sh[2].fy[ty][tx]) * g.dyi * 1.0 + (zhw - zlw) * g.dzi);
+            R rhs = -((sh[2].fx[ty][tx + 1] - sh[2].fx[ty][tx]) * dxi * R(1) +
+                      (sh[2].fy[ty + 1][tx] - sh[2].fy[ty][tx]) * dyi * R(1) + (zhw - zlw) * dzi);
             zlw = zhw;
             if (P.use_diff)
-                rhs -= ((t13[cidx(g, ip, j, k)] - t13[c]) * g.dxi * 1.0 + (t23[cidx(g, i, jp, k)] - t23[c]) * g.dyi * 1.0 +
-                        (t33[c] - t33[c - g.sk]) * g.dzi);
+                rhs -= ((t13[cidx(g, ip, j, k)] - t13[c]) * dxi * R(1) + (t23[cidx(g, i, jp, k)] - t23[c]) * dyi * R(1) +
+                        (t33[c] - t33[c - g.sk]) * dzi);
             double b;
             double g2 = -P.gravity;
             if (!P.moist) {
@@ -1488,25 +1343,26 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
                 double r0avg = 0.5 * (rd[k] + rd[k - 1]);
                 b = -qavg * r0avg * g2;
             }
-            double zsrc = b;
+            R zsrc = R(b);
             if (P.coriolis) {
-                double rul = 0.25 * (ru[cidx(g, ip, j, k)] + ru[c] + ru[cidx(g, ip, j, k - 1)] + ru[c - g.sk]);
-                zsrc += P.cf * rul * P.cosphi;
+                R rul = R(0.25) * (R(ru[cidx(g, ip, j, k)]) + R(ru[c]) + R(ru[cidx(g, ip, j, k - 1)]) + R(ru[c - g.sk]));
+                zsrc += R(P.cf) * rul * R(P.cosphi);
             }
-            zsrc += 0.5 * (cd[c] + cd[c - g.sk]) * P.geo2;
-            double gpz = g.dzi * (pp[c] - pp[c - g.sk]) / 1.0;
-            double q = 0.0;
-            if (P.moist) q = 0.5 * (prim[4 * N + c] + prim[4 * N + c - g.sk] + prim[5 * N + c] + prim[5 * N + c - g.sk]);
-            rhs += (zsrc - gpz - 0.0) / (1.0 + q);
+            zsrc += R(0.5) * (R(cd[c]) + R(cd[c - g.sk])) * R(P.geo2);
+            R gpz = dzi * (pp[c] - pp[c - g.sk]) / R(1);
+            R q = R(0);
+            if (P.moist) q = R(0.5) * (prim[4 * N + c] + prim[4 * N + c - g.sk] + prim[5 * N + c] + prim[5 * N + c - g.sk]);
+            rhs += (zsrc - gpz - R(0)) / (R(1) + q);
             Fmz[c] = rhs;
         }
-        if (ok && k == g.nz - 1) Fmz[c + g.sk] = 0.0;
+        if (ok && k == g.nz - 1) Fmz[c + g.sk] = R(0);
         __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
-// Host launchers for the tiled kernels: scheme dispatch and grid sizing.
+// Host launchers: scheme dispatch, grid sizing and the explicit
+// instantiations for the plain (double) and mixed (float) forms.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1533,64 +1389,147 @@ int pick_kz(K kern, const Geo& g) {
 }
 
 dim3 tile_grid(const Geo& g, int kz) { return dim3((g.nx + TTX - 1) / TTX, (g.ny + TTY - 1) / TTY, (g.nz + kz - 1) / kz); }
+dim3 cell_block() { return dim3(32, 4, 1); }
+dim3 cell_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.nz); }
 
 constexpr int U5 = ERF_ADV_UPWIND_5TH, W5 = ERF_ADV_WENO_5;
 
-}  // namespace
+template <class R>
+using SlowCellK = void (*)(Params, int, StateBuf, StageAux<R>, const R*, R*, R*, R*, R*);
+template <class R>
+using SlowMomK = void (*)(Params, int, StateBuf, StageAux<R>, const double*, const double*, const double*, const R*,
+                          const R*, const R*, const R*, const R*, const R*, const double*, R*, R*, R*);
+template <class R>
+using PostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, StateBuf, StageAux<R>, StageAux<R>, int,
+                       const R*, const R*, const R*, const R*, double*, double*, double*);
 
-using SlowCellK = void (*)(Params, int, StateBuf, StageAux, const double*, double*, double*, double*, double*);
-using SlowMomK = void (*)(Params, int, StateBuf, StageAux, const double*, const double*, const double*, const double*,
-                          const double*, const double*, const double*, const double*, const double*, const double*,
-                          double*, double*, double*);
-using PostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, StateBuf, StageAux, StageAux, int,
-                       const double*, const double*, const double*, const double*, double*, double*, double*);
-
-static SlowCellK slow_cell_kernel(const Params& P) {
-    if (P.dyc_h == U5 && P.dyc_v == U5) return k_slow_cell<U5, U5>;
-    if (P.dyc_h == W5 && P.dyc_v == W5) return k_slow_cell<W5, W5>;
-    return k_slow_cell<-1, -1>;
+template <class R>
+SlowCellK<R> slow_cell_kernel(const Params& P) {
+    if (P.dyc_h == U5 && P.dyc_v == U5) return k_slow_cell<R, U5, U5>;
+    if (P.dyc_h == W5 && P.dyc_v == W5) return k_slow_cell<R, W5, W5>;
+    return k_slow_cell<R, -1, -1>;
 }
-static SlowMomK slow_mom_kernel(const Params& P) {
-    if (P.dyc_h == U5 && P.dyc_v == U5) return k_slow_mom<U5, U5>;
-    return k_slow_mom<-1, -1>;
+template <class R>
+SlowMomK<R> slow_mom_kernel(const Params& P) {
+    if (P.dyc_h == U5 && P.dyc_v == U5) return k_slow_mom<R, U5, U5>;
+    return k_slow_mom<R, -1, -1>;
 }
-static PostK post_kernel(const Params& P) {
+template <class R>
+PostK<R> post_kernel(const Params& P) {
     bool dw = P.dry_h == W5 && P.dry_v == W5, du = P.dry_h == U5 && P.dry_v == U5;
     bool mw = P.moi_h == W5 && P.moi_v == W5, mu = P.moi_h == U5 && P.moi_v == U5;
     if (!P.moist) {
-        if (dw) return k_post<W5, W5, -1, -1>;
-        if (du) return k_post<U5, U5, -1, -1>;
+        if (dw) return k_post<R, W5, W5, -1, -1>;
+        if (du) return k_post<R, U5, U5, -1, -1>;
     } else {
-        if (dw && mw) return k_post<W5, W5, W5, W5>;
-        if (du && mu) return k_post<U5, U5, U5, U5>;
-        if (du && mw) return k_post<U5, U5, W5, W5>;
+        if (dw && mw) return k_post<R, W5, W5, W5, W5>;
+        if (du && mu) return k_post<R, U5, U5, U5, U5>;
+        if (du && mw) return k_post<R, U5, U5, W5, W5>;
     }
-    return k_post<-1, -1, -1, -1>;
+    return k_post<R, -1, -1, -1, -1>;
 }
 
+}  // namespace
+
+template <class R>
 void tiled_setup(const Params& P, TiledKz* t) {
-    t->cell = pick_kz(slow_cell_kernel(P), P.g);
-    t->mom = pick_kz(slow_mom_kernel(P), P.g);
-    t->post = pick_kz(post_kernel(P), P.g);
+    t->cell = pick_kz(slow_cell_kernel<R>(P), P.g);
+    t->mom = pick_kz(slow_mom_kernel<R>(P), P.g);
+    t->post = pick_kz(post_kernel<R>(P), P.g);
 }
 
-void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* mut,
-                      double* Fcons, double* avx, double* avy, double* avz) {
-    slow_cell_kernel(P)<<<tile_grid(P.g, t.cell), dim3(TTX, TTY, 1), 0, st>>>(P, t.cell, S, A, mut, Fcons, avx, avy, avz);
+template <class R>
+int vert_setup(size_t vert_smem, size_t coef_smem) {
+    if (cudaFuncSetAttribute(k_fast_vert<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vert_smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_fast_coef<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem) != cudaSuccess)
+        return 1;
+    return 0;
 }
-void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* u,
-                     const double* v, const double* w, const double* t11, const double* t22, const double* t33,
-                     const double* t12, const double* t13, const double* t23, const double* pavg, double* Fmx,
-                     double* Fmy, double* Fmz) {
-    slow_mom_kernel(P)<<<tile_grid(P.g, t.mom), dim3(TTX, TTY, 1), 0, st>>>(P, t.mom, S, A, u, v, w, t11, t22, t33,
-                                                                             t12, t13, t23, pavg, Fmx, Fmy, Fmz);
+
+template <class R>
+void launch_step_begin(const Params& P, cudaStream_t st, const double* cons, const double* uo, const double* vo,
+                       const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut) {
+    k_step_begin<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, uo, vo, wo, S, un, vn, wn, A, mut);
 }
+template <class R>
+void launch_tau(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
+                const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23) {
+    k_tau<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, u, v, w, mut, t11, t22, t33, t12, t13, t23);
+}
+template <class R>
+void launch_plane_avg(const Params& P, cudaStream_t st, const double* cons, const R* prim, double* avg) {
+    k_plane_avg<R><<<P.g.nz, 256, 0, st>>>(P, cons, prim, avg);
+}
+template <class R>
+void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double dtau, double facinv, StateBuf Sprev,
+                   int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in, R* lag_out,
+                   R* avx, R* avy, double* outx, double* outy) {
+    k_fast_h<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, step, nrk, dtau, facinv, Sprev, prev_rt, Sst, A, Fmx, Fmy,
+                                                         lag_in, lag_out, avx, avy, outx, outy);
+}
+template <class R>
+void launch_fast_coef(const Params& P, cudaStream_t st, dim3 grid, dim3 block, size_t smem, double D, StateBuf Sst,
+                      StageAux<R> A, R* cA, R* cInvB, R* cCB, R* cP, R* cQ) {
+    k_fast_coef<R><<<grid, block, smem, st>>>(P, D, Sst, A, cA, cInvB, cCB, cP, cQ);
+}
+template <class R>
+void launch_fast_vert(const Params& P, cudaStream_t st, dim3 grid, dim3 block, size_t smem, double dtau,
+                      double facinv, double beta_1, double beta_2, StateBuf Sprev, int prev_rt, StateBuf Sst,
+                      StageAux<R> A, const R* Fcons, const R* Fmz, const double* newx, const double* newy,
+                      const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz, double* out_cons,
+                      double* out_mz) {
+    k_fast_vert<R><<<grid, block, smem, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, prev_rt, Sst, A, Fcons, Fmz,
+                                              newx, newy, cA, cInvB, cCB, cP, cQ, avz, out_cons, out_mz);
+}
+template <class R>
+void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const R* mut,
+                      R* Fcons, R* avx, R* avy, R* avz) {
+    slow_cell_kernel<R>(P)<<<tile_grid(P.g, t.cell), dim3(TTX, TTY, 1), 0, st>>>(P, t.cell, S, A, mut, Fcons, avx,
+                                                                                  avy, avz);
+}
+template <class R>
+void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
+                     const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,
+                     const R* t13, const R* t23, const double* pavg, R* Fmx, R* Fmy, R* Fmz) {
+    slow_mom_kernel<R>(P)<<<tile_grid(P.g, t.mom), dim3(TTX, TTY, 1), 0, st>>>(P, t.mom, S, A, u, v, w, t11, t22, t33,
+                                                                                t12, t13, t23, pavg, Fmx, Fmy, Fmz);
+}
+template <class R>
 void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
-                 StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext, int make_next, const double* mut,
-                 const double* avx, const double* avy, const double* avz, double* un, double* vn, double* wn) {
-    post_kernel(P)<<<tile_grid(P.g, t.post), dim3(TTX, TTY, 1), 0, st>>>(P, t.post, slow_dt, Sold, Sst, Ssum, Snew,
-                                                                          Acur, Anext, make_next, mut, avx, avy, avz,
-                                                                          un, vn, wn);
+                 StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
+                 const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
+    post_kernel<R>(P)<<<tile_grid(P.g, t.post), dim3(TTX, TTY, 1), 0, st>>>(P, t.post, slow_dt, Sold, Sst, Ssum, Snew,
+                                                                             Acur, Anext, make_next, mut, avx, avy,
+                                                                             avz, un, vn, wn);
 }
+
+#define ERFB_INSTANTIATE(R)                                                                                          \
+    template void tiled_setup<R>(const Params&, TiledKz*);                                                           \
+    template int vert_setup<R>(size_t, size_t);                                                                      \
+    template void launch_step_begin<R>(const Params&, cudaStream_t, const double*, const double*, const double*,     \
+                                       const double*, StateBuf, double*, double*, double*, StageAux<R>, R*);         \
+    template void launch_tau<R>(const Params&, cudaStream_t, const double*, const double*, const double*,            \
+                                const double*, const R*, R*, R*, R*, R*, R*, R*);                                    \
+    template void launch_plane_avg<R>(const Params&, cudaStream_t, const double*, const R*, double*);                \
+    template void launch_fast_h<R>(const Params&, cudaStream_t, int, int, double, double, StateBuf, int, StateBuf,   \
+                                   StageAux<R>, const R*, const R*, const R*, R*, R*, R*, double*, double*);         \
+    template void launch_fast_coef<R>(const Params&, cudaStream_t, dim3, dim3, size_t, double, StateBuf,             \
+                                      StageAux<R>, R*, R*, R*, R*, R*);                                              \
+    template void launch_fast_vert<R>(const Params&, cudaStream_t, dim3, dim3, size_t, double, double, double,       \
+                                      double, StateBuf, int, StateBuf, StageAux<R>, const R*, const R*,              \
+                                      const double*, const double*, const R*, const R*, const R*, const R*,          \
+                                      const R*, R*, double*, double*);                                               \
+    template void launch_slow_cell<R>(const Params&, const TiledKz&, cudaStream_t, StateBuf, StageAux<R>, const R*,  \
+                                      R*, R*, R*, R*);                                                               \
+    template void launch_slow_mom<R>(const Params&, const TiledKz&, cudaStream_t, StateBuf, StageAux<R>,             \
+                                     const double*, const double*, const double*, const R*, const R*, const R*,      \
+                                     const R*, const R*, const R*, const double*, R*, R*, R*);                       \
+    template void launch_post<R>(const Params&, const TiledKz&, cudaStream_t, double, StateBuf, StateBuf, StateBuf,  \
+                                 StateBuf, StageAux<R>, StageAux<R>, int, const R*, const R*, const R*, const R*,    \
+                                 double*, double*, double*);
+
+ERFB_INSTANTIATE(double)
+ERFB_INSTANTIATE(float)
+#undef ERFB_INSTANTIATE
 
 }  // namespace erfb

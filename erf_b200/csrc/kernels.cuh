@@ -35,11 +35,12 @@ struct StateBuf {
     double* mz;   // nzf
 };
 
-// Quantities derived from a stage state.
+// Quantities derived from a stage state, stored in the bulk type R.
+template <class R>
 struct StageAux {
-    double* prim;   // nprim*ncell
-    double* pi;     // ncell
-    double* pp;     // ncell (p - p0)
+    R* prim;   // nprim*ncell
+    R* pi;     // ncell
+    R* pp;     // ncell (p - p0)
 };
 
 // x-y tile of the transport kernels (slow_cell, slow_mom, post) and the
@@ -48,15 +49,44 @@ constexpr int TTX = 32, TTY = 8;
 struct TiledKz {
     int cell, mom, post;
 };
+
+// Host launchers of the dycore kernels (kernels.cu), instantiated for
+// R = double (plain form) and R = float (mixed form).
+template <class R>
 void tiled_setup(const Params& P, TiledKz* t);
-void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* mut,
-                      double* Fcons, double* avx, double* avy, double* avz);
-void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux A, const double* u,
-                     const double* v, const double* w, const double* t11, const double* t22, const double* t33,
-                     const double* t12, const double* t13, const double* t23, const double* pavg, double* Fmx,
-                     double* Fmy, double* Fmz);
+template <class R>
+int vert_setup(size_t vert_smem, size_t coef_smem);
+template <class R>
+void launch_step_begin(const Params& P, cudaStream_t st, const double* cons, const double* uo, const double* vo,
+                       const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut);
+template <class R>
+void launch_tau(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
+                const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23);
+template <class R>
+void launch_plane_avg(const Params& P, cudaStream_t st, const double* cons, const R* prim, double* avg);
+template <class R>
+void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double dtau, double facinv, StateBuf Sprev,
+                   int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in, R* lag_out,
+                   R* avx, R* avy, double* outx, double* outy);
+template <class R>
+void launch_fast_coef(const Params& P, cudaStream_t st, dim3 grid, dim3 block, size_t smem, double D, StateBuf Sst,
+                      StageAux<R> A, R* cA, R* cInvB, R* cCB, R* cP, R* cQ);
+template <class R>
+void launch_fast_vert(const Params& P, cudaStream_t st, dim3 grid, dim3 block, size_t smem, double dtau,
+                      double facinv, double beta_1, double beta_2, StateBuf Sprev, int prev_rt, StateBuf Sst,
+                      StageAux<R> A, const R* Fcons, const R* Fmz, const double* newx, const double* newy,
+                      const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz, double* out_cons,
+                      double* out_mz);
+template <class R>
+void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const R* mut,
+                      R* Fcons, R* avx, R* avy, R* avz);
+template <class R>
+void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
+                     const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,
+                     const R* t13, const R* t23, const double* pavg, R* Fmx, R* Fmy, R* Fmz);
+template <class R>
 void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
-                 StateBuf Ssum, StateBuf Snew, StageAux Acur, StageAux Anext, int make_next, const double* mut,
-                 const double* avx, const double* avy, const double* avz, double* un, double* vn, double* wn);
+                 StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
+                 const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
 
 }  // namespace erfb
