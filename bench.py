@@ -204,6 +204,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="moist_bubble", choices=sorted(cases.CASES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed"],
+                    help="precision forms to time (the JSON line needs both; single forms are for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -347,6 +349,14 @@ def main():
         return err
 
     clock_samples = []
+    if args.form != "both":
+        res, _, _ = measure(C.PREC_MIXED if args.form == "mixed" else C.PREC_FP64, clock_samples)
+        if rank == 0:
+            print(json.dumps({"form": args.form, "value": res["value"], "ms_per_step": res["ms_per_step"],
+                              "kernels": res["kernels"], "status": res["status"]}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     plain, base, init = measure(C.PREC_FP64, clock_samples)
     mixed, _, _ = measure(C.PREC_MIXED, None)
     mixed_err = form_error(base, init, 100) if rank == 0 else None

@@ -73,6 +73,25 @@ class Case:
         u = np.broadcast_to(self.u_cc[:, None, None], (nz, ny, nx + 1)).copy()
         v = np.broadcast_to(self.v_cc[:, None, None], (nz, ny + 1, nx)).copy()
         w = np.zeros((nz + 1, ny, nx))
+        va = self.pert.get("vel_noise_amp", 0.0)
+        if va > 0.0:
+            # seeded velocity noise below vel_noise_zmax (periodic faces kept
+            # consistent, w = 0 on the walls)
+            zmax = self.pert.get("vel_noise_zmax", np.inf)
+            zf = np.arange(nz + 1) * cfg.dz
+            nu = va * (2.0 * splitmix64_uniform(self.seed + 101, nz * ny * nx).reshape(nz, ny, nx) - 1.0)
+            nv = va * (2.0 * splitmix64_uniform(self.seed + 202, nz * ny * nx).reshape(nz, ny, nx) - 1.0)
+            nw = va * (2.0 * splitmix64_uniform(self.seed + 303, (nz + 1) * ny * nx).reshape(nz + 1, ny, nx) - 1.0)
+            nu[z > zmax] = 0.0
+            nv[z > zmax] = 0.0
+            nw[zf > zmax] = 0.0
+            nw[0] = 0.0
+            nw[nz] = 0.0
+            u[:, :, :nx] += nu
+            u[:, :, nx] = u[:, :, 0]
+            v[:, :ny, :] += nv
+            v[:, ny, :] = v[:, 0, :]
+            w += nw
         return cons, u, v, w
 
     def theta_perturbation(self, x, y, z):
@@ -122,6 +141,26 @@ def abl_dry(nx=64, ny=64, nz=64, seed=0) -> Case:
     return Case("abl_dry", c, theta, np.zeros(nz), 300.0, 0.0, 1.0e5,
                 np.full(nz, 10.0), np.zeros(nz), seed,
                 pert={"noise_amp": 0.1, "noise_zmax": 400.0}, steps=10)
+
+
+def abl_fine(nx=512, ny=512, nz=128, dx=10.0, dz=10.0, u_g=10.0, dt=0.08, seed=0) -> Case:
+    """Fine-grid ABL with the physics of abl_dry (training data of the learned
+    closure): geostrophic wind (u_g, 0), Smagorinsky Cs 0.1, theta 300 K below
+    500 m then +3 K/km, +-0.1 K theta noise and +-0.5 m/s velocity noise below
+    400 m (the velocity noise starts the shear turbulence within the short
+    runs used for training)."""
+    case = abl_dry(nx=nx, ny=ny, nz=nz, seed=seed)
+    c = case.cfg
+    c.dx = c.dy = dx
+    c.dz = dz
+    c.dt = dt
+    C.set_coriolis(c, rotational_time_period=4.0 * math.pi / 1.0e-4, latitude_deg=90.0, geo_wind=(u_g, 0.0, 0.0))
+    z = (np.arange(nz) + 0.5) * dz
+    case.theta_cc = np.where(z < 500.0, 300.0, 300.0 + 3.0e-3 * (z - 500.0))
+    case.u_cc = np.full(nz, float(u_g))
+    case.name = "abl_fine"
+    case.pert.update({"vel_noise_amp": 0.5, "vel_noise_zmax": 400.0})
+    return case
 
 
 def moist_bubble(nx=128, ny=128, nz=80, seed=1) -> Case:

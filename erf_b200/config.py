@@ -19,7 +19,7 @@ ADV_NAMES = {
     "Upwind_5th": UPWIND_5TH, "Centered_6th": CENTERED_6TH, "WENO3": WENO_3, "WENOZ3": WENO_3Z,
     "WENO5": WENO_5, "WENOZ5": WENO_5Z, "WENOMZQ3": WENO_3MZQ, "WENO7": WENO_7, "WENOZ7": WENO_7Z,
 }
-LES_NONE, LES_SMAGORINSKY, LES_DEARDORFF = 0, 1, 2
+LES_NONE, LES_SMAGORINSKY, LES_DEARDORFF, LES_MLP = 0, 1, 2, 3
 MOLEC_NONE, MOLEC_CONSTANT, MOLEC_CONSTANT_ALPHA = 0, 1, 2
 MOIST_NONE, MOIST_KESSLER, MOIST_KESSLER_NORAIN = 0, 1, 2
 BC_NO_SLIP_WALL, BC_SLIP_WALL, BC_PERIODIC = 5, 6, 7

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "mlp.cuh"
 
 namespace erfb {
 __global__ void k_kessler(Params P, double* cons, double dtn, double dz);
@@ -32,6 +33,8 @@ struct Bulk {
     R* mut;                       // eddy viscosity
     R *t11, *t22, *t33, *t12, *t13, *t23;
     R *cA, *cInvB, *cCB, *cP, *cQ;  // fast coefficients of the current stage
+    R *c12 = nullptr, *c13 = nullptr, *c23 = nullptr;  // learned closure: cell-centred off-diagonal stresses
+    R *hx = nullptr, *hy = nullptr, *hz = nullptr;     // learned closure: rho * heat flux
 };
 
 // Threads per block of the vertical acoustic kernel (columns x level groups).
@@ -55,6 +58,11 @@ struct erf_b200_ctx {
     Bulk<double> bd;          // bulk arrays of the plain form
     Bulk<float> bf;           // bulk arrays of the mixed form
     bool mixed = false;
+    const erf_b200_mlp* net = nullptr;   // learned closure (les_type ERF_LES_MLP)
+    unsigned int* fallback = nullptr;    // cells that fell back to Smagorinsky
+    int closure_grid = 1;
+    double* feat_theta = nullptr;        // feature extraction scratch
+    float* feat_out = nullptr;
     int tile_tx = 32, vert_warps = 32, coef_warps = 8;
     TiledKz tkz{1, 1, 1};
     size_t vert_smem = 0, coef_smem = 0;
@@ -111,7 +119,9 @@ int validate(const erf_b200_config* c) {
     if (c->dycore_horiz_adv == ERF_ADV_CENTERED_2ND && c->dycore_vert_adv == ERF_ADV_CENTERED_2ND) return ERF_B200_ECONFIG;
     if (!adv_supported(c->dryscal_horiz_adv) || !adv_supported(c->dryscal_vert_adv)) return ERF_B200_ECONFIG;
     if (!adv_supported(c->moistscal_horiz_adv) || !adv_supported(c->moistscal_vert_adv)) return ERF_B200_ECONFIG;
-    if (c->les_type != ERF_LES_NONE && c->les_type != ERF_LES_SMAGORINSKY) return ERF_B200_ECONFIG;
+    if (c->les_type != ERF_LES_NONE && c->les_type != ERF_LES_SMAGORINSKY && c->les_type != ERF_LES_MLP)
+        return ERF_B200_ECONFIG;
+    if (c->les_type == ERF_LES_MLP && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
     if (c->molec_diff_type < 0 || c->molec_diff_type > 2) return ERF_B200_ECONFIG;
     if (c->moisture == ERF_MOIST_NONE) {
         if (c->ncomp != 5) return ERF_B200_ECONFIG;
@@ -253,10 +263,17 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
         int nsub; double dtau, slow_dt;
         stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
-        if (P.use_diff)
+        if (P.les == ERF_LES_MLP) {
+            ClosureNet net{c->net->wpack, c->net->bias, c->net->norm, c->net->env, c->fallback};
+            TIMED(1, launch_closure<R>(P, net, c->closure_grid, st, Sst.cons, Vnew[0], Vnew[1], Vnew[2], Acur.prim,
+                                       B.t11, B.t22, B.t33, B.c12, B.c13, B.c23, B.t12, B.t13, B.t23, B.hx, B.hy,
+                                       B.hz));
+        } else if (P.use_diff) {
             TIMED(1, launch_tau<R>(P, st, Sst.cons, Vnew[0], Vnew[1], Vnew[2], B.mut, B.t11, B.t22, B.t33, B.t12,
                                    B.t13, B.t23));
-        TIMED(2, launch_slow_cell<R>(P, c->tkz, st, Sst, Acur, B.mut, B.Fcons, B.avx, B.avy, B.avz));
+        }
+        TIMED(2, launch_slow_cell<R>(P, c->tkz, st, Sst, Acur, B.mut, B.hx, B.hy, B.hz, B.Fcons, B.avx, B.avy,
+                                     B.avz));
         if (P.moist && P.buoy_type == 2) TIMED(3, launch_plane_avg<R>(P, st, Sst.cons, Acur.prim, c->pavg));
         TIMED(4, launch_slow_mom<R>(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12,
                                     B.t13, B.t23, c->pavg, B.Fmx, B.Fmy, B.Fmz));
@@ -300,6 +317,9 @@ int alloc_bulk(erf_b200_ctx* c, Bulk<R>& B) {
     A(&B.mut, N);
     A(&B.t11, N); A(&B.t22, N); A(&B.t33, N); A(&B.t12, N); A(&B.t13, NZF); A(&B.t23, NZF);
     A(&B.cA, NZF); A(&B.cInvB, NZF); A(&B.cCB, NZF); A(&B.cP, NZF); A(&B.cQ, NZF);
+    if (cfg->les_type == ERF_LES_MLP) {
+        A(&B.c12, N); A(&B.c13, N); A(&B.c23, N); A(&B.hx, N); A(&B.hy, N); A(&B.hz, N);
+    }
     return rc;
 }
 
@@ -429,7 +449,15 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         }
         if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     }
-    rc = build_graphs(c);
+    if (cfg->les_type == ERF_LES_MLP) {
+        // the step graphs are built when the network is attached
+        void* q = nullptr;
+        if (cudaMalloc(&q, sizeof(unsigned int)) != cudaSuccess) rc = ERF_B200_ENOMEM;
+        else { c->allocs.push_back(q); c->fallback = (unsigned int*)q; cudaMemsetAsync(q, 0, sizeof(unsigned int), c->stream); }
+        if (rc == ERF_B200_OK) c->closure_grid = c->mixed ? closure_grid<float>(c->P) : closure_grid<double>(c->P);
+    } else {
+        rc = build_graphs(c);
+    }
     if (rc == ERF_B200_OK) rc = cuda_fail(cudaStreamSynchronize(c->stream));
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     *out = c;
@@ -461,6 +489,7 @@ int erf_b200_get_status(erf_b200_ctx* c) {
     int h = 0;
     CK(cudaMemcpy(&h, c->status, sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemset(c->status, 0, sizeof(int)));
+    if (h & ST_TIMEOUT) return ERF_B200_ETIMEOUT;
     if (h & ST_NAN) return ERF_B200_ENAN;
     if (h & ST_BADSTATE) return ERF_B200_EBADSTATE;
     return ERF_B200_OK;
@@ -504,6 +533,7 @@ int erf_b200_advance(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_f
     if ((rc = pack(c, xvel, 1, 1, c->vel[0][0]))) return rc;
     if ((rc = pack(c, yvel, 2, 1, c->vel[0][1]))) return rc;
     if ((rc = pack(c, zvel, 3, 1, c->vel[0][2]))) return rc;
+    if (!c->graph[0] || !c->graph[1]) return ERF_B200_EBADSTATE;   // learned closure not attached
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph[s & 1], c->stream));
     int p = nsteps & 1;
     if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[p].cons))) return rc;
@@ -554,6 +584,7 @@ int erf_b200_advance_profiled(erf_b200_ctx* c, const erf_b200_fab* cons, const e
                               int* kernel_launches, int nslots) {
     if (!c || nsteps < 0 || !kernel_ms || !kernel_launches || nslots < ERF_B200_NUM_KERNEL_SLOTS) return ERF_B200_EINVAL;
     if (!c->base_set) return ERF_B200_EINVAL;
+    if (c->P.les == ERF_LES_MLP && !c->net) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
         return ERF_B200_EINVAL;
@@ -592,23 +623,212 @@ int erf_b200_kernels_per_step(const erf_b200_ctx* c, int* launches) {
     for (int nrk = 0; nrk < 3; ++nrk) {
         int nsub; double a, b;
         stage_schedule(c->cfg, nrk, nsub, a, b);
-        n += 4 + (c->P.use_diff ? 1 : 0) + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0) + 2 * nsub;
+        int stress = c->P.les == ERF_LES_MLP ? 2 : (c->P.use_diff ? 1 : 0);
+        n += 4 + stress + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0) + 2 * nsub;
     }
     *launches = n;
     return ERF_B200_OK;
 }
 
-// Per-pass entry points that are not yet exposed separately from the fused
-// step return ERF_B200_EINVAL.
-int erf_b200_turbulent_viscosity(erf_b200_ctx*, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
-                                 const erf_b200_fab*) { return ERF_B200_EINVAL; }
-int erf_b200_slow_rhs_pre(erf_b200_ctx*, int, double, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
-                          const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*) { return ERF_B200_EINVAL; }
-int erf_b200_make_fast_coeffs(erf_b200_ctx*, const erf_b200_fab*, const erf_b200_fab*, double) { return ERF_B200_EINVAL; }
-int erf_b200_fast_rhs_N(erf_b200_ctx*, int, int, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
-                        const erf_b200_fab*, const erf_b200_fab*, double, double) { return ERF_B200_EINVAL; }
-int erf_b200_slow_rhs_post(erf_b200_ctx*, int, double, const erf_b200_fab*, const erf_b200_fab*, const erf_b200_fab*,
-                           const erf_b200_fab*, const erf_b200_fab*) { return ERF_B200_EINVAL; }
+// ---------------------------------------------------------------------------
+// Per-pass entry points (plain form).  Each packs the caller's fabs into the
+// context's valid-region arrays, runs the kernels of that pass and unpacks
+// the outputs.  State carried between passes lives in the context, as in
+// MRISplitIntegrator: the eddy viscosity (erf_b200_turbulent_viscosity), the
+// stage primitives of the last slow_rhs_pre (used by slow_rhs_post), and the
+// fast coefficients of the stage (made at substep 0).  A vector of fabs
+// S[4] is {cons, x-momentum, y-momentum, z-momentum}.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// The fab of one component of a multi-component fab.
+erf_b200_fab comp_fab(const erf_b200_fab* f, int n, int ncomp) {
+    erf_b200_fab r = *f;
+    r.p = f->p + (int64_t)n * f->nstride;
+    r.ncomp = ncomp;
+    return r;
+}
+
+bool fab4_ok(const erf_b200_fab* S, const Geo& g, int ncons) {
+    return S && fab_ok(&S[0], 0, g, ncons) && fab_ok(&S[1], 1, g, 1) && fab_ok(&S[2], 2, g, 1) &&
+           fab_ok(&S[3], 3, g, 1);
+}
+
+int pack4(erf_b200_ctx* c, const erf_b200_fab* S, int ncons, double* cons, double* mx, double* my, double* mz) {
+    int rc;
+    if (cons && (rc = pack(c, &S[0], 0, ncons, cons))) return rc;
+    if ((rc = pack(c, &S[1], 1, 1, mx))) return rc;
+    if ((rc = pack(c, &S[2], 2, 1, my))) return rc;
+    return pack(c, &S[3], 3, 1, mz);
+}
+
+int unpack4(erf_b200_ctx* c, const erf_b200_fab* S, int ncons, const double* cons, const double* mx,
+            const double* my, const double* mz) {
+    int rc;
+    if (cons && (rc = unpack(c, &S[0], 0, ncons, cons))) return rc;
+    if ((rc = unpack(c, &S[1], 1, 1, mx))) return rc;
+    if ((rc = unpack(c, &S[2], 2, 1, my))) return rc;
+    return unpack(c, &S[3], 3, 1, mz);
+}
+
+// A, 1/B', C, P, Q on the valid z-faces of a 5-component z-face fab; C is
+// recovered from the stored C/B'.
+__global__ void k_coef_export(Geo g, erf_b200_fab f, const double* cA, const double* cInvB, const double* cCB,
+                              const double* cP, const double* cQ) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    int64_t s = cidx(g, i, j, k);
+    int64_t d = (int64_t)(i - f.lo[0]) + (int64_t)(j - f.lo[1]) * f.jstride + (int64_t)(k - f.lo[2]) * f.kstride;
+    double invb = cInvB[s];
+    double cc = cCB[s] / invb;   // C/B' * B' (wall rows hold B' itself)
+    f.p[d] = cA[s];
+    f.p[d + f.nstride] = invb;
+    f.p[d + 2 * f.nstride] = cc;
+    f.p[d + 3 * f.nstride] = cP[s];
+    f.p[d + 4 * f.nstride] = cQ[s];
+}
+
+const double kBeta1 = 0.5 * (1.0 - 0.1), kBeta2 = 0.5 * (1.0 + 0.1);
+
+}  // namespace
+
+extern "C" {
+
+int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, const erf_b200_fab* yvel,
+                                 const erf_b200_fab* zvel, const erf_b200_fab* cons) {
+    if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
+        return ERF_B200_EINVAL;
+    int rc;
+    if ((rc = pack(c, cons, 0, c->cfg.ncomp, c->S[0].cons))) return rc;
+    if ((rc = pack(c, xvel, 1, 1, c->vel[0][0])) || (rc = pack(c, yvel, 2, 1, c->vel[0][1])) ||
+        (rc = pack(c, zvel, 3, 1, c->vel[0][2])))
+        return rc;
+    // the step prologue forms the eddy viscosity from these velocities (its
+    // other outputs go to scratch slots of the context)
+    launch_step_begin<double>(c->P, c->stream, c->S[0].cons, c->vel[0][0], c->vel[0][1], c->vel[0][2], c->S[1],
+                              c->vel[1][0], c->vel[1][1], c->vel[1][2], c->bd.aux[1], c->bd.mut);
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b200_fab* S_rhs,
+                          const erf_b200_fab* S_data, const erf_b200_fab* S_scratch, const erf_b200_fab* xvel,
+                          const erf_b200_fab* yvel, const erf_b200_fab* zvel) {
+    (void)nrk; (void)slow_dt;
+    if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
+    if (c->P.les == ERF_LES_MLP && !c->net) return ERF_B200_EBADSTATE;
+    const Geo& g = c->g;
+    const int nc = c->cfg.ncomp;
+    if (!fab4_ok(S_data, g, nc) || !fab4_ok(S_rhs, g, 2) || !fab4_ok(S_scratch, g, 1) || !fab_ok(xvel, 1, g, 1) ||
+        !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
+        return ERF_B200_EINVAL;
+    const Params& P = c->P;
+    Bulk<double>& B = c->bd;
+    StateBuf Sst = c->S[2];
+    double** V = c->vel[1];
+    int rc;
+    if ((rc = pack4(c, S_data, nc, Sst.cons, Sst.mx, Sst.my, Sst.mz))) return rc;
+    if ((rc = pack(c, xvel, 1, 1, V[0])) || (rc = pack(c, yvel, 2, 1, V[1])) || (rc = pack(c, zvel, 3, 1, V[2])))
+        return rc;
+    cudaStream_t st = c->stream;
+    launch_stage_aux<double>(P, st, Sst.cons, B.aux[0]);
+    if (P.les == ERF_LES_MLP) {
+        ClosureNet net{c->net->wpack, c->net->bias, c->net->norm, c->net->env, c->fallback};
+        launch_closure<double>(P, net, c->closure_grid, st, Sst.cons, V[0], V[1], V[2], B.aux[0].prim, B.t11, B.t22,
+                               B.t33, B.c12, B.c13, B.c23, B.t12, B.t13, B.t23, B.hx, B.hy, B.hz);
+    } else if (P.use_diff) {
+        launch_tau<double>(P, st, Sst.cons, V[0], V[1], V[2], B.mut, B.t11, B.t22, B.t33, B.t12, B.t13, B.t23);
+    }
+    launch_slow_cell<double>(P, c->tkz, st, Sst, B.aux[0], B.mut, B.hx, B.hy, B.hz, B.Fcons, B.avx, B.avy, B.avz);
+    if (P.moist && P.buoy_type == 2) launch_plane_avg<double>(P, st, Sst.cons, B.aux[0].prim, c->pavg);
+    launch_slow_mom<double>(P, c->tkz, st, Sst, B.aux[0], V[0], V[1], V[2], B.t11, B.t22, B.t33, B.t12, B.t13, B.t23,
+                            c->pavg, B.Fmx, B.Fmy, B.Fmz);
+    if ((rc = unpack4(c, S_rhs, 2, B.Fcons, B.Fmx, B.Fmy, B.Fmz))) return rc;
+    if ((rc = unpack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_make_fast_coeffs(erf_b200_ctx* c, const erf_b200_fab* fast_coeffs, const erf_b200_fab* S_stage,
+                              double dtau) {
+    if (!c || c->mixed || !c->base_set || !fast_coeffs) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab4_ok(S_stage, g, c->cfg.ncomp) || !fab_ok(fast_coeffs, 3, g, 5)) return ERF_B200_EINVAL;
+    StateBuf Sst = c->S[2];
+    Bulk<double>& B = c->bd;
+    int rc;
+    if ((rc = pack4(c, S_stage, c->cfg.ncomp, Sst.cons, Sst.mx, Sst.my, Sst.mz))) return rc;
+    launch_stage_aux<double>(c->P, c->stream, Sst.cons, B.aux[0]);
+    dim3 tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1), tcb(c->tile_tx, c->coef_warps, 1);
+    double D = dtau * dtau * kBeta2 * kBeta2 * g.dzi;
+    launch_fast_coef<double>(c->P, c->stream, tg, tcb, c->coef_smem, D, Sst, B.aux[0], B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
+    k_coef_export<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.nz + 1), dim3(32, 4, 1), 0, c->stream>>>(
+        g, *fast_coeffs, B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_fast_rhs_N(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* S_slow_rhs,
+                        const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
+                        const erf_b200_fab* S_scratch, double dtau, double facinv) {
+    if (!c || c->mixed || !c->base_set || step < 0 || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    const int nc = c->cfg.ncomp;
+    if (!fab4_ok(S_slow_rhs, g, 2) || !fab4_ok(S_prev, g, 2) || !fab4_ok(S_stage, g, nc) || !fab4_ok(S_data, g, 2) ||
+        !fab4_ok(S_scratch, g, 2))
+        return ERF_B200_EINVAL;
+    const Params& P = c->P;
+    Bulk<double>& B = c->bd;
+    StateBuf Sprev = c->S[0], Sst = c->S[2], OUT = c->S[3];
+    cudaStream_t st = c->stream;
+    int rc;
+    if ((rc = pack4(c, S_slow_rhs, 2, B.Fcons, B.Fmx, B.Fmy, B.Fmz))) return rc;
+    if ((rc = pack4(c, S_prev, 2, Sprev.cons, Sprev.mx, Sprev.my, Sprev.mz))) return rc;
+    if ((rc = pack4(c, S_stage, nc, Sst.cons, Sst.mx, Sst.my, Sst.mz))) return rc;
+    if ((rc = pack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
+    erf_b200_fab lagf = comp_fab(&S_scratch[0], 1, 1);   // lagged d(rho theta) in the rho-theta slot
+    if ((rc = pack(c, &lagf, 0, 1, B.lag[0]))) return rc;
+    if (step == 0) {
+        // make_fast_coeffs at the stage's first substep (ERF_fast_rhs_N.cpp:60-70)
+        launch_stage_aux<double>(P, st, Sst.cons, B.aux[0]);
+        dim3 tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1), tcb(c->tile_tx, c->coef_warps, 1);
+        double D = dtau * dtau * kBeta2 * kBeta2 * g.dzi;
+        launch_fast_coef<double>(P, st, tg, tcb, c->coef_smem, D, Sst, B.aux[0], B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
+    }
+    launch_fast_h<double>(P, st, step, nrk, dtau, facinv, Sprev, 0, Sst, B.aux[0], B.Fmx, B.Fmy, B.lag[0], B.lag[1],
+                          B.avx, B.avy, OUT.mx, OUT.my);
+    dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
+    launch_fast_vert<double>(P, st, tg, tb, c->vert_smem, dtau, facinv, kBeta1, kBeta2, Sprev, 0, Sst, B.aux[0],
+                             B.Fcons, B.Fmz, OUT.mx, OUT.my, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, OUT.cons, OUT.mz);
+    if ((rc = unpack4(c, S_data, 2, OUT.cons, OUT.mx, OUT.my, OUT.mz))) return rc;
+    if ((rc = unpack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
+    if ((rc = unpack(c, &lagf, 0, 1, B.lag[1]))) return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b200_fab* S_rhs,
+                           const erf_b200_fab* S_old, const erf_b200_fab* S_new, const erf_b200_fab* S_data,
+                           const erf_b200_fab* S_scratch) {
+    (void)S_rhs;
+    if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    const int nc = c->cfg.ncomp;
+    if (!fab4_ok(S_old, g, nc) || !fab4_ok(S_new, g, nc) || !fab4_ok(S_data, g, nc) || !fab4_ok(S_scratch, g, 1))
+        return ERF_B200_EINVAL;
+    Bulk<double>& B = c->bd;
+    StateBuf OLD = c->S[0], NEW = c->S[1], SUM = c->S[3];
+    int rc;
+    if ((rc = pack4(c, S_old, nc, OLD.cons, OLD.mx, OLD.my, OLD.mz))) return rc;
+    if ((rc = pack4(c, S_data, nc, SUM.cons, SUM.mx, SUM.my, SUM.mz))) return rc;
+    if ((rc = pack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
+    // stage state and primitives: those of the preceding slow_rhs_pre
+    launch_post<double>(c->P, c->tkz, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.avx,
+                        B.avy, B.avz, c->vel[1][0], c->vel[1][1], c->vel[1][2]);
+    if ((rc = unpack4(c, S_new, nc, NEW.cons, NEW.mx, NEW.my, NEW.mz))) return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
 int erf_b200_kessler_advance(erf_b200_ctx* c, const erf_b200_fab* cons, double dt) {
     if (!c || !c->P.moist) return ERF_B200_EINVAL;
     const Geo& g = c->g;
@@ -618,6 +838,71 @@ int erf_b200_kessler_advance(erf_b200_ctx* c, const erf_b200_fab* cons, double d
     k_kessler<<<col_grid(g), col_block(), 0, c->stream>>>(c->P, c->S[2].cons, dt, c->cfg.dz);
     if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[2].cons))) return rc;
     return cuda_fail(cudaGetLastError());
+}
+
+// Attach a trained network to a context created with les_type
+// ERF_LES_MLP; the step graphs are (re)built with its arrays.
+int erf_b200_set_closure(erf_b200_ctx* c, const erf_b200_mlp* m) {
+    if (!c || !m || c->P.les != ERF_LES_MLP) return ERF_B200_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    for (int p = 0; p < 2; ++p)
+        if (c->graph[p]) { cudaGraphExecDestroy(c->graph[p]); c->graph[p] = nullptr; }
+    c->net = m;
+    int rc = build_graphs(c);
+    if (rc) return rc;
+    return cuda_fail(cudaStreamSynchronize(c->stream));
+}
+
+// Cells that fell back to Smagorinsky since the last call (reset on read).
+int erf_b200_closure_fallbacks(erf_b200_ctx* c, unsigned long long* count) {
+    if (!c || !count || !c->fallback) return ERF_B200_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    unsigned int h = 0;
+    CK(cudaMemcpy(&h, c->fallback, sizeof(h), cudaMemcpyDeviceToHost));
+    CK(cudaMemset(c->fallback, 0, sizeof(h)));
+    *count = h;
+    return ERF_B200_OK;
+}
+
+// Closure features (13 per cell, cell order i fastest) of a state given as
+// dense host arrays in the layout of erf_b200_advance_host.
+int erf_b200_closure_features_host(erf_b200_ctx* c, const double* cons, const double* u, const double* v,
+                                   const double* w, float* features) {
+    if (!c || !cons || !u || !v || !w || !features) return ERF_B200_EINVAL;
+    const erf_b200_config& f = c->cfg;
+    const int64_t nc = f.ncomp, nx = f.nx, ny = f.ny, nz = f.nz, N = nx * ny * nz;
+    const int64_t ncons = nc * N, nu = (nx + 1) * ny * nz, nv = nx * (ny + 1) * nz, nw = nx * ny * (nz + 1);
+    int rc;
+    if (!c->h_stage && (rc = dalloc(c, &c->h_stage, ncons + nu + nv + nw))) return rc;
+    if (!c->feat_theta && (rc = dalloc(c, &c->feat_theta, N))) return rc;
+    if (!c->feat_out && (rc = dalloc(c, &c->feat_out, N * 13))) return rc;
+    double* dc = c->h_stage;
+    double* du = dc + ncons;
+    double* dv = du + nu;
+    double* dw = dv + nv;
+    CK(cudaMemcpyAsync(dc, cons, ncons * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(du, u, nu * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dv, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dw, w, nw * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    auto mk = [&](double* p, int hx, int hy, int hz, int ncomp) {
+        erf_b200_fab fb;
+        fb.p = p; fb.lo[0] = fb.lo[1] = fb.lo[2] = 0; fb.hi[0] = hx; fb.hi[1] = hy; fb.hi[2] = hz;
+        fb.jstride = hx + 1; fb.kstride = (int64_t)(hx + 1) * (hy + 1); fb.nstride = fb.kstride * (hz + 1);
+        fb.ncomp = ncomp;
+        return fb;
+    };
+    erf_b200_fab fc = mk(dc, nx - 1, ny - 1, nz - 1, nc), fu = mk(du, nx, ny - 1, nz - 1, 1),
+                 fv = mk(dv, nx - 1, ny, nz - 1, 1), fw = mk(dw, nx - 1, ny - 1, nz, 1);
+    if ((rc = pack(c, &fc, 0, f.ncomp, c->S[0].cons))) return rc;
+    if ((rc = pack(c, &fu, 1, 1, c->vel[0][0]))) return rc;
+    if ((rc = pack(c, &fv, 2, 1, c->vel[0][1]))) return rc;
+    if ((rc = pack(c, &fw, 3, 1, c->vel[0][2]))) return rc;
+    launch_features(c->P, c->stream, c->S[0].cons, c->vel[0][0], c->vel[0][1], c->vel[0][2], c->feat_theta,
+                    c->feat_out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(features, c->feat_out, N * 13 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ERF_B200_OK;
 }
 
 }  // extern "C"

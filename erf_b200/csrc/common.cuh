@@ -24,6 +24,7 @@ constexpr double Rd_on_Rv = R_d / R_v;
 // Status bits written by kernels (OR-ed into ctx->status)
 constexpr int ST_BADSTATE = 1;
 constexpr int ST_NAN = 2;
+constexpr int ST_TIMEOUT = 4;   // a bounded tensor-core wait ran out
 
 // ---------------------------------------------------------------------------
 // Equation of state (reference: Source/Utils/ERF_EOS.H:42-151).  Same

@@ -130,7 +130,7 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
     if (k == g.nz - 1) { S.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
     stage_aux_cell<R>(P, cons, A, c, k);
 
-    if (P.les == ERF_LES_SMAGORINSKY) {
+    if (P.les == ERF_LES_SMAGORINSKY || P.les == ERF_LES_MLP) {
         int ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
         double s11 = (uo[cidx(g, ip, j, k)] - uo[c]) * g.dxi;
         double s22 = (vo[cidx(g, i, jp, k)] - vo[c]) * g.dyi;
@@ -189,6 +189,16 @@ __global__ void k_tau(Params P, const double* __restrict__ cons, const double* _
         if (P.use_turb) m2 = m2 + R(2) * (R(0.25) * (mu(i, jm, kk) + mu(i, j, kk) + mu(i, jm, kk - 1) + mu(i, j, kk - 1)));
         t23[e] = R(strain23(v, w, g, i, j, kk)) * -m2;
     }
+}
+
+// Stage primitives, Exner function and p' of a state (cons_to_prim,
+// ERF_TI_utils.H:4-45), for the per-pass entry points.
+template <class R>
+__global__ void k_stage_aux(Params P, const double* __restrict__ cons, StageAux<R> A) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_coords(g, i, j, k)) return;
+    stage_aux_cell<R>(P, cons, A, cidx(g, i, j, k), k);
 }
 
 // ---------------------------------------------------------------------------
@@ -965,6 +975,9 @@ __device__ __forceinline__ R tile_div(const Geo& g, const FluxTile<R>& t, R zl, 
 template <class R, int TH, int TV>
 __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params P, int kz, StateBuf S, StageAux<R> A,
                                                                          const R* __restrict__ mut,
+                                                                         const R* __restrict__ hx,
+                                                                         const R* __restrict__ hy,
+                                                                         const R* __restrict__ hz,
                                                                          R* __restrict__ Fcons, R* __restrict__ avx,
                                                                          R* __restrict__ avy, R* __restrict__ avz) {
     __shared__ FluxTile<R> sh;
@@ -989,7 +1002,20 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
             if (k == g.nz - 1) avz[c + g.sk] = R(S.mz[c + g.sk]);
             Fcons[c] = R(-1.0 / 1.0 * ((S.mx[cidx(g, ip, j, k)] - S.mx[c]) * g.dxi +
                                        (S.my[cidx(g, i, jp, k)] - S.my[c]) * g.dyi + (S.mz[c + g.sk] - S.mz[c]) * g.dzi));
-            if (P.use_diff) frt -= scalar_diff<R>(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
+            if (P.les == ERF_LES_MLP) {
+                // divergence of the learned heat flux rho*q (cell values
+                // averaged to faces; no flux through the walls)
+                const int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
+                auto fz = [&](int kk) {
+                    if (kk <= 0 || kk >= g.nz) return R(0);
+                    return R(0.5) * (hz[cidx(g, i, j, kk - 1)] + hz[cidx(g, i, j, kk)]);
+                };
+                R fxl = R(0.5) * (hx[cidx(g, im, j, k)] + hx[c]), fxh = R(0.5) * (hx[c] + hx[cidx(g, ip, j, k)]);
+                R fyl = R(0.5) * (hy[cidx(g, i, jm, k)] + hy[c]), fyh = R(0.5) * (hy[c] + hy[cidx(g, i, jp, k)]);
+                frt -= (fxh - fxl) * R(g.dxi) + (fyh - fyl) * R(g.dyi) + (fz(k + 1) - fz(k)) * R(g.dzi);
+            } else if (P.use_diff) {
+                frt -= scalar_diff<R>(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
+            }
             Fcons[g.ncell + c] = frt;
         }
         __syncthreads();
@@ -1395,7 +1421,7 @@ dim3 cell_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.n
 constexpr int U5 = ERF_ADV_UPWIND_5TH, W5 = ERF_ADV_WENO_5;
 
 template <class R>
-using SlowCellK = void (*)(Params, int, StateBuf, StageAux<R>, const R*, R*, R*, R*, R*);
+using SlowCellK = void (*)(Params, int, StateBuf, StageAux<R>, const R*, const R*, const R*, const R*, R*, R*, R*, R*);
 template <class R>
 using SlowMomK = void (*)(Params, int, StateBuf, StageAux<R>, const double*, const double*, const double*, const R*,
                           const R*, const R*, const R*, const R*, const R*, const double*, R*, R*, R*);
@@ -1452,6 +1478,10 @@ void launch_step_begin(const Params& P, cudaStream_t st, const double* cons, con
     k_step_begin<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, uo, vo, wo, S, un, vn, wn, A, mut);
 }
 template <class R>
+void launch_stage_aux(const Params& P, cudaStream_t st, const double* cons, StageAux<R> A) {
+    k_stage_aux<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, A);
+}
+template <class R>
 void launch_tau(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
                 const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23) {
     k_tau<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, u, v, w, mut, t11, t22, t33, t12, t13, t23);
@@ -1483,9 +1513,9 @@ void launch_fast_vert(const Params& P, cudaStream_t st, dim3 grid, dim3 block, s
 }
 template <class R>
 void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const R* mut,
-                      R* Fcons, R* avx, R* avy, R* avz) {
-    slow_cell_kernel<R>(P)<<<tile_grid(P.g, t.cell), dim3(TTX, TTY, 1), 0, st>>>(P, t.cell, S, A, mut, Fcons, avx,
-                                                                                  avy, avz);
+                      const R* hx, const R* hy, const R* hz, R* Fcons, R* avx, R* avy, R* avz) {
+    slow_cell_kernel<R>(P)<<<tile_grid(P.g, t.cell), dim3(TTX, TTY, 1), 0, st>>>(P, t.cell, S, A, mut, hx, hy, hz,
+                                                                                  Fcons, avx, avy, avz);
 }
 template <class R>
 void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
@@ -1511,6 +1541,7 @@ void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow
     template void launch_tau<R>(const Params&, cudaStream_t, const double*, const double*, const double*,            \
                                 const double*, const R*, R*, R*, R*, R*, R*, R*);                                    \
     template void launch_plane_avg<R>(const Params&, cudaStream_t, const double*, const R*, double*);                \
+    template void launch_stage_aux<R>(const Params&, cudaStream_t, const double*, StageAux<R>);                      \
     template void launch_fast_h<R>(const Params&, cudaStream_t, int, int, double, double, StateBuf, int, StateBuf,   \
                                    StageAux<R>, const R*, const R*, const R*, R*, R*, R*, double*, double*);         \
     template void launch_fast_coef<R>(const Params&, cudaStream_t, dim3, dim3, size_t, double, StateBuf,             \
@@ -1520,7 +1551,7 @@ void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow
                                       const double*, const double*, const R*, const R*, const R*, const R*,          \
                                       const R*, R*, double*, double*);                                               \
     template void launch_slow_cell<R>(const Params&, const TiledKz&, cudaStream_t, StateBuf, StageAux<R>, const R*,  \
-                                      R*, R*, R*, R*);                                                               \
+                                      const R*, const R*, const R*, R*, R*, R*, R*);                                 \
     template void launch_slow_mom<R>(const Params&, const TiledKz&, cudaStream_t, StateBuf, StageAux<R>,             \
                                      const double*, const double*, const double*, const R*, const R*, const R*,      \
                                      const R*, const R*, const R*, const double*, R*, R*, R*);                       \

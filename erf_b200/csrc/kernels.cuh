@@ -63,6 +63,8 @@ template <class R>
 void launch_tau(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
                 const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23);
 template <class R>
+void launch_stage_aux(const Params& P, cudaStream_t st, const double* cons, StageAux<R> A);
+template <class R>
 void launch_plane_avg(const Params& P, cudaStream_t st, const double* cons, const R* prim, double* avg);
 template <class R>
 void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double dtau, double facinv, StateBuf Sprev,
@@ -79,7 +81,25 @@ void launch_fast_vert(const Params& P, cudaStream_t st, dim3 grid, dim3 block, s
                       double* out_mz);
 template <class R>
 void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const R* mut,
-                      R* Fcons, R* avx, R* avy, R* avz);
+                      const R* hx, const R* hy, const R* hz, R* Fcons, R* avx, R* avy, R* avz);
+
+// Learned closure (closure.cu): network arrays on the device, the fused
+// stress / heat-flux kernel with its edge averaging, and feature extraction.
+struct ClosureNet {
+    const unsigned char* wpack;
+    const float* bias;
+    const float* norm;   // in mean[13], in std[13], out mean[9], out std[9]
+    const float* env;    // lo[13], hi[13]
+    unsigned int* fallback;
+};
+template <class R>
+void launch_closure(const Params& P, const ClosureNet& net, int grid, cudaStream_t st, const double* cons,
+                    const double* u, const double* v, const double* w, const R* theta, R* t11, R* t22, R* t33, R* c12,
+                    R* c13, R* c23, R* t12, R* t13, R* t23, R* hx, R* hy, R* hz);
+template <class R>
+int closure_grid(const Params& P);
+void launch_features(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
+                     const double* w, double* theta_scratch, float* out);
 template <class R>
 void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
                      const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,

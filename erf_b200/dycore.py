@@ -27,6 +27,9 @@ EXPORTS = [
     "erf_b200_advance", "erf_b200_advance_host", "erf_b200_turbulent_viscosity", "erf_b200_slow_rhs_pre",
     "erf_b200_make_fast_coeffs", "erf_b200_fast_rhs_N", "erf_b200_slow_rhs_post", "erf_b200_kessler_advance",
     "erf_b200_advance_profiled", "erf_b200_kernels_per_step", "erf_b200_kessler_advance_noalloc",
+    "erf_b200_mlp_num_params", "erf_b200_mlp_create", "erf_b200_mlp_destroy", "erf_b200_mlp_set_params",
+    "erf_b200_mlp_get_params", "erf_b200_mlp_set_normalization", "erf_b200_mlp_gradient", "erf_b200_mlp_train",
+    "erf_b200_mlp_infer", "erf_b200_set_closure", "erf_b200_closure_fallbacks", "erf_b200_closure_features_host",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs"]
@@ -70,6 +73,9 @@ def load_library():
                                             ctypes.POINTER(ctypes.c_int), i]
     L.erf_b200_kernels_per_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.erf_b200_kessler_advance_noalloc.argtypes = [vp, fabp, ctypes.c_double, vp]
+    L.erf_b200_set_closure.argtypes = [vp, vp]
+    L.erf_b200_closure_fallbacks.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.erf_b200_closure_features_host.argtypes = [vp, dp, dp, dp, dp, dp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -173,6 +179,25 @@ class Dycore:
         fw = dense_fab(w_t, 3, c.nx, c.ny, c.nz)
         _check(self.lib.erf_b200_advance(self._ctx, ctypes.byref(fc), ctypes.byref(fu), ctypes.byref(fv),
                                          ctypes.byref(fw), int(nsteps)), "advance")
+
+    def set_closure(self, net):
+        """Attach a trained erf_b200.closure.MLP (les_type MLP contexts)."""
+        _check(self.lib.erf_b200_set_closure(self._ctx, net.h), "set_closure")
+        self._net = net
+
+    def closure_fallbacks(self) -> int:
+        n = ctypes.c_ulonglong()
+        _check(self.lib.erf_b200_closure_fallbacks(self._ctx, ctypes.byref(n)), "closure_fallbacks")
+        return n.value
+
+    def closure_features(self, cons, u, v, w):
+        """The 13 closure features of every cell of a dense host state: [nz*ny*nx][13] float32."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (cons, u, v, w)]
+        c = self.cfg
+        out = np.zeros((c.nx * c.ny * c.nz, 13), dtype=np.float32)
+        _check(self.lib.erf_b200_closure_features_host(self._ctx, *[a.ctypes.data for a in arrs], out.ctypes.data),
+               "closure_features")
+        return out
 
     def kernels_per_step(self) -> int:
         n = ctypes.c_int()

@@ -67,6 +67,9 @@ extern "C" {
 #define ERF_LES_NONE         0
 #define ERF_LES_SMAGORINSKY  1
 #define ERF_LES_DEARDORFF    2
+/* Learned closure (no reference counterpart): the erf_b200_mlp network of
+ * erf_b200_set_closure, with Smagorinsky outside its training envelope. */
+#define ERF_LES_MLP          3
 
 /* MolecDiffType (Source/DataStructs/ERF_DiffStruct.H) */
 #define ERF_MOLEC_NONE           0
@@ -310,6 +313,52 @@ int erf_b200_kessler_advance(erf_b200_ctx* ctx, const erf_b200_fab* cons, double
 int erf_b200_kessler_advance_noalloc(const erf_b200_config* cfg,
                                      const erf_b200_fab* cons, double dt,
                                      void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned subgrid closure (no reference counterpart; ERF's closures are
+ * ComputeTurbulentViscosity.cpp's Smagorinsky / Deardorff).  A 13-64-64-64-9
+ * GELU network in BF16 on the tcgen05 tensor cores (FP32 accumulation) maps
+ * the 9 resolved velocity-gradient components (du/dx du/dy du/dz dv/dx ...
+ * dw/dz), the 3 potential-temperature gradient components and the filter
+ * width to the 6 kinematic subgrid stresses (11 22 33 12 13 23) and the 3
+ * subgrid heat fluxes (x y z).  Parameters are NPAR FP32 values in the padded
+ * layout W1[64][16] W2[64][64] W3[64][64] W4[16][64] b1 b2 b3 b4[16].
+ * Training and inference arrays are device pointers, row-major.
+ * ------------------------------------------------------------------------ */
+typedef struct erf_b200_mlp erf_b200_mlp;
+
+int erf_b200_mlp_num_params(void);
+int erf_b200_mlp_create(erf_b200_mlp** out, void* stream);
+int erf_b200_mlp_destroy(erf_b200_mlp* m);
+/* host_params: NPAR floats; resets the optimiser state. */
+int erf_b200_mlp_set_params(erf_b200_mlp* m, const float* host_params);
+int erf_b200_mlp_get_params(erf_b200_mlp* m, float* host_params);
+/* Feature / target normalisation (host arrays: 13, 13, 9, 9) and the
+ * training envelope of the raw features (13 + 13, may be NULL). */
+int erf_b200_mlp_set_normalization(erf_b200_mlp* m, const float* in_mean, const float* in_std,
+                                   const float* out_mean, const float* out_std,
+                                   const float* in_lo, const float* in_hi);
+/* Loss sum((y-t)^2)/(9n) and its gradient (NPAR floats to host_grad) for
+ * normalised inputs xn[n][13] and targets tn[n][9]. */
+int erf_b200_mlp_gradient(erf_b200_mlp* m, const float* xn, const float* tn, int n,
+                          float* host_grad, float* host_loss);
+/* iters Adam steps (lr) over consecutive minibatches of `batch` rows. */
+int erf_b200_mlp_train(erf_b200_mlp* m, const float* xn, const float* tn, int n, int batch,
+                       int iters, float lr, float* host_loss);
+/* y[n][9] (raw units) from x[n][13] (raw units). */
+int erf_b200_mlp_infer(erf_b200_mlp* m, const float* x, int n, float* y);
+
+/* Attach a trained network to a context created with les_type ERF_LES_MLP
+ * (the step graphs are built here; advancing before it returns
+ * ERF_B200_EBADSTATE).  The network must outlive the context's use of it. */
+int erf_b200_set_closure(erf_b200_ctx* ctx, const erf_b200_mlp* m);
+/* Cells that fell back to Smagorinsky since the last call (reset on read). */
+int erf_b200_closure_fallbacks(erf_b200_ctx* ctx, unsigned long long* count);
+/* The 13 closure features of every cell (cell order i fastest) of a state
+ * given as host arrays in the erf_b200_advance_host layout; features is a
+ * host array of 13*nx*ny*nz floats. */
+int erf_b200_closure_features_host(erf_b200_ctx* ctx, const double* cons, const double* u, const double* v,
+                                   const double* w, float* features);
 
 #ifdef __cplusplus
 }
