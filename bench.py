@@ -146,6 +146,32 @@ def replica_throughput(world, n_cells, steps, seconds):
     return world * n_cells * steps / seconds
 
 
+CLOSURE_MODEL = os.path.join(ROOT, "erf_b200", "data", "closure_abl.npz")
+
+
+def learned_arm(measure, form_error, C):
+    """The learned closure on the coarse ABL grid it was trained for
+    (128 x 128 x 32, dx = dz = 40 m): plain FP64 with Smagorinsky, FP64 with
+    the network, and the mixed form with the network; the mixed form's error
+    is taken against FP64 with the same network after 100 steps."""
+    if not os.path.exists(CLOSURE_MODEL):
+        return {"unavailable": "no trained closure model (python -m erf_b200.closure --out ...)"}
+    from erf_b200.closure import coarse_case, load_closure
+    net = load_closure(CLOSURE_MODEL)
+    mk = lambda: coarse_case(cases.abl_fine(nx=512, ny=512, nz=128), 4)
+    smag, _, _ = measure(C.PREC_FP64, None, case=mk(), les=C.LES_SMAGORINSKY, light=True)
+    l64, base, init = measure(C.PREC_FP64, None, case=mk(), net=net, les=C.LES_MLP, light=True)
+    l32, _, _ = measure(C.PREC_MIXED, None, case=mk(), net=net, les=C.LES_MLP, light=True)
+    ce = mk()
+    ce.cfg.les_type = C.LES_MLP
+    err = form_error(base, init, 100, case=ce, net=net)
+    net.close()
+    return {"workload": "abl coarse 128x128x32, dx=dz=40 m, dt=0.32 s, learned closure (tcgen05 BF16 MLP)",
+            "fp64_smagorinsky": smag, "fp64_learned": l64, "mixed_learned": l32,
+            "speedup_mixed_learned_vs_fp64_smagorinsky": l32["value"] / smag["value"],
+            "rel_l2_mixed_vs_fp64_learned_after_100_steps": err}
+
+
 def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
     """Time the FP64 CPU oracle on a bounded sample of the workload."""
     import oracle
@@ -238,13 +264,21 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def measure(precision, clocks):
+    def measure(precision, clocks, case=case, net=None, les=None, light=False):
         """Time one precision form: graph replay (device-resident state),
-        eager per-kernel events, and end to end through the host entry point."""
+        eager per-kernel events, and end to end through the host entry point
+        (graph replay only when light)."""
+        cfg = case.cfg
+        n_cells = cfg.nx * cfg.ny * cfg.nz
+        vals = algorithmic_values_per_cell(cfg)
         cfg.precision = precision
+        if les is not None:
+            cfg.les_type = les
         dy = Dycore(cfg, stream=stream.cuda_stream)
         base = dy.make_base_state(case)
         dy.set_base_state(base)
+        if net is not None:
+            dy.set_closure(net)
         cons, u, v, w = case.build_state(base[0])
         dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (cons, u, v, w)]
         torch.cuda.synchronize()
@@ -270,6 +304,12 @@ def main():
         ms = max_over_ranks(ms, world, "cuda")
         st = dy.status()
         value = replica_throughput(world, n_cells, args.steps, ms * 1e-3)
+        if light:
+            out = {"value": value, "ms_per_step": ms / args.steps, "status": st}
+            if net is not None:
+                out["fallback_cells_per_step"] = dy.closure_fallbacks() / max(args.warmup + args.steps, 1)
+            dy.close()
+            return out, base, (cons, u, v, w)
         # ---- timed region 2: same K steps, eager launches with per-kernel events
         barrier()
         prof = dy.advance_profiled(*dev, args.steps)
@@ -319,14 +359,17 @@ def main():
         dy.close()
         return out, base, (cons, u, v, w)
 
-    def form_error(base, init, nsteps):
+    def form_error(base, init, nsteps, case=case, net=None):
         """Per-field relative L2 of the mixed form against the plain FP64 form
         (parity-pinned to the oracle) after nsteps from the same state."""
+        cfg = case.cfg
         res = {}
         for prec in (C.PREC_FP64, C.PREC_MIXED):
             cfg.precision = prec
             dy = Dycore(cfg, stream=stream.cuda_stream)
             dy.set_base_state(base)
+            if net is not None:
+                dy.set_closure(net)
             dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in init]
             dy.advance(*dev, nsteps)
             torch.cuda.synchronize()
@@ -361,6 +404,7 @@ def main():
     mixed, _, _ = measure(C.PREC_MIXED, None)
     mixed_err = form_error(base, init, 100) if rank == 0 else None
     cfg.precision = C.PREC_FP64
+    learned = learned_arm(measure, form_error, C) if rank == 0 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -390,6 +434,7 @@ def main():
                       "kernels": {k: {"ms_per_launch": v["ms_per_launch"], "gbs": v["gbs"]}
                                   for k, v in mixed["kernels"].items()},
                       "rel_l2_vs_fp64_after_100_steps": mixed_err, "status": mixed["status"]},
+            "learned": learned,
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clock_samples),
             "gpu_launches": plain["launches"],

@@ -72,7 +72,9 @@ struct erf_b200_ctx {
     bool base_set = false;
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraph_t graph_raw[2] = {nullptr, nullptr};   // kept for ensemble graphs
     int lag_parity_per_step = 0;
+    int cur = -1;             // slot of the resident state (-1: none loaded)
 };
 
 namespace {
@@ -331,10 +333,20 @@ int build_graphs(erf_b200_ctx* c) {
         enqueue_step(c, p);
         CK(cudaStreamEndCapture(c->stream, &gr));
         cudaError_t e = cudaGraphInstantiate(&c->graph[p], gr, 0);
-        cudaGraphDestroy(gr);
+        if (c->graph_raw[p]) cudaGraphDestroy(c->graph_raw[p]);
+        c->graph_raw[p] = gr;
         CK(e);
     }
     return ERF_B200_OK;
+}
+
+void drop_graphs(erf_b200_ctx* c) {
+    for (int p = 0; p < 2; ++p) {
+        if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
+        if (c->graph_raw[p]) cudaGraphDestroy(c->graph_raw[p]);
+        c->graph[p] = nullptr;
+        c->graph_raw[p] = nullptr;
+    }
 }
 
 bool fab_ok(const erf_b200_fab* f, int kind, const Geo& g, int ncomp) {
@@ -467,7 +479,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
 int erf_b200_destroy(erf_b200_ctx* c) {
     if (!c) return ERF_B200_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (int p = 0; p < 2; ++p) if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
+    drop_graphs(c);
     for (void* q : c->allocs) cudaFree(q);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -534,6 +546,7 @@ int erf_b200_advance(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_f
     if ((rc = pack(c, yvel, 2, 1, c->vel[0][1]))) return rc;
     if ((rc = pack(c, zvel, 3, 1, c->vel[0][2]))) return rc;
     if (!c->graph[0] || !c->graph[1]) return ERF_B200_EBADSTATE;   // learned closure not attached
+    c->cur = -1;
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph[s & 1], c->stream));
     int p = nsteps & 1;
     if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[p].cons))) return rc;
@@ -845,8 +858,7 @@ int erf_b200_kessler_advance(erf_b200_ctx* c, const erf_b200_fab* cons, double d
 int erf_b200_set_closure(erf_b200_ctx* c, const erf_b200_mlp* m) {
     if (!c || !m || c->P.les != ERF_LES_MLP) return ERF_B200_EINVAL;
     CK(cudaStreamSynchronize(c->stream));
-    for (int p = 0; p < 2; ++p)
-        if (c->graph[p]) { cudaGraphExecDestroy(c->graph[p]); c->graph[p] = nullptr; }
+    drop_graphs(c);
     c->net = m;
     int rc = build_graphs(c);
     if (rc) return rc;
@@ -902,6 +914,198 @@ int erf_b200_closure_features_host(erf_b200_ctx* c, const double* cons, const do
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(features, c->feat_out, N * 13 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return ERF_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Resident state, ensembles and autotuning (no reference counterpart: the
+// reference advances one level of one domain per call).
+// ---------------------------------------------------------------------------
+int erf_b200_load_state(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                        const erf_b200_fab* yvel, const erf_b200_fab* zvel) {
+    if (!c || !c->base_set) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
+        return ERF_B200_EINVAL;
+    int rc;
+    if ((rc = pack(c, cons, 0, c->cfg.ncomp, c->S[0].cons))) return rc;
+    if ((rc = pack(c, xvel, 1, 1, c->vel[0][0])) || (rc = pack(c, yvel, 2, 1, c->vel[0][1])) ||
+        (rc = pack(c, zvel, 3, 1, c->vel[0][2])))
+        return rc;
+    c->cur = 0;
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_store_state(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                         const erf_b200_fab* yvel, const erf_b200_fab* zvel) {
+    if (!c) return ERF_B200_EINVAL;
+    if (c->cur < 0) return ERF_B200_EBADSTATE;
+    const Geo& g = c->g;
+    if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
+        return ERF_B200_EINVAL;
+    int p = c->cur, rc;
+    if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[p].cons))) return rc;
+    if ((rc = unpack(c, xvel, 1, 1, c->vel[p][0])) || (rc = unpack(c, yvel, 2, 1, c->vel[p][1])) ||
+        (rc = unpack(c, zvel, 3, 1, c->vel[p][2])))
+        return rc;
+    return cuda_fail(cudaGetLastError());
+}
+
+int erf_b200_advance_resident(erf_b200_ctx* c, int nsteps) {
+    if (!c || nsteps < 0) return ERF_B200_EINVAL;
+    if (c->cur < 0 || !c->graph[0] || !c->graph[1]) return ERF_B200_EBADSTATE;
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaGraphLaunch(c->graph[c->cur], c->stream));
+        c->cur ^= 1;
+    }
+    return ERF_B200_OK;
+}
+
+// Runtime launch shapes of one context, chosen by timing candidate shapes on
+// the resident state.  Every trial recomputes the step from the resident slot
+// (a step reads only that slot's state and velocities and writes the other
+// slots), so the resident state is left unchanged.  Coordinate search over
+// the vertical solver's threads per block, the coefficient kernel's warps and
+// the levels per block of the three tiled transport kernels.
+int erf_b200_autotune(erf_b200_ctx* c, int reps, double* best_ms) {
+    if (!c || reps < 1) return ERF_B200_EINVAL;
+    if (c->cur < 0 || (c->P.les == ERF_LES_MLP && !c->net)) return ERF_B200_EBADSTATE;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int p = c->cur;
+    auto trial = [&](float& ms) -> int {
+        drop_graphs(c);
+        int rc = build_graphs(c);
+        if (rc) return rc;
+        CK(cudaGraphLaunch(c->graph[p], c->stream));
+        CK(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(c->graph[p], c->stream));
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        ms /= reps;
+        return ERF_B200_OK;
+    };
+    float best = 0.f;
+    int rc = trial(best);
+    const int nz = c->cfg.nz;
+    for (int threads : {256, 512, 1024}) {
+        int vw = threads / c->tile_tx;
+        if (rc || vw < 1 || vw == c->vert_warps) continue;
+        int keep = c->vert_warps;
+        c->vert_warps = vw;
+        float ms;
+        if ((rc = trial(ms))) break;
+        if (ms < best) best = ms; else c->vert_warps = keep;
+    }
+    for (int cw : {4, 8, 16}) {
+        if (rc || cw == c->coef_warps || cw * c->tile_tx > 1024) continue;
+        int keep = c->coef_warps;
+        c->coef_warps = cw;
+        float ms;
+        if ((rc = trial(ms))) break;
+        if (ms < best) best = ms; else c->coef_warps = keep;
+    }
+    int* kz[3] = {&c->tkz.cell, &c->tkz.mom, &c->tkz.post};
+    for (int q = 0; q < 3 && !rc; ++q) {
+        const int k0 = *kz[q];
+        for (int cand : {k0 / 2, k0 * 2, k0 * 3 / 2}) {
+            if (cand < 1 || cand > nz || cand == *kz[q]) continue;
+            int keep = *kz[q];
+            *kz[q] = cand;
+            float ms;
+            if ((rc = trial(ms))) break;
+            if (ms < best) best = ms; else *kz[q] = keep;
+        }
+    }
+    drop_graphs(c);
+    int rc2 = build_graphs(c);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_ms) *best_ms = best;
+    return rc ? rc : rc2;
+}
+
+}  // extern "C"
+
+// An ensemble of contexts advanced by one CUDA graph per step whose child
+// graphs are the members' step graphs (independent nodes, so members of
+// different sizes run concurrently).  Members hold resident states at the
+// same slot parity.
+struct erf_b200_ensemble {
+    std::vector<erf_b200_ctx*> m;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int parity = 0;
+};
+
+extern "C" {
+
+int erf_b200_ensemble_destroy(erf_b200_ensemble* e) {
+    if (!e) return ERF_B200_OK;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (int p = 0; p < 2; ++p) if (e->exec[p]) cudaGraphExecDestroy(e->exec[p]);
+    if (e->own_stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return ERF_B200_OK;
+}
+
+int erf_b200_ensemble_create(erf_b200_ensemble** out, erf_b200_ctx* const* members, int n, void* stream) {
+    if (!out || !members || n < 1) return ERF_B200_EINVAL;
+    *out = nullptr;
+    int parity = members[0] ? members[0]->cur : -1;
+    for (int q = 0; q < n; ++q) {
+        erf_b200_ctx* c = members[q];
+        if (!c || c->cur < 0 || c->cur != parity || !c->graph_raw[0] || !c->graph_raw[1]) return ERF_B200_EBADSTATE;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    erf_b200_ensemble* e = new (std::nothrow) erf_b200_ensemble();
+    if (!e) return ERF_B200_ENOMEM;
+    e->m.assign(members, members + n);
+    e->parity = parity;
+    if (stream) {
+        e->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) { delete e; return ERF_B200_ECUDA; }
+        e->own_stream = true;
+    }
+    for (int p = 0; p < 2; ++p) {
+        cudaGraph_t g;
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) { erf_b200_ensemble_destroy(e); return ERF_B200_ECUDA; }
+        cudaError_t err = cudaSuccess;
+        for (int q = 0; q < n && err == cudaSuccess; ++q) {
+            cudaGraphNode_t node;
+            err = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, members[q]->graph_raw[p]);
+        }
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&e->exec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (err != cudaSuccess) { erf_b200_ensemble_destroy(e); return cuda_fail(err); }
+    }
+    *out = e;
+    return ERF_B200_OK;
+}
+
+// nsteps steps of every member, one graph launch per step on the ensemble's
+// stream; the members' resident states advance.
+int erf_b200_ensemble_advance(erf_b200_ensemble* e, int nsteps) {
+    if (!e || nsteps < 0) return ERF_B200_EINVAL;
+    for (erf_b200_ctx* c : e->m)
+        if (c->cur != e->parity) return ERF_B200_EBADSTATE;
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaGraphLaunch(e->exec[e->parity], e->stream));
+        e->parity ^= 1;
+    }
+    for (erf_b200_ctx* c : e->m) c->cur = e->parity;
+    return ERF_B200_OK;
+}
+
+// Wait for the ensemble's work (before store_state or status reads on the
+// members' own streams).
+int erf_b200_ensemble_sync(erf_b200_ensemble* e) {
+    if (!e) return ERF_B200_EINVAL;
+    CK(cudaStreamSynchronize(e->stream));
     return ERF_B200_OK;
 }
 

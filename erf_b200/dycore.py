@@ -30,6 +30,8 @@ EXPORTS = [
     "erf_b200_mlp_num_params", "erf_b200_mlp_create", "erf_b200_mlp_destroy", "erf_b200_mlp_set_params",
     "erf_b200_mlp_get_params", "erf_b200_mlp_set_normalization", "erf_b200_mlp_gradient", "erf_b200_mlp_train",
     "erf_b200_mlp_infer", "erf_b200_set_closure", "erf_b200_closure_fallbacks", "erf_b200_closure_features_host",
+    "erf_b200_load_state", "erf_b200_store_state", "erf_b200_advance_resident", "erf_b200_autotune",
+    "erf_b200_ensemble_create", "erf_b200_ensemble_advance", "erf_b200_ensemble_sync", "erf_b200_ensemble_destroy",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs"]
@@ -76,6 +78,14 @@ def load_library():
     L.erf_b200_set_closure.argtypes = [vp, vp]
     L.erf_b200_closure_fallbacks.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.erf_b200_closure_features_host.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.erf_b200_load_state.argtypes = [vp, fabp, fabp, fabp, fabp]
+    L.erf_b200_store_state.argtypes = [vp, fabp, fabp, fabp, fabp]
+    L.erf_b200_advance_resident.argtypes = [vp, i]
+    L.erf_b200_autotune.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double)]
+    L.erf_b200_ensemble_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), i, vp]
+    L.erf_b200_ensemble_advance.argtypes = [vp, i]
+    L.erf_b200_ensemble_sync.argtypes = [vp]
+    L.erf_b200_ensemble_destroy.argtypes = [vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -101,6 +111,29 @@ def dense_fab(t, kind: int, nx: int, ny: int, nz: int, ncomp: int = 1) -> ErfFab
     f.nstride = f.kstride * (hz + 1)
     f.ncomp = ncomp
     return f
+
+
+class Ensemble:
+    """Contexts with resident states advanced by one CUDA graph per step."""
+
+    def __init__(self, members, stream=None):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.ctx.value for m in self.members])
+        self.h = ctypes.c_void_p()
+        _check(self.lib.erf_b200_ensemble_create(ctypes.byref(self.h), arr, len(self.members), stream),
+               "ensemble_create")
+
+    def advance(self, nsteps: int):
+        _check(self.lib.erf_b200_ensemble_advance(self.h, int(nsteps)), "ensemble_advance")
+
+    def sync(self):
+        _check(self.lib.erf_b200_ensemble_sync(self.h), "ensemble_sync")
+
+    def close(self):
+        if self.h:
+            self.lib.erf_b200_ensemble_destroy(self.h)
+            self.h = ctypes.c_void_p()
 
 
 class Dycore:
@@ -198,6 +231,38 @@ class Dycore:
         _check(self.lib.erf_b200_closure_features_host(self._ctx, *[a.ctypes.data for a in arrs], out.ctypes.data),
                "closure_features")
         return out
+
+    def load_state(self, cons, u, v, w):
+        """Make a dense host state resident on the device (graph steps then
+        advance it in place: advance_resident, Ensemble)."""
+        import torch
+        self._res = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda() for a in (cons, u, v, w)]
+        torch.cuda.synchronize()
+        c = self.cfg
+        f = [dense_fab(self._res[0], 0, c.nx, c.ny, c.nz, c.ncomp)] + \
+            [dense_fab(self._res[q], q, c.nx, c.ny, c.nz) for q in (1, 2, 3)]
+        _check(self.lib.erf_b200_load_state(self._ctx, *[ctypes.byref(x) for x in f]), "load_state")
+        _check(self.lib.erf_b200_get_status(self._ctx), "load_state sync")
+
+    def store_state(self, cons, u, v, w):
+        """Copy the resident state into new dense host arrays shaped like the given ones."""
+        import torch
+        out = [torch.zeros(np.shape(a), dtype=torch.float64, device="cuda") for a in (cons, u, v, w)]
+        torch.cuda.synchronize()
+        c = self.cfg
+        f = [dense_fab(out[0], 0, c.nx, c.ny, c.nz, c.ncomp)] + [dense_fab(out[q], q, c.nx, c.ny, c.nz) for q in (1, 2, 3)]
+        _check(self.lib.erf_b200_store_state(self._ctx, *[ctypes.byref(x) for x in f]), "store_state")
+        _check(self.lib.erf_b200_get_status(self._ctx), "store_state sync")
+        return tuple(t.cpu().numpy() for t in out)
+
+    def advance_resident(self, nsteps: int):
+        _check(self.lib.erf_b200_advance_resident(self._ctx, int(nsteps)), "advance_resident")
+
+    def autotune(self, reps: int = 3) -> float:
+        """Tune the launch shapes on the resident state; returns the tuned step time (ms)."""
+        ms = ctypes.c_double()
+        _check(self.lib.erf_b200_autotune(self._ctx, int(reps), ctypes.byref(ms)), "autotune")
+        return ms.value
 
     def kernels_per_step(self) -> int:
         n = ctypes.c_int()

@@ -348,6 +348,29 @@ int erf_b200_mlp_train(erf_b200_mlp* m, const float* xn, const float* tn, int n,
 /* y[n][9] (raw units) from x[n][13] (raw units). */
 int erf_b200_mlp_infer(erf_b200_mlp* m, const float* x, int n, float* y);
 
+/* ------------------------------------------------------------------------
+ * Resident state, autotuning and ensembles (no reference counterpart).
+ * ------------------------------------------------------------------------ */
+/* Load a state into the context; it stays on the device between calls. */
+int erf_b200_load_state(erf_b200_ctx* ctx, const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                        const erf_b200_fab* yvel, const erf_b200_fab* zvel);
+/* Copy the resident state out. */
+int erf_b200_store_state(erf_b200_ctx* ctx, const erf_b200_fab* cons, const erf_b200_fab* xvel,
+                         const erf_b200_fab* yvel, const erf_b200_fab* zvel);
+/* Advance the resident state nsteps steps (one graph launch per step). */
+int erf_b200_advance_resident(erf_b200_ctx* ctx, int nsteps);
+/* Pick the context's launch shapes by timing candidates on the resident
+ * state (which is left unchanged); best_ms receives the tuned step time. */
+int erf_b200_autotune(erf_b200_ctx* ctx, int reps, double* best_ms);
+
+typedef struct erf_b200_ensemble erf_b200_ensemble;
+/* An ensemble of contexts holding resident states (any sizes); one CUDA
+ * graph per step runs every member's step graph, members concurrently. */
+int erf_b200_ensemble_create(erf_b200_ensemble** out, erf_b200_ctx* const* members, int n, void* stream);
+int erf_b200_ensemble_advance(erf_b200_ensemble* e, int nsteps);
+int erf_b200_ensemble_sync(erf_b200_ensemble* e);
+int erf_b200_ensemble_destroy(erf_b200_ensemble* e);
+
 /* Attach a trained network to a context created with les_type ERF_LES_MLP
  * (the step graphs are built here; advancing before it returns
  * ERF_B200_EBADSTATE).  The network must outlive the context's use of it. */

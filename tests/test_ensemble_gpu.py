@@ -1,0 +1,63 @@
+"""GPU: resident states, the autotuner and the ensemble graph.
+
+* an ensemble of members of different sizes advanced by one graph launch
+  per step gives bit-identical states to advancing each member alone;
+* autotuning (which re-times candidate launch shapes on the resident state)
+  leaves the resident state unchanged and the tuned step bit-identical.
+"""
+import numpy as np
+import pytest
+
+from erf_b200 import cases, config as C
+
+pytestmark = pytest.mark.gpu
+
+
+def _member(nx, ny, nz, ug, seed, precision=C.PREC_FP64):
+    from erf_b200 import Dycore
+    case = cases.abl_dry(nx=nx, ny=ny, nz=nz, seed=seed)
+    C.set_coriolis(case.cfg, rotational_time_period=4.0 * np.pi / 1.0e-4, latitude_deg=90.0, geo_wind=(ug, 0.0, 0.0))
+    case.cfg.precision = precision
+    dy = Dycore(case.cfg)
+    base = dy.make_base_state(case)
+    dy.set_base_state(base)
+    return dy, case.build_state(base[0])
+
+
+def test_ensemble_matches_members_alone():
+    from erf_b200.dycore import Ensemble
+    specs = [(32, 32, 16, 6.0, 1), (48, 40, 24, 12.0, 2), (24, 24, 20, 9.0, 3)]
+    alone = []
+    for s in specs:
+        dy, st = _member(*s)
+        alone.append(dy.advance_host(*st, 3))
+        dy.close()
+    members = [_member(*s) for s in specs]
+    for dy, st in members:
+        dy.load_state(*st)
+    ens = Ensemble([dy for dy, _ in members])
+    ens.advance(3)
+    ens.sync()
+    for (dy, st), ref in zip(members, alone):
+        got = dy.store_state(*st)
+        assert dy.status() == 0
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)
+    ens.close()
+    for dy, _ in members:
+        dy.close()
+
+
+@pytest.mark.parametrize("precision", [C.PREC_FP64, C.PREC_MIXED])
+def test_autotune_keeps_results(precision):
+    dy, st = _member(64, 48, 32, 10.0, 4, precision)
+    ref = dy.advance_host(*st, 2)
+    dy.load_state(*st)
+    ms = dy.autotune(3)
+    assert ms > 0
+    dy.advance_resident(2)
+    got = dy.store_state(*st)
+    assert dy.status() == 0
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+    dy.close()
