@@ -270,7 +270,8 @@ __device__ __forceinline__ R scalar_diff(const Params& P, const double* __restri
 }
 
 // Horizontal plane averages of rho, theta, qv, qc, qp for buoyancy type 2
-// (SourceTerms/ERF_make_buoyancy.cpp:212-249): one block per level, FP64 sums.
+// (SourceTerms/ERF_make_buoyancy.cpp:212-249): one block per level, FP64 sums;
+// also the temperature of the mean state of each level.
 template <class R>
 __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* __restrict__ prim,
                             double* __restrict__ avg) {
@@ -296,8 +297,11 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* 
             for (int q = 0; q < 5; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
         for (int q = 0; q < 5; ++q) avg[q * g.nz + k] = sh[q][0];
+        // the plane-mean temperature used by make_buoyancy's type 2
+        avg[5 * g.nz + k] = eos_T(sh[0][0], sh[0][0] * sh[1][0], sh[2][0]);
+    }
 }
 
 // Momentum flux helpers: interpolated face velocity (FP64 state) in R
@@ -942,19 +946,70 @@ struct FluxTile {
     R fy[TTY + 1][TTX];
 };
 
-// Fluxes of one scalar for cell (i,j,k): x/y into the tile, z through zl/zh
-// (zl is computed only on the block's first level; otherwise it is the
-// carried top flux of the level below).
+// One level of a scalar over the block's tile plus a 3-cell halo on every
+// side (periodic in x and y), staged in shared memory so that the x and y
+// stencils read it at fixed offsets.
+constexpr int PH = 3;   // halo width (Upwind_5th / WENO5 stencils)
+template <class R>
+struct Plane {
+    R v[TTY + 2 * PH][TTX + 2 * PH];
+};
+template <class R>
+__device__ __forceinline__ void load_plane(const Geo& g, Plane<R>& p, const R* __restrict__ phi, int k) {
+    const int t = threadIdx.y * TTX + threadIdx.x;
+    const int i0 = blockIdx.x * TTX - PH, j0 = blockIdx.y * TTY - PH;
+    const R* __restrict__ lev = phi + g.sk * k;
+    constexpr int W = TTX + 2 * PH, NE = W * (TTY + 2 * PH);
+    for (int e = t; e < NE; e += TTX * TTY) {
+        const int b = e / W, a = e - b * W;
+        int gi = (i0 + a) % g.nx, gj = (j0 + b) % g.ny;
+        gi += gi < 0 ? g.nx : 0;
+        gj += gj < 0 ? g.ny : 0;
+        p.v[b][a] = __ldg(lev + gi + (int64_t)g.nx * gj);
+    }
+}
+// Flux through a face from the plane: x faces read row ty+PH from column
+// c0 (c0 = tx for the low face, tx+1 for the high face); y faces read column
+// tx+PH from row r0.
+template <int T, class R>
+__device__ __forceinline__ R plane_flux_x(const Plane<R>& p, int ty, int c0, R a, int type, R frac) {
+    R s[6];
+    const int w = width_of<T>(type);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const int off = m - 3;
+        s[m] = (off >= -w && off <= w - 1) ? p.v[ty + PH][c0 + m] : R(0);
+    }
+    return a * interp_of<T, R>(type, s, a, frac);
+}
+template <int T, class R>
+__device__ __forceinline__ R plane_flux_y(const Plane<R>& p, int r0, int tx, R a, int type, R frac) {
+    R s[6];
+    const int w = width_of<T>(type);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const int off = m - 3;
+        s[m] = (off >= -w && off <= w - 1) ? p.v[r0 + m][tx + PH] : R(0);
+    }
+    return a * interp_of<T, R>(type, s, a, frac);
+}
+
+// Fluxes of one scalar for cell (i,j,k): x/y into the tile from the staged
+// plane, z through zl/zh (zl is computed only on the block's first level;
+// otherwise it is the carried top flux of the level below).
 template <int TH, int TV, class R, class M>
-__device__ __forceinline__ void tile_put(const Geo& g, FluxTile<R>& t, const R* __restrict__ phi,
+__device__ __forceinline__ void tile_put(const Geo& g, FluxTile<R>& t, const Plane<R>& pl, const R* __restrict__ phi,
                                          const M* __restrict__ ax, const M* __restrict__ ay,
                                          const M* __restrict__ az, int th, int tv, R fh, R fv, int i, int j, int k,
                                          bool first, R& zl, R& zh) {
     const int tx = threadIdx.x, ty = threadIdx.y;
-    t.fx[ty][tx] = adv_flux_x<TH>(g, phi, ax, th, fh, i, j, k);
-    if (tx == TTX - 1 || i == g.nx - 1) t.fx[ty][tx + 1] = adv_flux_x<TH>(g, phi, ax, th, fh, wrap(i + 1, g.nx), j, k);
-    t.fy[ty][tx] = adv_flux_y<TH>(g, phi, ay, th, fh, i, j, k);
-    if (ty == TTY - 1 || j == g.ny - 1) t.fy[ty + 1][tx] = adv_flux_y<TH>(g, phi, ay, th, fh, i, wrap(j + 1, g.ny), k);
+    const int64_t c = cidx(g, i, j, k);
+    t.fx[ty][tx] = plane_flux_x<TH>(pl, ty, tx, R(__ldg(ax + c)), th, fh);
+    if (tx == TTX - 1 || i == g.nx - 1)
+        t.fx[ty][tx + 1] = plane_flux_x<TH>(pl, ty, tx + 1, R(__ldg(ax + cidx(g, wrap(i + 1, g.nx), j, k))), th, fh);
+    t.fy[ty][tx] = plane_flux_y<TH>(pl, ty, tx, R(__ldg(ay + c)), th, fh);
+    if (ty == TTY - 1 || j == g.ny - 1)
+        t.fy[ty + 1][tx] = plane_flux_y<TH>(pl, ty + 1, tx, R(__ldg(ay + cidx(g, i, wrap(j + 1, g.ny), k))), th, fh);
     if (first) zl = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k);
     zh = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k + 1);
 }
@@ -981,6 +1036,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
                                                                          R* __restrict__ Fcons, R* __restrict__ avx,
                                                                          R* __restrict__ avy, R* __restrict__ avz) {
     __shared__ FluxTile<R> sh;
+    __shared__ Plane<R> pl;
     const Geo& g = P.g;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
     const bool ok = i < g.nx && j < g.ny;
@@ -988,9 +1044,11 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
     R zl = R(0), zh = R(0);
     for (int k = k0; k < k1; ++k) {
+        load_plane(g, pl, A.prim, k);
+        __syncthreads();
         if (ok)
-            tile_put<TH, TV>(g, sh, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, R(P.f_dyc_h), R(P.f_dyc_v), i, j, k,
-                             k == k0, zl, zh);
+            tile_put<TH, TV>(g, sh, pl, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, R(P.f_dyc_h), R(P.f_dyc_v), i, j,
+                             k, k == k0, zl, zh);
         __syncthreads();
         if (ok) {
             R frt = tile_div(g, sh, zl, zh);
@@ -1045,6 +1103,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
                                                                     const R* __restrict__ avz, double* __restrict__ un,
                                                                     double* __restrict__ vn, double* __restrict__ wn) {
     __shared__ FluxTile<R> sh[MAX_SLOW];
+    __shared__ Plane<R> pl[MAX_SLOW];
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
@@ -1055,17 +1114,24 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
     R zl[MAX_SLOW], zh[MAX_SLOW];
 #pragma unroll
     for (int q = 0; q < MAX_SLOW; ++q) zl[q] = zh[q] = R(0);
+    auto slow_phi = [&](int q) {
+        return Acur.prim + (int64_t)((q == 0) ? ERF_RHOSCALAR_COMP - 1 : ERF_RHOQ1_COMP + q - 2) * N;
+    };
     for (int k = k0; k < k1; ++k) {
+#pragma unroll
+        for (int q = 0; q < MAX_SLOW; ++q)
+            if (q < nslow) load_plane(g, pl[q], slow_phi(q), k);
+        __syncthreads();
         if (ok) {
 #pragma unroll
             for (int q = 0; q < MAX_SLOW; ++q) {
                 if (q >= nslow) break;
                 if (q == 0)
-                    tile_put<DH, DV>(g, sh[0], Acur.prim + (int64_t)(ERF_RHOSCALAR_COMP - 1) * N, avx, avy, avz,
-                                     P.dry_h, P.dry_v, R(P.f_dry_h), R(P.f_dry_v), i, j, k, k == k0, zl[0], zh[0]);
+                    tile_put<DH, DV>(g, sh[0], pl[0], slow_phi(0), avx, avy, avz, P.dry_h, P.dry_v, R(P.f_dry_h),
+                                     R(P.f_dry_v), i, j, k, k == k0, zl[0], zh[0]);
                 else
-                    tile_put<MH, MV>(g, sh[q], Acur.prim + (int64_t)(ERF_RHOQ1_COMP + q - 2) * N, avx, avy, avz,
-                                     P.moi_h, P.moi_v, R(P.f_moi_h), R(P.f_moi_v), i, j, k, k == k0, zl[q], zh[q]);
+                    tile_put<MH, MV>(g, sh[q], pl[q], slow_phi(q), avx, avy, avz, P.moi_h, P.moi_v, R(P.f_moi_h),
+                                     R(P.f_moi_v), i, j, k, k == k0, zl[q], zh[q]);
             }
         }
         __syncthreads();
@@ -1249,6 +1315,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
     const R* prim = A.prim;
     const R* pp = A.pp;
     R zlu = R(0), zhu = R(0), zlv = R(0), zhv = R(0), zlw = R(0), zhw = R(0);
+    double t_below = 0.0;   // temperature of the cell below (buoyancy type 2, moist)
     for (int k = k0; k < k1; ++k) {
         const int64_t c = ok ? cidx(g, i, j, k) : 0;
         const bool zk = ok && k >= 1;   // z-momentum on interior faces only
@@ -1356,10 +1423,14 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
                 const double* qvd = pavg + 2 * g.nz;
                 const double* qcd = pavg + 3 * g.nz;
                 const double* qpd = pavg + 4 * g.nz;
-                double tp1 = eos_T(rd[k], rd[k] * thd[k], qvd[k]);
-                double tm1 = eos_T(rd[k - 1], rd[k - 1] * thd[k - 1], qvd[k - 1]);
+                (void)thd;
+                double tp1 = pavg[5 * g.nz + k], tm1 = pavg[5 * g.nz + k - 1];
+                // cell temperatures: this level's, and the one below carried
+                // up the block's column (evaluated once per cell)
                 double tp3 = eos_T(cd[c], cd[N + c], cd[5 * N + c] / cd[c]);
-                double tm3 = eos_T(cd[c - g.sk], cd[N + c - g.sk], cd[5 * N + c - g.sk] / cd[c - g.sk]);
+                double tm3 = (k == k0 || k == 1) ? eos_T(cd[c - g.sk], cd[N + c - g.sk], cd[5 * N + c - g.sk] / cd[c - g.sk])
+                                       : t_below;
+                t_below = tp3;
                 double qvp = nq >= 1 ? prim[4 * N + c] : 0.0, qvm = nq >= 1 ? prim[4 * N + c - g.sk] : 0.0;
                 double qcp = nq >= 2 ? prim[5 * N + c] : 0.0, qcm = nq >= 2 ? prim[5 * N + c - g.sk] : 0.0;
                 double qpp = nq >= 3 ? prim[6 * N + c] : 0.0, qpm = nq >= 3 ? prim[6 * N + c - g.sk] : 0.0;

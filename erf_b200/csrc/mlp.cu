@@ -1,6 +1,6 @@
 // mlp.cu -- learned subgrid closure on the 5th-generation tensor cores.
 //
-// A 13 -> 64 -> 64 -> 64 -> 9 multilayer perceptron with exact GELU
+// A 13 -> 64 -> 64 -> 64 -> 9 multilayer perceptron with GELU (tanh form)
 // activations maps the resolved velocity gradients (9), the potential
 // temperature gradient (3) and the filter width (1) to the six subgrid
 // stresses and three subgrid heat fluxes.  Weights and activations are BF16,

@@ -1,5 +1,5 @@
 // mlp.cuh -- the learned subgrid closure network (13 -> 64 -> 64 -> 64 -> 9,
-// exact GELU, BF16 operands, FP32 accumulation on tcgen05): parameter and
+// GELU in tanh form, BF16 operands, FP32 accumulation on tcgen05): parameter and
 // operand-tile layouts, the CTA forward pass shared by inference and the
 // dycore's closure kernel, and the network object behind the C-ABI handle.
 #pragma once
@@ -26,9 +26,22 @@ constexpr int T_W1F = 0, T_W2F = T_W1F + HID * KIN * 2, T_W3F = T_W2F + HID * HI
 constexpr int T_W4B = T_W4F + NOUTP * HID * 2, T_W3B = T_W4B + HID * NOUTP * 2, T_W2B = T_W3B + HID * HID * 2;
 constexpr int T_FWD_END = T_W4B, T_END = T_W2B + HID * HID * 2;  // 20480, 38912
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))
+// (Hendrycks & Gimpel 2016), with tanh from the hardware approximation
+// instruction; its derivative for the backward pass.
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float GELU_C = 0.7978845608028654f, GELU_A = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    float t = tanh_fast(GELU_C * (z + GELU_A * z * z * z));
+    return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+    float t = tanh_fast(GELU_C * (z + GELU_A * z * z * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * GELU_C * (1.0f + 3.0f * GELU_A * z * z);
 }
 
 
@@ -48,6 +61,7 @@ __device__ __forceinline__ bool forward_cta(const unsigned char* sW, unsigned ch
     fence_after();
     bool ok = true;
     float z[HID];
+#pragma unroll
     for (int layer = 0; layer < 4; ++layer) {
         const int N = layer == 3 ? NOUTP : HID;
         const int K = layer == 0 ? KIN : HID;
@@ -60,9 +74,11 @@ __device__ __forceinline__ bool forward_cta(const unsigned char* sW, unsigned ch
         ok = bar_wait(bar, phase) && ok;
         phase ^= 1;
         fence_after();
+#pragma unroll
         for (int c = 0; c < N / 16; ++c) tmem_ld16(tm + lane_base + c * 16, z + c * 16);
         const float* b = sB + layer * HID;
         if (layer < 3) {
+#pragma unroll
             for (int q = 0; q < HID; ++q) z[q] = gelu(z[q] + b[q]);
             put_row(sH, HID, t, z, HID);
         } else {

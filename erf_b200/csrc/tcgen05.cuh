@@ -95,6 +95,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 
 // Row r of a K-major tile with K columns from n FP32 values (columns >= n are 0).
 __device__ __forceinline__ void put_row(unsigned char* tile, int K, int r, const float* v, int n) {
+#pragma unroll
     for (int c = 0; c < K / 8; ++c) {
         __align__(16) __nv_bfloat16 h[8];
 #pragma unroll

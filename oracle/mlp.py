@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE ONLY: CPU restatement of the learned subgrid closure.
 
-The network is 13 -> 64 -> 64 -> 64 -> 9 with exact GELU
-(0.5 z (1 + erf(z / sqrt 2))) after the three hidden layers and a mean squared
+The network is 13 -> 64 -> 64 -> 64 -> 9 with GELU in its tanh form
+(0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))) after the three hidden layers and a mean squared
 error loss sum((y - t)^2) / (n * 9).  Parameters use the padded layout of the
 CUDA implementation (erf_b200/csrc/mlp.cu):
 
@@ -47,15 +47,17 @@ def bf16(a):
     return out.astype(np.float64)
 
 
-_erf = np.vectorize(math.erf)
+GELU_C, GELU_A = math.sqrt(2.0 / math.pi), 0.044715
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016)."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def unpack(p):
