@@ -28,16 +28,19 @@ constexpr int ST_TIMEOUT = 4;   // a bounded tensor-core wait ran out
 
 // ---------------------------------------------------------------------------
 // Equation of state (reference: Source/Utils/ERF_EOS.H:42-151).  Same
-// association of the operands as the reference so FP64 results agree to ulps.
+// association of the operands as the reference; the per-cell powers
+// x^y (x near 1, |y| < 2) are formed as exp(y log x), within a few ulps of
+// pow and cheaper.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double powxy(double x, double y) { return exp(y * log(x)); }
 __device__ __forceinline__ double eos_p(double rt, double qv) {
-    return p_0 * pow(R_d * rt * (1.0 + (R_v / R_d) * qv) * ip_0, Gamma_);
+    return p_0 * powxy(R_d * rt * (1.0 + (R_v / R_d) * qv) * ip_0, Gamma_);
 }
 __device__ __forceinline__ double eos_exner(double rt, double rdOcp) {
-    return pow(R_d * rt * (1.0 + R_v / R_d * 0.0) * ip_0, Gamma_ * rdOcp);
+    return powxy(R_d * rt * (1.0 + R_v / R_d * 0.0) * ip_0, Gamma_ * rdOcp);
 }
 __device__ __forceinline__ double eos_T(double rho, double rt, double qv) {
-    double p_loc = p_0 * pow(R_d * rt * (1.0 + R_v / R_d * qv) * ip_0, Gamma_);
+    double p_loc = p_0 * powxy(R_d * rt * (1.0 + R_v / R_d * qv) * ip_0, Gamma_);
     return p_loc / (R_d * rho * (1.0 + R_v / R_d * qv));
 }
 __device__ __forceinline__ double eos_rho_given_theta_p(double theta, double p, double rdOcp, double qv) {

@@ -699,7 +699,7 @@ __global__ void k_fast_coef(Params P, double D_d, StateBuf Sst, StageAux<R> A, R
 //   phase 2  right-hand side of the implicit w system per face, and
 //            d(rho w) of the previous solution;
 //   phase 3  Thomas forward / back substitution (one warp; FMA only, the
-//            stage's 1/B' and C/B' come from k_fast_coef);
+//            stage's A, 1/B' and C/B' come from k_fast_coef via L2);
 //   phase 4  vertical fluxes, average z-momentum, rho and rho*theta update.
 // All reads of the previous state happen in phases 1-2, before any write,
 // because the previous and new states may be the same buffers.  The W''
@@ -724,9 +724,7 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
     R* sT1 = sT0 + nz * TX;
     R* sR = sT1 + nz * TX;
     R* sD = sR + (nz + 1) * TX;
-    R* sA = sD + (nz + 1) * TX;
-    R* sI = sA + (nz + 1) * TX;
-    R* sCB = sI + (nz + 1) * TX;
+
     const int64_t N = g.ncell;
     const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi), halfg = R(P.halfg);
     const R dtau = R(dtau_d), beta_1 = R(beta_1d), beta_2 = R(beta_2d);
@@ -768,9 +766,6 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
             int64_t f = cidx(g, i, j, k);
             R Ok = R(prev_mz(k) - Sst.mz[f]);
             sD[k * TX + L] = Ok;
-            sA[k * TX + L] = cA[f];
-            sI[k * TX + L] = cInvB[f];
-            sCB[k * TX + L] = cCB[f];
             R rhs;
             if (k == 0 || k == nz) {
                 rhs = Ok + dtau * Fmz[f];
@@ -796,16 +791,23 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
         }
     }
     __syncthreads();
-    // ---- phase 3: tridiagonal solve, one warp
+    // ---- phase 3: tridiagonal solve, one warp.  The stage coefficients come
+    // from global memory (L2-resident across the stage's substeps); their
+    // loads do not depend on the recurrence, so the unrolled loops keep
+    // several levels of them in flight.
     if (t.w == 0 && t.ok) {
-        R s = sR[L] * sI[L];
+        const int64_t f0 = cidx(g, i, j, 0);
+        R s = sR[L] * __ldg(cInvB + f0);
         sR[L] = s;
+#pragma unroll 8
         for (int k = 1; k <= nz; ++k) {
-            s = (sR[k * TX + L] - sA[k * TX + L] * s) * sI[k * TX + L];
+            const int64_t f = f0 + g.sk * k;
+            s = (sR[k * TX + L] - __ldg(cA + f) * s) * __ldg(cInvB + f);
             sR[k * TX + L] = s;
         }
+#pragma unroll 8
         for (int k = nz - 1; k >= 0; --k) {
-            s = sR[k * TX + L] - sCB[k * TX + L] * s;
+            s = sR[k * TX + L] - __ldg(cCB + f0 + g.sk * k) * s;
             sR[k * TX + L] = s;
         }
     }
@@ -954,6 +956,9 @@ template <class R>
 struct Plane {
     R v[TTY + 2 * PH][TTX + 2 * PH];
 };
+// Asynchronous copy of the plane (cp.async): the copies land in shared
+// memory while the block works on the previous level; plane_wait() makes
+// this thread's copies complete (a barrier then publishes them).
 template <class R>
 __device__ __forceinline__ void load_plane(const Geo& g, Plane<R>& p, const R* __restrict__ phi, int k) {
     const int t = threadIdx.y * TTX + threadIdx.x;
@@ -965,9 +970,17 @@ __device__ __forceinline__ void load_plane(const Geo& g, Plane<R>& p, const R* _
         int gi = (i0 + a) % g.nx, gj = (j0 + b) % g.ny;
         gi += gi < 0 ? g.nx : 0;
         gj += gj < 0 ? g.ny : 0;
-        p.v[b][a] = __ldg(lev + gi + (int64_t)g.nx * gj);
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(&p.v[b][a]);
+        const R* src = lev + gi + (int64_t)g.nx * gj;
+        if constexpr (sizeof(R) == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
+__device__ __forceinline__ void plane_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Flux through a face from the plane: x faces read row ty+PH from column
 // c0 (c0 = tx for the low face, tx+1 for the high face); y faces read column
 // tx+PH from row r0.
@@ -1043,13 +1056,15 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
     const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
     R zl = R(0), zh = R(0);
+    load_plane(g, pl, A.prim, k0);
     for (int k = k0; k < k1; ++k) {
-        load_plane(g, pl, A.prim, k);
+        plane_wait();
         __syncthreads();
         if (ok)
             tile_put<TH, TV>(g, sh, pl, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, R(P.f_dyc_h), R(P.f_dyc_v), i, j,
                              k, k == k0, zl, zh);
         __syncthreads();
+        if (k + 1 < k1) load_plane(g, pl, A.prim, k + 1);   // overlaps the update below
         if (ok) {
             R frt = tile_div(g, sh, zl, zh);
             zl = zh;
@@ -1076,7 +1091,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
             }
             Fcons[g.ncell + c] = frt;
         }
-        __syncthreads();
+        // the next level's first barrier orders the reuse of sh
     }
 }
 
@@ -1117,10 +1132,11 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
     auto slow_phi = [&](int q) {
         return Acur.prim + (int64_t)((q == 0) ? ERF_RHOSCALAR_COMP - 1 : ERF_RHOQ1_COMP + q - 2) * N;
     };
-    for (int k = k0; k < k1; ++k) {
 #pragma unroll
-        for (int q = 0; q < MAX_SLOW; ++q)
-            if (q < nslow) load_plane(g, pl[q], slow_phi(q), k);
+    for (int q = 0; q < MAX_SLOW; ++q)
+        if (q < nslow) load_plane(g, pl[q], slow_phi(q), k0);
+    for (int k = k0; k < k1; ++k) {
+        plane_wait();
         __syncthreads();
         if (ok) {
 #pragma unroll
@@ -1135,6 +1151,11 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
             }
         }
         __syncthreads();
+        if (k + 1 < k1) {   // next level's planes arrive during the update below
+#pragma unroll
+            for (int q = 0; q < MAX_SLOW; ++q)
+                if (q < nslow) load_plane(g, pl[q], slow_phi(q), k + 1);
+        }
         if (ok) {
             int64_t c = cidx(g, i, j, k);
 #pragma unroll
@@ -1179,7 +1200,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
             if (k == g.nz - 1) { Snew.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
             if (make_next) stage_aux_cell<R>(P, Snew.cons, Anext, c, k);
         }
-        __syncthreads();
+        // the next level's first barrier orders the reuse of sh
     }
 }
 
