@@ -230,7 +230,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="moist_bubble", choices=sorted(cases.CASES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed"],
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned"],
                     help="precision forms to time (the JSON line needs both; single forms are for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -395,6 +395,12 @@ def main():
         return err
 
     clock_samples = []
+    if args.form == "learned":
+        if rank == 0:
+            print(json.dumps({"form": "learned", "learned": learned_arm(measure, form_error, C)}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     if args.form != "both":
         res, _, _ = measure(C.PREC_MIXED if args.form == "mixed" else C.PREC_FP64, clock_samples)
         if rank == 0:

@@ -39,7 +39,7 @@ struct Bulk {
 
 // Threads per block of the vertical acoustic kernel (columns x level groups).
 #ifndef ERFB_VERT_THREADS
-#define ERFB_VERT_THREADS 512
+#define ERFB_VERT_THREADS 1024
 #endif
 
 struct erf_b200_ctx {
@@ -449,8 +449,8 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         int nz = cfg->nz;
         c->tile_tx = 32;
         const size_t rs = c->mixed ? sizeof(float) : sizeof(double);
-        while (c->tile_tx > 4 && (size_t)(4 * nz + 2) * c->tile_tx * rs > max_smem) c->tile_tx /= 2;
-        c->vert_smem = (size_t)(4 * nz + 2) * c->tile_tx * rs;
+        while (c->tile_tx > 4 && (size_t)(7 * nz + 5) * c->tile_tx * rs > max_smem) c->tile_tx /= 2;
+        c->vert_smem = (size_t)(7 * nz + 5) * c->tile_tx * rs;
         c->coef_smem = (size_t)3 * (nz + 1) * c->tile_tx * rs;
         if (c->vert_smem > max_smem) rc = ERF_B200_ECONFIG;
         c->vert_warps = ERFB_VERT_THREADS / c->tile_tx;

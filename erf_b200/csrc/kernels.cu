@@ -699,7 +699,7 @@ __global__ void k_fast_coef(Params P, double D_d, StateBuf Sst, StageAux<R> A, R
 //   phase 2  right-hand side of the implicit w system per face, and
 //            d(rho w) of the previous solution;
 //   phase 3  Thomas forward / back substitution (one warp; FMA only, the
-//            stage's A, 1/B' and C/B' come from k_fast_coef via L2);
+//            stage's 1/B' and C/B' come from k_fast_coef);
 //   phase 4  vertical fluxes, average z-momentum, rho and rho*theta update.
 // All reads of the previous state happen in phases 1-2, before any write,
 // because the previous and new states may be the same buffers.  The W''
@@ -724,6 +724,9 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
     R* sT1 = sT0 + nz * TX;
     R* sR = sT1 + nz * TX;
     R* sD = sR + (nz + 1) * TX;
+    R* sA = sD + (nz + 1) * TX;
+    R* sI = sA + (nz + 1) * TX;
+    R* sCB = sI + (nz + 1) * TX;
 
     const int64_t N = g.ncell;
     const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi), halfg = R(P.halfg);
@@ -766,6 +769,9 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
             int64_t f = cidx(g, i, j, k);
             R Ok = R(prev_mz(k) - Sst.mz[f]);
             sD[k * TX + L] = Ok;
+            sA[k * TX + L] = cA[f];
+            sI[k * TX + L] = cInvB[f];
+            sCB[k * TX + L] = cCB[f];
             R rhs;
             if (k == 0 || k == nz) {
                 rhs = Ok + dtau * Fmz[f];
@@ -791,23 +797,16 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
         }
     }
     __syncthreads();
-    // ---- phase 3: tridiagonal solve, one warp.  The stage coefficients come
-    // from global memory (L2-resident across the stage's substeps); their
-    // loads do not depend on the recurrence, so the unrolled loops keep
-    // several levels of them in flight.
+    // ---- phase 3: tridiagonal solve, one warp
     if (t.w == 0 && t.ok) {
-        const int64_t f0 = cidx(g, i, j, 0);
-        R s = sR[L] * __ldg(cInvB + f0);
+        R s = sR[L] * sI[L];
         sR[L] = s;
-#pragma unroll 8
         for (int k = 1; k <= nz; ++k) {
-            const int64_t f = f0 + g.sk * k;
-            s = (sR[k * TX + L] - __ldg(cA + f) * s) * __ldg(cInvB + f);
+            s = (sR[k * TX + L] - sA[k * TX + L] * s) * sI[k * TX + L];
             sR[k * TX + L] = s;
         }
-#pragma unroll 8
         for (int k = nz - 1; k >= 0; --k) {
-            s = sR[k * TX + L] - __ldg(cCB + f0 + g.sk * k) * s;
+            s = sR[k * TX + L] - sCB[k * TX + L] * s;
             sR[k * TX + L] = s;
         }
     }
