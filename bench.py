@@ -172,6 +172,87 @@ def learned_arm(measure, form_error, C):
             "rel_l2_mixed_vs_fp64_learned_after_100_steps": err}
 
 
+def ensemble_members(n=32, seed=100):
+    """Member sizes (64^3 up to 192 x 192 x 96, multiples of 32 / 16) and
+    geostrophic winds (4-16 m/s), seeded."""
+    import numpy as _np
+    rng = _np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        nx = int(rng.integers(2, 7)) * 32
+        ny = int(rng.integers(2, 7)) * 32
+        nz = int(rng.integers(4, 7)) * 16
+        out.append((nx, ny, nz, float(rng.uniform(4.0, 16.0)), seed + q))
+    return out
+
+
+def ensemble_arm(args, C, Dycore, Ensemble, stream, n_err=4):
+    """32 ABL members of uneven sizes at dx = dz = 40 m (the learned closure's
+    grid spacing), mixed form with the learned closure, each member
+    autotuned, advanced together by one CUDA graph per step."""
+    import torch
+    if not os.path.exists(CLOSURE_MODEL):
+        return {"unavailable": "no trained closure model"}
+    from erf_b200.closure import load_closure
+    net = load_closure(CLOSURE_MODEL)
+    specs = ensemble_members()
+
+    def member_case(nx, ny, nz, ug, seed, precision):
+        case = cases.abl_fine(nx=nx, ny=ny, nz=nz, dx=40.0, dz=40.0, u_g=ug, dt=0.32, seed=seed)
+        case.cfg.precision = precision
+        case.cfg.les_type = C.LES_MLP
+        return case
+
+    def make(spec, precision):
+        case = member_case(*spec, precision)
+        dy = Dycore(case.cfg, stream=stream.cuda_stream)
+        base = dy.make_base_state(case)
+        dy.set_base_state(base)
+        dy.set_closure(net)
+        st = case.build_state(base[0])
+        dy.load_state(*st)
+        return dy, st
+
+    members = [make(sp, C.PREC_MIXED) for sp in specs]
+    tuned = [dy.autotune(2) for dy, _ in members]
+    cells = sum(sp[0] * sp[1] * sp[2] for sp in specs)
+    ens = Ensemble([dy for dy, _ in members], stream=stream.cuda_stream)
+    ens.advance(args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ens.sync()
+    status = [dy.status() for dy, _ in members]
+    # per-member error of the mixed form against FP64 (same closure) for the
+    # first n_err members after warmup + steps steps
+    errs = []
+    nsteps = args.warmup + args.steps
+    for q in range(n_err):
+        dy, st = members[q]
+        got = dy.store_state(*st)
+        ref_dy, _ = make(specs[q], C.PREC_FP64)
+        ref_dy.advance_resident(nsteps)
+        ref = ref_dy.store_state(*st)
+        ref_dy.close()
+        rl2 = lambda a, b: float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+        errs.append({"size": specs[q][:3], "u": rl2(got[1], ref[1]), "v": rl2(got[2], ref[2]), "w": rl2(got[3], ref[3]),
+                     "theta": rl2(got[0][1] / got[0][0], ref[0][1] / ref[0][0])})
+    ens.close()
+    for dy, _ in members:
+        dy.close()
+    net.close()
+    return {"workload": f"{len(specs)} ABL members 64^3..192x192x96 (seeded), dx=dz=40 m, u_g 4-16 m/s, "
+                        "mixed form + learned closure, one CUDA graph per step, autotuned",
+            "members": len(specs), "cells": cells, "steps": args.steps, "ms_per_step": ms / args.steps,
+            "value": cells * args.steps / (ms * 1e-3), "unit": "cell-steps/s",
+            "autotuned_ms_per_member_step": tuned, "status": max(status),
+            "rel_l2_mixed_vs_fp64_first_members": errs}
+
+
 def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
     """Time the FP64 CPU oracle on a bounded sample of the workload."""
     import oracle
@@ -230,7 +311,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="moist_bubble", choices=sorted(cases.CASES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned"],
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble"],
                     help="precision forms to time (the JSON line needs both; single forms are for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -395,6 +476,14 @@ def main():
         return err
 
     clock_samples = []
+    if args.form == "ensemble":
+        from erf_b200.dycore import Ensemble
+        if rank == 0:
+            print(json.dumps({"form": "ensemble", "ensemble": ensemble_arm(args, C, Dycore, Ensemble, stream)}),
+                  flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     if args.form == "learned":
         if rank == 0:
             print(json.dumps({"form": "learned", "learned": learned_arm(measure, form_error, C)}), flush=True)
@@ -414,6 +503,8 @@ def main():
     mixed_err = form_error(base, init, 100) if rank == 0 else None
     cfg.precision = C.PREC_FP64
     learned = learned_arm(measure, form_error, C) if rank == 0 else None
+    from erf_b200.dycore import Ensemble
+    ensemble = ensemble_arm(args, C, Dycore, Ensemble, stream) if rank == 0 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -444,6 +535,7 @@ def main():
                                   for k, v in mixed["kernels"].items()},
                       "rel_l2_vs_fp64_after_100_steps": mixed_err, "status": mixed["status"]},
             "learned": learned,
+            "ensemble": ensemble,
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clock_samples),
             "gpu_launches": plain["launches"],

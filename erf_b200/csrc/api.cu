@@ -79,8 +79,11 @@ struct erf_b200_ctx {
 
 namespace {
 
+thread_local cudaError_t g_last_cuda_error = cudaSuccess;   // for erf_b200_last_cuda_error
+
 int cuda_fail(cudaError_t e) {
     if (e == cudaSuccess) return ERF_B200_OK;
+    g_last_cuda_error = e;
     return e == cudaErrorMemoryAllocation ? ERF_B200_ENOMEM : ERF_B200_ECUDA;
 }
 #define CK(x)                                   \
@@ -990,22 +993,38 @@ int erf_b200_autotune(erf_b200_ctx* c, int reps, double* best_ms) {
     float best = 0.f;
     int rc = trial(best);
     const int nz = c->cfg.nz;
-    for (int threads : {256, 512, 1024}) {
-        int vw = threads / c->tile_tx;
-        if (rc || vw < 1 || vw == c->vert_warps) continue;
-        int keep = c->vert_warps;
-        c->vert_warps = vw;
-        float ms;
-        if ((rc = trial(ms))) break;
-        if (ms < best) best = ms; else c->vert_warps = keep;
+    // vertical kernels: columns per block (smaller tiles let two blocks share
+    // an SM, overlapping one block's serial sweep with the other's loads) and
+    // threads per block
+    const size_t rs = c->mixed ? sizeof(float) : sizeof(double);
+    for (int tx : {c->tile_tx, c->tile_tx / 2}) {
+        for (int threads : {256, 512, 1024}) {
+            int vw = threads / tx;
+            if (rc || tx < 4 || vw < 1 || (tx == c->tile_tx && vw == c->vert_warps)) continue;
+            int keep_tx = c->tile_tx, keep_vw = c->vert_warps, keep_cw = c->coef_warps;
+            size_t keep_vs = c->vert_smem, keep_cs = c->coef_smem;
+            c->tile_tx = tx;
+            c->vert_warps = vw;
+            c->vert_smem = (size_t)(7 * nz + 5) * tx * rs;
+            c->coef_smem = (size_t)3 * (nz + 1) * tx * rs;
+            if (c->coef_warps * tx > 1024) c->coef_warps = 1024 / tx;
+            float ms;
+            if (trial(ms) == ERF_B200_OK && ms < best) {
+                best = ms;
+            } else {   // slower, or not launchable: keep the previous shape
+                cudaGetLastError();
+                c->tile_tx = keep_tx; c->vert_warps = keep_vw; c->coef_warps = keep_cw;
+                c->vert_smem = keep_vs; c->coef_smem = keep_cs;
+            }
+        }
     }
     for (int cw : {4, 8, 16}) {
         if (rc || cw == c->coef_warps || cw * c->tile_tx > 1024) continue;
         int keep = c->coef_warps;
         c->coef_warps = cw;
         float ms;
-        if ((rc = trial(ms))) break;
-        if (ms < best) best = ms; else c->coef_warps = keep;
+        if (trial(ms) == ERF_B200_OK && ms < best) best = ms;
+        else { cudaGetLastError(); c->coef_warps = keep; }
     }
     int* kz[3] = {&c->tkz.cell, &c->tkz.mom, &c->tkz.post};
     for (int q = 0; q < 3 && !rc; ++q) {
@@ -1015,8 +1034,8 @@ int erf_b200_autotune(erf_b200_ctx* c, int reps, double* best_ms) {
             int keep = *kz[q];
             *kz[q] = cand;
             float ms;
-            if ((rc = trial(ms))) break;
-            if (ms < best) best = ms; else *kz[q] = keep;
+            if (trial(ms) == ERF_B200_OK && ms < best) best = ms;
+            else { cudaGetLastError(); *kz[q] = keep; }
         }
     }
     drop_graphs(c);
@@ -1108,5 +1127,9 @@ int erf_b200_ensemble_sync(erf_b200_ensemble* e) {
     CK(cudaStreamSynchronize(e->stream));
     return ERF_B200_OK;
 }
+
+// Name of the last CUDA error behind an ERF_B200_ECUDA / ENOMEM return on
+// this host thread ("no error" if none).
+const char* erf_b200_last_cuda_error(void) { return cudaGetErrorString(g_last_cuda_error); }
 
 }  // extern "C"

@@ -196,10 +196,19 @@ void launch_closure(const Params& P, const ClosureNet& net, int grid, cudaStream
 
 template <class R>
 int closure_grid(const Params& P) {
-    int dev = 0, nsm = 148, per = 1;
+    int dev = 0, nsm = 148, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_closure<R>, ROWS, 0) != cudaSuccess || per < 1) per = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_closure<R>, ROWS, 0) != cudaSuccess) per = 0;
+    // the same bound from the kernel's registers and shared memory
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_closure<R>) == cudaSuccess && fa.numRegs > 0) {
+        int by_regs = 65536 / (fa.numRegs * ROWS);
+        int by_smem = (int)(227 * 1024 / (fa.sharedSizeBytes + 1024));
+        int est = by_regs < by_smem ? by_regs : by_smem;
+        if (est > per) per = est;
+    }
+    if (per < 1) per = 1;
     per = per > 8 ? 8 : per;   // 8 x 64 TMEM columns per SM
     long nblk = (P.g.ncell + ROWS - 1) / ROWS;
     long grid = (long)per * nsm;

@@ -204,34 +204,10 @@ __global__ void k_stage_aux(Params P, const double* __restrict__ cons, StageAux<
 // ---------------------------------------------------------------------------
 // Scalar flux helpers
 // ---------------------------------------------------------------------------
-// Advective flux of a primitive scalar phi (type R) through the low x/y/z face
+// Advective flux of a primitive scalar phi (type R) through the low z face
 // of cell (i,j,k): mom * interp(phi) (Advection/ERF_AdvectionSrcForScalars.H:
 // 7-58).  The advecting momentum M is the FP64 stage momentum (rho, theta)
 // or the R average momentum (slow scalars).
-template <int T, class R, class M>
-__device__ __forceinline__ R adv_flux_x(const Geo& g, const R* __restrict__ phi, const M* __restrict__ mom, int type,
-                                        R frac, int i, int j, int k) {
-    R s[6];
-    const int w = width_of<T>(type);
-    for (int m = 0; m < 6; ++m) {
-        int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, wrap(i + off, g.nx), j, k)) : R(0);
-    }
-    R a = R(__ldg(mom + cidx(g, i, j, k)));
-    return a * interp_of<T, R>(type, s, a, frac);
-}
-template <int T, class R, class M>
-__device__ __forceinline__ R adv_flux_y(const Geo& g, const R* __restrict__ phi, const M* __restrict__ mom, int type,
-                                        R frac, int i, int j, int k) {
-    R s[6];
-    const int w = width_of<T>(type);
-    for (int m = 0; m < 6; ++m) {
-        int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? __ldg(phi + cidx(g, i, wrap(j + off, g.ny), k)) : R(0);
-    }
-    R a = R(__ldg(mom + cidx(g, i, j, k)));
-    return a * interp_of<T, R>(type, s, a, frac);
-}
 template <int T, class R, class M>
 __device__ __forceinline__ R adv_flux_z(const Geo& g, const R* __restrict__ phi, const M* __restrict__ mom, int type,
                                         R frac, int i, int j, int k) {
@@ -304,28 +280,8 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* 
     }
 }
 
-// Momentum flux helpers: interpolated face velocity (FP64 state) in R
+// Momentum flux helper: vertical stencil of a face velocity (FP64 state) in R
 // (ERF_AdvectionSrcForMom_N.H:17-274).
-template <int T, class R>
-__device__ __forceinline__ R gatherx_interp(const Geo& g, const double* f, int type, R upw, R frac, int i, int j, int k) {
-    R s[6];
-    const int w = width_of<T>(type);
-    for (int m = 0; m < 6; ++m) {
-        int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? R(__ldg(f + cidx(g, wrap(i + off, g.nx), j, k))) : R(0);
-    }
-    return interp_of<T, R>(type, s, upw, frac);
-}
-template <int T, class R>
-__device__ __forceinline__ R gathery_interp(const Geo& g, const double* f, int type, R upw, R frac, int i, int j, int k) {
-    R s[6];
-    const int w = width_of<T>(type);
-    for (int m = 0; m < 6; ++m) {
-        int off = m - 3;
-        s[m] = (off >= -w && off <= w - 1) ? R(__ldg(f + cidx(g, i, wrap(j + off, g.ny), k))) : R(0);
-    }
-    return interp_of<T, R>(type, s, upw, frac);
-}
 template <int T, class R>
 __device__ __forceinline__ R gatherz_tang(const Geo& g, const double* f, int type, R upw, R frac, int i, int j, int k) {
     R s[6];
@@ -1206,17 +1162,44 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
 // Momentum fluxes of AdvectionSrcFor{X,Y,Z}Mom_N (ERF_AdvectionSrcForMom_N.H:
 // 17-274).  Each is the flux through the low side of the face's control
 // volume in one direction; the high side is the same function one index up.
-template <int HT, class R>
-__device__ __forceinline__ R xmom_flux_x(const Params& P, const double* ru, const double* u, int i, int j, int k) {
-    const Geo& g = P.g;
-    R a = R(0.5) * (R(ru[cidx(g, wrap(i - 1, g.nx), j, k)]) + R(ru[cidx(g, i, j, k)]));
-    return a * gatherx_interp<HT, R>(g, u, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
+// The x / y stencils of the face velocity come from the level's staged
+// plane: column c0 = tx (low face) or tx + 1 (the tile edge's high face),
+// row r0 = ty or ty + 1 likewise.
+template <int T, class R, class V>
+__device__ __forceinline__ R plane_interp_x(const Plane<V>& p, int ty, int c0, int type, R upw, R frac) {
+    R s[6];
+    const int w = width_of<T>(type);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const int off = m - 3;
+        s[m] = (off >= -w && off <= w - 1) ? R(p.v[ty + PH][c0 + m]) : R(0);
+    }
+    return interp_of<T, R>(type, s, upw, frac);
+}
+template <int T, class R, class V>
+__device__ __forceinline__ R plane_interp_y(const Plane<V>& p, int r0, int tx, int type, R upw, R frac) {
+    R s[6];
+    const int w = width_of<T>(type);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const int off = m - 3;
+        s[m] = (off >= -w && off <= w - 1) ? R(p.v[r0 + m][tx + PH]) : R(0);
+    }
+    return interp_of<T, R>(type, s, upw, frac);
 }
 template <int HT, class R>
-__device__ __forceinline__ R xmom_flux_y(const Params& P, const double* rv, const double* u, int i, int j, int k) {
+__device__ __forceinline__ R xmom_flux_x(const Params& P, const double* ru, const Plane<double>& pu, int c0, int ty,
+                                         int i, int j, int k) {
+    const Geo& g = P.g;
+    R a = R(0.5) * (R(ru[cidx(g, wrap(i - 1, g.nx), j, k)]) + R(ru[cidx(g, i, j, k)]));
+    return a * plane_interp_x<HT, R>(pu, ty, c0, P.dyc_h, a, R(P.f_dyc_h));
+}
+template <int HT, class R>
+__device__ __forceinline__ R xmom_flux_y(const Params& P, const double* rv, const Plane<double>& pu, int tx, int r0,
+                                         int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(rv[cidx(g, i, j, k)]) + R(rv[cidx(g, wrap(i - 1, g.nx), j, k)]));
-    return a * gathery_interp<HT, R>(g, u, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
+    return a * plane_interp_y<HT, R>(pu, r0, tx, P.dyc_h, a, R(P.f_dyc_h));
 }
 template <int VT, class R>
 __device__ __forceinline__ R xmom_flux_z(const Params& P, const double* rw, const double* u, int i, int j, int k) {
@@ -1225,16 +1208,18 @@ __device__ __forceinline__ R xmom_flux_z(const Params& P, const double* rw, cons
     return a * gatherz_tang<VT, R>(g, u, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
 }
 template <int HT, class R>
-__device__ __forceinline__ R ymom_flux_x(const Params& P, const double* ru, const double* v, int i, int j, int k) {
+__device__ __forceinline__ R ymom_flux_x(const Params& P, const double* ru, const Plane<double>& pv, int c0, int ty,
+                                         int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(ru[cidx(g, i, j, k)]) + R(ru[cidx(g, i, wrap(j - 1, g.ny), k)]));
-    return a * gatherx_interp<HT, R>(g, v, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
+    return a * plane_interp_x<HT, R>(pv, ty, c0, P.dyc_h, a, R(P.f_dyc_h));
 }
 template <int HT, class R>
-__device__ __forceinline__ R ymom_flux_y(const Params& P, const double* rv, const double* v, int i, int j, int k) {
+__device__ __forceinline__ R ymom_flux_y(const Params& P, const double* rv, const Plane<double>& pv, int tx, int r0,
+                                         int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(rv[cidx(g, i, j, k)]) + R(rv[cidx(g, i, wrap(j - 1, g.ny), k)]));
-    return a * gathery_interp<HT, R>(g, v, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
+    return a * plane_interp_y<HT, R>(pv, r0, tx, P.dyc_h, a, R(P.f_dyc_h));
 }
 template <int VT, class R>
 __device__ __forceinline__ R ymom_flux_z(const Params& P, const double* rw, const double* v, int i, int j, int k) {
@@ -1243,16 +1228,18 @@ __device__ __forceinline__ R ymom_flux_z(const Params& P, const double* rw, cons
     return a * gatherz_tang<VT, R>(g, v, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
 }
 template <int HT, class R>
-__device__ __forceinline__ R zmom_flux_x(const Params& P, const double* ru, const double* w, int i, int j, int k) {
+__device__ __forceinline__ R zmom_flux_x(const Params& P, const double* ru, const Plane<double>& pw, int c0, int ty,
+                                         int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(ru[cidx(g, i, j, k)]) + R(ru[cidx(g, i, j, k - 1)])) * R(1);
-    return a * gatherx_interp<HT, R>(g, w, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
+    return a * plane_interp_x<HT, R>(pw, ty, c0, P.dyc_h, a, R(P.f_dyc_h));
 }
 template <int HT, class R>
-__device__ __forceinline__ R zmom_flux_y(const Params& P, const double* rv, const double* w, int i, int j, int k) {
+__device__ __forceinline__ R zmom_flux_y(const Params& P, const double* rv, const Plane<double>& pw, int tx, int r0,
+                                         int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(rv[cidx(g, i, j, k)]) + R(rv[cidx(g, i, j, k - 1)])) * R(1);
-    return a * gathery_interp<HT, R>(g, w, P.dyc_h, a, R(P.f_dyc_h), i, j, k);
+    return a * plane_interp_y<HT, R>(pw, r0, tx, P.dyc_h, a, R(P.f_dyc_h));
 }
 // Vertical flux of w between faces kk-1 and kk (the "lo" flux of face kk),
 // with the order reduction next to the walls (ERF_AdvectionSrcForMom_N.H:
@@ -1317,6 +1304,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
                                                                        R* __restrict__ Fmx, R* __restrict__ Fmy,
                                                                        R* __restrict__ Fmz) {
     __shared__ FluxTile<R> sh[3];
+    __shared__ Plane<double> pu, pv, pw;   // face velocities of the level, with halo
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -1336,32 +1324,42 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
     const R* pp = A.pp;
     R zlu = R(0), zhu = R(0), zlv = R(0), zhv = R(0), zlw = R(0), zhw = R(0);
     double t_below = 0.0;   // temperature of the cell below (buoyancy type 2, moist)
+    load_plane(g, pu, u, k0);
+    load_plane(g, pv, v, k0);
+    load_plane(g, pw, w, k0);
     for (int k = k0; k < k1; ++k) {
         const int64_t c = ok ? cidx(g, i, j, k) : 0;
         const bool zk = ok && k >= 1;   // z-momentum on interior faces only
+        plane_wait();
+        __syncthreads();
         if (ok) {
-            sh[0].fx[ty][tx] = xmom_flux_x<HT, R>(P, ru, u, i, j, k);
-            if (xedge) sh[0].fx[ty][tx + 1] = xmom_flux_x<HT, R>(P, ru, u, ip, j, k);
-            sh[0].fy[ty][tx] = xmom_flux_y<HT, R>(P, rv, u, i, j, k);
-            if (yedge) sh[0].fy[ty + 1][tx] = xmom_flux_y<HT, R>(P, rv, u, i, jp, k);
+            sh[0].fx[ty][tx] = xmom_flux_x<HT, R>(P, ru, pu, tx, ty, i, j, k);
+            if (xedge) sh[0].fx[ty][tx + 1] = xmom_flux_x<HT, R>(P, ru, pu, tx + 1, ty, ip, j, k);
+            sh[0].fy[ty][tx] = xmom_flux_y<HT, R>(P, rv, pu, tx, ty, i, j, k);
+            if (yedge) sh[0].fy[ty + 1][tx] = xmom_flux_y<HT, R>(P, rv, pu, tx, ty + 1, i, jp, k);
             if (k == k0) zlu = xmom_flux_z<VT, R>(P, rw, u, i, j, k);
             zhu = xmom_flux_z<VT, R>(P, rw, u, i, j, k + 1);
-            sh[1].fx[ty][tx] = ymom_flux_x<HT, R>(P, ru, v, i, j, k);
-            if (xedge) sh[1].fx[ty][tx + 1] = ymom_flux_x<HT, R>(P, ru, v, ip, j, k);
-            sh[1].fy[ty][tx] = ymom_flux_y<HT, R>(P, rv, v, i, j, k);
-            if (yedge) sh[1].fy[ty + 1][tx] = ymom_flux_y<HT, R>(P, rv, v, i, jp, k);
+            sh[1].fx[ty][tx] = ymom_flux_x<HT, R>(P, ru, pv, tx, ty, i, j, k);
+            if (xedge) sh[1].fx[ty][tx + 1] = ymom_flux_x<HT, R>(P, ru, pv, tx + 1, ty, ip, j, k);
+            sh[1].fy[ty][tx] = ymom_flux_y<HT, R>(P, rv, pv, tx, ty, i, j, k);
+            if (yedge) sh[1].fy[ty + 1][tx] = ymom_flux_y<HT, R>(P, rv, pv, tx, ty + 1, i, jp, k);
             if (k == k0) zlv = ymom_flux_z<VT, R>(P, rw, v, i, j, k);
             zhv = ymom_flux_z<VT, R>(P, rw, v, i, j, k + 1);
         }
         if (zk) {
-            sh[2].fx[ty][tx] = zmom_flux_x<HT, R>(P, ru, w, i, j, k);
-            if (xedge) sh[2].fx[ty][tx + 1] = zmom_flux_x<HT, R>(P, ru, w, ip, j, k);
-            sh[2].fy[ty][tx] = zmom_flux_y<HT, R>(P, rv, w, i, j, k);
-            if (yedge) sh[2].fy[ty + 1][tx] = zmom_flux_y<HT, R>(P, rv, w, i, jp, k);
+            sh[2].fx[ty][tx] = zmom_flux_x<HT, R>(P, ru, pw, tx, ty, i, j, k);
+            if (xedge) sh[2].fx[ty][tx + 1] = zmom_flux_x<HT, R>(P, ru, pw, tx + 1, ty, ip, j, k);
+            sh[2].fy[ty][tx] = zmom_flux_y<HT, R>(P, rv, pw, tx, ty, i, j, k);
+            if (yedge) sh[2].fy[ty + 1][tx] = zmom_flux_y<HT, R>(P, rv, pw, tx, ty + 1, i, jp, k);
             if (k == k0 || k == 1) zlw = zmom_flux_z<VT, R>(P, rw, w, i, j, k);
             zhw = zmom_flux_z<VT, R>(P, rw, w, i, j, k + 1);
         }
         __syncthreads();
+        if (k + 1 < k1) {   // next level's planes arrive during the right-hand sides below
+            load_plane(g, pu, u, k + 1);
+            load_plane(g, pv, v, k + 1);
+            load_plane(g, pw, w, k + 1);
+        }
         // ---------------- x-momentum on face i
         if (ok) {
             R rhs = -((sh[0].fx[ty][tx + 1] - sh[0].fx[ty][tx]) * dxi * R(1) +
@@ -1473,7 +1471,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
             Fmz[c] = rhs;
         }
         if (ok && k == g.nz - 1) Fmz[c + g.sk] = R(0);
-        __syncthreads();
+        // the next level's first barrier orders the reuse of sh
     }
 }
 
@@ -1555,10 +1553,18 @@ void tiled_setup(const Params& P, TiledKz* t) {
     t->post = pick_kz(post_kernel<R>(P), P.g);
 }
 
+// The dynamic shared-memory opt-in is a property of the kernel for the whole
+// process, shared by every context: it is raised to the device maximum (the
+// size passed at launch still sets each launch's footprint), so that contexts
+// of different sizes never lower it below one another's needs.
 template <class R>
 int vert_setup(size_t vert_smem, size_t coef_smem) {
-    if (cudaFuncSetAttribute(k_fast_vert<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vert_smem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_fast_coef<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem) != cudaSuccess)
+    int dev = 0, maxopt = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 1;
+    if (vert_smem > (size_t)maxopt || coef_smem > (size_t)maxopt) return 1;
+    if (cudaFuncSetAttribute(k_fast_vert<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxopt) != cudaSuccess ||
+        cudaFuncSetAttribute(k_fast_coef<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxopt) != cudaSuccess)
         return 1;
     return 0;
 }

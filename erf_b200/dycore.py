@@ -32,6 +32,7 @@ EXPORTS = [
     "erf_b200_mlp_infer", "erf_b200_set_closure", "erf_b200_closure_fallbacks", "erf_b200_closure_features_host",
     "erf_b200_load_state", "erf_b200_store_state", "erf_b200_advance_resident", "erf_b200_autotune",
     "erf_b200_ensemble_create", "erf_b200_ensemble_advance", "erf_b200_ensemble_sync", "erf_b200_ensemble_destroy",
+    "erf_b200_last_cuda_error",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs"]
@@ -88,12 +89,16 @@ def load_library():
     L.erf_b200_ensemble_destroy.argtypes = [vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
+    L.erf_b200_last_cuda_error.argtypes = []
+    L.erf_b200_last_cuda_error.restype = ctypes.c_char_p
     _lib = L
     return L
 
 
 def _check(rc: int, what: str):
     if rc != 0:
+        if rc in (2, 3) and _lib is not None:   # ECUDA / ENOMEM: name the CUDA error
+            what = f"{what} ({_lib.erf_b200_last_cuda_error().decode()})"
         raise ErfError(rc, what)
 
 

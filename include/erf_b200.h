@@ -348,6 +348,10 @@ int erf_b200_mlp_train(erf_b200_mlp* m, const float* xn, const float* tn, int n,
 /* y[n][9] (raw units) from x[n][13] (raw units). */
 int erf_b200_mlp_infer(erf_b200_mlp* m, const float* x, int n, float* y);
 
+/* Name of the CUDA error behind the last ERF_B200_ECUDA / ERF_B200_ENOMEM
+ * returned on this host thread. */
+const char* erf_b200_last_cuda_error(void);
+
 /* ------------------------------------------------------------------------
  * Resident state, autotuning and ensembles (no reference counterpart).
  * ------------------------------------------------------------------------ */

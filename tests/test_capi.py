@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "erf_b200.h")
 
 def declared_functions():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^int\s+(erf_b200_\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|const char\s*\*)\s*(erf_b200_\w+)\s*\(", txt, flags=re.M)))
 
 
 @pytest.fixture(scope="module")
