@@ -70,6 +70,9 @@ class Case:
         cons[1] = rho * theta
         if cfg.moisture != C.MOIST_NONE:
             cons[5] = rho * self.qv_cc[:, None, None]
+        if "tke0" in self.pert:   # initial subgrid TKE (Deardorff)
+            e0 = np.where(z <= self.pert.get("tke0_zmax", np.inf), self.pert["tke0"], 1.0e-3)
+            cons[2] = rho * e0[:, None, None]
         u = np.broadcast_to(self.u_cc[:, None, None], (nz, ny, nx + 1)).copy()
         v = np.broadcast_to(self.v_cc[:, None, None], (nz, ny + 1, nx)).copy()
         w = np.zeros((nz + 1, ny, nx))
@@ -163,6 +166,21 @@ def abl_fine(nx=512, ny=512, nz=128, dx=10.0, dz=10.0, u_g=10.0, dt=0.08, seed=0
     return case
 
 
+def abl_deardorff(nx=64, ny=64, nz=64, seed=0, tke0=0.1) -> Case:
+    """abl_dry with the Deardorff TKE closure (Ck 0.1, Ce 0.93, sigma_k 0.5,
+    theta_ref 300 K): initial subgrid TKE tke0 m^2/s^2 below 400 m and 1e-3
+    above, so that both the neutral and the stably stratified mixing-length
+    branches are used."""
+    case = abl_dry(nx=nx, ny=ny, nz=nz, seed=seed)
+    c = case.cfg
+    c.les_type = C.LES_DEARDORFF
+    c.Ck, c.Ce, c.Ce_wall, c.sigma_k, c.theta_ref = 0.1, 0.93, 0.0, 0.5, 300.0
+    case.name = "abl_deardorff"
+    case.pert["tke0"] = tke0
+    case.pert["tke0_zmax"] = 400.0
+    return case
+
+
 def moist_bubble(nx=128, ny=128, nz=80, seed=1) -> Case:
     c = C.defaults()
     c.nx, c.ny, c.nz = nx, ny, nz
@@ -203,4 +221,4 @@ def moist_bubble(nx=128, ny=128, nz=80, seed=1) -> Case:
                       "bubble_rz": 1500.0, "bubble_zc": 1500.0}, steps=100)
 
 
-CASES = {"abl_dry": abl_dry, "moist_bubble": moist_bubble}
+CASES = {"abl_dry": abl_dry, "moist_bubble": moist_bubble, "abl_deardorff": abl_deardorff}

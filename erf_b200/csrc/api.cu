@@ -35,6 +35,7 @@ struct Bulk {
     R *cA, *cInvB, *cCB, *cP, *cQ;  // fast coefficients of the current stage
     R *c12 = nullptr, *c13 = nullptr, *c23 = nullptr;  // learned closure: cell-centred off-diagonal stresses
     R *hx = nullptr, *hy = nullptr, *hz = nullptr;     // learned closure: rho * heat flux
+    TkeBuf<R> tke{nullptr, nullptr, nullptr, nullptr}; // Deardorff closure arrays
 };
 
 // Threads per block of the vertical acoustic kernel (columns x level groups).
@@ -124,7 +125,10 @@ int validate(const erf_b200_config* c) {
     if (c->dycore_horiz_adv == ERF_ADV_CENTERED_2ND && c->dycore_vert_adv == ERF_ADV_CENTERED_2ND) return ERF_B200_ECONFIG;
     if (!adv_supported(c->dryscal_horiz_adv) || !adv_supported(c->dryscal_vert_adv)) return ERF_B200_ECONFIG;
     if (!adv_supported(c->moistscal_horiz_adv) || !adv_supported(c->moistscal_vert_adv)) return ERF_B200_ECONFIG;
-    if (c->les_type != ERF_LES_NONE && c->les_type != ERF_LES_SMAGORINSKY && c->les_type != ERF_LES_MLP)
+    if (c->les_type != ERF_LES_NONE && c->les_type != ERF_LES_SMAGORINSKY && c->les_type != ERF_LES_DEARDORFF &&
+        c->les_type != ERF_LES_MLP)
+        return ERF_B200_ECONFIG;
+    if (c->les_type == ERF_LES_DEARDORFF && (!(c->theta_ref > 0.0) || !(c->sigma_k > 0.0) || !(c->Ck > 0.0)))
         return ERF_B200_ECONFIG;
     if (c->les_type == ERF_LES_MLP && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
     if (c->molec_diff_type < 0 || c->molec_diff_type > 2) return ERF_B200_ECONFIG;
@@ -166,6 +170,14 @@ void make_params(erf_b200_ctx* c) {
     double cellVolMsf = 1.0 / (g.dxi * 1.0 * g.dyi * 1.0 * g.dzi);
     double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
     P.CsDeltaSqr = f.Cs * f.Cs * DeltaMsf * DeltaMsf;
+    // Deardorff constants (ERF_ComputeTurbulentViscosity.cpp:129-142) and the
+    // buoyancy factor of the TKE source (ERF_DiffusionSrcForState_N.cpp:681-697)
+    P.Delta = DeltaMsf;
+    P.Ck = f.Ck;
+    P.Ce_wall = f.Ce_wall;
+    P.Ce_lcoeff = std::max(0.0, f.Ce - 1.9 * f.Ck);
+    P.g_over_theta0 = std::fabs(f.gravity) * (1.0 / f.theta_ref);
+    P.invSigmaK = 1.0 / f.sigma_k;
     P.invPr = 1.0 / f.Pr_t;
     P.invSc = 1.0 / f.Sc_t;
     P.alphaT_eff = P.use_consA ? f.alpha_T : f.rho0_trans * f.alpha_T;
@@ -251,7 +263,7 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     dim3 cb = cell_block(), cg = cell_grid(g);
 
     TIMED(0, launch_step_begin<R>(P, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
-                                  B.aux[0], B.mut));
+                                  B.aux[0], B.mut, B.tke));
     // stage outputs alternate between the two scratch states so that the last
     // one lands in slot 1-p (or in N1 when Kessler moves it to slot 1-p)
     StateBuf outs[3] = {N0, N1, N0};
@@ -277,8 +289,8 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
             TIMED(1, launch_tau<R>(P, st, Sst.cons, Vnew[0], Vnew[1], Vnew[2], B.mut, B.t11, B.t22, B.t33, B.t12,
                                    B.t13, B.t23));
         }
-        TIMED(2, launch_slow_cell<R>(P, c->tkz, st, Sst, Acur, B.mut, B.hx, B.hy, B.hz, B.Fcons, B.avx, B.avy,
-                                     B.avz));
+        TIMED(2, launch_slow_cell<R>(P, c->tkz, st, Sst, Acur, B.mut, B.hx, B.hy, B.hz, B.tke, B.Fcons, B.avx,
+                                     B.avy, B.avz));
         if (P.moist && P.buoy_type == 2) TIMED(3, launch_plane_avg<R>(P, st, Sst.cons, Acur.prim, c->pavg));
         TIMED(4, launch_slow_mom<R>(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12,
                                     B.t13, B.t23, c->pavg, B.Fmx, B.Fmy, B.Fmz));
@@ -296,7 +308,7 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                          B.avz, SUM.cons, SUM.mz));
         }
         TIMED(7, launch_post<R>(P, c->tkz, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut,
-                                B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
+                                B.tke, B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
     }
     if (P.moist) TIMED(8, (k_kessler_cells<<<cg, cb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
@@ -324,6 +336,9 @@ int alloc_bulk(erf_b200_ctx* c, Bulk<R>& B) {
     A(&B.cA, NZF); A(&B.cInvB, NZF); A(&B.cCB, NZF); A(&B.cP, NZF); A(&B.cQ, NZF);
     if (cfg->les_type == ERF_LES_MLP) {
         A(&B.c12, N); A(&B.c13, N); A(&B.c23, N); A(&B.hx, N); A(&B.hy, N); A(&B.hz, N);
+    }
+    if (cfg->les_type == ERF_LES_DEARDORFF) {
+        A(&B.tke.kthv, N); A(&B.tke.diss, N); A(&B.tke.smn, N); A(&B.tke.hfz, NZF);
     }
     return rc;
 }
@@ -726,7 +741,7 @@ int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, cons
     // the step prologue forms the eddy viscosity from these velocities (its
     // other outputs go to scratch slots of the context)
     launch_step_begin<double>(c->P, c->stream, c->S[0].cons, c->vel[0][0], c->vel[0][1], c->vel[0][2], c->S[1],
-                              c->vel[1][0], c->vel[1][1], c->vel[1][2], c->bd.aux[1], c->bd.mut);
+                              c->vel[1][0], c->vel[1][1], c->vel[1][2], c->bd.aux[1], c->bd.mut, c->bd.tke);
     return cuda_fail(cudaGetLastError());
 }
 
@@ -758,7 +773,8 @@ int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b2
     } else if (P.use_diff) {
         launch_tau<double>(P, st, Sst.cons, V[0], V[1], V[2], B.mut, B.t11, B.t22, B.t33, B.t12, B.t13, B.t23);
     }
-    launch_slow_cell<double>(P, c->tkz, st, Sst, B.aux[0], B.mut, B.hx, B.hy, B.hz, B.Fcons, B.avx, B.avy, B.avz);
+    launch_slow_cell<double>(P, c->tkz, st, Sst, B.aux[0], B.mut, B.hx, B.hy, B.hz, B.tke, B.Fcons, B.avx, B.avy,
+                             B.avz);
     if (P.moist && P.buoy_type == 2) launch_plane_avg<double>(P, st, Sst.cons, B.aux[0].prim, c->pavg);
     launch_slow_mom<double>(P, c->tkz, st, Sst, B.aux[0], V[0], V[1], V[2], B.t11, B.t22, B.t33, B.t12, B.t13, B.t23,
                             c->pavg, B.Fmx, B.Fmy, B.Fmz);
@@ -839,8 +855,8 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
     if ((rc = pack4(c, S_data, nc, SUM.cons, SUM.mx, SUM.my, SUM.mz))) return rc;
     if ((rc = pack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
     // stage state and primitives: those of the preceding slow_rhs_pre
-    launch_post<double>(c->P, c->tkz, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.avx,
-                        B.avy, B.avz, c->vel[1][0], c->vel[1][1], c->vel[1][2]);
+    launch_post<double>(c->P, c->tkz, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.tke,
+                        B.avx, B.avy, B.avz, c->vel[1][0], c->vel[1][1], c->vel[1][2]);
     if ((rc = unpack4(c, S_new, nc, NEW.cons, NEW.mx, NEW.my, NEW.mz))) return rc;
     return cuda_fail(cudaGetLastError());
 }

@@ -103,7 +103,7 @@ template <class R>
 __global__ void k_step_begin(Params P, const double* __restrict__ cons, const double* __restrict__ uo,
                              const double* __restrict__ vo, const double* __restrict__ wo, StateBuf S,
                              double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn,
-                             StageAux<R> A, R* __restrict__ mut) {
+                             StageAux<R> A, R* __restrict__ mut, TkeBuf<R> tke) {
     const Geo& g = P.g;
     int i, j, k;
     if (!cell_coords(g, i, j, k)) return;
@@ -130,7 +130,7 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
     if (k == g.nz - 1) { S.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
     stage_aux_cell<R>(P, cons, A, c, k);
 
-    if (P.les == ERF_LES_SMAGORINSKY || P.les == ERF_LES_MLP) {
+    if (P.les == ERF_LES_SMAGORINSKY || P.les == ERF_LES_MLP || P.les == ERF_LES_DEARDORFF) {
         int ip = wrap(i + 1, g.nx), jp = wrap(j + 1, g.ny);
         double s11 = (uo[cidx(g, ip, j, k)] - uo[c]) * g.dxi;
         double s22 = (vo[cidx(g, i, jp, k)] - vo[c]) * g.dyi;
@@ -142,7 +142,35 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
         double s23 = 0.25 * (strain23(vo, wo, g, i, j, k) + strain23(vo, wo, g, i, j, k + 1) +
                              strain23(vo, wo, g, i, jp, k) + strain23(vo, wo, g, i, jp, k + 1));
         double S2 = s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + 2.0 * s23 * s23;
-        mut[c] = R(P.CsDeltaSqr * rho * sqrt(2.0 * S2));
+        if (P.les != ERF_LES_DEARDORFF) {
+            mut[c] = R(P.CsDeltaSqr * rho * sqrt(2.0 * S2));
+        } else {
+            // Deardorff (ERF_ComputeTurbulentViscosity.cpp:129-229, no MOST):
+            // SmnSmn for the shear production (formed from the step's
+            // velocities, ERF_make_tau_terms.cpp:233-240), K = rho Ck l
+            // sqrt(e) with the stratification-limited length, the vertical
+            // heat diffusivity (1 + 2 l / Delta) K and the dissipation.
+            tke.smn[c] = R(S2);
+            const int64_t N = g.ncell;
+            const int kp = min(k + 1, g.nz - 1), km = max(k - 1, 0);
+            double dtheta_dz = 0.5 * (cons[N + cidx(g, i, j, kp)] / cons[cidx(g, i, j, kp)] -
+                                      cons[N + cidx(g, i, j, km)] / cons[cidx(g, i, j, km)]) * g.dzi;
+            double E = fmax(cons[2 * N + c] / rho, 0.0);
+            double strat = P.g_over_theta0 * dtheta_dz;
+            double length;
+            if (strat <= 2.220446049250313e-16) {   // DBL_EPSILON
+                length = P.Delta;
+            } else {
+                length = 0.76 * sqrt(E / strat);
+                length = fmin(length, P.Delta);
+                length = fmax(length, 0.001 * P.Delta);
+            }
+            double K = rho * P.Ck * length * sqrt(E);
+            mut[c] = R(K);
+            tke.kthv[c] = R((1. + 2. * length / P.Delta) * K);
+            double Ce = ((P.Ce_wall > 0) && (k == 0)) ? P.Ce_wall : 1.9 * P.Ck + P.Ce_lcoeff * length / P.Delta;
+            tke.diss[c] = R(rho * Ce * (E * sqrt(E)) / length);
+        }
     }
 }
 
@@ -225,7 +253,8 @@ __device__ __forceinline__ R adv_flux_z(const Geo& g, const R* __restrict__ phi,
 // 196-667), scalars foextrap at the walls; returns the amount subtracted.
 template <class R>
 __device__ __forceinline__ R scalar_diff(const Params& P, const double* __restrict__ rhoarr, const R* __restrict__ phi,
-                                         const R* __restrict__ mut, double ae_d, double fac_d, int i, int j, int k) {
+                                         const R* __restrict__ mut, double ae_d, double fac_d, int i, int j, int k,
+                                         const R* __restrict__ kv = nullptr, R* __restrict__ fz_out = nullptr) {
     const Geo& g = P.g;
     const R ae = R(ae_d), fac = R(fac_d);
     const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi);
@@ -236,12 +265,22 @@ __device__ __forceinline__ R scalar_diff(const Params& P, const double* __restri
         if (P.use_turb) r += R(0.5) * (ccz(mut, g, i0, j0, k0) * fac + ccz(mut, g, i1, j1, k1) * fac);
         return r;
     };
+    // vertical diffusivity: Deardorff's Theta_v when given
+    auto rAz = [&](int k0, int k1) {
+        if (kv == nullptr) return rA(i, j, k0, i, j, k1);
+        R r = P.use_consA ? R(0.5) * (R(ccz(rhoarr, g, i, j, k0)) + R(ccz(rhoarr, g, i, j, k1))) * ae : ae;
+        return r + R(0.5) * (ccz(kv, g, i, j, k0) + ccz(kv, g, i, j, k1));
+    };
     R fxl = -rA(i, j, k, im, j, k) * (ph(i, j, k) - ph(im, j, k)) * dxi * R(1);
     R fxh = -rA(ip, j, k, i, j, k) * (ph(ip, j, k) - ph(i, j, k)) * dxi * R(1);
     R fyl = -rA(i, j, k, i, jm, k) * (ph(i, j, k) - ph(i, jm, k)) * dyi * R(1);
     R fyh = -rA(i, jp, k, i, j, k) * (ph(i, jp, k) - ph(i, j, k)) * dyi * R(1);
-    R fzl = -rA(i, j, k, i, j, k - 1) * (ph(i, j, k) - ph(i, j, k - 1)) * dzi;
-    R fzh = -rA(i, j, k + 1, i, j, k) * (ph(i, j, k + 1) - ph(i, j, k)) * dzi;
+    R fzl = -rAz(k, k - 1) * (ph(i, j, k) - ph(i, j, k - 1)) * dzi;
+    R fzh = -rAz(k + 1, k) * (ph(i, j, k + 1) - ph(i, j, k)) * dzi;
+    if (fz_out) {   // the z-face fluxes (hfx_z of ERF_DiffusionSrcForState_N.cpp:422-425)
+        fz_out[cidx(g, i, j, k)] = fzl;
+        if (k == g.nz - 1) fz_out[cidx(g, i, j, k + 1)] = fzh;
+    }
     return (fxh - fxl) * dxi * R(1) + (fyh - fyl) * dyi * R(1) + (fzh - fzl) * dzi;
 }
 
@@ -1000,7 +1039,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
                                                                          const R* __restrict__ mut,
                                                                          const R* __restrict__ hx,
                                                                          const R* __restrict__ hy,
-                                                                         const R* __restrict__ hz,
+                                                                         const R* __restrict__ hz, TkeBuf<R> tke,
                                                                          R* __restrict__ Fcons, R* __restrict__ avx,
                                                                          R* __restrict__ avy, R* __restrict__ avz) {
     __shared__ FluxTile<R> sh;
@@ -1041,6 +1080,8 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
                 R fxl = R(0.5) * (hx[cidx(g, im, j, k)] + hx[c]), fxh = R(0.5) * (hx[c] + hx[cidx(g, ip, j, k)]);
                 R fyl = R(0.5) * (hy[cidx(g, i, jm, k)] + hy[c]), fyh = R(0.5) * (hy[c] + hy[cidx(g, i, jp, k)]);
                 frt -= (fxh - fxl) * R(g.dxi) + (fyh - fyl) * R(g.dyi) + (fz(k + 1) - fz(k)) * R(g.dzi);
+            } else if (P.les == ERF_LES_DEARDORFF) {
+                frt -= scalar_diff<R>(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k, tke.kthv, tke.hfz);
             } else if (P.use_diff) {
                 frt -= scalar_diff<R>(P, S.cons, A.prim, mut, P.alphaT_eff, P.invPr, i, j, k);
             }
@@ -1062,44 +1103,49 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
 //   * the stage velocities, and (unless last) the next stage's primitive
 //     variables, Exner function and p'.
 // ---------------------------------------------------------------------------
-constexpr int MAX_SLOW = 4;  // passive scalar + up to three moisture species
-template <class R, int DH, int DV, int MH, int MV>
+// Slow variables, in order: the passive scalar, the moisture species, then
+// (Deardorff) rho*KE.  NS is the kernel's capacity: 4 holds the scalar and
+// three species, 5 adds KE to them.
+template <class R, int DH, int DV, int MH, int MV, int NS>
 __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, int kz, double slow_dt, StateBuf Sold,
                                                                     StateBuf Sst, StateBuf Ssum, StateBuf Snew,
                                                                     StageAux<R> Acur, StageAux<R> Anext, int make_next,
-                                                                    const R* __restrict__ mut,
+                                                                    const R* __restrict__ mut, TkeBuf<R> tke,
                                                                     const R* __restrict__ avx,
                                                                     const R* __restrict__ avy,
                                                                     const R* __restrict__ avz, double* __restrict__ un,
                                                                     double* __restrict__ vn, double* __restrict__ wn) {
-    __shared__ FluxTile<R> sh[MAX_SLOW];
-    __shared__ Plane<R> pl[MAX_SLOW];
+    __shared__ FluxTile<R> sh[NS];
+    __shared__ Plane<R> pl[NS];
     const Geo& g = P.g;
     const int64_t N = g.ncell;
     const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
     const bool ok = i < g.nx && j < g.ny;
     const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
-    const int nslow = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
-    R zl[MAX_SLOW], zh[MAX_SLOW];
+    const bool dd = P.les == ERF_LES_DEARDORFF;
+    const int nscal = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
+    const int nslow = nscal + (dd ? 1 : 0);
+    R zl[NS], zh[NS];
 #pragma unroll
-    for (int q = 0; q < MAX_SLOW; ++q) zl[q] = zh[q] = R(0);
-    auto slow_phi = [&](int q) {
-        return Acur.prim + (int64_t)((q == 0) ? ERF_RHOSCALAR_COMP - 1 : ERF_RHOQ1_COMP + q - 2) * N;
+    for (int q = 0; q < NS; ++q) zl[q] = zh[q] = R(0);
+    auto comp_of = [&](int q) {
+        return q == 0 ? ERF_RHOSCALAR_COMP : (q < nscal ? ERF_RHOQ1_COMP + q - 1 : ERF_RHOKE_COMP);
     };
+    auto slow_phi = [&](int q) { return Acur.prim + (int64_t)(comp_of(q) - 1) * N; };
 #pragma unroll
-    for (int q = 0; q < MAX_SLOW; ++q)
+    for (int q = 0; q < NS; ++q)
         if (q < nslow) load_plane(g, pl[q], slow_phi(q), k0);
     for (int k = k0; k < k1; ++k) {
         plane_wait();
         __syncthreads();
         if (ok) {
 #pragma unroll
-            for (int q = 0; q < MAX_SLOW; ++q) {
+            for (int q = 0; q < NS; ++q) {
                 if (q >= nslow) break;
-                if (q == 0)
-                    tile_put<DH, DV>(g, sh[0], pl[0], slow_phi(0), avx, avy, avz, P.dry_h, P.dry_v, R(P.f_dry_h),
-                                     R(P.f_dry_v), i, j, k, k == k0, zl[0], zh[0]);
+                if (q == 0 || q >= nscal)   // scalar and KE: dry-scalar schemes
+                    tile_put<DH, DV>(g, sh[q], pl[q], slow_phi(q), avx, avy, avz, P.dry_h, P.dry_v, R(P.f_dry_h),
+                                     R(P.f_dry_v), i, j, k, k == k0, zl[q], zh[q]);
                 else
                     tile_put<MH, MV>(g, sh[q], pl[q], slow_phi(q), avx, avy, avz, P.moi_h, P.moi_v, R(P.f_moi_h),
                                      R(P.f_moi_v), i, j, k, k == k0, zl[q], zh[q]);
@@ -1108,25 +1154,36 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
         __syncthreads();
         if (k + 1 < k1) {   // next level's planes arrive during the update below
 #pragma unroll
-            for (int q = 0; q < MAX_SLOW; ++q)
+            for (int q = 0; q < NS; ++q)
                 if (q < nslow) load_plane(g, pl[q], slow_phi(q), k + 1);
         }
         if (ok) {
             int64_t c = cidx(g, i, j, k);
 #pragma unroll
-            for (int q = 0; q < MAX_SLOW; ++q) {
+            for (int q = 0; q < NS; ++q) {
                 if (q >= nslow) break;
-                int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOQ1_COMP + q - 1;
+                const int n = comp_of(q);
                 R r = tile_div(g, sh[q], zl[q], zh[q]);
                 zl[q] = zh[q];
-                if (P.use_diff)
-                    r -= scalar_diff<R>(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc, i, j, k);
+                if (q < nscal) {
+                    if (P.use_diff)
+                        r -= scalar_diff<R>(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, P.alphaC_eff, P.invSc,
+                                            i, j, k);
+                } else {
+                    // KE diffusion (alpha 0, K / sigma_k) and the TKE sources of
+                    // ERF_DiffusionSrcForState_N.cpp:681-707: buoyancy, shear
+                    // production, dissipation
+                    r -= scalar_diff<R>(P, Sst.cons, Acur.prim + (int64_t)(n - 1) * N, mut, 0.0, P.invSigmaK, i, j, k);
+                    r += R(P.g_over_theta0) * tke.hfz[c];
+                    r += R(2.0) * mut[c] * tke.smn[c];
+                    r -= tke.diss[c];
+                }
                 double v_ = Sold.cons[n * N + c] + slow_dt * double(r);
-                Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 0.0);
+                Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, q < nscal ? 0.0 : 2.220446049250313e-16);
             }
             Snew.cons[c] = Ssum.cons[c];
             Snew.cons[N + c] = Ssum.cons[N + c];
-            Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
+            if (!dd) Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
             Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
             double rho = Ssum.cons[c];
             {
@@ -1510,13 +1567,14 @@ dim3 cell_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.n
 constexpr int U5 = ERF_ADV_UPWIND_5TH, W5 = ERF_ADV_WENO_5;
 
 template <class R>
-using SlowCellK = void (*)(Params, int, StateBuf, StageAux<R>, const R*, const R*, const R*, const R*, R*, R*, R*, R*);
+using SlowCellK = void (*)(Params, int, StateBuf, StageAux<R>, const R*, const R*, const R*, const R*, TkeBuf<R>, R*, R*,
+                           R*, R*);
 template <class R>
 using SlowMomK = void (*)(Params, int, StateBuf, StageAux<R>, const double*, const double*, const double*, const R*,
                           const R*, const R*, const R*, const R*, const R*, const double*, R*, R*, R*);
 template <class R>
 using PostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, StateBuf, StageAux<R>, StageAux<R>, int,
-                       const R*, const R*, const R*, const R*, double*, double*, double*);
+                       const R*, TkeBuf<R>, const R*, const R*, const R*, double*, double*, double*);
 
 template <class R>
 SlowCellK<R> slow_cell_kernel(const Params& P) {
@@ -1533,15 +1591,21 @@ template <class R>
 PostK<R> post_kernel(const Params& P) {
     bool dw = P.dry_h == W5 && P.dry_v == W5, du = P.dry_h == U5 && P.dry_v == U5;
     bool mw = P.moi_h == W5 && P.moi_v == W5, mu = P.moi_h == U5 && P.moi_v == U5;
+    const int nslow = (P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1) + (P.les == ERF_LES_DEARDORFF ? 1 : 0);
     if (!P.moist) {
-        if (dw) return k_post<R, W5, W5, -1, -1>;
-        if (du) return k_post<R, U5, U5, -1, -1>;
+        if (dw) return k_post<R, W5, W5, -1, -1, 4>;
+        if (du) return k_post<R, U5, U5, -1, -1, 4>;
+    } else if (nslow <= 4) {
+        if (dw && mw) return k_post<R, W5, W5, W5, W5, 4>;
+        if (du && mu) return k_post<R, U5, U5, U5, U5, 4>;
+        if (du && mw) return k_post<R, U5, U5, W5, W5, 4>;
     } else {
-        if (dw && mw) return k_post<R, W5, W5, W5, W5>;
-        if (du && mu) return k_post<R, U5, U5, U5, U5>;
-        if (du && mw) return k_post<R, U5, U5, W5, W5>;
+        if (dw && mw) return k_post<R, W5, W5, W5, W5, 5>;
+        if (du && mu) return k_post<R, U5, U5, U5, U5, 5>;
+        if (du && mw) return k_post<R, U5, U5, W5, W5, 5>;
+        return k_post<R, -1, -1, -1, -1, 5>;
     }
-    return k_post<R, -1, -1, -1, -1>;
+    return k_post<R, -1, -1, -1, -1, 4>;
 }
 
 }  // namespace
@@ -1571,8 +1635,9 @@ int vert_setup(size_t vert_smem, size_t coef_smem) {
 
 template <class R>
 void launch_step_begin(const Params& P, cudaStream_t st, const double* cons, const double* uo, const double* vo,
-                       const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut) {
-    k_step_begin<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, uo, vo, wo, S, un, vn, wn, A, mut);
+                       const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut,
+                       TkeBuf<R> tke) {
+    k_step_begin<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, uo, vo, wo, S, un, vn, wn, A, mut, tke);
 }
 template <class R>
 void launch_stage_aux(const Params& P, cudaStream_t st, const double* cons, StageAux<R> A) {
@@ -1610,9 +1675,9 @@ void launch_fast_vert(const Params& P, cudaStream_t st, dim3 grid, dim3 block, s
 }
 template <class R>
 void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const R* mut,
-                      const R* hx, const R* hy, const R* hz, R* Fcons, R* avx, R* avy, R* avz) {
+                      const R* hx, const R* hy, const R* hz, TkeBuf<R> tke, R* Fcons, R* avx, R* avy, R* avz) {
     slow_cell_kernel<R>(P)<<<tile_grid(P.g, t.cell), dim3(TTX, TTY, 1), 0, st>>>(P, t.cell, S, A, mut, hx, hy, hz,
-                                                                                  Fcons, avx, avy, avz);
+                                                                                  tke, Fcons, avx, avy, avz);
 }
 template <class R>
 void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
@@ -1624,17 +1689,18 @@ void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBu
 template <class R>
 void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
                  StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
-                 const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
+                 TkeBuf<R> tke, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
     post_kernel<R>(P)<<<tile_grid(P.g, t.post), dim3(TTX, TTY, 1), 0, st>>>(P, t.post, slow_dt, Sold, Sst, Ssum, Snew,
-                                                                             Acur, Anext, make_next, mut, avx, avy,
-                                                                             avz, un, vn, wn);
+                                                                             Acur, Anext, make_next, mut, tke, avx,
+                                                                             avy, avz, un, vn, wn);
 }
 
 #define ERFB_INSTANTIATE(R)                                                                                          \
     template void tiled_setup<R>(const Params&, TiledKz*);                                                           \
     template int vert_setup<R>(size_t, size_t);                                                                      \
     template void launch_step_begin<R>(const Params&, cudaStream_t, const double*, const double*, const double*,     \
-                                       const double*, StateBuf, double*, double*, double*, StageAux<R>, R*);         \
+                                       const double*, StateBuf, double*, double*, double*, StageAux<R>, R*,          \
+                                       TkeBuf<R>);                                                                   \
     template void launch_tau<R>(const Params&, cudaStream_t, const double*, const double*, const double*,            \
                                 const double*, const R*, R*, R*, R*, R*, R*, R*);                                    \
     template void launch_plane_avg<R>(const Params&, cudaStream_t, const double*, const R*, double*);                \
@@ -1648,13 +1714,13 @@ void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow
                                       const double*, const double*, const R*, const R*, const R*, const R*,          \
                                       const R*, R*, double*, double*);                                               \
     template void launch_slow_cell<R>(const Params&, const TiledKz&, cudaStream_t, StateBuf, StageAux<R>, const R*,  \
-                                      const R*, const R*, const R*, R*, R*, R*, R*);                                 \
+                                      const R*, const R*, const R*, TkeBuf<R>, R*, R*, R*, R*);                      \
     template void launch_slow_mom<R>(const Params&, const TiledKz&, cudaStream_t, StateBuf, StageAux<R>,             \
                                      const double*, const double*, const double*, const R*, const R*, const R*,      \
                                      const R*, const R*, const R*, const double*, R*, R*, R*);                       \
     template void launch_post<R>(const Params&, const TiledKz&, cudaStream_t, double, StateBuf, StateBuf, StateBuf,  \
-                                 StateBuf, StageAux<R>, StageAux<R>, int, const R*, const R*, const R*, const R*,    \
-                                 double*, double*, double*);
+                                 StateBuf, StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, const R*, const R*,   \
+                                 const R*, double*, double*, double*);
 
 ERFB_INSTANTIATE(double)
 ERFB_INSTANTIATE(float)

@@ -12,6 +12,8 @@ struct Params {
     int moist, kessler_rain;
     int use_diff, use_turb, use_consA, les;
     double CsDeltaSqr;          // Cs^2 Delta^2 (host-computed, reference order)
+    double Delta;               // (dx dy dz)^(1/3)
+    double Ck, Ce_wall, Ce_lcoeff, g_over_theta0, invSigmaK;   // Deardorff constants
     double invPr, invSc;
     double alphaT_eff, alphaC_eff; // rhoAlpha (Constant) or alpha (ConstantAlpha)
     double mu_eff;              // 2*dynamicViscosity (/rho0_trans for ConstantAlpha)
@@ -43,6 +45,17 @@ struct StageAux {
     R* pp;     // ncell (p - p0)
 };
 
+// Deardorff TKE closure arrays (R): vertical heat diffusivity Theta_v,
+// dissipation and SmnSmn per cell, theta's vertical diffusive flux per z-face
+// (hfx_z).  All null for the other closures.
+template <class R>
+struct TkeBuf {
+    R* kthv;
+    R* diss;
+    R* smn;
+    R* hfz;
+};
+
 // x-y tile of the transport kernels (slow_cell, slow_mom, post) and the
 // levels each of their blocks marches through (chosen per context).
 constexpr int TTX = 32, TTY = 8;
@@ -58,7 +71,8 @@ template <class R>
 int vert_setup(size_t vert_smem, size_t coef_smem);
 template <class R>
 void launch_step_begin(const Params& P, cudaStream_t st, const double* cons, const double* uo, const double* vo,
-                       const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut);
+                       const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut,
+                       TkeBuf<R> tke);
 template <class R>
 void launch_tau(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
                 const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23);
@@ -81,7 +95,7 @@ void launch_fast_vert(const Params& P, cudaStream_t st, dim3 grid, dim3 block, s
                       double* out_mz);
 template <class R>
 void launch_slow_cell(const Params& P, const TiledKz& t, cudaStream_t st, StateBuf S, StageAux<R> A, const R* mut,
-                      const R* hx, const R* hy, const R* hz, R* Fcons, R* avx, R* avy, R* avz);
+                      const R* hx, const R* hy, const R* hz, TkeBuf<R> tke, R* Fcons, R* avx, R* avy, R* avz);
 
 // Learned closure (closure.cu): network arrays on the device, the fused
 // stress / heat-flux kernel with its edge averaging, and feature extraction.
@@ -107,6 +121,6 @@ void launch_slow_mom(const Params& P, const TiledKz& t, cudaStream_t st, StateBu
 template <class R>
 void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
                  StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
-                 const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
+                 TkeBuf<R> tke, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
 
 }  // namespace erfb

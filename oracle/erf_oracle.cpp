@@ -27,6 +27,7 @@
 // ============================================================================
 
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -489,15 +490,46 @@ struct Oracle {
         Bx txy = grow(Bx{{0, 0, 0}, {nx, ny, nz - 1}}, 1, 1, 0);
         Bx txz = grow(Bx{{0, 0, 0}, {nx, ny - 1, nz}}, 1, 1, 0);
         Bx tyz = grow(Bx{{0, 0, 0}, {nx - 1, ny, nz}}, 1, 1, 0);
-        compute_strain(bxcc, txy, txz, tyz, V.u, V.v, V.w, t11, t22, t33, t12, t13, t23);
-        double Cs = c.Cs;
-        loop(valid(CC), [&](int i, int j, int k) {
-            double S = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23);
-            double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dxInv[2]);
-            double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
-            double CsDeltaSqrMsf = Cs * Cs * DeltaMsf * DeltaMsf;
-            mut(i, j, k) = CsDeltaSqrMsf * cons(i, j, k, 0) * std::sqrt(2.0 * S);
-        });
+        if (c.les_type == ERF_LES_DEARDORFF) {
+            // ERF_ComputeTurbulentViscosity.cpp:129-229 (no terrain, no MOST)
+            const double l_C_k = c.Ck, l_C_e = c.Ce, l_C_e_wall = c.Ce_wall;
+            const double Ce_lcoeff = std::max(0.0, l_C_e - 1.9 * l_C_k);
+            const double l_abs_g = std::fabs(c.gravity), l_inv_theta0 = 1.0 / c.theta_ref;
+            loop(valid(CC), [&](int i, int j, int k) {
+                double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dxInv[2]);
+                double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
+                double eps = std::numeric_limits<double>::epsilon();
+                double dtheta_dz = 0.5 * (cons(i, j, k + 1, 1) / cons(i, j, k + 1, 0) -
+                                          cons(i, j, k - 1, 1) / cons(i, j, k - 1, 0)) * dxInv[2];
+                double E = std::max(cons(i, j, k, ERF_RHOKE_COMP) / cons(i, j, k, 0), 0.0);
+                double stratification = l_abs_g * dtheta_dz * l_inv_theta0;
+                double length;
+                if (stratification <= eps) {
+                    length = DeltaMsf;
+                } else {
+                    length = 0.76 * std::sqrt(E / stratification);
+                    length = std::min(length, DeltaMsf);
+                    length = std::max(length, 0.001 * DeltaMsf);
+                }
+                mut(i, j, k) = cons(i, j, k, 0) * l_C_k * length * std::sqrt(E);
+                kthv(i, j, k) = (1. + 2. * length / DeltaMsf) * mut(i, j, k);
+                double Ce = ((l_C_e_wall > 0) && (k == 0)) ? l_C_e_wall : 1.9 * l_C_k + Ce_lcoeff * length / DeltaMsf;
+                diss(i, j, k) = cons(i, j, k, 0) * Ce * std::pow(E, 1.5) / length;
+            });
+            fill_periodic(kthv, CC);
+            for (int j = -1; j <= ny; ++j)
+                for (int i = -1; i <= nx; ++i) { kthv(i, j, -1) = kthv(i, j, 0); kthv(i, j, nz) = kthv(i, j, nz - 1); }
+        } else {
+            compute_strain(bxcc, txy, txz, tyz, V.u, V.v, V.w, t11, t22, t33, t12, t13, t23);
+            double Cs = c.Cs;
+            loop(valid(CC), [&](int i, int j, int k) {
+                double S = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23);
+                double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dxInv[2]);
+                double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
+                double CsDeltaSqrMsf = Cs * Cs * DeltaMsf * DeltaMsf;
+                mut(i, j, k) = CsDeltaSqrMsf * cons(i, j, k, 0) * std::sqrt(2.0 * S);
+            });
+        }
         // FillBoundary (periodic) then top/bottom extrapolation
         fill_periodic(mut, CC);
         for (int j = -1; j <= ny; ++j)
@@ -509,6 +541,7 @@ struct Oracle {
     // moisture: 1/Sc_t.
     double eddy_factor(int prim_index) const {
         if (prim_index == 0) return 1.0 / c.Pr_t;
+        if (prim_index == 1 || prim_index == 2) return 1.0 / c.sigma_k;   // KE, QKE
         return 1.0 / c.Sc_t;
     }
     double alpha_eff(int prim_index) const {
@@ -542,14 +575,29 @@ struct Oracle {
                 if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j - 1, k));
                 fy(i, j, k) = -rA * (prim(i, j, k, pidx) - prim(i, j - 1, k, pidx)) * dxInv[1] * 1.0;
             });
+            const bool dd = c.les_type == ERF_LES_DEARDORFF;
             loop(valid(ZF), [&](int i, int j, int k) {
                 double rA = use_consA ? 0.5 * (cell_data(i, j, k, 0) + cell_data(i, j, k - 1, 0)) * ae : ae;
-                if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j, k - 1));
+                if (use_turb) {
+                    // Deardorff's vertical heat diffusivity is EddyDiff::Theta_v
+                    if (dd && pidx == 0) rA += 0.5 * (kthv(i, j, k) + kthv(i, j, k - 1));
+                    else rA += 0.5 * (mu(i, j, k) + mu(i, j, k - 1));
+                }
                 fz(i, j, k) = -rA * (prim(i, j, k, pidx) - prim(i, j, k - 1, pidx)) * dxInv[2];
+                if (q == ERF_RHOTHETA_COMP) hfz(i, j, k) = fz(i, j, k);   // hfx_z, :422-425
             });
             loop(valid(CC), [&](int i, int j, int k) {
                 rhs(i, j, k, q) -= (fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] * 1.0 + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] * 1.0 + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2];
             });
+            if (dd && q == ERF_RHOKE_COMP) {
+                // TKE sources (:681-707): buoyancy, shear production, dissipation
+                const double l_abs_g = std::fabs(c.gravity), l_inv_theta0 = 1.0 / c.theta_ref;
+                loop(valid(CC), [&](int i, int j, int k) {
+                    rhs(i, j, k, q) += l_abs_g * l_inv_theta0 * hfz(i, j, k);
+                    rhs(i, j, k, q) += 2.0 * mut(i, j, k) * smn(i, j, k);
+                    rhs(i, j, k, q) -= diss(i, j, k);
+                });
+            }
         }
     }
 
@@ -587,6 +635,7 @@ struct Oracle {
     State S_old, S_new, S_sum, S_scr, F_slow;
     Vel Vnew;
     Fab prim, pi_stage, mut, fast_coeffs;
+    mutable Fab kthv, diss, smn, hfz;   // Deardorff: Theta_v diffusivity, dissipation, SmnSmn, theta's vertical flux
     Fab xsrc, ysrc, zsrc;
 
     void init_storage() {
@@ -595,6 +644,8 @@ struct Oracle {
         alloc(prim, CC, ngc, nprim);
         alloc(pi_stage, CC, ngc, 1);
         alloc_cc1(mut);
+        alloc_cc1(kthv); alloc_cc1(diss); alloc_cc1(smn);
+        alloc(hfz, ZF, 0, 1);
         alloc(fast_coeffs, ZF, 0, 5);
         alloc(xsrc, XF, 1, 1); alloc(ysrc, YF, 1, 1); alloc(zsrc, ZF, 1, 1);
     }
@@ -699,6 +750,11 @@ struct Oracle {
             er(i, j, k) = (u(i + 1, j, k) - u(i, j, k)) * dxInv[0] + (v(i, j + 1, k) - v(i, j, k)) * dxInv[1] + (w(i, j, k + 1) - w(i, j, k)) * dxInv[2];
         });
         compute_strain(bxcc, txy, txz, tyz, u, v, w, s11, s22, s33, s12, s13, s23);
+        if (c.les_type == ERF_LES_DEARDORFF && tau_nrk == 0) {
+            // SmnSmn for the TKE shear production (ERF_make_tau_terms.cpp:233-240)
+            Fab& sm = smn;
+            loop(valid(CC), [&](int i, int j, int k) { sm(i, j, k) = smnsmn(i, j, k, s11, s22, s33, s12, s13, s23); });
+        }
         double mu_eff = use_consA ? 2.0 * c.dynamic_viscosity / c.rho0_trans : 2.0 * c.dynamic_viscosity;
         const double OneThird = 1. / 3.;
         Bx exy = Bx{{0, 0, 0}, {nx, ny, nz - 1}}, exz = Bx{{0, 0, 0}, {nx, ny - 1, nz}}, eyz = Bx{{0, 0, 0}, {nx - 1, ny, nz}};
@@ -732,7 +788,9 @@ struct Oracle {
 
     // erf_slow_rhs_pre (TimeIntegration/ERF_slow_rhs_pre.cpp:67-774), no terrain,
     // no anelastic, no mono advection, periodic laterally.
+    int tau_nrk = -1;   // stage of the current make_tau call (SmnSmn is formed at stage 0)
     void slow_rhs_pre(int nrk, double dt, State& R, const State& S, State& Scr, const Vel& V) {
+        tau_nrk = nrk;
         (void)nrk; (void)dt;
         make_mom_sources(S, prim);
         Fab t11, t22, t33, t12, t13, t23;
@@ -1069,11 +1127,19 @@ struct Oracle {
             advect_scalars(start, num_adv, Scr.mx, Scr.my, Scr.mz, prim, R.cons, htype, vtype, hf, vf);
             if (use_diff) diffusion_state(start, num_adv, Snew.cons, prim, R.cons, mut);
         };
+        const bool dd = c.les_type == ERF_LES_DEARDORFF;
+        if (dd)   // RhoKE is a slow variable with Deardorff (ERF_slow_rhs_post.cpp:169-172, 366-399)
+            do_var(ERF_RHOKE_COMP, 1, c.dryscal_horiz_adv, c.dryscal_vert_adv, c.dryscal_horiz_upw_frac, c.dryscal_vert_upw_frac);
         do_var(ERF_RHOSCALAR_COMP, 1, c.dryscal_horiz_adv, c.dryscal_vert_adv, c.dryscal_horiz_upw_frac, c.dryscal_vert_upw_frac);
         int nq = ncomp - ERF_RHOQ1_COMP;
         if (use_moisture && nq > 0)
             do_var(ERF_RHOQ1_COMP, nq, c.moistscal_horiz_adv, c.moistscal_vert_adv, c.moistscal_horiz_upw_frac, c.moistscal_vert_upw_frac);
         loop(valid(CC), [&](int i, int j, int k) {
+            if (dd) {
+                int n = ERF_RHOKE_COMP;
+                Sd.cons(i, j, k, n) = Sold.cons(i, j, k, n) + dt * R.cons(i, j, k, n);
+                Sd.cons(i, j, k, n) = std::max(Sd.cons(i, j, k, n), std::numeric_limits<double>::epsilon());
+            }
             int n = ERF_RHOSCALAR_COMP;
             Sd.cons(i, j, k, n) = Sold.cons(i, j, k, n) + dt * R.cons(i, j, k, n);
             if (use_moisture)

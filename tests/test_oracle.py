@@ -86,3 +86,30 @@ def test_splitmix64_stream_is_fixed():
     # first outputs of SplitMix64 seeded with 0 (Steele et al. 2014), top 53 bits
     ref = np.array([0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F], dtype=np.uint64)
     assert np.array_equal(r, (ref >> np.uint64(11)).astype(np.float64) / 2.0 ** 53)
+
+
+def test_oracle_deardorff_stationary_shear():
+    """Deardorff known answer (cf. the reference's Deardorff_stationary test):
+    in uniform shear u = S z with neutral theta, shear production
+    2 K SmnSmn = Ck Delta sqrt(e) S^2 balances dissipation Ce e^1.5 / Delta at
+    e = Ck/Ce (S Delta)^2, so interior cells keep that TKE."""
+    from erf_b200 import config as C
+    case = cases.abl_deardorff(nx=8, ny=8, nz=32)
+    cfg = case.cfg
+    cfg.use_coriolis = 0
+    cfg.abl_geo_forcing[0] = cfg.abl_geo_forcing[1] = 0.0
+    cfg.zlo_bc = cfg.zhi_bc = C.BC_SLIP_WALL
+    case.theta_cc = np.full(cfg.nz, 300.0)
+    case.pert = {}
+    base = oracle.make_base_state(cfg, case)
+    cons, u, v, w = case.build_state(base[0])
+    S = 0.01
+    z = (np.arange(cfg.nz) + 0.5) * cfg.dz
+    u[:] = (S * z)[:, None, None]
+    delta = (cfg.dx * cfg.dy * cfg.dz) ** (1.0 / 3.0)
+    e_eq = cfg.Ck / cfg.Ce * (S * delta) ** 2
+    cons[2] = cons[0] * e_eq
+    c2, *_ = oracle.advance(cfg, base, cons, u, v, w, 1)
+    e = c2[2] / c2[0]
+    inner = slice(12, 20)
+    assert np.max(np.abs(e[inner] / e_eq - 1.0)) < 1e-10
