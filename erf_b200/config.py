@@ -55,7 +55,8 @@ class ErfConfig(ctypes.Structure):
         ("coriolis_factor", ctypes.c_double), ("sinphi", ctypes.c_double), ("cosphi", ctypes.c_double),
         ("abl_geo_forcing", ctypes.c_double * 3),
         ("precision", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("use_terrain", ctypes.c_int),
+        ("reserved", ctypes.c_int * 6),
     ]
 
     def copy(self) -> "ErfConfig":

@@ -156,7 +156,10 @@ typedef struct erf_b200_config {
 
     /* arithmetic of the bulk (ERF_PREC_*) */
     int    precision;
-    int    reserved[7];
+    /* static terrain-following grid (SolverChoice::use_terrain with
+     * terrain_type Static): z_phys_nd installed by erf_b200_set_terrain */
+    int    use_terrain;
+    int    reserved[6];
 } erf_b200_config;
 
 /* Opaque context: owns all integrator scratch (S_sum, S_scratch, F_slow,

@@ -77,3 +77,58 @@ def interp(kind: int, s6, upw: float, frac: float = 1.0) -> float:
 
 def qsatw(t: float, p_hpa: float) -> float:
     return lib().oracle_qsatw(float(t), float(p_hpa))
+
+
+def _setup_terrain(L):
+    if getattr(L, "_terrain_ready", False):
+        return
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.oracle_make_base_state_terrain.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_double, dp, dp, dp, dp]
+    L.oracle_make_base_state_terrain.restype = ctypes.c_int
+    L.oracle_terrain_metrics.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp]
+    L.oracle_terrain_metrics.restype = ctypes.c_int
+    L.oracle_advance_terrain.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_int]
+    L.oracle_advance_terrain.restype = ctypes.c_int
+    L._terrain_ready = True
+
+
+def make_base_state_terrain(case):
+    """Base state over the terrain: four arrays of (nz+2)*ny*nx values."""
+    cfg = case.cfg
+    L = lib()
+    _setup_terrain(L)
+    n = (cfg.nz + 2) * cfg.ny * cfg.nx
+    out = [np.zeros(n) for _ in range(4)]
+    z = np.ascontiguousarray(case.z_nd, dtype=np.float64)
+    th = np.ascontiguousarray(case.theta3, dtype=np.float64)
+    qv = np.ascontiguousarray(case.qv3, dtype=np.float64)
+    L.oracle_make_base_state_terrain(ctypes.byref(cfg), _p(z), _p(th), _p(qv), case.theta_sfc, case.qv_sfc,
+                                     case.p_sfc, *[_p(a) for a in out])
+    return out
+
+
+def terrain_metrics(cfg, z_nd):
+    """detJ, z_cc [nz][ny][nx], ax [nz][ny][nx+1], ay [nz][ny+1][nx]."""
+    L = lib()
+    _setup_terrain(L)
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    detJ = np.zeros((nz, ny, nx)); zcc = np.zeros((nz, ny, nx))
+    ax = np.zeros((nz, ny, nx + 1)); ay = np.zeros((nz, ny + 1, nx))
+    z = np.ascontiguousarray(z_nd, dtype=np.float64)
+    L.oracle_terrain_metrics(ctypes.byref(cfg), _p(z), _p(detJ), _p(zcc), _p(ax), _p(ay))
+    return detJ, zcc, ax, ay
+
+
+def advance_terrain(cfg, z_nd, base, cons, u, v, w, nsteps):
+    """Advance copies of the dense state over terrain by nsteps."""
+    L = lib()
+    _setup_terrain(L)
+    cons, u, v, w = (np.ascontiguousarray(a, dtype=np.float64).copy() for a in (cons, u, v, w))
+    r0, p0, pi0, th0 = (np.ascontiguousarray(a, dtype=np.float64) for a in base)
+    z = np.ascontiguousarray(z_nd, dtype=np.float64)
+    rc = L.oracle_advance_terrain(ctypes.byref(cfg), _p(z), _p(r0), _p(p0), _p(pi0), _p(th0),
+                                  _p(cons), _p(u), _p(v), _p(w), int(nsteps))
+    if rc != 0:
+        raise RuntimeError("oracle_advance_terrain failed: %d" % rc)
+    return cons, u, v, w

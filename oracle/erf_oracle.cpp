@@ -284,7 +284,8 @@ struct Oracle {
         if (!cons_only) {
             physbcs_tangential(V.u, XF, ng_vel);
             physbcs_tangential(V.v, YF, ng_vel);
-            physbcs_w(V.w, ng_vel);
+            if (terrain) physbcs_w_T(V.w, V.u, V.v, ng_vel);
+            else physbcs_w(V.w, ng_vel);
             vel_to_mom(V.u, V.v, V.w, S.cons, S.mx, S.my, S.mz);
         }
         fill_periodic(S.cons, CC); fill_periodic(S.mx, XF); fill_periodic(S.my, YF); fill_periodic(S.mz, ZF);
@@ -496,11 +497,13 @@ struct Oracle {
             const double Ce_lcoeff = std::max(0.0, l_C_e - 1.9 * l_C_k);
             const double l_abs_g = std::fabs(c.gravity), l_inv_theta0 = 1.0 / c.theta_ref;
             loop(valid(CC), [&](int i, int j, int k) {
-                double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dxInv[2]);
+                double dzInv = dxInv[2];
+                if (terrain) dzInv /= hzeta_cc(i, j, k);   // the grid is deformed in z only
+                double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dzInv);
                 double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
                 double eps = std::numeric_limits<double>::epsilon();
                 double dtheta_dz = 0.5 * (cons(i, j, k + 1, 1) / cons(i, j, k + 1, 0) -
-                                          cons(i, j, k - 1, 1) / cons(i, j, k - 1, 0)) * dxInv[2];
+                                          cons(i, j, k - 1, 1) / cons(i, j, k - 1, 0)) * dzInv;
                 double E = std::max(cons(i, j, k, ERF_RHOKE_COMP) / cons(i, j, k, 0), 0.0);
                 double stratification = l_abs_g * dtheta_dz * l_inv_theta0;
                 double length;
@@ -520,11 +523,19 @@ struct Oracle {
             for (int j = -1; j <= ny; ++j)
                 for (int i = -1; i <= nx; ++i) { kthv(i, j, -1) = kthv(i, j, 0); kthv(i, j, nz) = kthv(i, j, nz - 1); }
         } else {
-            compute_strain(bxcc, txy, txz, tyz, V.u, V.v, V.w, t11, t22, t33, t12, t13, t23);
+            if (terrain) {
+                Fab t21, t31, t32;
+                alloc_edges(t21, t31, t32);
+                compute_strain_T(bxcc, txy, txz, tyz, V.u, V.v, V.w, t11, t22, t33, t12, t13, t21, t23, t31, t32);
+            } else {
+                compute_strain(bxcc, txy, txz, tyz, V.u, V.v, V.w, t11, t22, t33, t12, t13, t23);
+            }
             double Cs = c.Cs;
             loop(valid(CC), [&](int i, int j, int k) {
                 double S = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23);
-                double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dxInv[2]);
+                double dzInv = dxInv[2];
+                if (terrain) dzInv /= hzeta_cc(i, j, k);
+                double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dzInv);
                 double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
                 double CsDeltaSqrMsf = Cs * Cs * DeltaMsf * DeltaMsf;
                 mut(i, j, k) = CsDeltaSqrMsf * cons(i, j, k, 0) * std::sqrt(2.0 * S);
@@ -622,7 +633,7 @@ struct Oracle {
                 fz(i, j, k) = az(i, j, k) * interp(vtype, s, az(i, j, k), vfrac);
             });
             loop(valid(CC), [&](int i, int j, int k) {
-                double invdetJ = 1.;
+                double invdetJ = terrain ? 1. / detJ(i, j, k) : 1.;
                 double mfsq = 1.0;
                 rhs(i, j, k, q) = -invdetJ * mfsq * ((fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2]);
             });
@@ -662,16 +673,16 @@ struct Oracle {
         if (!use_moisture) {
             if (c.buoyancy_type == 1) {
                 loop(tbz_b, [&](int i, int j, int k) {
-                    zsrc(i, j, k) = g2 * 0.5 * ((cd(i, j, k, 0) - r0[k + 1]) + (cd(i, j, k - 1, 0) - r0[k]));
+                    zsrc(i, j, k) = g2 * 0.5 * ((cd(i, j, k, 0) - R0(i, j, k)) + (cd(i, j, k - 1, 0) - R0(i, j, k - 1)));
                 });
             } else {
                 // dry types 2/3 (T' based) use the base state p0
                 loop(tbz_b, [&](int i, int j, int k) {
-                    auto T0 = [&](int kk) { double rt0 = getRhoThetagivenP(p0[kk + 1]); return (rt0 / r0[kk + 1]) / std::pow(p_0 / p0[kk + 1], rdOcp); };
+                    auto T0 = [&](int kk) { double rt0 = getRhoThetagivenP(P0(i, j, kk)); return (rt0 / R0(i, j, kk)) / std::pow(p_0 / P0(i, j, kk), rdOcp); };
                     double t0_hi = T0(k), t_hi = getTgivenRandRTh(cd(i, j, k, 0), cd(i, j, k, 1));
                     double t0_lo = T0(k - 1), t_lo = getTgivenRandRTh(cd(i, j, k - 1, 0), cd(i, j, k - 1, 1));
                     double qplus = (t_hi - t0_hi) / t0_hi, qminus = (t_lo - t0_lo) / t0_lo;
-                    double r0_q_avg = 0.5 * (r0[k + 1] * qplus + r0[k] * qminus);
+                    double r0_q_avg = 0.5 * (R0(i, j, k) * qplus + R0(i, j, k - 1) * qminus);
                     zsrc(i, j, k) = -r0_q_avg * g2;
                 });
             }
@@ -793,10 +804,15 @@ struct Oracle {
         tau_nrk = nrk;
         (void)nrk; (void)dt;
         make_mom_sources(S, prim);
-        Fab t11, t22, t33, t12, t13, t23;
+        Fab t11, t22, t33, t12, t13, t23, t21, t31, t32;
         if (use_diff) {
-            alloc_cc1(t11); alloc_cc1(t22); alloc_cc1(t33); alloc_edges(t12, t13, t23);
-            make_tau(V, S, t11, t22, t33, t12, t13, t23);
+            if (terrain) {
+                alloc_tau_T(t11, t22, t33, t12, t13, t21, t23, t31, t32);
+                make_tau_T(V, S, t11, t22, t33, t12, t13, t21, t23, t31, t32);
+            } else {
+                alloc_cc1(t11); alloc_cc1(t22); alloc_cc1(t33); alloc_edges(t12, t13, t23);
+                make_tau(V, S, t11, t22, t33, t12, t13, t23);
+            }
         }
         std::fill(R.mz.d.begin(), R.mz.d.end(), 0.0);
         const Fab& cd = S.cons;
@@ -805,23 +821,41 @@ struct Oracle {
         Bx gbx = grow(valid(CC), 1, 1, 1); gbx.lo[2] = 0;
         loop(gbx, [&](int i, int j, int k) {
             double qv = use_moisture ? cd(i, j, k, ERF_RHOQ1_COMP) / cd(i, j, k, 0) : 0.0;
-            pp(i, j, k) = getPgivenRTh(cd(i, j, k, 1), qv) - p0[k + 1];
+            pp(i, j, k) = getPgivenRTh(cd(i, j, k, 1), qv) - P0(i, j, k);
         });
-        // Omega = rho_w (no terrain), on z-faces grown by one laterally
+        // Contravariant momentum Omega (ERF_slow_rhs_pre.cpp:365-420): rho_w
+        // without terrain; with terrain OmegaFromW on the interior faces, 0 at
+        // and below the bottom face, rho_w above the top face.
+        Fab Om; alloc(Om, ZF, 2, 1);
+        loop(grow(valid(ZF), 1, 1, 1), [&](int i, int j, int k) {
+            if (!terrain) Om(i, j, k) = S.mz(i, j, k);
+            else if (k <= 0) Om(i, j, k) = 0.;
+            else if (k >= nz + 1) Om(i, j, k) = S.mz(i, j, k);
+            else Om(i, j, k) = omega_from_w(i, j, k, S.mz(i, j, k), S.mx, S.my);
+        });
         // AdvectionSrcForRho (Advection/ERF_AdvectionSrcForState.cpp:30-93)
         Fab fx, fy, fz;
         alloc(fx, XF, 0, 1); alloc(fy, YF, 0, 1); alloc(fz, ZF, 0, 1);
-        loop(valid(XF), [&](int i, int j, int k) { fx(i, j, k) = 1.0 * S.mx(i, j, k) / 1.0; Scr.mx(i, j, k) = fx(i, j, k); });
-        loop(valid(YF), [&](int i, int j, int k) { fy(i, j, k) = 1.0 * S.my(i, j, k) / 1.0; Scr.my(i, j, k) = fy(i, j, k); });
-        loop(valid(ZF), [&](int i, int j, int k) { fz(i, j, k) = 1.0 * S.mz(i, j, k) / 1.0; Scr.mz(i, j, k) = fz(i, j, k); });
+        loop(valid(XF), [&](int i, int j, int k) { fx(i, j, k) = (terrain ? axA(i, j, k) : 1.0) * S.mx(i, j, k) / 1.0; Scr.mx(i, j, k) = fx(i, j, k); });
+        loop(valid(YF), [&](int i, int j, int k) { fy(i, j, k) = (terrain ? ayA(i, j, k) : 1.0) * S.my(i, j, k) / 1.0; Scr.my(i, j, k) = fy(i, j, k); });
+        loop(valid(ZF), [&](int i, int j, int k) { fz(i, j, k) = 1.0 * Om(i, j, k) / 1.0; Scr.mz(i, j, k) = fz(i, j, k); });
         loop(valid(CC), [&](int i, int j, int k) {
-            R.cons(i, j, k, 0) = -1.0 / 1.0 * ((fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2]);
+            R.cons(i, j, k, 0) = -1.0 / (terrain ? detJ(i, j, k) : 1.0) * ((fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2]);
         });
         // rho*theta is advected with the dycore scheme (ERF_slow_rhs_pre.cpp:139-142, 469-477)
         advect_scalars(1, 1, Scr.mx, Scr.my, Scr.mz, prim, R.cons, c.dycore_horiz_adv, c.dycore_vert_adv,
                        c.dycore_horiz_upw_frac, c.dycore_vert_upw_frac);
-        if (use_diff) diffusion_state(1, 1, cd, prim, R.cons, mut);
+        if (use_diff) {
+            if (terrain) diffusion_state_T(1, 1, cd, prim, R.cons);
+            else diffusion_state(1, 1, cd, prim, R.cons, mut);
+        }
         // cc_src is zero for the supported configurations
+        if (terrain) {
+            advect_mom_T(R, S, V, Om);
+            if (use_diff) diffusion_mom_T(R, t11, t22, t33, t12, t13, t21, t23, t31, t32);
+            pressure_and_sources(R, pp);
+            return;
+        }
 
         // AdvectionSrcForMom (Advection/ERF_AdvectionSrcForMom.cpp:41-204,
         // ERF_AdvectionSrcForMom_N.H:17-407)
@@ -932,9 +966,23 @@ struct Oracle {
                 R.mz(i, j, k) -= ((t13(i + 1, j, k) - t13(i, j, k)) * dxInv[0] * 1.0 + (t23(i, j + 1, k) - t23(i, j, k)) * dxInv[1] * 1.0 + (t33(i, j, k) - t33(i, j, k - 1)) * dxInv[2]);
             });
         }
-        // pressure gradient and momentum sources (ERF_slow_rhs_pre.cpp:594-744)
+        pressure_and_sources(R, pp);
+    }
+
+    // pressure gradient (terrain-corrected with terrain) and momentum sources
+    // (ERF_slow_rhs_pre.cpp:594-744)
+    void pressure_and_sources(State& R, const Fab& pp) const {
+        Bx tbx = valid(XF), tby = valid(YF), tbz = valid(ZF);
+        tbz.lo[2] = 1; tbz.hi[2] = nz - 1;
         loop(tbx, [&](int i, int j, int k) {
             double gpx = dxInv[0] * (pp(i, j, k) - pp(i - 1, j, k));
+            if (terrain) {
+                double mxi = hxi_I(i, j, k), mz = hzeta_I(i, j, k), gz;
+                if (k == 0) gz = 0.5 * dxInv[2] * (pp(i - 1, j, k + 1) + pp(i, j, k + 1) - pp(i - 1, j, k) - pp(i, j, k));
+                else if (k == nz - 1) gz = 0.5 * dxInv[2] * (pp(i - 1, j, k) + pp(i, j, k) - pp(i - 1, j, k - 1) - pp(i, j, k - 1));
+                else gz = 0.25 * dxInv[2] * (pp(i - 1, j, k + 1) + pp(i, j, k + 1) - pp(i - 1, j, k - 1) - pp(i, j, k - 1));
+                gpx -= (mxi / mz) * gz;
+            }
             gpx *= 1.0;
             double q = 0.0;
             if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i - 1, j, k, 4) + prim(i, j, k, 5) + prim(i - 1, j, k, 5));
@@ -942,13 +990,21 @@ struct Oracle {
         });
         loop(tby, [&](int i, int j, int k) {
             double gpy = dxInv[1] * (pp(i, j, k) - pp(i, j - 1, k));
+            if (terrain) {
+                double meta = heta_J(i, j, k), mz = hzeta_J(i, j, k), gz;
+                if (k == 0) gz = 0.5 * dxInv[2] * (pp(i, j, k + 1) + pp(i, j - 1, k + 1) - pp(i, j, k) - pp(i, j - 1, k));
+                else if (k == nz - 1) gz = 0.5 * dxInv[2] * (pp(i, j, k) + pp(i, j - 1, k) - pp(i, j, k - 1) - pp(i, j - 1, k - 1));
+                else gz = 0.25 * dxInv[2] * (pp(i, j, k + 1) + pp(i, j - 1, k + 1) - pp(i, j, k - 1) - pp(i, j - 1, k - 1));
+                gpy -= (meta / mz) * gz;
+            }
             gpy *= 1.0;
             double q = 0.0;
             if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i, j - 1, k, 4) + prim(i, j, k, 5) + prim(i, j - 1, k, 5));
             R.my(i, j, k) += (-gpy - 0.0) / (1.0 + q) + ysrc(i, j, k);
         });
         loop(tbz, [&](int i, int j, int k) {
-            double gpz = dxInv[2] * (pp(i, j, k) - pp(i, j, k - 1)) / 1.0;
+            double mz = terrain ? hzeta_K(i, j, k) : 1.0;
+            double gpz = dxInv[2] * (pp(i, j, k) - pp(i, j, k - 1)) / mz;
             double q = 0.0;
             if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i, j, k - 1, 4) + prim(i, j, k, 5) + prim(i, j, k - 1, 5));
             R.mz(i, j, k) += (zsrc(i, j, k) - gpz - 0.0) / (1.0 + q);
@@ -964,11 +1020,19 @@ struct Oracle {
         Fab& fc = fast_coeffs;
         Bx b = valid(CC); b.lo[2] = 1; b.hi[2] = nz - 1;
         loop(b, [&](int i, int j, int k) {
-            double rhobar_lo = r0[k], rhobar_hi = r0[k + 1], pibar_lo = pi0[k], pibar_hi = pi0[k + 1];
+            double rhobar_lo = R0(i, j, k - 1), rhobar_hi = R0(i, j, k), pibar_lo = PI0(i, j, k - 1), pibar_hi = PI0(i, j, k);
             double pi_c = 0.5 * (pi_stage(i, j, k - 1) + pi_stage(i, j, k));
-            double cP = -Gamma_ * R_d * dzi + halfg * R_d * rhobar_hi / (c_v * pibar_hi * Sst.cons(i, j, k, 1));
+            double cP, cQ, dJk = 1.0;
+            if (terrain) {   // ERF_make_fast_coeffs.cpp:110-140
+                dJk = 0.5 * (detJ(i, j, k) + detJ(i, j, k - 1));
+                double inv_dJk = 1. / dJk;
+                cP = -Gamma_ * R_d * dzi * inv_dJk + halfg * R_d * rhobar_hi / (c_v * pibar_hi * Sst.cons(i, j, k, 1));
+                cQ = Gamma_ * R_d * dzi * inv_dJk + halfg * R_d * rhobar_lo / (c_v * pibar_lo * Sst.cons(i, j, k - 1, 1));
+            } else {
+                cP = -Gamma_ * R_d * dzi + halfg * R_d * rhobar_hi / (c_v * pibar_hi * Sst.cons(i, j, k, 1));
+                cQ = Gamma_ * R_d * dzi + halfg * R_d * rhobar_lo / (c_v * pibar_lo * Sst.cons(i, j, k - 1, 1));
+            }
             cP *= pi_c;
-            double cQ = Gamma_ * R_d * dzi + halfg * R_d * rhobar_lo / (c_v * pibar_lo * Sst.cons(i, j, k - 1, 1));
             cQ *= pi_c;
             fc(i, j, k, 3) = cP; fc(i, j, k, 4) = cQ;
             if (use_moisture) {
@@ -981,7 +1045,7 @@ struct Oracle {
             double D = dtau * dtau * beta_2 * beta_2 * dzi;
             fc(i, j, k, 0) = D * (halfg - cQ * tlo);
             fc(i, j, k, 2) = D * (-halfg + cP * thi);
-            fc(i, j, k, 1) = 1.0 + D * (cQ - cP) * tmid;
+            fc(i, j, k, 1) = (terrain ? dJk : 1.0) + D * (cQ - cP) * tmid;
         });
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i) {
@@ -1125,7 +1189,10 @@ struct Oracle {
         // valid slow variables: RhoScalar always; moisture if present
         auto do_var = [&](int start, int num_adv, int htype, int vtype, double hf, double vf) {
             advect_scalars(start, num_adv, Scr.mx, Scr.my, Scr.mz, prim, R.cons, htype, vtype, hf, vf);
-            if (use_diff) diffusion_state(start, num_adv, Snew.cons, prim, R.cons, mut);
+            if (use_diff) {
+                if (terrain) diffusion_state_T(start, num_adv, Snew.cons, prim, R.cons);
+                else diffusion_state(start, num_adv, Snew.cons, prim, R.cons, mut);
+            }
         };
         const bool dd = c.les_type == ERF_LES_DEARDORFF;
         if (dd)   // RhoKE is a slow variable with Deardorff (ERF_slow_rhs_post.cpp:169-172, 366-399)
@@ -1254,6 +1321,893 @@ struct Oracle {
     Fab cons_state;
     Vel vel_state;
 
+    // ==================================================================
+    // Static terrain-following grid.  Metric terms of
+    // Utils/ERF_TerrainMetrics.H:33-395 and make_J / make_areas / make_zcc
+    // (Utils/ERF_TerrainMetrics.cpp:583-715); the _T variants of the slow
+    // and fast right-hand sides follow below, each citing its source.
+    // z_phys_nd is nodal with 3 lateral ghost nodes and one vertical ghost
+    // level on each side; az is 1 everywhere and map factors are 1.
+    // ==================================================================
+    bool terrain = false;
+    Fab znd, detJ, axA, ayA, zcc;
+    Fab r0f, p0f, pi0f, th0f;            // base state over the terrain (cell centred)
+    double R0(int i, int j, int k) const { return terrain ? r0f(i, j, k) : r0[k + 1]; }
+    double P0(int i, int j, int k) const { return terrain ? p0f(i, j, k) : p0[k + 1]; }
+    double PI0(int i, int j, int k) const { return terrain ? pi0f(i, j, k) : pi0[k + 1]; }
+
+    double Z(int i, int j, int k) const { return znd(i, j, k); }
+    double hzeta_cc(int i, int j, int k) const {
+        return 0.25 * dxInv[2] * (Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1) + Z(i, j, k + 1) + Z(i, j + 1, k + 1)
+                                  - Z(i + 1, j, k) - Z(i + 1, j + 1, k) - Z(i, j, k) - Z(i, j + 1, k));
+    }
+    double hxi_cc(int i, int j, int k) const {
+        return 0.25 * dxInv[0] * (Z(i + 1, j, k) + Z(i + 1, j + 1, k) + Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1)
+                                  - Z(i, j, k) - Z(i, j + 1, k) - Z(i, j, k + 1) - Z(i, j + 1, k + 1));
+    }
+    double heta_cc(int i, int j, int k) const {
+        return 0.25 * dxInv[1] * (Z(i, j + 1, k) + Z(i + 1, j + 1, k) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1)
+                                  - Z(i, j, k) - Z(i + 1, j, k) - Z(i, j, k + 1) - Z(i + 1, j, k + 1));
+    }
+    double hzeta_I(int i, int j, int k) const {
+        return 0.5 * dxInv[2] * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
+    }
+    double hxi_I(int i, int j, int k) const {
+        return 0.125 * dxInv[0] * (Z(i + 1, j, k) + Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k) + Z(i + 1, j + 1, k + 1)
+                                   - Z(i - 1, j, k) - Z(i - 1, j, k + 1) - Z(i - 1, j + 1, k) - Z(i - 1, j + 1, k + 1));
+    }
+    double heta_I(int i, int j, int k) const {
+        return 0.5 * dxInv[1] * (Z(i, j + 1, k) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j, k + 1));
+    }
+    double hzeta_J(int i, int j, int k) const {
+        return 0.5 * dxInv[2] * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i + 1, j, k));
+    }
+    double hxi_J(int i, int j, int k) const {
+        return 0.5 * dxInv[0] * (Z(i + 1, j, k) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i, j, k + 1));
+    }
+    double heta_J(int i, int j, int k) const {
+        return 0.125 * dxInv[1] * (Z(i, j + 1, k) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k) + Z(i + 1, j + 1, k + 1)
+                                   - Z(i, j - 1, k) - Z(i, j - 1, k + 1) - Z(i + 1, j - 1, k) - Z(i + 1, j - 1, k + 1));
+    }
+    double hzeta_K(int i, int j, int k) const {
+        return 0.125 * dxInv[2] * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1)
+                                   - Z(i, j, k - 1) - Z(i + 1, j, k - 1) - Z(i, j + 1, k - 1) - Z(i + 1, j + 1, k - 1));
+    }
+    double hxi_K(int i, int j, int k) const {
+        return 0.5 * dxInv[0] * (Z(i + 1, j, k) + Z(i + 1, j + 1, k) - Z(i, j, k) - Z(i, j + 1, k));
+    }
+    double heta_K(int i, int j, int k) const {
+        return 0.5 * dxInv[1] * (Z(i, j + 1, k) + Z(i + 1, j + 1, k) - Z(i, j, k) - Z(i + 1, j, k));
+    }
+    // xy-edge (EdgeCenterK), xz-edge (EdgeCenterJ), yz-edge (EdgeCenterI)
+    double hzeta_EK(int i, int j, int k) const { return dxInv[2] * (Z(i, j, k + 1) - Z(i, j, k)); }
+    double hxi_EK(int i, int j, int k) const {
+        return 0.25 * dxInv[0] * (Z(i + 1, j, k) + Z(i + 1, j, k + 1) - Z(i - 1, j, k) - Z(i - 1, j, k + 1));
+    }
+    double heta_EK(int i, int j, int k) const {
+        return 0.25 * dxInv[1] * (Z(i, j + 1, k) + Z(i, j + 1, k + 1) - Z(i, j - 1, k) - Z(i, j - 1, k + 1));
+    }
+    double hzeta_EJ(int i, int j, int k) const {
+        return 0.25 * dxInv[2] * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k - 1) - Z(i, j + 1, k - 1));
+    }
+    double hxi_EJ(int i, int j, int k) const {
+        return 0.25 * dxInv[0] * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i - 1, j + 1, k) - Z(i - 1, j, k));
+    }
+    double heta_EJ(int i, int j, int k) const { return dxInv[1] * (Z(i, j + 1, k) - Z(i, j, k)); }
+    double hzeta_EI(int i, int j, int k) const {
+        return 0.25 * dxInv[2] * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k - 1) - Z(i + 1, j, k - 1));
+    }
+    double hxi_EI(int i, int j, int k) const { return dxInv[0] * (Z(i + 1, j, k) - Z(i, j, k)); }
+    double heta_EI(int i, int j, int k) const {
+        return 0.25 * dxInv[1] * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j - 1, k) - Z(i, j - 1, k));
+    }
+    // OmegaFromW / WFromOmega (ERF_TerrainMetrics.H:455-520): metric slopes
+    // at the z-face and the face-averaged horizontal velocities (extrapolated
+    // to the bottom face).
+    void zface_uv(int i, int j, int k, const Fab& ua, const Fab& va, double& u, double& v) const {
+        u = (k == 0) ? 1.5 * (0.5 * (ua(i, j, k) + ua(i + 1, j, k))) - 0.5 * (0.5 * (ua(i, j, k + 1) + ua(i + 1, j, k + 1)))
+                     : 0.25 * (ua(i, j, k - 1) + ua(i + 1, j, k - 1) + ua(i, j, k) + ua(i + 1, j, k));
+        v = (k == 0) ? 1.5 * (0.5 * (va(i, j, k) + va(i, j + 1, k))) - 0.5 * (0.5 * (va(i, j, k + 1) + va(i, j + 1, k + 1)))
+                     : 0.25 * (va(i, j, k - 1) + va(i, j + 1, k - 1) + va(i, j, k) + va(i, j + 1, k));
+    }
+    double zlo_xi(int i, int j, int k) const {
+        return 0.5 * dxInv[0] * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k));
+    }
+    double zlo_eta(int i, int j, int k) const {
+        return 0.5 * dxInv[1] * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k));
+    }
+    double omega_from_w(int i, int j, int k, double w, const Fab& ua, const Fab& va) const {
+        double mx = zlo_xi(i, j, k), my = zlo_eta(i, j, k), u, v;
+        zface_uv(i, j, k, ua, va, u, v);
+        return w - mx * u - my * v;
+    }
+    double w_from_omega(int i, int j, int k, double om, const Fab& ua, const Fab& va) const {
+        double mx = zlo_xi(i, j, k), my = zlo_eta(i, j, k), u, v;
+        zface_uv(i, j, k, ua, va, u, v);
+        return om + mx * u + my * v;
+    }
+
+    // Install z_phys_nd (valid nodes, (nz+1)(ny+1)(nx+1), i fastest) and
+    // build its ghost nodes the way init_terrain_grid leaves them
+    // (Utils/ERF_TerrainMetrics.cpp:88-209, 320-333): lateral ghosts are the
+    // periodic images (FillBoundary of nodal data keeps node nx), k = -1 and
+    // k = nz+1 are linear extrapolations.  Then detJ, ax, ay, z_cc.
+    void set_terrain(const double* z) {
+        terrain = true;
+        int l[3] = {-3, -3, -1}, h[3] = {nx + 3, ny + 3, nz + 1};
+        znd.define(l, h, 1);
+        auto wrapn = [](int i, int n) { while (i < 0) i += n; while (i > n) i -= n; return i; };
+        for (int k = 0; k <= nz; ++k)
+            for (int j = l[1]; j <= h[1]; ++j)
+                for (int i = l[0]; i <= h[0]; ++i) {
+                    int is = (i >= 0 && i <= nx) ? i : wrapn(i, nx);
+                    int js = (j >= 0 && j <= ny) ? j : wrapn(j, ny);
+                    if (is == nx && !(i >= 0 && i <= nx)) is = 0;
+                    if (js == ny && !(j >= 0 && j <= ny)) js = 0;
+                    znd(i, j, k) = z[((size_t)k * (ny + 1) + js) * (nx + 1) + is];
+                }
+        for (int j = l[1]; j <= h[1]; ++j)
+            for (int i = l[0]; i <= h[0]; ++i) {
+                znd(i, j, -1) = 2.0 * znd(i, j, 0) - znd(i, j, 1);
+                znd(i, j, nz + 1) = 2.0 * znd(i, j, nz) - znd(i, j, nz - 1);
+            }
+        int lc[3] = {-2, -2, -1}, hc[3] = {nx + 1, ny + 1, nz};
+        detJ.define(lc, hc, 1, 1.0); zcc.define(lc, hc, 1);
+        int lx[3] = {-2, -2, -1}, hx[3] = {nx + 2, ny + 1, nz};
+        int ly[3] = {-2, -2, -1}, hy[3] = {nx + 1, ny + 2, nz};
+        axA.define(lx, hx, 1, 1.0); ayA.define(ly, hy, 1, 1.0);
+        const double dzi = dxInv[2];
+        for (int k = 0; k <= nz; ++k)
+            for (int j = lc[1]; j <= hc[1]; ++j)
+                for (int i = lc[0]; i <= hc[0]; ++i) {
+                    detJ(i, j, k) = .25 * dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1)
+                                                 - Z(i, j, k) - Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
+                    zcc(i, j, k) = .125 * (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k)
+                                           + Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1));
+                }
+        for (int j = lc[1]; j <= hc[1]; ++j)
+            for (int i = lc[0]; i <= hc[0]; ++i) { detJ(i, j, -1) = detJ(i, j, 0); zcc(i, j, -1) = zcc(i, j, 0); }
+        for (int k = 0; k <= nz; ++k) {
+            for (int j = lx[1]; j <= hx[1]; ++j)
+                for (int i = lx[0]; i <= hx[0]; ++i)
+                    axA(i, j, k) = .5 * dzi * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
+            for (int j = ly[1]; j <= hy[1]; ++j)
+                for (int i = ly[0]; i <= hy[0]; ++i)
+                    ayA(i, j, k) = .5 * dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i + 1, j, k));
+        }
+    }
+
+    // Base state over the terrain: per column the Newton hydrostatic
+    // integration of calc_rho_p (DataStructs/ERF_InputSoundingData.H:176-256)
+    // from p_sfc at z = 0 through the column's cell centres z_cc, then
+    // erf_enforce_hse with terrain (Initialization/ERF_init1d.cpp:152-241).
+    // Outputs (nz+2) planes of ny*nx, plane k+1 for cell level k.
+    void make_base_state_terrain(const double* th3, const double* qv3, double th_s, double qv_s, double p_s,
+                                 double* rho_o, double* p_o, double* pi_o, double* th_o) const {
+        const double tol = 1.0e-12, g = c.gravity;
+        std::vector<double> z(nz + 1), th(nz + 1), qv(nz + 1), pm(nz + 1), rd(nz + 1), r(nz + 2), p(nz + 2);
+        const size_t plane = (size_t)nx * ny;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                z[0] = 0.; th[0] = th_s; qv[0] = qv_s;
+                for (int k = 0; k < nz; ++k) {
+                    size_t cix = (size_t)k * plane + (size_t)j * nx + i;
+                    z[k + 1] = zcc(i, j, k); th[k + 1] = th3[cix]; qv[k + 1] = qv3[cix];
+                }
+                pm[0] = p_s;
+                rd[0] = getRhogivenThetaPress(th[0], p_s, R_d / Cp_d, qv[0]);
+                for (int k = 1; k <= nz; ++k) {
+                    double dz = z[k] - z[k - 1];
+                    double rlo = rd[k - 1] * (1. + qv[k - 1]);
+                    double C = -pm[k - 1] + 0.5 * rlo * g * dz;
+                    pm[k] = pm[k - 1];
+                    rd[k] = getRhogivenThetaPress(th[k], pm[k], R_d / Cp_d, qv[k]);
+                    double rhi = rd[k] * (1. + qv[k]);
+                    double F = pm[k] + 0.5 * rhi * g * dz + C;
+                    if (std::abs(F) > tol) {
+                        int iter = 0;
+                        double eps = 1.0e-6, ieps = 1.0e6;
+                        do {
+                            double hi = getRhogivenThetaPress(th[k], pm[k] + eps, R_d / Cp_d, qv[k]);
+                            double lo = getRhogivenThetaPress(th[k], pm[k] - eps, R_d / Cp_d, qv[k]);
+                            double dFdp = 1.0 + 0.25 * ieps * (hi - lo) * g * dz;
+                            pm[k] -= F / dFdp;
+                            rd[k] = getRhogivenThetaPress(th[k], pm[k], R_d / Cp_d, qv[k]);
+                            double rt = rd[k] * (1. + qv[k]);
+                            F = pm[k] + 0.5 * rt * g * dz + C;
+                            ++iter;
+                        } while (std::abs(F) > tol && iter < 30);
+                    }
+                }
+                for (int k = 0; k < nz; ++k) r[k + 1] = rd[k + 1];
+                r[0] = r[1]; r[nz + 1] = r[nz];
+                double hz = zcc(i, j, 0);
+                auto put = [&](int kk, double pv) {
+                    size_t o = (size_t)kk * plane + (size_t)j * nx + i;
+                    rho_o[o] = r[kk]; p_o[o] = pv; pi_o[o] = getExnergivenP(pv, rdOcp);
+                    th_o[o] = getRhoThetagivenP(pv) / r[kk];
+                };
+                p[1] = p_0 - hz * r[1] * g;
+                p[0] = p_0 + hz * r[1] * g;
+                put(1, p[1]); put(0, p[0]);
+                for (int k = 1; k <= nz; ++k) {
+                    int kk = k + 1;
+                    double dz_loc = zcc(i, j, k) - zcc(i, j, k - 1);
+                    double di = 0.5 * (r[kk] + r[kk - 1]);
+                    p[kk] = p[kk - 1] - dz_loc * di * g;
+                    put(kk, p[kk]);
+                }
+            }
+    }
+    // Base state arrays in the (nz+2)-plane layout -> cell-centred Fabs
+    // with periodic lateral ghosts.
+    void set_base_terrain(const double* rho_b, const double* p_b, const double* pi_b, const double* th_b) {
+        int l[3] = {-2, -2, -1}, h[3] = {nx + 1, ny + 1, nz};
+        Fab* f[4] = {&r0f, &p0f, &pi0f, &th0f};
+        const double* src[4] = {rho_b, p_b, pi_b, th_b};
+        for (int a = 0; a < 4; ++a) {
+            f[a]->define(l, h, 1);
+            for (int k = -1; k <= nz; ++k)
+                for (int j = l[1]; j <= h[1]; ++j)
+                    for (int i = l[0]; i <= h[0]; ++i) {
+                        int is = ((i % nx) + nx) % nx, js = ((j % ny) + ny) % ny;
+                        (*f[a])(i, j, k) = src[a][(size_t)(k + 1) * nx * ny + (size_t)js * nx + is];
+                    }
+        }
+    }
+
+    // ComputeStrain_T (Diffusion/ERF_ComputeStrain_T.cpp:28-507): z-wall
+    // planes first (one-sided derivatives at no-slip walls, GradWz
+    // extrapolation otherwise), then the interior.  Periodic laterally, so
+    // the x/y Dirichlet planes never apply.
+    void compute_strain_T(Bx bxcc, Bx txy, Bx txz, Bx tyz, const Fab& u, const Fab& v, const Fab& w, Fab& s11,
+                          Fab& s22, Fab& s33, Fab& s12, Fab& s13, Fab& s21, Fab& s23, Fab& s31, Fab& s32) const {
+        const double* di = dxInv;
+        const bool zl = zlo_noslip, zh = zhi_noslip;
+        if (zl) {
+            Bx p = txz; p.hi[2] = p.lo[2]; txz.lo[2] += 1;
+            loop(p, [&](int i, int j, int k) {
+                double GradWz = 0.5 * di[2] * (w(i, j, k + 1) + w(i - 1, j, k + 1) - w(i, j, k) - w(i - 1, j, k));
+                double mxi = hxi_EJ(i, j, k), mz = hzeta_EJ(i, j, k);
+                s13(i, j, k) = 0.5 * ((-(8. / 3.) * u(i, j, k - 1) + 3. * u(i, j, k) - (1. / 3.) * u(i, j, k + 1)) * di[2] / mz
+                                      + ((w(i, j, k) - w(i - 1, j, k)) * di[0] - (mxi / mz) * GradWz) * 1.0);
+                s31(i, j, k) = s13(i, j, k);
+            });
+        }
+        if (zh) {
+            Bx p = txz; p.lo[2] = p.hi[2]; txz.hi[2] -= 1;
+            loop(p, [&](int i, int j, int k) {
+                double mz = hzeta_EJ(i, j, k);
+                s13(i, j, k) = 0.5 * (-(-(8. / 3.) * u(i, j, k) + 3. * u(i, j, k - 1) - (1. / 3.) * u(i, j, k - 2)) * di[2] / mz
+                                      + (w(i, j, k) - w(i - 1, j, k)) * di[0] * 1.0);
+                s31(i, j, k) = s13(i, j, k);
+            });
+        }
+        if (zl) {
+            Bx p = tyz; p.hi[2] = p.lo[2]; tyz.lo[2] += 1;
+            loop(p, [&](int i, int j, int k) {
+                double GradWz = 0.5 * di[2] * (w(i, j, k + 1) + w(i, j - 1, k + 1) - w(i, j, k) - w(i, j - 1, k));
+                double meta = heta_EI(i, j, k), mz = hzeta_EI(i, j, k);
+                s23(i, j, k) = 0.5 * ((-(8. / 3.) * v(i, j, k - 1) + 3. * v(i, j, k) - (1. / 3.) * v(i, j, k + 1)) * di[2] / mz
+                                      + ((w(i, j, k) - w(i, j - 1, k)) * di[1] - (meta / mz) * GradWz) * 1.0);
+                s32(i, j, k) = s23(i, j, k);
+            });
+        }
+        if (zh) {
+            Bx p = tyz; p.lo[2] = p.hi[2]; tyz.hi[2] -= 1;
+            loop(p, [&](int i, int j, int k) {
+                double mz = hzeta_EI(i, j, k);
+                s23(i, j, k) = 0.5 * (-(-(8. / 3.) * v(i, j, k) + 3. * v(i, j, k - 1) - (1. / 3.) * v(i, j, k - 2)) * di[2] / mz
+                                      + (w(i, j, k) - w(i, j - 1, k)) * di[1] * 1.0);
+                s32(i, j, k) = s23(i, j, k);
+            });
+        }
+        if (zl) {
+            Bx pc = bxcc; pc.hi[2] = pc.lo[2]; bxcc.lo[2] += 1;
+            loop(pc, [&](int i, int j, int k) {
+                double GradUz = 0.5 * di[2] * ((-(8. / 3.) * u(i, j, k - 1) + 3. * u(i, j, k) - (1. / 3.) * u(i, j, k + 1))
+                                               + (-(8. / 3.) * u(i - 1, j, k - 1) + 3. * u(i - 1, j, k) - (1. / 3.) * u(i - 1, j, k + 1)));
+                double GradVz = 0.5 * di[2] * ((-(8. / 3.) * v(i, j, k - 1) + 3. * v(i, j, k) - (1. / 3.) * v(i, j, k + 1))
+                                               + (-(8. / 3.) * v(i, j - 1, k - 1) + 3. * v(i, j - 1, k) - (1. / 3.) * v(i, j - 1, k + 1)));
+                double mxi = hxi_cc(i, j, k), meta = heta_cc(i, j, k), mz = detJ(i, j, k);
+                s11(i, j, k) = ((u(i + 1, j, k) / 1.0 - u(i, j, k) / 1.0) * di[0] - (mxi / mz) * GradUz) * 1.0 * 1.0;
+                s22(i, j, k) = ((v(i, j + 1, k) / 1.0 - v(i, j, k) / 1.0) * di[1] - (meta / mz) * GradVz) * 1.0 * 1.0;
+                s33(i, j, k) = (w(i, j, k + 1) - w(i, j, k)) * di[2] / mz;
+            });
+            Bx pxy = txy; pxy.hi[2] = pxy.lo[2]; txy.lo[2] += 1;
+            loop(pxy, [&](int i, int j, int k) {
+                double GradUz = 0.5 * di[2] * ((-(8. / 3.) * u(i, j, k - 1) + 3. * u(i, j, k) - (1. / 3.) * u(i, j, k + 1))
+                                               + (-(8. / 3.) * u(i, j - 1, k - 1) + 3. * u(i, j - 1, k) - (1. / 3.) * u(i, j - 1, k + 1)));
+                double GradVz = 0.5 * di[2] * ((-(8. / 3.) * v(i, j, k - 1) + 3. * v(i, j, k) - (1. / 3.) * v(i, j, k + 1))
+                                               + (-(8. / 3.) * v(i - 1, j, k - 1) + 3. * v(i - 1, j, k) - (1. / 3.) * v(i - 1, j, k + 1)));
+                double mxi = hxi_EK(i, j, k), meta = heta_EK(i, j, k), mz = hzeta_EK(i, j, k);
+                s12(i, j, k) = 0.5 * ((u(i, j, k) / 1.0 - u(i, j - 1, k) / 1.0) * di[1] + (v(i, j, k) / 1.0 - v(i - 1, j, k) / 1.0) * di[0]
+                                      - (meta / mz) * GradUz - (mxi / mz) * GradVz) * 1.0 * 1.0;
+                s21(i, j, k) = s12(i, j, k);
+            });
+        }
+        if (!zl && txz.lo[2] == 0) {
+            Bx p = txz; p.hi[2] = p.lo[2]; txz.lo[2] += 1;
+            loop(p, [&](int i, int j, int k) {
+                double GradWz = 0.5 * di[2] * (w(i, j, k + 1) + w(i - 1, j, k + 1) - w(i, j, k) - w(i - 1, j, k));
+                double mxi = hxi_EJ(i, j, k), mz = hzeta_EJ(i, j, k);
+                s13(i, j, k) = 0.5 * ((u(i, j, k) - u(i, j, k - 1)) * di[2] / mz + ((w(i, j, k) - w(i - 1, j, k)) * di[0] - (mxi / mz) * GradWz) * 1.0);
+                s31(i, j, k) = s13(i, j, k);
+            });
+        }
+        if (!zl && tyz.lo[2] == 0) {
+            Bx p = tyz; p.hi[2] = p.lo[2]; tyz.lo[2] += 1;
+            loop(p, [&](int i, int j, int k) {
+                double GradWz = 0.5 * di[2] * (w(i, j, k + 1) + w(i, j - 1, k + 1) - w(i, j, k) - w(i, j - 1, k));
+                double meta = heta_EI(i, j, k), mz = hzeta_EI(i, j, k);
+                s23(i, j, k) = 0.5 * ((v(i, j, k) - v(i, j, k - 1)) * di[2] / mz + ((w(i, j, k) - w(i, j - 1, k)) * di[1] - (meta / mz) * GradWz) * 1.0);
+                s32(i, j, k) = s23(i, j, k);
+            });
+        }
+        if (!zh && txz.hi[2] == nz) {
+            Bx p = txz; p.lo[2] = p.hi[2]; txz.hi[2] -= 1;
+            loop(p, [&](int i, int j, int k) {
+                double mz = hzeta_EJ(i, j, k);
+                s13(i, j, k) = 0.5 * ((u(i, j, k) - u(i, j, k - 1)) * di[2] / mz + (w(i, j, k) - w(i - 1, j, k)) * di[0] * 1.0);
+                s31(i, j, k) = s13(i, j, k);
+            });
+        }
+        if (!zh && tyz.hi[2] == nz) {
+            Bx p = tyz; p.lo[2] = p.hi[2]; tyz.hi[2] -= 1;
+            loop(p, [&](int i, int j, int k) {
+                double mz = hzeta_EI(i, j, k);
+                s23(i, j, k) = 0.5 * ((v(i, j, k) - v(i, j, k - 1)) * di[2] / mz + (w(i, j, k) - w(i, j - 1, k)) * di[1] * 1.0);
+                s32(i, j, k) = s23(i, j, k);
+            });
+        }
+        loop(bxcc, [&](int i, int j, int k) {
+            double GradUz = 0.25 * di[2] * (u(i, j, k + 1) / 1.0 + u(i - 1, j, k + 1) / 1.0 - u(i, j, k - 1) / 1.0 - u(i - 1, j, k - 1) / 1.0);
+            double GradVz = 0.25 * di[2] * (v(i, j, k + 1) / 1.0 + v(i, j - 1, k + 1) / 1.0 - v(i, j, k - 1) / 1.0 - v(i, j - 1, k - 1) / 1.0);
+            double mxi = hxi_cc(i, j, k), meta = heta_cc(i, j, k), mz = detJ(i, j, k);
+            s11(i, j, k) = ((u(i + 1, j, k) / 1.0 - u(i, j, k) / 1.0) * di[0] - (mxi / mz) * GradUz) * 1.0 * 1.0;
+            s22(i, j, k) = ((v(i, j + 1, k) / 1.0 - v(i, j, k) / 1.0) * di[1] - (meta / mz) * GradVz) * 1.0 * 1.0;
+            s33(i, j, k) = (w(i, j, k + 1) - w(i, j, k)) * di[2] / mz;
+        });
+        loop(txy, [&](int i, int j, int k) {
+            double GradUz = 0.25 * di[2] * (u(i, j, k + 1) / 1.0 + u(i, j - 1, k + 1) / 1.0 - u(i, j, k - 1) / 1.0 - u(i, j - 1, k - 1) / 1.0);
+            double GradVz = 0.25 * di[2] * (v(i, j, k + 1) / 1.0 + v(i - 1, j, k + 1) / 1.0 - v(i, j, k - 1) / 1.0 - v(i - 1, j, k - 1) / 1.0);
+            double mxi = hxi_EK(i, j, k), meta = heta_EK(i, j, k), mz = hzeta_EK(i, j, k);
+            s12(i, j, k) = 0.5 * ((u(i, j, k) / 1.0 - u(i, j - 1, k) / 1.0) * di[1] + (v(i, j, k) / 1.0 - v(i - 1, j, k) / 1.0) * di[0]
+                                  - (meta / mz) * GradUz - (mxi / mz) * GradVz) * 1.0 * 1.0;
+            s21(i, j, k) = s12(i, j, k);
+        });
+        loop(txz, [&](int i, int j, int k) {
+            double GradWz = 0.25 * di[2] * (w(i, j, k + 1) + w(i - 1, j, k + 1) - w(i, j, k - 1) - w(i - 1, j, k - 1));
+            double mxi = hxi_EJ(i, j, k), mz = hzeta_EJ(i, j, k);
+            s13(i, j, k) = 0.5 * ((u(i, j, k) - u(i, j, k - 1)) * di[2] / mz + ((w(i, j, k) - w(i - 1, j, k)) * di[0] - (mxi / mz) * GradWz) * 1.0);
+            s31(i, j, k) = s13(i, j, k);
+        });
+        loop(tyz, [&](int i, int j, int k) {
+            double GradWz = 0.25 * di[2] * (w(i, j, k + 1) + w(i, j - 1, k + 1) - w(i, j, k - 1) - w(i, j - 1, k - 1));
+            double meta = heta_EI(i, j, k), mz = hzeta_EI(i, j, k);
+            s23(i, j, k) = 0.5 * ((v(i, j, k) - v(i, j, k - 1)) * di[2] / mz + ((w(i, j, k) - w(i, j - 1, k)) * di[1] - (meta / mz) * GradWz) * 1.0);
+            s32(i, j, k) = s23(i, j, k);
+        });
+    }
+
+    // The terrain strain boxes of advance_dycore / make_tau_terms: the valid
+    // region grown by one laterally (cells and edges).
+    void strain_boxes(Bx& bxcc, Bx& txy, Bx& txz, Bx& tyz) const {
+        bxcc = grow(valid(CC), 1, 1, 0);
+        txy = grow(Bx{{0, 0, 0}, {nx, ny, nz - 1}}, 1, 1, 0);
+        txz = grow(Bx{{0, 0, 0}, {nx, ny - 1, nz}}, 1, 1, 0);
+        tyz = grow(Bx{{0, 0, 0}, {nx - 1, ny, nz}}, 1, 1, 0);
+    }
+    void alloc_tau_T(Fab& t11, Fab& t22, Fab& t33, Fab& t12, Fab& t13, Fab& t21, Fab& t23, Fab& t31, Fab& t32) const {
+        alloc_cc1(t11); alloc_cc1(t22); alloc_cc1(t33);
+        alloc_edges(t12, t13, t23); alloc_edges(t21, t31, t32);
+    }
+
+    // make_tau_terms with terrain (TimeIntegration/ERF_make_tau_terms.cpp:
+    // 177-317): expansion rate from the contravariant velocity, strain,
+    // SmnSmn at stage 0 (Deardorff), then ComputeStressVarVisc_T
+    // (Diffusion/ERF_ComputeStress_T.cpp:302-577).
+    void make_tau_T(const Vel& V, const State& S, Fab& t11, Fab& t22, Fab& t33, Fab& t12, Fab& t13, Fab& t21,
+                    Fab& t23, Fab& t31, Fab& t32) const {
+        const Fab &u = V.u, &v = V.v, &w = V.w;
+        Bx bxcc, txy, txz, tyz;
+        strain_boxes(bxcc, txy, txz, tyz);
+        Fab om; alloc(om, ZF, 2, 1);
+        Bx ob = grow(valid(ZF), 1, 1, 0);
+        loop(ob, [&](int i, int j, int k) { om(i, j, k) = (k == 0) ? 0. : omega_from_w(i, j, k, w(i, j, k), u, v); });
+        Fab er; alloc_cc1(er);
+        loop(bxcc, [&](int i, int j, int k) {
+            double mhi = hzeta_I(i + 1, j, k), mlo = hzeta_I(i, j, k);
+            double nhi = hzeta_J(i, j + 1, k), nlo = hzeta_J(i, j, k);
+            double rate = (u(i + 1, j, k) / 1.0 * mhi - u(i, j, k) / 1.0 * mlo) * dxInv[0] * 1.0
+                          + (v(i, j + 1, k) / 1.0 * nhi - v(i, j, k) / 1.0 * nlo) * dxInv[1] * 1.0
+                          + (om(i, j, k + 1) - om(i, j, k)) * dxInv[2];
+            er(i, j, k) = rate / detJ(i, j, k);
+        });
+        compute_strain_T(bxcc, txy, txz, tyz, u, v, w, t11, t22, t33, t12, t13, t21, t23, t31, t32);
+        if (c.les_type == ERF_LES_DEARDORFF && tau_nrk == 0) {
+            Fab& sm = smn;
+            loop(valid(CC), [&](int i, int j, int k) { sm(i, j, k) = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23); });
+        }
+        // stress on the valid edges, tau_ii on the grown cells
+        txy = Bx{{0, 0, 0}, {nx, ny, nz - 1}};
+        txz = Bx{{0, 0, 0}, {nx, ny - 1, nz}};
+        tyz = Bx{{0, 0, 0}, {nx - 1, ny, nz}};
+        const double mu_eff = use_consA ? 2.0 * c.dynamic_viscosity / c.rho0_trans : 2.0 * c.dynamic_viscosity;
+        const Fab& cd = S.cons;
+        auto rA = [&](int i, int j, int k) { return use_consA ? cd(i, j, k, 0) * mu_eff : mu_eff; };
+        auto mt = [&](int i, int j, int k) { return use_turb ? mut(i, j, k) : 0.0; };
+        const double OneThird = (1. / 3.);
+        loop(bxcc, [&](int i, int j, int k) {
+            t11(i, j, k) -= OneThird * er(i, j, k);
+            t22(i, j, k) -= OneThird * er(i, j, k);
+            t33(i, j, k) -= OneThird * er(i, j, k);
+        });
+        loop(valid(CC), [&](int i, int j, int k) {
+            double mxi = hxi_cc(i, j, k), meta = heta_cc(i, j, k);
+            double t31b = 0.25 * (t31(i, j, k) + t31(i + 1, j, k) + t31(i, j, k + 1) + t31(i + 1, j, k + 1));
+            double t32b = 0.25 * (t32(i, j, k) + t32(i, j + 1, k) + t32(i, j, k + 1) + t32(i, j + 1, k + 1));
+            double mu_tot = rA(i, j, k) + 2.0 * mt(i, j, k);
+            t33(i, j, k) -= mxi * t31b + meta * t32b;
+            t33(i, j, k) *= -mu_tot;
+        });
+        auto edge13 = [&](int i, int j, int k, double t11b, double t12b) {
+            double mxi = hxi_EJ(i, j, k), meta = heta_EJ(i, j, k), mz = hzeta_EJ(i, j, k);
+            double mu_bar = 0.25 * (mt(i - 1, j, k) + mt(i, j, k) + mt(i - 1, j, k - 1) + mt(i, j, k - 1));
+            double ra_bar = 0.25 * (rA(i - 1, j, k) + rA(i, j, k) + rA(i - 1, j, k - 1) + rA(i, j, k - 1));
+            double mu_tot = ra_bar + 2.0 * mu_bar;
+            t13(i, j, k) -= mxi * t11b + meta * t12b;
+            t13(i, j, k) *= -mu_tot;
+            t31(i, j, k) *= -mu_tot * mz;
+        };
+        auto edge23 = [&](int i, int j, int k, double t21b, double t22b) {
+            double mxi = hxi_EI(i, j, k), meta = heta_EI(i, j, k), mz = hzeta_EI(i, j, k);
+            double mu_bar = 0.25 * (mt(i, j - 1, k) + mt(i, j, k) + mt(i, j - 1, k - 1) + mt(i, j, k - 1));
+            double ra_bar = 0.25 * (rA(i, j - 1, k) + rA(i, j, k) + rA(i, j - 1, k - 1) + rA(i, j, k - 1));
+            double mu_tot = ra_bar + 2.0 * mu_bar;
+            t23(i, j, k) -= mxi * t21b + meta * t22b;
+            t23(i, j, k) *= -mu_tot;
+            t32(i, j, k) *= -mu_tot * mz;
+        };
+        {   // bottom planes: linear extrapolation of the cell / xy-edge values
+            Bx p = txz; p.hi[2] = p.lo[2]; txz.lo[2] += 1;
+            loop(p, [&](int i, int j, int k) {
+                double a = 0.5 * (t11(i, j, k) + t11(i - 1, j, k)), b = 0.5 * (t11(i, j, k + 1) + t11(i - 1, j, k + 1));
+                double t11b = 1.5 * a - 0.5 * b;
+                double c1 = 0.5 * (t12(i, j, k) + t12(i, j + 1, k)), d = 0.5 * (t12(i, j, k + 1) + t12(i, j + 1, k + 1));
+                double t12b = 1.5 * c1 - 0.5 * d;
+                edge13(i, j, k, t11b, t12b);
+            });
+            Bx q = tyz; q.hi[2] = q.lo[2]; tyz.lo[2] += 1;
+            loop(q, [&](int i, int j, int k) {
+                double a = 0.5 * (t21(i, j, k) + t21(i + 1, j, k)), b = 0.5 * (t21(i, j, k + 1) + t21(i + 1, j, k + 1));
+                double t21b = 1.5 * a - 0.5 * b;
+                double c1 = 0.5 * (t22(i, j, k) + t22(i, j - 1, k)), d = 0.5 * (t22(i, j, k + 1) + t22(i, j - 1, k + 1));
+                double t22b = 1.5 * c1 - 0.5 * d;
+                edge23(i, j, k, t21b, t22b);
+            });
+        }
+        {   // top planes
+            Bx p = txz; p.lo[2] = p.hi[2]; txz.hi[2] -= 1;
+            loop(p, [&](int i, int j, int k) {
+                double lo = 0.5 * (t11(i, j, k - 2) + t11(i - 1, j, k - 2)), hi = 0.5 * (t11(i, j, k - 1) + t11(i - 1, j, k - 1));
+                double t11b = 1.5 * hi - 0.5 * lo;
+                double lo2 = 0.5 * (t12(i, j, k - 2) + t12(i, j + 1, k - 2)), hi2 = 0.5 * (t12(i, j, k - 1) + t12(i, j + 1, k - 1));
+                double t12b = 1.5 * hi2 - 0.5 * lo2;
+                edge13(i, j, k, t11b, t12b);
+            });
+            Bx q = tyz; q.lo[2] = q.hi[2]; tyz.hi[2] -= 1;
+            loop(q, [&](int i, int j, int k) {
+                double lo = 0.5 * (t21(i, j, k - 2) + t21(i + 1, j, k - 2)), hi = 0.5 * (t21(i, j, k - 1) + t21(i + 1, j, k - 1));
+                double t21b = 1.5 * hi - 0.5 * lo;
+                double lo2 = 0.5 * (t22(i, j, k - 2) + t22(i, j - 1, k - 2)), hi2 = 0.5 * (t22(i, j, k - 1) + t22(i, j - 1, k - 1));
+                double t22b = 1.5 * hi2 - 0.5 * lo2;
+                edge23(i, j, k, t21b, t22b);
+            });
+        }
+        loop(txz, [&](int i, int j, int k) {
+            double t11b = 0.25 * (t11(i, j, k) + t11(i - 1, j, k) + t11(i, j, k - 1) + t11(i - 1, j, k - 1));
+            double t12b = 0.25 * (t12(i, j, k) + t12(i, j + 1, k) + t12(i, j, k - 1) + t12(i, j + 1, k - 1));
+            edge13(i, j, k, t11b, t12b);
+        });
+        loop(tyz, [&](int i, int j, int k) {
+            double t21b = 0.25 * (t21(i, j, k) + t21(i + 1, j, k) + t21(i, j, k - 1) + t21(i + 1, j, k - 1));
+            double t22b = 0.25 * (t22(i, j, k) + t22(i, j - 1, k) + t22(i, j, k - 1) + t22(i, j - 1, k - 1));
+            edge23(i, j, k, t21b, t22b);
+        });
+        loop(bxcc, [&](int i, int j, int k) {
+            double mz = detJ(i, j, k);
+            double mu_tot = rA(i, j, k) + 2.0 * mt(i, j, k);
+            t11(i, j, k) *= -mu_tot * mz;
+            t22(i, j, k) *= -mu_tot * mz;
+        });
+        loop(txy, [&](int i, int j, int k) {
+            double mz = hzeta_EK(i, j, k);
+            double mu_bar = 0.25 * (mt(i - 1, j, k) + mt(i, j, k) + mt(i - 1, j - 1, k) + mt(i, j - 1, k));
+            double ra_bar = 0.25 * (rA(i - 1, j, k) + rA(i, j, k) + rA(i - 1, j - 1, k) + rA(i, j - 1, k));
+            double mu_tot = ra_bar + 2.0 * mu_bar;
+            t12(i, j, k) *= -mu_tot * mz;
+            t21(i, j, k) *= -mu_tot * mz;
+        });
+    }
+
+    // DiffusionSrcForMom_T (Diffusion/ERF_DiffusionSrcForMom_T.cpp:31-80)
+    void diffusion_mom_T(State& R, const Fab& t11, const Fab& t22, const Fab& t33, const Fab& t12, const Fab& t13,
+                         const Fab& t21, const Fab& t23, const Fab& t31, const Fab& t32) const {
+        Bx tbx = valid(XF), tby = valid(YF), tbz = valid(ZF);
+        tbz.lo[2] = 1; tbz.hi[2] = nz - 1;
+        const double dxi = dxInv[0], dyi = dxInv[1], dzi = dxInv[2];
+        loop(tbx, [&](int i, int j, int k) {
+            double d = ((t11(i, j, k) - t11(i - 1, j, k)) * dxi * 1.0 + (t12(i, j + 1, k) - t12(i, j, k)) * dyi * 1.0
+                        + (t13(i, j, k + 1) - t13(i, j, k)) * dzi);
+            d /= 0.5 * (detJ(i, j, k) + detJ(i - 1, j, k));
+            R.mx(i, j, k) -= d;
+        });
+        loop(tby, [&](int i, int j, int k) {
+            double d = ((t21(i + 1, j, k) - t21(i, j, k)) * dxi * 1.0 + (t22(i, j, k) - t22(i, j - 1, k)) * dyi * 1.0
+                        + (t23(i, j, k + 1) - t23(i, j, k)) * dzi);
+            d /= 0.5 * (detJ(i, j, k) + detJ(i, j - 1, k));
+            R.my(i, j, k) -= d;
+        });
+        loop(tbz, [&](int i, int j, int k) {
+            double d = ((t31(i + 1, j, k) - t31(i, j, k)) * dxi * 1.0 + (t32(i, j + 1, k) - t32(i, j, k)) * dyi * 1.0
+                        + (t33(i, j, k) - t33(i, j, k - 1)) * dzi);
+            d /= 0.5 * (detJ(i, j, k) + detJ(i, j, k - 1));
+            R.mz(i, j, k) -= d;
+        });
+    }
+
+    // DiffusionSrcForState_T (Diffusion/ERF_DiffusionSrcForState_T.cpp:
+    // 207-738) for comps [start_comp, start_comp+ncmp), no MOST, foextrap
+    // scalars at the walls: metric-corrected fluxes, the theta z-face flux
+    // kept as hfx_z before the cross-term correction, then the divergence
+    // over detJ and the Deardorff TKE sources.
+    void diffusion_state_T(int start_comp, int ncmp, const Fab& cell_data, const Fab& prm, Fab& rhs) const {
+        const bool dd = c.les_type == ERF_LES_DEARDORFF;
+        for (int n = 0; n < ncmp; ++n) {
+            int q = start_comp + n, pidx = q - 1;
+            double ae = alpha_eff(pidx), fac = eddy_factor(pidx);
+            Fab fx, fy, fz;
+            alloc(fx, XF, 0, 1); alloc(fy, YF, 0, 1); alloc(fz, ZF, 0, 1);
+            auto mu = [&](int i, int j, int k) { return mut(i, j, k) * fac; };
+            auto rAlpha = [&](double rho_face) { return use_consA ? rho_face * ae : ae; };
+            loop(valid(XF), [&](int i, int j, int k) {
+                double rA = rAlpha(0.5 * (cell_data(i, j, k, 0) + cell_data(i - 1, j, k, 0)));
+                if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i - 1, j, k));
+                double mxi = hxi_I(i, j, k), mz = axA(i, j, k);
+                double GradCz = 0.25 * dxInv[2] * (prm(i, j, k + 1, pidx) + prm(i - 1, j, k + 1, pidx) - prm(i, j, k - 1, pidx) - prm(i - 1, j, k - 1, pidx));
+                double GradCx = dxInv[0] * (prm(i, j, k, pidx) - prm(i - 1, j, k, pidx));
+                fx(i, j, k) = -rA * 1.0 * (GradCx - (mxi / mz) * GradCz);
+            });
+            loop(valid(YF), [&](int i, int j, int k) {
+                double rA = rAlpha(0.5 * (cell_data(i, j, k, 0) + cell_data(i, j - 1, k, 0)));
+                if (use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j - 1, k));
+                double meta = heta_J(i, j, k), mz = ayA(i, j, k);
+                double GradCz = 0.25 * dxInv[2] * (prm(i, j, k + 1, pidx) + prm(i, j - 1, k + 1, pidx) - prm(i, j, k - 1, pidx) - prm(i, j - 1, k - 1, pidx));
+                double GradCy = dxInv[1] * (prm(i, j, k, pidx) - prm(i, j - 1, k, pidx));
+                fy(i, j, k) = -rA * 1.0 * (GradCy - (meta / mz) * GradCz);
+            });
+            loop(valid(ZF), [&](int i, int j, int k) {
+                double rA = rAlpha(0.5 * (cell_data(i, j, k, 0) + cell_data(i, j, k - 1, 0)));
+                if (use_turb) {
+                    if (dd && pidx == 0) rA += 0.5 * (kthv(i, j, k) + kthv(i, j, k - 1));
+                    else rA += 0.5 * (mu(i, j, k) + mu(i, j, k - 1));
+                }
+                double GradCz = dxInv[2] * (prm(i, j, k, pidx) - prm(i, j, k - 1, pidx));
+                fz(i, j, k) = -rA * GradCz / 1.0;
+                if (q == ERF_RHOTHETA_COMP) hfz(i, j, k) = fz(i, j, k);
+            });
+            // cross terms on the z-faces: extrapolated at the bottom and top faces
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    {
+                        int k = 0;
+                        double mxi = hxi_K(i, j, k), meta = heta_K(i, j, k);
+                        double xlo = 0.5 * (fx(i, j, k) + fx(i + 1, j, k)), xhi = 0.5 * (fx(i, j, k + 1) + fx(i + 1, j, k + 1));
+                        double xb = 1.5 * xlo - 0.5 * xhi;
+                        double ylo = 0.5 * (fy(i, j, k) + fy(i, j + 1, k)), yhi = 0.5 * (fy(i, j, k + 1) + fy(i, j + 1, k + 1));
+                        double yb = 1.5 * ylo - 0.5 * yhi;
+                        fz(i, j, k) -= mxi * xb + meta * yb;
+                    }
+                    {
+                        int k = nz;
+                        double mxi = hxi_K(i, j, k), meta = heta_K(i, j, k);
+                        double xlo = 0.5 * (fx(i, j, k - 2) + fx(i + 1, j, k - 2)), xhi = 0.5 * (fx(i, j, k - 1) + fx(i + 1, j, k - 1));
+                        double xb = 1.5 * xhi - 0.5 * xlo;
+                        double ylo = 0.5 * (fy(i, j, k - 2) + fy(i, j + 1, k - 2)), yhi = 0.5 * (fy(i, j, k - 1) + fy(i, j + 1, k - 1));
+                        double yb = 1.5 * yhi - 0.5 * ylo;
+                        fz(i, j, k) -= mxi * xb + meta * yb;
+                    }
+                }
+            Bx z3 = valid(ZF); z3.lo[2] = 1; z3.hi[2] = nz - 1;
+            loop(z3, [&](int i, int j, int k) {
+                double mxi = hxi_K(i, j, k), meta = heta_K(i, j, k);
+                double xb = 0.25 * (fx(i, j, k) + fx(i + 1, j, k) + fx(i, j, k - 1) + fx(i + 1, j, k - 1));
+                double yb = 0.25 * (fy(i, j, k) + fy(i, j + 1, k) + fy(i, j, k - 1) + fy(i, j + 1, k - 1));
+                fz(i, j, k) -= mxi * xb + meta * yb;
+            });
+            loop(valid(XF), [&](int i, int j, int k) { fx(i, j, k) *= hzeta_I(i, j, k); });
+            loop(valid(YF), [&](int i, int j, int k) { fy(i, j, k) *= hzeta_J(i, j, k); });
+            loop(valid(CC), [&](int i, int j, int k) {
+                double s = (fx(i + 1, j, k) - fx(i, j, k)) * dxInv[0] * 1.0 + (fy(i, j + 1, k) - fy(i, j, k)) * dxInv[1] * 1.0
+                           + (fz(i, j, k + 1) - fz(i, j, k)) * dxInv[2];
+                s /= detJ(i, j, k);
+                rhs(i, j, k, q) -= s;
+            });
+            if (dd && q == ERF_RHOKE_COMP) {
+                const double l_abs_g = std::fabs(c.gravity), l_inv_theta0 = 1.0 / c.theta_ref;
+                loop(valid(CC), [&](int i, int j, int k) {
+                    rhs(i, j, k, q) += l_abs_g * l_inv_theta0 * hfz(i, j, k);
+                    rhs(i, j, k, q) += 2.0 * mut(i, j, k) * smn(i, j, k);
+                    rhs(i, j, k, q) -= diss(i, j, k);
+                });
+            }
+        }
+    }
+
+    // AdvectionSrcForMom with terrain (Advection/ERF_AdvectionSrcForMom.cpp:
+    // 208-288 for Centered_2nd, ERF_AdvectionSrcForMom_T.H:17-484 otherwise)
+    void advect_mom_T(State& R, const State& S, const Vel& V, const Fab& Om) const {
+        const Fab &ru = S.mx, &rv = S.my, &u = V.u, &v = V.v, &w = V.w;
+        const Fab &ax = axA, &ay = ayA;
+        int ht = c.dycore_horiz_adv, vt = c.dycore_vert_adv;
+        double hf = c.dycore_horiz_upw_frac, vf = c.dycore_vert_upw_frac;
+        bool c2 = (ht == ERF_ADV_CENTERED_2ND && vt == ERF_ADV_CENTERED_2ND);
+        auto iX = [&](const Fab& f, int i, int j, int k, double upw) { double s[6]; gather(f, 0, i, j, k, 0, ht, s); return interp(ht, s, upw, hf); };
+        auto iY = [&](const Fab& f, int i, int j, int k, double upw) { double s[6]; gather(f, 1, i, j, k, 0, ht, s); return interp(ht, s, upw, hf); };
+        auto iZ = [&](const Fab& f, int i, int j, int k, double upw) { double s[6]; gather(f, 2, i, j, k, 0, vt, s); return interp(vt, s, upw, vf); };
+        const double az = 1.0;
+        Bx tbx = valid(XF), tby = valid(YF), tbz = valid(ZF);
+        tbz.lo[2] = 1; tbz.hi[2] = nz - 1;
+        int lo_z_face = 0, hi_z_face = nz;
+        loop(tbx, [&](int i, int j, int k) {
+            double src;
+            if (c2) {
+                double xh = 0.25 * (ru(i, j, k) * 1.0 + ru(i + 1, j, k) * 1.0) * (u(i + 1, j, k) + u(i, j, k)) * 0.5 * (ax(i, j, k) + ax(i + 1, j, k));
+                double xl = 0.25 * (ru(i, j, k) * 1.0 + ru(i - 1, j, k) * 1.0) * (u(i - 1, j, k) + u(i, j, k)) * 0.5 * (ax(i, j, k) + ax(i - 1, j, k));
+                double yh = 0.25 * (rv(i, j + 1, k) * 1.0 + rv(i - 1, j + 1, k) * 1.0) * (u(i, j + 1, k) + u(i, j, k)) * hzeta_EK(i, j + 1, k);
+                double yl = 0.25 * (rv(i, j, k) * 1.0 + rv(i - 1, j, k) * 1.0) * (u(i, j - 1, k) + u(i, j, k)) * hzeta_EK(i, j, k);
+                double zh = 0.25 * (Om(i, j, k + 1) + Om(i - 1, j, k + 1)) * (u(i, j, k + 1) + u(i, j, k)) * 0.5 * (az + az);
+                double zl = 0.25 * (Om(i, j, k) + Om(i - 1, j, k)) * (u(i, j, k - 1) + u(i, j, k)) * 0.5 * (az + az);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+                src = -src / (0.5 * (detJ(i, j, k) + detJ(i - 1, j, k)));
+            } else {
+                double a, xh, xl, yh, yl, zh, zl;
+                a = 0.5 * (ru(i + 1, j, k) * 1.0 + ru(i, j, k) * 1.0); xh = a * iX(u, i + 1, j, k, a) * 0.5 * (ax(i, j, k) + ax(i + 1, j, k));
+                a = 0.5 * (ru(i - 1, j, k) * 1.0 + ru(i, j, k) * 1.0); xl = a * iX(u, i, j, k, a) * 0.5 * (ax(i, j, k) + ax(i - 1, j, k));
+                a = 0.5 * (rv(i, j + 1, k) * 1.0 + rv(i - 1, j + 1, k) * 1.0); yh = a * iY(u, i, j + 1, k, a) * hzeta_EK(i, j + 1, k);
+                a = 0.5 * (rv(i, j, k) * 1.0 + rv(i - 1, j, k) * 1.0); yl = a * iY(u, i, j, k, a) * hzeta_EK(i, j, k);
+                a = 0.5 * (Om(i, j, k + 1) + Om(i - 1, j, k + 1)) * 0.5 * (az + az); zh = a * iZ(u, i, j, k + 1, a);
+                a = 0.5 * (Om(i, j, k) + Om(i - 1, j, k)) * 0.5 * (az + az); zl = a * iZ(u, i, j, k, a);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+                src /= 0.5 * (detJ(i, j, k) + detJ(i - 1, j, k));
+                src = -src;
+            }
+            R.mx(i, j, k) = src;
+        });
+        loop(tby, [&](int i, int j, int k) {
+            double src;
+            if (c2) {
+                double xh = 0.25 * (ru(i + 1, j, k) * 1.0 + ru(i + 1, j - 1, k) * 1.0) * (v(i + 1, j, k) + v(i, j, k)) * hzeta_EK(i + 1, j, k);
+                double xl = 0.25 * (ru(i, j, k) * 1.0 + ru(i, j - 1, k) * 1.0) * (v(i - 1, j, k) + v(i, j, k)) * hzeta_EK(i, j, k);
+                double yh = 0.25 * (rv(i, j + 1, k) * 1.0 + rv(i, j, k) * 1.0) * (v(i, j + 1, k) + v(i, j, k)) * 0.5 * (ay(i, j, k) + ay(i, j + 1, k));
+                double yl = 0.25 * (rv(i, j, k) * 1.0 + rv(i, j - 1, k) * 1.0) * (v(i, j - 1, k) + v(i, j, k)) * 0.5 * (ay(i, j, k) + ay(i, j - 1, k));
+                double zh = 0.25 * (Om(i, j, k + 1) + Om(i, j - 1, k + 1)) * (v(i, j, k + 1) + v(i, j, k)) * 0.5 * (az + az);
+                double zl = 0.25 * (Om(i, j, k) + Om(i, j - 1, k)) * (v(i, j, k - 1) + v(i, j, k)) * 0.5 * (az + az);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+                src = -src / (0.5 * (detJ(i, j, k) + detJ(i, j - 1, k)));
+            } else {
+                double a, xh, xl, yh, yl, zh, zl;
+                a = 0.5 * (ru(i + 1, j, k) * 1.0 + ru(i + 1, j - 1, k) * 1.0); xh = a * iX(v, i + 1, j, k, a) * hzeta_EK(i + 1, j, k);
+                a = 0.5 * (ru(i, j, k) * 1.0 + ru(i, j - 1, k) * 1.0); xl = a * iX(v, i, j, k, a) * hzeta_EK(i, j, k);
+                a = 0.5 * (rv(i, j, k) * 1.0 + rv(i, j + 1, k) * 1.0); yh = a * 0.5 * (ay(i, j, k) + ay(i, j + 1, k)) * iY(v, i, j + 1, k, a);
+                a = 0.5 * (rv(i, j, k) * 1.0 + rv(i, j - 1, k) * 1.0); yl = a * 0.5 * (ay(i, j, k) + ay(i, j - 1, k)) * iY(v, i, j, k, a);
+                a = 0.5 * (Om(i, j, k + 1) + Om(i, j - 1, k + 1)) * 0.5 * (az + az); zh = a * iZ(v, i, j, k + 1, a);
+                a = 0.5 * (Om(i, j, k) + Om(i, j - 1, k)) * 0.5 * (az + az); zl = a * iZ(v, i, j, k, a);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+                src /= 0.5 * (detJ(i, j, k) + detJ(i, j - 1, k));
+                src = -src;
+            }
+            R.my(i, j, k) = src;
+        });
+        loop(tbz, [&](int i, int j, int k) {
+            double src;
+            if (c2) {
+                double xh = 0.25 * (ru(i + 1, j, k) + ru(i + 1, j, k - 1)) * 1.0 * (w(i + 1, j, k) + w(i, j, k)) * hzeta_EJ(i + 1, j, k);
+                double xl = 0.25 * (ru(i, j, k) + ru(i, j, k - 1)) * 1.0 * (w(i - 1, j, k) + w(i, j, k)) * hzeta_EJ(i, j, k);
+                double yh = 0.25 * (rv(i, j + 1, k) + rv(i, j + 1, k - 1)) * 1.0 * (w(i, j + 1, k) + w(i, j, k)) * hzeta_EI(i, j + 1, k);
+                double yl = 0.25 * (rv(i, j, k) + rv(i, j, k - 1)) * 1.0 * (w(i, j - 1, k) + w(i, j, k)) * hzeta_EI(i, j, k);
+                double zl = 0.25 * (Om(i, j, k) + Om(i, j, k - 1)) * (w(i, j, k) + w(i, j, k - 1));
+                double zh = (k == hi_z_face) ? Om(i, j, k) * w(i, j, k) * az
+                                             : 0.25 * (Om(i, j, k) + Om(i, j, k + 1)) * (w(i, j, k) + w(i, j, k + 1)) * 0.5 * (az + az);
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+                src = -src / (0.5 * (detJ(i, j, k) + detJ(i, j, k - 1)));
+            } else {
+                double a, xh, xl, yh, yl, zh, zl, ih = 0, il = 0;
+                a = 0.5 * (ru(i + 1, j, k) + ru(i + 1, j, k - 1)) * 1.0; xh = a * iX(w, i + 1, j, k, a) * hzeta_EJ(i + 1, j, k);
+                a = 0.5 * (ru(i, j, k) + ru(i, j, k - 1)) * 1.0; xl = a * iX(w, i, j, k, a) * hzeta_EJ(i, j, k);
+                a = 0.5 * (rv(i, j + 1, k) + rv(i, j + 1, k - 1)) * 1.0; yh = a * iY(w, i, j + 1, k, a) * hzeta_EI(i, j + 1, k);
+                a = 0.5 * (rv(i, j, k) + rv(i, j, k - 1)) * 1.0; yl = a * iY(w, i, j, k, a) * hzeta_EI(i, j, k);
+                auto iZall = [&](int kk, double upw, double frac, int type) { double s[6]; gather(w, 2, i, j, kk, 0, (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH) ? ERF_ADV_UPWIND_5TH : (type == ERF_ADV_CENTERED_2ND ? ERF_ADV_CENTERED_2ND : ERF_ADV_UPWIND_3RD), s); return interp_all(type, s, upw, frac); };
+                double Oh = (k == hi_z_face) ? Om(i, j, k) * az : 0.25 * (Om(i, j, k) + Om(i, j, k + 1)) * (az + az);
+                if (k == hi_z_face) { zh = Oh * w(i, j, k); }
+                else {
+                    if (k == hi_z_face - 1) ih = iZall(k + 1, Oh, 0, ERF_ADV_CENTERED_2ND);
+                    else if (k == hi_z_face - 2 || k == lo_z_face + 1) {
+                        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) ih = iZall(k + 1, Oh, 0, ERF_ADV_CENTERED_4TH);
+                        else ih = iZall(k + 1, Oh, vf, vt);
+                    } else ih = iZ(w, i, j, k + 1, Oh);
+                    zh = Oh * ih;
+                }
+                double Ol = (k == 0) ? Om(i, j, k) * az : 0.25 * (Om(i, j, k) + Om(i, j, k - 1)) * (az + az);
+                if (k == 0) { zl = Ol * w(i, j, k); }
+                else {
+                    if (k == lo_z_face + 1) il = iZall(k, Ol, 0, ERF_ADV_CENTERED_2ND);
+                    else if (k == lo_z_face + 2 || k == hi_z_face - 1) {
+                        if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) il = iZall(k, Ol, 0, ERF_ADV_CENTERED_4TH);
+                        else il = iZall(k, Ol, vf, vt);
+                    } else il = iZ(w, i, j, k, Ol);
+                    zl = Ol * il;
+                }
+                src = (xh - xl) * dxInv[0] * 1.0 + (yh - yl) * dxInv[1] * 1.0 + (zh - zl) * dxInv[2];
+                double denom = 0.5 * (detJ(i, j, k) + detJ(i, j, k - 1));
+                src /= denom;
+                src = -src;
+            }
+            R.mz(i, j, k) = src;
+        });
+    }
+
+    // ERFPhysBCFunct_w::impose_vertical_zvel_bcs with static terrain
+    // (BoundaryConditions/ERF_BoundaryConditions_zvel.cpp:200-262): w on the
+    // bottom face from Omega = 0; on a wall top likewise.
+    void physbcs_w_T(Fab& w, const Fab& u, const Fab& v, int ng) const {
+        fill_periodic(w, ZF);
+        Bx b = grow(valid(ZF), ng, ng, 0);
+        for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) {
+                w(i, j, 0) = w_from_omega(i, j, 0, 0.0, u, v);
+                w(i, j, nz) = w_from_omega(i, j, nz, 0.0, u, v);
+            }
+    }
+
+    // erf_fast_rhs_T (TimeIntegration/ERF_fast_rhs_T.cpp:39-704), static
+    // terrain, implicit substepping.
+    void fast_rhs_T(int step, const State& Rs, const State& Sprev_in, const State& Sst, State& Sd, State& Scr,
+                    double dtau, double beta_s, double facinv) {
+        State Sprev; alloc_state(Sprev); copy_state(Sprev, Sprev_in);
+        double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s), beta_d = 0.1;
+        double dxi = dxInv[0], dyi = dxInv[1], dzi = dxInv[2];
+        Fab odr, odrt, extrap, odu, odv, odw, ndu, ndv, trhs, om;
+        alloc(odr, CC, 1, 1); alloc(odrt, CC, 1, 1); alloc(extrap, CC, 1, 1);
+        alloc(odu, XF, 1, 1); alloc(odv, YF, 1, 1); alloc(odw, ZF, 1, 1);
+        alloc(ndu, XF, 1, 1); alloc(ndv, YF, 1, 1); alloc(trhs, CC, 0, 2); alloc(om, ZF, 0, 1);
+        Fab& lag = Scr.cons;
+        // cur = prev at the first substep (cons comps 0-1, ghosts included)
+        Fab& cur = Sd.cons;
+        if (step == 0)
+            loop(grow(valid(CC), 1, 1, 1), [&](int i, int j, int k) {
+                cur(i, j, k, 0) = Sprev.cons(i, j, k, 0); cur(i, j, k, 1) = Sprev.cons(i, j, k, 1);
+            });
+        loop(grow(valid(XF), 1, 1, 0), [&](int i, int j, int k) {
+            odu(i, j, k) = Sprev.mx(i, j, k) - Sst.mx(i, j, k);
+            if (k == nz - 1) odu(i, j, k + 1) = odu(i, j, k);
+        });
+        loop(grow(valid(YF), 1, 1, 0), [&](int i, int j, int k) {
+            odv(i, j, k) = Sprev.my(i, j, k) - Sst.my(i, j, k);
+            if (k == nz - 1) odv(i, j, k + 1) = odv(i, j, k);
+        });
+        loop(grow(valid(ZF), 1, 1, 0), [&](int i, int j, int k) { odw(i, j, k) = Sprev.mz(i, j, k) - Sst.mz(i, j, k); });
+        loop(grow(valid(CC), 1, 1, 1), [&](int i, int j, int k) {
+            odr(i, j, k) = cur(i, j, k, 0) - Sst.cons(i, j, k, 0);
+            odrt(i, j, k) = cur(i, j, k, 1) - Sst.cons(i, j, k, 1);
+            if (step == 0) extrap(i, j, k) = odrt(i, j, k);
+            else extrap(i, j, k) = odrt(i, j, k) + beta_d * (odrt(i, j, k) - lag(i, j, k, 1));
+        });
+        loop(grow(valid(CC), 1, 1, 1), [&](int i, int j, int k) { lag(i, j, k, 1) = odrt(i, j, k); });
+        Fab& avx = Scr.mx; Fab& avy = Scr.my; Fab& avz = Scr.mz;
+        loop(valid(XF), [&](int i, int j, int k) {
+            double mxi = hxi_I(i, j, k), mz = hzeta_I(i, j, k);
+            double gp_xi = (extrap(i, j, k) - extrap(i - 1, j, k)) * dxi;
+            double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k) - extrap(i, j, k))
+                                      : 0.25 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k - 1) - extrap(i, j, k - 1));
+            double gpx = gp_xi - (mxi / mz) * gp_zeta;
+            gpx *= 1.0;
+            if (use_moisture) {
+                double q = 0.5 * (prim(i, j, k, 4) + prim(i - 1, j, k, 4) + prim(i, j, k, 5) + prim(i - 1, j, k, 5));
+                gpx /= (1.0 + q);
+            }
+            double pi_c = 0.5 * (pi_stage(i - 1, j, k) + pi_stage(i, j, k));
+            double f = -Gamma_ * R_d * pi_c * gpx;
+            ndu(i, j, k) = odu(i, j, k) + dtau * f + dtau * Rs.mx(i, j, k);
+            avx(i, j, k) += facinv * ndu(i, j, k);
+            Sd.mx(i, j, k) = Sst.mx(i, j, k) + ndu(i, j, k);
+        });
+        loop(valid(YF), [&](int i, int j, int k) {
+            double meta = heta_J(i, j, k), mz = hzeta_J(i, j, k);
+            double gp_eta = (extrap(i, j, k) - extrap(i, j - 1, k)) * dyi;
+            double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k) - extrap(i, j - 1, k))
+                                      : 0.25 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k - 1) - extrap(i, j - 1, k - 1));
+            double gpy = gp_eta - (meta / mz) * gp_zeta;
+            gpy *= 1.0;
+            if (use_moisture) {
+                double q = 0.5 * (prim(i, j, k, 4) + prim(i, j - 1, k, 4) + prim(i, j, k, 5) + prim(i, j - 1, k, 5));
+                gpy /= (1.0 + q);
+            }
+            double pi_c = 0.5 * (pi_stage(i, j - 1, k) + pi_stage(i, j, k));
+            double f = -Gamma_ * R_d * pi_c * gpy;
+            ndv(i, j, k) = odv(i, j, k) + dtau * f + dtau * Rs.my(i, j, k);
+            avy(i, j, k) += facinv * ndv(i, j, k);
+            Sd.my(i, j, k) = Sst.my(i, j, k) + ndv(i, j, k);
+        });
+        // horizontal fluxes of rho and rho theta through the sloping faces
+        loop(valid(CC), [&](int i, int j, int k) {
+            double hxh = 0.5 * dzi * (Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j, k) - Z(i + 1, j + 1, k));
+            double hxl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
+            double hyh = 0.5 * dzi * (Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
+            double hyl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i + 1, j, k));
+            double xl = ndu(i, j, k) * hxl / 1.0, xh = ndu(i + 1, j, k) * hxh / 1.0;
+            double yl = ndv(i, j, k) * hyl / 1.0, yh = ndv(i, j + 1, k) * hyh / 1.0;
+            double mfsq = 1.0;
+            trhs(i, j, k, 0) = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
+            trhs(i, j, k, 1) = ((xh * (prim(i, j, k, 0) + prim(i + 1, j, k, 0)) - xl * (prim(i, j, k, 0) + prim(i - 1, j, k, 0))) * dxi * mfsq +
+                                (yh * (prim(i, j, k, 0) + prim(i, j + 1, k, 0)) - yl * (prim(i, j, k, 0) + prim(i, j - 1, k, 0))) * dyi * mfsq) * 0.5;
+        });
+        // contravariant vertical increment of the previous substep
+        loop(valid(ZF), [&](int i, int j, int k) {
+            if (k == 0) om(i, j, k) = 0.;
+            else if (k == nz) om(i, j, k) = odw(i, j, k);
+            else om(i, j, k) = omega_from_w(i, j, k, odw(i, j, k), odu, odv);
+        });
+        double halfg = std::abs(0.5 * -c.gravity);
+        Fab RHS, soln; alloc(RHS, ZF, 0, 1); alloc(soln, ZF, 0, 1);
+        Bx bs = valid(CC); bs.lo[2] = 1; bs.hi[2] = nz - 1;
+        const Fab& fc = fast_coeffs;
+        loop(bs, [&](int i, int j, int k) {
+            double dJk = 0.5 * (detJ(i, j, k) + detJ(i, j, k - 1));
+            double cP = fc(i, j, k, 3), cQ = fc(i, j, k, 4);
+            if (use_moisture) {
+                double q = 0.5 * (prim(i, j, k, 4) + prim(i, j, k - 1, 4) + prim(i, j, k, 5) + prim(i, j, k - 1, 5));
+                cP /= (1.0 + q); cQ /= (1.0 + q);
+            }
+            double tlo = 0.5 * (prim(i, j, k - 2, 0) + prim(i, j, k - 1, 0));
+            double tmid = 0.5 * (prim(i, j, k - 1, 0) + prim(i, j, k, 0));
+            double thi = 0.5 * (prim(i, j, k, 0) + prim(i, j, k + 1, 0));
+            double R0t = (-halfg * odr(i, j, k) + cP * odrt(i, j, k)) * detJ(i, j, k)
+                         + (-halfg * odr(i, j, k - 1) + cQ * odrt(i, j, k - 1)) * detJ(i, j, k - 1);
+            double R1t = -halfg * (Rs.cons(i, j, k, 0) * detJ(i, j, k) + Rs.cons(i, j, k - 1, 0) * detJ(i, j, k - 1))
+                         + (cP * Rs.cons(i, j, k, 1) * detJ(i, j, k) + cQ * Rs.cons(i, j, k - 1, 1) * detJ(i, j, k - 1));
+            double Okp1 = om(i, j, k + 1), Ok = om(i, j, k), Okm1 = om(i, j, k - 1);
+            R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + trhs(i, j, k, 0) + trhs(i, j, k - 1, 0));
+            R1t += -(cP * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + trhs(i, j, k, 1)) +
+                     cQ * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + trhs(i, j, k - 1, 1)));
+            RHS(i, j, k) = dJk * odw(i, j, k) + dtau * (dJk * Rs.mz(i, j, k) + R0t + dtau * beta_2 * R1t);
+            RHS(i, j, k) += dJk * omega_from_w(i, j, k, 0., ndu, ndv);
+        });
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                RHS(i, j, 0) = dtau * Rs.mz(i, j, 0);
+                RHS(i, j, nz) = dtau * Rs.mz(i, j, nz);
+                soln(i, j, 0) = RHS(i, j, 0) * fc(i, j, 0, 1);
+                for (int k = 1; k <= nz; ++k) soln(i, j, k) = (RHS(i, j, k) - fc(i, j, k, 0) * soln(i, j, k - 1)) * fc(i, j, k, 1);
+                for (int k = nz - 1; k >= 0; --k) soln(i, j, k) -= (fc(i, j, k, 2) * fc(i, j, k, 1)) * soln(i, j, k + 1);
+            }
+        loop(valid(ZF), [&](int i, int j, int k) {
+            Sd.mz(i, j, k) = Sst.mz(i, j, k);
+            if (k >= 1 && k <= nz - 1) Sd.mz(i, j, k) += w_from_omega(i, j, k, soln(i, j, k), ndu, ndv);
+        });
+        loop(valid(CC), [&](int i, int j, int k) {
+            double zl = beta_2 * soln(i, j, k) + beta_1 * om(i, j, k);
+            double zh = beta_2 * soln(i, j, k + 1) + beta_1 * om(i, j, k + 1);
+            avz(i, j, k) += facinv * zl / (1.0 * 1.0);
+            if (k == nz - 1) avz(i, j, k + 1) += facinv * zh / (1.0 * 1.0);
+            double frho = -(trhs(i, j, k, 0) + (zh - zl) * dzi) / detJ(i, j, k);
+            cur(i, j, k, 0) += dtau * (Rs.cons(i, j, k, 0) + frho);
+            double frt = -(trhs(i, j, k, 1) + 0.5 * (zh * (prim(i, j, k, 0) + prim(i, j, k + 1, 0)) - zl * (prim(i, j, k, 0) + prim(i, j, k - 1, 0))) * dzi) / detJ(i, j, k);
+            cur(i, j, k, 1) += dtau * (Rs.cons(i, j, k, 1) + frt);
+        });
+    }
+
     void step(double dt) {
         const double beta_s = 0.1;
         // FillPatch of the old state (ghost cells of cons and velocities)
@@ -1261,7 +2215,8 @@ struct Oracle {
         physbcs_cons(Sc, 0, ncomp, ngc);
         physbcs_tangential(vel_state.u, XF, ngv);
         physbcs_tangential(vel_state.v, YF, ngv);
-        physbcs_w(vel_state.w, ngv);
+        if (terrain) physbcs_w_T(vel_state.w, vel_state.u, vel_state.v, ngv);
+        else physbcs_w(vel_state.w, ngv);
         // S_old = {cons, V2M(old velocities)}
         S_old.cons.copy_from(Sc);
         // turbulent viscosity from the old velocities (strain + Smagorinsky)
@@ -1288,7 +2243,8 @@ struct Oracle {
             double inv_fac = 1.0 / (double)nsub;
             for (int ks = 0; ks < nsub; ++ks) {
                 if (ks == 0) make_fast_coeffs(S_new, dtau, beta_s);
-                fast_rhs_N(ks, nrk, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);
+                if (terrain) fast_rhs_T(ks, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);
+                else fast_rhs_N(ks, nrk, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);
                 apply_bcs(S_sum, Vnew, 1, 1, true, false);
             }
             slow_rhs_post(nrk, slow_dt, F_slow, S_old, S_new, S_sum, S_scr);
@@ -1403,6 +2359,62 @@ int oracle_advance(const erf_b200_config* cfg, const double* rho0, const double*
     std::unique_ptr<Oracle> o(new Oracle(*cfg));
     int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
     for (int k = 0; k < nz + 2; ++k) { o->r0[k] = rho0[k]; o->p0[k] = p0[k]; o->pi0[k] = pi0[k]; o->th0[k] = th0[k]; }
+    o->init_storage();
+    o->alloc(o->cons_state, CC, o->ngc, o->ncomp);
+    o->alloc_vel(o->vel_state);
+    load_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    load_box(o->vel_state.u, u, nx + 1, ny, nz);
+    load_box(o->vel_state.v, v, nx, ny + 1, nz);
+    load_box(o->vel_state.w, w, nx, ny, nz + 1);
+    for (int s = 0; s < nsteps; ++s) o->step(cfg->dt);
+    store_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    store_box(o->vel_state.u, u, nx + 1, ny, nz);
+    store_box(o->vel_state.v, v, nx, ny + 1, nz);
+    store_box(o->vel_state.w, w, nx, ny, nz + 1);
+    return 0;
+}
+
+// Base state over terrain.  z_nd: valid nodes (nz+1)(ny+1)(nx+1); th3/qv3:
+// nz*ny*nx cell values; outputs (nz+2)*ny*nx, plane k+1 for level k.
+int oracle_make_base_state_terrain(const erf_b200_config* cfg, const double* z_nd, const double* th3,
+                                   const double* qv3, double th_s, double qv_s, double p_s, double* rho0,
+                                   double* p0, double* pi0, double* th0) {
+    Oracle o(*cfg);
+    o.set_terrain(z_nd);
+    o.make_base_state_terrain(th3, qv3, th_s, qv_s, p_s, rho0, p0, pi0, th0);
+    return 0;
+}
+
+// Metrics of a terrain grid: detJ and z_cc (nz*ny*nx), ax ((nz)(ny)(nx+1)),
+// ay ((nz)(ny+1)(nx)), valid region, i fastest.
+int oracle_terrain_metrics(const erf_b200_config* cfg, const double* z_nd, double* detJ, double* zcc, double* ax,
+                           double* ay) {
+    Oracle o(*cfg);
+    o.set_terrain(z_nd);
+    int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                size_t c = ((size_t)k * ny + j) * nx + i;
+                detJ[c] = o.detJ(i, j, k); zcc[c] = o.zcc(i, j, k);
+            }
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i <= nx; ++i) ax[((size_t)k * ny + j) * (nx + 1) + i] = o.axA(i, j, k);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j <= ny; ++j)
+            for (int i = 0; i < nx; ++i) ay[((size_t)k * (ny + 1) + j) * nx + i] = o.ayA(i, j, k);
+    return 0;
+}
+
+// Advance over terrain: base state in the (nz+2)-plane layout.
+int oracle_advance_terrain(const erf_b200_config* cfg, const double* z_nd, const double* rho0, const double* p0,
+                           const double* pi0, const double* th0, double* cons, double* u, double* v, double* w,
+                           int nsteps) {
+    std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
+    o->set_terrain(z_nd);
+    o->set_base_terrain(rho0, p0, pi0, th0);
     o->init_storage();
     o->alloc(o->cons_state, CC, o->ngc, o->ncomp);
     o->alloc_vel(o->vel_state);
