@@ -36,6 +36,7 @@ struct Bulk {
     R *c12 = nullptr, *c13 = nullptr, *c23 = nullptr;  // learned closure: cell-centred off-diagonal stresses
     R *hx = nullptr, *hy = nullptr, *hz = nullptr;     // learned closure: rho * heat flux
     TkeBuf<R> tke{nullptr, nullptr, nullptr, nullptr}; // Deardorff closure arrays
+    TerBuf<R> ter{};                                    // static terrain scratch
 };
 
 // Threads per block of the vertical acoustic kernel (columns x level groups).
@@ -67,7 +68,9 @@ struct erf_b200_ctx {
     int tile_tx = 32, vert_warps = 32, coef_warps = 8;
     TiledKz tkz{1, 1, 1};
     size_t vert_smem = 0, coef_smem = 0;
-    double *r0, *p0, *pi0, *th0;
+    double *r0, *p0, *pi0, *th0;   // nz+2 values, or (nz+2) planes with terrain
+    double *znd = nullptr, *detJ = nullptr, *zcc = nullptr;   // static terrain
+    bool ter_set = false;
     double *h_stage;          // device staging buffers for the host-array entry point
     int* status;
     bool base_set = false;
@@ -131,6 +134,12 @@ int validate(const erf_b200_config* c) {
     if (c->les_type == ERF_LES_DEARDORFF && (!(c->theta_ref > 0.0) || !(c->sigma_k > 0.0) || !(c->Ck > 0.0)))
         return ERF_B200_ECONFIG;
     if (c->les_type == ERF_LES_MLP && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
+    if (c->use_terrain != 0 && c->use_terrain != 1) return ERF_B200_ECONFIG;
+    if (c->use_terrain) {
+        // terrain path: dry, LES closure (or no diffusion), explicit closures only
+        if (c->moisture != ERF_MOIST_NONE || c->les_type == ERF_LES_MLP) return ERF_B200_ECONFIG;
+        if (c->les_type == ERF_LES_NONE && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
+    }
     if (c->molec_diff_type < 0 || c->molec_diff_type > 2) return ERF_B200_ECONFIG;
     if (c->moisture == ERF_MOIST_NONE) {
         if (c->ncomp != 5) return ERF_B200_ECONFIG;
@@ -170,6 +179,10 @@ void make_params(erf_b200_ctx* c) {
     double cellVolMsf = 1.0 / (g.dxi * 1.0 * g.dyi * 1.0 * g.dzi);
     double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
     P.CsDeltaSqr = f.Cs * f.Cs * DeltaMsf * DeltaMsf;
+    P.Cs = f.Cs;
+    P.ter = f.use_terrain;
+    P.znd = c->znd;
+    P.detJ = c->detJ;
     // Deardorff constants (ERF_ComputeTurbulentViscosity.cpp:129-142) and the
     // buoyancy factor of the TKE source (ERF_DiffusionSrcForState_N.cpp:681-697)
     P.Delta = DeltaMsf;
@@ -251,9 +264,62 @@ struct LaunchTimer {
         if (T) T->done();                     \
     } while (0)
 
+// One full step over static terrain: the same stage / substep schedule with
+// the terrain passes (dry states only).
+template <class R>
+void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
+    const Params& P = c->P;
+    const Geo& g = c->g;
+    cudaStream_t st = c->stream;
+    StateBuf OLD = c->S[p], N0 = c->S[1 - p], N1 = c->S[2], SUM = c->S[3];
+    double** Vold = c->vel[p];
+    double** Vnew = c->vel[1 - p];
+    TIMED(0, launch_ter_step_begin<R>(P, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
+                                      B.aux[0], B.mut, B.tke));
+    StateBuf outs[3] = {N0, N1, N0};
+    StateBuf stage[3] = {OLD, outs[0], outs[1]};
+    dim3 tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1), tcb(c->tile_tx, c->coef_warps, 1);
+    int a = 0;
+    int lp = (p * c->lag_parity_per_step) & 1;
+    const double beta_s = 0.1;
+    const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
+    for (int nrk = 0; nrk < 3; ++nrk) {
+        StateBuf Sst = stage[nrk], Snew = outs[nrk];
+        StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
+        int nsub; double dtau, slow_dt;
+        stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
+        if (P.use_diff)
+            TIMED(1, launch_ter_tau<R>(P, st, nrk, Sst.cons, Vnew[0], Vnew[1], Vnew[2], B.mut, B.ter, B.tke, B.t11,
+                                       B.t22, B.t33, B.t12, B.t13, B.t23));
+        TIMED(2, launch_ter_slow_cell<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], B.mut, B.tke, B.Fcons, B.avx, B.avy,
+                                         B.avz));
+        TIMED(4, launch_ter_slow_mom<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12, B.t13,
+                                        B.t23, B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz));
+        double facinv = 1.0 / (double)nsub;
+        double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
+        TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
+        for (int ks = 0; ks < nsub; ++ks) {
+            StateBuf Sprev = (ks == 0) ? OLD : SUM;
+            int prt = ks > 0;
+            TIMED(5, launch_ter_fast_h<R>(P, st, ks, dtau, facinv, Sprev, prt, Sst, Acur, B.Fmx, B.Fmy, B.lag[lp],
+                                          B.lag[1 - lp], B.ter, B.avx, B.avy, SUM.mx, SUM.my));
+            lp ^= 1;
+            TIMED(6, launch_ter_fast_vert<R>(P, st, dtau, facinv, beta_1, beta_2, Sprev, prt, Sst, Acur, B.Fcons, B.Fmz,
+                                             B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, SUM.cons, SUM.mz));
+        }
+        TIMED(7, launch_ter_post<R>(P, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut, B.tke,
+                                    B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
+        a = 1 - a;
+    }
+}
+
 // Enqueue one full step with parity p (state slot p is the old state).
 template <class R>
 void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
+    if (c->P.ter) {
+        enqueue_step_ter<R>(c, B, p, T);
+        return;
+    }
     const Params& P = c->P;
     const Geo& g = c->g;
     cudaStream_t st = c->stream;
@@ -339,6 +405,12 @@ int alloc_bulk(erf_b200_ctx* c, Bulk<R>& B) {
     }
     if (cfg->les_type == ERF_LES_DEARDORFF) {
         A(&B.tke.kthv, N); A(&B.tke.diss, N); A(&B.tke.smn, N); A(&B.tke.hfz, NZF);
+    }
+    if (cfg->use_terrain) {
+        A(&B.ter.s11, N); A(&B.ter.s22, N); A(&B.ter.s33, N); A(&B.ter.s12, N); A(&B.ter.s13, NZF);
+        A(&B.ter.s23, NZF); A(&B.ter.t31, NZF); A(&B.ter.t32, NZF);
+        A(&B.ter.ndu, N); A(&B.ter.ndv, N); A(&B.ter.odu, N); A(&B.ter.odv, N);
+        if (rc == ERF_B200_OK) rc = dalloc(c, &B.ter.soln, (size_t)4 * (cfg->nz + 1) * cfg->nx * cfg->ny);
     }
     return rc;
 }
@@ -450,7 +522,14 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     A(&c->pavg, 6 * cfg->nz);
     c->mixed = cfg->precision == ERF_PREC_MIXED;
     if (rc == ERF_B200_OK) rc = c->mixed ? alloc_bulk(c, c->bf) : alloc_bulk(c, c->bd);
-    A(&c->r0, cfg->nz + 2); A(&c->p0, cfg->nz + 2); A(&c->pi0, cfg->nz + 2); A(&c->th0, cfg->nz + 2);
+    {
+        const size_t nb = cfg->use_terrain ? (size_t)(cfg->nz + 2) * cfg->nx * cfg->ny : (size_t)(cfg->nz + 2);
+        A(&c->r0, nb); A(&c->p0, nb); A(&c->pi0, nb); A(&c->th0, nb);
+    }
+    if (cfg->use_terrain) {
+        const size_t sk = (size_t)cfg->nx * cfg->ny;
+        A(&c->znd, (size_t)(cfg->nz + 3) * sk); A(&c->detJ, N); A(&c->zcc, (size_t)(cfg->nz + 1) * sk);
+    }
     if (rc == ERF_B200_OK) {
         void* q = nullptr;
         if (cudaMalloc(&q, sizeof(int)) != cudaSuccess) rc = ERF_B200_ENOMEM;
@@ -543,6 +622,7 @@ int erf_b200_set_base_state(erf_b200_ctx* c, const double* rho0, const double* p
                             const double* th0) {
     if (!c || !rho0 || !p0 || !pi0 || !th0) return ERF_B200_EINVAL;
     size_t b = (c->cfg.nz + 2) * sizeof(double);
+    if (c->cfg.use_terrain) b *= (size_t)c->cfg.nx * c->cfg.ny;
     CK(cudaMemcpyAsync(c->r0, rho0, b, cudaMemcpyDefault, c->stream));
     CK(cudaMemcpyAsync(c->p0, p0, b, cudaMemcpyDefault, c->stream));
     CK(cudaMemcpyAsync(c->pi0, pi0, b, cudaMemcpyDefault, c->stream));
@@ -551,10 +631,62 @@ int erf_b200_set_base_state(erf_b200_ctx* c, const double* rho0, const double* p
     return ERF_B200_OK;
 }
 
+// Install z_phys_nd for a context created with use_terrain: (nz+1)(ny+1)(nx+1)
+// node heights, i fastest (host or device memory).  The terrain must be
+// periodic (node nx equal to node 0, node ny to node 0).  The ghost levels
+// are extrapolated as init_terrain_grid does (ERF_TerrainMetrics.cpp:320-333)
+// and detJ / z_cc formed on the GPU (make_J, make_zcc).
+int erf_b200_set_terrain(erf_b200_ctx* c, const double* z_nd) {
+    if (!c || !z_nd || !c->cfg.use_terrain) return ERF_B200_EINVAL;
+    const int nx = c->cfg.nx, ny = c->cfg.ny, nz = c->cfg.nz;
+    const size_t nn = (size_t)(nx + 1) * (ny + 1) * (nz + 1), sk = (size_t)nx * ny;
+    std::vector<double> h(nn), z((size_t)(nz + 3) * sk);
+    CK(cudaMemcpy(h.data(), z_nd, nn * sizeof(double), cudaMemcpyDefault));
+    auto at = [&](int i, int j, int k) { return h[((size_t)k * (ny + 1) + j) * (nx + 1) + i]; };
+    for (int k = 0; k <= nz; ++k)
+        for (int j = 0; j <= ny; ++j)
+            if (at(nx, j, k) != at(0, j, k)) return ERF_B200_EINVAL;
+    for (int k = 0; k <= nz; ++k)
+        for (int i = 0; i <= nx; ++i)
+            if (at(i, ny, k) != at(i, 0, k)) return ERF_B200_EINVAL;
+    for (int k = -1; k <= nz + 1; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                double v;
+                if (k == -1) v = 2.0 * at(i, j, 0) - at(i, j, 1);
+                else if (k == nz + 1) v = 2.0 * at(i, j, nz) - at(i, j, nz - 1);
+                else v = at(i, j, k);
+                if (std::isnan(v)) return ERF_B200_EINVAL;
+                z[(size_t)(k + 1) * sk + (size_t)j * nx + i] = v;
+            }
+    CK(cudaMemcpyAsync(c->znd, z.data(), z.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    launch_ter_metrics(c->P, c->stream, c->detJ, c->zcc);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<double> J(sk * nz);
+    CK(cudaMemcpy(J.data(), c->detJ, J.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (double v : J)
+        if (!(v > 0.0)) return ERF_B200_EINVAL;   // folded or inverted cells
+    c->ter_set = true;
+    return ERF_B200_OK;
+}
+
+// Base state over the terrain (device pointers): theta3 / qv3 at the cell
+// centres (nz planes of nx*ny); rho0 / p0 / pi0 / th0 receive (nz+2) planes,
+// plane k+1 for level k.  calc_rho_p + erf_enforce_hse per column.
+int erf_b200_make_base_state_terrain(erf_b200_ctx* c, const double* theta3, const double* qv3, double theta_sfc,
+                                     double qv_sfc, double p_sfc, double* rho0, double* p0, double* pi0,
+                                     double* th0) {
+    if (!c || !c->ter_set || !theta3 || !qv3 || !rho0 || !p0 || !pi0 || !th0) return ERF_B200_EINVAL;
+    launch_ter_base_state(c->P, c->stream, c->zcc, theta3, qv3, theta_sfc, qv_sfc, p_sfc, rho0, p0, pi0, th0);
+    return cuda_fail(cudaGetLastError());
+}
+
 int erf_b200_advance(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_fab* xvel,
                      const erf_b200_fab* yvel, const erf_b200_fab* zvel, int nsteps) {
     if (!c || nsteps < 0) return ERF_B200_EINVAL;
     if (!c->base_set) return ERF_B200_EINVAL;
+    if (c->cfg.use_terrain && !c->ter_set) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
         return ERF_B200_EINVAL;
@@ -730,6 +862,7 @@ extern "C" {
 int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, const erf_b200_fab* yvel,
                                  const erf_b200_fab* zvel, const erf_b200_fab* cons) {
     if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
+    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
     const Geo& g = c->g;
     if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
         return ERF_B200_EINVAL;
@@ -750,6 +883,7 @@ int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b2
                           const erf_b200_fab* yvel, const erf_b200_fab* zvel) {
     (void)nrk; (void)slow_dt;
     if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
+    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
     if (c->P.les == ERF_LES_MLP && !c->net) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
@@ -786,6 +920,7 @@ int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b2
 int erf_b200_make_fast_coeffs(erf_b200_ctx* c, const erf_b200_fab* fast_coeffs, const erf_b200_fab* S_stage,
                               double dtau) {
     if (!c || c->mixed || !c->base_set || !fast_coeffs) return ERF_B200_EINVAL;
+    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
     const Geo& g = c->g;
     if (!fab4_ok(S_stage, g, c->cfg.ncomp) || !fab_ok(fast_coeffs, 3, g, 5)) return ERF_B200_EINVAL;
     StateBuf Sst = c->S[2];
@@ -805,6 +940,7 @@ int erf_b200_fast_rhs_N(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* 
                         const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
                         const erf_b200_fab* S_scratch, double dtau, double facinv) {
     if (!c || c->mixed || !c->base_set || step < 0 || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
+    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
     if (!fab4_ok(S_slow_rhs, g, 2) || !fab4_ok(S_prev, g, 2) || !fab4_ok(S_stage, g, nc) || !fab4_ok(S_data, g, 2) ||
@@ -844,6 +980,7 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
                            const erf_b200_fab* S_scratch) {
     (void)S_rhs;
     if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
+    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
     if (!fab4_ok(S_old, g, nc) || !fab4_ok(S_new, g, nc) || !fab4_ok(S_data, g, nc) || !fab4_ok(S_scratch, g, 1))

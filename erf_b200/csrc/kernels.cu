@@ -85,7 +85,7 @@ __device__ __forceinline__ void stage_aux_cell(const Params& P, const double* __
     for (int n = 1; n < P.nprim; ++n) A.prim[n * N + c] = R(cons[(n + 1) * N + c] / rho);
     A.pi[c] = R(eos_exner(rt, P.rdOcp));
     double qv = P.moist ? cons[5 * N + c] / rho : 0.0;
-    A.pp[c] = R(eos_p(rt, qv) - P.p0[k + 1]);
+    A.pp[c] = R(eos_p(rt, qv) - (P.ter ? P.p0[c + P.g.sk] : P.p0[k + 1]));
     if (!(rt > 0.0) || !(rho > 0.0)) atomicOr(P.status, ST_BADSTATE);
 }
 
@@ -644,9 +644,19 @@ __global__ void k_fast_coef(Params P, double D_d, StateBuf Sst, StageAux<R> A, R
         for (int k = 1 + t.w; k <= nz - 1; k += t.nw) {
             int64_t c = cidx(g, t.i, t.j, k), cm = c - g.sk;
             R pi_c = R(0.5) * (A.pi[cm] + A.pi[c]);
-            R P_ = R(-Gamma_ * R_d * g.dzi + P.halfg * R_d * P.r0[k + 1] / (P.c_v * P.pi0[k + 1] * Sst.cons[N + c]));
+            // with terrain (ERF_make_fast_coeffs.cpp:110-140): the 3-D base
+            // state, the acoustic terms over detJ at the face and B = detJ + ...
+            double dJk = 1.0, inv_dJk = 1.0, r_hi, r_lo, pi_hi, pi_lo;
+            if (P.ter) {
+                dJk = 0.5 * (P.detJ[c] + P.detJ[cm]);
+                inv_dJk = 1. / dJk;
+                r_hi = P.r0[c + g.sk]; r_lo = P.r0[c]; pi_hi = P.pi0[c + g.sk]; pi_lo = P.pi0[c];
+            } else {
+                r_hi = P.r0[k + 1]; r_lo = P.r0[k]; pi_hi = P.pi0[k + 1]; pi_lo = P.pi0[k];
+            }
+            R P_ = R(-Gamma_ * R_d * g.dzi * inv_dJk + P.halfg * R_d * r_hi / (P.c_v * pi_hi * Sst.cons[N + c]));
             P_ *= pi_c;
-            R Q_ = R(Gamma_ * R_d * g.dzi + P.halfg * R_d * P.r0[k] / (P.c_v * P.pi0[k] * Sst.cons[N + cm]));
+            R Q_ = R(Gamma_ * R_d * g.dzi * inv_dJk + P.halfg * R_d * r_lo / (P.c_v * pi_lo * Sst.cons[N + cm]));
             Q_ *= pi_c;
             if (P.moist) {
                 R q = R(0.5) * (th[4 * N + c] + th[4 * N + cm] + th[5 * N + c] + th[5 * N + cm]);
@@ -658,7 +668,7 @@ __global__ void k_fast_coef(Params P, double D_d, StateBuf Sst, StageAux<R> A, R
             R thi = R(0.5) * (th[c] + th[cidx(g, t.i, t.j, clampk(k + 1, nz))]);
             R a = D * (halfg - Q_ * tlo);
             R cc = D * (-halfg + P_ * thi);
-            R b = R(1) + D * (Q_ - P_) * tmid;
+            R b = R(dJk) + D * (Q_ - P_) * tmid;
             sA[k * TX + t.lane] = a; sB[k * TX + t.lane] = b; sC[k * TX + t.lane] = cc;
             cA[c] = a; cP[c] = P_; cQ[c] = Q_;
         }

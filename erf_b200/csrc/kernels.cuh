@@ -12,6 +12,7 @@ struct Params {
     int moist, kessler_rain;
     int use_diff, use_turb, use_consA, les;
     double CsDeltaSqr;          // Cs^2 Delta^2 (host-computed, reference order)
+    double Cs;
     double Delta;               // (dx dy dz)^(1/3)
     double Ck, Ce_wall, Ce_lcoeff, g_over_theta0, invSigmaK;   // Deardorff constants
     double invPr, invSc;
@@ -23,10 +24,15 @@ struct Params {
     double cf, sinphi, cosphi, geo0, geo1, geo2;
     int dyc_h, dyc_v, dry_h, dry_v, moi_h, moi_v;
     double f_dyc_h, f_dyc_v, f_dry_h, f_dry_v, f_moi_h, f_moi_v;
-    const double* r0;           // base state, index k+1 for cell k (nz+2)
-    const double* p0;
-    const double* pi0;
+    const double* r0;           // base state, index k+1 for cell k (nz+2); with
+    const double* p0;           // terrain (nz+2) planes of nx*ny, plane k+1
+    const double* pi0;          // for level k
     int* status;
+    // static terrain: z_phys_nd as (nz+3) planes of nx*ny nodes (plane k+1
+    // for node level k, lateral node index periodic) and detJ per cell
+    int ter;
+    const double* znd;
+    const double* detJ;
 };
 
 // One copy of the prognostic state: cons (ncomp*ncell), face momenta.
@@ -54,6 +60,18 @@ struct TkeBuf {
     R* diss;
     R* smn;
     R* hfz;
+};
+
+// Terrain scratch (R): strain components of the stage (tau_ii with the
+// expansion-rate third removed, S12, S13, S23 on edges), the non-symmetric
+// stresses tau31 / tau32, the substep's horizontal momentum increments, and
+// the column solution of the implicit solve (FP64, per z-face).
+template <class R>
+struct TerBuf {
+    R *s11, *s22, *s33, *s12, *s13, *s23;
+    R *t31, *t32;
+    R *ndu, *ndv, *odu, *odv;
+    double* soln;   // 4 (nz+1) per column
 };
 
 // x-y tile of the transport kernels (slow_cell, slow_mom, post) and the
@@ -122,5 +140,38 @@ template <class R>
 void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst,
                  StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
                  TkeBuf<R> tke, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
+
+// Static terrain (terrain.cu): metrics, base state and the _T passes.
+void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* zcc);
+void launch_ter_base_state(const Params& P, cudaStream_t st, const double* zcc, const double* th3, const double* qv3,
+                           double th_s, double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0);
+template <class R>
+void launch_ter_step_begin(const Params& P, cudaStream_t st, const double* cons, const double* uo, const double* vo,
+                           const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut,
+                           TkeBuf<R> tke);
+template <class R>
+void launch_ter_tau(const Params& P, cudaStream_t st, int nrk, const double* cons, const double* u, const double* v,
+                    const double* w, const R* mut, TerBuf<R> T, TkeBuf<R> tke, R* t11, R* t22, R* t33, R* t12, R* t13,
+                    R* t23);
+template <class R>
+void launch_ter_slow_cell(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
+                          const double* v, const R* mut, TkeBuf<R> tke, R* Fcons, R* avx, R* avy, R* avz);
+template <class R>
+void launch_ter_slow_mom(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
+                         const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,
+                         const R* t13, const R* t23, TerBuf<R> T, const R* Om, R* Fmx, R* Fmy, R* Fmz);
+template <class R>
+void launch_ter_fast_h(const Params& P, cudaStream_t st, int step, double dtau, double facinv, StateBuf Sprev,
+                       int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in,
+                       R* lag_out, TerBuf<R> T, R* avx, R* avy, double* outx, double* outy);
+template <class R>
+void launch_ter_fast_vert(const Params& P, cudaStream_t st, double dtau, double facinv, double beta_1, double beta_2,
+                          StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmz,
+                          TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz,
+                          double* out_cons, double* out_mz);
+template <class R>
+void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
+                     StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,
+                     const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
 
 }  // namespace erfb

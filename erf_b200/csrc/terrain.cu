@@ -1,0 +1,1439 @@
+// terrain.cu -- static terrain-following grid: metrics, per-column base state
+// and the terrain (_T) variants of the dycore passes.
+//
+// The grid is the reference's z_phys_nd (Utils/ERF_TerrainMetrics.cpp:88-335)
+// stored as (nz+3) planes of nx*ny nodes (plane k+1 holds node level k, so
+// the extrapolated levels -1 and nz+1 are included); the terrain must be
+// periodic (node nx equal to node 0), so lateral node indices wrap like the
+// cell indices.  Arithmetic is FP64 throughout; the bulk arrays (right-hand
+// sides, stresses, averaged momenta, primitives) are stored in R.
+//
+// Passes (each one thread per cell, face or column, reading neighbours
+// directly):
+//   k_ter_metrics     make_J / make_zcc (ERF_TerrainMetrics.cpp:583-715)
+//   k_ter_base_state  calc_rho_p + erf_enforce_hse per column
+//   k_ter_step_begin  old-state boundary round trip, w from Omega = 0 at the
+//                     ground and the lid, cons_to_prim, eddy viscosity
+//   k_ter_strain /    make_tau_terms with terrain (ERF_make_tau_terms.cpp:
+//   k_ter_stress      177-317, ComputeStrain_T, ComputeStressVarVisc_T)
+//   k_ter_slow_cell   rho / rho*theta slow RHS with face areas and detJ
+//   k_ter_slow_mom    AdvectionSrcForMom_T, DiffusionSrcForMom_T, terrain
+//                     pressure gradient, sources
+//   k_ter_fast_h /    erf_fast_rhs_T (TimeIntegration/ERF_fast_rhs_T.cpp)
+//   k_ter_fast_vert
+//   k_ter_post        erf_slow_rhs_post with terrain and the stage's
+//                     boundary round trips
+#include "kernels.cuh"
+
+namespace erfb {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Metric terms (Utils/ERF_TerrainMetrics.H:33-395), same operand order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double Zn(const Params& P, int i, int j, int k) {
+    const Geo& g = P.g;
+    return __ldg(P.znd + (int64_t)(k + 1) * g.sk + (int64_t)wrap(j, g.ny) * g.nx + wrap(i, g.nx));
+}
+#define ZN(a, b, c) Zn(P, a, b, c)
+__device__ __forceinline__ double detJ_at(const Params& P, int i, int j, int k) {
+    const Geo& g = P.g;
+    return __ldg(P.detJ + cidx(g, wrap(i, g.nx), wrap(j, g.ny), clampk(k, g.nz)));
+}
+__device__ double hzeta_cc(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dzi * (ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k + 1) + ZN(i, j, k + 1) + ZN(i, j + 1, k + 1)
+                             - ZN(i + 1, j, k) - ZN(i + 1, j + 1, k) - ZN(i, j, k) - ZN(i, j + 1, k));
+}
+__device__ double hxi_cc(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j + 1, k) + ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k + 1)
+                             - ZN(i, j, k) - ZN(i, j + 1, k) - ZN(i, j, k + 1) - ZN(i, j + 1, k + 1));
+}
+__device__ double heta_cc(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i + 1, j + 1, k) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k + 1)
+                             - ZN(i, j, k) - ZN(i + 1, j, k) - ZN(i, j, k + 1) - ZN(i + 1, j, k + 1));
+}
+// x faces (also ax) and y faces (also ay)
+__device__ double hzeta_I(const Params& P, int i, int j, int k) {
+    return 0.5 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i, j + 1, k + 1) - ZN(i, j, k) - ZN(i, j + 1, k));
+}
+__device__ double hxi_I(const Params& P, int i, int j, int k) {
+    return 0.125 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k) + ZN(i + 1, j + 1, k + 1)
+                              - ZN(i - 1, j, k) - ZN(i - 1, j, k + 1) - ZN(i - 1, j + 1, k) - ZN(i - 1, j + 1, k + 1));
+}
+__device__ double hzeta_J(const Params& P, int i, int j, int k) {
+    return 0.5 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) - ZN(i, j, k) - ZN(i + 1, j, k));
+}
+__device__ double heta_J(const Params& P, int i, int j, int k) {
+    return 0.125 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k) + ZN(i + 1, j + 1, k + 1)
+                              - ZN(i, j - 1, k) - ZN(i, j - 1, k + 1) - ZN(i + 1, j - 1, k) - ZN(i + 1, j - 1, k + 1));
+}
+// z faces
+__device__ double hzeta_K(const Params& P, int i, int j, int k) {
+    return 0.125 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k + 1)
+                              - ZN(i, j, k - 1) - ZN(i + 1, j, k - 1) - ZN(i, j + 1, k - 1) - ZN(i + 1, j + 1, k - 1));
+}
+__device__ double hxi_K(const Params& P, int i, int j, int k) {
+    return 0.5 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j + 1, k) - ZN(i, j, k) - ZN(i, j + 1, k));
+}
+__device__ double heta_K(const Params& P, int i, int j, int k) {
+    return 0.5 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i + 1, j + 1, k) - ZN(i, j, k) - ZN(i + 1, j, k));
+}
+// xy edges (EdgeCenterK), xz edges (EdgeCenterJ), yz edges (EdgeCenterI)
+__device__ double hzeta_EK(const Params& P, int i, int j, int k) { return P.g.dzi * (ZN(i, j, k + 1) - ZN(i, j, k)); }
+__device__ double hxi_EK(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j, k + 1) - ZN(i - 1, j, k) - ZN(i - 1, j, k + 1));
+}
+__device__ double heta_EK(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i, j + 1, k + 1) - ZN(i, j - 1, k) - ZN(i, j - 1, k + 1));
+}
+__device__ double hzeta_EJ(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i, j + 1, k + 1) - ZN(i, j, k - 1) - ZN(i, j + 1, k - 1));
+}
+__device__ double hxi_EJ(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dxi * (ZN(i + 1, j + 1, k) + ZN(i + 1, j, k) - ZN(i - 1, j + 1, k) - ZN(i - 1, j, k));
+}
+__device__ double heta_EJ(const Params& P, int i, int j, int k) { return P.g.dyi * (ZN(i, j + 1, k) - ZN(i, j, k)); }
+__device__ double hzeta_EI(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) - ZN(i, j, k - 1) - ZN(i + 1, j, k - 1));
+}
+__device__ double hxi_EI(const Params& P, int i, int j, int k) { return P.g.dxi * (ZN(i + 1, j, k) - ZN(i, j, k)); }
+__device__ double heta_EI(const Params& P, int i, int j, int k) {
+    return 0.25 * P.g.dyi * (ZN(i + 1, j + 1, k) + ZN(i, j + 1, k) - ZN(i + 1, j - 1, k) - ZN(i, j - 1, k));
+}
+// slopes of a z-face (OmegaFromW / WFromOmega, ERF_TerrainMetrics.H:455-520)
+__device__ double zlo_xi(const Params& P, int i, int j, int k) {
+    return 0.5 * P.g.dxi * (ZN(i + 1, j + 1, k) + ZN(i + 1, j, k) - ZN(i, j + 1, k) - ZN(i, j, k));
+}
+__device__ double zlo_eta(const Params& P, int i, int j, int k) {
+    return 0.5 * P.g.dyi * (ZN(i + 1, j + 1, k) + ZN(i, j + 1, k) - ZN(i + 1, j, k) - ZN(i, j, k));
+}
+#undef ZN
+
+// Face-averaged horizontal components at z-face (i,j,k) of x/y-face arrays
+// given as accessors (extrapolated to the bottom face).
+template <class FU, class FV>
+__device__ __forceinline__ void zface_uv(int i, int j, int k, FU ua, FV va, double& u, double& v) {
+    if (k == 0) {
+        u = 1.5 * (0.5 * (ua(i, j, k) + ua(i + 1, j, k))) - 0.5 * (0.5 * (ua(i, j, k + 1) + ua(i + 1, j, k + 1)));
+        v = 1.5 * (0.5 * (va(i, j, k) + va(i, j + 1, k))) - 0.5 * (0.5 * (va(i, j, k + 1) + va(i, j + 1, k + 1)));
+    } else {
+        u = 0.25 * (ua(i, j, k - 1) + ua(i + 1, j, k - 1) + ua(i, j, k) + ua(i + 1, j, k));
+        v = 0.25 * (va(i, j, k - 1) + va(i, j + 1, k - 1) + va(i, j, k) + va(i, j + 1, k));
+    }
+}
+template <class FU, class FV>
+__device__ __forceinline__ double omega_from_w(const Params& P, int i, int j, int k, double w, FU ua, FV va) {
+    double mx = zlo_xi(P, i, j, k), my = zlo_eta(P, i, j, k), u, v;
+    zface_uv(i, j, k, ua, va, u, v);
+    return w - mx * u - my * v;
+}
+template <class FU, class FV>
+__device__ __forceinline__ double w_from_omega(const Params& P, int i, int j, int k, double om, FU ua, FV va) {
+    double mx = zlo_xi(P, i, j, k), my = zlo_eta(P, i, j, k), u, v;
+    zface_uv(i, j, k, ua, va, u, v);
+    return om + mx * u + my * v;
+}
+
+// Base state at (i,j,k), k in [-1, nz].
+__device__ __forceinline__ double bs(const double* f, const Geo& g, int i, int j, int k) {
+    return __ldg(f + (int64_t)(k + 1) * g.sk + (int64_t)j * g.nx + i);
+}
+
+// Horizontal momentum after the M -> V -> M round trip of a boundary fill
+// (face (i,j,k) wrapped laterally, k in [0, nz)) and the velocity it gives.
+__device__ __forceinline__ double rt_u(const Geo& g, const double* cons, const double* mx, int i, int j, int k) {
+    i = wrap(i, g.nx); j = wrap(j, g.ny);
+    double rs = cons[cidx(g, i, j, k)] + cons[cidx(g, wrap(i - 1, g.nx), j, k)];
+    return (mx[cidx(g, i, j, k)] * 2.0) / rs;
+}
+__device__ __forceinline__ double rt_v(const Geo& g, const double* cons, const double* my, int i, int j, int k) {
+    i = wrap(i, g.nx); j = wrap(j, g.ny);
+    double rs = cons[cidx(g, i, j, k)] + cons[cidx(g, i, wrap(j - 1, g.ny), k)];
+    return (my[cidx(g, i, j, k)] * 2.0) / rs;
+}
+
+// Tangential velocity with its wall ghost (ext_dir 0 or foextrap), lateral
+// indices wrapped here.
+__device__ __forceinline__ double tvel(const double* f, const Geo& g, int i, int j, int k) {
+    i = wrap(i, g.nx); j = wrap(j, g.ny);
+    if (k < 0) return g.zlo_noslip ? 0.0 : __ldg(f + cidx(g, i, j, 0));
+    if (k >= g.nz) return g.zhi_noslip ? 0.0 : __ldg(f + cidx(g, i, j, g.nz - 1));
+    return __ldg(f + cidx(g, i, j, k));
+}
+// w at z-face k in [0, nz], lateral wrap
+__device__ __forceinline__ double wvel(const double* f, const Geo& g, int i, int j, int k) {
+    i = wrap(i, g.nx); j = wrap(j, g.ny);
+    k = k < 0 ? 0 : (k > g.nz ? g.nz : k);
+    return __ldg(f + cidx(g, i, j, k));
+}
+// cell-centred value with lateral wrap and foextrap in z
+template <class V>
+__device__ __forceinline__ double ccw(const V* f, const Geo& g, int i, int j, int k) {
+    return double(__ldg(f + cidx(g, wrap(i, g.nx), wrap(j, g.ny), clampk(k, g.nz))));
+}
+
+__device__ __forceinline__ bool cell_ij(const Geo& g, int& i, int& j, int& k) {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y * blockDim.y + threadIdx.y;
+    k = blockIdx.z;
+    return i < g.nx && j < g.ny && k < g.nz;
+}
+dim3 ter_block() { return dim3(32, 4, 1); }
+dim3 ter_grid(const Geo& g, int nk) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, nk); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Metrics: detJ per cell and z at cell centres (levels 0..nz, the top one
+// from the extrapolated node level).
+// ---------------------------------------------------------------------------
+__global__ void k_ter_metrics(Params P, double* __restrict__ detJ, double* __restrict__ zcc) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    auto Z = [&](int a, int b, int c) { return Zn(P, a, b, c); };
+    if (k < g.nz)
+        detJ[cidx(g, i, j, k)] = .25 * g.dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1)
+                                                - Z(i, j, k) - Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
+    zcc[cidx(g, i, j, k)] = .125 * (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k)
+                                    + Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1));
+}
+void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* zcc) {
+    k_ter_metrics<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, detJ, zcc);
+}
+
+// ---------------------------------------------------------------------------
+// Base state over the terrain, one thread per column: calc_rho_p Newton
+// integration from p_sfc at z = 0 through the column's cell centres
+// (ERF_InputSoundingData.H:176-256), then erf_enforce_hse with terrain
+// (ERF_init1d.cpp:152-241).  Output (nz+2) planes, plane k+1 for level k.
+// ---------------------------------------------------------------------------
+__global__ void k_ter_base_state(Params P, const double* __restrict__ zcc, const double* __restrict__ th3,
+                                 const double* __restrict__ qv3, double th_s, double qv_s, double p_s,
+                                 double* __restrict__ rho0, double* __restrict__ p0o, double* __restrict__ pi0o,
+                                 double* __restrict__ th0o) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const double tol = 1.0e-12, grav = P.gravity, rdOcp = P.rdOcp;
+    const double RdOCp = R_d / Cp_d;
+    const int64_t col = (int64_t)j * g.nx + i, sk = g.sk;
+    const int nz = g.nz;
+    double pm = p_s;
+    double rd = eos_rho_given_theta_p(th_s, p_s, RdOCp, qv_s);
+    double zprev = 0.0, qprev = qv_s;
+    for (int k = 1; k <= nz; ++k) {
+        int64_t c = (int64_t)(k - 1) * sk + col;
+        double z = zcc[c];
+        double th = th3[c], qv = qv3[c];
+        double dzl = z - zprev;
+        double rlo = rd * (1. + qprev);
+        double C = -pm + 0.5 * rlo * grav * dzl;
+        double pk = pm;
+        double rk = eos_rho_given_theta_p(th, pk, RdOCp, qv);
+        double rhi = rk * (1. + qv);
+        double F = pk + 0.5 * rhi * grav * dzl + C;
+        if (fabs(F) > tol) {
+            int iter = 0;
+            double eps = 1.0e-6, ieps = 1.0e6;
+            do {
+                double hi = eos_rho_given_theta_p(th, pk + eps, RdOCp, qv);
+                double lo = eos_rho_given_theta_p(th, pk - eps, RdOCp, qv);
+                double dFdp = 1.0 + 0.25 * ieps * (hi - lo) * grav * dzl;
+                pk -= F / dFdp;
+                rk = eos_rho_given_theta_p(th, pk, RdOCp, qv);
+                double rt = rk * (1. + qv);
+                F = pk + 0.5 * rt * grav * dzl + C;
+                ++iter;
+            } while (fabs(F) > tol && iter < 30);
+        }
+        rho0[(int64_t)k * sk + col] = rk;
+        pm = pk; rd = rk; zprev = z; qprev = qv;
+    }
+    rho0[col] = rho0[sk + col];
+    rho0[(int64_t)(nz + 1) * sk + col] = rho0[(int64_t)nz * sk + col];
+    auto put = [&](int kk, double pv) {
+        int64_t o = (int64_t)kk * sk + col;
+        p0o[o] = pv;
+        pi0o[o] = eos_exner_p(pv, rdOcp);
+        th0o[o] = eos_rt_given_p(pv) / rho0[o];
+    };
+    double hz = zcc[col];
+    double r1 = rho0[sk + col];
+    double pprev = p_0 - hz * r1 * grav;
+    put(1, pprev);
+    put(0, p_0 + hz * r1 * grav);
+    for (int k = 1; k <= nz; ++k) {
+        int kk = k + 1;
+        double dz_loc = zcc[(int64_t)k * sk + col] - zcc[(int64_t)(k - 1) * sk + col];
+        double di = 0.5 * (rho0[(int64_t)kk * sk + col] + rho0[(int64_t)(kk - 1) * sk + col]);
+        pprev = pprev - dz_loc * di * grav;
+        put(kk, pprev);
+    }
+}
+void launch_ter_base_state(const Params& P, cudaStream_t st, const double* zcc, const double* th3, const double* qv3,
+                           double th_s, double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0) {
+    dim3 b(32, 4, 1), gr((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1);
+    k_ter_base_state<<<gr, b, 0, st>>>(P, zcc, th3, qv3, th_s, qv_s, p_s, rho0, p0, pi0, th0);
+}
+
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Strain rates with terrain (ComputeStrain_T, Diffusion/ERF_ComputeStrain_T.cpp:
+// 268-505) at one cell / edge, for velocity accessors U(i,j,k), V, W that
+// supply the wall ghosts.  k ranges: cells [0,nz), xy edges [0,nz), xz / yz
+// edges [0,nz].
+// ---------------------------------------------------------------------------
+template <class FU, class FV, class FW>
+__device__ void strain_cc_T(const Params& P, int i, int j, int k, FU U, FV V, FW W, double& s11, double& s22,
+                            double& s33) {
+    const double dxi = P.g.dxi, dyi = P.g.dyi, dzi = P.g.dzi;
+    double GradUz, GradVz;
+    if (k == 0 && P.g.zlo_noslip) {
+        GradUz = 0.5 * dzi * ((-(8. / 3.) * U(i, j, k - 1) + 3. * U(i, j, k) - (1. / 3.) * U(i, j, k + 1))
+                              + (-(8. / 3.) * U(i - 1, j, k - 1) + 3. * U(i - 1, j, k) - (1. / 3.) * U(i - 1, j, k + 1)));
+        GradVz = 0.5 * dzi * ((-(8. / 3.) * V(i, j, k - 1) + 3. * V(i, j, k) - (1. / 3.) * V(i, j, k + 1))
+                              + (-(8. / 3.) * V(i, j - 1, k - 1) + 3. * V(i, j - 1, k) - (1. / 3.) * V(i, j - 1, k + 1)));
+    } else {
+        GradUz = 0.25 * dzi * (U(i, j, k + 1) / 1.0 + U(i - 1, j, k + 1) / 1.0 - U(i, j, k - 1) / 1.0 - U(i - 1, j, k - 1) / 1.0);
+        GradVz = 0.25 * dzi * (V(i, j, k + 1) / 1.0 + V(i, j - 1, k + 1) / 1.0 - V(i, j, k - 1) / 1.0 - V(i, j - 1, k - 1) / 1.0);
+    }
+    double mxi = hxi_cc(P, i, j, k), meta = heta_cc(P, i, j, k), mz = detJ_at(P, i, j, k);
+    s11 = ((U(i + 1, j, k) / 1.0 - U(i, j, k) / 1.0) * dxi - (mxi / mz) * GradUz) * 1.0 * 1.0;
+    s22 = ((V(i, j + 1, k) / 1.0 - V(i, j, k) / 1.0) * dyi - (meta / mz) * GradVz) * 1.0 * 1.0;
+    s33 = (W(i, j, k + 1) - W(i, j, k)) * dzi / mz;
+}
+template <class FU, class FV>
+__device__ double strain12_T(const Params& P, int i, int j, int k, FU U, FV V) {
+    const double dxi = P.g.dxi, dyi = P.g.dyi, dzi = P.g.dzi;
+    double GradUz, GradVz;
+    if (k == 0 && P.g.zlo_noslip) {
+        GradUz = 0.5 * dzi * ((-(8. / 3.) * U(i, j, k - 1) + 3. * U(i, j, k) - (1. / 3.) * U(i, j, k + 1))
+                              + (-(8. / 3.) * U(i, j - 1, k - 1) + 3. * U(i, j - 1, k) - (1. / 3.) * U(i, j - 1, k + 1)));
+        GradVz = 0.5 * dzi * ((-(8. / 3.) * V(i, j, k - 1) + 3. * V(i, j, k) - (1. / 3.) * V(i, j, k + 1))
+                              + (-(8. / 3.) * V(i - 1, j, k - 1) + 3. * V(i - 1, j, k) - (1. / 3.) * V(i - 1, j, k + 1)));
+    } else {
+        GradUz = 0.25 * dzi * (U(i, j, k + 1) / 1.0 + U(i, j - 1, k + 1) / 1.0 - U(i, j, k - 1) / 1.0 - U(i, j - 1, k - 1) / 1.0);
+        GradVz = 0.25 * dzi * (V(i, j, k + 1) / 1.0 + V(i - 1, j, k + 1) / 1.0 - V(i, j, k - 1) / 1.0 - V(i - 1, j, k - 1) / 1.0);
+    }
+    double mxi = hxi_EK(P, i, j, k), meta = heta_EK(P, i, j, k), mz = hzeta_EK(P, i, j, k);
+    return 0.5 * ((U(i, j, k) / 1.0 - U(i, j - 1, k) / 1.0) * dyi + (V(i, j, k) / 1.0 - V(i - 1, j, k) / 1.0) * dxi
+                  - (meta / mz) * GradUz - (mxi / mz) * GradVz) * 1.0 * 1.0;
+}
+template <class FU, class FW>
+__device__ double strain13_T(const Params& P, int i, int j, int k, FU U, FW W) {
+    const double dxi = P.g.dxi, dzi = P.g.dzi;
+    const int nz = P.g.nz;
+    double mz = hzeta_EJ(P, i, j, k);
+    if (k == 0) {
+        double GradWz = 0.5 * dzi * (W(i, j, k + 1) + W(i - 1, j, k + 1) - W(i, j, k) - W(i - 1, j, k));
+        double mxi = hxi_EJ(P, i, j, k);
+        if (P.g.zlo_noslip)
+            return 0.5 * ((-(8. / 3.) * U(i, j, k - 1) + 3. * U(i, j, k) - (1. / 3.) * U(i, j, k + 1)) * dzi / mz
+                          + ((W(i, j, k) - W(i - 1, j, k)) * dxi - (mxi / mz) * GradWz) * 1.0);
+        return 0.5 * ((U(i, j, k) - U(i, j, k - 1)) * dzi / mz + ((W(i, j, k) - W(i - 1, j, k)) * dxi - (mxi / mz) * GradWz) * 1.0);
+    }
+    if (k == nz) {
+        if (P.g.zhi_noslip)
+            return 0.5 * (-(-(8. / 3.) * U(i, j, k) + 3. * U(i, j, k - 1) - (1. / 3.) * U(i, j, k - 2)) * dzi / mz
+                          + (W(i, j, k) - W(i - 1, j, k)) * dxi * 1.0);
+        return 0.5 * ((U(i, j, k) - U(i, j, k - 1)) * dzi / mz + (W(i, j, k) - W(i - 1, j, k)) * dxi * 1.0);
+    }
+    double GradWz = 0.25 * dzi * (W(i, j, k + 1) + W(i - 1, j, k + 1) - W(i, j, k - 1) - W(i - 1, j, k - 1));
+    double mxi = hxi_EJ(P, i, j, k);
+    return 0.5 * ((U(i, j, k) - U(i, j, k - 1)) * dzi / mz + ((W(i, j, k) - W(i - 1, j, k)) * dxi - (mxi / mz) * GradWz) * 1.0);
+}
+template <class FV, class FW>
+__device__ double strain23_T(const Params& P, int i, int j, int k, FV V, FW W) {
+    const double dyi = P.g.dyi, dzi = P.g.dzi;
+    const int nz = P.g.nz;
+    double mz = hzeta_EI(P, i, j, k);
+    if (k == 0) {
+        double GradWz = 0.5 * dzi * (W(i, j, k + 1) + W(i, j - 1, k + 1) - W(i, j, k) - W(i, j - 1, k));
+        double meta = heta_EI(P, i, j, k);
+        if (P.g.zlo_noslip)
+            return 0.5 * ((-(8. / 3.) * V(i, j, k - 1) + 3. * V(i, j, k) - (1. / 3.) * V(i, j, k + 1)) * dzi / mz
+                          + ((W(i, j, k) - W(i, j - 1, k)) * dyi - (meta / mz) * GradWz) * 1.0);
+        return 0.5 * ((V(i, j, k) - V(i, j, k - 1)) * dzi / mz + ((W(i, j, k) - W(i, j - 1, k)) * dyi - (meta / mz) * GradWz) * 1.0);
+    }
+    if (k == nz) {
+        if (P.g.zhi_noslip)
+            return 0.5 * (-(-(8. / 3.) * V(i, j, k) + 3. * V(i, j, k - 1) - (1. / 3.) * V(i, j, k - 2)) * dzi / mz
+                          + (W(i, j, k) - W(i, j - 1, k)) * dyi * 1.0);
+        return 0.5 * ((V(i, j, k) - V(i, j, k - 1)) * dzi / mz + (W(i, j, k) - W(i, j - 1, k)) * dyi * 1.0);
+    }
+    double GradWz = 0.25 * dzi * (W(i, j, k + 1) + W(i, j - 1, k + 1) - W(i, j, k - 1) - W(i, j - 1, k - 1));
+    double meta = heta_EI(P, i, j, k);
+    return 0.5 * ((V(i, j, k) - V(i, j, k - 1)) * dzi / mz + ((W(i, j, k) - W(i, j - 1, k)) * dyi - (meta / mz) * GradWz) * 1.0);
+}
+// ComputeSmnSmn (Diffusion/ERF_EddyViscosity.H:31-83) from the terrain strains
+template <class FU, class FV, class FW>
+__device__ double smnsmn_T(const Params& P, int i, int j, int k, FU U, FV V, FW W) {
+    double s11, s22, s33;
+    strain_cc_T(P, i, j, k, U, V, W, s11, s22, s33);
+    double s12 = 0.25 * (strain12_T(P, i, j, k, U, V) + strain12_T(P, i, j + 1, k, U, V) + strain12_T(P, i + 1, j, k, U, V)
+                         + strain12_T(P, i + 1, j + 1, k, U, V));
+    double s13 = 0.25 * (strain13_T(P, i, j, k, U, W) + strain13_T(P, i, j, k + 1, U, W) + strain13_T(P, i + 1, j, k, U, W)
+                         + strain13_T(P, i + 1, j, k + 1, U, W));
+    double s23 = 0.25 * (strain23_T(P, i, j, k, V, W) + strain23_T(P, i, j, k + 1, V, W) + strain23_T(P, i, j + 1, k, V, W)
+                         + strain23_T(P, i, j + 1, k + 1, V, W));
+    return s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + 2.0 * s23 * s23;
+}
+
+// Base-state pressure at the cell of linear index c (level k) with terrain.
+__device__ __forceinline__ double p0_at(const Params& P, int64_t c, int k) {
+    return P.ter ? P.p0[c + P.g.sk] : P.p0[k + 1];
+}
+template <class R>
+__device__ __forceinline__ void stage_aux_ter(const Params& P, const double* __restrict__ cons, StageAux<R> A,
+                                              int64_t c, int k) {
+    const int64_t N = P.g.ncell;
+    double rho = cons[c];
+    double rt = cons[N + c];
+    A.prim[c] = R(rt / rho);
+    for (int n = 1; n < P.nprim; ++n) A.prim[n * N + c] = R(cons[(n + 1) * N + c] / rho);
+    A.pi[c] = R(eos_exner(rt, P.rdOcp));
+    double qv = P.moist ? cons[5 * N + c] / rho : 0.0;
+    A.pp[c] = R(eos_p(rt, qv) - p0_at(P, c, k));
+    if (!(rt > 0.0) || !(rho > 0.0)) atomicOr(P.status, ST_BADSTATE);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Step prologue with terrain.  The old velocities give the momenta through
+// the V -> M -> V -> M round trip of apply_bcs(state_old) (as without
+// terrain); w on the ground and on the lid is WFromOmega(Omega = 0) of the
+// round-tripped u, v (ERF_BoundaryConditions_zvel.cpp:200-262).  The eddy
+// viscosity uses the input velocities with w from the same condition, the
+// terrain strain and a local filter width (dz / h_zeta;
+// ERF_ComputeTurbulentViscosity.cpp:85-229).
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_step_begin(Params P, const double* __restrict__ cons, const double* __restrict__ uo,
+                                 const double* __restrict__ vo, const double* __restrict__ wo, StateBuf S,
+                                 double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn,
+                                 StageAux<R> A, R* __restrict__ mut, TkeBuf<R> tke) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
+    int64_t c = cidx(g, i, j, k);
+    double rho = cons[c];
+    // round-tripped old velocity at a face (the value apply_bcs leaves), with
+    // the wall ghost
+    auto urt = [&](int ii, int jj, int kk) {
+        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+        int kc = clampk(kk, nz);
+        if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
+        double rs = cons[cidx(g, ii, jj, kc)] + cons[cidx(g, wrap(ii - 1, g.nx), jj, kc)];
+        double m0 = (uo[cidx(g, ii, jj, kc)] * 0.5) * rs;
+        return (m0 * 2.0) / rs;
+    };
+    auto vrt = [&](int ii, int jj, int kk) {
+        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+        int kc = clampk(kk, nz);
+        if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
+        double rs = cons[cidx(g, ii, jj, kc)] + cons[cidx(g, ii, wrap(jj - 1, g.ny), kc)];
+        double m0 = (vo[cidx(g, ii, jj, kc)] * 0.5) * rs;
+        return (m0 * 2.0) / rs;
+    };
+    {
+        double rs = rho + cons[cidx(g, im, j, k)];
+        double m0 = (uo[c] * 0.5) * rs, u1 = (m0 * 2.0) / rs;
+        S.mx[c] = (u1 * 0.5) * rs; un[c] = u1;
+    }
+    {
+        double rs = rho + cons[cidx(g, i, jm, k)];
+        double m0 = (vo[c] * 0.5) * rs, v1 = (m0 * 2.0) / rs;
+        S.my[c] = (v1 * 0.5) * rs; vn[c] = v1;
+    }
+    if (k == 0) {
+        double wb = w_from_omega(P, i, j, 0, 0.0, urt, vrt);
+        S.mz[c] = (wb * 0.5) * (rho + rho); wn[c] = wb;
+    } else {
+        double rs = rho + cons[c - g.sk];
+        double m0 = (wo[c] * 0.5) * rs, w1 = (m0 * 2.0) / rs;
+        S.mz[c] = (w1 * 0.5) * rs; wn[c] = w1;
+    }
+    if (k == nz - 1) {
+        double wt = w_from_omega(P, i, j, nz, 0.0, urt, vrt);
+        S.mz[c + g.sk] = (wt * 0.5) * (rho + rho); wn[c + g.sk] = wt;
+    }
+    stage_aux_ter<R>(P, cons, A, c, k);
+
+    if (P.les == ERF_LES_NONE) return;
+    // input velocities with their wall ghosts; w on the walls from Omega = 0
+    auto U = [&](int ii, int jj, int kk) { return tvel(uo, g, ii, jj, kk); };
+    auto V = [&](int ii, int jj, int kk) { return tvel(vo, g, ii, jj, kk); };
+    auto W = [&](int ii, int jj, int kk) {
+        if (kk <= 0 || kk >= nz) return w_from_omega(P, ii, jj, kk <= 0 ? 0 : nz, 0.0, U, V);
+        return wvel(wo, g, ii, jj, kk);
+    };
+    double dzInv = g.dzi / hzeta_cc(P, i, j, k);
+    double cellVolMsf = 1.0 / (g.dxi * 1.0 * g.dyi * 1.0 * dzInv);
+    double DeltaMsf = pow(cellVolMsf, 1.0 / 3.0);
+    if (P.les == ERF_LES_SMAGORINSKY) {
+        double S2 = smnsmn_T(P, i, j, k, U, V, W);
+        double CsDeltaSqrMsf = P.Cs * P.Cs * DeltaMsf * DeltaMsf;
+        mut[c] = R(CsDeltaSqrMsf * rho * sqrt(2.0 * S2));
+    } else if (P.les == ERF_LES_DEARDORFF) {
+        const int64_t N = g.ncell;
+        const int kp = min(k + 1, nz - 1), km = max(k - 1, 0);
+        double dtheta_dz = 0.5 * (cons[N + cidx(g, i, j, kp)] / cons[cidx(g, i, j, kp)] -
+                                  cons[N + cidx(g, i, j, km)] / cons[cidx(g, i, j, km)]) * dzInv;
+        double E = fmax(cons[2 * N + c] / rho, 0.0);
+        double strat = P.g_over_theta0 * dtheta_dz;
+        double length;
+        if (strat <= 2.220446049250313e-16) {
+            length = DeltaMsf;
+        } else {
+            length = 0.76 * sqrt(E / strat);
+            length = fmin(length, DeltaMsf);
+            length = fmax(length, 0.001 * DeltaMsf);
+        }
+        double K = rho * P.Ck * length * sqrt(E);
+        mut[c] = R(K);
+        tke.kthv[c] = R((1. + 2. * length / DeltaMsf) * K);
+        double Ce = ((P.Ce_wall > 0) && (k == 0)) ? P.Ce_wall : 1.9 * P.Ck + P.Ce_lcoeff * length / DeltaMsf;
+        tke.diss[c] = R(rho * Ce * (E * sqrt(E)) / length);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// make_tau_terms with terrain, pass 1: strain rates of the stage velocities,
+// tau_ii less a third of the expansion rate (from the contravariant
+// velocity, ERF_make_tau_terms.cpp:185-216), S12 / S13 / S23 on the edges,
+// and SmnSmn of the first stage for the Deardorff shear production.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_strain(Params P, int nrk, const double* __restrict__ u, const double* __restrict__ v,
+                             const double* __restrict__ w, TerBuf<R> T, TkeBuf<R> tke) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    int64_t c = cidx(g, i, j, k);
+    auto U = [&](int ii, int jj, int kk) { return tvel(u, g, ii, jj, kk); };
+    auto V = [&](int ii, int jj, int kk) { return tvel(v, g, ii, jj, kk); };
+    auto W = [&](int ii, int jj, int kk) { return wvel(w, g, ii, jj, kk); };
+    auto om = [&](int kk) { return (kk == 0) ? 0. : omega_from_w(P, i, j, kk, W(i, j, kk), U, V); };
+    double mhi = hzeta_I(P, i + 1, j, k), mlo = hzeta_I(P, i, j, k);
+    double nhi = hzeta_J(P, i, j + 1, k), nlo = hzeta_J(P, i, j, k);
+    double rate = (U(i + 1, j, k) / 1.0 * mhi - U(i, j, k) / 1.0 * mlo) * g.dxi * 1.0
+                  + (V(i, j + 1, k) / 1.0 * nhi - V(i, j, k) / 1.0 * nlo) * g.dyi * 1.0
+                  + (om(k + 1) - om(k)) * g.dzi;
+    double er = rate / detJ_at(P, i, j, k);
+    double s11, s22, s33;
+    strain_cc_T(P, i, j, k, U, V, W, s11, s22, s33);
+    const double OneThird = (1. / 3.);
+    T.s11[c] = R(s11 - OneThird * er);
+    T.s22[c] = R(s22 - OneThird * er);
+    T.s33[c] = R(s33 - OneThird * er);
+    T.s12[c] = R(strain12_T(P, i, j, k, U, V));
+    T.s13[c] = R(strain13_T(P, i, j, k, U, W));
+    T.s23[c] = R(strain23_T(P, i, j, k, V, W));
+    if (k == nz - 1) {
+        T.s13[c + g.sk] = R(strain13_T(P, i, j, nz, U, W));
+        T.s23[c + g.sk] = R(strain23_T(P, i, j, nz, V, W));
+    }
+    if (P.les == ERF_LES_DEARDORFF && nrk == 0) tke.smn[c] = R(smnsmn_T(P, i, j, k, U, V, W));
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: ComputeStressVarVisc_T (Diffusion/ERF_ComputeStress_T.cpp:302-577).
+// tau33 takes the raw S31 / S32 cross terms; tau13 / tau23 the tau11 / tau12
+// (tau21 / tau22) averages, linearly extrapolated to the bottom and top
+// faces; tau31 = -mu h_zeta S13, tau32 likewise; tau11, tau22 and tau12
+// (= tau21) carry h_zeta.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_stress(Params P, const double* __restrict__ cons, const R* __restrict__ mut, TerBuf<R> T,
+                             R* __restrict__ t11, R* __restrict__ t22, R* __restrict__ t33, R* __restrict__ t12,
+                             R* __restrict__ t13, R* __restrict__ t23) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    int64_t c = cidx(g, i, j, k);
+    const double mu_eff = P.mu_eff;
+    auto rA = [&](int ii, int jj, int kk) { return P.use_consA ? ccw(cons, g, ii, jj, kk) * mu_eff : mu_eff; };
+    auto mt = [&](int ii, int jj, int kk) { return P.use_turb ? ccw(mut, g, ii, jj, kk) : 0.0; };
+    auto S11 = [&](int ii, int jj, int kk) { return ccw(T.s11, g, ii, jj, kk); };
+    auto S22 = [&](int ii, int jj, int kk) { return ccw(T.s22, g, ii, jj, kk); };
+    auto E12 = [&](int ii, int jj, int kk) { return double(T.s12[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), clampk(kk, nz))]); };
+    auto E13 = [&](int ii, int jj, int kk) { return double(T.s13[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto E23 = [&](int ii, int jj, int kk) { return double(T.s23[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    {   // tau33
+        double mxi = hxi_cc(P, i, j, k), meta = heta_cc(P, i, j, k);
+        double t31b = 0.25 * (E13(i, j, k) + E13(i + 1, j, k) + E13(i, j, k + 1) + E13(i + 1, j, k + 1));
+        double t32b = 0.25 * (E23(i, j, k) + E23(i, j + 1, k) + E23(i, j, k + 1) + E23(i, j + 1, k + 1));
+        double mu_tot = rA(i, j, k) + 2.0 * mt(i, j, k);
+        double v33 = double(T.s33[c]);
+        v33 -= mxi * t31b + meta * t32b;
+        v33 *= -mu_tot;
+        t33[c] = R(v33);
+        double mz = detJ_at(P, i, j, k);
+        t11[c] = R(double(T.s11[c]) * (-mu_tot * mz));
+        t22[c] = R(double(T.s22[c]) * (-mu_tot * mz));
+    }
+    {   // tau12 (= tau21) on the xy edge (i,j,k)
+        double mz = hzeta_EK(P, i, j, k);
+        double mu_bar = 0.25 * (mt(i - 1, j, k) + mt(i, j, k) + mt(i - 1, j - 1, k) + mt(i, j - 1, k));
+        double ra_bar = 0.25 * (rA(i - 1, j, k) + rA(i, j, k) + rA(i - 1, j - 1, k) + rA(i, j - 1, k));
+        double mu_tot = ra_bar + 2.0 * mu_bar;
+        t12[c] = R(double(T.s12[c]) * (-mu_tot * mz));
+    }
+    for (int kk = k; kk <= (k == nz - 1 ? nz : k); ++kk) {
+        int64_t e = cidx(g, i, j, kk);
+        double t11b, t12b, t21b, t22b;
+        if (kk == 0) {
+            double a = 0.5 * (S11(i, j, kk) + S11(i - 1, j, kk)), b = 0.5 * (S11(i, j, kk + 1) + S11(i - 1, j, kk + 1));
+            t11b = 1.5 * a - 0.5 * b;
+            double c1 = 0.5 * (E12(i, j, kk) + E12(i, j + 1, kk)), d = 0.5 * (E12(i, j, kk + 1) + E12(i, j + 1, kk + 1));
+            t12b = 1.5 * c1 - 0.5 * d;
+            double a2 = 0.5 * (E12(i, j, kk) + E12(i + 1, j, kk)), b2 = 0.5 * (E12(i, j, kk + 1) + E12(i + 1, j, kk + 1));
+            t21b = 1.5 * a2 - 0.5 * b2;
+            double c2 = 0.5 * (S22(i, j, kk) + S22(i, j - 1, kk)), d2 = 0.5 * (S22(i, j, kk + 1) + S22(i, j - 1, kk + 1));
+            t22b = 1.5 * c2 - 0.5 * d2;
+        } else if (kk == nz) {
+            double lo = 0.5 * (S11(i, j, kk - 2) + S11(i - 1, j, kk - 2)), hi = 0.5 * (S11(i, j, kk - 1) + S11(i - 1, j, kk - 1));
+            t11b = 1.5 * hi - 0.5 * lo;
+            double lo2 = 0.5 * (E12(i, j, kk - 2) + E12(i, j + 1, kk - 2)), hi2 = 0.5 * (E12(i, j, kk - 1) + E12(i, j + 1, kk - 1));
+            t12b = 1.5 * hi2 - 0.5 * lo2;
+            double lo3 = 0.5 * (E12(i, j, kk - 2) + E12(i + 1, j, kk - 2)), hi3 = 0.5 * (E12(i, j, kk - 1) + E12(i + 1, j, kk - 1));
+            t21b = 1.5 * hi3 - 0.5 * lo3;
+            double lo4 = 0.5 * (S22(i, j, kk - 2) + S22(i, j - 1, kk - 2)), hi4 = 0.5 * (S22(i, j, kk - 1) + S22(i, j - 1, kk - 1));
+            t22b = 1.5 * hi4 - 0.5 * lo4;
+        } else {
+            t11b = 0.25 * (S11(i, j, kk) + S11(i - 1, j, kk) + S11(i, j, kk - 1) + S11(i - 1, j, kk - 1));
+            t12b = 0.25 * (E12(i, j, kk) + E12(i, j + 1, kk) + E12(i, j, kk - 1) + E12(i, j + 1, kk - 1));
+            t21b = 0.25 * (E12(i, j, kk) + E12(i + 1, j, kk) + E12(i, j, kk - 1) + E12(i + 1, j, kk - 1));
+            t22b = 0.25 * (S22(i, j, kk) + S22(i, j - 1, kk) + S22(i, j, kk - 1) + S22(i, j - 1, kk - 1));
+        }
+        {
+            double mxi = hxi_EJ(P, i, j, kk), meta = heta_EJ(P, i, j, kk), mz = hzeta_EJ(P, i, j, kk);
+            double mu_bar = 0.25 * (mt(i - 1, j, kk) + mt(i, j, kk) + mt(i - 1, j, kk - 1) + mt(i, j, kk - 1));
+            double ra_bar = 0.25 * (rA(i - 1, j, kk) + rA(i, j, kk) + rA(i - 1, j, kk - 1) + rA(i, j, kk - 1));
+            double mu_tot = ra_bar + 2.0 * mu_bar;
+            double s13 = double(T.s13[e]);
+            double v13 = s13;
+            v13 -= mxi * t11b + meta * t12b;
+            v13 *= -mu_tot;
+            t13[e] = R(v13);
+            T.t31[e] = R(s13 * (-mu_tot * mz));
+        }
+        {
+            double mxi = hxi_EI(P, i, j, kk), meta = heta_EI(P, i, j, kk), mz = hzeta_EI(P, i, j, kk);
+            double mu_bar = 0.25 * (mt(i, j - 1, kk) + mt(i, j, kk) + mt(i, j - 1, kk - 1) + mt(i, j, kk - 1));
+            double ra_bar = 0.25 * (rA(i, j - 1, kk) + rA(i, j, kk) + rA(i, j - 1, kk - 1) + rA(i, j, kk - 1));
+            double mu_tot = ra_bar + 2.0 * mu_bar;
+            double s23 = double(T.s23[e]);
+            double v23 = s23;
+            v23 -= mxi * t21b + meta * t22b;
+            v23 *= -mu_tot;
+            t23[e] = R(v23);
+            T.t32[e] = R(s23 * (-mu_tot * mz));
+        }
+    }
+}
+
+namespace {
+// Scalar diffusion with terrain (DiffusionSrcForState_T,
+// Diffusion/ERF_DiffusionSrcForState_T.cpp:207-738) for one primitive field:
+// metric-corrected x / y fluxes, z fluxes with the cross terms (extrapolated
+// at the bottom and top faces), x / y fluxes scaled by h_zeta, divergence
+// over detJ.  kv, when given, is the vertical diffusivity (Deardorff Theta_v).
+template <class R>
+struct DiffT {
+    const Params& P;
+    const double* rho;
+    const R* phi;
+    const R* mut;
+    const R* kv;
+    double ae, fac;
+    __device__ double p(int i, int j, int k) const { return ccw(phi, P.g, i, j, k); }
+    __device__ double mu(int i, int j, int k) const { return ccw(mut, P.g, i, j, k) * fac; }
+    __device__ double xraw(int i, int j, int k) const {
+        const Geo& g = P.g;
+        double rA = P.use_consA ? (0.5 * (ccw(rho, g, i, j, k) + ccw(rho, g, i - 1, j, k))) * ae : ae;
+        if (P.use_turb) rA += 0.5 * (mu(i, j, k) + mu(i - 1, j, k));
+        double mxi = hxi_I(P, i, j, k), mz = hzeta_I(P, i, j, k);
+        double GradCz = 0.25 * g.dzi * (p(i, j, k + 1) + p(i - 1, j, k + 1) - p(i, j, k - 1) - p(i - 1, j, k - 1));
+        double GradCx = g.dxi * (p(i, j, k) - p(i - 1, j, k));
+        return -rA * 1.0 * (GradCx - (mxi / mz) * GradCz);
+    }
+    __device__ double yraw(int i, int j, int k) const {
+        const Geo& g = P.g;
+        double rA = P.use_consA ? (0.5 * (ccw(rho, g, i, j, k) + ccw(rho, g, i, j - 1, k))) * ae : ae;
+        if (P.use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j - 1, k));
+        double meta = heta_J(P, i, j, k), mz = hzeta_J(P, i, j, k);
+        double GradCz = 0.25 * g.dzi * (p(i, j, k + 1) + p(i, j - 1, k + 1) - p(i, j, k - 1) - p(i, j - 1, k - 1));
+        double GradCy = g.dyi * (p(i, j, k) - p(i, j - 1, k));
+        return -rA * 1.0 * (GradCy - (meta / mz) * GradCz);
+    }
+    // z-face flux (k in [0, nz]); raw receives the flux before the cross terms
+    __device__ double zflux(int i, int j, int k, double& raw) const {
+        const Geo& g = P.g;
+        const int nz = g.nz;
+        double rA = P.use_consA ? (0.5 * (ccw(rho, g, i, j, k) + ccw(rho, g, i, j, k - 1))) * ae : ae;
+        if (P.use_turb) {
+            if (kv) rA += 0.5 * (ccw(kv, g, i, j, k) + ccw(kv, g, i, j, k - 1));
+            else rA += 0.5 * (mu(i, j, k) + mu(i, j, k - 1));
+        }
+        double GradCz = g.dzi * (p(i, j, k) - p(i, j, k - 1));
+        double fz = -rA * GradCz / 1.0;
+        raw = fz;
+        double mxi = hxi_K(P, i, j, k), meta = heta_K(P, i, j, k), xb, yb;
+        if (k == 0) {
+            double xlo = 0.5 * (xraw(i, j, k) + xraw(i + 1, j, k)), xhi = 0.5 * (xraw(i, j, k + 1) + xraw(i + 1, j, k + 1));
+            xb = 1.5 * xlo - 0.5 * xhi;
+            double ylo = 0.5 * (yraw(i, j, k) + yraw(i, j + 1, k)), yhi = 0.5 * (yraw(i, j, k + 1) + yraw(i, j + 1, k + 1));
+            yb = 1.5 * ylo - 0.5 * yhi;
+        } else if (k == nz) {
+            double xlo = 0.5 * (xraw(i, j, k - 2) + xraw(i + 1, j, k - 2)), xhi = 0.5 * (xraw(i, j, k - 1) + xraw(i + 1, j, k - 1));
+            xb = 1.5 * xhi - 0.5 * xlo;
+            double ylo = 0.5 * (yraw(i, j, k - 2) + yraw(i, j + 1, k - 2)), yhi = 0.5 * (yraw(i, j, k - 1) + yraw(i, j + 1, k - 1));
+            yb = 1.5 * yhi - 0.5 * ylo;
+        } else {
+            xb = 0.25 * (xraw(i, j, k) + xraw(i + 1, j, k) + xraw(i, j, k - 1) + xraw(i + 1, j, k - 1));
+            yb = 0.25 * (yraw(i, j, k) + yraw(i, j + 1, k) + yraw(i, j, k - 1) + yraw(i, j + 1, k - 1));
+        }
+        fz -= mxi * xb + meta * yb;
+        return fz;
+    }
+    // divergence over detJ (the amount the reference subtracts from the RHS)
+    __device__ double div(int i, int j, int k, double& raw_lo, double& raw_hi) const {
+        const Geo& g = P.g;
+        double fxl = xraw(i, j, k) * hzeta_I(P, i, j, k), fxh = xraw(i + 1, j, k) * hzeta_I(P, i + 1, j, k);
+        double fyl = yraw(i, j, k) * hzeta_J(P, i, j, k), fyh = yraw(i, j + 1, k) * hzeta_J(P, i, j + 1, k);
+        double fzl = zflux(i, j, k, raw_lo), fzh = zflux(i, j, k + 1, raw_hi);
+        double s = (fxh - fxl) * g.dxi * 1.0 + (fyh - fyl) * g.dyi * 1.0 + (fzh - fzl) * g.dzi;
+        return s / detJ_at(P, i, j, k);
+    }
+};
+
+// Contravariant momentum Omega at z-face (i,j,k) of a state whose face
+// velocities are u, v (for the momentum ghost above the lid):
+// 0 at the ground, OmegaFromW inside and at the lid (ERF_slow_rhs_pre.cpp:365-420).
+__device__ double omega_mom(const Params& P, StateBuf S, const double* u, const double* v, int i, int j, int k) {
+    const Geo& g = P.g;
+    if (k <= 0) return 0.;
+    auto MX = [&](int ii, int jj, int kk) {
+        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+        if (kk < g.nz) return S.mx[cidx(g, ii, jj, kk)];
+        // momentum ghost above the lid: V2M of the tangential ghost velocity
+        int kt = g.nz - 1;
+        double rs = S.cons[cidx(g, ii, jj, kt)] + S.cons[cidx(g, wrap(ii - 1, g.nx), jj, kt)];
+        return tvel(u, g, ii, jj, g.nz) * 0.5 * rs;
+    };
+    auto MY = [&](int ii, int jj, int kk) {
+        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+        if (kk < g.nz) return S.my[cidx(g, ii, jj, kk)];
+        int kt = g.nz - 1;
+        double rs = S.cons[cidx(g, ii, jj, kt)] + S.cons[cidx(g, ii, wrap(jj - 1, g.ny), kt)];
+        return tvel(v, g, ii, jj, g.nz) * 0.5 * rs;
+    };
+    double rw = S.mz[cidx(g, wrap(i, g.nx), wrap(j, g.ny), k)];
+    return omega_from_w(P, i, j, k, rw, MX, MY);
+}
+
+// Face interpolation of a cell field along x / y / z with run-time scheme
+// (the stencil's unused entries are zero); upw the advecting flux.
+template <class FP>
+__device__ double interp_dir(int dir, int i, int j, int k, FP phi, int type, double upw, double frac) {
+    double s[6];
+    const int w = stencil_width(type);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        int off = m - 3;
+        bool used = (off >= -w && off <= w - 1);
+        s[m] = used ? phi(i + (dir == 0 ? off : 0), j + (dir == 1 ? off : 0), k + (dir == 2 ? off : 0)) : 0.0;
+    }
+    return interp_rt<double>(type, s, upw, frac);
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Slow RHS of rho and rho*theta with terrain (ERF_slow_rhs_pre.cpp:365-500):
+// Omega, AdvectionSrcForRho with the face areas (ax = h_zeta at x faces,
+// ay likewise, az = 1) over detJ, the average momenta, theta advection with
+// the dycore scheme, DiffusionSrcForState_T and hfx_z.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
+                                const double* __restrict__ v, const R* __restrict__ mut, TkeBuf<R> tke,
+                                R* __restrict__ Fcons, R* __restrict__ avx, R* __restrict__ avy, R* __restrict__ avz) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    int64_t c = cidx(g, i, j, k);
+    auto fxm = [&](int ii, int jj, int kk) {   // ax * rho_u
+        return hzeta_I(P, ii, jj, kk) * S.mx[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)] / 1.0;
+    };
+    auto fym = [&](int ii, int jj, int kk) {
+        return hzeta_J(P, ii, jj, kk) * S.my[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)] / 1.0;
+    };
+    auto fzm = [&](int ii, int jj, int kk) { return 1.0 * omega_mom(P, S, u, v, ii, jj, kk) / 1.0; };
+    double fxl = fxm(i, j, k), fxh = fxm(i + 1, j, k), fyl = fym(i, j, k), fyh = fym(i, j + 1, k);
+    double fzl = fzm(i, j, k), fzh = fzm(i, j, k + 1);
+    avx[c] = R(fxl); avy[c] = R(fyl); avz[c] = R(fzl);
+    if (k == nz - 1) avz[c + g.sk] = R(fzh);
+    const double Jc = detJ_at(P, i, j, k);
+    double frho = -1.0 / Jc * ((fxh - fxl) * g.dxi + (fyh - fyl) * g.dyi + (fzh - fzl) * g.dzi);
+    // theta with the dycore scheme, advected by the average momenta
+    auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
+    const int ht = P.dyc_h, vt = P.dyc_v;
+    const double hf = P.f_dyc_h, vf = P.f_dyc_v;
+    double tx_l = fxl * interp_dir(0, i, j, k, th, ht, fxl, hf), tx_h = fxh * interp_dir(0, i + 1, j, k, th, ht, fxh, hf);
+    double ty_l = fyl * interp_dir(1, i, j, k, th, ht, fyl, hf), ty_h = fyh * interp_dir(1, i, j + 1, k, th, ht, fyh, hf);
+    double tz_l = fzl * interp_dir(2, i, j, k, th, vt, fzl, vf), tz_h = fzh * interp_dir(2, i, j, k + 1, th, vt, fzh, vf);
+    double invdetJ = 1. / Jc;
+    double frt = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
+    if (P.use_diff) {
+        const bool dd = P.les == ERF_LES_DEARDORFF;
+        DiffT<R> D{P, S.cons, A.prim, mut, dd ? tke.kthv : nullptr, P.alphaT_eff, P.invPr};
+        double rlo, rhi;
+        frt -= D.div(i, j, k, rlo, rhi);
+        if (dd) {
+            tke.hfz[c] = R(rlo);
+            if (k == nz - 1) tke.hfz[c + g.sk] = R(rhi);
+        }
+    }
+    Fcons[c] = R(frho);
+    Fcons[N + c] = R(frt);
+}
+
+// ---------------------------------------------------------------------------
+// Slow RHS of the momenta with terrain (ERF_slow_rhs_pre.cpp:556-744):
+// AdvectionSrcForMom (terrain; Centered_2nd inline or the
+// ERF_AdvectionSrcForMom_T.H templates), DiffusionSrcForMom_T, the pressure
+// gradient with the terrain correction, buoyancy about the 3-D base state,
+// Coriolis and geostrophic forcing.  One thread per cell handles the x, y
+// and (k >= 1) z faces at (i,j,k).  Omega is the stage's, left in avz by
+// k_ter_slow_cell.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_slow_mom(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
+                               const double* __restrict__ v, const double* __restrict__ w, const R* __restrict__ t11,
+                               const R* __restrict__ t22, const R* __restrict__ t33, const R* __restrict__ t12,
+                               const R* __restrict__ t13, const R* __restrict__ t23, TerBuf<R> T,
+                               const R* __restrict__ Om_in, R* __restrict__ Fmx, R* __restrict__ Fmy,
+                               R* __restrict__ Fmz) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    int64_t c = cidx(g, i, j, k);
+    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
+    auto RU = [&](int ii, int jj, int kk) { return S.mx[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)] * 1.0; };
+    auto RV = [&](int ii, int jj, int kk) { return S.my[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)] * 1.0; };
+    auto Om = [&](int ii, int jj, int kk) { return double(Om_in[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto U = [&](int ii, int jj, int kk) { return tvel(u, g, ii, jj, kk); };
+    auto V = [&](int ii, int jj, int kk) { return tvel(v, g, ii, jj, kk); };
+    auto W = [&](int ii, int jj, int kk) { return wvel(w, g, ii, jj, kk); };
+    auto Jt = [&](int ii, int jj, int kk) { return detJ_at(P, ii, jj, kk); };
+    auto pp = [&](int ii, int jj, int kk) { return ccw(A.pp, g, ii, jj, kk); };
+    const int ht = P.dyc_h, vt = P.dyc_v;
+    const double hf = P.f_dyc_h, vf = P.f_dyc_v;
+    const bool c2 = (ht == ERF_ADV_CENTERED_2ND && vt == ERF_ADV_CENTERED_2ND);
+    const double az = 1.0;
+    const double g2 = -P.gravity;
+    // ---------------- x-momentum at face (i,j,k)
+    {
+        double src;
+        if (c2) {
+            double xh = 0.25 * (RU(i, j, k) * 1.0 + RU(i + 1, j, k) * 1.0) * (U(i + 1, j, k) + U(i, j, k)) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i + 1, j, k));
+            double xl = 0.25 * (RU(i, j, k) * 1.0 + RU(i - 1, j, k) * 1.0) * (U(i - 1, j, k) + U(i, j, k)) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i - 1, j, k));
+            double yh = 0.25 * (RV(i, j + 1, k) * 1.0 + RV(i - 1, j + 1, k) * 1.0) * (U(i, j + 1, k) + U(i, j, k)) * hzeta_EK(P, i, j + 1, k);
+            double yl = 0.25 * (RV(i, j, k) * 1.0 + RV(i - 1, j, k) * 1.0) * (U(i, j - 1, k) + U(i, j, k)) * hzeta_EK(P, i, j, k);
+            double zh = 0.25 * (Om(i, j, k + 1) + Om(i - 1, j, k + 1)) * (U(i, j, k + 1) + U(i, j, k)) * 0.5 * (az + az);
+            double zl = 0.25 * (Om(i, j, k) + Om(i - 1, j, k)) * (U(i, j, k - 1) + U(i, j, k)) * 0.5 * (az + az);
+            src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
+            src = -src / (0.5 * (Jt(i, j, k) + Jt(i - 1, j, k)));
+        } else {
+            double a, xh, xl, yh, yl, zh, zl;
+            a = 0.5 * (RU(i + 1, j, k) * 1.0 + RU(i, j, k) * 1.0); xh = a * interp_dir(0, i + 1, j, k, U, ht, a, hf) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i + 1, j, k));
+            a = 0.5 * (RU(i - 1, j, k) * 1.0 + RU(i, j, k) * 1.0); xl = a * interp_dir(0, i, j, k, U, ht, a, hf) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i - 1, j, k));
+            a = 0.5 * (RV(i, j + 1, k) * 1.0 + RV(i - 1, j + 1, k) * 1.0); yh = a * interp_dir(1, i, j + 1, k, U, ht, a, hf) * hzeta_EK(P, i, j + 1, k);
+            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i - 1, j, k) * 1.0); yl = a * interp_dir(1, i, j, k, U, ht, a, hf) * hzeta_EK(P, i, j, k);
+            a = 0.5 * (Om(i, j, k + 1) + Om(i - 1, j, k + 1)) * 0.5 * (az + az); zh = a * interp_dir(2, i, j, k + 1, U, vt, a, vf);
+            a = 0.5 * (Om(i, j, k) + Om(i - 1, j, k)) * 0.5 * (az + az); zl = a * interp_dir(2, i, j, k, U, vt, a, vf);
+            src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
+            src /= 0.5 * (Jt(i, j, k) + Jt(i - 1, j, k));
+            src = -src;
+        }
+        double r = src;
+        if (P.use_diff) {
+            auto T11 = [&](int ii) { return double(t11[cidx(g, wrap(ii, g.nx), j, k)]); };
+            double d = ((T11(i) - T11(i - 1)) * dxi * 1.0 + (double(t12[cidx(g, i, wrap(j + 1, g.ny), k)]) - double(t12[c])) * dyi * 1.0
+                        + (double(t13[c + g.sk]) - double(t13[c])) * dzi);
+            d /= 0.5 * (Jt(i, j, k) + Jt(i - 1, j, k));
+            r -= d;
+        }
+        double gpx = dxi * (pp(i, j, k) - pp(i - 1, j, k));
+        {
+            double mxi = hxi_I(P, i, j, k), mz = hzeta_I(P, i, j, k), gz;
+            if (k == 0) gz = 0.5 * dzi * (pp(i - 1, j, k + 1) + pp(i, j, k + 1) - pp(i - 1, j, k) - pp(i, j, k));
+            else if (k == nz - 1) gz = 0.5 * dzi * (pp(i - 1, j, k) + pp(i, j, k) - pp(i - 1, j, k - 1) - pp(i, j, k - 1));
+            else gz = 0.25 * dzi * (pp(i - 1, j, k + 1) + pp(i, j, k + 1) - pp(i - 1, j, k - 1) - pp(i, j, k - 1));
+            gpx -= (mxi / mz) * gz;
+        }
+        gpx *= 1.0;
+        double xsrc = 0.0;
+        if (P.coriolis) {
+            double rvl = 0.25 * (RV(i, j + 1, k) + RV(i, j, k) + RV(i - 1, j + 1, k) + RV(i - 1, j, k));
+            double rwl = 0.25 * (S.mz[cidx(g, i, j, k + 1)] + S.mz[c] + S.mz[cidx(g, i, wrap(j - 1, g.ny), k + 1)] + S.mz[cidx(g, i, wrap(j - 1, g.ny), k)]);
+            xsrc += P.cf * (rvl * P.sinphi - rwl * P.cosphi);
+        }
+        xsrc += 0.5 * (S.cons[c] + S.cons[cidx(g, wrap(i - 1, g.nx), j, k)]) * P.geo0;
+        r += (-gpx - 0.0) / (1.0 + 0.0) + xsrc;
+        Fmx[c] = R(r);
+    }
+    // ---------------- y-momentum at face (i,j,k)
+    {
+        double src;
+        if (c2) {
+            double xh = 0.25 * (RU(i + 1, j, k) * 1.0 + RU(i + 1, j - 1, k) * 1.0) * (V(i + 1, j, k) + V(i, j, k)) * hzeta_EK(P, i + 1, j, k);
+            double xl = 0.25 * (RU(i, j, k) * 1.0 + RU(i, j - 1, k) * 1.0) * (V(i - 1, j, k) + V(i, j, k)) * hzeta_EK(P, i, j, k);
+            double yh = 0.25 * (RV(i, j + 1, k) * 1.0 + RV(i, j, k) * 1.0) * (V(i, j + 1, k) + V(i, j, k)) * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j + 1, k));
+            double yl = 0.25 * (RV(i, j, k) * 1.0 + RV(i, j - 1, k) * 1.0) * (V(i, j - 1, k) + V(i, j, k)) * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j - 1, k));
+            double zh = 0.25 * (Om(i, j, k + 1) + Om(i, j - 1, k + 1)) * (V(i, j, k + 1) + V(i, j, k)) * 0.5 * (az + az);
+            double zl = 0.25 * (Om(i, j, k) + Om(i, j - 1, k)) * (V(i, j, k - 1) + V(i, j, k)) * 0.5 * (az + az);
+            src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
+            src = -src / (0.5 * (Jt(i, j, k) + Jt(i, j - 1, k)));
+        } else {
+            double a, xh, xl, yh, yl, zh, zl;
+            a = 0.5 * (RU(i + 1, j, k) * 1.0 + RU(i + 1, j - 1, k) * 1.0); xh = a * interp_dir(0, i + 1, j, k, V, ht, a, hf) * hzeta_EK(P, i + 1, j, k);
+            a = 0.5 * (RU(i, j, k) * 1.0 + RU(i, j - 1, k) * 1.0); xl = a * interp_dir(0, i, j, k, V, ht, a, hf) * hzeta_EK(P, i, j, k);
+            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i, j + 1, k) * 1.0); yh = a * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j + 1, k)) * interp_dir(1, i, j + 1, k, V, ht, a, hf);
+            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i, j - 1, k) * 1.0); yl = a * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j - 1, k)) * interp_dir(1, i, j, k, V, ht, a, hf);
+            a = 0.5 * (Om(i, j, k + 1) + Om(i, j - 1, k + 1)) * 0.5 * (az + az); zh = a * interp_dir(2, i, j, k + 1, V, vt, a, vf);
+            a = 0.5 * (Om(i, j, k) + Om(i, j - 1, k)) * 0.5 * (az + az); zl = a * interp_dir(2, i, j, k, V, vt, a, vf);
+            src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
+            src /= 0.5 * (Jt(i, j, k) + Jt(i, j - 1, k));
+            src = -src;
+        }
+        double r = src;
+        if (P.use_diff) {
+            auto T22 = [&](int jj) { return double(t22[cidx(g, i, wrap(jj, g.ny), k)]); };
+            double d = ((double(t12[cidx(g, wrap(i + 1, g.nx), j, k)]) - double(t12[c])) * dxi * 1.0 + (T22(j) - T22(j - 1)) * dyi * 1.0
+                        + (double(t23[c + g.sk]) - double(t23[c])) * dzi);
+            d /= 0.5 * (Jt(i, j, k) + Jt(i, j - 1, k));
+            r -= d;
+        }
+        double gpy = dyi * (pp(i, j, k) - pp(i, j - 1, k));
+        {
+            double meta = heta_J(P, i, j, k), mz = hzeta_J(P, i, j, k), gz;
+            if (k == 0) gz = 0.5 * dzi * (pp(i, j, k + 1) + pp(i, j - 1, k + 1) - pp(i, j, k) - pp(i, j - 1, k));
+            else if (k == nz - 1) gz = 0.5 * dzi * (pp(i, j, k) + pp(i, j - 1, k) - pp(i, j, k - 1) - pp(i, j - 1, k - 1));
+            else gz = 0.25 * dzi * (pp(i, j, k + 1) + pp(i, j - 1, k + 1) - pp(i, j, k - 1) - pp(i, j - 1, k - 1));
+            gpy -= (meta / mz) * gz;
+        }
+        gpy *= 1.0;
+        double ysrc = 0.0;
+        if (P.coriolis) {
+            double rul = 0.25 * (RU(i + 1, j, k) + RU(i, j, k) + RU(i + 1, j - 1, k) + RU(i, j - 1, k));
+            ysrc += -P.cf * rul * P.sinphi;
+        }
+        ysrc += 0.5 * (S.cons[c] + S.cons[cidx(g, i, wrap(j - 1, g.ny), k)]) * P.geo1;
+        r += (-gpy - 0.0) / (1.0 + 0.0) + ysrc;
+        Fmy[c] = R(r);
+    }
+    // ---------------- z-momentum at face (i,j,k), 1 <= k <= nz-1
+    if (k == 0) {
+        Fmz[c] = R(0);
+        if (nz == 1) Fmz[c + g.sk] = R(0);
+        return;
+    }
+    {
+        const int lo_z_face = 0, hi_z_face = nz;
+        double src;
+        if (c2) {
+            double xh = 0.25 * (RU(i + 1, j, k) + RU(i + 1, j, k - 1)) * 1.0 * (W(i + 1, j, k) + W(i, j, k)) * hzeta_EJ(P, i + 1, j, k);
+            double xl = 0.25 * (RU(i, j, k) + RU(i, j, k - 1)) * 1.0 * (W(i - 1, j, k) + W(i, j, k)) * hzeta_EJ(P, i, j, k);
+            double yh = 0.25 * (RV(i, j + 1, k) + RV(i, j + 1, k - 1)) * 1.0 * (W(i, j + 1, k) + W(i, j, k)) * hzeta_EI(P, i, j + 1, k);
+            double yl = 0.25 * (RV(i, j, k) + RV(i, j, k - 1)) * 1.0 * (W(i, j - 1, k) + W(i, j, k)) * hzeta_EI(P, i, j, k);
+            double zl = 0.25 * (Om(i, j, k) + Om(i, j, k - 1)) * (W(i, j, k) + W(i, j, k - 1));
+            double zh = (k == hi_z_face) ? Om(i, j, k) * W(i, j, k) * az
+                                         : 0.25 * (Om(i, j, k) + Om(i, j, k + 1)) * (W(i, j, k) + W(i, j, k + 1)) * 0.5 * (az + az);
+            src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
+            src = -src / (0.5 * (Jt(i, j, k) + Jt(i, j, k - 1)));
+        } else {
+            double a, xh, xl, yh, yl, zh, zl;
+            a = 0.5 * (RU(i + 1, j, k) + RU(i + 1, j, k - 1)) * 1.0; xh = a * interp_dir(0, i + 1, j, k, W, ht, a, hf) * hzeta_EJ(P, i + 1, j, k);
+            a = 0.5 * (RU(i, j, k) + RU(i, j, k - 1)) * 1.0; xl = a * interp_dir(0, i, j, k, W, ht, a, hf) * hzeta_EJ(P, i, j, k);
+            a = 0.5 * (RV(i, j + 1, k) + RV(i, j + 1, k - 1)) * 1.0; yh = a * interp_dir(1, i, j + 1, k, W, ht, a, hf) * hzeta_EI(P, i, j + 1, k);
+            a = 0.5 * (RV(i, j, k) + RV(i, j, k - 1)) * 1.0; yl = a * interp_dir(1, i, j, k, W, ht, a, hf) * hzeta_EI(P, i, j, k);
+            auto iZall = [&](int kk, double upw, double frac, int type) {
+                int gt = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH) ? ERF_ADV_UPWIND_5TH
+                         : (type == ERF_ADV_CENTERED_2ND ? ERF_ADV_CENTERED_2ND : ERF_ADV_UPWIND_3RD);
+                double s[6];
+                const int wd = stencil_width(gt);
+                for (int m = 0; m < 6; ++m) {
+                    int off = m - 3;
+                    s[m] = (off >= -wd && off <= wd - 1) ? W(i, j, kk + off) : 0.0;
+                }
+                return interp_all<double>(type, s, upw, frac);
+            };
+            double Oh = (k == hi_z_face) ? Om(i, j, k) * az : 0.25 * (Om(i, j, k) + Om(i, j, k + 1)) * (az + az);
+            double ih, il;
+            if (k == hi_z_face - 1) ih = iZall(k + 1, Oh, 0, ERF_ADV_CENTERED_2ND);
+            else if (k == hi_z_face - 2 || k == lo_z_face + 1) {
+                if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) ih = iZall(k + 1, Oh, 0, ERF_ADV_CENTERED_4TH);
+                else ih = iZall(k + 1, Oh, vf, vt);
+            } else ih = interp_dir(2, i, j, k + 1, W, vt, Oh, vf);
+            zh = Oh * ih;
+            double Ol = 0.25 * (Om(i, j, k) + Om(i, j, k - 1)) * (az + az);
+            if (k == lo_z_face + 1) il = iZall(k, Ol, 0, ERF_ADV_CENTERED_2ND);
+            else if (k == lo_z_face + 2 || k == hi_z_face - 1) {
+                if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) il = iZall(k, Ol, 0, ERF_ADV_CENTERED_4TH);
+                else il = iZall(k, Ol, vf, vt);
+            } else il = interp_dir(2, i, j, k, W, vt, Ol, vf);
+            zl = Ol * il;
+            src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
+            double denom = 0.5 * (Jt(i, j, k) + Jt(i, j, k - 1));
+            src /= denom;
+            src = -src;
+        }
+        double r = src;
+        if (P.use_diff) {
+            double d = ((double(T.t31[cidx(g, wrap(i + 1, g.nx), j, k)]) - double(T.t31[c])) * dxi * 1.0
+                        + (double(T.t32[cidx(g, i, wrap(j + 1, g.ny), k)]) - double(T.t32[c])) * dyi * 1.0
+                        + (double(t33[c]) - double(t33[c - g.sk])) * dzi);
+            d /= 0.5 * (Jt(i, j, k) + Jt(i, j, k - 1));
+            r -= d;
+        }
+        double mz = hzeta_K(P, i, j, k);
+        double gpz = dzi * (pp(i, j, k) - pp(i, j, k - 1)) / mz;
+        double zsrc = 0.0;
+        if (P.buoy_type == 1) {
+            zsrc = g2 * 0.5 * ((S.cons[c] - bs(P.r0, g, i, j, k)) + (S.cons[c - g.sk] - bs(P.r0, g, i, j, k - 1)));
+        } else {
+            auto T0 = [&](int kk) {
+                double p0v = bs(P.p0, g, i, j, kk);
+                double rt0 = eos_rt_given_p(p0v);
+                return (rt0 / bs(P.r0, g, i, j, kk)) / pow(p_0 / p0v, P.rdOcp);
+            };
+            double t0_hi = T0(k), t_hi = eos_T(S.cons[c], S.cons[N + c], 0.0);
+            double t0_lo = T0(k - 1), t_lo = eos_T(S.cons[c - g.sk], S.cons[N + c - g.sk], 0.0);
+            double qplus = (t_hi - t0_hi) / t0_hi, qminus = (t_lo - t0_lo) / t0_lo;
+            double r0_q_avg = 0.5 * (bs(P.r0, g, i, j, k) * qplus + bs(P.r0, g, i, j, k - 1) * qminus);
+            zsrc = -r0_q_avg * g2;
+        }
+        if (P.coriolis) {
+            double rul = 0.25 * (RU(i + 1, j, k) + RU(i, j, k) + RU(i + 1, j, k - 1) + RU(i, j, k - 1));
+            zsrc += P.cf * rul * P.cosphi;
+        }
+        zsrc += 0.5 * (S.cons[c] + S.cons[c - g.sk]) * P.geo2;
+        r += (zsrc - gpz - 0.0) / (1.0 + 0.0);
+        Fmz[c] = R(r);
+        if (k == nz - 1) Fmz[c + g.sk] = R(0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Acoustic substep with terrain, horizontal part (ERF_fast_rhs_T.cpp:130-320):
+// lagged d(rho theta) and its extrapolation, U'' / V'' with the
+// terrain-corrected gradient of the extrapolated d(rho theta); the old and
+// new increments are kept for the vertical part.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_fast_h(Params P, int step, double dtau, double facinv, StateBuf Sprev, int prev_rt,
+                             StateBuf Sst, StageAux<R> A, const R* __restrict__ Fmx, const R* __restrict__ Fmy,
+                             const R* __restrict__ lag_in, R* __restrict__ lag_out, TerBuf<R> T, R* __restrict__ avx,
+                             R* __restrict__ avy, double* __restrict__ outx, double* __restrict__ outy) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
+    int64_t c = cidx(g, i, j, k), cxm = cidx(g, im, j, k), cym = cidx(g, i, jm, k);
+    const double beta_d = 0.1, dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
+    auto extrap = [&](int ii, int jj, int kk) {
+        int64_t e = cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), clampk(kk, nz));
+        double drt = Sprev.cons[N + e] - Sst.cons[N + e];
+        if (step == 0) return drt;
+        return drt + beta_d * (drt - double(lag_in[e]));
+    };
+    lag_out[c] = R(Sprev.cons[N + c] - Sst.cons[N + c]);
+    double px = Sprev.mx[c], py = Sprev.my[c];
+    if (prev_rt) {
+        double rs = Sprev.cons[c] + Sprev.cons[cxm];
+        double ut = (px * 2.0) / rs;
+        px = (ut * 0.5) * rs;
+        rs = Sprev.cons[c] + Sprev.cons[cym];
+        double vt = (py * 2.0) / rs;
+        py = (vt * 0.5) * rs;
+    }
+    double odu = px - Sst.mx[c], odv = py - Sst.my[c];
+    double gpx, gpy;
+    {
+        double mxi = hxi_I(P, i, j, k), mz = hzeta_I(P, i, j, k);
+        double gp_xi = (extrap(i, j, k) - extrap(i - 1, j, k)) * dxi;
+        double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k) - extrap(i, j, k))
+                                  : 0.25 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k - 1) - extrap(i, j, k - 1));
+        gpx = gp_xi - (mxi / mz) * gp_zeta;
+        gpx *= 1.0;
+    }
+    {
+        double meta = heta_J(P, i, j, k), mz = hzeta_J(P, i, j, k);
+        double gp_eta = (extrap(i, j, k) - extrap(i, j - 1, k)) * dyi;
+        double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k) - extrap(i, j - 1, k))
+                                  : 0.25 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k - 1) - extrap(i, j - 1, k - 1));
+        gpy = gp_eta - (meta / mz) * gp_zeta;
+        gpy *= 1.0;
+    }
+    double pix = 0.5 * (double(A.pi[cxm]) + double(A.pi[c]));
+    double piy = 0.5 * (double(A.pi[cym]) + double(A.pi[c]));
+    double fx = -Gamma_ * R_d * pix * gpx;
+    double fy = -Gamma_ * R_d * piy * gpy;
+    double ndu = odu + dtau * fx + dtau * double(Fmx[c]);
+    double ndv = odv + dtau * fy + dtau * double(Fmy[c]);
+    T.ndu[c] = R(ndu); T.ndv[c] = R(ndv);
+    T.odu[c] = R(odu); T.odv[c] = R(odv);
+    avx[c] += R(facinv * ndu);
+    avy[c] += R(facinv * ndv);
+    outx[c] = Sst.mx[c] + ndu;
+    outy[c] = Sst.my[c] + ndv;
+}
+
+// ---------------------------------------------------------------------------
+// Acoustic substep with terrain, vertical part (ERF_fast_rhs_T.cpp:320-680),
+// one thread per column: horizontal rho / rho*theta fluxes through the
+// sloping faces, Omega of the previous increments, the detJ-weighted
+// implicit system for Omega'' (coefficients from the stage), w'' from
+// Omega'' and the new horizontal increments, vertical fluxes, average
+// contravariant momentum, rho and rho*theta.  The previous top z-momentum is
+// the one the boundary fill leaves (w from Omega = 0 at the lid).
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
+                                int prev_rt, StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons,
+                                const R* __restrict__ Fmz, TerBuf<R> T, const R* __restrict__ cA,
+                                const R* __restrict__ cInvB, const R* __restrict__ cCB, const R* __restrict__ cP,
+                                const R* __restrict__ cQ, R* __restrict__ avz, double* out_cons, double* out_mz) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell, sk = g.sk, col = (int64_t)j * g.nx + i;
+    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi, halfg = P.halfg;
+    // per-column scratch: soln, omega, trhs0, trhs1 (nz+1 each)
+    double* sol = T.soln + col * 4 * (int64_t)(nz + 1);
+    double* om = sol + (nz + 1);
+    double* tr0 = om + (nz + 1);
+    double* tr1 = tr0 + (nz + 1);
+    auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
+    auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto ODU = [&](int ii, int jj, int kk) { return double(T.odu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto ODV = [&](int ii, int jj, int kk) { return double(T.odv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto Z = [&](int a, int b, int cc) { return Zn(P, a, b, cc); };
+    // previous z-momentum as the boundary fill leaves it
+    auto prev_mz = [&](int k) {
+        int64_t f = (int64_t)k * sk + col;
+        double m = Sprev.mz[f];
+        if (!prev_rt) return m;
+        if (k == 0 || k == nz) {
+            auto U1 = [&](int ii, int jj, int kk) {
+                if (kk >= nz) {
+                    if (g.zhi_noslip) return 0.0;
+                    kk = nz - 1;
+                }
+                return rt_u(g, Sprev.cons, Sprev.mx, ii, jj, kk);
+            };
+            auto V1 = [&](int ii, int jj, int kk) {
+                if (kk >= nz) {
+                    if (g.zhi_noslip) return 0.0;
+                    kk = nz - 1;
+                }
+                return rt_v(g, Sprev.cons, Sprev.my, ii, jj, kk);
+            };
+            int kc = (k == 0) ? 0 : nz - 1;
+            double r = Sprev.cons[(int64_t)kc * sk + col];
+            double wb = w_from_omega(P, i, j, k, 0.0, U1, V1);
+            return (wb * 0.5) * (r + r);
+        }
+        double rs = Sprev.cons[f] + Sprev.cons[f - sk];
+        double wt = (m * 2.0) / rs;
+        return (wt * 0.5) * rs;
+    };
+    // horizontal fluxes of rho and rho theta
+    for (int k = 0; k < nz; ++k) {
+        double hxh = 0.5 * dzi * (Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j, k) - Z(i + 1, j + 1, k));
+        double hxl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
+        double hyh = 0.5 * dzi * (Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
+        double hyl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i + 1, j, k));
+        double xl = NDU(i, j, k) * hxl / 1.0, xh = NDU(i + 1, j, k) * hxh / 1.0;
+        double yl = NDV(i, j, k) * hyl / 1.0, yh = NDV(i, j + 1, k) * hyh / 1.0;
+        double mfsq = 1.0;
+        double tc = th(i, j, k);
+        tr0[k] = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
+        tr1[k] = ((xh * (tc + th(i + 1, j, k)) - xl * (tc + th(i - 1, j, k))) * dxi * mfsq +
+                  (yh * (tc + th(i, j + 1, k)) - yl * (tc + th(i, j - 1, k))) * dyi * mfsq) * 0.5;
+    }
+    // Omega of the previous increments
+    for (int k = 0; k <= nz; ++k) {
+        double odw = prev_mz(k) - Sst.mz[(int64_t)k * sk + col];
+        if (k == 0) om[k] = 0.;
+        else if (k == nz) om[k] = odw;
+        else om[k] = omega_from_w(P, i, j, k, odw, ODU, ODV);
+    }
+    // right-hand side and forward elimination
+    {
+        int64_t f0 = col;
+        double s = (dtau * double(Fmz[f0])) * double(cInvB[f0]);
+        sol[0] = s;
+        for (int k = 1; k <= nz; ++k) {
+            int64_t f = (int64_t)k * sk + col;
+            double rhs;
+            if (k == nz) {
+                rhs = dtau * double(Fmz[f]);
+            } else {
+                int64_t cm = f - sk;
+                double Jk = detJ_at(P, i, j, k), Jkm = detJ_at(P, i, j, k - 1);
+                double dJk = 0.5 * (Jk + Jkm);
+                double cPk = double(cP[f]), cQk = double(cQ[f]);
+                double tlo = 0.5 * (th(i, j, k - 2) + th(i, j, k - 1));
+                double tmid = 0.5 * (th(i, j, k - 1) + th(i, j, k));
+                double thi = 0.5 * (th(i, j, k) + th(i, j, k + 1));
+                double odr_k = Sprev.cons[f] - Sst.cons[f], odr_km = Sprev.cons[cm] - Sst.cons[cm];
+                double odrt_k = Sprev.cons[N + f] - Sst.cons[N + f], odrt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
+                double R0t = (-halfg * odr_k + cPk * odrt_k) * Jk + (-halfg * odr_km + cQk * odrt_km) * Jkm;
+                double R1t = -halfg * (double(Fcons[f]) * Jk + double(Fcons[cm]) * Jkm)
+                             + (cPk * double(Fcons[N + f]) * Jk + cQk * double(Fcons[N + cm]) * Jkm);
+                double Okp1 = om[k + 1], Ok = om[k], Okm1 = om[k - 1];
+                R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + tr0[k] + tr0[k - 1]);
+                R1t += -(cPk * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + tr1[k]) +
+                         cQk * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + tr1[k - 1]));
+                double odw = prev_mz(k) - Sst.mz[f];
+                rhs = dJk * odw + dtau * (dJk * double(Fmz[f]) + R0t + dtau * beta_2 * R1t);
+                rhs += dJk * omega_from_w(P, i, j, k, 0., NDU, NDV);
+            }
+            s = (rhs - double(cA[f]) * s) * double(cInvB[f]);
+            sol[k] = s;
+        }
+        for (int k = nz - 1; k >= 0; --k) {
+            int64_t f = (int64_t)k * sk + col;
+            s = sol[k] - double(cCB[f]) * s;
+            sol[k] = s;
+        }
+    }
+    // z-momentum, vertical fluxes, rho and rho theta
+    for (int k = 0; k <= nz; ++k) {
+        int64_t f = (int64_t)k * sk + col;
+        double m = Sst.mz[f];
+        if (k >= 1 && k <= nz - 1) m += w_from_omega(P, i, j, k, sol[k], NDU, NDV);
+        out_mz[f] = m;
+    }
+    for (int k = 0; k < nz; ++k) {
+        int64_t c = (int64_t)k * sk + col;
+        double zl = beta_2 * sol[k] + beta_1 * om[k];
+        double zh = beta_2 * sol[k + 1] + beta_1 * om[k + 1];
+        avz[c] += R(facinv * zl / (1.0 * 1.0));
+        if (k == nz - 1) avz[c + sk] += R(facinv * zh / (1.0 * 1.0));
+        double Jc = detJ_at(P, i, j, k);
+        double tc = th(i, j, k);
+        double frho = -(tr0[k] + (zh - zl) * dzi) / Jc;
+        double frt = -(tr1[k] + 0.5 * (zh * (tc + th(i, j, k + 1)) - zl * (tc + th(i, j, k - 1))) * dzi) / Jc;
+        double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
+        out_cons[c] = pr + dtau * (double(Fcons[c]) + frho);
+        out_cons[N + c] = prt + dtau * (double(Fcons[N + c]) + frt);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Slow RHS of the slow variables with terrain and the stage update
+// (ERF_slow_rhs_post.cpp:169-530): passive scalar and (Deardorff) rho*KE
+// advected with the average momenta (over detJ), DiffusionSrcForState_T with
+// the TKE sources, S_new = S_old + dt RHS (KE clipped at DBL_EPSILON); rho,
+// rho*theta and the momenta from the fast solution through the two boundary
+// round trips, w on the ground and the lid from Omega = 0 of the new u, v;
+// the next stage's primitives.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
+                           StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* __restrict__ mut,
+                           TkeBuf<R> tke, const R* __restrict__ avx, const R* __restrict__ avy,
+                           const R* __restrict__ avz, double* __restrict__ un, double* __restrict__ vn,
+                           double* __restrict__ wn) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    int64_t c = cidx(g, i, j, k);
+    const bool dd = P.les == ERF_LES_DEARDORFF;
+    const double Jc = detJ_at(P, i, j, k);
+    auto AX = [&](int ii) { return double(avx[cidx(g, wrap(ii, g.nx), j, k)]); };
+    auto AY = [&](int jj) { return double(avy[cidx(g, i, wrap(jj, g.ny), k)]); };
+    auto AZ = [&](int kk) { return double(avz[cidx(g, i, j, kk)]); };
+    const int nslow = 1 + (dd ? 1 : 0);
+    for (int q = 0; q < nslow; ++q) {
+        const int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOKE_COMP;
+        const R* phi = Acur.prim + (int64_t)(n - 1) * N;
+        auto ph = [&](int ii, int jj, int kk) { return ccw(phi, g, ii, jj, kk); };
+        const int ht = P.dry_h, vt = P.dry_v;
+        const double hf = P.f_dry_h, vf = P.f_dry_v;
+        double fxl = AX(i), fxh = AX(i + 1), fyl = AY(j), fyh = AY(j + 1), fzl = AZ(k), fzh = AZ(k + 1);
+        double tx_l = fxl * interp_dir(0, i, j, k, ph, ht, fxl, hf), tx_h = fxh * interp_dir(0, i + 1, j, k, ph, ht, fxh, hf);
+        double ty_l = fyl * interp_dir(1, i, j, k, ph, ht, fyl, hf), ty_h = fyh * interp_dir(1, i, j + 1, k, ph, ht, fyh, hf);
+        double tz_l = fzl * interp_dir(2, i, j, k, ph, vt, fzl, vf), tz_h = fzh * interp_dir(2, i, j, k + 1, ph, vt, fzh, vf);
+        double invdetJ = 1. / Jc;
+        double r = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
+        if (P.use_diff) {
+            DiffT<R> D{P, Sst.cons, phi, mut, nullptr, q == 0 ? P.alphaC_eff : 0.0, q == 0 ? P.invSc : P.invSigmaK};
+            double rlo, rhi;
+            r -= D.div(i, j, k, rlo, rhi);
+        }
+        if (q == 1) {
+            r += P.g_over_theta0 * double(tke.hfz[c]);
+            r += 2.0 * double(mut[c]) * double(tke.smn[c]);
+            r -= double(tke.diss[c]);
+        }
+        double v_ = Sold.cons[n * N + c] + slow_dt * r;
+        Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 2.220446049250313e-16);
+    }
+    Snew.cons[c] = Ssum.cons[c];
+    Snew.cons[N + c] = Ssum.cons[N + c];
+    if (!dd) Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
+    Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
+    double rho = Ssum.cons[c];
+    // horizontal momenta through the two round trips; velocity u2
+    auto u2f = [&](int ii, int jj, int kk) {
+        if (kk < 0 || kk >= nz) {
+            if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
+            kk = kk < 0 ? 0 : nz - 1;
+        }
+        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+        int64_t e = cidx(g, ii, jj, kk);
+        double rs = Ssum.cons[e] + Ssum.cons[cidx(g, wrap(ii - 1, g.nx), jj, kk)];
+        double m = Ssum.mx[e];
+        double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
+        return (m * 2.0) / rs;
+    };
+    auto v2f = [&](int ii, int jj, int kk) {
+        if (kk < 0 || kk >= nz) {
+            if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
+            kk = kk < 0 ? 0 : nz - 1;
+        }
+        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+        int64_t e = cidx(g, ii, jj, kk);
+        double rs = Ssum.cons[e] + Ssum.cons[cidx(g, ii, wrap(jj - 1, g.ny), kk)];
+        double m = Ssum.my[e];
+        double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
+        return (m * 2.0) / rs;
+    };
+    {
+        double rs = rho + Ssum.cons[cidx(g, wrap(i - 1, g.nx), j, k)];
+        double u2 = u2f(i, j, k);
+        Snew.mx[c] = (u2 * 0.5) * rs; un[c] = u2;
+    }
+    {
+        double rs = rho + Ssum.cons[cidx(g, i, wrap(j - 1, g.ny), k)];
+        double v2 = v2f(i, j, k);
+        Snew.my[c] = (v2 * 0.5) * rs; vn[c] = v2;
+    }
+    if (k == 0) {
+        double wb = w_from_omega(P, i, j, 0, 0.0, u2f, v2f);
+        Snew.mz[c] = (wb * 0.5) * (rho + rho); wn[c] = wb;
+    } else {
+        double rs = rho + Ssum.cons[c - g.sk];
+        double m = Ssum.mz[c];
+        double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
+        double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
+        Snew.mz[c] = m; wn[c] = w2;
+    }
+    if (k == nz - 1) {
+        double wt = w_from_omega(P, i, j, nz, 0.0, u2f, v2f);
+        Snew.mz[c + g.sk] = (wt * 0.5) * (rho + rho); wn[c + g.sk] = wt;
+    }
+    if (make_next) stage_aux_ter<R>(P, Snew.cons, Anext, c, k);
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+template <class R>
+void launch_ter_step_begin(const Params& P, cudaStream_t st, const double* cons, const double* uo, const double* vo,
+                           const double* wo, StateBuf S, double* un, double* vn, double* wn, StageAux<R> A, R* mut,
+                           TkeBuf<R> tke) {
+    k_ter_step_begin<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, cons, uo, vo, wo, S, un, vn, wn, A, mut, tke);
+}
+template <class R>
+void launch_ter_tau(const Params& P, cudaStream_t st, int nrk, const double* cons, const double* u, const double* v,
+                    const double* w, const R* mut, TerBuf<R> T, TkeBuf<R> tke, R* t11, R* t22, R* t33, R* t12, R* t13,
+                    R* t23) {
+    k_ter_strain<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, nrk, u, v, w, T, tke);
+    k_ter_stress<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, cons, mut, T, t11, t22, t33, t12, t13, t23);
+}
+template <class R>
+void launch_ter_slow_cell(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
+                          const double* v, const R* mut, TkeBuf<R> tke, R* Fcons, R* avx, R* avy, R* avz) {
+    k_ter_slow_cell<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S, A, u, v, mut, tke, Fcons, avx, avy, avz);
+}
+template <class R>
+void launch_ter_slow_mom(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
+                         const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,
+                         const R* t13, const R* t23, TerBuf<R> T, const R* Om, R* Fmx, R* Fmy, R* Fmz) {
+    k_ter_slow_mom<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S, A, u, v, w, t11, t22, t33, t12, t13, t23, T,
+                                                                     Om, Fmx, Fmy, Fmz);
+}
+template <class R>
+void launch_ter_fast_h(const Params& P, cudaStream_t st, int step, double dtau, double facinv, StateBuf Sprev,
+                       int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in,
+                       R* lag_out, TerBuf<R> T, R* avx, R* avy, double* outx, double* outy) {
+    k_ter_fast_h<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, step, dtau, facinv, Sprev, prev_rt, Sst, A, Fmx,
+                                                                   Fmy, lag_in, lag_out, T, avx, avy, outx, outy);
+}
+template <class R>
+void launch_ter_fast_vert(const Params& P, cudaStream_t st, double dtau, double facinv, double beta_1, double beta_2,
+                          StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmz,
+                          TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz,
+                          double* out_cons, double* out_mz) {
+    dim3 b(32, 4, 1), gr((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1);
+    k_ter_fast_vert<R><<<gr, b, 0, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, prev_rt, Sst, A, Fcons, Fmz, T, cA,
+                                         cInvB, cCB, cP, cQ, avz, out_cons, out_mz);
+}
+template <class R>
+void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
+                     StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,
+                     const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
+    k_ter_post<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, slow_dt, Sold, Sst, Ssum, Snew, Acur, Anext,
+                                                                 make_next, mut, tke, avx, avy, avz, un, vn, wn);
+}
+
+#define ERFB_TER_INSTANTIATE(R)                                                                                     \
+    template void launch_ter_step_begin<R>(const Params&, cudaStream_t, const double*, const double*, const double*, \
+                                           const double*, StateBuf, double*, double*, double*, StageAux<R>, R*,      \
+                                           TkeBuf<R>);                                                               \
+    template void launch_ter_tau<R>(const Params&, cudaStream_t, int, const double*, const double*, const double*,   \
+                                    const double*, const R*, TerBuf<R>, TkeBuf<R>, R*, R*, R*, R*, R*, R*);          \
+    template void launch_ter_slow_cell<R>(const Params&, cudaStream_t, StateBuf, StageAux<R>, const double*,         \
+                                          const double*, const R*, TkeBuf<R>, R*, R*, R*, R*);                       \
+    template void launch_ter_slow_mom<R>(const Params&, cudaStream_t, StateBuf, StageAux<R>, const double*,          \
+                                         const double*, const double*, const R*, const R*, const R*, const R*,       \
+                                         const R*, const R*, TerBuf<R>, const R*, R*, R*, R*);                       \
+    template void launch_ter_fast_h<R>(const Params&, cudaStream_t, int, double, double, StateBuf, int, StateBuf,    \
+                                       StageAux<R>, const R*, const R*, const R*, R*, TerBuf<R>, R*, R*, double*,    \
+                                       double*);                                                                     \
+    template void launch_ter_fast_vert<R>(const Params&, cudaStream_t, double, double, double, double, StateBuf,     \
+                                          int, StateBuf, StageAux<R>, const R*, const R*, TerBuf<R>, const R*,       \
+                                          const R*, const R*, const R*, const R*, R*, double*, double*);             \
+    template void launch_ter_post<R>(const Params&, cudaStream_t, double, StateBuf, StateBuf, StateBuf, StateBuf,    \
+                                     StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, const R*, const R*,         \
+                                     const R*, double*, double*, double*);
+
+ERFB_TER_INSTANTIATE(double)
+ERFB_TER_INSTANTIATE(float)
+#undef ERFB_TER_INSTANTIATE
+
+}  // namespace erfb

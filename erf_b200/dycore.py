@@ -32,7 +32,7 @@ EXPORTS = [
     "erf_b200_mlp_infer", "erf_b200_set_closure", "erf_b200_closure_fallbacks", "erf_b200_closure_features_host",
     "erf_b200_load_state", "erf_b200_store_state", "erf_b200_advance_resident", "erf_b200_autotune",
     "erf_b200_ensemble_create", "erf_b200_ensemble_advance", "erf_b200_ensemble_sync", "erf_b200_ensemble_destroy",
-    "erf_b200_last_cuda_error",
+    "erf_b200_last_cuda_error", "erf_b200_set_terrain", "erf_b200_make_base_state_terrain",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs"]
@@ -68,6 +68,9 @@ def load_library():
     L.erf_b200_make_base_state.argtypes = [vp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                            dp, dp, dp, dp]
     L.erf_b200_set_base_state.argtypes = [vp, dp, dp, dp, dp]
+    L.erf_b200_set_terrain.argtypes = [vp, dp]
+    L.erf_b200_make_base_state_terrain.argtypes = [vp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                   dp, dp, dp, dp]
     fabp = ctypes.POINTER(ErfFab)
     L.erf_b200_advance.argtypes = [vp, fabp, fabp, fabp, fabp, i]
     L.erf_b200_advance_host.argtypes = [vp, dp, dp, dp, dp, i]
@@ -189,6 +192,28 @@ class Dycore:
         _check(self.lib.erf_b200_make_base_state(self._ctx, th.data_ptr(), qv.data_ptr(), case.theta_sfc,
                                                  case.qv_sfc, case.p_sfc, *[o.data_ptr() for o in out]),
                "make_base_state")
+        torch.cuda.synchronize()
+        return [o.cpu().numpy() for o in out]
+
+    def set_terrain(self, z_nd):
+        """Install z_phys_nd ([nz+1][ny+1][nx+1] node heights, periodic)."""
+        z = np.ascontiguousarray(z_nd, dtype=np.float64)
+        cfg = self.cfg
+        assert z.shape == (cfg.nz + 1, cfg.ny + 1, cfg.nx + 1)
+        _check(self.lib.erf_b200_set_terrain(self._ctx, z.ctypes.data), "set_terrain")
+
+    def make_base_state_terrain(self, case):
+        """Base state over the terrain on the GPU: 4 arrays of (nz+2)*ny*nx."""
+        import torch
+        cfg = self.cfg
+        th = torch.tensor(np.ascontiguousarray(case.theta3, dtype=np.float64), device="cuda")
+        qv = torch.tensor(np.ascontiguousarray(case.qv3, dtype=np.float64), device="cuda")
+        n = (cfg.nz + 2) * cfg.ny * cfg.nx
+        out = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(4)]
+        torch.cuda.synchronize()
+        _check(self.lib.erf_b200_make_base_state_terrain(self._ctx, th.data_ptr(), qv.data_ptr(), case.theta_sfc,
+                                                         case.qv_sfc, case.p_sfc, *[o.data_ptr() for o in out]),
+               "make_base_state_terrain")
         torch.cuda.synchronize()
         return [o.cpu().numpy() for o in out]
 

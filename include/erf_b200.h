@@ -203,9 +203,32 @@ int erf_b200_make_base_state(erf_b200_ctx* ctx,
                              double theta_sfc, double qv_sfc, double p_sfc,
                              double* rho0, double* p0, double* pi0, double* th0);
 
-/* Install the base state the dycore uses (same nz+2 layout as above). */
+/* Install the base state the dycore uses (same nz+2 layout as above; with
+ * terrain, nz+2 planes of nx*ny). */
 int erf_b200_set_base_state(erf_b200_ctx* ctx, const double* rho0,
                             const double* p0, const double* pi0, const double* th0);
+
+/* ----------------------------------------------------------------------------
+ * Static terrain (contexts created with use_terrain = 1)
+ * ------------------------------------------------------------------------- */
+
+/* Install the terrain-following grid: z_phys_nd at the (nx+1)(ny+1)(nz+1)
+ * nodes of the valid box, i fastest (host or device pointer), as built by
+ * init_terrain_grid (Source/Utils/ERF_TerrainMetrics.cpp:88-335).  The
+ * terrain must be periodic (node nx equal to node 0 and node ny to node 0).
+ * Ghost levels and the metrics detJ / z_cc (make_J, make_zcc,
+ * ERF_TerrainMetrics.cpp:583-715) are formed here.  EINVAL for a
+ * non-periodic or folded grid. */
+int erf_b200_set_terrain(erf_b200_ctx* ctx, const double* z_nd);
+
+/* Hydrostatic base state over the terrain (device pointers): theta3 / qv3 at
+ * the cell centres, nz planes of nx*ny; rho0, p0, pi0, th0 receive nz+2
+ * planes (plane k+1 for level k), the layout erf_b200_set_base_state expects
+ * with terrain.  Replaces calc_rho_p + ERF::erf_enforce_hse with terrain
+ * (Initialization/ERF_init1d.cpp:152-241). */
+int erf_b200_make_base_state_terrain(erf_b200_ctx* ctx, const double* theta3, const double* qv3,
+                                     double theta_sfc, double qv_sfc, double p_sfc,
+                                     double* rho0, double* p0, double* pi0, double* th0);
 
 /* ----------------------------------------------------------------------------
  * Full step: replaces ERF::advance_dycore + MRISplitIntegrator::advance +
