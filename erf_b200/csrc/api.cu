@@ -18,7 +18,7 @@ __global__ void k_base_state(int nz, double dz, double g, double rdOcp, const do
                              double* th0o);
 __global__ void k_pack(Geo g, erf_b200_fab f, int kind, int ncomp, double* dst);
 __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const double* src, int tang_lo_zero,
-                         int tang_hi_zero);
+                         int tang_hi_zero, int wall_w);
 }  // namespace erfb
 
 using namespace erfb;
@@ -458,7 +458,7 @@ int unpack(erf_b200_ctx* c, const erf_b200_fab* f, int kind, int ncomp, const do
     const Geo& g = c->g;
     int nxb = f->hi[0] - f->lo[0] + 1, nyb = f->hi[1] - f->lo[1] + 1, nzb = f->hi[2] - f->lo[2] + 1;
     dim3 b(32, 4, 1), gr((nxb + 31) / 32, (nyb + 3) / 4, nzb);
-    k_unpack<<<gr, b, 0, c->stream>>>(g, *f, kind, ncomp, src, g.zlo_noslip, g.zhi_noslip);
+    k_unpack<<<gr, b, 0, c->stream>>>(g, *f, kind, ncomp, src, g.zlo_noslip, g.zhi_noslip, c->P.ter);
     return cuda_fail(cudaGetLastError());
 }
 

@@ -572,7 +572,7 @@ __global__ void k_pack(Geo g, erf_b200_fab f, int kind, int ncomp, double* __res
 }
 
 __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const double* __restrict__ src,
-                         int tang_lo_zero, int tang_hi_zero) {
+                         int tang_lo_zero, int tang_hi_zero, int wall_w) {
     // thread over the caller's whole box
     int64_t nxb = f.hi[0] - f.lo[0] + 1, nyb = f.hi[1] - f.lo[1] + 1;
     int ib = blockIdx.x * blockDim.x + threadIdx.x;
@@ -586,7 +586,9 @@ __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const doubl
     for (int n = 0; n < ncomp; ++n) {
         double val;
         if (kind == 3) {
-            if (k <= 0 || k >= g.nz) val = 0.0;  // walls (and beyond): w = 0
+            // beyond the walls 0; on the walls 0 without terrain, the stored
+            // value (w from Omega = 0) with terrain
+            if (k < 0 || k > g.nz || (!wall_w && (k == 0 || k == g.nz))) val = 0.0;
             else val = src[n * per + cidx(g, ii, jj, k)];
         } else if (k < 0 || k >= g.nz) {
             bool lo = k < 0;

@@ -19,7 +19,7 @@ namespace erfb {
 __global__ void k_kessler(Params P, double* cons, double dtn, double dz);
 __global__ void k_pack(Geo g, erf_b200_fab f, int kind, int ncomp, double* dst);
 __global__ void k_unpack(Geo g, erf_b200_fab f, int kind, int ncomp, const double* src, int tang_lo_zero,
-                         int tang_hi_zero);
+                         int tang_hi_zero, int wall_w);
 }  // namespace erfb
 
 using namespace erfb;
@@ -99,7 +99,7 @@ extern "C" int erf_b200_kessler_advance_noalloc(const erf_b200_config* cfg, cons
     k_kessler<<<gc, b, 0, st>>>(P, scratch, dt, cfg->dz);
     int nxb = cons->hi[0] - cons->lo[0] + 1, nyb = cons->hi[1] - cons->lo[1] + 1, nzb = cons->hi[2] - cons->lo[2] + 1;
     dim3 gu((nxb + 31) / 32, (nyb + 3) / 4, nzb);
-    k_unpack<<<gu, b, 0, st>>>(g, *cons, 0, cfg->ncomp, scratch, g.zlo_noslip, g.zhi_noslip);
+    k_unpack<<<gu, b, 0, st>>>(g, *cons, 0, cfg->ncomp, scratch, g.zlo_noslip, g.zhi_noslip, 0);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ERF_B200_OK : ERF_B200_ECUDA;
 }
