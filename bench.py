@@ -253,6 +253,62 @@ def ensemble_arm(args, C, Dycore, Ensemble, stream, n_err=4):
             "rel_l2_mixed_vs_fp64_first_members": errs}
 
 
+def terrain_arm(args, C, Dycore, stream, n_err=100):
+    """Terrain-following ABL (static terrain, Deardorff): throughput of the
+    plain and mixed forms (graph replay, device-resident state) and the
+    mixed form's error against the plain form after n_err steps."""
+    import torch
+    from erf_b200 import terrain as T
+    case = T.abl_terrain(dt=0.25)
+    cfg = case.cfg
+    n_cells = cfg.nx * cfg.ny * cfg.nz
+    out = {"workload": f"terrain ABL {cfg.nx}x{cfg.ny}x{cfg.nz}, dx={cfg.dx:g} m, levels stretched from 5 m "
+                       f"(ratio 1.04, top {case.z_nd[-1, 0, 0]:.0f} m), 300 m hill + 20 m sinusoids, Deardorff, "
+                       f"dt={cfg.dt} s, {cfg.mri_ratio} substeps/RK stage 3",
+           "cells": n_cells}
+    base = init = None
+    res = {}
+    for prec, name in ((C.PREC_FP64, "fp64"), (C.PREC_MIXED, "mixed")):
+        c = cfg.copy()
+        c.precision = prec
+        dy = Dycore(c, stream=stream.cuda_stream)
+        dy.set_terrain(case.z_nd)
+        if base is None:
+            base = dy.make_base_state_terrain(case)
+            init = case.build_state(base[0])
+        dy.set_base_state(base)
+        dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in init]
+        torch.cuda.synchronize()
+        dy.advance(*dev, args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dy.advance(*dev, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        prof = dy.advance_profiled(*dev, 2)
+        kern = {k: {"launches": n, "ms_per_launch": t / n} for k, (t, n) in prof.items() if n}
+        out[name] = {"value": n_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                     "status": dy.status(), "kernels": kern}
+        # error run from the initial state
+        dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in init]
+        dy.advance(*dev, n_err)
+        torch.cuda.synchronize()
+        res[name] = [t.cpu().numpy() for t in dev]
+        out[name]["status_after_error_run"] = dy.status()
+        dy.close()
+
+    def rl2(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+    (c64, u64, v64, w64), (c32, u32, v32, w32) = res["fp64"], res["mixed"]
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["mixed"][f"rel_l2_vs_fp64_after_{n_err}_steps"] = {
+        "u": rl2(u32, u64), "v": rl2(v32, v64), "w": rl2(w32, w64),
+        "theta": rl2(c32[1] / c32[0], c64[1] / c64[0]), "tke": rl2(c32[2] / c32[0], c64[2] / c64[0])}
+    return out
+
+
 def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
     """Time the FP64 CPU oracle on a bounded sample of the workload."""
     import oracle
@@ -311,7 +367,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="moist_bubble", choices=sorted(cases.CASES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble"],
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble", "terrain"],
                     help="precision forms to time (the JSON line needs both; single forms are for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -484,6 +540,12 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return 0
+    if args.form == "terrain":
+        if rank == 0:
+            print(json.dumps({"form": "terrain", "terrain": terrain_arm(args, C, Dycore, stream)}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     if args.form == "learned":
         if rank == 0:
             print(json.dumps({"form": "learned", "learned": learned_arm(measure, form_error, C)}), flush=True)
@@ -505,6 +567,7 @@ def main():
     learned = learned_arm(measure, form_error, C) if rank == 0 else None
     from erf_b200.dycore import Ensemble
     ensemble = ensemble_arm(args, C, Dycore, Ensemble, stream) if rank == 0 else None
+    terrain_res = terrain_arm(args, C, Dycore, stream) if rank == 0 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -536,6 +599,7 @@ def main():
                       "rel_l2_vs_fp64_after_100_steps": mixed_err, "status": mixed["status"]},
             "learned": learned,
             "ensemble": ensemble,
+            "terrain": terrain_res,
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clock_samples),
             "gpu_launches": plain["launches"],
