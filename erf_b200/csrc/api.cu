@@ -291,8 +291,8 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         if (P.use_diff)
             TIMED(1, launch_ter_tau<R>(P, st, nrk, Sst.cons, Vnew[0], Vnew[1], Vnew[2], B.mut, B.ter, B.tke, B.t11,
                                        B.t22, B.t33, B.t12, B.t13, B.t23));
-        TIMED(2, launch_ter_slow_cell<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], B.mut, B.tke, B.Fcons, B.avx, B.avy,
-                                         B.avz));
+        TIMED(2, launch_ter_slow_cell<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], B.mut, B.tke, B.ter, B.Fcons, B.avx,
+                                         B.avy, B.avz));
         TIMED(4, launch_ter_slow_mom<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12, B.t13,
                                         B.t23, B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz));
         double facinv = 1.0 / (double)nsub;
@@ -308,7 +308,7 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                              B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, SUM.cons, SUM.mz));
         }
         TIMED(7, launch_ter_post<R>(P, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut, B.tke,
-                                    B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
+                                    B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
     }
 }
@@ -410,7 +410,9 @@ int alloc_bulk(erf_b200_ctx* c, Bulk<R>& B) {
         A(&B.ter.s11, N); A(&B.ter.s22, N); A(&B.ter.s33, N); A(&B.ter.s12, N); A(&B.ter.s13, NZF);
         A(&B.ter.s23, NZF); A(&B.ter.t31, NZF); A(&B.ter.t32, NZF);
         A(&B.ter.ndu, N); A(&B.ter.ndv, N); A(&B.ter.odu, N); A(&B.ter.odv, N);
-        if (rc == ERF_B200_OK) rc = dalloc(c, &B.ter.soln, (size_t)4 * (cfg->nz + 1) * cfg->nx * cfg->ny);
+        A(&B.ter.fx[0], N); A(&B.ter.fy[0], N); A(&B.ter.fx[1], N); A(&B.ter.fy[1], N);
+        auto D = [&](double** q, size_t n) { if (rc == ERF_B200_OK) rc = dalloc(c, q, n); };
+        D(&B.ter.tr0, N); D(&B.ter.tr1, N); D(&B.ter.om, NZF); D(&B.ter.sol, NZF);
     }
     return rc;
 }

@@ -71,7 +71,10 @@ struct TerBuf {
     R *s11, *s22, *s33, *s12, *s13, *s23;
     R *t31, *t32;
     R *ndu, *ndv, *odu, *odv;
-    double* soln;   // 4 (nz+1) per column
+    R *fx[2], *fy[2];            // raw diffusive face fluxes (two fields)
+    double *tr0, *tr1, *om, *sol;  // substep: horizontal rho / rho theta fluxes
+                                   // (cells), Omega of the old increments and
+                                   // the implicit solve (z faces)
 };
 
 // x-y tile of the transport kernels (slow_cell, slow_mom, post) and the
@@ -155,7 +158,8 @@ void launch_ter_tau(const Params& P, cudaStream_t st, int nrk, const double* con
                     R* t23);
 template <class R>
 void launch_ter_slow_cell(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
-                          const double* v, const R* mut, TkeBuf<R> tke, R* Fcons, R* avx, R* avy, R* avz);
+                          const double* v, const R* mut, TkeBuf<R> tke, TerBuf<R> T, R* Fcons, R* avx, R* avy,
+                          R* avz);
 template <class R>
 void launch_ter_slow_mom(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
                          const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,
@@ -172,6 +176,6 @@ void launch_ter_fast_vert(const Params& P, cudaStream_t st, double dtau, double 
 template <class R>
 void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
                      StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,
-                     const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
+                     TerBuf<R> T, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
 
 }  // namespace erfb

@@ -16,11 +16,12 @@
 //                     ground and the lid, cons_to_prim, eddy viscosity
 //   k_ter_strain /    make_tau_terms with terrain (ERF_make_tau_terms.cpp:
 //   k_ter_stress      177-317, ComputeStrain_T, ComputeStressVarVisc_T)
+//   k_ter_rawflux     raw diffusive face fluxes (shared by the cross terms)
 //   k_ter_slow_cell   rho / rho*theta slow RHS with face areas and detJ
 //   k_ter_slow_mom    AdvectionSrcForMom_T, DiffusionSrcForMom_T, terrain
 //                     pressure gradient, sources
-//   k_ter_fast_h /    erf_fast_rhs_T (TimeIntegration/ERF_fast_rhs_T.cpp)
-//   k_ter_fast_vert
+//   k_ter_fast_h,     erf_fast_rhs_T (TimeIntegration/ERF_fast_rhs_T.cpp)
+//   k_ter_fv_*
 //   k_ter_post        erf_slow_rhs_post with terrain and the stage's
 //                     boundary round trips
 #include "kernels.cuh"
@@ -655,6 +656,8 @@ struct DiffT {
     const R* mut;
     const R* kv;
     double ae, fac;
+    const R* fxr = nullptr;   // raw face fluxes from k_ter_rawflux, when given
+    const R* fyr = nullptr;
     __device__ double p(int i, int j, int k) const { return ccw(phi, P.g, i, j, k); }
     __device__ double mu(int i, int j, int k) const { return ccw(mut, P.g, i, j, k) * fac; }
     __device__ double xraw(int i, int j, int k) const {
@@ -675,6 +678,14 @@ struct DiffT {
         double GradCy = g.dyi * (p(i, j, k) - p(i, j - 1, k));
         return -rA * 1.0 * (GradCy - (meta / mz) * GradCz);
     }
+    __device__ double xr(int i, int j, int k) const {
+        if (fxr) return double(fxr[cidx(P.g, wrap(i, P.g.nx), wrap(j, P.g.ny), k)]);
+        return xraw(i, j, k);
+    }
+    __device__ double yr(int i, int j, int k) const {
+        if (fyr) return double(fyr[cidx(P.g, wrap(i, P.g.nx), wrap(j, P.g.ny), k)]);
+        return yraw(i, j, k);
+    }
     // z-face flux (k in [0, nz]); raw receives the flux before the cross terms
     __device__ double zflux(int i, int j, int k, double& raw) const {
         const Geo& g = P.g;
@@ -689,18 +700,18 @@ struct DiffT {
         raw = fz;
         double mxi = hxi_K(P, i, j, k), meta = heta_K(P, i, j, k), xb, yb;
         if (k == 0) {
-            double xlo = 0.5 * (xraw(i, j, k) + xraw(i + 1, j, k)), xhi = 0.5 * (xraw(i, j, k + 1) + xraw(i + 1, j, k + 1));
+            double xlo = 0.5 * (xr(i, j, k) + xr(i + 1, j, k)), xhi = 0.5 * (xr(i, j, k + 1) + xr(i + 1, j, k + 1));
             xb = 1.5 * xlo - 0.5 * xhi;
-            double ylo = 0.5 * (yraw(i, j, k) + yraw(i, j + 1, k)), yhi = 0.5 * (yraw(i, j, k + 1) + yraw(i, j + 1, k + 1));
+            double ylo = 0.5 * (yr(i, j, k) + yr(i, j + 1, k)), yhi = 0.5 * (yr(i, j, k + 1) + yr(i, j + 1, k + 1));
             yb = 1.5 * ylo - 0.5 * yhi;
         } else if (k == nz) {
-            double xlo = 0.5 * (xraw(i, j, k - 2) + xraw(i + 1, j, k - 2)), xhi = 0.5 * (xraw(i, j, k - 1) + xraw(i + 1, j, k - 1));
+            double xlo = 0.5 * (xr(i, j, k - 2) + xr(i + 1, j, k - 2)), xhi = 0.5 * (xr(i, j, k - 1) + xr(i + 1, j, k - 1));
             xb = 1.5 * xhi - 0.5 * xlo;
-            double ylo = 0.5 * (yraw(i, j, k - 2) + yraw(i, j + 1, k - 2)), yhi = 0.5 * (yraw(i, j, k - 1) + yraw(i, j + 1, k - 1));
+            double ylo = 0.5 * (yr(i, j, k - 2) + yr(i, j + 1, k - 2)), yhi = 0.5 * (yr(i, j, k - 1) + yr(i, j + 1, k - 1));
             yb = 1.5 * yhi - 0.5 * ylo;
         } else {
-            xb = 0.25 * (xraw(i, j, k) + xraw(i + 1, j, k) + xraw(i, j, k - 1) + xraw(i + 1, j, k - 1));
-            yb = 0.25 * (yraw(i, j, k) + yraw(i, j + 1, k) + yraw(i, j, k - 1) + yraw(i, j + 1, k - 1));
+            xb = 0.25 * (xr(i, j, k) + xr(i + 1, j, k) + xr(i, j, k - 1) + xr(i + 1, j, k - 1));
+            yb = 0.25 * (yr(i, j, k) + yr(i, j + 1, k) + yr(i, j, k - 1) + yr(i, j + 1, k - 1));
         }
         fz -= mxi * xb + meta * yb;
         return fz;
@@ -708,8 +719,8 @@ struct DiffT {
     // divergence over detJ (the amount the reference subtracts from the RHS)
     __device__ double div(int i, int j, int k, double& raw_lo, double& raw_hi) const {
         const Geo& g = P.g;
-        double fxl = xraw(i, j, k) * hzeta_I(P, i, j, k), fxh = xraw(i + 1, j, k) * hzeta_I(P, i + 1, j, k);
-        double fyl = yraw(i, j, k) * hzeta_J(P, i, j, k), fyh = yraw(i, j + 1, k) * hzeta_J(P, i, j + 1, k);
+        double fxl = xr(i, j, k) * hzeta_I(P, i, j, k), fxh = xr(i + 1, j, k) * hzeta_I(P, i + 1, j, k);
+        double fyl = yr(i, j, k) * hzeta_J(P, i, j, k), fyh = yr(i, j + 1, k) * hzeta_J(P, i, j + 1, k);
         double fzl = zflux(i, j, k, raw_lo), fzh = zflux(i, j, k + 1, raw_hi);
         double s = (fxh - fxl) * g.dxi * 1.0 + (fyh - fyl) * g.dyi * 1.0 + (fzh - fzl) * g.dzi;
         return s / detJ_at(P, i, j, k);
@@ -758,6 +769,31 @@ __device__ double interp_dir(int dir, int i, int j, int k, FP phi, int type, dou
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Raw diffusive face fluxes of DiffusionSrcForState_T (before the cross
+// terms and the h_zeta scaling) for up to two fields, one thread per cell
+// writing its low x and y faces, so that the z-face cross terms read them
+// instead of re-evaluating them.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_ter_rawflux(Params P, const double* __restrict__ rho, const R* __restrict__ mut,
+                              const R* __restrict__ phiA, double aeA, double facA, R* __restrict__ fxA,
+                              R* __restrict__ fyA, const R* __restrict__ phiB, double aeB, double facB,
+                              R* __restrict__ fxB, R* __restrict__ fyB) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    int64_t c = cidx(g, i, j, k);
+    DiffT<R> A{P, rho, phiA, mut, nullptr, aeA, facA};
+    fxA[c] = R(A.xraw(i, j, k));
+    fyA[c] = R(A.yraw(i, j, k));
+    if (phiB) {
+        DiffT<R> B{P, rho, phiB, mut, nullptr, aeB, facB};
+        fxB[c] = R(B.xraw(i, j, k));
+        fyB[c] = R(B.yraw(i, j, k));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Slow RHS of rho and rho*theta with terrain (ERF_slow_rhs_pre.cpp:365-500):
 // Omega, AdvectionSrcForRho with the face areas (ax = h_zeta at x faces,
 // ay likewise, az = 1) over detJ, the average momenta, theta advection with
@@ -765,7 +801,7 @@ __device__ double interp_dir(int dir, int i, int j, int k, FP phi, int type, dou
 // ---------------------------------------------------------------------------
 template <class R>
 __global__ void k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
-                                const double* __restrict__ v, const R* __restrict__ mut, TkeBuf<R> tke,
+                                const double* __restrict__ v, const R* __restrict__ mut, TkeBuf<R> tke, TerBuf<R> T,
                                 R* __restrict__ Fcons, R* __restrict__ avx, R* __restrict__ avy, R* __restrict__ avz) {
     const Geo& g = P.g;
     int i, j, k;
@@ -797,7 +833,7 @@ __global__ void k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const doubl
     double frt = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
     if (P.use_diff) {
         const bool dd = P.les == ERF_LES_DEARDORFF;
-        DiffT<R> D{P, S.cons, A.prim, mut, dd ? tke.kthv : nullptr, P.alphaT_eff, P.invPr};
+        DiffT<R> D{P, S.cons, A.prim, mut, dd ? tke.kthv : nullptr, P.alphaT_eff, P.invPr, T.fx[0], T.fy[0]};
         double rlo, rhi;
         frt -= D.div(i, j, k, rlo, rhi);
         if (dd) {
@@ -1107,67 +1143,66 @@ __global__ void k_ter_fast_h(Params P, int step, double dtau, double facinv, Sta
 
 // ---------------------------------------------------------------------------
 // Acoustic substep with terrain, vertical part (ERF_fast_rhs_T.cpp:320-680),
-// one thread per column: horizontal rho / rho*theta fluxes through the
-// sloping faces, Omega of the previous increments, the detJ-weighted
-// implicit system for Omega'' (coefficients from the stage), w'' from
-// Omega'' and the new horizontal increments, vertical fluxes, average
-// contravariant momentum, rho and rho*theta.  The previous top z-momentum is
-// the one the boundary fill leaves (w from Omega = 0 at the lid).
+// in four passes so that only the Thomas sweep is serial in k:
+//   k_ter_fv_prep    horizontal rho / rho*theta fluxes through the sloping
+//                    faces (cells) and Omega of the previous increments
+//                    (faces; the previous top z-momentum is the one the
+//                    boundary fill leaves: w from Omega = 0 at the lid);
+//   k_ter_fv_rhs     the detJ-weighted right-hand side of the Omega'' system;
+//   k_ter_fv_solve   forward elimination / back substitution per column on
+//                    the stage's coefficients (plane-major, coalesced);
+//   k_ter_fv_update  w'' from Omega'' and the new increments, vertical fluxes,
+//                    average contravariant momentum, rho and rho*theta.
 // ---------------------------------------------------------------------------
+namespace {
 template <class R>
-__global__ void k_ter_fast_vert(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
-                                int prev_rt, StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons,
-                                const R* __restrict__ Fmz, TerBuf<R> T, const R* __restrict__ cA,
-                                const R* __restrict__ cInvB, const R* __restrict__ cCB, const R* __restrict__ cP,
-                                const R* __restrict__ cQ, R* __restrict__ avz, double* out_cons, double* out_mz) {
+__device__ double prev_mz_ter(const Params& P, StateBuf Sprev, int prev_rt, int i, int j, int k) {
     const Geo& g = P.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.nx || j >= g.ny) return;
     const int nz = g.nz;
-    const int64_t N = g.ncell, sk = g.sk, col = (int64_t)j * g.nx + i;
-    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi, halfg = P.halfg;
-    // per-column scratch: soln, omega, trhs0, trhs1 (nz+1 each)
-    double* sol = T.soln + col * 4 * (int64_t)(nz + 1);
-    double* om = sol + (nz + 1);
-    double* tr0 = om + (nz + 1);
-    double* tr1 = tr0 + (nz + 1);
+    int64_t f = cidx(g, i, j, k);
+    double m = Sprev.mz[f];
+    if (!prev_rt) return m;
+    if (k == 0 || k == nz) {
+        auto U1 = [&](int ii, int jj, int kk) {
+            if (kk >= nz) {
+                if (g.zhi_noslip) return 0.0;
+                kk = nz - 1;
+            }
+            return rt_u(g, Sprev.cons, Sprev.mx, ii, jj, kk);
+        };
+        auto V1 = [&](int ii, int jj, int kk) {
+            if (kk >= nz) {
+                if (g.zhi_noslip) return 0.0;
+                kk = nz - 1;
+            }
+            return rt_v(g, Sprev.cons, Sprev.my, ii, jj, kk);
+        };
+        int kc = (k == 0) ? 0 : nz - 1;
+        double r = Sprev.cons[cidx(g, i, j, kc)];
+        double wb = w_from_omega(P, i, j, k, 0.0, U1, V1);
+        return (wb * 0.5) * (r + r);
+    }
+    double rs = Sprev.cons[f] + Sprev.cons[f - g.sk];
+    double wt = (m * 2.0) / rs;
+    return (wt * 0.5) * rs;
+}
+}  // namespace
+
+template <class R>
+__global__ void k_ter_fv_prep(Params P, StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, TerBuf<R> T) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int nz = g.nz;
+    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
     auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
     auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto ODU = [&](int ii, int jj, int kk) { return double(T.odu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto ODV = [&](int ii, int jj, int kk) { return double(T.odv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto Z = [&](int a, int b, int cc) { return Zn(P, a, b, cc); };
-    // previous z-momentum as the boundary fill leaves it
-    auto prev_mz = [&](int k) {
-        int64_t f = (int64_t)k * sk + col;
-        double m = Sprev.mz[f];
-        if (!prev_rt) return m;
-        if (k == 0 || k == nz) {
-            auto U1 = [&](int ii, int jj, int kk) {
-                if (kk >= nz) {
-                    if (g.zhi_noslip) return 0.0;
-                    kk = nz - 1;
-                }
-                return rt_u(g, Sprev.cons, Sprev.mx, ii, jj, kk);
-            };
-            auto V1 = [&](int ii, int jj, int kk) {
-                if (kk >= nz) {
-                    if (g.zhi_noslip) return 0.0;
-                    kk = nz - 1;
-                }
-                return rt_v(g, Sprev.cons, Sprev.my, ii, jj, kk);
-            };
-            int kc = (k == 0) ? 0 : nz - 1;
-            double r = Sprev.cons[(int64_t)kc * sk + col];
-            double wb = w_from_omega(P, i, j, k, 0.0, U1, V1);
-            return (wb * 0.5) * (r + r);
-        }
-        double rs = Sprev.cons[f] + Sprev.cons[f - sk];
-        double wt = (m * 2.0) / rs;
-        return (wt * 0.5) * rs;
-    };
-    // horizontal fluxes of rho and rho theta
-    for (int k = 0; k < nz; ++k) {
+    int64_t f = cidx(g, i, j, k);
+    if (k < nz) {
         double hxh = 0.5 * dzi * (Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j, k) - Z(i + 1, j + 1, k));
         double hxl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
         double hyh = 0.5 * dzi * (Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
@@ -1176,78 +1211,111 @@ __global__ void k_ter_fast_vert(Params P, double dtau, double facinv, double bet
         double yl = NDV(i, j, k) * hyl / 1.0, yh = NDV(i, j + 1, k) * hyh / 1.0;
         double mfsq = 1.0;
         double tc = th(i, j, k);
-        tr0[k] = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
-        tr1[k] = ((xh * (tc + th(i + 1, j, k)) - xl * (tc + th(i - 1, j, k))) * dxi * mfsq +
-                  (yh * (tc + th(i, j + 1, k)) - yl * (tc + th(i, j - 1, k))) * dyi * mfsq) * 0.5;
+        T.tr0[f] = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
+        T.tr1[f] = ((xh * (tc + th(i + 1, j, k)) - xl * (tc + th(i - 1, j, k))) * dxi * mfsq +
+                    (yh * (tc + th(i, j + 1, k)) - yl * (tc + th(i, j - 1, k))) * dyi * mfsq) * 0.5;
     }
-    // Omega of the previous increments
-    for (int k = 0; k <= nz; ++k) {
-        double odw = prev_mz(k) - Sst.mz[(int64_t)k * sk + col];
-        if (k == 0) om[k] = 0.;
-        else if (k == nz) om[k] = odw;
-        else om[k] = omega_from_w(P, i, j, k, odw, ODU, ODV);
+    double odw = prev_mz_ter<R>(P, Sprev, prev_rt, i, j, k) - Sst.mz[f];
+    double om;
+    if (k == 0) om = 0.;
+    else if (k == nz) om = odw;
+    else om = omega_from_w(P, i, j, k, odw, ODU, ODV);
+    T.om[f] = om;
+}
+
+template <class R>
+__global__ void k_ter_fv_rhs(Params P, double dtau, double beta_1, double beta_2, StateBuf Sprev, int prev_rt,
+                             StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons, const R* __restrict__ Fmz,
+                             TerBuf<R> T, const R* __restrict__ cP, const R* __restrict__ cQ) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell, sk = g.sk;
+    const double dzi = g.dzi, halfg = P.halfg;
+    int64_t f = cidx(g, i, j, k);
+    if (k == 0 || k == nz) {
+        T.sol[f] = dtau * double(Fmz[f]);
+        return;
     }
-    // right-hand side and forward elimination
-    {
-        int64_t f0 = col;
-        double s = (dtau * double(Fmz[f0])) * double(cInvB[f0]);
-        sol[0] = s;
-        for (int k = 1; k <= nz; ++k) {
-            int64_t f = (int64_t)k * sk + col;
-            double rhs;
-            if (k == nz) {
-                rhs = dtau * double(Fmz[f]);
-            } else {
-                int64_t cm = f - sk;
-                double Jk = detJ_at(P, i, j, k), Jkm = detJ_at(P, i, j, k - 1);
-                double dJk = 0.5 * (Jk + Jkm);
-                double cPk = double(cP[f]), cQk = double(cQ[f]);
-                double tlo = 0.5 * (th(i, j, k - 2) + th(i, j, k - 1));
-                double tmid = 0.5 * (th(i, j, k - 1) + th(i, j, k));
-                double thi = 0.5 * (th(i, j, k) + th(i, j, k + 1));
-                double odr_k = Sprev.cons[f] - Sst.cons[f], odr_km = Sprev.cons[cm] - Sst.cons[cm];
-                double odrt_k = Sprev.cons[N + f] - Sst.cons[N + f], odrt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
-                double R0t = (-halfg * odr_k + cPk * odrt_k) * Jk + (-halfg * odr_km + cQk * odrt_km) * Jkm;
-                double R1t = -halfg * (double(Fcons[f]) * Jk + double(Fcons[cm]) * Jkm)
-                             + (cPk * double(Fcons[N + f]) * Jk + cQk * double(Fcons[N + cm]) * Jkm);
-                double Okp1 = om[k + 1], Ok = om[k], Okm1 = om[k - 1];
-                R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + tr0[k] + tr0[k - 1]);
-                R1t += -(cPk * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + tr1[k]) +
-                         cQk * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + tr1[k - 1]));
-                double odw = prev_mz(k) - Sst.mz[f];
-                rhs = dJk * odw + dtau * (dJk * double(Fmz[f]) + R0t + dtau * beta_2 * R1t);
-                rhs += dJk * omega_from_w(P, i, j, k, 0., NDU, NDV);
-            }
-            s = (rhs - double(cA[f]) * s) * double(cInvB[f]);
-            sol[k] = s;
-        }
-        for (int k = nz - 1; k >= 0; --k) {
-            int64_t f = (int64_t)k * sk + col;
-            s = sol[k] - double(cCB[f]) * s;
-            sol[k] = s;
-        }
-    }
-    // z-momentum, vertical fluxes, rho and rho theta
-    for (int k = 0; k <= nz; ++k) {
+    auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
+    auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    int64_t cm = f - sk;
+    double Jk = detJ_at(P, i, j, k), Jkm = detJ_at(P, i, j, k - 1);
+    double dJk = 0.5 * (Jk + Jkm);
+    double cPk = double(cP[f]), cQk = double(cQ[f]);
+    double tlo = 0.5 * (th(i, j, k - 2) + th(i, j, k - 1));
+    double tmid = 0.5 * (th(i, j, k - 1) + th(i, j, k));
+    double thi = 0.5 * (th(i, j, k) + th(i, j, k + 1));
+    double odr_k = Sprev.cons[f] - Sst.cons[f], odr_km = Sprev.cons[cm] - Sst.cons[cm];
+    double odrt_k = Sprev.cons[N + f] - Sst.cons[N + f], odrt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
+    double R0t = (-halfg * odr_k + cPk * odrt_k) * Jk + (-halfg * odr_km + cQk * odrt_km) * Jkm;
+    double R1t = -halfg * (double(Fcons[f]) * Jk + double(Fcons[cm]) * Jkm)
+                 + (cPk * double(Fcons[N + f]) * Jk + cQk * double(Fcons[N + cm]) * Jkm);
+    double Okp1 = T.om[f + sk], Ok = T.om[f], Okm1 = T.om[cm];
+    R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + T.tr0[f] + T.tr0[cm]);
+    R1t += -(cPk * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + T.tr1[f]) +
+             cQk * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + T.tr1[cm]));
+    double odw = prev_mz_ter<R>(P, Sprev, prev_rt, i, j, k) - Sst.mz[f];
+    double rhs = dJk * odw + dtau * (dJk * double(Fmz[f]) + R0t + dtau * beta_2 * R1t);
+    rhs += dJk * omega_from_w(P, i, j, k, 0., NDU, NDV);
+    T.sol[f] = rhs;
+}
+
+template <class R>
+__global__ void k_ter_fv_solve(Params P, TerBuf<R> T, const R* __restrict__ cA, const R* __restrict__ cInvB,
+                               const R* __restrict__ cCB) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const int nz = g.nz;
+    const int64_t sk = g.sk, col = (int64_t)j * g.nx + i;
+    double* sol = T.sol;
+    double s = sol[col] * double(cInvB[col]);
+    sol[col] = s;
+    for (int k = 1; k <= nz; ++k) {
         int64_t f = (int64_t)k * sk + col;
-        double m = Sst.mz[f];
-        if (k >= 1 && k <= nz - 1) m += w_from_omega(P, i, j, k, sol[k], NDU, NDV);
-        out_mz[f] = m;
+        s = (sol[f] - double(cA[f]) * s) * double(cInvB[f]);
+        sol[f] = s;
     }
-    for (int k = 0; k < nz; ++k) {
-        int64_t c = (int64_t)k * sk + col;
-        double zl = beta_2 * sol[k] + beta_1 * om[k];
-        double zh = beta_2 * sol[k + 1] + beta_1 * om[k + 1];
-        avz[c] += R(facinv * zl / (1.0 * 1.0));
-        if (k == nz - 1) avz[c + sk] += R(facinv * zh / (1.0 * 1.0));
-        double Jc = detJ_at(P, i, j, k);
-        double tc = th(i, j, k);
-        double frho = -(tr0[k] + (zh - zl) * dzi) / Jc;
-        double frt = -(tr1[k] + 0.5 * (zh * (tc + th(i, j, k + 1)) - zl * (tc + th(i, j, k - 1))) * dzi) / Jc;
-        double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
-        out_cons[c] = pr + dtau * (double(Fcons[c]) + frho);
-        out_cons[N + c] = prt + dtau * (double(Fcons[N + c]) + frt);
+    for (int k = nz - 1; k >= 0; --k) {
+        int64_t f = (int64_t)k * sk + col;
+        s = sol[f] - double(cCB[f]) * s;
+        sol[f] = s;
     }
+}
+
+template <class R>
+__global__ void k_ter_fv_update(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
+                                StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons, TerBuf<R> T,
+                                R* __restrict__ avz, double* out_cons, double* out_mz) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell, sk = g.sk;
+    const double dzi = g.dzi;
+    auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
+    auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
+    int64_t f = cidx(g, i, j, k);
+    double m = Sst.mz[f];
+    if (k >= 1 && k <= nz - 1) m += w_from_omega(P, i, j, k, T.sol[f], NDU, NDV);
+    out_mz[f] = m;
+    if (k == nz) return;
+    int64_t c = f;
+    double zl = beta_2 * T.sol[c] + beta_1 * T.om[c];
+    double zh = beta_2 * T.sol[c + sk] + beta_1 * T.om[c + sk];
+    avz[c] += R(facinv * zl / (1.0 * 1.0));
+    if (k == nz - 1) avz[c + sk] += R(facinv * zh / (1.0 * 1.0));
+    double Jc = detJ_at(P, i, j, k);
+    double tc = th(i, j, k);
+    double frho = -(T.tr0[c] + (zh - zl) * dzi) / Jc;
+    double frt = -(T.tr1[c] + 0.5 * (zh * (tc + th(i, j, k + 1)) - zl * (tc + th(i, j, k - 1))) * dzi) / Jc;
+    double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
+    out_cons[c] = pr + dtau * (double(Fcons[c]) + frho);
+    out_cons[N + c] = prt + dtau * (double(Fcons[N + c]) + frt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1262,7 +1330,7 @@ __global__ void k_ter_fast_vert(Params P, double dtau, double facinv, double bet
 template <class R>
 __global__ void k_ter_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
                            StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* __restrict__ mut,
-                           TkeBuf<R> tke, const R* __restrict__ avx, const R* __restrict__ avy,
+                           TkeBuf<R> tke, TerBuf<R> T, const R* __restrict__ avx, const R* __restrict__ avy,
                            const R* __restrict__ avz, double* __restrict__ un, double* __restrict__ vn,
                            double* __restrict__ wn) {
     const Geo& g = P.g;
@@ -1290,7 +1358,8 @@ __global__ void k_ter_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst
         double invdetJ = 1. / Jc;
         double r = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
         if (P.use_diff) {
-            DiffT<R> D{P, Sst.cons, phi, mut, nullptr, q == 0 ? P.alphaC_eff : 0.0, q == 0 ? P.invSc : P.invSigmaK};
+            DiffT<R> D{P, Sst.cons, phi, mut, nullptr, q == 0 ? P.alphaC_eff : 0.0, q == 0 ? P.invSc : P.invSigmaK,
+                       T.fx[q], T.fy[q]};
             double rlo, rhi;
             r -= D.div(i, j, k, rlo, rhi);
         }
@@ -1377,8 +1446,14 @@ void launch_ter_tau(const Params& P, cudaStream_t st, int nrk, const double* con
 }
 template <class R>
 void launch_ter_slow_cell(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
-                          const double* v, const R* mut, TkeBuf<R> tke, R* Fcons, R* avx, R* avy, R* avz) {
-    k_ter_slow_cell<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S, A, u, v, mut, tke, Fcons, avx, avy, avz);
+                          const double* v, const R* mut, TkeBuf<R> tke, TerBuf<R> T, R* Fcons, R* avx, R* avy,
+                          R* avz) {
+    if (P.use_diff)
+        k_ter_rawflux<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S.cons, mut, A.prim, P.alphaT_eff, P.invPr,
+                                                                        T.fx[0], T.fy[0], nullptr, 0.0, 0.0, nullptr,
+                                                                        nullptr);
+    k_ter_slow_cell<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S, A, u, v, mut, tke, T, Fcons, avx, avy,
+                                                                      avz);
 }
 template <class R>
 void launch_ter_slow_mom(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
@@ -1399,16 +1474,27 @@ void launch_ter_fast_vert(const Params& P, cudaStream_t st, double dtau, double 
                           StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmz,
                           TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz,
                           double* out_cons, double* out_mz) {
-    dim3 b(32, 4, 1), gr((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1);
-    k_ter_fast_vert<R><<<gr, b, 0, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, prev_rt, Sst, A, Fcons, Fmz, T, cA,
-                                         cInvB, cCB, cP, cQ, avz, out_cons, out_mz);
+    dim3 b = ter_block(), gf = ter_grid(P.g, P.g.nz + 1), gc((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1);
+    k_ter_fv_prep<R><<<gf, b, 0, st>>>(P, Sprev, prev_rt, Sst, A, T);
+    k_ter_fv_rhs<R><<<gf, b, 0, st>>>(P, dtau, beta_1, beta_2, Sprev, prev_rt, Sst, A, Fcons, Fmz, T, cP, cQ);
+    k_ter_fv_solve<R><<<gc, b, 0, st>>>(P, T, cA, cInvB, cCB);
+    k_ter_fv_update<R><<<gf, b, 0, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, Sst, A, Fcons, T, avz, out_cons,
+                                         out_mz);
 }
 template <class R>
 void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
                      StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,
-                     const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
+                     TerBuf<R> T, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
+    if (P.use_diff) {
+        const int64_t N = P.g.ncell;
+        const bool dd = P.les == ERF_LES_DEARDORFF;
+        k_ter_rawflux<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(
+            P, Sst.cons, mut, Acur.prim + (int64_t)(ERF_RHOSCALAR_COMP - 1) * N, P.alphaC_eff, P.invSc, T.fx[0],
+            T.fy[0], dd ? Acur.prim + (int64_t)(ERF_RHOKE_COMP - 1) * N : nullptr, 0.0, P.invSigmaK, T.fx[1],
+            T.fy[1]);
+    }
     k_ter_post<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, slow_dt, Sold, Sst, Ssum, Snew, Acur, Anext,
-                                                                 make_next, mut, tke, avx, avy, avz, un, vn, wn);
+                                                                 make_next, mut, tke, T, avx, avy, avz, un, vn, wn);
 }
 
 #define ERFB_TER_INSTANTIATE(R)                                                                                     \
@@ -1418,7 +1504,7 @@ void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf 
     template void launch_ter_tau<R>(const Params&, cudaStream_t, int, const double*, const double*, const double*,   \
                                     const double*, const R*, TerBuf<R>, TkeBuf<R>, R*, R*, R*, R*, R*, R*);          \
     template void launch_ter_slow_cell<R>(const Params&, cudaStream_t, StateBuf, StageAux<R>, const double*,         \
-                                          const double*, const R*, TkeBuf<R>, R*, R*, R*, R*);                       \
+                                          const double*, const R*, TkeBuf<R>, TerBuf<R>, R*, R*, R*, R*);            \
     template void launch_ter_slow_mom<R>(const Params&, cudaStream_t, StateBuf, StageAux<R>, const double*,          \
                                          const double*, const double*, const R*, const R*, const R*, const R*,       \
                                          const R*, const R*, TerBuf<R>, const R*, R*, R*, R*);                       \
@@ -1429,8 +1515,8 @@ void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf 
                                           int, StateBuf, StageAux<R>, const R*, const R*, TerBuf<R>, const R*,       \
                                           const R*, const R*, const R*, const R*, R*, double*, double*);             \
     template void launch_ter_post<R>(const Params&, cudaStream_t, double, StateBuf, StateBuf, StateBuf, StateBuf,    \
-                                     StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, const R*, const R*,         \
-                                     const R*, double*, double*, double*);
+                                     StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, TerBuf<R>, const R*,        \
+                                     const R*, const R*, double*, double*, double*);
 
 ERFB_TER_INSTANTIATE(double)
 ERFB_TER_INSTANTIATE(float)
