@@ -721,7 +721,26 @@ int erf_b200_advance_host(erf_b200_ctx* c, double* cons, double* u, double* v, d
     double* du = dc + ncons;
     double* dv = du + nu;
     double* dw = dv + nv;
-    CK(cudaMemcpyAsync(dc, cons, ncons * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    // Components the configuration neither reads nor changes (rho*KE without
+    // Deardorff, rho*QKE always: no PBL scheme on this path) keep their host
+    // values and are not copied; the others move as contiguous runs.
+    const int64_t ncell = nx * ny * nz;
+    auto live = [&](int n) { return !(n == ERF_RHOQKE_COMP || (n == ERF_RHOKE_COMP && f.les_type != ERF_LES_DEARDORFF)); };
+    auto copy_cons = [&](bool to_device) -> int {
+        for (int n0 = 0; n0 < nc;) {
+            if (!live(n0)) { ++n0; continue; }
+            int n1 = n0;
+            while (n1 < nc && live(n1)) ++n1;
+            size_t off = (size_t)n0 * ncell, cnt = (size_t)(n1 - n0) * ncell;
+            cudaError_t e = to_device ? cudaMemcpyAsync(dc + off, cons + off, cnt * sizeof(double), cudaMemcpyHostToDevice, c->stream)
+                                      : cudaMemcpyAsync(cons + off, dc + off, cnt * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+            if (e != cudaSuccess) return cuda_fail(e);
+            n0 = n1;
+        }
+        return ERF_B200_OK;
+    };
+    int crc = copy_cons(true);
+    if (crc) return crc;
     CK(cudaMemcpyAsync(du, u, nu * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(dv, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(dw, w, nw * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -736,7 +755,8 @@ int erf_b200_advance_host(erf_b200_ctx* c, double* cons, double* u, double* v, d
                  fv = mk(dv, nx - 1, ny, nz - 1, 1), fw = mk(dw, nx - 1, ny - 1, nz, 1);
     int rc = erf_b200_advance(c, &fc, &fu, &fv, &fw, nsteps);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(cons, dc, ncons * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    crc = copy_cons(false);
+    if (crc) return crc;
     CK(cudaMemcpyAsync(u, du, nu * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(v, dv, nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(w, dw, nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

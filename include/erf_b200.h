@@ -246,7 +246,9 @@ int erf_b200_advance(erf_b200_ctx* ctx,
 
 /* Same as erf_b200_advance with host buffers: copies in, advances, copies out.
  * Host arrays are dense valid-region arrays (no ghosts), i fastest:
- * cons[ncomp][nz][ny][nx], u[nz][ny][nx+1], v[nz][ny+1][nx], w[nz+1][ny][nx]. */
+ * cons[ncomp][nz][ny][nx], u[nz][ny][nx+1], v[nz][ny+1][nx], w[nz+1][ny][nx].
+ * Components the step neither reads nor changes (rho*QKE, and rho*KE unless
+ * les_type is ERF_LES_DEARDORFF) are left in place on the host, uncopied. */
 int erf_b200_advance_host(erf_b200_ctx* ctx, double* cons, double* u,
                           double* v, double* w, int nsteps);
 
