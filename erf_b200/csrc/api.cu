@@ -884,7 +884,7 @@ extern "C" {
 int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, const erf_b200_fab* yvel,
                                  const erf_b200_fab* zvel, const erf_b200_fab* cons) {
     if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
-    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
+    if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
         return ERF_B200_EINVAL;
@@ -895,6 +895,12 @@ int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, cons
         return rc;
     // the step prologue forms the eddy viscosity from these velocities (its
     // other outputs go to scratch slots of the context)
+    if (c->P.ter) {   // ComputeStrain_T + the terrain filter width
+        launch_ter_step_begin<double>(c->P, c->stream, c->S[0].cons, c->vel[0][0], c->vel[0][1], c->vel[0][2],
+                                      c->S[1], c->vel[1][0], c->vel[1][1], c->vel[1][2], c->bd.aux[1], c->bd.mut,
+                                      c->bd.tke);
+        return cuda_fail(cudaGetLastError());
+    }
     launch_step_begin<double>(c->P, c->stream, c->S[0].cons, c->vel[0][0], c->vel[0][1], c->vel[0][2], c->S[1],
                               c->vel[1][0], c->vel[1][1], c->vel[1][2], c->bd.aux[1], c->bd.mut, c->bd.tke);
     return cuda_fail(cudaGetLastError());
@@ -903,9 +909,9 @@ int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, cons
 int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b200_fab* S_rhs,
                           const erf_b200_fab* S_data, const erf_b200_fab* S_scratch, const erf_b200_fab* xvel,
                           const erf_b200_fab* yvel, const erf_b200_fab* zvel) {
-    (void)nrk; (void)slow_dt;
-    if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
-    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
+    (void)slow_dt;
+    if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
+    if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
     if (c->P.les == ERF_LES_MLP && !c->net) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
@@ -922,6 +928,18 @@ int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b2
         return rc;
     cudaStream_t st = c->stream;
     launch_stage_aux<double>(P, st, Sst.cons, B.aux[0]);
+    if (P.ter) {   // terrain passes; S_scratch's z-momentum receives Omega (avg_zmom)
+        if (P.use_diff)
+            launch_ter_tau<double>(P, st, nrk, Sst.cons, V[0], V[1], V[2], B.mut, B.ter, B.tke, B.t11, B.t22, B.t33,
+                                   B.t12, B.t13, B.t23);
+        launch_ter_slow_cell<double>(P, st, Sst, B.aux[0], V[0], V[1], B.mut, B.tke, B.ter, B.Fcons, B.avx, B.avy,
+                                     B.avz);
+        launch_ter_slow_mom<double>(P, st, Sst, B.aux[0], V[0], V[1], V[2], B.t11, B.t22, B.t33, B.t12, B.t13, B.t23,
+                                    B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz);
+        if ((rc = unpack4(c, S_rhs, 2, B.Fcons, B.Fmx, B.Fmy, B.Fmz))) return rc;
+        if ((rc = unpack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
+        return cuda_fail(cudaGetLastError());
+    }
     if (P.les == ERF_LES_MLP) {
         ClosureNet net{c->net->wpack, c->net->bias, c->net->norm, c->net->env, c->fallback};
         launch_closure<double>(P, net, c->closure_grid, st, Sst.cons, V[0], V[1], V[2], B.aux[0].prim, B.t11, B.t22,
@@ -942,7 +960,7 @@ int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b2
 int erf_b200_make_fast_coeffs(erf_b200_ctx* c, const erf_b200_fab* fast_coeffs, const erf_b200_fab* S_stage,
                               double dtau) {
     if (!c || c->mixed || !c->base_set || !fast_coeffs) return ERF_B200_EINVAL;
-    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
+    if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     if (!fab4_ok(S_stage, g, c->cfg.ncomp) || !fab_ok(fast_coeffs, 3, g, 5)) return ERF_B200_EINVAL;
     StateBuf Sst = c->S[2];
@@ -958,11 +976,16 @@ int erf_b200_make_fast_coeffs(erf_b200_ctx* c, const erf_b200_fab* fast_coeffs, 
     return cuda_fail(cudaGetLastError());
 }
 
-int erf_b200_fast_rhs_N(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* S_slow_rhs,
-                        const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
-                        const erf_b200_fab* S_scratch, double dtau, double facinv) {
+}  // extern "C"
+
+namespace {
+// erf_fast_rhs_N / erf_fast_rhs_T per-pass body (terrain selects the _T kernels)
+int fast_rhs_pass(erf_b200_ctx* c, bool terrain, int step, int nrk, const erf_b200_fab* S_slow_rhs,
+                  const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
+                  const erf_b200_fab* S_scratch, double dtau, double facinv) {
     if (!c || c->mixed || !c->base_set || step < 0 || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
-    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
+    if (terrain != (c->P.ter != 0)) return ERF_B200_ECONFIG;   // _N without terrain, _T with it
+    if (terrain && !c->ter_set) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
     if (!fab4_ok(S_slow_rhs, g, 2) || !fab4_ok(S_prev, g, 2) || !fab4_ok(S_stage, g, nc) || !fab4_ok(S_data, g, 2) ||
@@ -986,15 +1009,39 @@ int erf_b200_fast_rhs_N(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* 
         double D = dtau * dtau * kBeta2 * kBeta2 * g.dzi;
         launch_fast_coef<double>(P, st, tg, tcb, c->coef_smem, D, Sst, B.aux[0], B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
     }
-    launch_fast_h<double>(P, st, step, nrk, dtau, facinv, Sprev, 0, Sst, B.aux[0], B.Fmx, B.Fmy, B.lag[0], B.lag[1],
-                          B.avx, B.avy, OUT.mx, OUT.my);
-    dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
-    launch_fast_vert<double>(P, st, tg, tb, c->vert_smem, dtau, facinv, kBeta1, kBeta2, Sprev, 0, Sst, B.aux[0],
-                             B.Fcons, B.Fmz, OUT.mx, OUT.my, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, OUT.cons, OUT.mz);
+    if (terrain) {
+        launch_ter_fast_h<double>(P, st, step, dtau, facinv, Sprev, 0, Sst, B.aux[0], B.Fmx, B.Fmy, B.lag[0],
+                                  B.lag[1], B.ter, B.avx, B.avy, OUT.mx, OUT.my);
+        launch_ter_fast_vert<double>(P, st, dtau, facinv, kBeta1, kBeta2, Sprev, 0, Sst, B.aux[0], B.Fcons, B.Fmz,
+                                     B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, OUT.cons, OUT.mz);
+    } else {
+        launch_fast_h<double>(P, st, step, nrk, dtau, facinv, Sprev, 0, Sst, B.aux[0], B.Fmx, B.Fmy, B.lag[0],
+                              B.lag[1], B.avx, B.avy, OUT.mx, OUT.my);
+        dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
+        launch_fast_vert<double>(P, st, tg, tb, c->vert_smem, dtau, facinv, kBeta1, kBeta2, Sprev, 0, Sst, B.aux[0],
+                                 B.Fcons, B.Fmz, OUT.mx, OUT.my, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, OUT.cons,
+                                 OUT.mz);
+    }
     if ((rc = unpack4(c, S_data, 2, OUT.cons, OUT.mx, OUT.my, OUT.mz))) return rc;
     if ((rc = unpack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
     if ((rc = unpack(c, &lagf, 0, 1, B.lag[1]))) return rc;
     return cuda_fail(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+int erf_b200_fast_rhs_N(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* S_slow_rhs,
+                        const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
+                        const erf_b200_fab* S_scratch, double dtau, double facinv) {
+    return fast_rhs_pass(c, false, step, nrk, S_slow_rhs, S_prev, S_stage, S_data, S_scratch, dtau, facinv);
+}
+
+int erf_b200_fast_rhs_T(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* S_slow_rhs,
+                        const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
+                        const erf_b200_fab* S_scratch, double dtau, double facinv) {
+    return fast_rhs_pass(c, true, step, nrk, S_slow_rhs, S_prev, S_stage, S_data, S_scratch, dtau, facinv);
 }
 
 int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b200_fab* S_rhs,
@@ -1002,7 +1049,7 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
                            const erf_b200_fab* S_scratch) {
     (void)S_rhs;
     if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
-    if (c->P.ter) return ERF_B200_ECONFIG;   // the per-pass entries are the flat-grid (_N) passes
+    if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
     if (!fab4_ok(S_old, g, nc) || !fab4_ok(S_new, g, nc) || !fab4_ok(S_data, g, nc) || !fab4_ok(S_scratch, g, 1))
@@ -1014,6 +1061,10 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
     if ((rc = pack4(c, S_data, nc, SUM.cons, SUM.mx, SUM.my, SUM.mz))) return rc;
     if ((rc = pack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
     // stage state and primitives: those of the preceding slow_rhs_pre
+    if (c->P.ter)
+        launch_ter_post<double>(c->P, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.tke,
+                                B.ter, B.avx, B.avy, B.avz, c->vel[1][0], c->vel[1][1], c->vel[1][2]);
+    else
     launch_post<double>(c->P, c->tkz, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.tke,
                         B.avx, B.avy, B.avz, c->vel[1][0], c->vel[1][1], c->vel[1][2]);
     if ((rc = unpack4(c, S_new, nc, NEW.cons, NEW.mx, NEW.my, NEW.mz))) return rc;

@@ -309,6 +309,19 @@ int erf_b200_fast_rhs_N(erf_b200_ctx* ctx, int step, int nrk,
                         const erf_b200_fab* S_scratch,
                         double dtau, double facinv);
 
+/* erf_fast_rhs_T (TimeIntegration/ERF_fast_rhs_T.cpp:39-704, declared in
+ * ERF_TI_fast_headers.H:47-75): the same substep over static terrain, for a
+ * context created with use_terrain; S_scratch's z-momentum is the average
+ * contravariant momentum (Omega).  The other per-pass entries (turbulent
+ * viscosity, slow_rhs_pre / post, make_fast_coeffs) take the terrain branch
+ * themselves in such a context, as their reference counterparts do;
+ * erf_b200_fast_rhs_N returns ERF_B200_ECONFIG there. */
+int erf_b200_fast_rhs_T(erf_b200_ctx* ctx, int step, int nrk,
+                        const erf_b200_fab* S_slow_rhs, const erf_b200_fab* S_prev,
+                        const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
+                        const erf_b200_fab* S_scratch,
+                        double dtau, double facinv);
+
 /* erf_slow_rhs_post (TimeIntegration/ERF_slow_rhs_post.cpp:49-559). */
 int erf_b200_slow_rhs_post(erf_b200_ctx* ctx, int nrk, double slow_dt,
                            const erf_b200_fab* S_rhs, const erf_b200_fab* S_old,

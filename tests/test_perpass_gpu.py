@@ -161,3 +161,142 @@ def test_make_fast_coeffs_export():
     Bp = 1.0 / invB[1:12]
     assert np.all(Bp > 0)
     assert np.all(np.abs(Pc[1:12]) > 0) and np.all(np.abs(Qc[1:12]) > 0)
+
+
+def _w_walls(z_nd, u, v, dx, dy, zhi_noslip):
+    """w on the ground and the lid from Omega = 0 (WFromOmega) for face
+    velocities u [nz][ny][nx+1], v [nz+1... ] given as numpy arrays."""
+    nz = u.shape[0]
+    out = []
+    for k in (0, nz):
+        z = z_nd[k]
+        mx = 0.5 / dx * (z[1:, 1:] + z[:-1, 1:] - z[1:, :-1] - z[:-1, :-1])
+        my = 0.5 / dy * (z[1:, 1:] + z[1:, :-1] - z[:-1, 1:] - z[:-1, :-1])
+        if k == 0:
+            uf = 1.5 * (0.5 * (u[0, :, :-1] + u[0, :, 1:])) - 0.5 * (0.5 * (u[1, :, :-1] + u[1, :, 1:]))
+            vf = 1.5 * (0.5 * (v[0, :-1, :] + v[0, 1:, :])) - 0.5 * (0.5 * (v[1, :-1, :] + v[1, 1:, :]))
+        else:
+            ug = 0.0 * u[nz - 1] if zhi_noslip else u[nz - 1]
+            vg = 0.0 * v[nz - 1] if zhi_noslip else v[nz - 1]
+            uf = 0.25 * (u[nz - 1, :, :-1] + u[nz - 1, :, 1:] + ug[:, :-1] + ug[:, 1:])
+            vf = 0.25 * (v[nz - 1, :-1, :] + v[nz - 1, 1:, :] + vg[:-1, :] + vg[1:, :])
+        out.append(0.0 + mx * uf + my * vf)
+    return out
+
+
+def test_per_pass_terrain_composition_matches_fused_step():
+    """The per-pass entries over terrain (turbulent_viscosity, slow_rhs_pre,
+    fast_rhs_T, slow_rhs_post) composed by the host schedule reproduce the
+    fused terrain step; the host supplies w on the ground and the lid."""
+    import ctypes
+    import torch
+    from erf_b200 import Dycore
+    from erf_b200 import terrain as T
+    from erf_b200.dycore import dense_fab, ErfFab
+    case = T.abl_terrain(nx=16, ny=12, nz=16, dx=25.0, dz0=20.0, h0=100.0, r0=100.0, amp=5.0)
+    cfg = case.cfg
+    nx, ny, nz, nc = cfg.nx, cfg.ny, cfg.nz, cfg.ncomp
+    dy = Dycore(cfg)
+    dy.set_terrain(case.z_nd)
+    base = dy.make_base_state_terrain(case)
+    dy.set_base_state(base)
+    cons0, u0, v0, w0 = case.build_state(base[0])
+    fused = dy.advance_host(cons0, u0, v0, w0, 1)
+    assert dy.status() == 0
+
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    zeros = lambda *s: torch.zeros(s, dtype=torch.float64, device="cuda")
+    cons = t(cons0)
+    rho = cons[0]
+    rx = rho + torch.roll(rho, 1, dims=2)
+    ry = rho + torch.roll(rho, 1, dims=1)
+    rz = rho[1:] + rho[:-1]
+
+    def faces(a, kind):
+        if kind == 0:
+            return torch.cat([a, a[:, :, :1]], dim=2).contiguous()
+        return torch.cat([a, a[:, :1, :]], dim=1).contiguous()
+
+    def with_walls(wint, uu, vv):
+        lo, hi = _w_walls(case.z_nd, uu.cpu().numpy(), vv.cpu().numpy(), cfg.dx, cfg.dy, cfg.zhi_bc == C.BC_NO_SLIP_WALL)
+        return torch.cat([t(lo)[None], wint, t(hi)[None]], dim=0).contiguous()
+
+    def mz_of(wf):
+        m = torch.empty_like(wf)
+        m[1:nz] = (wf[1:nz] * 0.5) * rz
+        m[0] = (wf[0] * 0.5) * (rho[0] + rho[0])
+        m[nz] = (wf[nz] * 0.5) * (rho[nz - 1] + rho[nz - 1])
+        return m
+
+    # the fused prologue: V -> M -> V -> M round trip, w from Omega = 0 on the walls
+    u, v, w = t(u0), t(v0), t(w0)
+    out = []
+    for f, rs in ((u[:, :, :nx], rx), (v[:, :ny, :], ry), (w[1:nz], rz)):
+        m0 = (f * 0.5) * rs
+        out.append((m0 * 2.0) / rs)
+    u1, v1 = faces(out[0], 0), faces(out[1], 1)
+    w1 = with_walls(out[2], u1, v1)
+    S_old = [cons.clone(), faces((out[0] * 0.5) * rx, 0), faces((out[1] * 0.5) * ry, 1), mz_of(w1)]
+    vel = [u1, v1, w1]
+
+    def fabs(S, ncons):
+        arr = (ErfFab * 4)()
+        arr[0] = dense_fab(S[0], 0, nx, ny, nz, ncons)
+        for q, kind in ((1, 1), (2, 2), (3, 3)):
+            arr[q] = dense_fab(S[q], kind, nx, ny, nz)
+        return arr
+
+    def state(ncons):
+        return [zeros(ncons, nz, ny, nx), zeros(nz, ny, nx + 1), zeros(nz, ny + 1, nx), zeros(nz + 1, ny, nx)]
+
+    L = dy.lib
+    vf = lambda V: [ctypes.byref(dense_fab(V[q], q + 1, nx, ny, nz)) for q in range(3)]
+    L.erf_b200_turbulent_viscosity.argtypes = [ctypes.c_void_p] * 5
+    L.erf_b200_slow_rhs_pre.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double] + [ctypes.c_void_p] * 6
+    L.erf_b200_fast_rhs_T.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5 + [ctypes.c_double] * 2
+    L.erf_b200_fast_rhs_N.argtypes = L.erf_b200_fast_rhs_T.argtypes
+    L.erf_b200_slow_rhs_post.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double] + [ctypes.c_void_p] * 5
+    fc = dense_fab(cons, 0, nx, ny, nz, nc)
+    wv = dense_fab(w, 3, nx, ny, nz)
+    torch.cuda.synchronize()
+    assert L.erf_b200_turbulent_viscosity(dy.ctx, ctypes.byref(dense_fab(u, 1, nx, ny, nz)),
+                                          ctypes.byref(dense_fab(v, 2, nx, ny, nz)), ctypes.byref(wv),
+                                          ctypes.byref(fc)) == 0
+    stage = [a.clone() for a in S_old]
+    S_rhs, S_scr = state(2), state(2)
+    for nrk in range(3):
+        nsub, dtau, slow_dt = schedule(cfg, nrk)
+        assert L.erf_b200_slow_rhs_pre(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(stage, nc), fabs(S_scr, 2),
+                                       *vf(vel)) == 0
+        S_data = [a.clone() for a in S_old]
+        for ks in range(nsub):
+            prev = S_old if ks == 0 else [a.clone() for a in S_data]
+            assert L.erf_b200_fast_rhs_T(dy.ctx, ks, nrk, fabs(S_rhs, 2), fabs(prev, nc), fabs(stage, nc),
+                                         fabs(S_data, nc), fabs(S_scr, 2), dtau, 1.0 / nsub) == 0
+        if nrk == 0:   # the flat-grid substep is refused in a terrain context
+            assert L.erf_b200_fast_rhs_N(dy.ctx, 0, 0, fabs(S_rhs, 2), fabs(prev, nc), fabs(stage, nc),
+                                         fabs(S_data, nc), fabs(S_scr, 2), dtau, 1.0) != 0
+        S_new = state(nc)
+        assert L.erf_b200_slow_rhs_post(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(S_old, nc), fabs(S_new, nc),
+                                        fabs(S_data, nc), fabs(S_scr, 2)) == 0
+        torch.cuda.synchronize()
+        rho = S_data[0][0]
+        rx = rho + torch.roll(rho, 1, dims=2)
+        ry = rho + torch.roll(rho, 1, dims=1)
+        rz = rho[1:] + rho[:-1]
+        vv = []
+        for q, rs in ((1, rx), (2, ry), (3, rz)):
+            m = S_data[q]
+            m = m[:, :, :nx] if q == 1 else (m[:, :ny, :] if q == 2 else m[1:nz])
+            a1 = (m * 2.0) / rs
+            m1 = (a1 * 0.5) * rs
+            vv.append((m1 * 2.0) / rs)
+        u2, v2 = faces(vv[0], 0), faces(vv[1], 1)
+        vel = [u2, v2, with_walls(vv[2], u2, v2)]
+        stage = S_new
+    assert dy.status() == 0
+    got = (stage[0].cpu().numpy(), vel[0].cpu().numpy(), vel[1].cpu().numpy(), vel[2].cpu().numpy())
+    dy.close()
+    errs = compare_states(got, fused)
+    bad = {k: e for k, e in errs.items() if not e <= 1e-10}
+    assert not bad, errs
