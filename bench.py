@@ -369,6 +369,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble", "terrain"],
                     help="precision forms to time (the JSON line needs both; single forms are for profiling)")
+    ap.add_argument("--err-steps", type=int, default=100,
+                    help="steps of the mixed-vs-plain error runs (100; fewer only to shorten profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -545,7 +547,8 @@ def main():
         return 0
     if args.form == "terrain":
         if rank == 0:
-            print(json.dumps({"form": "terrain", "terrain": terrain_arm(args, C, Dycore, stream)}), flush=True)
+            print(json.dumps({"form": "terrain", "terrain": terrain_arm(args, C, Dycore, stream, n_err=args.err_steps)}),
+                  flush=True)
         if world > 1:
             dist.destroy_process_group()
         return 0

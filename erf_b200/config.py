@@ -24,6 +24,8 @@ MOLEC_NONE, MOLEC_CONSTANT, MOLEC_CONSTANT_ALPHA = 0, 1, 2
 MOIST_NONE, MOIST_KESSLER, MOIST_KESSLER_NORAIN = 0, 1, 2
 BC_NO_SLIP_WALL, BC_SLIP_WALL, BC_PERIODIC = 5, 6, 7
 PREC_FP64, PREC_MIXED = 0, 1
+# conserved components (Source/ERF_IndexDefines.H:36-43)
+RHO_COMP, RHOTHETA_COMP, RHOKE_COMP, RHOQKE_COMP, RHOSCALAR_COMP, RHOQ1_COMP = 0, 1, 2, 3, 4, 5
 
 R_D = 287.0
 CP_D = 1004.5

@@ -393,6 +393,21 @@ int erf_b200_mlp_infer(erf_b200_mlp* m, const float* x, int n, float* y);
  * returned on this host thread. */
 const char* erf_b200_last_cuda_error(void);
 
+/* Write an AMReX plotfile (single level, one grid) of a host state, as
+ * ERF::WritePlotFile does (Source/IO/ERF_Plotfile.cpp:186-1500): directory
+ * `dir` gets Header, Level_0/Cell_H and Level_0/Cell_D_00000.  Arrays are in
+ * the erf_b200_advance_host layout.  Variables: density, x/y/z_velocity
+ * (cell-centred), temp, theta, KE (Deardorff only), scalar, pres_hse and
+ * dens_hse (when rho0 and p0 are given: the base state as passed to
+ * erf_b200_set_base_state), pressure, qv / qc / qrain (moist), z_phys and detJ
+ * (when z_nd, the node heights given to erf_b200_set_terrain, is given with
+ * use_terrain; the nodal Level_0/Nu_nd is written then too).  Host-only: no
+ * context or device is needed.  Returns ERF_B200_EINVAL on a bad argument or
+ * a failed file write. */
+int erf_b200_write_plotfile(const erf_b200_config* cfg, const char* dir, const double* cons, const double* u,
+                            const double* v, const double* w, const double* rho0, const double* p0,
+                            const double* z_nd, double time, int step);
+
 /* ------------------------------------------------------------------------
  * Resident state, autotuning and ensembles (no reference counterpart).
  * ------------------------------------------------------------------------ */

@@ -22,5 +22,6 @@ if __name__ == "__main__":
     for name in TESTS:
         pf = read_plotfile(os.path.join(ref, "Tests", "ERFGoldFiles", name))
         out = os.path.join(HERE, f"{name}_gold.npz")
-        np.savez_compressed(out, data=pf["data"], names=np.array(pf["names"]), time=pf["time"])
+        np.savez_compressed(out, data=pf["data"], names=np.array(pf["names"]), time=pf["time"],
+                            header=np.array(pf["header"]))
         print(out, pf["data"].shape, pf["names"], pf["time"])

@@ -1,10 +1,41 @@
 """Minimal reader for AMReX plotfiles (single level): the text Header, the
 Level_0/Cell_H box list and the Cell_D_* FAB blocks (a text FAB header
-followed by raw little-endian float64, Fortran order per component)."""
+followed by raw little-endian float64, Fortran order per component), and the
+nodal MultiFab that terrain plotfiles list after the cell one."""
 import os
 import re
 
 import numpy as np
+
+
+def _read_multifab(prefix, nodal):
+    """Assemble the FABs listed in <prefix>_H; returns [ncomp, nz, ny, nx]."""
+    d = os.path.dirname(prefix)
+    with open(prefix + "_H") as fh:
+        ch = fh.read()
+    files = re.findall(r"FabOnDisk:\s+(\S+)\s+(\d+)", ch)
+    boxes = []
+    for fname, off in files:
+        with open(os.path.join(d, fname), "rb") as fh:
+            fh.seek(int(off))
+            head = b""
+            while not head.endswith(b"\n"):
+                head += fh.read(1)
+            txt = head.decode()
+            assert txt.startswith("FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (8 7 6 5 4 3 2 1)))"), txt
+            nums = re.findall(r"\(\((-?\d+),(-?\d+),(-?\d+)\) \((-?\d+),(-?\d+),(-?\d+)\) \((\d),(\d),(\d)\)", txt)
+            blo = list(map(int, nums[0][0:3])); bhi = list(map(int, nums[0][3:6]))
+            assert all(int(t) == nodal for t in nums[0][6:9]), txt
+            nc = int(txt.strip().split()[-1])
+            bshape = [bhi[q] - blo[q] + 1 for q in range(3)]
+            n = bshape[0] * bshape[1] * bshape[2]
+            raw = np.frombuffer(fh.read(8 * n * nc), dtype="<f8").reshape(nc, bshape[2], bshape[1], bshape[0])
+            boxes.append((blo, bhi, raw))
+    hi = np.max([b[1] for b in boxes], axis=0)
+    data = np.zeros((boxes[0][2].shape[0], hi[2] + 1, hi[1] + 1, hi[0] + 1))
+    for blo, bhi, raw in boxes:
+        data[:, blo[2]:bhi[2] + 1, blo[1]:bhi[1] + 1, blo[0]:bhi[0] + 1] = raw
+    return data
 
 
 def read_plotfile(path):
@@ -13,28 +44,13 @@ def read_plotfile(path):
     nvar = int(lines[1])
     names = lines[2:2 + nvar]
     p = 2 + nvar
-    ndim = int(lines[p]); p += 1
-    time = float(lines[p]); p += 1
-    domain = re.findall(r"-?\d+", lines[p + 4])
-    lo = list(map(int, domain[0:3])); hi = list(map(int, domain[3:6]))
-    shape = [hi[d] - lo[d] + 1 for d in range(3)]
-    data = np.zeros((nvar, shape[2], shape[1], shape[0]))
-    lvl = os.path.join(path, "Level_0")
-    with open(os.path.join(lvl, "Cell_H")) as fh:
-        ch = fh.read()
-    files = re.findall(r"FabOnDisk:\s+(\S+)\s+(\d+)", ch)
-    for fname, off in files:
-        with open(os.path.join(lvl, fname), "rb") as fh:
-            fh.seek(int(off))
-            head = b""
-            while not head.endswith(b"\n"):
-                head += fh.read(1)
-            txt = head.decode()
-            nums = re.findall(r"\(\((-?\d+),(-?\d+),(-?\d+)\) \((-?\d+),(-?\d+),(-?\d+)\)", txt)
-            blo = list(map(int, nums[0][0:3])); bhi = list(map(int, nums[0][3:6]))
-            nc = int(txt.strip().split()[-1])
-            bshape = [bhi[d] - blo[d] + 1 for d in range(3)]
-            n = bshape[0] * bshape[1] * bshape[2]
-            raw = np.frombuffer(fh.read(8 * n * nc), dtype="<f8").reshape(nc, bshape[2], bshape[1], bshape[0])
-            data[:, blo[2]:bhi[2] + 1, blo[1]:bhi[1] + 1, blo[0]:bhi[0] + 1] = raw
-    return {"names": names, "time": time, "data": data}
+    time = float(lines[p + 1])
+    ngrids = int(lines[p + 11].split()[1])
+    q = p + 13 + 3 * ngrids
+    data = _read_multifab(os.path.join(path, lines[q]), 0)
+    out = {"names": names, "time": time, "data": data, "header": lines}
+    if len(lines) > q + 5 and lines[q + 1] == "1":
+        nn = int(lines[q + 2])
+        out["nodal_names"] = lines[q + 3:q + 3 + nn]
+        out["nodal"] = _read_multifab(os.path.join(path, lines[q + 3 + nn]), 1)
+    return out
