@@ -16,19 +16,14 @@
 // heights are given; the terrain plotfile also carries the nodal MultiFab
 // Level_0/Nu_nd (node displacements 0, 0, z - k dz) listed at the end of the
 // Header, as WriteMultiLevelPlotfileWithTerrain (ERF_Plotfile.cpp:1505-1680)
-// writes it.  Cell_H carries VisMF version 1, "how" 1, no ghost cells, and the
-// per-FAB min / max blocks, as AMReX writes them.
-#include <sys/stat.h>
-#include <sys/types.h>
-
-#include <cerrno>
+// writes it.  The MultiFab files themselves are written by amrex_io.h.
 #include <cmath>
 #include <cstdio>
-#include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/erf_b200.h"
+#include "amrex_io.h"
 
 namespace {
 
@@ -40,44 +35,6 @@ double eos_p(double rt, double qv) { return kP0 * std::pow(kRd * rt * (1.0 + (kR
 double eos_T(double rho, double rt, double qv) {
     double p = kP0 * std::pow(kRd * rt * (1.0 + kRv / kRd * qv) * kIP0, kGamma);
     return p / (kRd * rho * (1.0 + kRv / kRd * qv));
-}
-
-int make_dir(const std::string& d) {
-    if (mkdir(d.c_str(), 0755) != 0 && errno != EEXIST) return -1;
-    return 0;
-}
-
-// One FAB over box (0,0,0)..(hx,hy,hz) of index type t (0 cell, 1 node):
-// <prefix>_D_00000 (FAB header line, then little-endian FP64, component-major,
-// i fastest) and <prefix>_H, the VisMF header with per-component min / max.
-int write_fab(const std::string& prefix, int hx, int hy, int hz, int t, int ncomp, const std::vector<double>& data) {
-    const size_t n = data.size() / ncomp;
-    const std::string dname = prefix.substr(prefix.rfind('/') + 1) + "_D_00000";
-    FILE* f = std::fopen((prefix + "_D_00000").c_str(), "wb");
-    if (!f) return -1;
-    std::fprintf(f, "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (8 7 6 5 4 3 2 1)))((0,0,0) (%d,%d,%d) (%d,%d,%d)) %d\n",
-                 hx, hy, hz, t, t, t, ncomp);
-    size_t wrote = std::fwrite(data.data(), sizeof(double), data.size(), f);
-    std::fclose(f);
-    if (wrote != data.size()) return -1;
-    f = std::fopen((prefix + "_H").c_str(), "w");
-    if (!f) return -1;
-    std::fprintf(f, "1\n1\n%d\n0\n(1 0\n((0,0,0) (%d,%d,%d) (%d,%d,%d))\n)\n1\nFabOnDisk: %s 0\n\n", ncomp, hx, hy,
-                 hz, t, t, t, dname.c_str());
-    for (int pass = 0; pass < 2; ++pass) {
-        std::fprintf(f, "1,%d\n", ncomp);
-        for (int q = 0; q < ncomp; ++q) {
-            double m = data[(size_t)q * n];
-            for (size_t c = 1; c < n; ++c) {
-                double x = data[(size_t)q * n + c];
-                m = pass == 0 ? std::fmin(m, x) : std::fmax(m, x);
-            }
-            std::fprintf(f, "%.16e,", m);
-        }
-        std::fprintf(f, "\n\n");
-    }
-    std::fclose(f);
-    return 0;
 }
 
 }  // namespace
@@ -146,7 +103,7 @@ int erf_b200_write_plotfile(const erf_b200_config* cfg, const char* dir, const d
             }
 
     const std::string root(dir);
-    if (make_dir(root) || make_dir(root + "/Level_0")) return ERF_B200_EINVAL;
+    if (erfio::make_dir(root) || erfio::make_dir(root + "/Level_0")) return ERF_B200_EINVAL;
     const double prob_hi[3] = {nx * cfg->dx, ny * cfg->dy, nz * cfg->dz};
     const double dxs[3] = {cfg->dx, cfg->dy, cfg->dz};
     // ---- Header
@@ -166,7 +123,8 @@ int erf_b200_write_plotfile(const erf_b200_config* cfg, const char* dir, const d
         if (terrain) std::fprintf(f, "1\n3\namrexvec_nu_x\namrexvec_nu_y\namrexvec_nu_z\nLevel_0/Nu_nd\n");
         std::fclose(f);
     }
-    if (write_fab(root + "/Level_0/Cell", nx - 1, ny - 1, nz - 1, 0, nvar, data)) return ERF_B200_EINVAL;
+    if (erfio::write_multifab(root + "/Level_0/Cell", erfio::box(nx - 1, ny - 1, nz - 1), 0, nvar, data))
+        return ERF_B200_EINVAL;
     if (terrain) {
         // node displacements (0, 0, z - k dz) over the nodal box, as the reference's Nu_nd
         const size_t M = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
@@ -176,7 +134,8 @@ int erf_b200_write_plotfile(const erf_b200_config* cfg, const char* dir, const d
                 size_t c = (size_t)k * (nx + 1) * (ny + 1) + p;
                 nd[2 * M + c] = z_nd[c] - k * cfg->dz;
             }
-        if (write_fab(root + "/Level_0/Nu_nd", nx, ny, nz, 1, 3, nd)) return ERF_B200_EINVAL;
+        if (erfio::write_multifab(root + "/Level_0/Nu_nd", erfio::box(nx, ny, nz, 1, 1, 1), 0, 3, nd))
+            return ERF_B200_EINVAL;
     }
     return ERF_B200_OK;
 }

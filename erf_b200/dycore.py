@@ -33,7 +33,7 @@ EXPORTS = [
     "erf_b200_load_state", "erf_b200_store_state", "erf_b200_advance_resident", "erf_b200_autotune",
     "erf_b200_ensemble_create", "erf_b200_ensemble_advance", "erf_b200_ensemble_sync", "erf_b200_ensemble_destroy",
     "erf_b200_last_cuda_error", "erf_b200_set_terrain", "erf_b200_make_base_state_terrain",
-    "erf_b200_fast_rhs_T", "erf_b200_write_plotfile",
+    "erf_b200_fast_rhs_T", "erf_b200_write_plotfile", "erf_b200_write_checkpoint", "erf_b200_read_checkpoint",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs"]
@@ -92,6 +92,9 @@ def load_library():
     L.erf_b200_ensemble_sync.argtypes = [vp]
     L.erf_b200_ensemble_destroy.argtypes = [vp]
     L.erf_b200_write_plotfile.argtypes = [vp, ctypes.c_char_p, dp, dp, dp, dp, dp, dp, dp, ctypes.c_double, i]
+    L.erf_b200_write_checkpoint.argtypes = [vp, ctypes.c_char_p] + [dp] * 9 + [i, ctypes.c_double, ctypes.c_double]
+    L.erf_b200_read_checkpoint.argtypes = [vp, ctypes.c_char_p] + [dp] * 9 + [ctypes.POINTER(i),
+                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.erf_b200_last_cuda_error.argtypes = []

@@ -408,6 +408,28 @@ int erf_b200_write_plotfile(const erf_b200_config* cfg, const char* dir, const d
                             const double* v, const double* w, const double* rho0, const double* p0,
                             const double* z_nd, double time, int step);
 
+/* Checkpoint / restart in ERF's native checkpoint layout
+ * (ERF::WriteCheckpointFile / ReadCheckpointFile, Source/IO/
+ * ERF_Checkpoint.cpp:25-470), single level: Header (istep, dt, t_new, the
+ * BoxArray), Level_0/Cell, XFace, YFace, ZFace, BaseState (r0, p0, pi0, th0,
+ * 3 ghost cells), Z_Phys_nd (terrain) and MapFactor_m/_u/_v (all 1).  Arrays
+ * are host arrays in the erf_b200_advance_host layout; the base state is laid
+ * out as for erf_b200_set_base_state; z_nd as for erf_b200_set_terrain
+ * (required with use_terrain, ignored otherwise).  Host-only.
+ *
+ * The reader accepts checkpoints with any number of grids and ghost widths
+ * (the reference's own included) whose Header matches cfg: one level, ncomp
+ * conserved components.  The base-state pointers may all be NULL (not read),
+ * as may z_nd and the step / dt / time outputs.  Returns ERF_B200_EINVAL on a
+ * missing or malformed file or a shape mismatch. */
+int erf_b200_write_checkpoint(const erf_b200_config* cfg, const char* dir, const double* cons, const double* u,
+                              const double* v, const double* w, const double* r0, const double* p0,
+                              const double* pi0, const double* th0, const double* z_nd, int step, double dt,
+                              double time);
+int erf_b200_read_checkpoint(const erf_b200_config* cfg, const char* dir, double* cons, double* u, double* v,
+                             double* w, double* r0, double* p0, double* pi0, double* th0, double* z_nd, int* step,
+                             double* dt, double* time);
+
 /* ------------------------------------------------------------------------
  * Resident state, autotuning and ensembles (no reference counterpart).
  * ------------------------------------------------------------------------ */

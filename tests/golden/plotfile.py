@@ -9,7 +9,8 @@ import numpy as np
 
 
 def _read_multifab(prefix, nodal):
-    """Assemble the FABs listed in <prefix>_H; returns [ncomp, nz, ny, nx]."""
+    """Assemble the FABs listed in <prefix>_H over the union of their stored
+    (grown) boxes; returns [ncomp, nz, ny, nx] starting at the lowest corner."""
     d = os.path.dirname(prefix)
     with open(prefix + "_H") as fh:
         ch = fh.read()
@@ -31,10 +32,12 @@ def _read_multifab(prefix, nodal):
             n = bshape[0] * bshape[1] * bshape[2]
             raw = np.frombuffer(fh.read(8 * n * nc), dtype="<f8").reshape(nc, bshape[2], bshape[1], bshape[0])
             boxes.append((blo, bhi, raw))
-    hi = np.max([b[1] for b in boxes], axis=0)
+    lo = np.min([b[0] for b in boxes], axis=0)
+    hi = np.max([b[1] for b in boxes], axis=0) - lo
     data = np.zeros((boxes[0][2].shape[0], hi[2] + 1, hi[1] + 1, hi[0] + 1))
     for blo, bhi, raw in boxes:
-        data[:, blo[2]:bhi[2] + 1, blo[1]:bhi[1] + 1, blo[0]:bhi[0] + 1] = raw
+        a, b = np.array(blo) - lo, np.array(bhi) - lo
+        data[:, a[2]:b[2] + 1, a[1]:b[1] + 1, a[0]:b[0] + 1] = raw
     return data
 
 
