@@ -18,7 +18,7 @@ from .dycore import _check, load_library
 def _shapes(cfg: C.ErfConfig):
     nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
     nb = (nz + 2) * (nx * ny if cfg.use_terrain else 1)
-    return dict(cons=(cfg.ncomp, nx * ny * nz), u=(nz, ny, nx + 1), v=(nz, ny + 1, nx), w=(nz + 1, ny, nx),
+    return dict(cons=(cfg.ncomp, nz, ny, nx), u=(nz, ny, nx + 1), v=(nz, ny + 1, nx), w=(nz + 1, ny, nx),
                 base=nb, z_nd=(nz + 1, ny + 1, nx + 1))
 
 
