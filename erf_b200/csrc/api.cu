@@ -521,7 +521,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         A(&c->S[s].cons, nc * N); A(&c->S[s].mx, N); A(&c->S[s].my, N); A(&c->S[s].mz, NZF);
     }
     for (int p = 0; p < 2; ++p) { A(&c->vel[p][0], N); A(&c->vel[p][1], N); A(&c->vel[p][2], NZF); }
-    A(&c->pavg, 6 * cfg->nz);
+    A(&c->pavg, plane_avg_doubles(cfg->nz));
     c->mixed = cfg->precision == ERF_PREC_MIXED;
     if (rc == ERF_B200_OK) rc = c->mixed ? alloc_bulk(c, c->bf) : alloc_bulk(c, c->bd);
     {

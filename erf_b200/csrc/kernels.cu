@@ -285,18 +285,27 @@ __device__ __forceinline__ R scalar_diff(const Params& P, const double* __restri
 }
 
 // Horizontal plane averages of rho, theta, qv, qc, qp for buoyancy type 2
-// (SourceTerms/ERF_make_buoyancy.cpp:212-249): one block per level, FP64 sums;
-// also the temperature of the mean state of each level.
+// (SourceTerms/ERF_make_buoyancy.cpp:212-249), FP64 sums; also the
+// temperature of the mean state of each level.  Each level is split over
+// PAVG_PARTS blocks (grid nz x PAVG_PARTS) that write partial sums; the last
+// block of a level to finish (counted with an atomic ticket after a memory
+// fence) adds the partials in part order and resets the ticket, so the result
+// does not depend on which block finishes last.  Buffer layout after the
+// 6 nz results: 5 nz PAVG_PARTS partials, then nz tickets (one per double slot).
 template <class R>
 __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* __restrict__ prim,
                             double* __restrict__ avg) {
     const Geo& g = P.g;
-    int k = blockIdx.x;
+    const int k = blockIdx.x, part = blockIdx.y, nz = g.nz;
     const int64_t N = g.ncell;
+    double* partial = avg + 6 * nz;
+    unsigned int* ticket = reinterpret_cast<unsigned int*>(partial + 5 * nz * PAVG_PARTS);
     double denom = 1.0 / (double)(g.nx * g.ny);
     int nq = P.ncomp - ERF_RHOQ1_COMP;
+    const int64_t span = (g.sk + PAVG_PARTS - 1) / PAVG_PARTS;
+    const int64_t t0 = part * span, t1 = min(g.sk, t0 + span);
     double acc[5] = {0, 0, 0, 0, 0};
-    for (int64_t t = threadIdx.x; t < g.sk; t += blockDim.x) {
+    for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
         int64_t c = g.sk * k + t;
         acc[0] += cons[c] * denom;
         acc[1] += double(prim[c]) * denom;
@@ -305,6 +314,7 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* 
         if (nq >= 3) acc[4] += double(prim[6 * N + c]) * denom;
     }
     __shared__ double sh[5][256];
+    __shared__ bool last;
     for (int q = 0; q < 5; ++q) sh[q][threadIdx.x] = acc[q];
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
@@ -313,9 +323,24 @@ __global__ void k_plane_avg(Params P, const double* __restrict__ cons, const R* 
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        for (int q = 0; q < 5; ++q) avg[q * g.nz + k] = sh[q][0];
+        for (int q = 0; q < 5; ++q) partial[(q * nz + k) * PAVG_PARTS + part] = sh[q][0];
+        __threadfence();
+        last = atomicAdd(&ticket[2 * k], 1u) == PAVG_PARTS - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double m[5];
+        for (int q = 0; q < 5; ++q) {
+            const volatile double* pq = partial + (q * nz + k) * PAVG_PARTS;
+            double sum = 0.0;
+            for (int p = 0; p < PAVG_PARTS; ++p) sum += pq[p];
+            m[q] = sum;
+            avg[q * nz + k] = sum;
+        }
         // the plane-mean temperature used by make_buoyancy's type 2
-        avg[5 * g.nz + k] = eos_T(sh[0][0], sh[0][0] * sh[1][0], sh[2][0]);
+        avg[5 * nz + k] = eos_T(m[0], m[0] * m[1], m[2]);
+        ticket[2 * k] = 0u;
     }
 }
 
@@ -1662,7 +1687,7 @@ void launch_tau(const Params& P, cudaStream_t st, const double* cons, const doub
 }
 template <class R>
 void launch_plane_avg(const Params& P, cudaStream_t st, const double* cons, const R* prim, double* avg) {
-    k_plane_avg<R><<<P.g.nz, 256, 0, st>>>(P, cons, prim, avg);
+    k_plane_avg<R><<<dim3(P.g.nz, PAVG_PARTS), 256, 0, st>>>(P, cons, prim, avg);
 }
 template <class R>
 void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double dtau, double facinv, StateBuf Sprev,

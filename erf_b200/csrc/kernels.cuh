@@ -99,6 +99,11 @@ void launch_tau(const Params& P, cudaStream_t st, const double* cons, const doub
                 const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23);
 template <class R>
 void launch_stage_aux(const Params& P, cudaStream_t st, const double* cons, StageAux<R> A);
+// Blocks per level of the plane averages; the avg buffer holds 6 nz results,
+// 5 nz PAVG_PARTS partial sums and nz tickets (plane_avg_doubles(nz) doubles,
+// zero-initialised).
+constexpr int PAVG_PARTS = 16;
+inline size_t plane_avg_doubles(int nz) { return (size_t)6 * nz + (size_t)5 * nz * PAVG_PARTS + nz; }
 template <class R>
 void launch_plane_avg(const Params& P, cudaStream_t st, const double* cons, const R* prim, double* avg);
 template <class R>
