@@ -50,6 +50,11 @@ struct erf_b200_ctx {
     Geo g;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // side branch of a stage: the plane averages and the fast coefficients
+    // depend only on the stage state, so they run beside tau / slow_cell /
+    // slow_mom (forked and joined with events; captured into the graphs)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_pavg = nullptr, ev_coef = nullptr;
     int device = 0;
     size_t bytes = 0;
     std::vector<void*> allocs;
@@ -279,6 +284,7 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     StateBuf outs[3] = {N0, N1, N0};
     StateBuf stage[3] = {OLD, outs[0], outs[1]};
     dim3 tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1), tcb(c->tile_tx, c->coef_warps, 1);
+    const bool fork = T == nullptr && c->side;
     int a = 0;
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
@@ -288,6 +294,14 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
         int nsub; double dtau, slow_dt;
         stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
+        double facinv = 1.0 / (double)nsub;
+        double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
+        if (fork) {
+            cudaEventRecord(c->ev_fork, st);
+            cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+            launch_fast_coef<R>(P, c->side, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
+            cudaEventRecord(c->ev_coef, c->side);
+        }
         if (P.use_diff)
             TIMED(1, launch_ter_tau<R>(P, st, nrk, Sst.cons, Vnew[0], Vnew[1], Vnew[2], B.mut, B.ter, B.tke, B.t11,
                                        B.t22, B.t33, B.t12, B.t13, B.t23));
@@ -295,9 +309,10 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                          B.avy, B.avz));
         TIMED(4, launch_ter_slow_mom<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12, B.t13,
                                         B.t23, B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz));
-        double facinv = 1.0 / (double)nsub;
-        double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
-        TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
+        if (!fork)
+            TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
+        else
+            cudaStreamWaitEvent(st, c->ev_coef, 0);
         for (int ks = 0; ks < nsub; ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
@@ -337,6 +352,7 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     StateBuf stage[3] = {OLD, outs[0], outs[1]};
     dim3 tb(c->tile_tx, c->vert_warps, 1), tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1);
     dim3 tcb(c->tile_tx, c->coef_warps, 1);
+    const bool fork = T == nullptr && c->side;   // per-kernel timing keeps one stream
     int a = 0;
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
@@ -346,6 +362,19 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
         int nsub; double dtau, slow_dt;
         stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
+        const bool plane = P.moist && P.buoy_type == 2;
+        double facinv = 1.0 / (double)nsub;
+        double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
+        if (fork) {
+            cudaEventRecord(c->ev_fork, st);
+            cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+            if (plane) {
+                launch_plane_avg<R>(P, c->side, Sst.cons, Acur.prim, c->pavg);
+                cudaEventRecord(c->ev_pavg, c->side);
+            }
+            launch_fast_coef<R>(P, c->side, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
+            cudaEventRecord(c->ev_coef, c->side);
+        }
         if (P.les == ERF_LES_MLP) {
             ClosureNet net{c->net->wpack, c->net->bias, c->net->norm, c->net->env, c->fallback};
             TIMED(1, launch_closure<R>(P, net, c->closure_grid, st, Sst.cons, Vnew[0], Vnew[1], Vnew[2], Acur.prim,
@@ -357,12 +386,14 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         }
         TIMED(2, launch_slow_cell<R>(P, c->tkz, st, Sst, Acur, B.mut, B.hx, B.hy, B.hz, B.tke, B.Fcons, B.avx,
                                      B.avy, B.avz));
-        if (P.moist && P.buoy_type == 2) TIMED(3, launch_plane_avg<R>(P, st, Sst.cons, Acur.prim, c->pavg));
+        if (plane && !fork) TIMED(3, launch_plane_avg<R>(P, st, Sst.cons, Acur.prim, c->pavg));
+        if (plane && fork) cudaStreamWaitEvent(st, c->ev_pavg, 0);
         TIMED(4, launch_slow_mom<R>(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12,
                                     B.t13, B.t23, c->pavg, B.Fmx, B.Fmy, B.Fmz));
-        double facinv = 1.0 / (double)nsub;
-        double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
-        TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
+        if (!fork)
+            TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
+        else
+            cudaStreamWaitEvent(st, c->ev_coef, 0);
         for (int ks = 0; ks < nsub; ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
@@ -512,6 +543,13 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return ERF_B200_ECUDA; }
         c->own_stream = true;
     }
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_pavg, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_coef, cudaEventDisableTiming) != cudaSuccess) {
+        erf_b200_destroy(c);
+        return ERF_B200_ECUDA;
+    }
     const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
     const int64_t NZF = (int64_t)cfg->nx * cfg->ny * (cfg->nz + 1);
     const int nc = cfg->ncomp;
@@ -578,8 +616,12 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
 int erf_b200_destroy(erf_b200_ctx* c) {
     if (!c) return ERF_B200_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->side) cudaStreamSynchronize(c->side);
     drop_graphs(c);
     for (void* q : c->allocs) cudaFree(q);
+    if (c->side) cudaStreamDestroy(c->side);
+    for (cudaEvent_t e : {c->ev_fork, c->ev_pavg, c->ev_coef})
+        if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return ERF_B200_OK;
