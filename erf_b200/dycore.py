@@ -150,7 +150,15 @@ class Ensemble:
 
 
 class Dycore:
-    """One dycore context on the current CUDA device."""
+    """One dycore context on the current CUDA device.
+
+    The context runs on `stream` (a cudaStream_t handle), by default torch's
+    current stream.  When that is the legacy default stream (handle 0) the
+    library creates a non-blocking stream of its own, which does not order
+    after torch's work: synchronise (torch.cuda.synchronize) between torch
+    operations on tensors and library calls that read or write them.
+    advance_host and the make_base_state* methods return synchronised host
+    results."""
 
     def __init__(self, cfg: C.ErfConfig, stream=None):
         import torch

@@ -36,6 +36,7 @@ def _advance_device(case, nsteps, precision=C.PREC_FP64, z_nd=None):
     dy.set_base_state(base)
     cons, u, v, w = case.build_state(base[0])
     dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (cons, u, v, w)]
+    torch.cuda.synchronize()   # the context's stream does not order after torch's default stream
     dy.advance(*dev, nsteps)
     torch.cuda.synchronize()
     st = dy.status()

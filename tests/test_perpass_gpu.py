@@ -3,7 +3,11 @@ fast_rhs_N with make_fast_coeffs at substep 0, slow_rhs_post) composed by a
 host-side MRISplitIntegrator schedule (ERF_MRI.H:187-369) reproduce the fused
 step.  The composed step omits the momentum round trip between substeps that
 the fused step applies (a boundary fill of the caller's), so the bar is
-relative L2 <= 1e-10 per field after one step."""
+relative L2 <= 1e-10 per field after one step.
+
+The library runs on its own stream here (torch is on the legacy default
+stream, which a context cannot share), so the host synchronises the device
+around every library call that reads or writes tensors made by torch."""
 import numpy as np
 import pytest
 
@@ -94,14 +98,18 @@ def test_per_pass_composition_matches_fused_step():
     S_rhs, S_scr = state(2), state(2)
     for nrk in range(3):
         nsub, dtau, slow_dt = schedule(cfg, nrk)
+        torch.cuda.synchronize()
         assert L.erf_b200_slow_rhs_pre(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(stage, nc), fabs(S_scr, 2),
                                        *vf(vel)) == 0
         S_data = [a.clone() for a in S_old]
         for ks in range(nsub):
             prev = S_old if ks == 0 else [a.clone() for a in S_data]
+            torch.cuda.synchronize()
             assert L.erf_b200_fast_rhs_N(dy.ctx, ks, nrk, fabs(S_rhs, 2), fabs(prev, nc), fabs(stage, nc),
                                          fabs(S_data, nc), fabs(S_scr, 2), dtau, 1.0 / nsub) == 0
+            torch.cuda.synchronize()
         S_new = state(nc)
+        torch.cuda.synchronize()
         assert L.erf_b200_slow_rhs_post(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(S_old, nc), fabs(S_new, nc),
                                         fabs(S_data, nc), fabs(S_scr, 2)) == 0
         torch.cuda.synchronize()
@@ -266,17 +274,21 @@ def test_per_pass_terrain_composition_matches_fused_step():
     S_rhs, S_scr = state(2), state(2)
     for nrk in range(3):
         nsub, dtau, slow_dt = schedule(cfg, nrk)
+        torch.cuda.synchronize()
         assert L.erf_b200_slow_rhs_pre(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(stage, nc), fabs(S_scr, 2),
                                        *vf(vel)) == 0
         S_data = [a.clone() for a in S_old]
         for ks in range(nsub):
             prev = S_old if ks == 0 else [a.clone() for a in S_data]
+            torch.cuda.synchronize()
             assert L.erf_b200_fast_rhs_T(dy.ctx, ks, nrk, fabs(S_rhs, 2), fabs(prev, nc), fabs(stage, nc),
                                          fabs(S_data, nc), fabs(S_scr, 2), dtau, 1.0 / nsub) == 0
+            torch.cuda.synchronize()
         if nrk == 0:   # the flat-grid substep is refused in a terrain context
             assert L.erf_b200_fast_rhs_N(dy.ctx, 0, 0, fabs(S_rhs, 2), fabs(prev, nc), fabs(stage, nc),
                                          fabs(S_data, nc), fabs(S_scr, 2), dtau, 1.0) != 0
         S_new = state(nc)
+        torch.cuda.synchronize()
         assert L.erf_b200_slow_rhs_post(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(S_old, nc), fabs(S_new, nc),
                                         fabs(S_data, nc), fabs(S_scr, 2)) == 0
         torch.cuda.synchronize()
