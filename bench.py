@@ -447,7 +447,7 @@ def main():
         st = dy.status()
         value = replica_throughput(world, n_cells, args.steps, ms * 1e-3)
         if light:
-            out = {"value": value, "ms_per_step": ms / args.steps, "status": st, "autotuned_ms": tuned_ms, "autotuned_ms": tuned_ms}
+            out = {"value": value, "ms_per_step": ms / args.steps, "status": st, "autotuned_ms": tuned_ms}
             if net is not None:
                 out["fallback_cells_per_step"] = dy.closure_fallbacks() / max(args.warmup + args.steps, 1)
             dy.close()

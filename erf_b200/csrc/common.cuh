@@ -250,6 +250,14 @@ struct Geo {
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+// Periodic index for offsets that may exceed one period (tile halos on grids
+// narrower than a tile): the common one-period cases without a division.
+__device__ __forceinline__ int wrap_far(int i, int n) {
+    if (i < 0) i += n;
+    if (i >= n) i -= n;
+    if ((unsigned)i >= (unsigned)n) i = ((i % n) + n) % n;
+    return i;
+}
 __device__ __forceinline__ int clampk(int k, int nz) { return k < 0 ? 0 : (k >= nz ? nz - 1 : k); }
 __device__ __forceinline__ int64_t cidx(const Geo& g, int i, int j, int k) {
     return (int64_t)i + (int64_t)g.nx * j + g.sk * k;

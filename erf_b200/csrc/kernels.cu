@@ -998,9 +998,7 @@ __device__ __forceinline__ void load_plane(const Geo& g, Plane<R>& p, const R* _
     constexpr int W = TTX + 2 * PH, NE = W * (TTY + 2 * PH);
     for (int e = t; e < NE; e += TTX * TTY) {
         const int b = e / W, a = e - b * W;
-        int gi = (i0 + a) % g.nx, gj = (j0 + b) % g.ny;
-        gi += gi < 0 ? g.nx : 0;
-        gj += gj < 0 ? g.ny : 0;
+        const int gi = wrap_far(i0 + a, g.nx), gj = wrap_far(j0 + b, g.ny);
         const unsigned dst = (unsigned)__cvta_generic_to_shared(&p.v[b][a]);
         const R* src = lev + gi + (int64_t)g.nx * gj;
         if constexpr (sizeof(R) == 8)
