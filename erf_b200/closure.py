@@ -169,9 +169,17 @@ def fine_snapshots(case, spinup, nsnap, every):
 
 
 def coarse_case(fine_case, r):
-    """The coarse-grid configuration matching a fine case."""
+    """The coarse-grid configuration matching a fine case.  Its seeded noise
+    amplitudes are those of the fine case's noise block-averaged over r^3
+    cells (the standard deviation of a mean of r^3 independent samples is
+    r^-3/2 of theirs), so that a coarse run starts with the coarse-grained
+    statistics the closure is trained on, not with grid-scale noise r^3/2
+    times stronger."""
     import copy
     c = copy.deepcopy(fine_case)
+    for key in ("noise_amp", "vel_noise_amp"):
+        if key in c.pert:
+            c.pert[key] = c.pert[key] * float(r) ** -1.5
     cfg = c.cfg.copy()
     cfg.nx, cfg.ny, cfg.nz = fine_case.cfg.nx // r, fine_case.cfg.ny // r, fine_case.cfg.nz // r
     cfg.dx, cfg.dy, cfg.dz = fine_case.cfg.dx * r, fine_case.cfg.dy * r, fine_case.cfg.dz * r
