@@ -300,6 +300,7 @@ def terrain_arm(args, C, Dycore, stream, n_err=100):
                      "status": dy.status(), "kernels": kern}
         # error run from the initial state
         dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in init]
+        torch.cuda.synchronize()   # the copies run on torch's default stream
         dy.advance(*dev, n_err)
         torch.cuda.synchronize()
         res[name] = [t.cpu().numpy() for t in dev]
@@ -528,6 +529,7 @@ def main():
             if net is not None:
                 dy.set_closure(net)
             dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in init]
+            torch.cuda.synchronize()   # the copies run on torch's default stream
             dy.advance(*dev, nsteps)
             torch.cuda.synchronize()
             res[prec] = [t.cpu().numpy() for t in dev]
