@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -31,17 +32,20 @@ def _stale(target: str, deps: list[str]) -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "erf_b200.h")]
-    objs = []
-    for s in SOURCES:
-        src = os.path.join(CSRC, s)
-        obj = os.path.join(OBJ, s.replace(".cu", ".o"))
-        objs.append(obj)
-        if force or _stale(obj, [src] + hdrs):
-            cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
-            out = subprocess.run(cmd, capture_output=True, text=True)
-            log = os.path.join(OBJ, s + ".log")
-            with open(log, "w") as fh:
-                fh.write(" ".join(cmd) + "\n" + out.stdout + out.stderr)
+    objs = [os.path.join(OBJ, s.replace(".cu", ".o")) for s in SOURCES]
+    todo = [(s, o) for s, o in zip(SOURCES, objs) if force or _stale(o, [os.path.join(CSRC, s)] + hdrs)]
+
+    def compile_one(job):
+        s, obj = job
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, s), "-o", obj]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        with open(os.path.join(OBJ, s + ".log"), "w") as fh:
+            fh.write(" ".join(cmd) + "\n" + out.stdout + out.stderr)
+        return s, out
+
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        for s, out in ex.map(compile_one, todo):
             if out.returncode != 0:
                 raise RuntimeError(f"nvcc failed for {s}:\n{out.stderr[-4000:]}")
             if verbose:
