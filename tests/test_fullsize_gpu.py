@@ -8,7 +8,8 @@ workloads at their full sizes, advanced a few steps on the device.
   * dry ABL 64x64x64: total mass and total rho*theta are conserved (no heat
     flux through the walls);
   * terrain ABL 256x256x96: total sum(detJ * rho) is conserved;
-and a parity case at prime sizes (partial tiles in every direction).
+and parity cases at prime sizes (partial tiles in every direction) and at
+the smallest accepted grid (4 cells across).
 """
 import numpy as np
 import pytest
@@ -94,6 +95,25 @@ def test_prime_sizes_parity():
     assert dy.status() == 0
     dy.close()
     ref = oracle.advance(case.cfg, base, *init, 5)
+    errs = compare_states(got, ref)
+    bad = {k: v for k, v in errs.items() if not v <= 1e-10}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("mk", [cases.abl_deardorff, cases.moist_bubble])
+def test_minimum_sizes_parity(mk):
+    """The smallest grid the library accepts (4 cells, so periodic stencils of
+    +-3 wrap once) and odd sizes in y and z."""
+    from erf_b200 import Dycore
+    case = mk(nx=4, ny=5, nz=7)
+    dy = Dycore(case.cfg)
+    base = dy.make_base_state(case)
+    dy.set_base_state(base)
+    init = case.build_state(base[0])
+    got = dy.advance_host(*init, 3)
+    assert dy.status() == 0
+    dy.close()
+    ref = oracle.advance(case.cfg, base, *init, 3)
     errs = compare_states(got, ref)
     bad = {k: v for k, v in errs.items() if not v <= 1e-10}
     assert not bad, errs
