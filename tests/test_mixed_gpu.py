@@ -20,7 +20,7 @@ TOL_MIXED = 1e-2
 
 
 def output_errors(got, ref, moist):
-    """Relative L2 of the north-star output fields."""
+    """Relative L2 of the output fields (u, v, w, theta, water species, surface pressure)."""
     cg, ug, vg, wg = got
     cr, ur, vr, wr = ref
     err = {"u": rel_l2(ug, ur), "v": rel_l2(vg, vr), "w": rel_l2(wg, wr),
