@@ -14,6 +14,8 @@
 // the mixed form.  The prognostic state (conserved variables, momenta,
 // between-step velocities), the base state and the equation of state stay
 // FP64 in both, and every update of the state is accumulated in FP64.
+#include <cfloat>
+
 #include "kernels.cuh"
 
 namespace erfb {
@@ -128,6 +130,10 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
         S.mz[c] = (w1 * 0.5) * rs; wn[c] = w1;
     }
     if (k == g.nz - 1) { S.mz[c + g.sk] = 0.0; wn[c + g.sk] = 0.0; }
+    // a NaN or infinite velocity in the step's input (the state checks of
+    // stage_aux_cell cover rho and rho*theta)
+    if (!(fabs(uo[c]) <= DBL_MAX) || !(fabs(vo[c]) <= DBL_MAX) || !(fabs(wo[c]) <= DBL_MAX))
+        atomicOr(P.status, ST_NAN);
     stage_aux_cell<R>(P, cons, A, c, k);
 
     if (P.les == ERF_LES_SMAGORINSKY || P.les == ERF_LES_MLP || P.les == ERF_LES_DEARDORFF) {

@@ -298,6 +298,17 @@ int ensure_blocks(erf_b200_mlp* M, int nblk) {
     M->max_blocks = rc == ERF_B200_OK ? nblk : 0;
     return rc;
 }
+
+// Failure-detection self-test: an mbarrier that expects one arrival which
+// never comes, waited on with the bounded poll of the tensor-core kernels;
+// the wait must end by its limit and report, never hang.
+__global__ void k_selftest_wait(int limit, int* timed_out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) bar_init(&bar);
+    __syncthreads();
+    const bool done = bar_wait(&bar, 0u, limit);
+    if (threadIdx.x == 0) *timed_out = done ? 0 : 1;
+}
 }  // namespace
 
 extern "C" {
@@ -445,6 +456,20 @@ int erf_b200_mlp_infer(erf_b200_mlp* M, const float* x, int n, float* y) {
     int st = 0;
     cudaMemcpy(&st, M->status, sizeof(int), cudaMemcpyDeviceToHost);
     return st ? ERF_B200_ETIMEOUT : ERF_B200_OK;
+}
+
+int erf_b200_selftest_bounded_wait(int limit, int* timed_out) {
+    if (limit < 1 || !timed_out) return ERF_B200_EINVAL;
+    int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return ERF_B200_ENOMEM;
+    cudaMemset(d, 0xff, sizeof(int));
+    k_selftest_wait<<<1, 32>>>(limit, d);
+    int h = -1;
+    cudaError_t e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess || h < 0) return ERF_B200_ECUDA;
+    *timed_out = h;
+    return ERF_B200_OK;
 }
 
 }  // extern "C"

@@ -49,9 +49,9 @@ __device__ __forceinline__ void bar_init(uint64_t* bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// Bounded wait on the mbarrier phase; false if the limit ran out.
-__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
-    for (int it = 0; it < (1 << 22); ++it) {
+// Bounded wait on the mbarrier phase; false if the limit (polls) ran out.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, int limit = 1 << 22) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"

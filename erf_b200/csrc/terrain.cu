@@ -24,6 +24,8 @@
 //   k_ter_fv_*
 //   k_ter_post        erf_slow_rhs_post with terrain and the stage's
 //                     boundary round trips
+#include <cfloat>
+
 #include "kernels.cuh"
 
 namespace erfb {
@@ -464,6 +466,8 @@ __global__ void k_ter_step_begin(Params P, const double* __restrict__ cons, cons
         double wt = w_from_omega(P, i, j, nz, 0.0, urt, vrt);
         S.mz[c + g.sk] = (wt * 0.5) * (rho + rho); wn[c + g.sk] = wt;
     }
+    if (!(fabs(uo[c]) <= DBL_MAX) || !(fabs(vo[c]) <= DBL_MAX) || !(fabs(wo[c]) <= DBL_MAX))
+        atomicOr(P.status, ST_NAN);
     stage_aux_ter<R>(P, cons, A, c, k);
 
     if (P.les == ERF_LES_NONE) return;

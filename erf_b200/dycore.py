@@ -34,6 +34,7 @@ EXPORTS = [
     "erf_b200_ensemble_create", "erf_b200_ensemble_advance", "erf_b200_ensemble_sync", "erf_b200_ensemble_destroy",
     "erf_b200_last_cuda_error", "erf_b200_set_terrain", "erf_b200_make_base_state_terrain",
     "erf_b200_fast_rhs_T", "erf_b200_write_plotfile", "erf_b200_write_checkpoint", "erf_b200_read_checkpoint",
+    "erf_b200_selftest_bounded_wait",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs"]
@@ -91,6 +92,7 @@ def load_library():
     L.erf_b200_ensemble_advance.argtypes = [vp, i]
     L.erf_b200_ensemble_sync.argtypes = [vp]
     L.erf_b200_ensemble_destroy.argtypes = [vp]
+    L.erf_b200_selftest_bounded_wait.argtypes = [i, ctypes.POINTER(i)]
     L.erf_b200_write_plotfile.argtypes = [vp, ctypes.c_char_p, dp, dp, dp, dp, dp, dp, dp, ctypes.c_double, i]
     L.erf_b200_write_checkpoint.argtypes = [vp, ctypes.c_char_p] + [dp] * 9 + [i, ctypes.c_double, ctypes.c_double]
     L.erf_b200_read_checkpoint.argtypes = [vp, ctypes.c_char_p] + [dp] * 9 + [ctypes.POINTER(i),

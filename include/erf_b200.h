@@ -393,6 +393,13 @@ int erf_b200_mlp_infer(erf_b200_mlp* m, const float* x, int n, float* y);
  * returned on this host thread. */
 const char* erf_b200_last_cuda_error(void);
 
+/* Failure-detection self-test of the current device: one kernel waits on an
+ * mbarrier phase that can never complete, with the bounded poll the
+ * tensor-core kernels use (at most `limit` polls).  *timed_out is 1 when the
+ * bound ended the wait, as it must (the library's kernels then raise
+ * ERF_B200_ETIMEOUT and return instead of hanging).  Synchronous. */
+int erf_b200_selftest_bounded_wait(int limit, int* timed_out);
+
 /* Write an AMReX plotfile (single level, one grid) of a host state, as
  * ERF::WritePlotFile does (Source/IO/ERF_Plotfile.cpp:186-1500): directory
  * `dir` gets Header, Level_0/Cell_H and Level_0/Cell_D_00000.  Arrays are in
