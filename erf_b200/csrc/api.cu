@@ -341,7 +341,6 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     StateBuf OLD = c->S[p], N0 = c->S[1 - p], N1 = c->S[2], SUM = c->S[3];
     double** Vold = c->vel[p];
     double** Vnew = c->vel[1 - p];
-    dim3 cb = cell_block(), cg = cell_grid(g);
 
     TIMED(0, launch_step_begin<R>(P, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
                                   B.aux[0], B.mut, B.tke));
@@ -408,7 +407,10 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                 B.tke, B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
     }
-    if (P.moist) TIMED(8, (k_kessler_cells<<<cg, cb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
+    if (P.moist) {
+        dim3 kb(32, 1, KESS_KB), kg((g.nx + 31) / 32, g.ny, (g.nz + KESS_KB - 1) / KESS_KB);
+        TIMED(8, (k_kessler_cells<<<kg, kb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
+    }
 }
 
 void enqueue_step(erf_b200_ctx* c, int p, LaunchTimer* T = nullptr) {

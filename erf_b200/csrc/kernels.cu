@@ -874,19 +874,26 @@ __global__ void __launch_bounds__(1024) k_fast_vert(Params P, double dtau_d, dou
 // ---------------------------------------------------------------------------
 // Kessler, one thread per cell: the fall fluxes through the cell's bottom and
 // top faces are evaluated from the pre-update neighbours, so cells are
-// independent (same arithmetic as k_kessler).
+// independent (same arithmetic as k_kessler).  A block holds 32 columns x
+// KESS_KB levels: each thread evaluates the fall flux through its bottom face
+// and takes its top face's from the thread above through shared memory (the
+// block's top level evaluates its own), so each face's flux, with its two
+// pow() calls, is formed once.  The pressure is formed once per cell for
+// both the temperature and the saturation pressure.
 // ---------------------------------------------------------------------------
-__global__ void k_kessler_cells(Params P, const double* __restrict__ cin, double* __restrict__ cout, double dtn,
-                                double dz) {
+__global__ void __launch_bounds__(32 * KESS_KB) k_kessler_cells(Params P, const double* __restrict__ cin,
+                                                                double* __restrict__ cout, double dtn, double dz) {
+    __shared__ double sfz[KESS_KB][32];
     const Geo& g = P.g;
-    int i, j, k;
-    if (!cell_coords(g, i, j, k)) return;
+    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y, tz = threadIdx.z;
+    const int k = blockIdx.z * KESS_KB + tz;
+    const bool live = i < g.nx && k < g.nz;
     const int64_t N = g.ncell;
     const int nz = g.nz;
     const bool rain = P.kessler_rain;
     const bool has_qp = P.ncomp > 7;
     const double fac_cond = lcond / P.c_p;
-    int64_t c = cidx(g, i, j, k);
+    const int64_t c = live ? cidx(g, i, j, k) : 0;
     auto qp_of = [&](int64_t cc) { return has_qp ? cin[7 * N + cc] / cin[cc] : 0.0; };
     auto flux = [&](double ra, double qa) {
         qa = fmax(0.0, qa);
@@ -894,19 +901,29 @@ __global__ void k_kessler_cells(Params P, const double* __restrict__ cin, double
         double f = ra * Vt * qa;
         return (fabs(f) < 1e-14) ? 0.0 : f;
     };
-    double rho = cin[c];
+    double rho = 1.0, qp = 0.0, fz_lo = 0.0;
+    if (live) {
+        rho = cin[c];
+        qp = qp_of(c);
+        if (rain) {
+            if (k == 0) fz_lo = flux(rho, qp);
+            else fz_lo = flux(0.5 * (cin[c - g.sk] + rho), 0.5 * (qp_of(c - g.sk) + qp));
+        }
+    }
+    sfz[tz][threadIdx.x] = fz_lo;
+    __syncthreads();
+    if (!live) return;
     double rt = cin[N + c];
     double theta = rt / rho;
     double qv = cin[5 * N + c] / rho;
     double qc = cin[6 * N + c] / rho;
-    double qp = qp_of(c);
-    double tabs = eos_T(rho, rt, qv);
-    double pres = eos_p(rt, qv) / 100.;
+    const double p_pa = eos_p(rt, qv);
+    double tabs = p_pa / (R_d * rho * (1.0 + R_v / R_d * qv));   // eos_T(rho, rt, qv) with p formed once
+    double pres = p_pa / 100.;
     if (rain) {
-        double fz_lo, fz_hi;
-        if (k == 0) fz_lo = flux(rho, qp);
-        else fz_lo = flux(0.5 * (cin[c - g.sk] + rho), 0.5 * (qp_of(c - g.sk) + qp));
+        double fz_hi;
         if (k == nz - 1) fz_hi = flux(rho, qp);
+        else if (tz + 1 < KESS_KB) fz_hi = sfz[tz + 1][threadIdx.x];
         else fz_hi = flux(0.5 * (rho + cin[c + g.sk]), 0.5 * (qp + qp_of(c + g.sk)));
         qv = fmax(0.0, qv); qc = fmax(0.0, qc); qp = fmax(0.0, qp);
         double es = esatw(tabs);

@@ -86,6 +86,8 @@ struct TiledKz {
 
 // Host launchers of the dycore kernels (kernels.cu), instantiated for
 // R = double (plain form) and R = float (mixed form).
+// Levels per block of k_kessler_cells (blocks of 32 columns x KESS_KB levels)
+constexpr int KESS_KB = 8;
 template <class R>
 void tiled_setup(const Params& P, TiledKz* t);
 template <class R>
