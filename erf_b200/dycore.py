@@ -248,6 +248,19 @@ class Dycore:
                "advance_host")
         return tuple(arrs)
 
+    def write_plotfile(self, path: str, cons, u, v, w, z_nd=None, time: float = 0.0, step: int = 0):
+        """AMReX plotfile of a host state of this context's grid (base state
+        from set_base_state for pres_hse / dens_hse)."""
+        from .plotfile import write_plotfile
+        write_plotfile(self.cfg, path, cons, u, v, w, base=self.base, z_nd=z_nd, time=time, step=step)
+
+    def write_checkpoint(self, path: str, cons, u, v, w, z_nd=None, step: int = 0, time: float = 0.0):
+        """ERF-layout checkpoint of a host state with this context's base state."""
+        from .checkpoint import write_checkpoint
+        if self.base is None:
+            raise RuntimeError("write_checkpoint needs the base state (set_base_state)")
+        write_checkpoint(self.cfg, path, cons, u, v, w, self.base, z_nd=z_nd, step=step, dt=self.cfg.dt, time=time)
+
     def advance(self, cons_t, u_t, v_t, w_t, nsteps: int):
         """Advance dense device tensors in place (asynchronous on the context stream)."""
         c = self.cfg

@@ -6,7 +6,7 @@ import pytest
 
 from erf_b200 import cases
 from erf_b200 import terrain as T
-from erf_b200.checkpoint import read_checkpoint, write_checkpoint
+from erf_b200.checkpoint import read_checkpoint
 
 pytestmark = pytest.mark.gpu
 
@@ -43,7 +43,10 @@ def test_restart_is_bit_identical(tmp_path, kind):
     mid = b.advance_host(*init, 2)
     b.close()
     path = str(tmp_path / "chk00002")
-    write_checkpoint(case.cfg, path, *mid, base, z_nd=z, step=2, dt=case.cfg.dt, time=2 * case.cfg.dt)
+    b = _ctx(case, base, z)          # the context's own writer (its base state)
+    b.write_checkpoint(path, *mid, z_nd=z, step=2, time=2 * case.cfg.dt)
+    b.write_plotfile(str(tmp_path / "plt00002"), *mid, z_nd=z, time=2 * case.cfg.dt, step=2)
+    b.close()
     r = read_checkpoint(case.cfg, path)
     assert r["step"] == 2
     c = _ctx(case, r["base"], r["z_nd"])
