@@ -97,11 +97,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 __device__ __forceinline__ void put_row(unsigned char* tile, int K, int r, const float* v, int n) {
 #pragma unroll
     for (int c = 0; c < K / 8; ++c) {
-        __align__(16) __nv_bfloat16 h[8];
+        __align__(16) __nv_bfloat162 h[4];   // pairs: one round-to-nearest conversion per two values
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            int k = c * 8 + q;
-            h[q] = __float2bfloat16_rn(k < n ? v[k] : 0.0f);
+        for (int q = 0; q < 4; ++q) {
+            const int k = c * 8 + 2 * q;
+            h[q] = __floats2bfloat162_rn(k < n ? v[k] : 0.0f, k + 1 < n ? v[k + 1] : 0.0f);
         }
         *reinterpret_cast<uint4*>(tile + kmaj(r, c * 8, K)) = *reinterpret_cast<const uint4*>(h);
     }
