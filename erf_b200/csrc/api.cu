@@ -499,6 +499,10 @@ int unpack(erf_b200_ctx* c, const erf_b200_fab* f, int kind, int ncomp, const do
 
 }  // namespace
 
+// The configuration checks of erf_b200_create, shared with the entry points
+// that take a configuration without a context.
+int erfb::validate_config(const erf_b200_config* c) { return validate(c); }
+
 extern "C" {
 
 int erf_b200_config_defaults(erf_b200_config* cfg) {

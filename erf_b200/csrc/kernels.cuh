@@ -84,6 +84,9 @@ struct TiledKz {
     int cell, mom, post;
 };
 
+// erf_b200_create's configuration checks (api.cu): ERF_B200_OK or an error code.
+int validate_config(const erf_b200_config* c);
+
 // Host launchers of the dycore kernels (kernels.cu), instantiated for
 // R = double (plain form) and R = float (mixed form).
 // Levels per block of k_kessler_cells (blocks of 32 columns x KESS_KB levels)

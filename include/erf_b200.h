@@ -337,17 +337,22 @@ int erf_b200_kessler_advance(erf_b200_ctx* ctx, const erf_b200_fab* cons, double
  * Allocation-free Kessler step.  No counterpart in the reference: it is the
  * same computation as erf_b200_kessler_advance for callers that cannot
  * allocate device memory -- a host code whose device memory is all reserved
- * by its own pool (an AMReX arena, say), or code that runs while a CUDA graph
- * is being captured on its stream, where cudaMalloc is not allowed.  It takes
- * no context.  Its scratch is one library-owned device array of
- * ERF_B200_NOALLOC_MAX_DOUBLES doubles (16 MiB), present on every GPU that
- * loads the library until the process exits; requests with
- * ncomp*nx*ny*nz > ERF_B200_NOALLOC_MAX_DOUBLES are rejected with
- * ERF_B200_EINVAL.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current, so make that first
- * call before any stream capture.  All calls share the one array: calls that
+ * up front by its own pool (an AMReX arena, say) and which must not see a
+ * second allocator beside it.  It takes no context.  Its scratch is one
+ * library-owned device array of ERF_B200_NOALLOC_MAX_DOUBLES doubles
+ * (16 MiB), present on every GPU that loads the library until the process
+ * exits; requests with ncomp*nx*ny*nz > ERF_B200_NOALLOC_MAX_DOUBLES, or
+ * with more than 65535 levels in the valid region or the view, are rejected
+ * with ERF_B200_EINVAL, and configurations erf_b200_create rejects (Kessler
+ * over terrain among them) with ERF_B200_ECONFIG.  The first call in a
+ * device's context looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current, so make that first call
+ * before any stream capture; after cudaDeviceReset the next call looks it up
+ * again in the new context.  All calls share the one array: calls that
  * overlap on the GPU (different streams, or different host threads on the
- * same device) race, so serialise them.  Asynchronous on `stream`
+ * same device) race, so serialise them.  If a CUDA error from earlier work
+ * is pending on the calling thread, the call launches nothing, leaves that
+ * error in place and returns ERF_B200_ECUDA.  Asynchronous on `stream`
  * (a cudaStream_t; NULL = legacy default stream).
  * ------------------------------------------------------------------------- */
 #define ERF_B200_NOALLOC_MAX_DOUBLES 2097152

@@ -70,6 +70,18 @@ def advance(cfg, base, cons, u, v, w, nsteps):
     return cons, u, v, w
 
 
+def kessler(cfg, cons, dt):
+    """Kessler microphysics alone on a copy of a dense cons array."""
+    L = lib()
+    L.oracle_kessler.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_double]
+    L.oracle_kessler.restype = ctypes.c_int
+    out = np.ascontiguousarray(cons, dtype=np.float64).copy()
+    rc = L.oracle_kessler(ctypes.byref(cfg), _p(out), float(dt))
+    if rc != 0:
+        raise RuntimeError("oracle_kessler failed: %d" % rc)
+    return out
+
+
 def interp(kind: int, s6, upw: float, frac: float = 1.0) -> float:
     s = np.ascontiguousarray(s6, dtype=np.float64)
     return lib().oracle_interp(int(kind), _p(s), float(upw), float(frac))

@@ -2430,6 +2430,21 @@ int oracle_advance_terrain(const erf_b200_config* cfg, const double* z_nd, const
     return 0;
 }
 
+// Kessler alone on a dense valid-region state (cons[ncomp][nz][ny][nx]), as
+// ERF::advance_microphysics runs it after the dycore (ERF_Advance.cpp:174 ->
+// Kessler::Copy_State_to_Micro, AdvanceKessler, Copy_Micro_to_State).
+int oracle_kessler(const erf_b200_config* cfg, double* cons, double dt) {
+    if (cfg->moisture != ERF_MOIST_KESSLER && cfg->moisture != ERF_MOIST_KESSLER_NORAIN) return 1;
+    std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
+    Fab f;
+    o->alloc(f, CC, o->ngc, o->ncomp);
+    load_cc(f, cons, nx, ny, nz, o->ncomp);
+    o->kessler(f, dt);
+    store_cc(f, cons, nx, ny, nz, o->ncomp);
+    return 0;
+}
+
 // Interpolant known-answer hook: evaluates one face interpolant.
 double oracle_interp(int type, const double* s6, double upw, double frac) { return Oracle::interp(type, s6, upw, frac); }
 

@@ -1,6 +1,7 @@
 """Full-size GPU checks through properties that do not depend on the grid
-size (the oracle is too slow at these sizes): the three single-GPU
-workloads at their full sizes, advanced a few steps on the device.
+size, over runs longer than the field-by-field oracle comparisons of
+test_fullsize_parity_gpu.py: the three single-GPU workloads at their full
+sizes, advanced on the device.
 
   * moist bubble 128x128x80 (plain FP64 and the FP32-bulk form): total mass
     is conserved (flux form, no flux through the walls), water stays
