@@ -24,6 +24,7 @@ MOLEC_NONE, MOLEC_CONSTANT, MOLEC_CONSTANT_ALPHA = 0, 1, 2
 MOIST_NONE, MOIST_KESSLER, MOIST_KESSLER_NORAIN = 0, 1, 2
 BC_NO_SLIP_WALL, BC_SLIP_WALL, BC_PERIODIC = 5, 6, 7
 PREC_FP64, PREC_MIXED = 0, 1
+SUBSTEP_IMPLICIT, SUBSTEP_NONE = 0, 1
 # conserved components (Source/ERF_IndexDefines.H:36-43)
 RHO_COMP, RHOTHETA_COMP, RHOKE_COMP, RHOQKE_COMP, RHOSCALAR_COMP, RHOQ1_COMP = 0, 1, 2, 3, 4, 5
 
@@ -58,7 +59,8 @@ class ErfConfig(ctypes.Structure):
         ("abl_geo_forcing", ctypes.c_double * 3),
         ("precision", ctypes.c_int),
         ("use_terrain", ctypes.c_int),
-        ("reserved", ctypes.c_int * 6),
+        ("substepping_type", ctypes.c_int),
+        ("reserved", ctypes.c_int * 5),
     ]
 
     def copy(self) -> "ErfConfig":
@@ -163,4 +165,7 @@ def from_inputs(keys: dict) -> ErfConfig:
             c.mri_ratio = int(g(k))
     if g("buoyancy_type") is not None:
         c.buoyancy_type = int(g("buoyancy_type"))
+    st = g("substepping_type")
+    if st is not None:
+        c.substepping_type = {"None": SUBSTEP_NONE, "Implicit": SUBSTEP_IMPLICIT}[str(st).strip('"')]
     return c

@@ -122,7 +122,10 @@ int validate(const erf_b200_config* c) {
     if (!c) return ERF_B200_EINVAL;
     if (c->nx < 4 || c->ny < 4 || c->nz < 4) return ERF_B200_ECONFIG;
     if (!(c->dx > 0 && c->dy > 0 && c->dz > 0 && c->dt > 0)) return ERF_B200_ECONFIG;
-    if (c->mri_ratio < 2 || (c->mri_ratio % 2) != 0) return ERF_B200_ECONFIG;
+    if (c->substepping_type != ERF_SUBSTEP_IMPLICIT && c->substepping_type != ERF_SUBSTEP_NONE) return ERF_B200_ECONFIG;
+    // the substep ratio matters with substepping only (ERF_MRI.H:202-204)
+    if (c->substepping_type == ERF_SUBSTEP_IMPLICIT && (c->mri_ratio < 2 || (c->mri_ratio % 2) != 0))
+        return ERF_B200_ECONFIG;
     if (c->zlo_bc != ERF_BC_NO_SLIP_WALL && c->zlo_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
     if (c->zhi_bc != ERF_BC_NO_SLIP_WALL && c->zhi_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
     // the vertical momentum stencils reduce order near walls only for the
@@ -225,22 +228,30 @@ dim3 cell_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.n
 dim3 col_block() { return dim3(32, 4, 1); }
 dim3 col_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, 1); }
 
-// Substep schedule of MRISplitIntegrator::advance (ERF_MRI.H:255-282)
+// Substep schedule of MRISplitIntegrator::advance (ERF_MRI.H:255-282).
+// Without substepping every stage takes one update of its whole length.
+bool no_substepping(const erf_b200_config& f) { return f.substepping_type == ERF_SUBSTEP_NONE; }
 void stage_schedule(const erf_b200_config& f, int nrk, int& nsub, double& dtau, double& slow_dt) {
     double dt = f.dt;
-    double sub_dt = dt / f.mri_ratio;
+    const bool nosub = no_substepping(f);
+    double sub_dt = nosub ? 0.0 : dt / f.mri_ratio;
     if (nrk == 0) {
-        if (f.force_stage1_single_substep) { nsub = 1; dtau = dt / 3.0; }
+        if (f.force_stage1_single_substep || nosub) { nsub = 1; dtau = dt / 3.0; }
         else { nsub = f.mri_ratio / 3; dtau = sub_dt; }
         slow_dt = dt / 3.0;
     } else if (nrk == 1) {
-        nsub = f.mri_ratio / 2; dtau = sub_dt; slow_dt = dt / 2.0;
+        if (nosub) { nsub = 1; dtau = 0.5 * dt; }
+        else { nsub = f.mri_ratio / 2; dtau = sub_dt; }
+        slow_dt = dt / 2.0;
     } else {
-        nsub = f.mri_ratio; dtau = sub_dt; slow_dt = dt;
+        if (nosub) { nsub = 1; dtau = dt; }
+        else { nsub = f.mri_ratio; dtau = sub_dt; }
+        slow_dt = dt;
     }
 }
 
 int substeps_per_step(const erf_b200_config& f) {
+    if (no_substepping(f)) return 0;   // no acoustic substeps, no lagged d(rho theta)
     int tot = 0;
     for (int nrk = 0; nrk < 3; ++nrk) { int n; double a, b; stage_schedule(f, nrk, n, a, b); tot += n; }
     return tot;
@@ -289,6 +300,7 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
     const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
+    const bool nosub = no_substepping(c->cfg);
     for (int nrk = 0; nrk < 3; ++nrk) {
         StateBuf Sst = stage[nrk], Snew = outs[nrk];
         StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
@@ -296,7 +308,7 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
         double facinv = 1.0 / (double)nsub;
         double D = dtau * dtau * beta_2 * beta_2 * g.dzi;
-        if (fork) {
+        if (fork && !nosub) {
             cudaEventRecord(c->ev_fork, st);
             cudaStreamWaitEvent(c->side, c->ev_fork, 0);
             launch_fast_coef<R>(P, c->side, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
@@ -309,11 +321,13 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                          B.avy, B.avz));
         TIMED(4, launch_ter_slow_mom<R>(P, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12, B.t13,
                                         B.t23, B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz));
-        if (!fork)
+        if (nosub)
+            TIMED(10, launch_no_substep<R>(P, st, slow_dt, OLD, B.Fcons, B.Fmx, B.Fmy, B.Fmz, SUM));
+        else if (!fork)
             TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
         else
             cudaStreamWaitEvent(st, c->ev_coef, 0);
-        for (int ks = 0; ks < nsub; ++ks) {
+        for (int ks = 0; ks < (nosub ? 0 : nsub); ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
             TIMED(5, launch_ter_fast_h<R>(P, st, ks, dtau, facinv, Sprev, prt, Sst, Acur, B.Fmx, B.Fmy, B.lag[lp],
@@ -356,6 +370,7 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     int lp = (p * c->lag_parity_per_step) & 1;
     const double beta_s = 0.1;
     const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
+    const bool nosub = no_substepping(c->cfg);
     for (int nrk = 0; nrk < 3; ++nrk) {
         StateBuf Sst = stage[nrk], Snew = outs[nrk];
         StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
@@ -371,7 +386,8 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                 launch_plane_avg<R>(P, c->side, Sst.cons, Acur.prim, c->pavg);
                 cudaEventRecord(c->ev_pavg, c->side);
             }
-            launch_fast_coef<R>(P, c->side, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
+            if (!nosub)
+                launch_fast_coef<R>(P, c->side, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ);
             cudaEventRecord(c->ev_coef, c->side);
         }
         if (P.les == ERF_LES_MLP) {
@@ -389,11 +405,13 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         if (plane && fork) cudaStreamWaitEvent(st, c->ev_pavg, 0);
         TIMED(4, launch_slow_mom<R>(P, c->tkz, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12,
                                     B.t13, B.t23, c->pavg, B.Fmx, B.Fmy, B.Fmz));
-        if (!fork)
-            TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
-        else
+        if (fork)
             cudaStreamWaitEvent(st, c->ev_coef, 0);
-        for (int ks = 0; ks < nsub; ++ks) {
+        if (nosub)
+            TIMED(10, launch_no_substep<R>(P, st, slow_dt, OLD, B.Fcons, B.Fmx, B.Fmy, B.Fmz, SUM));
+        else if (!fork)
+            TIMED(9, launch_fast_coef<R>(P, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP, B.cQ));
+        for (int ks = 0; ks < (nosub ? 0 : nsub); ++ks) {
             StateBuf Sprev = (ks == 0) ? OLD : SUM;
             int prt = ks > 0;
             TIMED(5, launch_fast_h<R>(P, st, ks, nrk, dtau, facinv, Sprev, prt, Sst, Acur, B.Fmx, B.Fmy, B.lag[lp],
@@ -859,7 +877,9 @@ int erf_b200_kernels_per_step(const erf_b200_ctx* c, int* launches) {
         int nsub; double a, b;
         stage_schedule(c->cfg, nrk, nsub, a, b);
         int stress = c->P.les == ERF_LES_MLP ? 2 : (c->P.use_diff ? 1 : 0);
-        n += 4 + stress + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0) + 2 * nsub;
+        // slow_cell, slow_mom, post + (fast_coeffs and 2 per substep, or the no-substep update)
+        int fast = no_substepping(c->cfg) ? 1 : 1 + 2 * nsub;
+        n += 3 + fast + stress + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0);
     }
     *launches = n;
     return ERF_B200_OK;
@@ -1092,6 +1112,24 @@ int erf_b200_fast_rhs_T(erf_b200_ctx* c, int step, int nrk, const erf_b200_fab* 
                         const erf_b200_fab* S_prev, const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
                         const erf_b200_fab* S_scratch, double dtau, double facinv) {
     return fast_rhs_pass(c, true, step, nrk, S_slow_rhs, S_prev, S_stage, S_data, S_scratch, dtau, facinv);
+}
+
+// The no_substep hook (ERF_TI_no_substep_fun.H:6-150): S_sum's fast
+// variables (rho, rho*theta, momenta) = S_old + slow_dt * F_slow, then the
+// boundary fill of S_sum's ghost cells.
+int erf_b200_no_substep(erf_b200_ctx* c, const erf_b200_fab* S_sum, const erf_b200_fab* S_old,
+                        const erf_b200_fab* F_slow, double slow_dt, int nrk) {
+    if (!c || c->mixed || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
+    const Geo& g = c->g;
+    if (!fab4_ok(S_sum, g, 2) || !fab4_ok(S_old, g, 2) || !fab4_ok(F_slow, g, 2)) return ERF_B200_EINVAL;
+    Bulk<double>& B = c->bd;
+    StateBuf OLD = c->S[0], SUM = c->S[3];
+    int rc;
+    if ((rc = pack4(c, F_slow, 2, B.Fcons, B.Fmx, B.Fmy, B.Fmz))) return rc;
+    if ((rc = pack4(c, S_old, 2, OLD.cons, OLD.mx, OLD.my, OLD.mz))) return rc;
+    launch_no_substep<double>(c->P, c->stream, slow_dt, OLD, B.Fcons, B.Fmx, B.Fmy, B.Fmz, SUM);
+    if ((rc = unpack4(c, S_sum, 2, SUM.cons, SUM.mx, SUM.my, SUM.mz))) return rc;
+    return cuda_fail(cudaGetLastError());
 }
 
 int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b200_fab* S_rhs,

@@ -432,6 +432,29 @@ __global__ void k_fast_h(Params P, int step, int nrk, double dtau_d, double faci
 }
 
 // ---------------------------------------------------------------------------
+// The stage update without acoustic substepping (no_substep_fun,
+// TimeIntegration/ERF_TI_no_substep_fun.H:6-150, fixed or no terrain):
+// S_sum = S_old + slow_dt * F_slow for rho, rho*theta and the three momenta,
+// accumulated in FP64 from the slow right-hand side (type R).  The boundary
+// fill that follows in the reference (apply_bcs of S_sum) is the first of the
+// two momentum round trips the slow-post kernels apply on read.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_no_substep(Geo g, double slow_dt, StateBuf Sold, const R* __restrict__ Fcons,
+                             const R* __restrict__ Fmx, const R* __restrict__ Fmy, const R* __restrict__ Fmz,
+                             StateBuf Ssum) {
+    int i, j, k;
+    if (!cell_coords(g, i, j, k)) return;
+    const int64_t N = g.ncell, c = cidx(g, i, j, k);
+    Ssum.cons[c] = Sold.cons[c] + slow_dt * (double(Fcons[c]));
+    Ssum.cons[N + c] = Sold.cons[N + c] + slow_dt * (double(Fcons[N + c]));
+    Ssum.mx[c] = Sold.mx[c] + slow_dt * double(Fmx[c]);
+    Ssum.my[c] = Sold.my[c] + slow_dt * double(Fmy[c]);
+    Ssum.mz[c] = Sold.mz[c] + slow_dt * double(Fmz[c]);
+    if (k == g.nz - 1) Ssum.mz[c + g.sk] = Sold.mz[c + g.sk] + slow_dt * double(Fmz[c + g.sk]);
+}
+
+// ---------------------------------------------------------------------------
 // Kessler warm-rain microphysics, one thread per column, in place
 // (Microphysics/Kessler/ERF_Kessler.cpp:11-185, ERF_Init_Kessler.cpp:64-99,
 // ERF_Update_Kessler.cpp:14-40).  The rain flux through face k+1 is computed
@@ -1718,6 +1741,11 @@ void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double d
                                                          lag_in, lag_out, avx, avy, outx, outy);
 }
 template <class R>
+void launch_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons, const R* Fmx,
+                       const R* Fmy, const R* Fmz, StateBuf Ssum) {
+    k_no_substep<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P.g, slow_dt, Sold, Fcons, Fmx, Fmy, Fmz, Ssum);
+}
+template <class R>
 void launch_fast_coef(const Params& P, cudaStream_t st, dim3 grid, dim3 block, size_t smem, double D, StateBuf Sst,
                       StageAux<R> A, R* cA, R* cInvB, R* cCB, R* cP, R* cQ) {
     k_fast_coef<R><<<grid, block, smem, st>>>(P, D, Sst, A, cA, cInvB, cCB, cP, cQ);
@@ -1765,6 +1793,8 @@ void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow
     template void launch_stage_aux<R>(const Params&, cudaStream_t, const double*, StageAux<R>);                      \
     template void launch_fast_h<R>(const Params&, cudaStream_t, int, int, double, double, StateBuf, int, StateBuf,   \
                                    StageAux<R>, const R*, const R*, const R*, R*, R*, R*, double*, double*);         \
+    template void launch_no_substep<R>(const Params&, cudaStream_t, double, StateBuf, const R*, const R*, const R*, \
+                                       const R*, StateBuf);                                                          \
     template void launch_fast_coef<R>(const Params&, cudaStream_t, dim3, dim3, size_t, double, StateBuf,             \
                                       StageAux<R>, R*, R*, R*, R*, R*);                                              \
     template void launch_fast_vert<R>(const Params&, cudaStream_t, dim3, dim3, size_t, double, double, double,       \

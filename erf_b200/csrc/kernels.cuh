@@ -116,6 +116,9 @@ void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double d
                    int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in, R* lag_out,
                    R* avx, R* avy, double* outx, double* outy);
 template <class R>
+void launch_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons, const R* Fmx,
+                       const R* Fmy, const R* Fmz, StateBuf Ssum);
+template <class R>
 void launch_fast_coef(const Params& P, cudaStream_t st, dim3 grid, dim3 block, size_t smem, double D, StateBuf Sst,
                       StageAux<R> A, R* cA, R* cInvB, R* cCB, R* cP, R* cQ);
 template <class R>

@@ -117,6 +117,10 @@ typedef struct erf_b200_fab {
  * ERF_AdvStruct.H:26-186, ERF_TurbStruct.H:29-210, ERF_DiffStruct.H:26-32),
  * plus the grid and the fixed time step.  POD, passed by pointer.
  * ------------------------------------------------------------------------- */
+/* Substepping types (SubsteppingType, DataStructs/ERF_DataStruct.H) */
+#define ERF_SUBSTEP_IMPLICIT 0
+#define ERF_SUBSTEP_NONE     1
+
 typedef struct erf_b200_config {
     /* grid: one box covering the domain, periodic in x and y */
     int    nx, ny, nz;
@@ -159,7 +163,12 @@ typedef struct erf_b200_config {
     /* static terrain-following grid (SolverChoice::use_terrain with
      * terrain_type Static): z_phys_nd installed by erf_b200_set_terrain */
     int    use_terrain;
-    int    reserved[6];
+    /* SolverChoice::substepping_type: ERF_SUBSTEP_IMPLICIT (acoustic
+     * substepping, the default) or ERF_SUBSTEP_NONE (one update per RK stage
+     * with the whole slow right-hand side, MRISplitIntegrator::set_no_substep,
+     * TimeIntegration/ERF_MRI.H:177-180, 255-324; mri_ratio is then unused) */
+    int    substepping_type;
+    int    reserved[5];
 } erf_b200_config;
 
 /* Opaque context: owns all integrator scratch (S_sum, S_scratch, F_slow,
@@ -259,9 +268,10 @@ int erf_b200_advance_host(erf_b200_ctx* ctx, double* cons, double* u,
  * kernel_launches (nslots >= ERF_B200_NUM_KERNEL_SLOTS) receive the summed
  * device time and launch count per kernel slot:
  *   0 step_begin, 1 stress, 2 slow_cell, 3 plane_avg, 4 slow_mom,
- *   5 fast_horizontal, 6 fast_column, 7 slow_post, 8 kessler, 9 fast_coeffs.
+ *   5 fast_horizontal, 6 fast_column, 7 slow_post, 8 kessler, 9 fast_coeffs,
+ *   10 no_substep (the stage update without acoustic substepping).
  * ------------------------------------------------------------------------- */
-#define ERF_B200_NUM_KERNEL_SLOTS 10
+#define ERF_B200_NUM_KERNEL_SLOTS 11
 int erf_b200_advance_profiled(erf_b200_ctx* ctx,
                               const erf_b200_fab* cons, const erf_b200_fab* xvel,
                               const erf_b200_fab* yvel, const erf_b200_fab* zvel,
@@ -321,6 +331,15 @@ int erf_b200_fast_rhs_T(erf_b200_ctx* ctx, int step, int nrk,
                         const erf_b200_fab* S_stage, const erf_b200_fab* S_data,
                         const erf_b200_fab* S_scratch,
                         double dtau, double facinv);
+
+/* The no_substep hook of MRISplitIntegrator (set_no_substep,
+ * TimeIntegration/ERF_MRI.H:177-180, called at :320; the lambda of
+ * ERF_TI_no_substep_fun.H:6-150) for substepping_type ERF_SUBSTEP_NONE:
+ * S_sum's rho, rho*theta and momenta = S_old + slow_dt * F_slow, then the
+ * boundary fill of S_sum.  nrk is the RK stage (0..2). */
+int erf_b200_no_substep(erf_b200_ctx* ctx, const erf_b200_fab* S_sum,
+                        const erf_b200_fab* S_old, const erf_b200_fab* F_slow,
+                        double slow_dt, int nrk);
 
 /* erf_slow_rhs_post (TimeIntegration/ERF_slow_rhs_post.cpp:49-559). */
 int erf_b200_slow_rhs_post(erf_b200_ctx* ctx, int nrk, double slow_dt,

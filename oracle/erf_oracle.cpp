@@ -1313,6 +1313,21 @@ struct Oracle {
     }
 
     // ------------------------------------------------------------------
+    // The stage update without acoustic substepping (no_substep_fun,
+    // TimeIntegration/ERF_TI_no_substep_fun.H:6-150, fixed or no terrain):
+    // the fast variables (rho, rho*theta and the three momenta) of S_sum are
+    // S_old + slow_dt * F_slow over the valid cells and faces.
+    // ------------------------------------------------------------------
+    void no_substep(State& Ssum, const State& Sold, const State& F, double slow_dt) const {
+        loop(valid(CC), [&](int i, int j, int k) {
+            for (int n = 0; n < 2; ++n) Ssum.cons(i, j, k, n) = Sold.cons(i, j, k, n) + slow_dt * (F.cons(i, j, k, n));
+        });
+        loop(valid(XF), [&](int i, int j, int k) { Ssum.mx(i, j, k) = Sold.mx(i, j, k) + slow_dt * F.mx(i, j, k); });
+        loop(valid(YF), [&](int i, int j, int k) { Ssum.my(i, j, k) = Sold.my(i, j, k) + slow_dt * F.my(i, j, k); });
+        loop(valid(ZF), [&](int i, int j, int k) { Ssum.mz(i, j, k) = Sold.mz(i, j, k) + slow_dt * F.mz(i, j, k); });
+    }
+
+    // ------------------------------------------------------------------
     // One full time step: ERF::Advance (TimeIntegration/ERF_Advance.cpp:19-233)
     // -> advance_dycore (ERF_advance_dycore.cpp:37-305) -> MRISplitIntegrator::
     // advance (ERF_MRI.H:187-369) -> advance_microphysics.
@@ -2226,22 +2241,32 @@ struct Oracle {
         apply_bcs(S_old, Vnew, ngc, ngv, false, true);
         cons_to_prim(S_old.cons, ngc, prim, pi_stage);
 
-        // MRISplitIntegrator::advance
+        // MRISplitIntegrator::advance (ERF_MRI.H:187-324)
         copy_state(S_new, S_old);
+        const bool nosub = c.substepping_type == ERF_SUBSTEP_NONE;
         int ratio = c.mri_ratio;
-        double sub_dt = dt / ratio;
+        double sub_dt = nosub ? 0.0 : dt / ratio;
         for (int nrk = 0; nrk < 3; ++nrk) {
             int nsub; double dtau;
             if (nrk == 0) {
-                if (c.force_stage1_single_substep) { nsub = 1; dtau = dt / 3.0; }
+                if (c.force_stage1_single_substep || nosub) { nsub = 1; dtau = dt / 3.0; }
                 else { nsub = ratio / 3; dtau = sub_dt; }
-            } else if (nrk == 1) { nsub = ratio / 2; dtau = sub_dt; }
-            else { nsub = ratio; dtau = sub_dt; }
+            } else if (nrk == 1) {
+                if (nosub) { nsub = 1; dtau = 0.5 * dt; }
+                else { nsub = ratio / 2; dtau = sub_dt; }
+            } else {
+                if (nosub) { nsub = 1; dtau = dt; }
+                else { nsub = ratio; dtau = sub_dt; }
+            }
             double slow_dt = (nrk == 0 ? dt / 3.0 : (nrk == 1 ? dt / 2.0 : dt));
             if (nrk > 0) cons_to_prim(S_new.cons, ngc, prim, pi_stage);
             slow_rhs_pre(nrk, slow_dt, F_slow, S_new, S_scr, Vnew);
             double inv_fac = 1.0 / (double)nsub;
-            for (int ks = 0; ks < nsub; ++ks) {
+            if (nosub) {
+                no_substep(S_sum, S_old, F_slow, nsub * dtau);
+                apply_bcs(S_sum, Vnew, ngc, ngv, true, false);
+            }
+            for (int ks = 0; ks < (nosub ? 0 : nsub); ++ks) {
                 if (ks == 0) make_fast_coeffs(S_new, dtau, beta_s);
                 if (terrain) fast_rhs_T(ks, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);
                 else fast_rhs_N(ks, nrk, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 from plotfile import read_plotfile  # noqa: E402
 
-TESTS = ["TaylorGreenAdvecting", "TaylorGreenAdvectingDiffusing"]
+TESTS = ["TaylorGreenAdvecting", "TaylorGreenAdvectingDiffusing", "EkmanSpiral", "IsentropicVortexAdvecting"]
 
 if __name__ == "__main__":
     ref = sys.argv[1]

@@ -26,13 +26,20 @@ def schedule(cfg, nrk):
     return cfg.mri_ratio, sub, cfg.dt
 
 
-def test_per_pass_composition_matches_fused_step():
+@pytest.mark.parametrize("nosub", [False, True])
+def test_per_pass_composition_matches_fused_step(nosub):
+    """With nosub the stages call the no_substep hook entry
+    (erf_b200_no_substep) in place of the acoustic substeps, at a time step
+    inside the explicit acoustic limit."""
     import ctypes
     import torch
     from erf_b200 import Dycore
     from erf_b200.dycore import dense_fab, ErfFab
     case = cases.abl_dry(nx=32, ny=24, nz=16)
     cfg = case.cfg
+    if nosub:
+        cfg.substepping_type = C.SUBSTEP_NONE
+        cfg.dt = 0.05
     nx, ny, nz, nc = cfg.nx, cfg.ny, cfg.nz, cfg.ncomp
     dy = Dycore(cfg)
     base = dy.make_base_state(case)
@@ -91,6 +98,7 @@ def test_per_pass_composition_matches_fused_step():
     L.erf_b200_slow_rhs_pre.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double] + [ctypes.c_void_p] * 6
     L.erf_b200_fast_rhs_N.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5 + [ctypes.c_double] * 2
     L.erf_b200_slow_rhs_post.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double] + [ctypes.c_void_p] * 5
+    L.erf_b200_no_substep.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_double, ctypes.c_int]
     fc = dense_fab(cons, 0, nx, ny, nz, nc)
     torch.cuda.synchronize()
     assert L.erf_b200_turbulent_viscosity(dy.ctx, *vf([u, v, w]), ctypes.byref(fc)) == 0
@@ -102,7 +110,11 @@ def test_per_pass_composition_matches_fused_step():
         assert L.erf_b200_slow_rhs_pre(dy.ctx, nrk, slow_dt, fabs(S_rhs, 2), fabs(stage, nc), fabs(S_scr, 2),
                                        *vf(vel)) == 0
         S_data = [a.clone() for a in S_old]
-        for ks in range(nsub):
+        if nosub:
+            torch.cuda.synchronize()
+            assert L.erf_b200_no_substep(dy.ctx, fabs(S_data, nc), fabs(S_old, nc), fabs(S_rhs, 2), slow_dt, nrk) == 0
+            torch.cuda.synchronize()
+        for ks in range(0 if nosub else nsub):
             prev = S_old if ks == 0 else [a.clone() for a in S_data]
             torch.cuda.synchronize()
             assert L.erf_b200_fast_rhs_N(dy.ctx, ks, nrk, fabs(S_rhs, 2), fabs(prev, nc), fabs(stage, nc),
