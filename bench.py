@@ -86,6 +86,44 @@ def algorithmic_values_per_cell(cfg):
     }
 
 
+def survey_bytes_per_cell_step(cfg, substeps):
+    """The pass model of the benchmark's byte budget: each value counted once
+    per forced pass at 8 bytes.  Per cell per step: slow-pre 3 x (5 read +
+    5 write); each acoustic substep prev 5 + stage 5 + rhs 5 + new 5 + average
+    momenta 3 read + 3 write; slow-post 3 x (3 + 3 S) with S slow scalars
+    (the passive scalar, rho*KE with Deardorff, the moisture species);
+    closure 7 values (Smagorinsky) or 9 (Deardorff); Kessler 9; terrain adds
+    4 values to each slow-pre and substep pass.  Dry ABL 64^3: 315 values
+    (2520 B); moist bubble: 344 (2752 B); terrain ABL: 378 (3024 B)."""
+    nq = cfg.ncomp - 5
+    S = 1 + (1 if cfg.les_type == 2 else 0) + nq
+    vals = 3 * 10 + substeps * 26 + 3 * (3 + 3 * S)
+    vals += {0: 0, 1: 7, 2: 9}.get(cfg.les_type, 7)
+    vals += 9 if cfg.moisture != 0 else 0
+    vals += 4 * (3 + substeps) if cfg.use_terrain else 0
+    return 8 * vals
+
+
+def substeps_per_step(cfg):
+    """Acoustic substeps per RK3 step (ERF_MRI.H:255-282): R/3 (or 1 with
+    force_stage1_single_substep), R/2 and R; none without substepping."""
+    if getattr(cfg, "substepping_type", 0) == 1:
+        return 0
+    r = cfg.mri_ratio
+    return (1 if cfg.force_stage1_single_substep else r // 3) + r // 2 + r
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def bytes_per_cell(vals, bulk_bytes):
     return {k: 8 * a + bulk_bytes * b for k, (a, b) in vals.items()}
 
@@ -318,17 +356,18 @@ def terrain_arm(args, C, Dycore, stream, n_err=100):
 
 
 def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
-    """Time the FP64 CPU oracle on a bounded sample of the workload."""
+    """Time the FP64 CPU oracle on a bounded sample of the workload; returns
+    cell-steps/s, seconds, cores and the seconds of each pass."""
     import oracle
     case = case_fn(nx=nx, ny=ny, nz=nz)
     base = oracle.make_base_state(case.cfg, case)
     cons, u, v, w = case.build_state(base[0])
     oracle.advance(case.cfg, base, cons, u, v, w, 1)  # warm the library / page in
     t0 = time.perf_counter()
-    oracle.advance(case.cfg, base, cons, u, v, w, nsteps)
+    _, passes = oracle.advance_timed(case.cfg, base, cons, u, v, w, nsteps)
     dt = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return nx * ny * nz * nsteps / dt, dt, cores
+    return nx * ny * nz * nsteps / dt, dt, cores, passes
 
 
 def run_reference(args, rank, world):
@@ -338,29 +377,46 @@ def run_reference(args, rank, world):
         return 0
     case_fn = cases.CASES[args.case]
     full = case_fn()
-    # each step is a bounded sample: a 64 x 64 column block of the same case
-    nx, ny, nz = min(64, full.cfg.nx), min(64, full.cfg.ny), full.cfg.nz
     import oracle
-    case = case_fn(nx=nx, ny=ny, nz=nz)
+    # the whole grid of the workload when its steps fit in about three
+    # minutes of host time, else a 64 x 64 column block of the same case
+    # (timed from one untimed warm-up step of the whole grid)
+    case = full
     base = oracle.make_base_state(case.cfg, case)
-    cons, u, v, w = case.build_state(base[0])
-    st = (cons, u, v, w)
-    for _ in range(args.warmup):
+    st = case.build_state(base[0])
+    t0 = time.perf_counter()
+    st = oracle.advance(case.cfg, base, *st, 1)
+    per_step = time.perf_counter() - t0
+    if per_step * (args.steps + max(args.warmup - 1, 0)) > 180.0:
+        case = case_fn(nx=min(64, full.cfg.nx), ny=min(64, full.cfg.ny), nz=full.cfg.nz)
+        base = oracle.make_base_state(case.cfg, case)
+        st = case.build_state(base[0])
         st = oracle.advance(case.cfg, base, *st, 1)
+    nx, ny, nz = case.cfg.nx, case.cfg.ny, case.cfg.nz
+    for _ in range(args.warmup - 1):
+        st = oracle.advance(case.cfg, base, *st, 1)
+    passes = {}
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        st = oracle.advance(case.cfg, base, *st, 1)
+        st, p = oracle.advance_timed(case.cfg, base, *st, 1)
+        for kq, vq in p.items():
+            passes[kq] = passes.get(kq, 0.0) + vq
     dt = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     value = nx * ny * nz * args.steps / dt
-    sample = f"{args.steps} steps of a {nx}x{ny}x{nz} block of the {args.case} case per run, FP64, OpenMP"
+    whole = (nx, ny, nz) == (full.cfg.nx, full.cfg.ny, full.cfg.nz)
+    sample = (f"{args.steps} steps of the whole {nx}x{ny}x{nz} grid" if whole else
+              f"{args.steps} steps of a {nx}x{ny}x{nz} block") + f" of the {args.case} case, FP64, OpenMP"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.case} {full.cfg.nx}x{full.cfg.ny}x{full.cfg.nz} (sampled {nx}x{ny}x{nz})",
+        "config": {"workload": f"{args.case} {full.cfg.nx}x{full.cfg.ny}x{full.cfg.nz}" +
+                               ("" if whole else f" (sampled {nx}x{ny}x{nz})"),
                    "parallelism": "cpu-openmp"},
-        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": sample,
+                         "cpu_model": cpu_model(), "build": "g++ -O3 -fopenmp -ffp-contract=off",
+                         "seconds_per_pass": passes},
         "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -508,11 +564,15 @@ def main():
                     "algo_bytes_per_launch": dk["algo_bytes"], "ms_per_launch": dk["ms_per_launch"]}
         step_bytes = sum(bpc[k] * n_cells * (kern[k]["launches"] / args.steps) for k in kern)
         roof_cells = hbm * 1e9 / (step_bytes / n_cells)
+        sb = survey_bytes_per_cell_step(cfg, substeps_per_step(cfg))
+        survey_roof = {"bytes_per_cell_step": sb, "hbm_roof_cell_steps_per_s": hbm * 1e9 / sb,
+                       "frac": value / world / (hbm * 1e9 / sb), "peak_gbs": hbm, "peak_kind": peak_kind}
         out = {"value": value, "ms_per_step": ms / args.steps, "status": st, "autotuned_ms": tuned_ms,
                "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                "roofline": roofline,
                "step_roofline": {"algo_bytes_per_cell_step": step_bytes / n_cells,
                                  "hbm_roof_cell_steps_per_s": roof_cells, "frac": value / world / roof_cells},
+               "survey_roofline": survey_roof,
                "kernels": kern, "launches": dy.kernels_per_step() * args.steps}
         dy.close()
         return out, base, (cons, u, v, w)
@@ -582,6 +642,16 @@ def main():
         return 0
     plain, base, init = measure(C.PREC_FP64, clock_samples)
     mixed, _, _ = measure(C.PREC_MIXED, None)
+    # the dry neutral ABL 64^3 (Smagorinsky, dt 0.5 s, 6 substeps), plain form
+    c0 = None
+    if args.case != "abl_dry":
+        c0_res, _, _ = measure(C.PREC_FP64, None, case=cases.abl_dry())
+        c0 = {"workload": "abl_dry 64x64x64, Smagorinsky, no-slip ground, Coriolis + geostrophic, dt=0.5 s, "
+                          "6 substeps/RK stage 3, FP64 plain form",
+              "value": c0_res["value"], "ms_per_step": c0_res["ms_per_step"], "e2e": c0_res["e2e"],
+              "survey_roofline": c0_res["survey_roofline"], "step_roofline": c0_res["step_roofline"],
+              "roofline": c0_res["roofline"], "status": c0_res["status"]}
+    cfg.precision = C.PREC_FP64
     mixed_err = form_error(base, init, 100) if rank == 0 else None
     cfg.precision = C.PREC_FP64
     learned = learned_arm(measure, form_error, C) if rank == 0 else None
@@ -592,10 +662,12 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         bx, by = min(64, cfg.nx), min(64, cfg.ny)
-        v_cpu, t_cpu, cores = cpu_baseline_run(cases.CASES[args.case], bx, by, cfg.nz, 2)
+        v_cpu, t_cpu, cores, passes = cpu_baseline_run(cases.CASES[args.case], bx, by, cfg.nz, 2)
         cpu = {"value": v_cpu, "unit": "cell-steps/s", "cores": cores, "kind": "port",
                "sample": f"2 steps of a {bx}x{by}x{cfg.nz} block of the {args.case} case "
-                         f"({t_cpu:.1f} s, FP64 oracle, OpenMP)"}
+                         f"({t_cpu:.1f} s, FP64 oracle, OpenMP)",
+               "cpu_model": cpu_model(), "build": "g++ -O3 -fopenmp -ffp-contract=off",
+               "seconds_per_pass": passes}
 
     if rank == 0:
         line = {
@@ -610,7 +682,9 @@ def main():
             "e2e": plain["e2e"],
             "roofline": plain["roofline"],
             "step_roofline": plain["step_roofline"],
+            "survey_roofline": plain["survey_roofline"],
             "kernels": plain["kernels"],
+            "abl_dry_64": c0,
             "mixed": {"value": mixed["value"], "ms_per_step": mixed["ms_per_step"],
                       "speedup_vs_fp64": mixed["value"] / plain["value"], "dtype": "f32 bulk / f64 state",
                       "e2e": mixed["e2e"], "roofline": mixed["roofline"], "step_roofline": mixed["step_roofline"],

@@ -82,6 +82,25 @@ def kessler(cfg, cons, dt):
     return out
 
 
+PASSES = ("closure", "slow_rhs_pre", "fast", "slow_rhs_post", "kessler", "other")
+
+
+def advance_timed(cfg, base, cons, u, v, w, nsteps):
+    """advance() plus the wall seconds spent in each pass (dict over PASSES)."""
+    L = lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.oracle_advance_timed.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_int, dp]
+    L.oracle_advance_timed.restype = ctypes.c_int
+    cons, u, v, w = (np.ascontiguousarray(a, dtype=np.float64).copy() for a in (cons, u, v, w))
+    r0, p0, pi0, th0 = (np.ascontiguousarray(a, dtype=np.float64) for a in base)
+    sec = np.zeros(6)
+    rc = L.oracle_advance_timed(ctypes.byref(cfg), _p(r0), _p(p0), _p(pi0), _p(th0),
+                                _p(cons), _p(u), _p(v), _p(w), int(nsteps), _p(sec))
+    if rc != 0:
+        raise RuntimeError("oracle_advance_timed failed: %d" % rc)
+    return (cons, u, v, w), dict(zip(PASSES, (float(x) for x in sec)))
+
+
 def interp(kind: int, s6, upw: float, frac: float = 1.0) -> float:
     s = np.ascontiguousarray(s6, dtype=np.float64)
     return lib().oracle_interp(int(kind), _p(s), float(upw), float(frac))

@@ -32,6 +32,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <chrono>
 #include <memory>
 
 #include "../include/erf_b200.h"
@@ -1335,6 +1336,17 @@ struct Oracle {
     // ------------------------------------------------------------------
     Fab cons_state;
     Vel vel_state;
+    // wall seconds per pass for the CPU baseline's split: 0 closure (strain +
+    // eddy viscosity), 1 slow_rhs_pre, 2 fast (coefficients + substeps, or the
+    // no-substep update), 3 slow_rhs_post (+ boundary fill), 4 Kessler, 5 rest
+    double pass_s[6] = {0, 0, 0, 0, 0, 0};
+    std::chrono::steady_clock::time_point tmark;
+    void tick() { tmark = std::chrono::steady_clock::now(); }
+    void tock(int slot) {
+        auto now = std::chrono::steady_clock::now();
+        pass_s[slot] += std::chrono::duration<double>(now - tmark).count();
+        tmark = now;
+    }
 
     // ==================================================================
     // Static terrain-following grid.  Metric terms of
@@ -2226,6 +2238,7 @@ struct Oracle {
     void step(double dt) {
         const double beta_s = 0.1;
         // FillPatch of the old state (ghost cells of cons and velocities)
+        tick();
         Fab& Sc = cons_state;
         physbcs_cons(Sc, 0, ncomp, ngc);
         physbcs_tangential(vel_state.u, XF, ngv);
@@ -2235,7 +2248,9 @@ struct Oracle {
         // S_old = {cons, V2M(old velocities)}
         S_old.cons.copy_from(Sc);
         // turbulent viscosity from the old velocities (strain + Smagorinsky)
+        tock(5);
         if (use_turb) turbulent_viscosity(vel_state, S_old.cons, mut);
+        tock(0);
         vel_to_mom(vel_state.u, vel_state.v, vel_state.w, S_old.cons, S_old.mx, S_old.my, S_old.mz);
         Vnew.u.copy_from(vel_state.u); Vnew.v.copy_from(vel_state.v); Vnew.w.copy_from(vel_state.w);
         apply_bcs(S_old, Vnew, ngc, ngv, false, true);
@@ -2260,7 +2275,9 @@ struct Oracle {
             }
             double slow_dt = (nrk == 0 ? dt / 3.0 : (nrk == 1 ? dt / 2.0 : dt));
             if (nrk > 0) cons_to_prim(S_new.cons, ngc, prim, pi_stage);
+            tock(5);
             slow_rhs_pre(nrk, slow_dt, F_slow, S_new, S_scr, Vnew);
+            tock(1);
             double inv_fac = 1.0 / (double)nsub;
             if (nosub) {
                 no_substep(S_sum, S_old, F_slow, nsub * dtau);
@@ -2272,13 +2289,17 @@ struct Oracle {
                 else fast_rhs_N(ks, nrk, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, dtau, beta_s, inv_fac);
                 apply_bcs(S_sum, Vnew, 1, 1, true, false);
             }
+            tock(2);
             slow_rhs_post(nrk, slow_dt, F_slow, S_old, S_new, S_sum, S_scr);
             apply_bcs(S_new, Vnew, ngc, ngv, false, false);
+            tock(3);
         }
         // new state: cons of S_new, velocities from the last post_update
         Sc.copy_from(S_new.cons);
         vel_state.u.copy_from(Vnew.u); vel_state.v.copy_from(Vnew.v); vel_state.w.copy_from(Vnew.w);
+        tock(5);
         if (use_moisture) kessler(Sc, dt);
+        tock(4);
     }
 
     // ------------------------------------------------------------------
@@ -2399,6 +2420,30 @@ int oracle_advance(const erf_b200_config* cfg, const double* rho0, const double*
     return 0;
 }
 
+// oracle_advance with the wall seconds of each pass summed into pass_s[6]
+// (closure, slow_rhs_pre, fast, slow_rhs_post, Kessler, rest).
+int oracle_advance_timed(const erf_b200_config* cfg, const double* rho0, const double* p0, const double* pi0,
+                         const double* th0, double* cons, double* u, double* v, double* w, int nsteps,
+                         double* pass_s) {
+    std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
+    for (int k = 0; k < nz + 2; ++k) { o->r0[k] = rho0[k]; o->p0[k] = p0[k]; o->pi0[k] = pi0[k]; o->th0[k] = th0[k]; }
+    o->init_storage();
+    o->alloc(o->cons_state, CC, o->ngc, o->ncomp);
+    o->alloc_vel(o->vel_state);
+    load_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    load_box(o->vel_state.u, u, nx + 1, ny, nz);
+    load_box(o->vel_state.v, v, nx, ny + 1, nz);
+    load_box(o->vel_state.w, w, nx, ny, nz + 1);
+    for (int s = 0; s < nsteps; ++s) o->step(cfg->dt);
+    store_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    store_box(o->vel_state.u, u, nx + 1, ny, nz);
+    store_box(o->vel_state.v, v, nx, ny + 1, nz);
+    store_box(o->vel_state.w, w, nx, ny, nz + 1);
+    for (int q = 0; q < 6; ++q) pass_s[q] = o->pass_s[q];
+    return 0;
+}
+
 // Base state over terrain.  z_nd: valid nodes (nz+1)(ny+1)(nx+1); th3/qv3:
 // nz*ny*nx cell values; outputs (nz+2)*ny*nx, plane k+1 for level k.
 int oracle_make_base_state_terrain(const erf_b200_config* cfg, const double* z_nd, const double* th3,
@@ -2467,6 +2512,122 @@ int oracle_kessler(const erf_b200_config* cfg, double* cons, double dt) {
     load_cc(f, cons, nx, ny, nz, o->ncomp);
     o->kessler(f, dt);
     store_cc(f, cons, nx, ny, nz, o->ncomp);
+    return 0;
+}
+
+// ----------------------------------------------------------------------------
+// Operator hooks: single operators of the restatement on caller arrays, for
+// the tests that pin them to the reference's own operator code
+// (oracle/ref).  Arrays are the valid box of their index type grown by a
+// ghost width g, i fastest, components slowest (a Fab's storage).
+// ----------------------------------------------------------------------------
+static void fab_in(Fab& f, const double* a) { std::copy(a, a + f.d.size(), f.d.begin()); }
+static void fab_out(const Fab& f, double* a) { std::copy(f.d.begin(), f.d.end(), a); }
+static void fab_sub_in(Fab& f, const double* a, const int l[3], const int h[3], int nc) {
+    // copy a smaller box [l, h] x nc (i fastest) into f
+    long sx = h[0] - l[0] + 1, sy = h[1] - l[1] + 1, sz = h[2] - l[2] + 1;
+    for (int n = 0; n < nc; ++n)
+        for (int k = l[2]; k <= h[2]; ++k)
+            for (int j = l[1]; j <= h[1]; ++j)
+                for (int i = l[0]; i <= h[0]; ++i)
+                    f(i, j, k, n) = a[(i - l[0]) + (j - l[1]) * sx + (k - l[2]) * sx * sy + n * sx * sy * sz];
+}
+static void fab_sub_out(const Fab& f, double* a, const int l[3], const int h[3], int nc) {
+    long sx = h[0] - l[0] + 1, sy = h[1] - l[1] + 1, sz = h[2] - l[2] + 1;
+    for (int n = 0; n < nc; ++n)
+        for (int k = l[2]; k <= h[2]; ++k)
+            for (int j = l[1]; j <= h[1]; ++j)
+                for (int i = l[0]; i <= h[0]; ++i)
+                    a[(i - l[0]) + (j - l[1]) * sx + (k - l[2]) * sx * sy + n * sx * sy * sz] = f(i, j, k, n);
+}
+
+// AdvectionSrcForScalars of comps icomp..icomp+ncomp-1: avg momenta on faces
+// (g = 0), primitives (nprim comps, g = 3), rhs (ncons comps, g = 0).
+int oracle_op_advect_scalars(const erf_b200_config* cfg, int icomp, int ncomp, int htype, int vtype, double hfrac,
+                             double vfrac, const double* avx, const double* avy, const double* avz,
+                             const double* prim, int nprim, double* rhs, int ncons) {
+    Oracle o(*cfg);
+    Fab ax, ay, az, pr, r;
+    o.alloc(ax, XF, 0, 1); o.alloc(ay, YF, 0, 1); o.alloc(az, ZF, 0, 1);
+    o.alloc(pr, CC, 3, nprim); o.alloc(r, CC, 0, ncons);
+    fab_in(ax, avx); fab_in(ay, avy); fab_in(az, avz); fab_in(pr, prim); fab_in(r, rhs);
+    o.advect_scalars(icomp, ncomp, ax, ay, az, pr, r, htype, vtype, hfrac, vfrac);
+    fab_out(r, rhs);
+    return 0;
+}
+
+// Strain of advance_dycore's prologue on its boxes: velocities with g = 2;
+// outputs on the cell box grown by one (s11, s22, s33) and the same extent
+// nodal in x, y and z (s12, s13, s23), i.e. (nx+2)(ny+2)(nz+2) and
+// (nx+3)(ny+3)(nz+3) values from index -1.
+int oracle_op_strain(const erf_b200_config* cfg, const double* u, const double* v, const double* w, double* s11,
+                     double* s22, double* s33, double* s12, double* s13, double* s23) {
+    Oracle o(*cfg);
+    int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    Fab U, V, W;
+    o.alloc(U, XF, 2, 1); o.alloc(V, YF, 2, 1); o.alloc(W, ZF, 2, 1);
+    fab_in(U, u); fab_in(V, v); fab_in(W, w);
+    int lc[3] = {-1, -1, -1}, hc[3] = {nx, ny, nz}, he[3] = {nx + 1, ny + 1, nz + 1};
+    Fab a11(lc, hc, 1), a22(lc, hc, 1), a33(lc, hc, 1), a12(lc, he, 1), a13(lc, he, 1), a23(lc, he, 1);
+    Bx bxcc = Oracle::grow(o.valid(CC), 1, 1, 0);
+    Bx txy = Oracle::grow(Bx{{0, 0, 0}, {nx, ny, nz - 1}}, 1, 1, 0);
+    Bx txz = Oracle::grow(Bx{{0, 0, 0}, {nx, ny - 1, nz}}, 1, 1, 0);
+    Bx tyz = Oracle::grow(Bx{{0, 0, 0}, {nx - 1, ny, nz}}, 1, 1, 0);
+    o.compute_strain(bxcc, txy, txz, tyz, U, V, W, a11, a22, a33, a12, a13, a23);
+    fab_out(a11, s11); fab_out(a22, s22); fab_out(a33, s33); fab_out(a12, s12); fab_out(a13, s13); fab_out(a23, s23);
+    return 0;
+}
+
+// The terrain strain on the same boxes (z_nd: valid nodes, the oracle adds
+// its ghost nodes); also returns the ghosted node heights (nodes -3..n+3
+// laterally, -1..nz+1 vertically) and detJ (cells -2..n+1 laterally,
+// -1..nz vertically) the oracle derived, for the reference run.
+int oracle_op_strain_T(const erf_b200_config* cfg, const double* z_valid, const double* u, const double* v,
+                       const double* w, double* z_g1, double* detJ_g1, double* s11, double* s22, double* s33,
+                       double* s12, double* s13, double* s21, double* s23, double* s31, double* s32) {
+    Oracle o(*cfg);
+    int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    o.set_terrain(z_valid);
+    Fab U, V, W;
+    o.alloc(U, XF, 2, 1); o.alloc(V, YF, 2, 1); o.alloc(W, ZF, 2, 1);
+    fab_in(U, u); fab_in(V, v); fab_in(W, w);
+    int lc[3] = {-1, -1, -1}, hc[3] = {nx, ny, nz}, he[3] = {nx + 1, ny + 1, nz + 1};
+    Fab a11(lc, hc, 1), a22(lc, hc, 1), a33(lc, hc, 1), a12(lc, he, 1), a13(lc, he, 1), a21(lc, he, 1), a23(lc, he, 1),
+        a31(lc, he, 1), a32(lc, he, 1);
+    Bx bxcc = Oracle::grow(o.valid(CC), 1, 1, 0);
+    Bx txy = Oracle::grow(Bx{{0, 0, 0}, {nx, ny, nz - 1}}, 1, 1, 0);
+    Bx txz = Oracle::grow(Bx{{0, 0, 0}, {nx, ny - 1, nz}}, 1, 1, 0);
+    Bx tyz = Oracle::grow(Bx{{0, 0, 0}, {nx - 1, ny, nz}}, 1, 1, 0);
+    o.compute_strain_T(bxcc, txy, txz, tyz, U, V, W, a11, a22, a33, a12, a13, a21, a23, a31, a32);
+    fab_out(a11, s11); fab_out(a22, s22); fab_out(a33, s33); fab_out(a12, s12); fab_out(a13, s13); fab_out(a21, s21);
+    fab_out(a23, s23); fab_out(a31, s31); fab_out(a32, s32);
+    fab_out(o.znd, z_g1);      // nodes -3..n+3 laterally, -1..nz+1 vertically
+    fab_out(o.detJ, detJ_g1);  // cells -2..n+1 laterally, -1..nz vertically
+    return 0;
+}
+
+// Eddy viscosity of the step prologue (Smagorinsky or Deardorff by
+// cfg->les_type): velocities g = 2, cons (ncomp) g = 1; outputs g = 1:
+// mu_t, the Deardorff vertical heat diffusivity and the dissipation.
+int oracle_op_eddy_viscosity(const erf_b200_config* cfg, const double* u, const double* v, const double* w,
+                             const double* cons, double* mut_out, double* kthv_out, double* diss_out) {
+    Oracle o(*cfg);
+    int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    o.init_storage();
+    Oracle::Vel V;
+    o.alloc_vel(V);
+    int lx[3] = {-2, -2, -2}, hx[3] = {nx + 2, ny + 1, nz + 1};
+    int ly[3] = {-2, -2, -2}, hy[3] = {nx + 1, ny + 2, nz + 1};
+    int lz[3] = {-2, -2, -2}, hz[3] = {nx + 1, ny + 1, nz + 2};
+    fab_sub_in(V.u, u, lx, hx, 1); fab_sub_in(V.v, v, ly, hy, 1); fab_sub_in(V.w, w, lz, hz, 1);
+    Fab C;
+    o.alloc(C, CC, o.ngc, o.ncomp);
+    int lc[3] = {-1, -1, -1}, hc[3] = {nx, ny, nz};
+    fab_sub_in(C, cons, lc, hc, o.ncomp);
+    o.turbulent_viscosity(V, C, o.mut);
+    fab_sub_out(o.mut, mut_out, lc, hc, 1);
+    fab_sub_out(o.kthv, kthv_out, lc, hc, 1);
+    fab_sub_out(o.diss, diss_out, lc, hc, 1);
     return 0;
 }
 
