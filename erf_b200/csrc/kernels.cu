@@ -1082,9 +1082,33 @@ __device__ __forceinline__ R plane_flux_y(const Plane<R>& p, int r0, int tx, R a
     return a * interp_of<T, R>(type, s, a, frac);
 }
 
-// Fluxes of one scalar for cell (i,j,k): x/y into the tile from the staged
-// plane, z through zl/zh (zl is computed only on the block's first level;
-// otherwise it is the carried top flux of the level below).
+// The tile's high-side halo faces: the x-face after the last valid column
+// of each valid row (nvy of them) and the y-face above the last valid row
+// of each valid column (nvx).  Warp 0 evaluates the y-faces (lane = column)
+// and warp 1 the x-faces (lane = row), so the other warps run no extra
+// interpolant pass; with the faces assigned to the cells' own threads
+// instead, every warp would repeat the whole interpolant for its last lane.
+struct TileEdge {
+    int nvx, nvy;   // valid columns / rows of the tile
+    int col;        // >= 0: this thread evaluates the high y-face of column col
+    int row;        // >= 0: this thread evaluates the high x-face of row row
+    int i0, j0;
+};
+__device__ __forceinline__ TileEdge tile_edge(const Geo& g) {
+    TileEdge e;
+    e.i0 = blockIdx.x * TTX;
+    e.j0 = blockIdx.y * TTY;
+    e.nvx = min(TTX, g.nx - e.i0);
+    e.nvy = min(TTY, g.ny - e.j0);
+    const int t = threadIdx.y * TTX + threadIdx.x;
+    e.col = t < e.nvx ? t : -1;
+    e.row = (t >= TTX && t < TTX + e.nvy) ? t - TTX : -1;
+    return e;
+}
+
+// Fluxes of one scalar for cell (i,j,k): the low x / y faces into the tile
+// from the staged plane, z through zl/zh (zl is computed only on the block's
+// first level; otherwise it is the carried top flux of the level below).
 template <int TH, int TV, class R, class M>
 __device__ __forceinline__ void tile_put(const Geo& g, FluxTile<R>& t, const Plane<R>& pl, const R* __restrict__ phi,
                                          const M* __restrict__ ax, const M* __restrict__ ay,
@@ -1093,13 +1117,23 @@ __device__ __forceinline__ void tile_put(const Geo& g, FluxTile<R>& t, const Pla
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int64_t c = cidx(g, i, j, k);
     t.fx[ty][tx] = plane_flux_x<TH>(pl, ty, tx, R(__ldg(ax + c)), th, fh);
-    if (tx == TTX - 1 || i == g.nx - 1)
-        t.fx[ty][tx + 1] = plane_flux_x<TH>(pl, ty, tx + 1, R(__ldg(ax + cidx(g, wrap(i + 1, g.nx), j, k))), th, fh);
     t.fy[ty][tx] = plane_flux_y<TH>(pl, ty, tx, R(__ldg(ay + c)), th, fh);
-    if (ty == TTY - 1 || j == g.ny - 1)
-        t.fy[ty + 1][tx] = plane_flux_y<TH>(pl, ty + 1, tx, R(__ldg(ay + cidx(g, i, wrap(j + 1, g.ny), k))), th, fh);
     if (first) zl = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k);
     zh = adv_flux_z<TV>(g, phi, az, tv, fv, i, j, k + 1);
+}
+// The tile's high-side halo faces of one scalar at level k (see TileEdge).
+template <int TH, class R, class M>
+__device__ __forceinline__ void tile_put_edge(const Geo& g, const TileEdge& e, FluxTile<R>& t, const Plane<R>& pl,
+                                              const M* __restrict__ ax, const M* __restrict__ ay, int th, R fh,
+                                              int k) {
+    if (e.row >= 0) {
+        const int ih = wrap(e.i0 + e.nvx, g.nx);
+        t.fx[e.row][e.nvx] = plane_flux_x<TH>(pl, e.row, e.nvx, R(__ldg(ax + cidx(g, ih, e.j0 + e.row, k))), th, fh);
+    }
+    if (e.col >= 0) {
+        const int jh = wrap(e.j0 + e.nvy, g.ny);
+        t.fy[e.nvy][e.col] = plane_flux_y<TH>(pl, e.nvy, e.col, R(__ldg(ay + cidx(g, e.i0 + e.col, jh, k))), th, fh);
+    }
 }
 template <class R>
 __device__ __forceinline__ R tile_div(const Geo& g, const FluxTile<R>& t, R zl, R zh) {
@@ -1131,6 +1165,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
     const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
     R zl = R(0), zh = R(0);
+    const TileEdge edge = tile_edge(g);
     load_plane(g, pl, A.prim, k0);
     for (int k = k0; k < k1; ++k) {
         plane_wait();
@@ -1138,6 +1173,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_CELL) k_slow_cell(Params 
         if (ok)
             tile_put<TH, TV>(g, sh, pl, A.prim, S.mx, S.my, S.mz, P.dyc_h, P.dyc_v, R(P.f_dyc_h), R(P.f_dyc_v), i, j,
                              k, k == k0, zl, zh);
+        tile_put_edge<TH>(g, edge, sh, pl, S.mx, S.my, P.dyc_h, R(P.f_dyc_h), k);
         __syncthreads();
         if (k + 1 < k1) load_plane(g, pl, A.prim, k + 1);   // overlaps the update below
         if (ok) {
@@ -1210,6 +1246,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
     R zl[NS], zh[NS];
 #pragma unroll
     for (int q = 0; q < NS; ++q) zl[q] = zh[q] = R(0);
+    const TileEdge edge = tile_edge(g);
     auto comp_of = [&](int q) {
         return q == 0 ? ERF_RHOSCALAR_COMP : (q < nscal ? ERF_RHOQ1_COMP + q - 1 : ERF_RHOKE_COMP);
     };
@@ -1231,6 +1268,14 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_POST) k_post(Params P, in
                     tile_put<MH, MV>(g, sh[q], pl[q], slow_phi(q), avx, avy, avz, P.moi_h, P.moi_v, R(P.f_moi_h),
                                      R(P.f_moi_v), i, j, k, k == k0, zl[q], zh[q]);
             }
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            if (q >= nslow) break;
+            if (q == 0 || q >= nscal)
+                tile_put_edge<DH>(g, edge, sh[q], pl[q], avx, avy, P.dry_h, R(P.f_dry_h), k);
+            else
+                tile_put_edge<MH>(g, edge, sh[q], pl[q], avx, avy, P.moi_h, R(P.f_moi_h), k);
         }
         __syncthreads();
         if (k + 1 < k1) {   // next level's planes arrive during the update below
@@ -1451,8 +1496,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
     const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const int im = ok ? wrap(i - 1, g.nx) : 0, jm = ok ? wrap(j - 1, g.ny) : 0;
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
-    const bool xedge = ok && (tx == TTX - 1 || i == g.nx - 1);
-    const bool yedge = ok && (ty == TTY - 1 || j == g.ny - 1);
+    const TileEdge edge = tile_edge(g);
     const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi);
     const double* ru = S.mx;
     const double* rv = S.my;
@@ -1472,25 +1516,32 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
         __syncthreads();
         if (ok) {
             sh[0].fx[ty][tx] = xmom_flux_x<HT, R>(P, ru, pu, tx, ty, i, j, k);
-            if (xedge) sh[0].fx[ty][tx + 1] = xmom_flux_x<HT, R>(P, ru, pu, tx + 1, ty, ip, j, k);
             sh[0].fy[ty][tx] = xmom_flux_y<HT, R>(P, rv, pu, tx, ty, i, j, k);
-            if (yedge) sh[0].fy[ty + 1][tx] = xmom_flux_y<HT, R>(P, rv, pu, tx, ty + 1, i, jp, k);
             if (k == k0) zlu = xmom_flux_z<VT, R>(P, rw, u, i, j, k);
             zhu = xmom_flux_z<VT, R>(P, rw, u, i, j, k + 1);
             sh[1].fx[ty][tx] = ymom_flux_x<HT, R>(P, ru, pv, tx, ty, i, j, k);
-            if (xedge) sh[1].fx[ty][tx + 1] = ymom_flux_x<HT, R>(P, ru, pv, tx + 1, ty, ip, j, k);
             sh[1].fy[ty][tx] = ymom_flux_y<HT, R>(P, rv, pv, tx, ty, i, j, k);
-            if (yedge) sh[1].fy[ty + 1][tx] = ymom_flux_y<HT, R>(P, rv, pv, tx, ty + 1, i, jp, k);
             if (k == k0) zlv = ymom_flux_z<VT, R>(P, rw, v, i, j, k);
             zhv = ymom_flux_z<VT, R>(P, rw, v, i, j, k + 1);
         }
         if (zk) {
             sh[2].fx[ty][tx] = zmom_flux_x<HT, R>(P, ru, pw, tx, ty, i, j, k);
-            if (xedge) sh[2].fx[ty][tx + 1] = zmom_flux_x<HT, R>(P, ru, pw, tx + 1, ty, ip, j, k);
             sh[2].fy[ty][tx] = zmom_flux_y<HT, R>(P, rv, pw, tx, ty, i, j, k);
-            if (yedge) sh[2].fy[ty + 1][tx] = zmom_flux_y<HT, R>(P, rv, pw, tx, ty + 1, i, jp, k);
             if (k == k0 || k == 1) zlw = zmom_flux_z<VT, R>(P, rw, w, i, j, k);
             zhw = zmom_flux_z<VT, R>(P, rw, w, i, j, k + 1);
+        }
+        // the tile's high-side halo faces (see TileEdge)
+        if (edge.row >= 0) {
+            const int r = edge.row, ih = wrap(edge.i0 + edge.nvx, g.nx), jr = edge.j0 + r;
+            sh[0].fx[r][edge.nvx] = xmom_flux_x<HT, R>(P, ru, pu, edge.nvx, r, ih, jr, k);
+            sh[1].fx[r][edge.nvx] = ymom_flux_x<HT, R>(P, ru, pv, edge.nvx, r, ih, jr, k);
+            if (k >= 1) sh[2].fx[r][edge.nvx] = zmom_flux_x<HT, R>(P, ru, pw, edge.nvx, r, ih, jr, k);
+        }
+        if (edge.col >= 0) {
+            const int cc = edge.col, ic = edge.i0 + cc, jh = wrap(edge.j0 + edge.nvy, g.ny);
+            sh[0].fy[edge.nvy][cc] = xmom_flux_y<HT, R>(P, rv, pu, cc, edge.nvy, ic, jh, k);
+            sh[1].fy[edge.nvy][cc] = ymom_flux_y<HT, R>(P, rv, pv, cc, edge.nvy, ic, jh, k);
+            if (k >= 1) sh[2].fy[edge.nvy][cc] = zmom_flux_y<HT, R>(P, rv, pw, cc, edge.nvy, ic, jh, k);
         }
         __syncthreads();
         if (k + 1 < k1) {   // next level's planes arrive during the right-hand sides below
