@@ -858,8 +858,28 @@ struct Oracle {
             return;
         }
 
-        // AdvectionSrcForMom (Advection/ERF_AdvectionSrcForMom.cpp:41-204,
-        // ERF_AdvectionSrcForMom_N.H:17-407)
+        advect_mom_N(R, S, V);
+        Bx tbx = valid(XF), tby = valid(YF), tbz = valid(ZF);
+        tbz.lo[2] = 1; tbz.hi[2] = nz - 1;
+        if (use_diff) {
+            // DiffusionSrcForMom_N (Diffusion/ERF_DiffusionSrcForMom_N.cpp:25-67)
+            loop(tbx, [&](int i, int j, int k) {
+                R.mx(i, j, k) -= ((t11(i, j, k) - t11(i - 1, j, k)) * dxInv[0] * 1.0 + (t12(i, j + 1, k) - t12(i, j, k)) * dxInv[1] * 1.0 + (t13(i, j, k + 1) - t13(i, j, k)) * dxInv[2]);
+            });
+            loop(tby, [&](int i, int j, int k) {
+                R.my(i, j, k) -= ((t12(i + 1, j, k) - t12(i, j, k)) * dxInv[0] * 1.0 + (t22(i, j, k) - t22(i, j - 1, k)) * dxInv[1] * 1.0 + (t23(i, j, k + 1) - t23(i, j, k)) * dxInv[2]);
+            });
+            loop(tbz, [&](int i, int j, int k) {
+                R.mz(i, j, k) -= ((t13(i + 1, j, k) - t13(i, j, k)) * dxInv[0] * 1.0 + (t23(i, j + 1, k) - t23(i, j, k)) * dxInv[1] * 1.0 + (t33(i, j, k) - t33(i, j, k - 1)) * dxInv[2]);
+            });
+        }
+        pressure_and_sources(R, pp);
+    }
+
+    // AdvectionSrcForMom without terrain (Advection/ERF_AdvectionSrcForMom.cpp:
+    // 41-204, ERF_AdvectionSrcForMom_N.H:17-407): assigns R's momentum rhs on
+    // x- and y-faces and the interior z-faces.
+    void advect_mom_N(State& R, const State& S, const Vel& V) const {
         const Fab &ru = S.mx, &rv = S.my, &rw = S.mz, &u = V.u, &v = V.v, &w = V.w;
         int ht = c.dycore_horiz_adv, vt = c.dycore_vert_adv;
         double hf = c.dycore_horiz_upw_frac, vf = c.dycore_vert_upw_frac;
@@ -955,19 +975,6 @@ struct Oracle {
             }
             R.mz(i, j, k) = -src;
         });
-        if (use_diff) {
-            // DiffusionSrcForMom_N (Diffusion/ERF_DiffusionSrcForMom_N.cpp:25-67)
-            loop(tbx, [&](int i, int j, int k) {
-                R.mx(i, j, k) -= ((t11(i, j, k) - t11(i - 1, j, k)) * dxInv[0] * 1.0 + (t12(i, j + 1, k) - t12(i, j, k)) * dxInv[1] * 1.0 + (t13(i, j, k + 1) - t13(i, j, k)) * dxInv[2]);
-            });
-            loop(tby, [&](int i, int j, int k) {
-                R.my(i, j, k) -= ((t12(i + 1, j, k) - t12(i, j, k)) * dxInv[0] * 1.0 + (t22(i, j, k) - t22(i, j - 1, k)) * dxInv[1] * 1.0 + (t23(i, j, k + 1) - t23(i, j, k)) * dxInv[2]);
-            });
-            loop(tbz, [&](int i, int j, int k) {
-                R.mz(i, j, k) -= ((t13(i + 1, j, k) - t13(i, j, k)) * dxInv[0] * 1.0 + (t23(i, j + 1, k) - t23(i, j, k)) * dxInv[1] * 1.0 + (t33(i, j, k) - t33(i, j, k - 1)) * dxInv[2]);
-            });
-        }
-        pressure_and_sources(R, pp);
     }
 
     // pressure gradient (terrain-corrected with terrain) and momentum sources
@@ -2628,6 +2635,24 @@ int oracle_op_eddy_viscosity(const erf_b200_config* cfg, const double* u, const 
     fab_sub_out(o.mut, mut_out, lc, hc, 1);
     fab_sub_out(o.kthv, kthv_out, lc, hc, 1);
     fab_sub_out(o.diss, diss_out, lc, hc, 1);
+    return 0;
+}
+
+// Momentum advection without terrain (AdvectionSrcForMom): momenta and
+// velocities as faces with g = 3; rhs outputs as faces with g = 0 (z-faces
+// written for k = 1..nz-1).
+int oracle_op_advect_mom(const erf_b200_config* cfg, const double* ru, const double* rv, const double* rw,
+                         const double* u, const double* v, const double* w, double* rx, double* ry, double* rz) {
+    Oracle o(*cfg);
+    Oracle::State S, R;
+    Oracle::Vel V;
+    o.alloc(S.cons, CC, 1, o.ncomp);
+    o.alloc(S.mx, XF, 3, 1); o.alloc(S.my, YF, 3, 1); o.alloc(S.mz, ZF, 3, 1);
+    o.alloc(V.u, XF, 3, 1); o.alloc(V.v, YF, 3, 1); o.alloc(V.w, ZF, 3, 1);
+    o.alloc(R.mx, XF, 0, 1); o.alloc(R.my, YF, 0, 1); o.alloc(R.mz, ZF, 0, 1);
+    fab_in(S.mx, ru); fab_in(S.my, rv); fab_in(S.mz, rw); fab_in(V.u, u); fab_in(V.v, v); fab_in(V.w, w);
+    o.advect_mom_N(R, S, V);
+    fab_out(R.mx, rx); fab_out(R.my, ry); fab_out(R.mz, rz);
     return 0;
 }
 

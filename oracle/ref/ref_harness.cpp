@@ -137,6 +137,32 @@ int ref_advect_scalars(int nx, int ny, int nz, double dx, double dy, double dz, 
     return 0;
 }
 
+// AdvectionSrcForMom without terrain on erf_slow_rhs_pre's boxes (x/y faces;
+// interior z faces): momenta and velocities with g = 3, rhs with g = 0.
+int ref_advect_mom(int nx, int ny, int nz, double dx, double dy, double dz, int htype, int vtype, double hfrac,
+                   double vfrac, const double* ru, const double* rv, const double* rw, const double* u,
+                   const double* v, const double* w, double* rx, double* ry, double* rz) {
+    set_domain(nx, ny, nz);
+    Box bx = vbox(nx, ny, nz, 0);
+    Box bxx = vbox(nx, ny, nz, 1), bxy = vbox(nx, ny, nz, 2), bxz = vbox(nx, ny, nz, 3);
+    bxz.growLo(2, -1);
+    bxz.growHi(2, -1);
+    auto RU = cview(ru, nx, ny, nz, 1, 3, 1), RV = cview(rv, nx, ny, nz, 2, 3, 1), RW = cview(rw, nx, ny, nz, 3, 3, 1);
+    auto U = cview(u, nx, ny, nz, 1, 3, 1), V = cview(v, nx, ny, nz, 2, 3, 1), W = cview(w, nx, ny, nz, 3, 3, 1);
+    auto X = mview(rx, nx, ny, nz, 1, 0, 1), Y = mview(ry, nx, ny, nz, 2, 0, 1), Z = mview(rz, nx, ny, nz, 3, 0, 1);
+    Box big = grow(convert(vbox(nx, ny, nz, 0), IntVect(1, 1, 1)), 4);
+    std::vector<Real> ones((size_t)big.numPts(), 1.0);
+    auto one3 = view<const Real>(ones.data(), big, 1);
+    auto mf = view<const Real>(ones.data(), Box(IntVect(-4, -4, 0), IntVect(nx + 4, ny + 4, 0)), 1);
+    std::vector<Real> cons((size_t)grow(bx, 1).numPts(), 1.0);
+    auto cd = view<const Real>(cons.data(), grow(bx, 1), 1);
+    GpuArray<Real, 3> dxi{{1.0 / dx, 1.0 / dy, 1.0 / dz}};
+    auto bcs = wall_bcs(0, 0);
+    AdvectionSrcForMom(bx, bxx, bxy, bxz, X, Y, Z, cd, U, V, W, RU, RV, RW, one3, one3, one3, one3, one3, dxi, mf, mf,
+                       mf, AdvType(htype), AdvType(vtype), hfrac, vfrac, false, 0, nz, bx, bcs.data());
+    return 0;
+}
+
 // ComputeStrain_N over the boxes advance_dycore uses (cells and edges grown by
 // one laterally): velocities with g = 2, outputs on the cell box grown by one
 // in every direction (tau11/22/33 as cells, tau12/13/23 as the same box

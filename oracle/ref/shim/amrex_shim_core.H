@@ -455,7 +455,7 @@ class FArrayBox {
     std::shared_ptr<std::vector<Real>> store;   // owned or shared (aliases)
     Real* p = nullptr;
     FArrayBox() = default;
-    FArrayBox(const Box& b, int n = 1) { resize(b, n); }
+    FArrayBox(const Box& b, int n = 1, Arena* = nullptr) { resize(b, n); }
     void resize(const Box& b, int n = 1, Arena* = nullptr) {
         bx = b; nc = n;
         store = std::make_shared<std::vector<Real>>((size_t)b.numPts() * n, 0.0);

@@ -51,6 +51,8 @@ def lib():
         L.ref_qsatw.restype = d
         L.ref_advect_scalars.restype = i
         L.ref_advect_scalars.argtypes = [i, i, i, d, d, d, i, i, i, i, d, d, p, p, p, p, i, p, i]
+        L.ref_advect_mom.argtypes = [i, i, i, d, d, d, i, i, d, d] + [p] * 9
+        L.ref_advect_mom.restype = i
         L.ref_strain_N.argtypes = [i, i, i, d, d, d, i, i] + [p] * 9
         L.ref_strain_T.argtypes = [i, i, i, d, d, d, i, i] + [p] * 14
         L.ref_eddy_viscosity.argtypes = [i, i, i, d, d, d, i, i, i] + [d] * 9 + [p, p, p, p, i, p, p, p]

@@ -11,6 +11,9 @@ cells included, and compares every output value:
     (Utils/ERF_Interpolation_UPW.H, ERF_Interpolation_WENO.H);
   * AdvectionSrcForScalars with each scheme pair
     (Advection/ERF_AdvectionSrcForState.cpp:119-395);
+  * AdvectionSrcForMom with each scheme pair, the vertical w fluxes reduced
+    in order next to the walls (Advection/ERF_AdvectionSrcForMom.cpp:41-204,
+    ERF_AdvectionSrcForMom_N.H);
   * ComputeStrain_N with slip and no-slip walls, including the one-sided
     wall stencils (Diffusion/ERF_ComputeStrain_N.cpp:28-229);
   * ComputeStrain_T over a terrain-following grid
@@ -114,6 +117,35 @@ def test_advect_scalars_matches_reference(h, v):
     assert np.any(out[1][4:8])
     for n in range(4, 8):
         assert rel(out[0][n], out[1][n]) <= TOL, (n, rel(out[0][n], out[1][n]))
+
+
+@pytest.mark.parametrize("h,v", [(C.UPWIND_5TH, C.UPWIND_5TH), (C.UPWIND_3RD, C.UPWIND_3RD),
+                                 (C.CENTERED_4TH, C.CENTERED_6TH), (C.CENTERED_2ND, C.CENTERED_2ND),
+                                 (C.UPWIND_5TH, C.CENTERED_2ND)])
+def test_advect_mom_matches_reference(h, v):
+    """AdvectionSrcForMom: the three momentum flux divergences, including the
+    order reduction of the vertical w fluxes next to the walls."""
+    cfg = _cfg(nz=11)
+    cfg.dycore_horiz_adv, cfg.dycore_vert_adv = h, v
+    cfg.dycore_horiz_upw_frac, cfg.dycore_vert_upw_frac = 1.0, 0.6
+    rng = np.random.default_rng(h + 3 * v)
+    mom = [np.ascontiguousarray(rng.normal(size=refops.shape(cfg, t, 3))[0]) for t in (1, 2, 3)]
+    vel = [np.ascontiguousarray(rng.normal(size=refops.shape(cfg, t, 3))[0]) for t in (1, 2, 3)]
+    res = []
+    for side in ("oracle", "ref"):
+        outs = [np.zeros(refops.shape(cfg, t, 0)[1:]) for t in (1, 2, 3)]
+        if side == "oracle":
+            _ocall("oracle_op_advect_mom", ctypes.byref(cfg), *mom, *vel, *outs)
+        else:
+            assert refops.lib().ref_advect_mom(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz, h, v,
+                                               cfg.dycore_horiz_upw_frac, cfg.dycore_vert_upw_frac,
+                                               *[refops.ptr(a) for a in mom + vel + outs]) == 0
+        res.append(outs)
+    for q, (a, b) in enumerate(zip(*res)):
+        if q == 2:   # z-momentum on the interior faces only
+            a, b = a[1:-1], b[1:-1]
+        assert np.any(b), q
+        assert rel(a, b) <= TOL, (q, rel(a, b))
 
 
 def _vel(cfg, rng, g=2):
