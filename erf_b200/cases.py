@@ -181,6 +181,20 @@ def abl_deardorff(nx=64, ny=64, nz=64, seed=0, tke0=0.1) -> Case:
     return case
 
 
+def abl_most(nx=64, ny=64, nz=64, seed=0, les="smagorinsky", z0=0.1, zref=0.0) -> Case:
+    """abl_dry (or abl_deardorff with les="deardorff") over a MOST ground
+    (Moeng stress, adiabatic, roughness z0, reference height zref; 0 = the
+    first cell centre) with +-0.5 m/s velocity noise below 400 m, so that the
+    ground stress varies over the plane."""
+    case = abl_deardorff(nx=nx, ny=ny, nz=nz, seed=seed) if les == "deardorff" else abl_dry(nx=nx, ny=ny, nz=nz, seed=seed)
+    c = case.cfg
+    c.zlo_bc = C.BC_MOST
+    c.most_z0, c.most_zref = z0, zref
+    case.name = "abl_most_" + les
+    case.pert.update({"vel_noise_amp": 0.5, "vel_noise_zmax": 400.0})
+    return case
+
+
 def moist_bubble(nx=128, ny=128, nz=80, seed=1) -> Case:
     c = C.defaults()
     c.nx, c.ny, c.nz = nx, ny, nz

@@ -22,7 +22,7 @@ ADV_NAMES = {
 LES_NONE, LES_SMAGORINSKY, LES_DEARDORFF, LES_MLP = 0, 1, 2, 3
 MOLEC_NONE, MOLEC_CONSTANT, MOLEC_CONSTANT_ALPHA = 0, 1, 2
 MOIST_NONE, MOIST_KESSLER, MOIST_KESSLER_NORAIN = 0, 1, 2
-BC_NO_SLIP_WALL, BC_SLIP_WALL, BC_PERIODIC = 5, 6, 7
+BC_NO_SLIP_WALL, BC_SLIP_WALL, BC_PERIODIC, BC_MOST = 5, 6, 7, 8
 PREC_FP64, PREC_MIXED = 0, 1
 SUBSTEP_IMPLICIT, SUBSTEP_NONE = 0, 1
 # conserved components (Source/ERF_IndexDefines.H:36-43)
@@ -61,6 +61,7 @@ class ErfConfig(ctypes.Structure):
         ("use_terrain", ctypes.c_int),
         ("substepping_type", ctypes.c_int),
         ("reserved", ctypes.c_int * 5),
+        ("most_z0", ctypes.c_double), ("most_zref", ctypes.c_double),
     ]
 
     def copy(self) -> "ErfConfig":
@@ -120,6 +121,8 @@ def defaults() -> ErfConfig:
     c.use_coriolis = 0
     c.coriolis_factor = c.sinphi = c.cosphi = 0.0
     c.precision = PREC_FP64
+    c.most_z0 = 0.1      # ABLMost z0_const
+    c.most_zref = 0.0    # 0: half the lowest cell (MOSTAverage's default)
     return c
 
 

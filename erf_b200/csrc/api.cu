@@ -62,6 +62,8 @@ struct erf_b200_ctx {
     StateBuf S[4];            // [0],[1] alternate old/new, [2] second stage buffer, [3] fast sum
     double* vel[2][3];        // alternating old/new face velocities (FP64 prognostic)
     double* pavg;
+    double* most_avg;         // MOST plane means {u, v, |U|, u*} of the step
+    bool most_set = false;    // per-pass entries: most_avg made by erf_b200_most_update_fluxes
     Bulk<double> bd;          // bulk arrays of the plain form
     Bulk<float> bf;           // bulk arrays of the mixed form
     bool mixed = false;
@@ -118,6 +120,15 @@ bool adv_supported(int t) {
            t == ERF_ADV_UPWIND_5TH || t == ERF_ADV_CENTERED_6TH || t == ERF_ADV_WENO_3 || t == ERF_ADV_WENO_5;
 }
 
+// The MOST reference height snapped to the cell centre of its level
+// (MOSTAverage::set_z_positions, ERF_MOSTAverage.cpp:257-300, no
+// interpolation); 0 means the first cell centre.
+void most_reference_level(const erf_b200_config& c, int& k, double& zref) {
+    const double zr = c.most_zref > 0.0 ? c.most_zref : 0.5 * c.dz;
+    k = static_cast<int>(std::floor(zr / c.dz - 0.5));
+    zref = (k + 0.5) * c.dz;
+}
+
 int validate(const erf_b200_config* c) {
     if (!c) return ERF_B200_EINVAL;
     if (c->nx < 4 || c->ny < 4 || c->nz < 4) return ERF_B200_ECONFIG;
@@ -126,8 +137,20 @@ int validate(const erf_b200_config* c) {
     // the substep ratio matters with substepping only (ERF_MRI.H:202-204)
     if (c->substepping_type == ERF_SUBSTEP_IMPLICIT && (c->mri_ratio < 2 || (c->mri_ratio % 2) != 0))
         return ERF_B200_ECONFIG;
-    if (c->zlo_bc != ERF_BC_NO_SLIP_WALL && c->zlo_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
+    if (c->zlo_bc != ERF_BC_NO_SLIP_WALL && c->zlo_bc != ERF_BC_SLIP_WALL && c->zlo_bc != ERF_BC_MOST)
+        return ERF_B200_ECONFIG;
     if (c->zhi_bc != ERF_BC_NO_SLIP_WALL && c->zhi_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
+    if (c->zlo_bc == ERF_BC_MOST) {
+        // MOST ground: flat, dry, under an eddy-viscosity closure (eta of the
+        // ghost rule), z0 below the snapped reference height
+        if (c->use_terrain || c->moisture != ERF_MOIST_NONE) return ERF_B200_ECONFIG;
+        if (c->les_type != ERF_LES_SMAGORINSKY && c->les_type != ERF_LES_DEARDORFF) return ERF_B200_ECONFIG;
+        if (!(c->most_z0 > 0.0) || !(c->most_zref >= 0.0) || !(c->most_zref < c->nz * c->dz)) return ERF_B200_ECONFIG;
+        int k;
+        double zr;
+        most_reference_level(*c, k, zr);
+        if (k < 0 || k >= c->nz || !(zr > c->most_z0)) return ERF_B200_ECONFIG;
+    }
     // the vertical momentum stencils reduce order near walls only for the
     // Upwind/Centered family (ERF_AdvectionSrcForMom_N.H:225-265)
     if (!adv_supported(c->dycore_horiz_adv) || !adv_supported(c->dycore_vert_adv)) return ERF_B200_ECONFIG;
@@ -221,6 +244,13 @@ void make_params(erf_b200_ctx* c) {
     P.f_moi_h = f.moistscal_horiz_upw_frac; P.f_moi_v = f.moistscal_vert_upw_frac;
     P.r0 = c->r0; P.p0 = c->p0; P.pi0 = c->pi0;
     P.status = c->status;
+    P.most = f.zlo_bc == ERF_BC_MOST;
+    most_reference_level(f, P.most_k, P.most_zref);
+    P.most_z0 = f.most_z0;
+    P.most_dz = f.dz;
+    P.most_avg = c->most_avg;
+    P.most_mut_f32 = c->mixed ? 1 : 0;
+    P.most_mut = c->mixed ? (const void*)c->bf.mut : (const void*)c->bd.mut;
 }
 
 dim3 cell_block() { return dim3(32, 4, 1); }
@@ -358,6 +388,8 @@ void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
 
     TIMED(0, launch_step_begin<R>(P, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
                                   B.aux[0], B.mut, B.tke));
+    // the MOST plane means and u* of the step (ERF_Advance.cpp:62-86)
+    if (P.most) TIMED(0, launch_most_avg(P, st, Vold[0], Vold[1]));
     // stage outputs alternate between the two scratch states so that the last
     // one lands in slot 1-p (or in N1 when Kessler moves it to slot 1-p)
     StateBuf outs[3] = {N0, N1, N0};
@@ -532,6 +564,8 @@ int erf_b200_config_defaults(erf_b200_config* cfg) {
     cfg->dt = 1.0;
     cfg->mri_ratio = 6;
     cfg->force_stage1_single_substep = 1;
+    cfg->most_z0 = 0.1;
+    cfg->most_zref = 0.0;
     cfg->ncomp = 5;
     cfg->dycore_horiz_adv = cfg->dycore_vert_adv = ERF_ADV_UPWIND_3RD;
     cfg->dryscal_horiz_adv = cfg->dryscal_vert_adv = ERF_ADV_UPWIND_3RD;
@@ -584,6 +618,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     }
     for (int p = 0; p < 2; ++p) { A(&c->vel[p][0], N); A(&c->vel[p][1], N); A(&c->vel[p][2], NZF); }
     A(&c->pavg, plane_avg_doubles(cfg->nz));
+    A(&c->most_avg, 4);
     c->mixed = cfg->precision == ERF_PREC_MIXED;
     if (rc == ERF_B200_OK) rc = c->mixed ? alloc_bulk(c, c->bf) : alloc_bulk(c, c->bd);
     {
@@ -872,11 +907,11 @@ int erf_b200_advance_profiled(erf_b200_ctx* c, const erf_b200_fab* cons, const e
 
 int erf_b200_kernels_per_step(const erf_b200_ctx* c, int* launches) {
     if (!c || !launches) return ERF_B200_EINVAL;
-    int n = 1 + (c->P.moist ? 1 : 0);
+    int n = 1 + (c->P.moist ? 1 : 0) + (c->P.most ? 1 : 0);
     for (int nrk = 0; nrk < 3; ++nrk) {
         int nsub; double a, b;
         stage_schedule(c->cfg, nrk, nsub, a, b);
-        int stress = c->P.les == ERF_LES_MLP ? 2 : (c->P.use_diff ? 1 : 0);
+        int stress = c->P.les == ERF_LES_MLP ? 2 : (c->P.use_diff ? (c->P.most ? 2 : 1) : 0);
         // slow_cell, slow_mom, post + (fast_coeffs and 2 per substep, or the no-substep update)
         int fast = no_substepping(c->cfg) ? 1 : 1 + 2 * nsub;
         n += 3 + fast + stress + ((c->P.moist && c->P.buoy_type == 2) ? 1 : 0);
@@ -976,12 +1011,26 @@ int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, cons
     return cuda_fail(cudaGetLastError());
 }
 
+int erf_b200_most_update_fluxes(erf_b200_ctx* c, const erf_b200_fab* xvel, const erf_b200_fab* yvel) {
+    if (!c || c->mixed) return ERF_B200_EINVAL;
+    if (!c->P.most) return ERF_B200_ECONFIG;
+    const Geo& g = c->g;
+    if (!fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1)) return ERF_B200_EINVAL;
+    int rc;
+    if ((rc = pack(c, xvel, 1, 1, c->vel[0][0])) || (rc = pack(c, yvel, 2, 1, c->vel[0][1]))) return rc;
+    launch_most_avg(c->P, c->stream, c->vel[0][0], c->vel[0][1]);
+    rc = cuda_fail(cudaGetLastError());
+    if (rc == ERF_B200_OK) c->most_set = true;
+    return rc;
+}
+
 int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b200_fab* S_rhs,
                           const erf_b200_fab* S_data, const erf_b200_fab* S_scratch, const erf_b200_fab* xvel,
                           const erf_b200_fab* yvel, const erf_b200_fab* zvel) {
     (void)slow_dt;
     if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
     if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (c->P.most && !c->most_set) return ERF_B200_EBADSTATE;
     if (c->P.les == ERF_LES_MLP && !c->net) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;

@@ -31,6 +31,77 @@ __device__ __forceinline__ double tang(const double* __restrict__ f, const Geo& 
     if (k >= g.nz) return g.zhi_noslip ? 0.0 : __ldg(f + cidx(g, i, j, g.nz - 1));
     return __ldg(f + cidx(g, i, j, k));
 }
+// ---------------------------------------------------------------------------
+// MOST ground (ABLMost::compute_most_bcs with moeng_flux, implicit MOST,
+// BoundaryConditions/ERF_ABLMost.cpp:289-489, ERF_MOSTStress.H:1395-1555):
+// the tangential velocity d levels below the ground is the level-0 value plus
+// tau / eta * dz * d, with the Moeng stress from the level-0 velocities, the
+// step's plane means and u*, and eta the level-0 eddy viscosity averaged to
+// the face (floored at 1e-8).  The stage boundary fills impose it, so the
+// readers of stage velocities evaluate it where they reach below the ground.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double most_mu(const Params& P, int64_t c) {
+    return P.most_mut_f32 ? double(static_cast<const float*>(P.most_mut)[c])
+                          : static_cast<const double*>(P.most_mut)[c];
+}
+__device__ __forceinline__ double most_ghost_u(const Params& P, const double* __restrict__ u,
+                                               const double* __restrict__ v, const double* __restrict__ cons, int i,
+                                               int j, int d) {
+    const Geo& g = P.g;
+    const int im = wrap(i - 1, g.nx), jp = wrap(j + 1, g.ny);
+    const double velx = u[cidx(g, i, j, 0)];
+    const double vely = 0.25 * (v[cidx(g, i, j, 0)] + v[cidx(g, i, jp, 0)] + v[cidx(g, im, j, 0)] + v[cidx(g, im, jp, 0)]);
+    const double rho = 0.5 * (cons[cidx(g, im, j, 0)] + cons[cidx(g, i, j, 0)]);
+    const double umean = P.most_avg[0];
+    double wsp_mean = 0.5 * (P.most_avg[2] + P.most_avg[2]);
+    const double ustar = 0.5 * (P.most_avg[3] + P.most_avg[3]);
+    const double wsp = sqrt(velx * velx + vely * vely);
+    const double num1 = wsp * umean;
+    const double num2 = wsp_mean * (velx - umean);
+    const double deltaz = P.most_dz * (0 + d);
+    wsp_mean = fmax(wsp_mean, 0.1);
+    const double stressx = -rho * ustar * ustar * (num1 + num2) / (wsp_mean * wsp_mean);
+    double eta = 0.5 * (most_mu(P, cidx(g, im, j, 0)) + most_mu(P, cidx(g, i, j, 0)));
+    eta = fmax(eta, 1e-8);
+    return velx + stressx / eta * deltaz;
+}
+__device__ __forceinline__ double most_ghost_v(const Params& P, const double* __restrict__ u,
+                                               const double* __restrict__ v, const double* __restrict__ cons, int i,
+                                               int j, int d) {
+    const Geo& g = P.g;
+    const int jm = wrap(j - 1, g.ny), ip = wrap(i + 1, g.nx);
+    const double velx = 0.25 * (u[cidx(g, i, j, 0)] + u[cidx(g, ip, j, 0)] + u[cidx(g, i, jm, 0)] + u[cidx(g, ip, jm, 0)]);
+    const double vely = v[cidx(g, i, j, 0)];
+    const double rho = 0.5 * (cons[cidx(g, i, jm, 0)] + cons[cidx(g, i, j, 0)]);
+    const double vmean = P.most_avg[1];
+    double wsp_mean = 0.5 * (P.most_avg[2] + P.most_avg[2]);
+    const double ustar = 0.5 * (P.most_avg[3] + P.most_avg[3]);
+    const double wsp = sqrt(velx * velx + vely * vely);
+    const double num1 = wsp * vmean;
+    const double num2 = wsp_mean * (vely - vmean);
+    const double deltaz = P.most_dz * (0 + d);
+    wsp_mean = fmax(wsp_mean, 0.1);
+    const double stressy = -rho * ustar * ustar * (num1 + num2) / (wsp_mean * wsp_mean);
+    double eta = 0.5 * (most_mu(P, cidx(g, i, jm, 0)) + most_mu(P, cidx(g, i, j, 0)));
+    eta = fmax(eta, 1e-8);
+    return vely + stressy / eta * deltaz;
+}
+// Stage velocities with the MOST ghost rule below the ground: the fields a
+// stage reader holds (u, v, cons of the stage), none for the other grounds.
+struct MostView {
+    const double* u;
+    const double* v;
+    const double* cons;
+};
+__device__ __forceinline__ double tang_u(const Params& P, const MostView& m, int i, int j, int k) {
+    if (k < 0 && P.most) return most_ghost_u(P, m.u, m.v, m.cons, i, j, -k);
+    return tang(m.u, P.g, i, j, k);
+}
+__device__ __forceinline__ double tang_v(const Params& P, const MostView& m, int i, int j, int k) {
+    if (k < 0 && P.most) return most_ghost_v(P, m.u, m.v, m.cons, i, j, -k);
+    return tang(m.v, P.g, i, j, k);
+}
+
 // Cell-centred scalar with foextrap in z.
 template <class V>
 __device__ __forceinline__ V ccz(const V* __restrict__ f, const Geo& g, int i, int j, int k) {
@@ -47,6 +118,20 @@ __device__ __forceinline__ double strain12(const double* u, const double* v, con
     int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
     return 0.5 * ((__ldg(u + cidx(g, i, j, k)) - __ldg(u + cidx(g, i, jm, k))) * g.dyi +
                   (__ldg(v + cidx(g, i, j, k)) - __ldg(v + cidx(g, im, j, k))) * g.dxi);
+}
+// Stage strain at the ground face of a MOST ground: the centred difference
+// with the MOST ghost velocity below
+__device__ __forceinline__ double strain13_most(const Params& P, const MostView& m, const double* w, int i, int j) {
+    const Geo& g = P.g;
+    int im = wrap(i - 1, g.nx);
+    double wx = (__ldg(w + cidx(g, i, j, 0)) - __ldg(w + cidx(g, im, j, 0))) * g.dxi;
+    return 0.5 * ((tang_u(P, m, i, j, 0) - tang_u(P, m, i, j, -1)) * g.dzi + wx);
+}
+__device__ __forceinline__ double strain23_most(const Params& P, const MostView& m, const double* w, int i, int j) {
+    const Geo& g = P.g;
+    int jm = wrap(j - 1, g.ny);
+    double wy = (__ldg(w + cidx(g, i, j, 0)) - __ldg(w + cidx(g, i, jm, 0))) * g.dyi;
+    return 0.5 * ((tang_v(P, m, i, j, 0) - tang_v(P, m, i, j, -1)) * g.dzi + wy);
 }
 __device__ __forceinline__ double strain13(const double* u, const double* w, const Geo& g, int i, int j, int k) {
     int im = wrap(i - 1, g.nx);
@@ -143,10 +228,18 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
         double s33 = (wo[c + g.sk] - wo[c]) * g.dzi;
         double s12 = 0.25 * (strain12(uo, vo, g, i, j, k) + strain12(uo, vo, g, i, jp, k) +
                              strain12(uo, vo, g, ip, j, k) + strain12(uo, vo, g, ip, jp, k));
-        double s13 = 0.25 * (strain13(uo, wo, g, i, j, k) + strain13(uo, wo, g, i, j, k + 1) +
-                             strain13(uo, wo, g, ip, j, k) + strain13(uo, wo, g, ip, j, k + 1));
-        double s23 = 0.25 * (strain23(vo, wo, g, i, j, k) + strain23(vo, wo, g, i, j, k + 1) +
-                             strain23(vo, wo, g, i, jp, k) + strain23(vo, wo, g, i, jp, k + 1));
+        double s13, s23;
+        if (P.most && k == 0) {
+            // over a MOST ground the ground-face strains are left out and the
+            // faces above averaged (ComputeSmnSmn, Diffusion/ERF_EddyViscosity.H:59-77)
+            s13 = 0.5 * (strain13(uo, wo, g, i, j, k + 1) + strain13(uo, wo, g, ip, j, k + 1));
+            s23 = 0.5 * (strain23(vo, wo, g, i, j, k + 1) + strain23(vo, wo, g, i, jp, k + 1));
+        } else {
+            s13 = 0.25 * (strain13(uo, wo, g, i, j, k) + strain13(uo, wo, g, i, j, k + 1) +
+                          strain13(uo, wo, g, ip, j, k) + strain13(uo, wo, g, ip, j, k + 1));
+            s23 = 0.25 * (strain23(vo, wo, g, i, j, k) + strain23(vo, wo, g, i, j, k + 1) +
+                          strain23(vo, wo, g, i, jp, k) + strain23(vo, wo, g, i, jp, k + 1));
+        }
         double S2 = s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + 2.0 * s23 * s23;
         if (P.les != ERF_LES_DEARDORFF) {
             mut[c] = R(P.CsDeltaSqr * rho * sqrt(2.0 * S2));
@@ -159,8 +252,15 @@ __global__ void k_step_begin(Params P, const double* __restrict__ cons, const do
             tke.smn[c] = R(S2);
             const int64_t N = g.ncell;
             const int kp = min(k + 1, g.nz - 1), km = max(k - 1, 0);
-            double dtheta_dz = 0.5 * (cons[N + cidx(g, i, j, kp)] / cons[cidx(g, i, j, kp)] -
-                                      cons[N + cidx(g, i, j, km)] / cons[cidx(g, i, j, km)]) * g.dzi;
+            double dtheta_dz;
+            if (P.most && k == 0) {
+                // one-sided over a MOST ground (ERF_ComputeTurbulentViscosity.cpp:175-188)
+                const int64_t c1 = cidx(g, i, j, 1), c2 = cidx(g, i, j, 2);
+                dtheta_dz = 0.5 * (-3 * cons[N + c] / cons[c] + 4 * cons[N + c1] / cons[c1] - cons[N + c2] / cons[c2]) * g.dzi;
+            } else {
+                dtheta_dz = 0.5 * (cons[N + cidx(g, i, j, kp)] / cons[cidx(g, i, j, kp)] -
+                                   cons[N + cidx(g, i, j, km)] / cons[cidx(g, i, j, km)]) * g.dzi;
+            }
             double E = fmax(cons[2 * N + c] / rho, 0.0);
             double strat = P.g_over_theta0 * dtheta_dz;
             double length;
@@ -223,6 +323,28 @@ __global__ void k_tau(Params P, const double* __restrict__ cons, const double* _
         if (P.use_turb) m2 = m2 + R(2) * (R(0.25) * (mu(i, jm, kk) + mu(i, j, kk) + mu(i, jm, kk - 1) + mu(i, j, kk - 1)));
         t23[e] = R(strain23(v, w, g, i, j, kk)) * -m2;
     }
+}
+// tau_13 / tau_23 on the ground faces of a MOST ground, from the strain with
+// the MOST ghost velocities below (run after k_tau, over one plane)
+template <class R>
+__global__ void k_tau_most_ground(Params P, const double* __restrict__ cons, const double* __restrict__ u,
+                                  const double* __restrict__ v, const double* __restrict__ w,
+                                  const R* __restrict__ mut, R* __restrict__ t13, R* __restrict__ t23) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
+    const R mu_eff = R(P.mu_eff);
+    auto mu = [&](int ii, int jj, int kk) { return __ldg(mut + cidx(g, ii, jj, clampk(kk, g.nz))); };
+    auto rho = [&](int ii, int jj, int kk) { return R(__ldg(cons + cidx(g, ii, jj, clampk(kk, g.nz)))); };
+    const MostView mv{u, v, cons};
+    const int64_t e = cidx(g, i, j, 0);
+    R m = P.use_consA ? R(0.25) * (rho(im, j, 0) + rho(i, j, 0) + rho(im, j, -1) + rho(i, j, -1)) * mu_eff : mu_eff;
+    m = m + R(2) * (R(0.25) * (mu(im, j, 0) + mu(i, j, 0) + mu(im, j, -1) + mu(i, j, -1)));
+    t13[e] = R(strain13_most(P, mv, w, i, j)) * -m;
+    R m2 = P.use_consA ? R(0.25) * (rho(i, jm, 0) + rho(i, j, 0) + rho(i, jm, -1) + rho(i, j, -1)) * mu_eff : mu_eff;
+    m2 = m2 + R(2) * (R(0.25) * (mu(i, jm, 0) + mu(i, j, 0) + mu(i, jm, -1) + mu(i, j, -1)));
+    t23[e] = R(strain23_most(P, mv, w, i, j)) * -m2;
 }
 
 // Stage primitives, Exner function and p' of a state (cons_to_prim,
@@ -359,6 +481,19 @@ __device__ __forceinline__ R gatherz_tang(const Geo& g, const double* f, int typ
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         s[m] = (off >= -w && off <= w - 1) ? R(tang(f, g, i, j, k + off)) : R(0);
+    }
+    return interp_of<T, R>(type, s, upw, frac);
+}
+// The same for the stage's u (comp 0) or v (comp 1) over a MOST ground.
+template <int T, class R>
+__device__ __forceinline__ R gatherz_most(const Params& P, const MostView& mv, int comp, int type, R upw, R frac, int i,
+                                          int j, int k) {
+    R s[6];
+    const int w = width_of<T>(type);
+    for (int m = 0; m < 6; ++m) {
+        int off = m - 3;
+        s[m] = (off >= -w && off <= w - 1) ? R(comp == 0 ? tang_u(P, mv, i, j, k + off) : tang_v(P, mv, i, j, k + off))
+                                           : R(0);
     }
     return interp_of<T, R>(type, s, upw, frac);
 }
@@ -1385,10 +1520,11 @@ __device__ __forceinline__ R xmom_flux_y(const Params& P, const double* rv, cons
     return a * plane_interp_y<HT, R>(pu, r0, tx, P.dyc_h, a, R(P.f_dyc_h));
 }
 template <int VT, class R>
-__device__ __forceinline__ R xmom_flux_z(const Params& P, const double* rw, const double* u, int i, int j, int k) {
+__device__ __forceinline__ R xmom_flux_z(const Params& P, const double* rw, const MostView& mv, int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(rw[cidx(g, i, j, k)]) + R(rw[cidx(g, wrap(i - 1, g.nx), j, k)]));
-    return a * gatherz_tang<VT, R>(g, u, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
+    if (P.most && k < 3) return a * gatherz_most<VT, R>(P, mv, 0, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
+    return a * gatherz_tang<VT, R>(g, mv.u, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
 }
 template <int HT, class R>
 __device__ __forceinline__ R ymom_flux_x(const Params& P, const double* ru, const Plane<double>& pv, int c0, int ty,
@@ -1405,10 +1541,11 @@ __device__ __forceinline__ R ymom_flux_y(const Params& P, const double* rv, cons
     return a * plane_interp_y<HT, R>(pv, r0, tx, P.dyc_h, a, R(P.f_dyc_h));
 }
 template <int VT, class R>
-__device__ __forceinline__ R ymom_flux_z(const Params& P, const double* rw, const double* v, int i, int j, int k) {
+__device__ __forceinline__ R ymom_flux_z(const Params& P, const double* rw, const MostView& mv, int i, int j, int k) {
     const Geo& g = P.g;
     R a = R(0.5) * (R(rw[cidx(g, i, j, k)]) + R(rw[cidx(g, i, wrap(j - 1, g.ny), k)]));
-    return a * gatherz_tang<VT, R>(g, v, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
+    if (P.most && k < 3) return a * gatherz_most<VT, R>(P, mv, 1, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
+    return a * gatherz_tang<VT, R>(g, mv.v, P.dyc_v, a, R(P.f_dyc_v), i, j, k);
 }
 template <int HT, class R>
 __device__ __forceinline__ R zmom_flux_x(const Params& P, const double* ru, const Plane<double>& pw, int c0, int ty,
@@ -1498,6 +1635,7 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
     const int ip = ok ? wrap(i + 1, g.nx) : 0, jp = ok ? wrap(j + 1, g.ny) : 0;
     const TileEdge edge = tile_edge(g);
     const R dxi = R(g.dxi), dyi = R(g.dyi), dzi = R(g.dzi);
+    const MostView mv{u, v, S.cons};   // stage velocities (MOST ghosts below a MOST ground)
     const double* ru = S.mx;
     const double* rv = S.my;
     const double* rw = S.mz;
@@ -1517,12 +1655,12 @@ __global__ void __launch_bounds__(TTX * TTY, ERFB_MINB_MOM) k_slow_mom(Params P,
         if (ok) {
             sh[0].fx[ty][tx] = xmom_flux_x<HT, R>(P, ru, pu, tx, ty, i, j, k);
             sh[0].fy[ty][tx] = xmom_flux_y<HT, R>(P, rv, pu, tx, ty, i, j, k);
-            if (k == k0) zlu = xmom_flux_z<VT, R>(P, rw, u, i, j, k);
-            zhu = xmom_flux_z<VT, R>(P, rw, u, i, j, k + 1);
+            if (k == k0) zlu = xmom_flux_z<VT, R>(P, rw, mv, i, j, k);
+            zhu = xmom_flux_z<VT, R>(P, rw, mv, i, j, k + 1);
             sh[1].fx[ty][tx] = ymom_flux_x<HT, R>(P, ru, pv, tx, ty, i, j, k);
             sh[1].fy[ty][tx] = ymom_flux_y<HT, R>(P, rv, pv, tx, ty, i, j, k);
-            if (k == k0) zlv = ymom_flux_z<VT, R>(P, rw, v, i, j, k);
-            zhv = ymom_flux_z<VT, R>(P, rw, v, i, j, k + 1);
+            if (k == k0) zlv = ymom_flux_z<VT, R>(P, rw, mv, i, j, k);
+            zhv = ymom_flux_z<VT, R>(P, rw, mv, i, j, k + 1);
         }
         if (zk) {
             sh[2].fx[ty][tx] = zmom_flux_x<HT, R>(P, ru, pw, tx, ty, i, j, k);
@@ -1779,6 +1917,9 @@ template <class R>
 void launch_tau(const Params& P, cudaStream_t st, const double* cons, const double* u, const double* v,
                 const double* w, const R* mut, R* t11, R* t22, R* t33, R* t12, R* t13, R* t23) {
     k_tau<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, cons, u, v, w, mut, t11, t22, t33, t12, t13, t23);
+    if (P.most)   // the validated MOST configurations carry an eddy-viscosity closure
+        k_tau_most_ground<R><<<dim3((P.g.nx + 31) / 32, (P.g.ny + 3) / 4), dim3(32, 4), 0, st>>>(P, cons, u, v, w, mut,
+                                                                                               t13, t23);
 }
 template <class R>
 void launch_plane_avg(const Params& P, cudaStream_t st, const double* cons, const R* prim, double* avg) {
@@ -1790,6 +1931,49 @@ void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double d
                    R* avx, R* avy, double* outx, double* outy) {
     k_fast_h<R><<<cell_grid(P.g), cell_block(), 0, st>>>(P, step, nrk, dtau, facinv, Sprev, prev_rt, Sst, A, Fmx, Fmy,
                                                          lag_in, lag_out, avx, avy, outx, outy);
+}
+// ABLMost::update_fluxes (BoundaryConditions/ERF_ABLMost.cpp:11-142) on the
+// step's old velocities: plane means of u and v on their faces (the periodic
+// high face excluded) and of sqrt(uc^2 + vc^2) at the cell centres of level
+// most_k (MOSTAverage::compute_plane_averages, ERF_MOSTAverage.cpp:674-940),
+// then u* = kappa |U| / ln(z_ref / z0) of the adiabatic surface
+// (ERF_MOSTStress.H:89-124).  One block; each thread sums a fixed stride and
+// the partial sums are added in a fixed tree, so the result is reproducible.
+constexpr int MOST_THREADS = 512;
+__global__ void __launch_bounds__(MOST_THREADS) k_most_avg(Params P, const double* __restrict__ u,
+                                                           const double* __restrict__ v) {
+    __shared__ double red[3][MOST_THREADS];
+    const Geo& g = P.g;
+    const int k = P.most_k;
+    double su = 0.0, sv = 0.0, sm = 0.0;
+    for (int64_t q = threadIdx.x; q < g.sk; q += MOST_THREADS) {
+        const int i = (int)(q % g.nx), j = (int)(q / g.nx);
+        const double uf = u[cidx(g, i, j, k)], vf = v[cidx(g, i, j, k)];
+        su += uf;
+        sv += vf;
+        const double uc = 0.5 * (uf + u[cidx(g, wrap(i + 1, g.nx), j, k)]);
+        const double vc = 0.5 * (vf + v[cidx(g, i, wrap(j + 1, g.ny), k)]);
+        sm += sqrt(uc * uc + vc * vc + 0.0 * 0.0);
+    }
+    red[0][threadIdx.x] = su;
+    red[1][threadIdx.x] = sv;
+    red[2][threadIdx.x] = sm;
+    __syncthreads();
+    for (int h = MOST_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int q = 0; q < 3; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double denom = 1.0 / (double)g.sk;
+        P.most_avg[0] = red[0][0] * denom;
+        P.most_avg[1] = red[1][0] * denom;
+        P.most_avg[2] = red[2][0] * denom;
+        P.most_avg[3] = 0.41 * P.most_avg[2] / log(P.most_zref / P.most_z0);
+    }
+}
+void launch_most_avg(const Params& P, cudaStream_t st, const double* u, const double* v) {
+    k_most_avg<<<1, MOST_THREADS, 0, st>>>(P, u, v);
 }
 template <class R>
 void launch_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons, const R* Fmx,

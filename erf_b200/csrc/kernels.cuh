@@ -33,6 +33,13 @@ struct Params {
     int ter;
     const double* znd;
     const double* detJ;
+    // MOST ground (Moeng stress, adiabatic): the level of the reference
+    // height, the step's plane means {u, v, |U|, u*} (most_avg, device), the
+    // eddy viscosity (R = double or float by most_mut_f32) for eta
+    int most, most_k, most_mut_f32;
+    double most_zref, most_z0, most_dz;
+    double* most_avg;
+    const void* most_mut;
 };
 
 // One copy of the prognostic state: cons (ncomp*ncell), face momenta.
@@ -115,6 +122,8 @@ template <class R>
 void launch_fast_h(const Params& P, cudaStream_t st, int step, int nrk, double dtau, double facinv, StateBuf Sprev,
                    int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in, R* lag_out,
                    R* avx, R* avy, double* outx, double* outy);
+// MOST plane means and friction velocity of a step from its old velocities
+void launch_most_avg(const Params& P, cudaStream_t st, const double* u, const double* v);
 template <class R>
 void launch_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons, const R* Fmx,
                        const R* Fmy, const R* Fmz, StateBuf Ssum);

@@ -34,7 +34,7 @@ EXPORTS = [
     "erf_b200_ensemble_create", "erf_b200_ensemble_advance", "erf_b200_ensemble_sync", "erf_b200_ensemble_destroy",
     "erf_b200_last_cuda_error", "erf_b200_set_terrain", "erf_b200_make_base_state_terrain",
     "erf_b200_fast_rhs_T", "erf_b200_write_plotfile", "erf_b200_write_checkpoint", "erf_b200_read_checkpoint",
-    "erf_b200_selftest_bounded_wait", "erf_b200_no_substep",
+    "erf_b200_selftest_bounded_wait", "erf_b200_no_substep", "erf_b200_most_update_fluxes",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs", "no_substep"]

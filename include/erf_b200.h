@@ -85,6 +85,7 @@ extern "C" {
 #define ERF_BC_NO_SLIP_WALL  5
 #define ERF_BC_SLIP_WALL     6
 #define ERF_BC_PERIODIC      7
+#define ERF_BC_MOST          8   /* Monin-Obukhov surface layer (ground only) */
 
 /* Arithmetic of the bulk dycore */
 #define ERF_PREC_FP64        0   /* plain FP64 form                          */
@@ -125,7 +126,7 @@ typedef struct erf_b200_config {
     /* grid: one box covering the domain, periodic in x and y */
     int    nx, ny, nz;
     double dx, dy, dz;
-    int    zlo_bc, zhi_bc;            /* ERF_BC_NO_SLIP_WALL / ERF_BC_SLIP_WALL */
+    int    zlo_bc, zhi_bc;            /* ERF_BC_NO_SLIP_WALL / _SLIP_WALL (/ _MOST below) */
 
     /* time stepping: fixed_dt, fixed_mri_dt_ratio, force_stage1_single_substep */
     double dt;
@@ -169,6 +170,11 @@ typedef struct erf_b200_config {
      * TimeIntegration/ERF_MRI.H:177-180, 255-324; mri_ratio is then unused) */
     int    substepping_type;
     int    reserved[5];
+    /* MOST surface layer for zlo_bc ERF_BC_MOST (ABLMost, erf.most.*): the
+     * roughness length z0 and the reference height zref (moved to the
+     * centre of the cell level that contains it, as MOSTAverage does); Moeng
+     * stress, adiabatic surface, plane averages */
+    double most_z0, most_zref;
 } erf_b200_config;
 
 /* Opaque context: owns all integrator scratch (S_sum, S_scratch, F_slow,
@@ -294,6 +300,18 @@ int erf_b200_kernels_per_step(const erf_b200_ctx* ctx, int* launches);
 int erf_b200_turbulent_viscosity(erf_b200_ctx* ctx, const erf_b200_fab* xvel,
                                  const erf_b200_fab* yvel, const erf_b200_fab* zvel,
                                  const erf_b200_fab* cons);
+
+/* ABLMost::update_fluxes (BoundaryConditions/ERF_ABLMost.cpp:11-142) for a
+ * context with a MOST ground (zlo_bc ERF_BC_MOST; ERF_B200_ECONFIG
+ * otherwise): the plane means of u, v and the horizontal speed at the
+ * reference level and the friction velocity, from the step's old velocities
+ * (ERF_Advance.cpp:62-86 calls it once per step, before the step's boundary
+ * fills).  erf_b200_slow_rhs_pre then evaluates the MOST ghost velocities of
+ * the stage fills (ABLMost::impose_most_bcs, ERF_ABLMost.cpp:289-489) from
+ * them; it returns ERF_B200_EBADSTATE over a MOST ground until this has been
+ * called once.  erf_b200_advance makes them itself each step. */
+int erf_b200_most_update_fluxes(erf_b200_ctx* ctx, const erf_b200_fab* xvel,
+                                const erf_b200_fab* yvel);
 
 /* erf_slow_rhs_pre (TimeIntegration/ERF_slow_rhs_pre.cpp:67-774, declared in
  * ERF_TI_slow_headers.H:54-110) including make_mom_sources/make_buoyancy and

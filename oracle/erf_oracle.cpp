@@ -157,6 +157,12 @@ struct Oracle {
     bool use_moisture, kessler_rain;
     bool use_diff, use_turb, use_consA;
     bool zlo_noslip, zhi_noslip;
+    // MOST surface layer at the ground (BoundaryConditions/ERF_ABLMost.*):
+    // Moeng stress, adiabatic surface, constant roughness, plane averages at
+    // the reference height snapped to the cell centre of level most_k
+    bool most = false;
+    int most_k = 0;
+    double most_zref = 0.0, most_um = 0.0, most_vm = 0.0, most_umm = 0.0, most_ustar = 0.0;
     // base state, index k+1 for cell k
     std::vector<double> r0, p0, pi0, th0;
 
@@ -171,6 +177,14 @@ struct Oracle {
         use_consA = (c.molec_diff_type == ERF_MOLEC_CONSTANT_ALPHA);
         zlo_noslip = (c.zlo_bc == ERF_BC_NO_SLIP_WALL);
         zhi_noslip = (c.zhi_bc == ERF_BC_NO_SLIP_WALL);
+        most = (c.zlo_bc == ERF_BC_MOST);
+        if (most) {
+            // MOSTAverage::set_k_indices_N (ERF_MOSTAverage.cpp:366-388):
+            // the level of z_ref, and z_ref moved to that level's centre
+            const double zr = c.most_zref > 0.0 ? c.most_zref : 0.5 * c.dz;
+            most_k = static_cast<int>(std::floor(zr / c.dz - 0.5));
+            most_zref = (most_k + 0.5) * c.dz;
+        }
         r0.assign(nz + 2, 0.); p0.assign(nz + 2, 0.); pi0.assign(nz + 2, 0.); th0.assign(nz + 2, 0.);
     }
 
@@ -232,7 +246,9 @@ struct Oracle {
             }
     }
     // ERFPhysBCFunct_u / _v (ERF_BoundaryConditions_xvel.cpp:155-230): tangential
-    // velocity below/above the walls: ext_dir (no-slip, value 0) or foextrap.
+    // velocity below/above the walls: ext_dir (no-slip, value 0) or foextrap;
+    // below a MOST ground reflect_odd (ERF_init_bcs.cpp:404-410), which the
+    // MOST fill of the stage boundary fills then overwrites.
     void physbcs_tangential(Fab& f, int t, int ng) const {
         fill_periodic(f, t);
         Bx b = grow(valid(t), ng, ng, ng);
@@ -242,7 +258,10 @@ struct Oracle {
             bool noslip = lo ? zlo_noslip : zhi_noslip;
             int ks = lo ? 0 : nz - 1;
             for (int j = b.lo[1]; j <= b.hi[1]; ++j)
-                for (int i = b.lo[0]; i <= b.hi[0]; ++i) f(i, j, k) = noslip ? 0.0 : f(i, j, ks);
+                for (int i = b.lo[0]; i <= b.hi[0]; ++i) {
+                    if (lo && most) f(i, j, k) = -f(i, j, -1 - k);
+                    else f(i, j, k) = noslip ? 0.0 : f(i, j, ks);
+                }
         }
     }
     // ERFPhysBCFunct_w (ERF_BoundaryConditions_zvel.cpp:151-227): w = 0 on the
@@ -278,8 +297,12 @@ struct Oracle {
         d.cons.copy_from(s.cons); d.mx.copy_from(s.mx); d.my.copy_from(s.my); d.mz.copy_from(s.mz);
     }
 
-    // FillIntermediatePatch (BoundaryConditions/ERF_FillIntermediatePatch.cpp:32-261), level 0
-    void fill_intermediate(State& S, Vel& V, int ng_cons, int ng_vel, bool cons_only, int icomp, int ncmp) const {
+    // FillIntermediatePatch (BoundaryConditions/ERF_FillIntermediatePatch.cpp:32-261), level 0;
+    // the MOST ghost velocities are imposed after the physical boundary
+    // conditions when allowed (:222-237; apply_bcs allows them outside the
+    // acoustic substeps)
+    void fill_intermediate(State& S, Vel& V, int ng_cons, int ng_vel, bool cons_only, int icomp, int ncmp,
+                           bool allow_most = false) const {
         if (!cons_only) mom_to_vel(V.u, V.v, V.w, S.cons, S.mx, S.my, S.mz);
         physbcs_cons(S.cons, icomp, ncmp, ng_cons);
         if (!cons_only) {
@@ -287,9 +310,103 @@ struct Oracle {
             physbcs_tangential(V.v, YF, ng_vel);
             if (terrain) physbcs_w_T(V.w, V.u, V.v, ng_vel);
             else physbcs_w(V.w, ng_vel);
+            if (most && allow_most) impose_most(S.cons, V.u, V.v);
             vel_to_mom(V.u, V.v, V.w, S.cons, S.mx, S.my, S.mz);
         }
         fill_periodic(S.cons, CC); fill_periodic(S.mx, XF); fill_periodic(S.my, YF); fill_periodic(S.mz, ZF);
+    }
+
+    // ABLMost::update_fluxes (BoundaryConditions/ERF_ABLMost.cpp:11-142) on
+    // the step's old velocities: MOSTAverage::compute_plane_averages
+    // (ERF_MOSTAverage.cpp:674-940; policy 0, no interpolation, no time
+    // filter) of u and v on their faces (the periodic high face excluded) and
+    // of the horizontal speed sqrt(uc^2 + vc^2) at the cell centres of level
+    // most_k, then the adiabatic friction velocity of ERF_MOSTStress.H:89-124,
+    // u* = kappa umm / ln(z_ref / z0).
+    void most_update_fluxes(const Vel& V) {
+        const int k = most_k;
+        double su = 0.0, sv = 0.0, sm = 0.0;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                su += V.u(i, j, k);
+                sv += V.v(i, j, k);
+                double uc = 0.5 * (V.u(i, j, k) + V.u(i + 1, j, k));
+                double vc = 0.5 * (V.v(i, j, k) + V.v(i, j + 1, k));
+                sm += std::sqrt(uc * uc + vc * vc + 0.0 * 0.0);
+            }
+        const double denom = 1.0 / (double)(nx * ny);
+        most_um = su * denom;
+        most_vm = sv * denom;
+        most_umm = sm * denom;
+        most_ustar = 0.41 * most_umm / std::log(most_zref / c.most_z0);
+    }
+
+    // moeng_flux::compute_u_flux / compute_v_flux (ERF_MOSTStress.H:1395-1555)
+    // of ABLMost::compute_most_bcs (ERF_ABLMost.cpp:289-489), implicit
+    // (not explicit) MOST: every ghost level below the ground gets
+    // u(k) = u(0) + tau/eta * dz * (0 - k), with the Moeng stress from the
+    // level-0 velocity, the plane means and u*, and eta the eddy viscosity at
+    // level 0 averaged to the face (floored at 1e-8).  Index clamps follow
+    // the reference's array bounds (velocities 3 ghosts, cons 4, eddy
+    // viscosity 2).  The adiabatic surface leaves rho*theta's foextrap ghosts.
+    void impose_most(const Fab& cons, Fab& u, Fab& v) const {
+        const double WSMIN = 0.1, eta_eps = 1e-8, dz = c.dz;
+        const int klo = 0;
+        auto clampi = [](int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); };
+        // eddy viscosity bounds of a 2-ghost cell array
+        const int elx = -2, ehx = nx + 1, ely = -2, ehy = ny + 1;
+        auto eta_at = [&](int ie, int je) { return mut(ie, je, klo); };
+        for (int k = u.lo[2]; k <= -1; ++k)
+            for (int j = u.lo[1]; j <= u.hi[1]; ++j)
+                for (int i = u.lo[0]; i <= u.hi[0]; ++i) {
+                    int iylo = i <= v.lo[0] ? v.lo[0] : i - 1;
+                    int iyhi = i > v.hi[0] ? v.hi[0] : i;
+                    int jy = clampi(j, v.lo[1], v.hi[1] - 1);
+                    int ic = clampi(i, cons.lo[0] + 1, cons.hi[0]);
+                    int jc = clampi(j, cons.lo[1], cons.hi[1]);
+                    double velx = u(i, j, klo);
+                    double vely = 0.25 * (v(iyhi, jy, klo) + v(iyhi, jy + 1, klo) + v(iylo, jy, klo) + v(iylo, jy + 1, klo));
+                    double rho = 0.5 * (cons(ic - 1, jc, klo, 0) + cons(ic, jc, klo, 0));
+                    double umean = most_um;
+                    double wsp_mean = 0.5 * (most_umm + most_umm);
+                    double ustar = 0.5 * (most_ustar + most_ustar);
+                    double wsp = std::sqrt(velx * velx + vely * vely);
+                    double num1 = wsp * umean;
+                    double num2 = wsp_mean * (velx - umean);
+                    double deltaz = dz * (klo - k);
+                    wsp_mean = std::max(wsp_mean, WSMIN);
+                    double stressx = -rho * ustar * ustar * (num1 + num2) / (wsp_mean * wsp_mean);
+                    int ie = clampi(i, elx + 1, ehx), je = clampi(j, ely, ehy);
+                    double eta = 0.5 * (eta_at(ie - 1, je) + eta_at(ie, je));
+                    eta = std::max(eta, eta_eps);
+                    u(i, j, k) = u(i, j, klo) + stressx / eta * deltaz;
+                }
+        for (int k = v.lo[2]; k <= -1; ++k)
+            for (int j = v.lo[1]; j <= v.hi[1]; ++j)
+                for (int i = v.lo[0]; i <= v.hi[0]; ++i) {
+                    int ix = clampi(i, u.lo[0], u.hi[0]);
+                    ix = ix > u.hi[0] - 1 ? u.hi[0] - 1 : ix;
+                    int jxlo = j <= u.lo[1] ? u.lo[1] : j - 1;
+                    int jxhi = j > u.hi[1] ? u.hi[1] : j;
+                    int ic = clampi(i, cons.lo[0], cons.hi[0]);
+                    int jc = clampi(j, cons.lo[1] + 1, cons.hi[1]);
+                    double velx = 0.25 * (u(ix, jxhi, klo) + u(ix + 1, jxhi, klo) + u(ix, jxlo, klo) + u(ix + 1, jxlo, klo));
+                    double vely = v(i, j, klo);
+                    double rho = 0.5 * (cons(ic, jc - 1, klo, 0) + cons(ic, jc, klo, 0));
+                    double vmean = most_vm;
+                    double wsp_mean = 0.5 * (most_umm + most_umm);
+                    double ustar = 0.5 * (most_ustar + most_ustar);
+                    double wsp = std::sqrt(velx * velx + vely * vely);
+                    double num1 = wsp * vmean;
+                    double num2 = wsp_mean * (vely - vmean);
+                    double deltaz = dz * (klo - k);
+                    wsp_mean = std::max(wsp_mean, WSMIN);
+                    double stressy = -rho * ustar * ustar * (num1 + num2) / (wsp_mean * wsp_mean);
+                    int ie = clampi(i, elx, ehx), je = clampi(j, ely + 1, ehy);
+                    double eta = 0.5 * (eta_at(ie, je - 1) + eta_at(ie, je));
+                    eta = std::max(eta, eta_eps);
+                    v(i, j, k) = v(i, j, klo) + stressy / eta * deltaz;
+                }
     }
 
     // apply_bcs (TimeIntegration/ERF_TI_utils.H:53-150)
@@ -306,7 +423,7 @@ struct Oracle {
             scomp = 1; ncmp = fast_only ? 1 : ncomp - 1;
             ngu = ng_cons;
         }
-        fill_intermediate(S, V, ngu, ng_vel, false, scomp, ncmp);
+        fill_intermediate(S, V, ngu, ng_vel, false, scomp, ncmp, !fast_only);
     }
 
     // cons_to_prim (TimeIntegration/ERF_TI_utils.H:4-45)
@@ -472,12 +589,17 @@ struct Oracle {
         f.define(l, h, n);
     }
 
-    // ComputeSmnSmn (Diffusion/ERF_EddyViscosity.H:31-83), no MOST
-    static double smnsmn(int i, int j, int k, const Fab& t11, const Fab& t22, const Fab& t33, const Fab& t12, const Fab& t13, const Fab& t23) {
+    // ComputeSmnSmn (Diffusion/ERF_EddyViscosity.H:31-83); over a MOST ground
+    // (implicit) the level-0 cells leave out the strains on the ground faces
+    // and take the one-sided average of the faces above (:59-77)
+    static double smnsmn(int i, int j, int k, const Fab& t11, const Fab& t22, const Fab& t33, const Fab& t12, const Fab& t13, const Fab& t23,
+                         bool most_k0 = false) {
         double s11 = t11(i, j, k), s22 = t22(i, j, k), s33 = t33(i, j, k);
         double s12 = 0.25 * (t12(i, j, k) + t12(i, j + 1, k) + t12(i + 1, j, k) + t12(i + 1, j + 1, k));
-        double s13 = 0.25 * (t13(i, j, k) + t13(i, j, k + 1) + t13(i + 1, j, k) + t13(i + 1, j, k + 1));
-        double s23 = 0.25 * (t23(i, j, k) + t23(i, j, k + 1) + t23(i, j + 1, k) + t23(i, j + 1, k + 1));
+        double s13 = most_k0 ? 0.5 * (t13(i, j, k + 1) + t13(i + 1, j, k + 1))
+                             : 0.25 * (t13(i, j, k) + t13(i, j, k + 1) + t13(i + 1, j, k) + t13(i + 1, j, k + 1));
+        double s23 = most_k0 ? 0.5 * (t23(i, j, k + 1) + t23(i, j + 1, k + 1))
+                             : 0.25 * (t23(i, j, k) + t23(i, j, k + 1) + t23(i, j + 1, k) + t23(i, j + 1, k + 1));
         return s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + 2.0 * s23 * s23;
     }
 
@@ -503,8 +625,15 @@ struct Oracle {
                 double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dzInv);
                 double DeltaMsf = std::pow(cellVolMsf, 1.0 / 3.0);
                 double eps = std::numeric_limits<double>::epsilon();
-                double dtheta_dz = 0.5 * (cons(i, j, k + 1, 1) / cons(i, j, k + 1, 0) -
-                                          cons(i, j, k - 1, 1) / cons(i, j, k - 1, 0)) * dzInv;
+                double dtheta_dz;
+                if (most && k == 0) {
+                    // one-sided over a MOST ground (ERF_ComputeTurbulentViscosity.cpp:175-188)
+                    dtheta_dz = 0.5 * (-3 * cons(i, j, k, 1) / cons(i, j, k, 0) + 4 * cons(i, j, k + 1, 1) / cons(i, j, k + 1, 0) -
+                                       cons(i, j, k + 2, 1) / cons(i, j, k + 2, 0)) * dzInv;
+                } else {
+                    dtheta_dz = 0.5 * (cons(i, j, k + 1, 1) / cons(i, j, k + 1, 0) -
+                                       cons(i, j, k - 1, 1) / cons(i, j, k - 1, 0)) * dzInv;
+                }
                 double E = std::max(cons(i, j, k, ERF_RHOKE_COMP) / cons(i, j, k, 0), 0.0);
                 double stratification = l_abs_g * dtheta_dz * l_inv_theta0;
                 double length;
@@ -533,7 +662,7 @@ struct Oracle {
             }
             double Cs = c.Cs;
             loop(valid(CC), [&](int i, int j, int k) {
-                double S = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23);
+                double S = smnsmn(i, j, k, t11, t22, t33, t12, t13, t23, most && k == 0);
                 double dzInv = dxInv[2];
                 if (terrain) dzInv /= hzeta_cc(i, j, k);
                 double cellVolMsf = 1.0 / (dxInv[0] * 1.0 * dxInv[1] * 1.0 * dzInv);
@@ -765,7 +894,7 @@ struct Oracle {
         if (c.les_type == ERF_LES_DEARDORFF && tau_nrk == 0) {
             // SmnSmn for the TKE shear production (ERF_make_tau_terms.cpp:233-240)
             Fab& sm = smn;
-            loop(valid(CC), [&](int i, int j, int k) { sm(i, j, k) = smnsmn(i, j, k, s11, s22, s33, s12, s13, s23); });
+            loop(valid(CC), [&](int i, int j, int k) { sm(i, j, k) = smnsmn(i, j, k, s11, s22, s33, s12, s13, s23, most && k == 0); });
         }
         double mu_eff = use_consA ? 2.0 * c.dynamic_viscosity / c.rho0_trans : 2.0 * c.dynamic_viscosity;
         const double OneThird = 1. / 3.;
@@ -2260,9 +2389,11 @@ struct Oracle {
         tock(0);
         vel_to_mom(vel_state.u, vel_state.v, vel_state.w, S_old.cons, S_old.mx, S_old.my, S_old.mz);
         Vnew.u.copy_from(vel_state.u); Vnew.v.copy_from(vel_state.v); Vnew.w.copy_from(vel_state.w);
+        // the MOST fluxes of the step from its old velocities, taken before the
+        // prologue fill imposes them (ERF_Advance.cpp:62-86)
+        if (most) most_update_fluxes(vel_state);
         apply_bcs(S_old, Vnew, ngc, ngv, false, true);
         cons_to_prim(S_old.cons, ngc, prim, pi_stage);
-
         // MRISplitIntegrator::advance (ERF_MRI.H:187-324)
         copy_state(S_new, S_old);
         const bool nosub = c.substepping_type == ERF_SUBSTEP_NONE;

@@ -13,9 +13,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
-from plotfile import read_plotfile  # noqa: E402
+from plotfile import read_plotfile, read_plotfile_minmax  # noqa: E402
 
 TESTS = ["TaylorGreenAdvecting", "TaylorGreenAdvectingDiffusing", "EkmanSpiral", "IsentropicVortexAdvecting"]
+# gold plotfiles stored without their FAB data: only the per-variable
+# min / max of the MultiFab header travel
+MINMAX_TESTS = ["ABL_MOST"]
 
 if __name__ == "__main__":
     ref = sys.argv[1]
@@ -25,3 +28,8 @@ if __name__ == "__main__":
         np.savez_compressed(out, data=pf["data"], names=np.array(pf["names"]), time=pf["time"],
                             header=np.array(pf["header"]))
         print(out, pf["data"].shape, pf["names"], pf["time"])
+    for name in MINMAX_TESTS:
+        pf = read_plotfile_minmax(os.path.join(ref, "Tests", "ERFGoldFiles", name))
+        out = os.path.join(HERE, f"{name}_minmax.npz")
+        np.savez_compressed(out, names=np.array(pf["names"]), time=pf["time"], vmin=pf["min"], vmax=pf["max"])
+        print(out, pf["names"], pf["time"], pf["min"], pf["max"])

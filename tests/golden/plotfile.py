@@ -57,3 +57,21 @@ def read_plotfile(path):
         out["nodal_names"] = lines[q + 3:q + 3 + nn]
         out["nodal"] = _read_multifab(os.path.join(path, lines[q + 3 + nn]), 1)
     return out
+
+
+def read_plotfile_minmax(path):
+    """Names, time and the per-component min / max of a single-box plotfile
+    whose FAB data is not stored: the two value lines that follow the FAB
+    list in Level_0/Cell_H (the MultiFab header's per-FAB minima, then
+    maxima)."""
+    with open(os.path.join(path, "Header")) as fh:
+        lines = [ln.rstrip("\n") for ln in fh]
+    nvar = int(lines[1])
+    names = lines[2:2 + nvar]
+    time = float(lines[2 + nvar + 1])
+    with open(os.path.join(path, "Level_0", "Cell_H")) as fh:
+        ch = [ln.strip() for ln in fh]
+    rows = [ln for ln in ch if ln.count(",") >= nvar and not ln.startswith("FabOnDisk")]
+    vals = [np.array([float(x) for x in r.split(",") if x], dtype=np.float64) for r in rows]
+    assert len(vals) == 2 and all(v.size == nvar for v in vals), rows
+    return {"names": names, "time": time, "min": vals[0], "max": vals[1]}

@@ -205,3 +205,36 @@ def gold_errors(gold, state, rtol=2.0e-10, atol=2.0e-10):
         ab = float(np.max(np.abs(a - b)))
         out[nm] = (float(rel), ab, bool(rel <= rtol or ab <= atol))
     return out
+
+
+def abl_most():
+    """Tests/test_files/ABL_MOST/ABL_MOST.i with Exec/ABL/ERF_prob.cpp:
+    64^3 cells over a 1024 m cube, periodic x/y, a MOST ground (z0 = 0.1 m,
+    z_ref = 8 m, Moeng stress, adiabatic) under a slip lid, no gravity,
+    Deardorff (Ck = 0.1, Ce = 0.1, sigma_k = 1), uniform rho = 1,
+    rho*theta = 300, u = 10 m/s, rho*KE = 0.1, fixed dt 0.1 s.  The substep
+    ratio is ERF's acoustic CFL estimate for this state (estTimeStep,
+    TimeIntegration/ERF_ComputeTimestep.cpp:55-225): ceil(0.1 / (0.8 /
+    ((10 + c) / 16))) = 3, made even: 4."""
+    n = 64
+    c = C.defaults()
+    c.nx = c.ny = c.nz = n
+    c.dx = c.dy = c.dz = 1024.0 / n
+    c.zlo_bc, c.zhi_bc = C.BC_MOST, C.BC_SLIP_WALL
+    c.most_z0, c.most_zref = 0.1, 8.0
+    c.dt, c.mri_ratio = 0.1, 4
+    c.ncomp = 5
+    c.molec_diff_type = C.MOLEC_NONE
+    c.alpha_T, c.alpha_C = 0.0, 1.0
+    c.les_type = C.LES_DEARDORFF
+    c.Ck, c.Ce, c.sigma_k, c.Ce_wall, c.theta_ref = 0.1, 0.1, 1.0, 0.0, 300.0
+    c.gravity = 0.0
+    cons = np.zeros((5, n, n, n))
+    cons[0] = 1.0
+    cons[1] = 300.0
+    cons[2] = 0.1
+    cons[3] = 0.2
+    u = np.full((n, n, n + 1), 10.0)
+    v = np.zeros((n, n + 1, n))
+    w = np.zeros((n + 1, n, n))
+    return "ABL_MOST", c, _uniform_base(n, 1.0), (cons, u, v, w), 10

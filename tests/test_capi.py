@@ -49,9 +49,10 @@ def test_struct_layouts_match_c():
 #include <stddef.h>
 #include "erf_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu\n", sizeof(erf_b200_config), sizeof(erf_b200_fab),
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(erf_b200_config), sizeof(erf_b200_fab),
          offsetof(erf_b200_config, abl_geo_forcing), offsetof(erf_b200_config, precision),
-         offsetof(erf_b200_fab, nstride));
+         offsetof(erf_b200_fab, nstride), offsetof(erf_b200_config, substepping_type),
+         offsetof(erf_b200_config, most_zref));
   return 0;
 }
 '''
@@ -61,12 +62,14 @@ int main(void) {
         open(cpath, "w").write(src)
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), cpath, "-o", exe], check=True)
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
-    sc, sf, og, op, on = map(int, out)
+    sc, sf, og, op, on, osub, ozref = map(int, out)
     assert sc == ctypes.sizeof(C.ErfConfig)
     assert sf == ctypes.sizeof(dycore.ErfFab)
     assert og == C.ErfConfig.abl_geo_forcing.offset
     assert op == C.ErfConfig.precision.offset
     assert on == dycore.ErfFab.nstride.offset
+    assert osub == C.ErfConfig.substepping_type.offset
+    assert ozref == C.ErfConfig.most_zref.offset
 
 
 def test_config_defaults_match_c(lib):
@@ -87,3 +90,50 @@ def test_create_rejects_bad_config_without_gpu(lib):
     ctx = ctypes.c_void_p()
     lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
     assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
+
+
+@pytest.mark.parametrize("change", ["terrain", "no_closure", "mlp", "moist", "z0_above_zref", "zref_outside",
+                                    "most_lid"])
+def test_create_rejects_unsupported_most_config(lib, change):
+    """A MOST ground is accepted flat, dry and under Smagorinsky or
+    Deardorff, with z0 below the snapped reference height, and only as the
+    lower boundary; the rest is refused before any CUDA call."""
+    c = C.defaults()
+    c.zlo_bc = C.BC_MOST
+    c.les_type = C.LES_SMAGORINSKY
+    c.most_z0, c.most_zref = 0.1, 8.0
+    if change == "terrain":
+        c.use_terrain = 1
+    elif change == "no_closure":
+        c.les_type = C.LES_NONE
+    elif change == "mlp":
+        c.les_type = C.LES_MLP
+        c.molec_diff_type = C.MOLEC_NONE
+    elif change == "moist":
+        c.moisture, c.ncomp = C.MOIST_KESSLER, 8
+    elif change == "z0_above_zref":
+        c.most_z0 = 0.5 * c.dz + 1.0   # above the first cell centre
+        c.most_zref = 0.0
+    elif change == "zref_outside":
+        c.most_zref = c.nz * c.dz + 1.0
+    elif change == "most_lid":
+        c.zhi_bc = C.BC_MOST
+    ctx = ctypes.c_void_p()
+    lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
+    assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
+
+
+def test_create_accepts_most_config(lib):
+    """The supported MOST ground passes validation (without a GPU the create
+    call then fails at its first CUDA call, ERF_B200_ECUDA)."""
+    c = C.defaults()
+    c.zlo_bc = C.BC_MOST
+    c.les_type = C.LES_DEARDORFF
+    c.most_z0, c.most_zref = 0.1, 8.0
+    ctx = ctypes.c_void_p()
+    lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
+    lib.erf_b200_destroy.argtypes = [ctypes.c_void_p]
+    rc = lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None)
+    assert rc in (0, 2)
+    if rc == 0:
+        lib.erf_b200_destroy(ctx)

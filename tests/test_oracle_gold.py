@@ -50,3 +50,32 @@ def test_oracle_reproduces_no_substep_gold(case):
     assert not bad, errs
     # tighter than fcompare: every non-trivial field to 1e-14
     assert all(v[0] <= 1e-14 or v[1] <= 1e-14 for v in errs.values()), errs
+
+
+def abl_most_minmax(state):
+    """Min / max of the ABL_MOST plot variables (ERF_Plotfile.cpp's
+    density, rhoadv_0, velocities, temp, theta, pressure) of a dense state."""
+    from golden.reference_cases import plot_fields
+    f = plot_fields(state)
+    f["rhoadv_0"] = state[0][4]
+    return f
+
+
+def test_oracle_reproduces_abl_most_gold():
+    """Tests/ERFGoldFiles/ABL_MOST (a MOST ground with Moeng stress under
+    Deardorff, 10 steps of 0.1 s on 64^3): the reference keeps only the
+    header of this plotfile, so the per-variable min / max are compared.  The
+    ground stress slows the lowest level from 10 m/s to 9.9456 m/s; the
+    oracle reproduces every min / max to the last digit printed (fcompare's
+    tolerance is 2e-10)."""
+    from golden.reference_cases import abl_most
+    name, cfg, base, state, nsteps = abl_most()
+    gold = np.load(os.path.join(HERE, "golden", f"{name}_minmax.npz"))
+    assert gold["time"] == pytest.approx(nsteps * cfg.dt, rel=1e-14)
+    out = oracle.advance(cfg, base, *state, nsteps)
+    f = abl_most_minmax(out)
+    for nm, lo, hi in zip(gold["names"], gold["vmin"], gold["vmax"]):
+        a = f[str(nm)]
+        assert a.min() == pytest.approx(lo, rel=1e-15, abs=1e-300), (str(nm), a.min(), lo)
+        assert a.max() == pytest.approx(hi, rel=1e-15, abs=1e-300), (str(nm), a.max(), hi)
+    assert f["x_velocity"].min() < 9.95   # the surface stress acted

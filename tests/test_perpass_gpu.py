@@ -26,16 +26,18 @@ def schedule(cfg, nrk):
     return cfg.mri_ratio, sub, cfg.dt
 
 
-@pytest.mark.parametrize("nosub", [False, True])
-def test_per_pass_composition_matches_fused_step(nosub):
+@pytest.mark.parametrize("nosub,most", [(False, False), (True, False), (False, True)])
+def test_per_pass_composition_matches_fused_step(nosub, most):
     """With nosub the stages call the no_substep hook entry
     (erf_b200_no_substep) in place of the acoustic substeps, at a time step
-    inside the explicit acoustic limit."""
+    inside the explicit acoustic limit.  With most the ground is a MOST
+    surface and the schedule first calls erf_b200_most_update_fluxes on the
+    old velocities, as ERF_Advance.cpp:62-86 calls ABLMost::update_fluxes."""
     import ctypes
     import torch
     from erf_b200 import Dycore
     from erf_b200.dycore import dense_fab, ErfFab
-    case = cases.abl_dry(nx=32, ny=24, nz=16)
+    case = cases.abl_most(nx=32, ny=24, nz=16) if most else cases.abl_dry(nx=32, ny=24, nz=16)
     cfg = case.cfg
     if nosub:
         cfg.substepping_type = C.SUBSTEP_NONE
@@ -102,6 +104,9 @@ def test_per_pass_composition_matches_fused_step(nosub):
     fc = dense_fab(cons, 0, nx, ny, nz, nc)
     torch.cuda.synchronize()
     assert L.erf_b200_turbulent_viscosity(dy.ctx, *vf([u, v, w]), ctypes.byref(fc)) == 0
+    if most:
+        L.erf_b200_most_update_fluxes.argtypes = [ctypes.c_void_p] * 3
+        assert L.erf_b200_most_update_fluxes(dy.ctx, *vf([u, v, w])[:2]) == 0
     stage = [a.clone() for a in S_old]
     S_rhs, S_scr = state(2), state(2)
     for nrk in range(3):
