@@ -77,6 +77,7 @@ struct erf_b200_ctx {
     size_t vert_smem = 0, coef_smem = 0;
     double *r0, *p0, *pi0, *th0;   // nz+2 values, or (nz+2) planes with terrain
     double *znd = nullptr, *detJ = nullptr, *zcc = nullptr;   // static terrain
+    double* met = nullptr;                                    // its metric tables
     bool ter_set = false;
     double *h_stage;          // device staging buffers for the host-array entry point
     int* status;
@@ -214,6 +215,7 @@ void make_params(erf_b200_ctx* c) {
     P.ter = f.use_terrain;
     P.znd = c->znd;
     P.detJ = c->detJ;
+    P.met = c->met;
     // Deardorff constants (ERF_ComputeTurbulentViscosity.cpp:129-142) and the
     // buoyancy factor of the TKE source (ERF_DiffusionSrcForState_N.cpp:681-697)
     P.Delta = DeltaMsf;
@@ -628,6 +630,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     if (cfg->use_terrain) {
         const size_t sk = (size_t)cfg->nx * cfg->ny;
         A(&c->znd, (size_t)(cfg->nz + 3) * sk); A(&c->detJ, N); A(&c->zcc, (size_t)(cfg->nz + 1) * sk);
+        A(&c->met, (size_t)TER_NMET * NZF);
     }
     if (rc == ERF_B200_OK) {
         void* q = nullptr;
@@ -1411,24 +1414,138 @@ int erf_b200_autotune(erf_b200_ctx* c, int reps, double* best_ms) {
 
 }  // extern "C"
 
-// An ensemble of contexts advanced by one CUDA graph per step whose child
-// graphs are the members' step graphs (independent nodes, so members of
-// different sizes run concurrently).  Members hold resident states at the
-// same slot parity.
+// An ensemble of contexts advanced inside one graph launch: a conditional
+// WHILE node whose body runs two steps of every member (the members' step
+// graphs as child graphs, members concurrently) and then a one-thread
+// kernel that counts the steps, polls the host's abort word (mapped pinned
+// memory) and sets the loop condition.  An odd remaining step runs in a
+// second graph whose IF node is gated by the same word.  An abort is seen
+// between two steps, so every member's state is a whole number of steps old;
+// the device counts the steps that ran and the host reads the count at the
+// next sync to put the members' state slots right.
+struct EnsCtl {
+    int aborted;      // sticky: set when the abort word was seen
+    int steps_done;   // steps run since the ensemble was made
+    int pairs_left;   // pairs still to run in this launch
+    int pairs_req;    // pairs asked for by the launch (written before it)
+};
+
+__global__ void k_ens_loop_begin(const volatile int* abort_word, EnsCtl* ctl, cudaGraphConditionalHandle h) {
+    const int ab = ctl->aborted | (*abort_word != 0);
+    ctl->aborted = ab;
+    ctl->pairs_left = ctl->pairs_req;
+    cudaGraphSetConditional(h, (!ab && ctl->pairs_left > 0) ? 1u : 0u);
+}
+__global__ void k_ens_loop_end(const volatile int* abort_word, EnsCtl* ctl, cudaGraphConditionalHandle h) {
+    ctl->steps_done += 2;
+    const int left = --ctl->pairs_left;
+    const int ab = ctl->aborted | (*abort_word != 0);
+    ctl->aborted = ab;
+    cudaGraphSetConditional(h, (!ab && left > 0) ? 1u : 0u);
+}
+__global__ void k_ens_gate(const volatile int* abort_word, EnsCtl* ctl, cudaGraphConditionalHandle h) {
+    const int ab = ctl->aborted | (*abort_word != 0);
+    ctl->aborted = ab;
+    if (!ab) ctl->steps_done += 1;
+    cudaGraphSetConditional(h, ab ? 0u : 1u);
+}
+
 struct erf_b200_ensemble {
     std::vector<erf_b200_ctx*> m;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    int parity = 0;
+    cudaGraphExec_t loop[2] = {nullptr, nullptr};   // pairs of steps from slot parity p
+    cudaGraphExec_t one[2] = {nullptr, nullptr};    // one gated step from parity p
+    int* abort_word = nullptr;                      // pinned, mapped
+    EnsCtl* ctl = nullptr;                          // device
+    int parity = 0;                                 // slot parity when all launched steps have run
+    int parity_synced = 0;                          // parity at the last sync
+    int steps_synced = 0;                           // ctl->steps_done at the last sync
 };
+
+namespace {
+cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps, void* fn,
+                       void** args) {
+    cudaKernelNodeParams kp{};
+    kp.func = fn;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    return cudaGraphAddKernelNode(node, g, deps, ndeps, &kp);
+}
+cudaError_t add_conditional(cudaGraph_t g, cudaGraphNode_t* node, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                            cudaGraphConditionalNodeType type, cudaGraph_t* body) {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(node, g, &dep, 1, &cp);
+    if (e == cudaSuccess) *body = cp.conditional.phGraph_out[0];
+    return e;
+}
+// The loop graph from parity p: begin kernel, then WHILE { steps p and 1-p
+// of every member, end kernel }.
+cudaError_t build_loop_graph(erf_b200_ensemble* e, int p, cudaGraphExec_t* out) {
+    cudaGraph_t g;
+    cudaError_t err = cudaGraphCreate(&g, 0);
+    if (err != cudaSuccess) return err;
+    cudaGraphConditionalHandle h;
+    err = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+    const volatile int* aw = e->abort_word;
+    EnsCtl* ctl = e->ctl;
+    void* args[3] = {(void*)&aw, (void*)&ctl, (void*)&h};
+    cudaGraphNode_t begin, wnode, endk;
+    cudaGraph_t body = nullptr;
+    if (err == cudaSuccess) err = add_kernel(g, &begin, nullptr, 0, (void*)k_ens_loop_begin, args);
+    if (err == cudaSuccess) err = add_conditional(g, &wnode, begin, h, cudaGraphCondTypeWhile, &body);
+    std::vector<cudaGraphNode_t> second;
+    for (size_t q = 0; q < e->m.size() && err == cudaSuccess; ++q) {
+        cudaGraphNode_t a, b;
+        err = cudaGraphAddChildGraphNode(&a, body, nullptr, 0, e->m[q]->graph_raw[p]);
+        if (err == cudaSuccess) err = cudaGraphAddChildGraphNode(&b, body, &a, 1, e->m[q]->graph_raw[1 - p]);
+        if (err == cudaSuccess) second.push_back(b);
+    }
+    if (err == cudaSuccess) err = add_kernel(body, &endk, second.data(), second.size(), (void*)k_ens_loop_end, args);
+    if (err == cudaSuccess) err = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    return err;
+}
+// One gated step from parity p: gate kernel, then IF { step p of every member }.
+cudaError_t build_one_graph(erf_b200_ensemble* e, int p, cudaGraphExec_t* out) {
+    cudaGraph_t g;
+    cudaError_t err = cudaGraphCreate(&g, 0);
+    if (err != cudaSuccess) return err;
+    cudaGraphConditionalHandle h;
+    err = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+    const volatile int* aw = e->abort_word;
+    EnsCtl* ctl = e->ctl;
+    void* args[3] = {(void*)&aw, (void*)&ctl, (void*)&h};
+    cudaGraphNode_t gate, inode;
+    cudaGraph_t body = nullptr;
+    if (err == cudaSuccess) err = add_kernel(g, &gate, nullptr, 0, (void*)k_ens_gate, args);
+    if (err == cudaSuccess) err = add_conditional(g, &inode, gate, h, cudaGraphCondTypeIf, &body);
+    for (size_t q = 0; q < e->m.size() && err == cudaSuccess; ++q) {
+        cudaGraphNode_t a;
+        err = cudaGraphAddChildGraphNode(&a, body, nullptr, 0, e->m[q]->graph_raw[p]);
+    }
+    if (err == cudaSuccess) err = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    return err;
+}
+}  // namespace
 
 extern "C" {
 
 int erf_b200_ensemble_destroy(erf_b200_ensemble* e) {
     if (!e) return ERF_B200_OK;
     if (e->stream) cudaStreamSynchronize(e->stream);
-    for (int p = 0; p < 2; ++p) if (e->exec[p]) cudaGraphExecDestroy(e->exec[p]);
+    for (int p = 0; p < 2; ++p) {
+        if (e->loop[p]) cudaGraphExecDestroy(e->loop[p]);
+        if (e->one[p]) cudaGraphExecDestroy(e->one[p]);
+    }
+    if (e->ctl) cudaFree(e->ctl);
+    if (e->abort_word) cudaFreeHost(e->abort_word);
     if (e->own_stream) cudaStreamDestroy(e->stream);
     delete e;
     return ERF_B200_OK;
@@ -1446,48 +1563,85 @@ int erf_b200_ensemble_create(erf_b200_ensemble** out, erf_b200_ctx* const* membe
     erf_b200_ensemble* e = new (std::nothrow) erf_b200_ensemble();
     if (!e) return ERF_B200_ENOMEM;
     e->m.assign(members, members + n);
-    e->parity = parity;
+    e->parity = e->parity_synced = parity;
+    auto fail = [&](cudaError_t err) { erf_b200_ensemble_destroy(e); return cuda_fail(err); };
     if (stream) {
         e->stream = (cudaStream_t)stream;
     } else {
-        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) { delete e; return ERF_B200_ECUDA; }
+        cudaError_t err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+        if (err != cudaSuccess) { e->stream = nullptr; return fail(err); }
         e->own_stream = true;
     }
+    cudaError_t err = cudaHostAlloc((void**)&e->abort_word, sizeof(int), cudaHostAllocMapped);
+    if (err != cudaSuccess) { e->abort_word = nullptr; return fail(err); }
+    *(volatile int*)e->abort_word = 0;
+    err = cudaMalloc((void**)&e->ctl, sizeof(EnsCtl));
+    if (err != cudaSuccess) { e->ctl = nullptr; return fail(err); }
+    if ((err = cudaMemsetAsync(e->ctl, 0, sizeof(EnsCtl), e->stream)) != cudaSuccess) return fail(err);
     for (int p = 0; p < 2; ++p) {
-        cudaGraph_t g;
-        if (cudaGraphCreate(&g, 0) != cudaSuccess) { erf_b200_ensemble_destroy(e); return ERF_B200_ECUDA; }
-        cudaError_t err = cudaSuccess;
-        for (int q = 0; q < n && err == cudaSuccess; ++q) {
-            cudaGraphNode_t node;
-            err = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, members[q]->graph_raw[p]);
-        }
-        if (err == cudaSuccess) err = cudaGraphInstantiate(&e->exec[p], g, 0);
-        cudaGraphDestroy(g);
-        if (err != cudaSuccess) { erf_b200_ensemble_destroy(e); return cuda_fail(err); }
+        if ((err = build_loop_graph(e, p, &e->loop[p])) != cudaSuccess) return fail(err);
+        if ((err = build_one_graph(e, p, &e->one[p])) != cudaSuccess) return fail(err);
     }
+    if ((err = cudaStreamSynchronize(e->stream)) != cudaSuccess) return fail(err);
     *out = e;
     return ERF_B200_OK;
 }
 
-// nsteps steps of every member, one graph launch per step on the ensemble's
-// stream; the members' resident states advance.
+// nsteps steps of every member: the pairs in one launch of the loop graph,
+// an odd last step in one launch of the gated single-step graph.  The
+// members' resident states advance; the slot parity is settled at the next
+// erf_b200_ensemble_sync.
 int erf_b200_ensemble_advance(erf_b200_ensemble* e, int nsteps) {
     if (!e || nsteps < 0) return ERF_B200_EINVAL;
-    for (erf_b200_ctx* c : e->m)
-        if (c->cur != e->parity) return ERF_B200_EBADSTATE;
-    for (int s = 0; s < nsteps; ++s) {
-        CK(cudaGraphLaunch(e->exec[e->parity], e->stream));
+    const int pairs = nsteps / 2;
+    if (pairs > 0) {
+        CK(cudaMemcpyAsync(&e->ctl->pairs_req, &pairs, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        CK(cudaGraphLaunch(e->loop[e->parity], e->stream));
+    }
+    if (nsteps & 1) {
+        CK(cudaGraphLaunch(e->one[e->parity], e->stream));
         e->parity ^= 1;
     }
-    for (erf_b200_ctx* c : e->m) c->cur = e->parity;
+    for (erf_b200_ctx* c : e->m) c->cur = -1;   // unknown until the next sync
     return ERF_B200_OK;
 }
 
-// Wait for the ensemble's work (before store_state or status reads on the
-// members' own streams).
+// Ask the ensemble's device loop to stop (flag != 0) or clear a stop (0).
+// The loop reads the word between steps; the members then keep the state of
+// the last whole step and erf_b200_ensemble_sync returns ERF_B200_EABORTED.
+// Clearing waits for the ensemble's stream and resets the device's sticky
+// flag, so that later advances run again.
+int erf_b200_ensemble_abort(erf_b200_ensemble* e, int flag) {
+    if (!e) return ERF_B200_EINVAL;
+    *(volatile int*)e->abort_word = flag ? 1 : 0;
+    if (!flag) {
+        CK(cudaStreamSynchronize(e->stream));
+        CK(cudaMemsetAsync(&e->ctl->aborted, 0, sizeof(int), e->stream));
+        CK(cudaStreamSynchronize(e->stream));
+    }
+    return ERF_B200_OK;
+}
+
+// Wait for the ensemble's work, then settle the members' state slots from
+// the steps that ran (before store_state or status reads on the members'
+// own streams).  ERF_B200_EABORTED when an abort stopped the loop.
 int erf_b200_ensemble_sync(erf_b200_ensemble* e) {
     if (!e) return ERF_B200_EINVAL;
     CK(cudaStreamSynchronize(e->stream));
+    EnsCtl h;
+    CK(cudaMemcpy(&h, e->ctl, sizeof(EnsCtl), cudaMemcpyDeviceToHost));
+    const int ran = h.steps_done - e->steps_synced;
+    e->steps_synced = h.steps_done;
+    e->parity_synced ^= (ran & 1);
+    e->parity = e->parity_synced;
+    for (erf_b200_ctx* c : e->m) c->cur = e->parity;
+    return h.aborted ? ERF_B200_EABORTED : ERF_B200_OK;
+}
+
+// Steps every member ran since the ensemble was made (after a sync).
+int erf_b200_ensemble_steps(const erf_b200_ensemble* e, int* steps) {
+    if (!e || !steps) return ERF_B200_EINVAL;
+    *steps = e->steps_synced;
     return ERF_B200_OK;
 }
 

@@ -19,7 +19,8 @@ LIB_PATH = os.path.join(_HERE, "liberf_b200.so")
 _lib = None
 
 ERRORS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "EBADSTATE", 5: "ENAN", 6: "EPIVOT",
-          7: "ETIMEOUT", 8: "ECONFIG"}
+          7: "ETIMEOUT", 8: "ECONFIG", 9: "EABORTED"}
+EABORTED = 9
 
 EXPORTS = [
     "erf_b200_config_defaults", "erf_b200_create", "erf_b200_destroy", "erf_b200_set_stream",
@@ -35,6 +36,7 @@ EXPORTS = [
     "erf_b200_last_cuda_error", "erf_b200_set_terrain", "erf_b200_make_base_state_terrain",
     "erf_b200_fast_rhs_T", "erf_b200_write_plotfile", "erf_b200_write_checkpoint", "erf_b200_read_checkpoint",
     "erf_b200_selftest_bounded_wait", "erf_b200_no_substep", "erf_b200_most_update_fluxes",
+    "erf_b200_ensemble_abort", "erf_b200_ensemble_steps",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs", "no_substep"]
@@ -91,6 +93,8 @@ def load_library():
     L.erf_b200_ensemble_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), i, vp]
     L.erf_b200_ensemble_advance.argtypes = [vp, i]
     L.erf_b200_ensemble_sync.argtypes = [vp]
+    L.erf_b200_ensemble_abort.argtypes = [vp, i]
+    L.erf_b200_ensemble_steps.argtypes = [vp, ctypes.POINTER(i)]
     L.erf_b200_ensemble_destroy.argtypes = [vp]
     L.erf_b200_selftest_bounded_wait.argtypes = [i, ctypes.POINTER(i)]
     L.erf_b200_write_plotfile.argtypes = [vp, ctypes.c_char_p, dp, dp, dp, dp, dp, dp, dp, ctypes.c_double, i]
@@ -129,7 +133,8 @@ def dense_fab(t, kind: int, nx: int, ny: int, nz: int, ncomp: int = 1) -> ErfFab
 
 
 class Ensemble:
-    """Contexts with resident states advanced by one CUDA graph per step."""
+    """Contexts with resident states advanced together: a device-side loop
+    over steps inside one graph launch, stoppable through an abort word."""
 
     def __init__(self, members, stream=None):
         self.lib = load_library()
@@ -142,8 +147,21 @@ class Ensemble:
     def advance(self, nsteps: int):
         _check(self.lib.erf_b200_ensemble_advance(self.h, int(nsteps)), "ensemble_advance")
 
-    def sync(self):
-        _check(self.lib.erf_b200_ensemble_sync(self.h), "ensemble_sync")
+    def sync(self) -> bool:
+        """Wait for the ensemble's work; False when an abort stopped it."""
+        rc = self.lib.erf_b200_ensemble_sync(self.h)
+        if rc == EABORTED:
+            return False
+        _check(rc, "ensemble_sync")
+        return True
+
+    def abort(self, flag: bool = True):
+        _check(self.lib.erf_b200_ensemble_abort(self.h, 1 if flag else 0), "ensemble_abort")
+
+    def steps(self) -> int:
+        n = ctypes.c_int()
+        _check(self.lib.erf_b200_ensemble_steps(self.h, ctypes.byref(n)), "ensemble_steps")
+        return n.value
 
     def close(self):
         if self.h:

@@ -44,6 +44,7 @@ extern "C" {
 #define ERF_B200_EPIVOT           6   /* vertical tridiagonal pivot ~ 0         */
 #define ERF_B200_ETIMEOUT         7   /* a bounded device wait ran out          */
 #define ERF_B200_ECONFIG          8   /* configuration rejected                 */
+#define ERF_B200_EABORTED         9   /* an ensemble run was stopped by its abort word */
 
 /* ----------------------------------------------------------------------------
  * Enumerations: numeric values match the reference's enums so that a caller
@@ -495,11 +496,28 @@ int erf_b200_advance_resident(erf_b200_ctx* ctx, int nsteps);
 int erf_b200_autotune(erf_b200_ctx* ctx, int reps, double* best_ms);
 
 typedef struct erf_b200_ensemble erf_b200_ensemble;
-/* An ensemble of contexts holding resident states (any sizes); one CUDA
- * graph per step runs every member's step graph, members concurrently. */
+/* An ensemble of contexts holding resident states (any sizes, all at the
+ * same state slot).  erf_b200_ensemble_advance runs nsteps steps of every
+ * member in one graph launch: a device-side loop (a conditional WHILE graph
+ * node) whose body holds two steps of every member's step graph, members
+ * concurrently, and a one-thread kernel that counts the steps and polls the
+ * host's abort word in mapped pinned memory; an odd last step runs in a
+ * second launch behind the same check.  The members' state slots are
+ * settled by erf_b200_ensemble_sync, which must come before any other call
+ * on a member (they return ERF_B200_EBADSTATE until then). */
 int erf_b200_ensemble_create(erf_b200_ensemble** out, erf_b200_ctx* const* members, int n, void* stream);
 int erf_b200_ensemble_advance(erf_b200_ensemble* e, int nsteps);
+/* Set (flag != 0) or clear the abort word.  The loop reads it between
+ * steps: once set, no further step starts, every member keeps the state of
+ * its last whole step, and sync returns ERF_B200_EABORTED.  Clearing waits
+ * for the ensemble's stream and re-arms the loop. */
+int erf_b200_ensemble_abort(erf_b200_ensemble* e, int flag);
+/* Wait for the ensemble's work and settle the members' state slots;
+ * ERF_B200_EABORTED if an abort stopped it. */
 int erf_b200_ensemble_sync(erf_b200_ensemble* e);
+/* Steps every member has run since the ensemble was made (as of the last
+ * sync). */
+int erf_b200_ensemble_steps(const erf_b200_ensemble* e, int* steps);
 int erf_b200_ensemble_destroy(erf_b200_ensemble* e);
 
 /* Attach a trained network to a context created with les_type ERF_LES_MLP
