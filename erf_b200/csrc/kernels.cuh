@@ -33,6 +33,7 @@ struct Params {
     int ter;
     const double* znd;
     const double* detJ;
+    const double* met;          // metric tables (terrain.cu), TER_NMET planes of nzf
     // MOST ground (Moeng stress, adiabatic): the level of the reference
     // height, the step's plane means {u, v, |U|, u*} (most_avg, device), the
     // eddy viscosity (R = double or float by most_mut_f32) for eta
@@ -41,6 +42,9 @@ struct Params {
     double* most_avg;
     const void* most_mut;
 };
+
+// Number of static-terrain metric tables (planes of nzf values each).
+constexpr int TER_NMET = 11;
 
 // One copy of the prognostic state: cons (ncomp*ncell), face momenta.
 struct StateBuf {

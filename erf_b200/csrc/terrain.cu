@@ -31,6 +31,15 @@
 namespace erfb {
 namespace {
 
+// Resident blocks of 128 threads per SM asked of the compiler for the
+// heavy one-thread-per-cell passes (register caps 128 / 64): above their
+// natural register counts these kernels are latency-bound at 3-5 blocks.
+#define TER_MINB_SLOW_CELL 4
+#define TER_MINB_STRAIN 8
+#define TER_MINB_POST 8
+#define TER_MINB_SLOW_MOM 8
+#define TER_MINB_STRESS 8
+
 // ---------------------------------------------------------------------------
 // Metric terms (Utils/ERF_TerrainMetrics.H:33-395), same operand order.
 // ---------------------------------------------------------------------------
@@ -56,17 +65,17 @@ __device__ double heta_cc(const Params& P, int i, int j, int k) {
                              - ZN(i, j, k) - ZN(i + 1, j, k) - ZN(i, j, k + 1) - ZN(i + 1, j, k + 1));
 }
 // x faces (also ax) and y faces (also ay)
-__device__ double hzeta_I(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hzeta_I_fn(const Params& P, int i, int j, int k) {
     return 0.5 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i, j + 1, k + 1) - ZN(i, j, k) - ZN(i, j + 1, k));
 }
-__device__ double hxi_I(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hxi_I_fn(const Params& P, int i, int j, int k) {
     return 0.125 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k) + ZN(i + 1, j + 1, k + 1)
                               - ZN(i - 1, j, k) - ZN(i - 1, j, k + 1) - ZN(i - 1, j + 1, k) - ZN(i - 1, j + 1, k + 1));
 }
-__device__ double hzeta_J(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hzeta_J_fn(const Params& P, int i, int j, int k) {
     return 0.5 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) - ZN(i, j, k) - ZN(i + 1, j, k));
 }
-__device__ double heta_J(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double heta_J_fn(const Params& P, int i, int j, int k) {
     return 0.125 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k) + ZN(i + 1, j + 1, k + 1)
                               - ZN(i, j - 1, k) - ZN(i, j - 1, k + 1) - ZN(i + 1, j - 1, k) - ZN(i + 1, j - 1, k + 1));
 }
@@ -75,28 +84,28 @@ __device__ double hzeta_K(const Params& P, int i, int j, int k) {
     return 0.125 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k + 1)
                               - ZN(i, j, k - 1) - ZN(i + 1, j, k - 1) - ZN(i, j + 1, k - 1) - ZN(i + 1, j + 1, k - 1));
 }
-__device__ double hxi_K(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hxi_K_fn(const Params& P, int i, int j, int k) {
     return 0.5 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j + 1, k) - ZN(i, j, k) - ZN(i, j + 1, k));
 }
-__device__ double heta_K(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double heta_K_fn(const Params& P, int i, int j, int k) {
     return 0.5 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i + 1, j + 1, k) - ZN(i, j, k) - ZN(i + 1, j, k));
 }
 // xy edges (EdgeCenterK), xz edges (EdgeCenterJ), yz edges (EdgeCenterI)
-__device__ double hzeta_EK(const Params& P, int i, int j, int k) { return P.g.dzi * (ZN(i, j, k + 1) - ZN(i, j, k)); }
+__device__ __forceinline__ double hzeta_EK_fn(const Params& P, int i, int j, int k) { return P.g.dzi * (ZN(i, j, k + 1) - ZN(i, j, k)); }
 __device__ double hxi_EK(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j, k + 1) - ZN(i - 1, j, k) - ZN(i - 1, j, k + 1));
 }
 __device__ double heta_EK(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i, j + 1, k + 1) - ZN(i, j - 1, k) - ZN(i, j - 1, k + 1));
 }
-__device__ double hzeta_EJ(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hzeta_EJ_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i, j + 1, k + 1) - ZN(i, j, k - 1) - ZN(i, j + 1, k - 1));
 }
 __device__ double hxi_EJ(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dxi * (ZN(i + 1, j + 1, k) + ZN(i + 1, j, k) - ZN(i - 1, j + 1, k) - ZN(i - 1, j, k));
 }
 __device__ double heta_EJ(const Params& P, int i, int j, int k) { return P.g.dyi * (ZN(i, j + 1, k) - ZN(i, j, k)); }
-__device__ double hzeta_EI(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hzeta_EI_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) - ZN(i, j, k - 1) - ZN(i + 1, j, k - 1));
 }
 __device__ double hxi_EI(const Params& P, int i, int j, int k) { return P.g.dxi * (ZN(i + 1, j, k) - ZN(i, j, k)); }
@@ -104,13 +113,43 @@ __device__ double heta_EI(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dyi * (ZN(i + 1, j + 1, k) + ZN(i, j + 1, k) - ZN(i + 1, j - 1, k) - ZN(i, j - 1, k));
 }
 // slopes of a z-face (OmegaFromW / WFromOmega, ERF_TerrainMetrics.H:455-520)
-__device__ double zlo_xi(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double zlo_xi_fn(const Params& P, int i, int j, int k) {
     return 0.5 * P.g.dxi * (ZN(i + 1, j + 1, k) + ZN(i + 1, j, k) - ZN(i, j + 1, k) - ZN(i, j, k));
 }
-__device__ double zlo_eta(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double zlo_eta_fn(const Params& P, int i, int j, int k) {
     return 0.5 * P.g.dyi * (ZN(i + 1, j + 1, k) + ZN(i, j + 1, k) - ZN(i + 1, j, k) - ZN(i, j, k));
 }
 #undef ZN
+
+// Static-terrain metric tables: the metric terms the passes read most,
+// evaluated once per face / edge by the functions above (so bit-identical to
+// evaluating them in place) and stored as TER_NMET planes of (nz+1) x ny x
+// nx values, k in [0, nz].  A pass reads one value instead of re-deriving it
+// from four to eight nodes of z_phys_nd; outside [0, nz] the function runs.
+enum { MT_HZETA_I, MT_HXI_I, MT_HZETA_J, MT_HETA_J, MT_HXI_K, MT_HETA_K, MT_HZETA_EK, MT_HZETA_EJ, MT_HZETA_EI,
+       MT_ZLO_XI, MT_ZLO_ETA, MT_COUNT };
+static_assert(MT_COUNT == TER_NMET, "metric table count");
+__device__ __forceinline__ double mt_at(const Params& P, int q, int i, int j, int k) {
+    const Geo& g = P.g;
+    return __ldg(P.met + (int64_t)q * g.nzf + cidx(g, wrap(i, g.nx), wrap(j, g.ny), k));
+}
+#define ERFB_MT(name, q)                                                           \
+    __device__ __forceinline__ double name(const Params& P, int i, int j, int k) { \
+        if (k >= 0 && k <= P.g.nz) return mt_at(P, q, i, j, k);                   \
+        return name##_fn(P, i, j, k);                                              \
+    }
+ERFB_MT(hzeta_I, MT_HZETA_I)
+ERFB_MT(hxi_I, MT_HXI_I)
+ERFB_MT(hzeta_J, MT_HZETA_J)
+ERFB_MT(heta_J, MT_HETA_J)
+ERFB_MT(hxi_K, MT_HXI_K)
+ERFB_MT(heta_K, MT_HETA_K)
+ERFB_MT(hzeta_EK, MT_HZETA_EK)
+ERFB_MT(hzeta_EJ, MT_HZETA_EJ)
+ERFB_MT(hzeta_EI, MT_HZETA_EI)
+ERFB_MT(zlo_xi, MT_ZLO_XI)
+ERFB_MT(zlo_eta, MT_ZLO_ETA)
+#undef ERFB_MT
 
 // Face-averaged horizontal components at z-face (i,j,k) of x/y-face arrays
 // given as accessors (extrapolated to the bottom face).
@@ -201,8 +240,28 @@ __global__ void k_ter_metrics(Params P, double* __restrict__ detJ, double* __res
     zcc[cidx(g, i, j, k)] = .125 * (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k)
                                     + Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1));
 }
+// The metric tables (k in [0, nz] for every plane)
+__global__ void k_ter_met_tables(Params P, double* __restrict__ met) {
+    const Geo& g = P.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    double* m = met + cidx(g, i, j, k);
+    const int64_t s = g.nzf;
+    m[MT_HZETA_I * s] = hzeta_I_fn(P, i, j, k);
+    m[MT_HXI_I * s] = hxi_I_fn(P, i, j, k);
+    m[MT_HZETA_J * s] = hzeta_J_fn(P, i, j, k);
+    m[MT_HETA_J * s] = heta_J_fn(P, i, j, k);
+    m[MT_HXI_K * s] = hxi_K_fn(P, i, j, k);
+    m[MT_HETA_K * s] = heta_K_fn(P, i, j, k);
+    m[MT_HZETA_EK * s] = hzeta_EK_fn(P, i, j, k);
+    m[MT_HZETA_EJ * s] = hzeta_EJ_fn(P, i, j, k);
+    m[MT_HZETA_EI * s] = hzeta_EI_fn(P, i, j, k);
+    m[MT_ZLO_XI * s] = zlo_xi_fn(P, i, j, k);
+    m[MT_ZLO_ETA * s] = zlo_eta_fn(P, i, j, k);
+}
 void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* zcc) {
     k_ter_metrics<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, detJ, zcc);
+    k_ter_met_tables<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, const_cast<double*>(P.met));
 }
 
 // ---------------------------------------------------------------------------
@@ -515,7 +574,7 @@ __global__ void k_ter_step_begin(Params P, const double* __restrict__ cons, cons
 // and SmnSmn of the first stage for the Deardorff shear production.
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_ter_strain(Params P, int nrk, const double* __restrict__ u, const double* __restrict__ v,
+__global__ void __launch_bounds__(128, TER_MINB_STRAIN) k_ter_strain(Params P, int nrk, const double* __restrict__ u, const double* __restrict__ v,
                              const double* __restrict__ w, TerBuf<R> T, TkeBuf<R> tke) {
     const Geo& g = P.g;
     int i, j, k;
@@ -556,7 +615,7 @@ __global__ void k_ter_strain(Params P, int nrk, const double* __restrict__ u, co
 // (= tau21) carry h_zeta.
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_ter_stress(Params P, const double* __restrict__ cons, const R* __restrict__ mut, TerBuf<R> T,
+__global__ void __launch_bounds__(128, TER_MINB_STRESS) k_ter_stress(Params P, const double* __restrict__ cons, const R* __restrict__ mut, TerBuf<R> T,
                              R* __restrict__ t11, R* __restrict__ t22, R* __restrict__ t33, R* __restrict__ t12,
                              R* __restrict__ t13, R* __restrict__ t23) {
     const Geo& g = P.g;
@@ -804,7 +863,7 @@ __global__ void k_ter_rawflux(Params P, const double* __restrict__ rho, const R*
 // the dycore scheme, DiffusionSrcForState_T and hfx_z.
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
+__global__ void __launch_bounds__(128, TER_MINB_SLOW_CELL) k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
                                 const double* __restrict__ v, const R* __restrict__ mut, TkeBuf<R> tke, TerBuf<R> T,
                                 R* __restrict__ Fcons, R* __restrict__ avx, R* __restrict__ avy, R* __restrict__ avz) {
     const Geo& g = P.g;
@@ -859,7 +918,7 @@ __global__ void k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const doubl
 // k_ter_slow_cell.
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_ter_slow_mom(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
+__global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
                                const double* __restrict__ v, const double* __restrict__ w, const R* __restrict__ t11,
                                const R* __restrict__ t22, const R* __restrict__ t33, const R* __restrict__ t12,
                                const R* __restrict__ t13, const R* __restrict__ t23, TerBuf<R> T,
@@ -1332,7 +1391,7 @@ __global__ void k_ter_fv_update(Params P, double dtau, double facinv, double bet
 // the next stage's primitives.
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_ter_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
+__global__ void __launch_bounds__(128, TER_MINB_POST) k_ter_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
                            StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* __restrict__ mut,
                            TkeBuf<R> tke, TerBuf<R> T, const R* __restrict__ avx, const R* __restrict__ avy,
                            const R* __restrict__ avz, double* __restrict__ un, double* __restrict__ vn,
