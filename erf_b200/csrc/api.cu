@@ -78,6 +78,8 @@ struct erf_b200_ctx {
     double *r0, *p0, *pi0, *th0;   // nz+2 values, or (nz+2) planes with terrain
     double *znd = nullptr, *detJ = nullptr, *zcc = nullptr;   // static terrain
     double* met = nullptr;                                    // its metric tables
+    int ter_tx = 0;                                           // k_ter_fast_vert columns per block
+    size_t ter_smem = 0;                                      // and its shared memory
     bool ter_set = false;
     double *h_stage;          // device staging buffers for the host-array entry point
     int* status;
@@ -365,8 +367,9 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
             TIMED(5, launch_ter_fast_h<R>(P, st, ks, dtau, facinv, Sprev, prt, Sst, Acur, B.Fmx, B.Fmy, B.lag[lp],
                                           B.lag[1 - lp], B.ter, B.avx, B.avy, SUM.mx, SUM.my));
             lp ^= 1;
-            TIMED(6, launch_ter_fast_vert<R>(P, st, dtau, facinv, beta_1, beta_2, Sprev, prt, Sst, Acur, B.Fcons, B.Fmz,
-                                             B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, SUM.cons, SUM.mz));
+            TIMED(6, launch_ter_fast_vert<R>(P, st, c->ter_tx, c->ter_smem, dtau, facinv, beta_1, beta_2, Sprev, prt,
+                                             Sst, Acur, B.Fcons, B.Fmz, B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ,
+                                             B.avz, SUM.cons, SUM.mz));
         }
         TIMED(7, launch_ter_post<R>(P, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut, B.tke,
                                     B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
@@ -497,7 +500,7 @@ int alloc_bulk(erf_b200_ctx* c, Bulk<R>& B) {
         A(&B.ter.ndu, N); A(&B.ter.ndv, N); A(&B.ter.odu, N); A(&B.ter.odv, N);
         A(&B.ter.fx[0], N); A(&B.ter.fy[0], N); A(&B.ter.fx[1], N); A(&B.ter.fy[1], N);
         auto D = [&](double** q, size_t n) { if (rc == ERF_B200_OK) rc = dalloc(c, q, n); };
-        D(&B.ter.tr0, N); D(&B.ter.tr1, N); D(&B.ter.om, NZF); D(&B.ter.sol, NZF);
+        D(&B.ter.bnd, 2 * (int64_t)cfg->nx * cfg->ny);
     }
     return rc;
 }
@@ -659,6 +662,10 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         if (rc == ERF_B200_OK) {
             if ((c->mixed ? vert_setup<float>(c->vert_smem, c->coef_smem) : vert_setup<double>(c->vert_smem, c->coef_smem)) != 0)
                 rc = ERF_B200_ECUDA;
+        }
+        if (rc == ERF_B200_OK && cfg->use_terrain) {
+            ter_vert_shape(nz, &c->ter_tx, &c->ter_smem);
+            if (c->ter_tx < 1) rc = ERF_B200_ECONFIG;
         }
         if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     }
@@ -1134,8 +1141,9 @@ int fast_rhs_pass(erf_b200_ctx* c, bool terrain, int step, int nrk, const erf_b2
     if (terrain) {
         launch_ter_fast_h<double>(P, st, step, dtau, facinv, Sprev, 0, Sst, B.aux[0], B.Fmx, B.Fmy, B.lag[0],
                                   B.lag[1], B.ter, B.avx, B.avy, OUT.mx, OUT.my);
-        launch_ter_fast_vert<double>(P, st, dtau, facinv, kBeta1, kBeta2, Sprev, 0, Sst, B.aux[0], B.Fcons, B.Fmz,
-                                     B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz, OUT.cons, OUT.mz);
+        launch_ter_fast_vert<double>(P, st, c->ter_tx, c->ter_smem, dtau, facinv, kBeta1, kBeta2, Sprev, 0, Sst,
+                                     B.aux[0], B.Fcons, B.Fmz, B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ, B.avz,
+                                     OUT.cons, OUT.mz);
     } else {
         launch_fast_h<double>(P, st, step, nrk, dtau, facinv, Sprev, 0, Sst, B.aux[0], B.Fmx, B.Fmy, B.lag[0],
                               B.lag[1], B.avx, B.avy, OUT.mx, OUT.my);

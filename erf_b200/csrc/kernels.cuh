@@ -76,16 +76,15 @@ struct TkeBuf {
 // Terrain scratch (R): strain components of the stage (tau_ii with the
 // expansion-rate third removed, S12, S13, S23 on edges), the non-symmetric
 // stresses tau31 / tau32, the substep's horizontal momentum increments, and
-// the column solution of the implicit solve (FP64, per z-face).
+// the boundary-face momenta of the previous substep (FP64).
 template <class R>
 struct TerBuf {
     R *s11, *s22, *s33, *s12, *s13, *s23;
     R *t31, *t32;
     R *ndu, *ndv, *odu, *odv;
     R *fx[2], *fy[2];            // raw diffusive face fluxes (two fields)
-    double *tr0, *tr1, *om, *sol;  // substep: horizontal rho / rho theta fluxes
-                                   // (cells), Omega of the old increments and
-                                   // the implicit solve (z faces)
+    double* bnd;                 // substep: the previous momentum on the ground
+                                 // and lid faces (two planes)
 };
 
 // x-y tile of the transport kernels (slow_cell, slow_mom, post) and the
@@ -195,10 +194,11 @@ void launch_ter_fast_h(const Params& P, cudaStream_t st, int step, double dtau, 
                        int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fmx, const R* Fmy, const R* lag_in,
                        R* lag_out, TerBuf<R> T, R* avx, R* avy, double* outx, double* outy);
 template <class R>
-void launch_ter_fast_vert(const Params& P, cudaStream_t st, double dtau, double facinv, double beta_1, double beta_2,
-                          StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmz,
-                          TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz,
-                          double* out_cons, double* out_mz);
+void launch_ter_fast_vert(const Params& P, cudaStream_t st, int tx, size_t smem, double dtau, double facinv,
+                          double beta_1, double beta_2, StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A,
+                          const R* Fcons, const R* Fmz, TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB,
+                          const R* cP, const R* cQ, R* avz, double* out_cons, double* out_mz);
+void ter_vert_shape(int nz, int* tx, size_t* smem);
 template <class R>
 void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
                      StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,

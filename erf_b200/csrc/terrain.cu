@@ -21,7 +21,8 @@
 //   k_ter_slow_mom    AdvectionSrcForMom_T, DiffusionSrcForMom_T, terrain
 //                     pressure gradient, sources
 //   k_ter_fast_h,     erf_fast_rhs_T (TimeIntegration/ERF_fast_rhs_T.cpp)
-//   k_ter_fv_*
+//   k_ter_fv_bnd,
+//   k_ter_fast_vert
 //   k_ter_post        erf_slow_rhs_post with terrain and the stage's
 //                     boundary round trips
 #include <cfloat>
@@ -1205,17 +1206,12 @@ __global__ void k_ter_fast_h(Params P, int step, double dtau, double facinv, Sta
 }
 
 // ---------------------------------------------------------------------------
-// Acoustic substep with terrain, vertical part (ERF_fast_rhs_T.cpp:320-680),
-// in four passes so that only the Thomas sweep is serial in k:
-//   k_ter_fv_prep    horizontal rho / rho*theta fluxes through the sloping
-//                    faces (cells) and Omega of the previous increments
-//                    (faces; the previous top z-momentum is the one the
-//                    boundary fill leaves: w from Omega = 0 at the lid);
-//   k_ter_fv_rhs     the detJ-weighted right-hand side of the Omega'' system;
-//   k_ter_fv_solve   forward elimination / back substitution per column on
-//                    the stage's coefficients (plane-major, coalesced);
-//   k_ter_fv_update  w'' from Omega'' and the new increments, vertical fluxes,
-//                    average contravariant momentum, rho and rho*theta.
+// Acoustic substep with terrain, vertical part (ERF_fast_rhs_T.cpp:320-680):
+// horizontal rho / rho*theta fluxes through the sloping faces, Omega of the
+// previous increments, the detJ-weighted right-hand side of the Omega''
+// system, the Thomas sweep on the stage's coefficients, then w'' from
+// Omega'', the vertical fluxes, the average contravariant momentum, rho and
+// rho*theta (k_ter_fast_vert below).
 // ---------------------------------------------------------------------------
 namespace {
 template <class R>
@@ -1251,134 +1247,151 @@ __device__ double prev_mz_ter(const Params& P, StateBuf Sprev, int prev_rt, int 
 }
 }  // namespace
 
+// The same vertical part as one pass per column tile (the layout of
+// k_fast_vert: TX columns of a row j, the block's warps spread over the
+// levels, the column arrays in shared memory), so that the horizontal
+// fluxes, Omega of the old increments, the right-hand side and the solution
+// never leave the SM; one warp runs the Thomas sweep.  The momentum of the
+// previous substep on the ground and lid faces (w from Omega = 0 of its
+// round-tripped u, v) reads neighbouring columns of a state the update
+// overwrites in place, so k_ter_fv_bnd forms it first.
 template <class R>
-__global__ void k_ter_fv_prep(Params P, StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, TerBuf<R> T) {
+__global__ void k_ter_fv_bnd(Params P, StateBuf Sprev, TerBuf<R> T) {
     const Geo& g = P.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny || k > g.nz) return;
-    const int nz = g.nz;
-    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const int64_t col = (int64_t)j * g.nx + i;
+    T.bnd[col] = prev_mz_ter<R>(P, Sprev, 1, i, j, 0);
+    T.bnd[g.sk + col] = prev_mz_ter<R>(P, Sprev, 1, i, j, g.nz);
+}
+
+template <class R>
+__global__ void __launch_bounds__(1024) k_ter_fast_vert(Params P, double dtau, double facinv, double beta_1,
+                                                        double beta_2, StateBuf Sprev, int prev_rt, StateBuf Sst,
+                                                        StageAux<R> A, const R* __restrict__ Fcons,
+                                                        const R* __restrict__ Fmz, TerBuf<R> T,
+                                                        const R* __restrict__ cA, const R* __restrict__ cInvB,
+                                                        const R* __restrict__ cCB, const R* __restrict__ cP,
+                                                        const R* __restrict__ cQ, R* __restrict__ avz,
+                                                        double* out_cons, double* out_mz) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double* sm = reinterpret_cast<double*>(sm_raw);
+    const Geo& g = P.g;
+    const int nz = g.nz, TX = blockDim.x, L = threadIdx.x, w0 = threadIdx.y, nw = blockDim.y;
+    const int i = blockIdx.x * TX + L, j = blockIdx.y;
+    const bool ok = i < g.nx;
+    double* sT0 = sm;                   // horizontal rho flux divergence (cells)
+    double* sT1 = sT0 + nz * TX;        // horizontal rho*theta flux divergence (cells)
+    double* sO = sT1 + nz * TX;         // Omega of the old increments (faces)
+    double* sR = sO + (nz + 1) * TX;    // right-hand side, then the solution (faces)
+    double* sA = sR + (nz + 1) * TX;
+    double* sI = sA + (nz + 1) * TX;
+    double* sCB = sI + (nz + 1) * TX;
+    const int64_t N = g.ncell, sk = g.sk;
+    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi, halfg = P.halfg;
     auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
     auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto ODU = [&](int ii, int jj, int kk) { return double(T.odu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
     auto ODV = [&](int ii, int jj, int kk) { return double(T.odv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
-    auto Z = [&](int a, int b, int cc) { return Zn(P, a, b, cc); };
-    int64_t f = cidx(g, i, j, k);
-    if (k < nz) {
-        double hxh = 0.5 * dzi * (Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j, k) - Z(i + 1, j + 1, k));
-        double hxl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
-        double hyh = 0.5 * dzi * (Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
-        double hyl = 0.5 * dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i + 1, j, k));
-        double xl = NDU(i, j, k) * hxl / 1.0, xh = NDU(i + 1, j, k) * hxh / 1.0;
-        double yl = NDV(i, j, k) * hyl / 1.0, yh = NDV(i, j + 1, k) * hyh / 1.0;
-        double mfsq = 1.0;
-        double tc = th(i, j, k);
-        T.tr0[f] = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
-        T.tr1[f] = ((xh * (tc + th(i + 1, j, k)) - xl * (tc + th(i - 1, j, k))) * dxi * mfsq +
-                    (yh * (tc + th(i, j + 1, k)) - yl * (tc + th(i, j - 1, k))) * dyi * mfsq) * 0.5;
+    auto prev_mz = [&](int k) {
+        if (prev_rt && (k == 0 || k == nz)) return T.bnd[(k == 0 ? 0 : sk) + (int64_t)j * g.nx + i];
+        return prev_mz_ter<R>(P, Sprev, prev_rt, i, j, k);
+    };
+    // ---- phase 1: horizontal fluxes (cells), Omega'' of the old increments and the coefficients (faces)
+    if (ok) {
+        for (int k = w0; k <= nz; k += nw) {
+            const int64_t f = cidx(g, i, j, k);
+            if (k < nz) {
+                double hxh = hzeta_I(P, i + 1, j, k), hxl = hzeta_I(P, i, j, k);
+                double hyh = hzeta_J(P, i, j + 1, k), hyl = hzeta_J(P, i, j, k);
+                double xl = NDU(i, j, k) * hxl / 1.0, xh = NDU(i + 1, j, k) * hxh / 1.0;
+                double yl = NDV(i, j, k) * hyl / 1.0, yh = NDV(i, j + 1, k) * hyh / 1.0;
+                double mfsq = 1.0;
+                double tc = th(i, j, k);
+                sT0[k * TX + L] = (xh - xl) * dxi * mfsq + (yh - yl) * dyi * mfsq;
+                sT1[k * TX + L] = ((xh * (tc + th(i + 1, j, k)) - xl * (tc + th(i - 1, j, k))) * dxi * mfsq +
+                                   (yh * (tc + th(i, j + 1, k)) - yl * (tc + th(i, j - 1, k))) * dyi * mfsq) * 0.5;
+            }
+            double odw = prev_mz(k) - Sst.mz[f];
+            double om;
+            if (k == 0) om = 0.;
+            else if (k == nz) om = odw;
+            else om = omega_from_w(P, i, j, k, odw, ODU, ODV);
+            sO[k * TX + L] = om;
+            sA[k * TX + L] = double(cA[f]);
+            sI[k * TX + L] = double(cInvB[f]);
+            sCB[k * TX + L] = double(cCB[f]);
+        }
     }
-    double odw = prev_mz_ter<R>(P, Sprev, prev_rt, i, j, k) - Sst.mz[f];
-    double om;
-    if (k == 0) om = 0.;
-    else if (k == nz) om = odw;
-    else om = omega_from_w(P, i, j, k, odw, ODU, ODV);
-    T.om[f] = om;
-}
-
-template <class R>
-__global__ void k_ter_fv_rhs(Params P, double dtau, double beta_1, double beta_2, StateBuf Sprev, int prev_rt,
-                             StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons, const R* __restrict__ Fmz,
-                             TerBuf<R> T, const R* __restrict__ cP, const R* __restrict__ cQ) {
-    const Geo& g = P.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny || k > g.nz) return;
-    const int nz = g.nz;
-    const int64_t N = g.ncell, sk = g.sk;
-    const double dzi = g.dzi, halfg = P.halfg;
-    int64_t f = cidx(g, i, j, k);
-    if (k == 0 || k == nz) {
-        T.sol[f] = dtau * double(Fmz[f]);
-        return;
+    __syncthreads();
+    // ---- phase 2: the detJ-weighted right-hand side of the Omega'' system (faces)
+    if (ok) {
+        for (int k = w0; k <= nz; k += nw) {
+            const int64_t f = cidx(g, i, j, k);
+            if (k == 0 || k == nz) {
+                sR[k * TX + L] = dtau * double(Fmz[f]);
+                continue;
+            }
+            int64_t cm = f - sk;
+            double Jk = detJ_at(P, i, j, k), Jkm = detJ_at(P, i, j, k - 1);
+            double dJk = 0.5 * (Jk + Jkm);
+            double cPk = double(cP[f]), cQk = double(cQ[f]);
+            double tlo = 0.5 * (th(i, j, k - 2) + th(i, j, k - 1));
+            double tmid = 0.5 * (th(i, j, k - 1) + th(i, j, k));
+            double thi = 0.5 * (th(i, j, k) + th(i, j, k + 1));
+            double odr_k = Sprev.cons[f] - Sst.cons[f], odr_km = Sprev.cons[cm] - Sst.cons[cm];
+            double odrt_k = Sprev.cons[N + f] - Sst.cons[N + f], odrt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
+            double R0t = (-halfg * odr_k + cPk * odrt_k) * Jk + (-halfg * odr_km + cQk * odrt_km) * Jkm;
+            double R1t = -halfg * (double(Fcons[f]) * Jk + double(Fcons[cm]) * Jkm)
+                         + (cPk * double(Fcons[N + f]) * Jk + cQk * double(Fcons[N + cm]) * Jkm);
+            double Okp1 = sO[(k + 1) * TX + L], Ok = sO[k * TX + L], Okm1 = sO[(k - 1) * TX + L];
+            R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + sT0[k * TX + L] + sT0[(k - 1) * TX + L]);
+            R1t += -(cPk * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + sT1[k * TX + L]) +
+                     cQk * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + sT1[(k - 1) * TX + L]));
+            double odw = prev_mz(k) - Sst.mz[f];
+            double rhs = dJk * odw + dtau * (dJk * double(Fmz[f]) + R0t + dtau * beta_2 * R1t);
+            rhs += dJk * omega_from_w(P, i, j, k, 0., NDU, NDV);
+            sR[k * TX + L] = rhs;
+        }
     }
-    auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
-    auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
-    auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
-    int64_t cm = f - sk;
-    double Jk = detJ_at(P, i, j, k), Jkm = detJ_at(P, i, j, k - 1);
-    double dJk = 0.5 * (Jk + Jkm);
-    double cPk = double(cP[f]), cQk = double(cQ[f]);
-    double tlo = 0.5 * (th(i, j, k - 2) + th(i, j, k - 1));
-    double tmid = 0.5 * (th(i, j, k - 1) + th(i, j, k));
-    double thi = 0.5 * (th(i, j, k) + th(i, j, k + 1));
-    double odr_k = Sprev.cons[f] - Sst.cons[f], odr_km = Sprev.cons[cm] - Sst.cons[cm];
-    double odrt_k = Sprev.cons[N + f] - Sst.cons[N + f], odrt_km = Sprev.cons[N + cm] - Sst.cons[N + cm];
-    double R0t = (-halfg * odr_k + cPk * odrt_k) * Jk + (-halfg * odr_km + cQk * odrt_km) * Jkm;
-    double R1t = -halfg * (double(Fcons[f]) * Jk + double(Fcons[cm]) * Jkm)
-                 + (cPk * double(Fcons[N + f]) * Jk + cQk * double(Fcons[N + cm]) * Jkm);
-    double Okp1 = T.om[f + sk], Ok = T.om[f], Okm1 = T.om[cm];
-    R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + T.tr0[f] + T.tr0[cm]);
-    R1t += -(cPk * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + T.tr1[f]) +
-             cQk * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + T.tr1[cm]));
-    double odw = prev_mz_ter<R>(P, Sprev, prev_rt, i, j, k) - Sst.mz[f];
-    double rhs = dJk * odw + dtau * (dJk * double(Fmz[f]) + R0t + dtau * beta_2 * R1t);
-    rhs += dJk * omega_from_w(P, i, j, k, 0., NDU, NDV);
-    T.sol[f] = rhs;
-}
-
-template <class R>
-__global__ void k_ter_fv_solve(Params P, TerBuf<R> T, const R* __restrict__ cA, const R* __restrict__ cInvB,
-                               const R* __restrict__ cCB) {
-    const Geo& g = P.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.nx || j >= g.ny) return;
-    const int nz = g.nz;
-    const int64_t sk = g.sk, col = (int64_t)j * g.nx + i;
-    double* sol = T.sol;
-    double s = sol[col] * double(cInvB[col]);
-    sol[col] = s;
-    for (int k = 1; k <= nz; ++k) {
-        int64_t f = (int64_t)k * sk + col;
-        s = (sol[f] - double(cA[f]) * s) * double(cInvB[f]);
-        sol[f] = s;
+    __syncthreads();
+    // ---- phase 3: forward elimination / back substitution, one warp
+    if (w0 == 0 && ok) {
+        double s = sR[L] * sI[L];
+        sR[L] = s;
+        for (int k = 1; k <= nz; ++k) {
+            s = (sR[k * TX + L] - sA[k * TX + L] * s) * sI[k * TX + L];
+            sR[k * TX + L] = s;
+        }
+        for (int k = nz - 1; k >= 0; --k) {
+            s = sR[k * TX + L] - sCB[k * TX + L] * s;
+            sR[k * TX + L] = s;
+        }
     }
-    for (int k = nz - 1; k >= 0; --k) {
-        int64_t f = (int64_t)k * sk + col;
-        s = sol[f] - double(cCB[f]) * s;
-        sol[f] = s;
+    __syncthreads();
+    // ---- phase 4: w'' from Omega'', vertical fluxes, average Omega, rho and rho*theta
+    if (ok) {
+        for (int k = w0; k <= nz; k += nw) {
+            const int64_t f = cidx(g, i, j, k);
+            double m = Sst.mz[f];
+            if (k >= 1 && k <= nz - 1) m += w_from_omega(P, i, j, k, sR[k * TX + L], NDU, NDV);
+            out_mz[f] = m;
+            if (k == nz) continue;
+            const int64_t c = f;
+            double zl = beta_2 * sR[k * TX + L] + beta_1 * sO[k * TX + L];
+            double zh = beta_2 * sR[(k + 1) * TX + L] + beta_1 * sO[(k + 1) * TX + L];
+            avz[c] += R(facinv * zl / (1.0 * 1.0));
+            if (k == nz - 1) avz[c + sk] += R(facinv * zh / (1.0 * 1.0));
+            double Jc = detJ_at(P, i, j, k);
+            double tc = th(i, j, k);
+            double frho = -(sT0[k * TX + L] + (zh - zl) * dzi) / Jc;
+            double frt = -(sT1[k * TX + L] + 0.5 * (zh * (tc + th(i, j, k + 1)) - zl * (tc + th(i, j, k - 1))) * dzi) / Jc;
+            double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
+            out_cons[c] = pr + dtau * (double(Fcons[c]) + frho);
+            out_cons[N + c] = prt + dtau * (double(Fcons[N + c]) + frt);
+        }
     }
-}
-
-template <class R>
-__global__ void k_ter_fv_update(Params P, double dtau, double facinv, double beta_1, double beta_2, StateBuf Sprev,
-                                StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons, TerBuf<R> T,
-                                R* __restrict__ avz, double* out_cons, double* out_mz) {
-    const Geo& g = P.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny || k > g.nz) return;
-    const int nz = g.nz;
-    const int64_t N = g.ncell, sk = g.sk;
-    const double dzi = g.dzi;
-    auto NDU = [&](int ii, int jj, int kk) { return double(T.ndu[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
-    auto NDV = [&](int ii, int jj, int kk) { return double(T.ndv[cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), kk)]); };
-    auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
-    int64_t f = cidx(g, i, j, k);
-    double m = Sst.mz[f];
-    if (k >= 1 && k <= nz - 1) m += w_from_omega(P, i, j, k, T.sol[f], NDU, NDV);
-    out_mz[f] = m;
-    if (k == nz) return;
-    int64_t c = f;
-    double zl = beta_2 * T.sol[c] + beta_1 * T.om[c];
-    double zh = beta_2 * T.sol[c + sk] + beta_1 * T.om[c + sk];
-    avz[c] += R(facinv * zl / (1.0 * 1.0));
-    if (k == nz - 1) avz[c + sk] += R(facinv * zh / (1.0 * 1.0));
-    double Jc = detJ_at(P, i, j, k);
-    double tc = th(i, j, k);
-    double frho = -(T.tr0[c] + (zh - zl) * dzi) / Jc;
-    double frt = -(T.tr1[c] + 0.5 * (zh * (tc + th(i, j, k + 1)) - zl * (tc + th(i, j, k - 1))) * dzi) / Jc;
-    double pr = Sprev.cons[c], prt = Sprev.cons[N + c];
-    out_cons[c] = pr + dtau * (double(Fcons[c]) + frho);
-    out_cons[N + c] = prt + dtau * (double(Fcons[N + c]) + frt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1533,16 +1546,30 @@ void launch_ter_fast_h(const Params& P, cudaStream_t st, int step, double dtau, 
                                                                    Fmy, lag_in, lag_out, T, avx, avy, outx, outy);
 }
 template <class R>
-void launch_ter_fast_vert(const Params& P, cudaStream_t st, double dtau, double facinv, double beta_1, double beta_2,
-                          StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmz,
-                          TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB, const R* cP, const R* cQ, R* avz,
-                          double* out_cons, double* out_mz) {
-    dim3 b = ter_block(), gf = ter_grid(P.g, P.g.nz + 1), gc((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1);
-    k_ter_fv_prep<R><<<gf, b, 0, st>>>(P, Sprev, prev_rt, Sst, A, T);
-    k_ter_fv_rhs<R><<<gf, b, 0, st>>>(P, dtau, beta_1, beta_2, Sprev, prev_rt, Sst, A, Fcons, Fmz, T, cP, cQ);
-    k_ter_fv_solve<R><<<gc, b, 0, st>>>(P, T, cA, cInvB, cCB);
-    k_ter_fv_update<R><<<gf, b, 0, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, Sst, A, Fcons, T, avz, out_cons,
-                                         out_mz);
+void launch_ter_fast_vert(const Params& P, cudaStream_t st, int tx, size_t smem, double dtau, double facinv,
+                          double beta_1, double beta_2, StateBuf Sprev, int prev_rt, StateBuf Sst, StageAux<R> A,
+                          const R* Fcons, const R* Fmz, TerBuf<R> T, const R* cA, const R* cInvB, const R* cCB,
+                          const R* cP, const R* cQ, R* avz, double* out_cons, double* out_mz) {
+    if (prev_rt)
+        k_ter_fv_bnd<R><<<dim3((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1), ter_block(), 0, st>>>(P, Sprev, T);
+    dim3 grid((P.g.nx + tx - 1) / tx, P.g.ny, 1), block(tx, 1024 / tx, 1);
+    k_ter_fast_vert<R><<<grid, block, smem, st>>>(P, dtau, facinv, beta_1, beta_2, Sprev, prev_rt, Sst, A, Fcons, Fmz,
+                                                  T, cA, cInvB, cCB, cP, cQ, avz, out_cons, out_mz);
+}
+// Columns per block of k_ter_fast_vert (the widest power of two up to 32 whose
+// FP64 column arrays fit) and its shared memory; 0 columns if none fits.
+void ter_vert_shape(int nz, int* tx, size_t* smem) {
+    int dev = 0, maxopt = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    int t = 32;
+    while (t >= 1 && (size_t)(7 * nz + 5) * t * sizeof(double) > (size_t)maxopt) t /= 2;
+    *tx = t;
+    *smem = t >= 1 ? (size_t)(7 * nz + 5) * t * sizeof(double) : 0;
+    if (t >= 1) {
+        cudaFuncSetAttribute(k_ter_fast_vert<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+        cudaFuncSetAttribute(k_ter_fast_vert<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+    }
 }
 template <class R>
 void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
@@ -1574,9 +1601,9 @@ void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf 
     template void launch_ter_fast_h<R>(const Params&, cudaStream_t, int, double, double, StateBuf, int, StateBuf,    \
                                        StageAux<R>, const R*, const R*, const R*, R*, TerBuf<R>, R*, R*, double*,    \
                                        double*);                                                                     \
-    template void launch_ter_fast_vert<R>(const Params&, cudaStream_t, double, double, double, double, StateBuf,     \
-                                          int, StateBuf, StageAux<R>, const R*, const R*, TerBuf<R>, const R*,       \
-                                          const R*, const R*, const R*, const R*, R*, double*, double*);             \
+    template void launch_ter_fast_vert<R>(const Params&, cudaStream_t, int, size_t, double, double, double, double, \
+                                          StateBuf, int, StateBuf, StageAux<R>, const R*, const R*, TerBuf<R>,       \
+                                          const R*, const R*, const R*, const R*, const R*, R*, double*, double*);   \
     template void launch_ter_post<R>(const Params&, cudaStream_t, double, StateBuf, StateBuf, StateBuf, StateBuf,    \
                                      StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, TerBuf<R>, const R*,        \
                                      const R*, const R*, double*, double*, double*);
