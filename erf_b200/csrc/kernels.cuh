@@ -44,7 +44,7 @@ struct Params {
 };
 
 // Number of static-terrain metric tables (planes of nzf values each).
-constexpr int TER_NMET = 11;
+constexpr int TER_NMET = 21;
 
 // One copy of the prognostic state: cons (ncomp*ncell), face momenta.
 struct StateBuf {

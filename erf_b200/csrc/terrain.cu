@@ -53,15 +53,15 @@ __device__ __forceinline__ double detJ_at(const Params& P, int i, int j, int k) 
     const Geo& g = P.g;
     return __ldg(P.detJ + cidx(g, wrap(i, g.nx), wrap(j, g.ny), clampk(k, g.nz)));
 }
-__device__ double hzeta_cc(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hzeta_cc_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dzi * (ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k + 1) + ZN(i, j, k + 1) + ZN(i, j + 1, k + 1)
                              - ZN(i + 1, j, k) - ZN(i + 1, j + 1, k) - ZN(i, j, k) - ZN(i, j + 1, k));
 }
-__device__ double hxi_cc(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hxi_cc_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j + 1, k) + ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k + 1)
                              - ZN(i, j, k) - ZN(i, j + 1, k) - ZN(i, j, k + 1) - ZN(i, j + 1, k + 1));
 }
-__device__ double heta_cc(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double heta_cc_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i + 1, j + 1, k) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k + 1)
                              - ZN(i, j, k) - ZN(i + 1, j, k) - ZN(i, j, k + 1) - ZN(i + 1, j, k + 1));
 }
@@ -81,7 +81,7 @@ __device__ __forceinline__ double heta_J_fn(const Params& P, int i, int j, int k
                               - ZN(i, j - 1, k) - ZN(i, j - 1, k + 1) - ZN(i + 1, j - 1, k) - ZN(i + 1, j - 1, k + 1));
 }
 // z faces
-__device__ double hzeta_K(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hzeta_K_fn(const Params& P, int i, int j, int k) {
     return 0.125 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k + 1)
                               - ZN(i, j, k - 1) - ZN(i + 1, j, k - 1) - ZN(i, j + 1, k - 1) - ZN(i + 1, j + 1, k - 1));
 }
@@ -93,24 +93,24 @@ __device__ __forceinline__ double heta_K_fn(const Params& P, int i, int j, int k
 }
 // xy edges (EdgeCenterK), xz edges (EdgeCenterJ), yz edges (EdgeCenterI)
 __device__ __forceinline__ double hzeta_EK_fn(const Params& P, int i, int j, int k) { return P.g.dzi * (ZN(i, j, k + 1) - ZN(i, j, k)); }
-__device__ double hxi_EK(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hxi_EK_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dxi * (ZN(i + 1, j, k) + ZN(i + 1, j, k + 1) - ZN(i - 1, j, k) - ZN(i - 1, j, k + 1));
 }
-__device__ double heta_EK(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double heta_EK_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dyi * (ZN(i, j + 1, k) + ZN(i, j + 1, k + 1) - ZN(i, j - 1, k) - ZN(i, j - 1, k + 1));
 }
 __device__ __forceinline__ double hzeta_EJ_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i, j + 1, k + 1) - ZN(i, j, k - 1) - ZN(i, j + 1, k - 1));
 }
-__device__ double hxi_EJ(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hxi_EJ_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dxi * (ZN(i + 1, j + 1, k) + ZN(i + 1, j, k) - ZN(i - 1, j + 1, k) - ZN(i - 1, j, k));
 }
-__device__ double heta_EJ(const Params& P, int i, int j, int k) { return P.g.dyi * (ZN(i, j + 1, k) - ZN(i, j, k)); }
+__device__ __forceinline__ double heta_EJ_fn(const Params& P, int i, int j, int k) { return P.g.dyi * (ZN(i, j + 1, k) - ZN(i, j, k)); }
 __device__ __forceinline__ double hzeta_EI_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dzi * (ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) - ZN(i, j, k - 1) - ZN(i + 1, j, k - 1));
 }
-__device__ double hxi_EI(const Params& P, int i, int j, int k) { return P.g.dxi * (ZN(i + 1, j, k) - ZN(i, j, k)); }
-__device__ double heta_EI(const Params& P, int i, int j, int k) {
+__device__ __forceinline__ double hxi_EI_fn(const Params& P, int i, int j, int k) { return P.g.dxi * (ZN(i + 1, j, k) - ZN(i, j, k)); }
+__device__ __forceinline__ double heta_EI_fn(const Params& P, int i, int j, int k) {
     return 0.25 * P.g.dyi * (ZN(i + 1, j + 1, k) + ZN(i, j + 1, k) - ZN(i + 1, j - 1, k) - ZN(i, j - 1, k));
 }
 // slopes of a z-face (OmegaFromW / WFromOmega, ERF_TerrainMetrics.H:455-520)
@@ -122,13 +122,14 @@ __device__ __forceinline__ double zlo_eta_fn(const Params& P, int i, int j, int 
 }
 #undef ZN
 
-// Static-terrain metric tables: the metric terms the passes read most,
-// evaluated once per face / edge by the functions above (so bit-identical to
+// Static-terrain metric tables: the metric terms the passes read,
+// evaluated once per cell / face / edge by the functions above (so bit-identical to
 // evaluating them in place) and stored as TER_NMET planes of (nz+1) x ny x
 // nx values, k in [0, nz].  A pass reads one value instead of re-deriving it
 // from four to eight nodes of z_phys_nd; outside [0, nz] the function runs.
 enum { MT_HZETA_I, MT_HXI_I, MT_HZETA_J, MT_HETA_J, MT_HXI_K, MT_HETA_K, MT_HZETA_EK, MT_HZETA_EJ, MT_HZETA_EI,
-       MT_ZLO_XI, MT_ZLO_ETA, MT_COUNT };
+       MT_ZLO_XI, MT_ZLO_ETA, MT_HZETA_CC, MT_HXI_CC, MT_HETA_CC, MT_HZETA_K, MT_HXI_EK, MT_HETA_EK, MT_HXI_EJ,
+       MT_HETA_EJ, MT_HXI_EI, MT_HETA_EI, MT_COUNT };
 static_assert(MT_COUNT == TER_NMET, "metric table count");
 __device__ __forceinline__ double mt_at(const Params& P, int q, int i, int j, int k) {
     const Geo& g = P.g;
@@ -150,6 +151,16 @@ ERFB_MT(hzeta_EJ, MT_HZETA_EJ)
 ERFB_MT(hzeta_EI, MT_HZETA_EI)
 ERFB_MT(zlo_xi, MT_ZLO_XI)
 ERFB_MT(zlo_eta, MT_ZLO_ETA)
+ERFB_MT(hzeta_cc, MT_HZETA_CC)
+ERFB_MT(hxi_cc, MT_HXI_CC)
+ERFB_MT(heta_cc, MT_HETA_CC)
+ERFB_MT(hzeta_K, MT_HZETA_K)
+ERFB_MT(hxi_EK, MT_HXI_EK)
+ERFB_MT(heta_EK, MT_HETA_EK)
+ERFB_MT(hxi_EJ, MT_HXI_EJ)
+ERFB_MT(heta_EJ, MT_HETA_EJ)
+ERFB_MT(hxi_EI, MT_HXI_EI)
+ERFB_MT(heta_EI, MT_HETA_EI)
 #undef ERFB_MT
 
 // Face-averaged horizontal components at z-face (i,j,k) of x/y-face arrays
@@ -259,6 +270,16 @@ __global__ void k_ter_met_tables(Params P, double* __restrict__ met) {
     m[MT_HZETA_EI * s] = hzeta_EI_fn(P, i, j, k);
     m[MT_ZLO_XI * s] = zlo_xi_fn(P, i, j, k);
     m[MT_ZLO_ETA * s] = zlo_eta_fn(P, i, j, k);
+    m[MT_HZETA_CC * s] = hzeta_cc_fn(P, i, j, k);
+    m[MT_HXI_CC * s] = hxi_cc_fn(P, i, j, k);
+    m[MT_HETA_CC * s] = heta_cc_fn(P, i, j, k);
+    m[MT_HZETA_K * s] = hzeta_K_fn(P, i, j, k);
+    m[MT_HXI_EK * s] = hxi_EK_fn(P, i, j, k);
+    m[MT_HETA_EK * s] = heta_EK_fn(P, i, j, k);
+    m[MT_HXI_EJ * s] = hxi_EJ_fn(P, i, j, k);
+    m[MT_HETA_EJ * s] = heta_EJ_fn(P, i, j, k);
+    m[MT_HXI_EI * s] = hxi_EI_fn(P, i, j, k);
+    m[MT_HETA_EI * s] = heta_EI_fn(P, i, j, k);
 }
 void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* zcc) {
     k_ter_metrics<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, detJ, zcc);
