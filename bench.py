@@ -280,6 +280,9 @@ def ensemble_arm(args, C, Dycore, Ensemble, stream, n_err=32):
     # warmup + ens_steps steps
     errs = []
     nsteps = args.warmup + nsteps_t
+
+    def rl2(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
     for q in range(n_err):
         dy, st = members[q]
         got = dy.store_state(*st)
@@ -287,7 +290,6 @@ def ensemble_arm(args, C, Dycore, Ensemble, stream, n_err=32):
         ref_dy.advance_resident(nsteps)
         ref = ref_dy.store_state(*st)
         ref_dy.close()
-        rl2 = lambda a, b: float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
         errs.append({"size": specs[q][:3], "u": rl2(got[1], ref[1]), "v": rl2(got[2], ref[2]), "w": rl2(got[3], ref[3]),
                      "theta": rl2(got[0][1] / got[0][0], ref[0][1] / ref[0][0])})
     ens.close()
@@ -295,6 +297,26 @@ def ensemble_arm(args, C, Dycore, Ensemble, stream, n_err=32):
         dy.close()
     net.close()
     worst = {f: max(e[f] for e in errs) for f in ("u", "v", "w", "theta")} if errs else {}
+    # the same comparison with the Smagorinsky closure for the first members:
+    # if these also decorrelate, the learned run's v / w error is the flow's
+    # sensitivity to FP32 rounding, not the network's
+    smag_errs = []
+    for q in range(2):
+        outs = {}
+        for prec in (C.PREC_FP64, C.PREC_MIXED):
+            case = member_case(*specs[q], prec)
+            case.cfg.les_type = C.LES_SMAGORINSKY
+            dy = Dycore(case.cfg, stream=stream.cuda_stream)
+            base = dy.make_base_state(case)
+            dy.set_base_state(base)
+            st = case.build_state(base[0])
+            dy.load_state(*st)
+            dy.advance_resident(nsteps)
+            outs[prec] = dy.store_state(*st)
+            dy.close()
+        got, ref = outs[C.PREC_MIXED], outs[C.PREC_FP64]
+        smag_errs.append({"size": specs[q][:3], "u": rl2(got[1], ref[1]), "v": rl2(got[2], ref[2]),
+                          "w": rl2(got[3], ref[3]), "theta": rl2(got[0][1] / got[0][0], ref[0][1] / ref[0][0])})
     return {"workload": f"{len(specs)} ABL members 64^3..192x192x96 (seeded), dx=dz=40 m, u_g 4-16 m/s, "
                         "mixed form + learned closure, all steps in one graph launch (device-side loop over "
                         "pairs of steps, host-polled abort word), autotuned",
@@ -302,7 +324,8 @@ def ensemble_arm(args, C, Dycore, Ensemble, stream, n_err=32):
             "finished": finished, "ms_per_step": ms / nsteps_t,
             "value": cells * nsteps_t / (ms * 1e-3), "unit": "cell-steps/s",
             "autotuned_ms_per_member_step": tuned, "status": max(status), "fallback_fraction": fb_frac,
-            "rel_l2_mixed_vs_fp64_per_member": errs, "rel_l2_mixed_vs_fp64_worst_member": worst}
+            "rel_l2_mixed_vs_fp64_per_member": errs, "rel_l2_mixed_vs_fp64_worst_member": worst,
+            "rel_l2_mixed_vs_fp64_smagorinsky_first_members": smag_errs}
 
 
 def terrain_arm(args, C, Dycore, stream, n_err=100):
@@ -311,7 +334,8 @@ def terrain_arm(args, C, Dycore, stream, n_err=100):
     mixed form's error against the plain form after n_err steps."""
     import torch
     from erf_b200 import terrain as T
-    case = T.abl_terrain(dt=0.25)
+    tn = [int(x) for x in args.terrain_size.split("x")]
+    case = T.abl_terrain(nx=tn[0], ny=tn[1], nz=tn[2], dt=0.25)
     cfg = case.cfg
     n_cells = cfg.nx * cfg.ny * cfg.nz
     out = {"workload": f"terrain ABL {cfg.nx}x{cfg.ny}x{cfg.nz}, dx={cfg.dx:g} m, levels stretched from 5 m "
@@ -440,6 +464,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble", "terrain"],
                     help="precision forms to time (the JSON line needs both; single forms are for profiling)")
+    ap.add_argument("--terrain-size", default="256x256x96",
+                    help="cells of the terrain ABL (nx x ny x nz); smaller only for profiling")
     ap.add_argument("--ens-steps", type=int, default=200,
                     help="steps of the ensemble arm (one graph launch)")
     ap.add_argument("--err-steps", type=int, default=100,

@@ -170,9 +170,11 @@ int validate(const erf_b200_config* c) {
     if (c->les_type == ERF_LES_MLP && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
     if (c->use_terrain != 0 && c->use_terrain != 1) return ERF_B200_ECONFIG;
     if (c->use_terrain) {
-        // terrain path: dry, LES closure (or no diffusion), explicit closures only
-        if (c->moisture != ERF_MOIST_NONE || c->les_type == ERF_LES_MLP) return ERF_B200_ECONFIG;
+        // terrain path: LES closure (or no diffusion), explicit closures only;
+        // with moisture, buoyancy type 1 (total density against the 3-D base state)
+        if (c->les_type == ERF_LES_MLP) return ERF_B200_ECONFIG;
         if (c->les_type == ERF_LES_NONE && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
+        if (c->moisture != ERF_MOIST_NONE && c->buoyancy_type != 1) return ERF_B200_ECONFIG;
     }
     if (c->molec_diff_type < 0 || c->molec_diff_type > 2) return ERF_B200_ECONFIG;
     if (c->moisture == ERF_MOIST_NONE) {
@@ -326,7 +328,10 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     double** Vnew = c->vel[1 - p];
     TIMED(0, launch_ter_step_begin<R>(P, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
                                       B.aux[0], B.mut, B.tke));
+    // stage outputs alternate between the two scratch states so that the last
+    // one lands in slot 1-p (or in N1 when Kessler moves it to slot 1-p)
     StateBuf outs[3] = {N0, N1, N0};
+    if (P.moist) { outs[0] = N1; outs[1] = N0; outs[2] = N1; }
     StateBuf stage[3] = {OLD, outs[0], outs[1]};
     dim3 tg((g.nx + c->tile_tx - 1) / c->tile_tx, g.ny, 1), tcb(c->tile_tx, c->coef_warps, 1);
     const bool fork = T == nullptr && c->side;
@@ -374,6 +379,10 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
         TIMED(7, launch_ter_post<R>(P, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut, B.tke,
                                     B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
+    }
+    if (P.moist) {   // Kessler with the sedimentation over detJ
+        dim3 kb(32, 1, KESS_KB), kg((g.nx + 31) / 32, g.ny, (g.nz + KESS_KB - 1) / KESS_KB);
+        TIMED(8, (k_kessler_cells<<<kg, kb, 0, st>>>(P, N1.cons, N0.cons, c->cfg.dt, c->cfg.dz)));
     }
 }
 
@@ -1221,6 +1230,7 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
 
 int erf_b200_kessler_advance(erf_b200_ctx* c, const erf_b200_fab* cons, double dt) {
     if (!c || !c->P.moist) return ERF_B200_EINVAL;
+    if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;   // the sedimentation reads detJ
     const Geo& g = c->g;
     if (!fab_ok(cons, 0, g, c->cfg.ncomp)) return ERF_B200_EINVAL;
     int rc;

@@ -654,7 +654,10 @@ __global__ void k_kessler(Params P, double* __restrict__ cons, double dtn, doubl
                 d_c2r = dtn * (accrr * qc + auto_r * (qc - 1.e-3));
                 d_c2r = fmin(d_c2r, qc);
             }
-            double dq_sed = dtn * 1.0 * (1.0 / rho) * (fz_hi - fz_lo) / dz;
+            // over terrain the fall-flux divergence is per unit computational volume
+            // (dJinv, ERF_Kessler.cpp:82-97)
+            const double dJinv = P.ter ? 1.0 / P.detJ[cidx(g, i, j, k)] : 1.0;
+            double dq_sed = dtn * dJinv * (1.0 / rho) * (fz_hi - fz_lo) / dz;
             if (fabs(dq_sed) < 1e-14) dq_sed = 0.0;
             qv += -d_v2c + d_c2v + d_r2v;
             qc += d_v2c - d_c2v - d_c2r;
@@ -1103,7 +1106,8 @@ __global__ void __launch_bounds__(32 * KESS_KB) k_kessler_cells(Params P, const 
             d_c2r = dtn * (accrr * qc + auto_r * (qc - 1.e-3));
             d_c2r = fmin(d_c2r, qc);
         }
-        double dq_sed = dtn * 1.0 * (1.0 / rho) * (fz_hi - fz_lo) / dz;
+        const double dJinv = P.ter ? 1.0 / P.detJ[c] : 1.0;   // ERF_Kessler.cpp:82-97
+        double dq_sed = dtn * dJinv * (1.0 / rho) * (fz_hi - fz_lo) / dz;
         if (fabs(dq_sed) < 1e-14) dq_sed = 0.0;
         qv += -d_v2c + d_c2v + d_r2v;
         qc += d_v2c - d_c2v - d_c2r;

@@ -99,11 +99,12 @@ int scratch_address(double** out) {
 extern "C" int erf_b200_kessler_advance_noalloc(const erf_b200_config* cfg, const erf_b200_fab* cons, double dt,
                                                 void* stream) {
     if (!cfg || !cons || !cons->p) return ERF_B200_EINVAL;
-    // the configuration rules of erf_b200_create (this rejects, among others,
-    // Kessler over terrain, whose sedimentation needs 1/detJ), plus Kessler
+    // the configuration rules of erf_b200_create, plus Kessler on a flat grid
+    // (over terrain the sedimentation needs 1/detJ, which only a context holds)
     int v = validate_config(cfg);
     if (v != ERF_B200_OK) return v;
     if (cfg->moisture != ERF_MOIST_KESSLER && cfg->moisture != ERF_MOIST_KESSLER_NORAIN) return ERF_B200_ECONFIG;
+    if (cfg->use_terrain) return ERF_B200_ECONFIG;
     if (!(cfg->c_p > 0.0)) return ERF_B200_ECONFIG;
     // the caller's view must cover the valid region with all components
     if (cons->lo[0] > 0 || cons->lo[1] > 0 || cons->lo[2] > 0 || cons->hi[0] < cfg->nx - 1 ||

@@ -188,6 +188,16 @@ __device__ __forceinline__ double w_from_omega(const Params& P, int i, int j, in
     return om + mx * u + my * v;
 }
 
+// qv + qc averaged over two cells (the moist pressure-gradient factor
+// 1 + q of ERF_slow_rhs_pre.cpp:594-744 and ERF_fast_rhs_T.cpp:230-300);
+// 0 for a dry state.
+template <class R>
+__device__ __forceinline__ double moist_q(const Params& P, const R* prim, int64_t a, int64_t b) {
+    if (!P.moist) return 0.0;
+    const int64_t N = P.g.ncell;
+    return 0.5 * (double(prim[4 * N + a]) + double(prim[4 * N + b]) + double(prim[5 * N + a]) + double(prim[5 * N + b]));
+}
+
 // Base state at (i,j,k), k in [-1, nz].
 __device__ __forceinline__ double bs(const double* f, const Geo& g, int i, int j, int k) {
     return __ldg(f + (int64_t)(k + 1) * g.sk + (int64_t)j * g.nx + i);
@@ -371,7 +381,7 @@ namespace {
 // edges [0,nz].
 // ---------------------------------------------------------------------------
 template <class FU, class FV, class FW>
-__device__ void strain_cc_T(const Params& P, int i, int j, int k, FU U, FV V, FW W, double& s11, double& s22,
+__device__ __forceinline__ void strain_cc_T(const Params& P, int i, int j, int k, FU U, FV V, FW W, double& s11, double& s22,
                             double& s33) {
     const double dxi = P.g.dxi, dyi = P.g.dyi, dzi = P.g.dzi;
     double GradUz, GradVz;
@@ -390,7 +400,7 @@ __device__ void strain_cc_T(const Params& P, int i, int j, int k, FU U, FV V, FW
     s33 = (W(i, j, k + 1) - W(i, j, k)) * dzi / mz;
 }
 template <class FU, class FV>
-__device__ double strain12_T(const Params& P, int i, int j, int k, FU U, FV V) {
+__device__ __forceinline__ double strain12_T(const Params& P, int i, int j, int k, FU U, FV V) {
     const double dxi = P.g.dxi, dyi = P.g.dyi, dzi = P.g.dzi;
     double GradUz, GradVz;
     if (k == 0 && P.g.zlo_noslip) {
@@ -407,7 +417,7 @@ __device__ double strain12_T(const Params& P, int i, int j, int k, FU U, FV V) {
                   - (meta / mz) * GradUz - (mxi / mz) * GradVz) * 1.0 * 1.0;
 }
 template <class FU, class FW>
-__device__ double strain13_T(const Params& P, int i, int j, int k, FU U, FW W) {
+__device__ __forceinline__ double strain13_T(const Params& P, int i, int j, int k, FU U, FW W) {
     const double dxi = P.g.dxi, dzi = P.g.dzi;
     const int nz = P.g.nz;
     double mz = hzeta_EJ(P, i, j, k);
@@ -430,7 +440,7 @@ __device__ double strain13_T(const Params& P, int i, int j, int k, FU U, FW W) {
     return 0.5 * ((U(i, j, k) - U(i, j, k - 1)) * dzi / mz + ((W(i, j, k) - W(i - 1, j, k)) * dxi - (mxi / mz) * GradWz) * 1.0);
 }
 template <class FV, class FW>
-__device__ double strain23_T(const Params& P, int i, int j, int k, FV V, FW W) {
+__device__ __forceinline__ double strain23_T(const Params& P, int i, int j, int k, FV V, FW W) {
     const double dyi = P.g.dyi, dzi = P.g.dzi;
     const int nz = P.g.nz;
     double mz = hzeta_EI(P, i, j, k);
@@ -454,7 +464,7 @@ __device__ double strain23_T(const Params& P, int i, int j, int k, FV V, FW W) {
 }
 // ComputeSmnSmn (Diffusion/ERF_EddyViscosity.H:31-83) from the terrain strains
 template <class FU, class FV, class FW>
-__device__ double smnsmn_T(const Params& P, int i, int j, int k, FU U, FV V, FW W) {
+__device__ __forceinline__ double smnsmn_T(const Params& P, int i, int j, int k, FU U, FV V, FW W) {
     double s11, s22, s33;
     strain_cc_T(P, i, j, k, U, V, W, s11, s22, s33);
     double s12 = 0.25 * (strain12_T(P, i, j, k, U, V) + strain12_T(P, i, j + 1, k, U, V) + strain12_T(P, i + 1, j, k, U, V)
@@ -743,9 +753,9 @@ struct DiffT {
     double ae, fac;
     const R* fxr = nullptr;   // raw face fluxes from k_ter_rawflux, when given
     const R* fyr = nullptr;
-    __device__ double p(int i, int j, int k) const { return ccw(phi, P.g, i, j, k); }
-    __device__ double mu(int i, int j, int k) const { return ccw(mut, P.g, i, j, k) * fac; }
-    __device__ double xraw(int i, int j, int k) const {
+    __device__ __forceinline__ double p(int i, int j, int k) const { return ccw(phi, P.g, i, j, k); }
+    __device__ __forceinline__ double mu(int i, int j, int k) const { return ccw(mut, P.g, i, j, k) * fac; }
+    __device__ __forceinline__ double xraw(int i, int j, int k) const {
         const Geo& g = P.g;
         double rA = P.use_consA ? (0.5 * (ccw(rho, g, i, j, k) + ccw(rho, g, i - 1, j, k))) * ae : ae;
         if (P.use_turb) rA += 0.5 * (mu(i, j, k) + mu(i - 1, j, k));
@@ -754,7 +764,7 @@ struct DiffT {
         double GradCx = g.dxi * (p(i, j, k) - p(i - 1, j, k));
         return -rA * 1.0 * (GradCx - (mxi / mz) * GradCz);
     }
-    __device__ double yraw(int i, int j, int k) const {
+    __device__ __forceinline__ double yraw(int i, int j, int k) const {
         const Geo& g = P.g;
         double rA = P.use_consA ? (0.5 * (ccw(rho, g, i, j, k) + ccw(rho, g, i, j - 1, k))) * ae : ae;
         if (P.use_turb) rA += 0.5 * (mu(i, j, k) + mu(i, j - 1, k));
@@ -763,16 +773,16 @@ struct DiffT {
         double GradCy = g.dyi * (p(i, j, k) - p(i, j - 1, k));
         return -rA * 1.0 * (GradCy - (meta / mz) * GradCz);
     }
-    __device__ double xr(int i, int j, int k) const {
+    __device__ __forceinline__ double xr(int i, int j, int k) const {
         if (fxr) return double(fxr[cidx(P.g, wrap(i, P.g.nx), wrap(j, P.g.ny), k)]);
         return xraw(i, j, k);
     }
-    __device__ double yr(int i, int j, int k) const {
+    __device__ __forceinline__ double yr(int i, int j, int k) const {
         if (fyr) return double(fyr[cidx(P.g, wrap(i, P.g.nx), wrap(j, P.g.ny), k)]);
         return yraw(i, j, k);
     }
     // z-face flux (k in [0, nz]); raw receives the flux before the cross terms
-    __device__ double zflux(int i, int j, int k, double& raw) const {
+    __device__ __forceinline__ double zflux(int i, int j, int k, double& raw) const {
         const Geo& g = P.g;
         const int nz = g.nz;
         double rA = P.use_consA ? (0.5 * (ccw(rho, g, i, j, k) + ccw(rho, g, i, j, k - 1))) * ae : ae;
@@ -802,7 +812,7 @@ struct DiffT {
         return fz;
     }
     // divergence over detJ (the amount the reference subtracts from the RHS)
-    __device__ double div(int i, int j, int k, double& raw_lo, double& raw_hi) const {
+    __device__ __forceinline__ double div(int i, int j, int k, double& raw_lo, double& raw_hi) const {
         const Geo& g = P.g;
         double fxl = xr(i, j, k) * hzeta_I(P, i, j, k), fxh = xr(i + 1, j, k) * hzeta_I(P, i + 1, j, k);
         double fyl = yr(i, j, k) * hzeta_J(P, i, j, k), fyh = yr(i, j + 1, k) * hzeta_J(P, i, j + 1, k);
@@ -815,7 +825,7 @@ struct DiffT {
 // Contravariant momentum Omega at z-face (i,j,k) of a state whose face
 // velocities are u, v (for the momentum ghost above the lid):
 // 0 at the ground, OmegaFromW inside and at the lid (ERF_slow_rhs_pre.cpp:365-420).
-__device__ double omega_mom(const Params& P, StateBuf S, const double* u, const double* v, int i, int j, int k) {
+__device__ __forceinline__ double omega_mom(const Params& P, StateBuf S, const double* u, const double* v, int i, int j, int k) {
     const Geo& g = P.g;
     if (k <= 0) return 0.;
     auto MX = [&](int ii, int jj, int kk) {
@@ -840,7 +850,7 @@ __device__ double omega_mom(const Params& P, StateBuf S, const double* u, const 
 // Face interpolation of a cell field along x / y / z with run-time scheme
 // (the stencil's unused entries are zero); upw the advecting flux.
 template <class FP>
-__device__ double interp_dir(int dir, int i, int j, int k, FP phi, int type, double upw, double frac) {
+__device__ __forceinline__ double interp_dir(int dir, int i, int j, int k, FP phi, int type, double upw, double frac) {
     double s[6];
     const int w = stencil_width(type);
 #pragma unroll
@@ -1014,7 +1024,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             xsrc += P.cf * (rvl * P.sinphi - rwl * P.cosphi);
         }
         xsrc += 0.5 * (S.cons[c] + S.cons[cidx(g, wrap(i - 1, g.nx), j, k)]) * P.geo0;
-        r += (-gpx - 0.0) / (1.0 + 0.0) + xsrc;
+        r += (-gpx - 0.0) / (1.0 + moist_q(P, A.prim, c, cidx(g, wrap(i - 1, g.nx), j, k))) + xsrc;
         Fmx[c] = R(r);
     }
     // ---------------- y-momentum at face (i,j,k)
@@ -1064,7 +1074,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             ysrc += -P.cf * rul * P.sinphi;
         }
         ysrc += 0.5 * (S.cons[c] + S.cons[cidx(g, i, wrap(j - 1, g.ny), k)]) * P.geo1;
-        r += (-gpy - 0.0) / (1.0 + 0.0) + ysrc;
+        r += (-gpy - 0.0) / (1.0 + moist_q(P, A.prim, c, cidx(g, i, wrap(j - 1, g.ny), k))) + ysrc;
         Fmy[c] = R(r);
     }
     // ---------------- z-momentum at face (i,j,k), 1 <= k <= nz-1
@@ -1134,7 +1144,14 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
         double mz = hzeta_K(P, i, j, k);
         double gpz = dzi * (pp(i, j, k) - pp(i, j, k - 1)) / mz;
         double zsrc = 0.0;
-        if (P.buoy_type == 1) {
+        if (P.buoy_type == 1 && P.moist) {
+            // total density of air and water (make_buoyancy, ERF_make_buoyancy.cpp:92-130)
+            const int nq = P.ncomp - ERF_RHOQ1_COMP;
+            double hi = S.cons[c] + S.cons[5 * N + c] + S.cons[6 * N + c] - bs(P.r0, g, i, j, k);
+            double lo = S.cons[c - g.sk] + S.cons[5 * N + c - g.sk] + S.cons[6 * N + c - g.sk] - bs(P.r0, g, i, j, k - 1);
+            for (int qo = 2; qo < nq; ++qo) { hi += S.cons[(5 + qo) * N + c]; lo += S.cons[(5 + qo) * N + c - g.sk]; }
+            zsrc = g2 * 0.5 * (hi + lo);
+        } else if (P.buoy_type == 1) {
             zsrc = g2 * 0.5 * ((S.cons[c] - bs(P.r0, g, i, j, k)) + (S.cons[c - g.sk] - bs(P.r0, g, i, j, k - 1)));
         } else {
             auto T0 = [&](int kk) {
@@ -1153,7 +1170,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             zsrc += P.cf * rul * P.cosphi;
         }
         zsrc += 0.5 * (S.cons[c] + S.cons[c - g.sk]) * P.geo2;
-        r += (zsrc - gpz - 0.0) / (1.0 + 0.0);
+        r += (zsrc - gpz - 0.0) / (1.0 + moist_q(P, A.prim, c, c - g.sk));
         Fmz[c] = R(r);
         if (k == nz - 1) Fmz[c + g.sk] = R(0);
     }
@@ -1203,6 +1220,7 @@ __global__ void k_ter_fast_h(Params P, int step, double dtau, double facinv, Sta
                                   : 0.25 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k - 1) - extrap(i, j, k - 1));
         gpx = gp_xi - (mxi / mz) * gp_zeta;
         gpx *= 1.0;
+        gpx /= (1.0 + moist_q(P, A.prim, c, cxm));
     }
     {
         double meta = heta_J(P, i, j, k), mz = hzeta_J(P, i, j, k);
@@ -1211,6 +1229,7 @@ __global__ void k_ter_fast_h(Params P, int step, double dtau, double facinv, Sta
                                   : 0.25 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k - 1) - extrap(i, j - 1, k - 1));
         gpy = gp_eta - (meta / mz) * gp_zeta;
         gpy *= 1.0;
+        gpy /= (1.0 + moist_q(P, A.prim, c, cym));
     }
     double pix = 0.5 * (double(A.pi[cxm]) + double(A.pi[c]));
     double piy = 0.5 * (double(A.pi[cym]) + double(A.pi[c]));
@@ -1236,7 +1255,7 @@ __global__ void k_ter_fast_h(Params P, int step, double dtau, double facinv, Sta
 // ---------------------------------------------------------------------------
 namespace {
 template <class R>
-__device__ double prev_mz_ter(const Params& P, StateBuf Sprev, int prev_rt, int i, int j, int k) {
+__device__ __forceinline__ double prev_mz_ter(const Params& P, StateBuf Sprev, int prev_rt, int i, int j, int k) {
     const Geo& g = P.g;
     const int nz = g.nz;
     int64_t f = cidx(g, i, j, k);
@@ -1441,13 +1460,16 @@ __global__ void __launch_bounds__(128, TER_MINB_POST) k_ter_post(Params P, doubl
     auto AX = [&](int ii) { return double(avx[cidx(g, wrap(ii, g.nx), j, k)]); };
     auto AY = [&](int jj) { return double(avy[cidx(g, i, wrap(jj, g.ny), k)]); };
     auto AZ = [&](int kk) { return double(avz[cidx(g, i, j, kk)]); };
-    const int nslow = 1 + (dd ? 1 : 0);
+    // slow variables: the passive scalar, the moisture species, then (Deardorff) rho*KE
+    const int nscal = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
+    const int nslow = nscal + (dd ? 1 : 0);
     for (int q = 0; q < nslow; ++q) {
-        const int n = (q == 0) ? ERF_RHOSCALAR_COMP : ERF_RHOKE_COMP;
+        const bool ke = q >= nscal, species = q > 0 && q < nscal;
+        const int n = q == 0 ? ERF_RHOSCALAR_COMP : (ke ? ERF_RHOKE_COMP : ERF_RHOQ1_COMP + q - 1);
         const R* phi = Acur.prim + (int64_t)(n - 1) * N;
         auto ph = [&](int ii, int jj, int kk) { return ccw(phi, g, ii, jj, kk); };
-        const int ht = P.dry_h, vt = P.dry_v;
-        const double hf = P.f_dry_h, vf = P.f_dry_v;
+        const int ht = species ? P.moi_h : P.dry_h, vt = species ? P.moi_v : P.dry_v;
+        const double hf = species ? P.f_moi_h : P.f_dry_h, vf = species ? P.f_moi_v : P.f_dry_v;
         double fxl = AX(i), fxh = AX(i + 1), fyl = AY(j), fyh = AY(j + 1), fzl = AZ(k), fzh = AZ(k + 1);
         double tx_l = fxl * interp_dir(0, i, j, k, ph, ht, fxl, hf), tx_h = fxh * interp_dir(0, i + 1, j, k, ph, ht, fxh, hf);
         double ty_l = fyl * interp_dir(1, i, j, k, ph, ht, fyl, hf), ty_h = fyh * interp_dir(1, i, j + 1, k, ph, ht, fyh, hf);
@@ -1455,18 +1477,19 @@ __global__ void __launch_bounds__(128, TER_MINB_POST) k_ter_post(Params P, doubl
         double invdetJ = 1. / Jc;
         double r = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
         if (P.use_diff) {
-            DiffT<R> D{P, Sst.cons, phi, mut, nullptr, q == 0 ? P.alphaC_eff : 0.0, q == 0 ? P.invSc : P.invSigmaK,
-                       T.fx[q], T.fy[q]};
+            // raw x / y fluxes precomputed for the scalar and KE; the species' formed here
+            DiffT<R> D{P, Sst.cons, phi, mut, nullptr, ke ? 0.0 : P.alphaC_eff, ke ? P.invSigmaK : P.invSc,
+                       species ? nullptr : T.fx[ke ? 1 : 0], species ? nullptr : T.fy[ke ? 1 : 0]};
             double rlo, rhi;
             r -= D.div(i, j, k, rlo, rhi);
         }
-        if (q == 1) {
+        if (ke) {
             r += P.g_over_theta0 * double(tke.hfz[c]);
             r += 2.0 * double(mut[c]) * double(tke.smn[c]);
             r -= double(tke.diss[c]);
         }
         double v_ = Sold.cons[n * N + c] + slow_dt * r;
-        Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, 2.220446049250313e-16);
+        Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, species ? 0.0 : 2.220446049250313e-16);
     }
     Snew.cons[c] = Ssum.cons[c];
     Snew.cons[N + c] = Ssum.cons[N + c];

@@ -110,6 +110,10 @@ class TerrainCase:
         cons[1] = rho * theta
         if "tke0" in self.pert:
             cons[2] = rho * self.pert["tke0"]
+        if cfg.moisture != C.MOIST_NONE:
+            cons[5] = rho * self.qv3
+            if "qr0" in self.pert and cfg.ncomp > 7:
+                cons[7] = rho * self.pert["qr0"]
         u = np.full((nz, ny, nx + 1), float(self.u0))
         v = np.full((nz, ny + 1, nx), float(self.v0))
         w = np.zeros((nz + 1, ny, nx))
@@ -153,3 +157,50 @@ def abl_terrain(nx=256, ny=256, nz=96, dx=25.0, dz0=5.0, stretch=1.04, seed=2, l
         pert["tke0"] = 0.1
     return TerrainCase("abl_terrain", c, z_nd, theta3, np.zeros_like(theta3), 300.0, 0.0, 1.0e5,
                        u0, 0.0, seed, pert=pert, steps=100)
+
+
+def moist_hill(nx=24, ny=20, nz=24, dx=1000.0, dz=250.0, h0=1000.0, r0=4000.0, seed=3, dt=0.5) -> TerrainCase:
+    """A moist warm bubble over a Gaussian hill (Kessler with rain, WENO5
+    moisture, buoyancy type 1, slip walls, no diffusion): theta 300 K at the
+    ground rising as 43 K (z / 12 km)^1.25, relative humidity 0.95 falling to
+    0.25 aloft (Tetens saturation over a dry hydrostatic pressure estimate),
+    a +2 K bubble of 4 km radius centred 2 km above the hill top in which the
+    air is 2 % supersaturated and carries 0.1 g/kg of rain, so that
+    condensation, evaporation and sedimentation all act from the first
+    step, and a 5 m/s wind across the hill."""
+    from . import cases as CS
+    c = C.defaults()
+    c.nx, c.ny, c.nz = nx, ny, nz
+    c.dx = c.dy = dx
+    c.dz = dz
+    c.zlo_bc = c.zhi_bc = C.BC_SLIP_WALL
+    c.dt, c.mri_ratio = dt, 4
+    c.ncomp, c.moisture = 8, C.MOIST_KESSLER
+    c.dycore_horiz_adv = c.dycore_vert_adv = C.UPWIND_5TH
+    c.dryscal_horiz_adv = c.dryscal_vert_adv = C.UPWIND_5TH
+    c.moistscal_horiz_adv = c.moistscal_vert_adv = C.WENO_5
+    c.molec_diff_type = C.MOLEC_NONE
+    c.les_type = C.LES_NONE
+    c.gravity = C.CONST_GRAV
+    c.buoyancy_type = 1
+    c.use_terrain = 1
+    zl = zlevels(nz, dz)
+    h = hill(nx, ny, dx, dx, h0, r0, 0.0, 1)
+    z_nd = btf_nodes(zl, h)
+    zc = cell_heights(z_nd)
+    theta3 = 300.0 + 43.0 * (zc / 12000.0) ** 1.25
+    rh = 0.95 - 0.70 * (zc / 12000.0) ** 1.25
+    p = 1.0e5 * (1.0 - C.CONST_GRAV * zc / (C.CP_D * 300.0)) ** (C.CP_D / C.R_D)
+    T3 = theta3 * (p / 1.0e5) ** (C.R_D / C.CP_D)
+    xc = (np.arange(nx) + 0.5) * dx
+    yc = (np.arange(ny) + 0.5) * dx
+    X, Y = np.meshgrid(xc, yc)
+    zb = h0 + 2000.0
+    rr = np.sqrt(((X - 0.5 * nx * dx) / r0)[None] ** 2 + ((Y - 0.5 * ny * dx) / r0)[None] ** 2
+                 + ((zc - zb) / 1500.0) ** 2)
+    inside = rr < 1.0
+    theta3 = theta3 + np.where(inside, 2.0 * np.cos(0.5 * np.pi * np.minimum(rr, 1.0)) ** 2, 0.0)
+    qsat = CS._tetens_qsat(T3, p)
+    qv3 = np.where(inside, 1.02 * qsat, np.minimum(0.014, rh * qsat))
+    return TerrainCase("moist_hill", c, z_nd, theta3, qv3, 300.0, float(qv3[0].mean()), 1.0e5, 5.0, 0.0, seed,
+                       pert={"qr0": np.where(inside, 1.0e-4, 0.0)}, steps=10)

@@ -82,6 +82,20 @@ def kessler(cfg, cons, dt):
     return out
 
 
+def kessler_terrain(cfg, z_nd, cons, dt):
+    """Kessler alone over a terrain grid (sedimentation over detJ)."""
+    L = lib()
+    L.oracle_kessler_terrain.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double), ctypes.c_double]
+    L.oracle_kessler_terrain.restype = ctypes.c_int
+    out = np.ascontiguousarray(cons, dtype=np.float64).copy()
+    z = np.ascontiguousarray(z_nd, dtype=np.float64)
+    rc = L.oracle_kessler_terrain(ctypes.byref(cfg), _p(z), _p(out), float(dt))
+    if rc != 0:
+        raise RuntimeError("oracle_kessler_terrain failed: %d" % rc)
+    return out
+
+
 PASSES = ("closure", "slow_rhs_pre", "fast", "slow_rhs_post", "kessler", "other")
 
 

@@ -15,10 +15,12 @@
 // reference gold plotfiles checked in tests/test_oracle_gold.py.
 //
 // Scope (what the C-ABI product supports): one box covering the domain,
-// periodic in x and y, SlipWall / NoSlipWall at the bottom and top, no terrain,
-// map factors 1, implicit acoustic substepping, Smagorinsky or no LES closure,
-// Constant / ConstantAlpha / no molecular diffusion, dry buoyancy type 1 or
-// moist type 2, Coriolis and geostrophic forcing, Kessler microphysics.
+// periodic in x and y, SlipWall / NoSlipWall at the bottom and top or a MOST
+// ground (flat), flat or static terrain-following grids, map factors 1,
+// implicit acoustic substepping or none, Smagorinsky / Deardorff or no LES
+// closure, Constant / ConstantAlpha / no molecular diffusion, buoyancy types
+// 1-3 (moist over terrain: type 1), Coriolis and geostrophic forcing, Kessler
+// microphysics with or without rain.
 //
 // Layout of the arrays exchanged through the C entry points: dense valid
 // regions, i fastest:  cons[ncomp][nz][ny][nx], u[nz][ny][nx+1],
@@ -819,8 +821,8 @@ struct Oracle {
         } else if (c.buoyancy_type == 1) {
             int nq = ncomp - ERF_RHOQ1_COMP;
             loop(tbz_b, [&](int i, int j, int k) {
-                double hi = cd(i, j, k, 0) + cd(i, j, k, 5) + cd(i, j, k, 6) - r0[k + 1];
-                double lo = cd(i, j, k - 1, 0) + cd(i, j, k - 1, 5) + cd(i, j, k - 1, 6) - r0[k];
+                double hi = cd(i, j, k, 0) + cd(i, j, k, 5) + cd(i, j, k, 6) - R0(i, j, k);
+                double lo = cd(i, j, k - 1, 0) + cd(i, j, k - 1, 5) + cd(i, j, k - 1, 6) - R0(i, j, k - 1);
                 for (int qo = 2; qo < nq; ++qo) { hi += cd(i, j, k, 5 + qo); lo += cd(i, j, k - 1, 5 + qo); }
                 zsrc(i, j, k) = g2 * 0.5 * (hi + lo);
             });
@@ -1412,7 +1414,9 @@ struct Oracle {
                     d_c2r = dtn * (accrr * qcc + auto_r * (qcc - qcw0));
                     d_c2r = std::min(d_c2r, qc(i, j, k));
                 }
-                double dq_sed = dtn * 1.0 * (1.0 / rho(i, j, k)) * (fz(i, j, k + 1) - fz(i, j, k)) / dz;
+                // over terrain per unit computational volume (ERF_Kessler.cpp:82-97)
+                double dJinv = terrain ? 1.0 / detJ(i, j, k) : 1.0;
+                double dq_sed = dtn * dJinv * (1.0 / rho(i, j, k)) * (fz(i, j, k + 1) - fz(i, j, k)) / dz;
                 if (std::fabs(dq_sed) < 1e-14) dq_sed = 0.0;
                 qv(i, j, k) += -d_v2c + d_c2v + d_r2v;
                 qc(i, j, k) += d_v2c - d_c2v - d_c2r;
@@ -2644,6 +2648,21 @@ int oracle_advance_terrain(const erf_b200_config* cfg, const double* z_nd, const
 int oracle_kessler(const erf_b200_config* cfg, double* cons, double dt) {
     if (cfg->moisture != ERF_MOIST_KESSLER && cfg->moisture != ERF_MOIST_KESSLER_NORAIN) return 1;
     std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
+    Fab f;
+    o->alloc(f, CC, o->ngc, o->ncomp);
+    load_cc(f, cons, nx, ny, nz, o->ncomp);
+    o->kessler(f, dt);
+    store_cc(f, cons, nx, ny, nz, o->ncomp);
+    return 0;
+}
+
+// Kessler alone over a terrain grid (z_nd: valid nodes): the sedimentation
+// divergence over detJ (ERF_Kessler.cpp:82-97).
+int oracle_kessler_terrain(const erf_b200_config* cfg, const double* z_nd, double* cons, double dt) {
+    if (cfg->moisture != ERF_MOIST_KESSLER && cfg->moisture != ERF_MOIST_KESSLER_NORAIN) return 1;
+    std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    o->set_terrain(z_nd);
     int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
     Fab f;
     o->alloc(f, CC, o->ngc, o->ncomp);
