@@ -203,11 +203,17 @@ def learned_arm(measure, form_error, C):
     ce = mk()
     ce.cfg.les_type = C.LES_MLP
     err = form_error(base, init, 100, case=ce, net=net)
+    # the same mixed-vs-FP64 comparison with Smagorinsky: the share of the
+    # error that the flow's sensitivity to FP32 rounding gives by itself
+    cs = mk()
+    cs.cfg.les_type = C.LES_SMAGORINSKY
+    err_smag = form_error(base, init, 100, case=cs)
     net.close()
     return {"workload": "abl coarse 128x128x32, dx=dz=40 m, dt=0.32 s, learned closure (tcgen05 BF16 MLP)",
             "fp64_smagorinsky": smag, "fp64_learned": l64, "mixed_learned": l32,
             "speedup_mixed_learned_vs_fp64_smagorinsky": l32["value"] / smag["value"],
-            "rel_l2_mixed_vs_fp64_learned_after_100_steps": err}
+            "rel_l2_mixed_vs_fp64_learned_after_100_steps": err,
+            "rel_l2_mixed_vs_fp64_smagorinsky_after_100_steps": err_smag}
 
 
 def ensemble_members(n=32, seed=100):
