@@ -101,3 +101,26 @@ def test_fallback_outside_envelope():
     assert all(np.all(np.isfinite(a)) for a in out)
     dy.close()
     net.close()
+
+
+def test_trained_closure_aposteriori_gain():
+    """The shipped network (erf_b200/data/closure_abl.npz, trained by
+    `python -m erf_b200.closure` on four fine ABL runs) against Smagorinsky a
+    posteriori on the held-out run (u_g = 15 m/s, seed 4, 256x256x64 fine,
+    coarse-grained by 4, 25 coarse steps after a 400-step spin-up): both
+    coarse runs start from the coarse-grained fine state and are compared with
+    the coarse-grained fine run.  The network's u (the mean-flow component)
+    is closer to the truth than Smagorinsky's, and its theta is no worse; the
+    fluctuating v and w are printed (both closures decorrelate from the fine
+    run's turbulence within these steps)."""
+    import os
+    from erf_b200 import closure
+    path = os.path.join(os.path.dirname(closure.__file__), "data", "closure_abl.npz")
+    net = closure.load_closure(path)
+    held = cases.abl_fine(nx=256, ny=256, nz=64, u_g=15.0, seed=4)
+    post = closure.aposteriori(net, held, 4, spinup=400, nsteps_coarse=25)
+    net.close()
+    print("a posteriori, held-out run:", json.dumps(post))
+    assert post["mlp"]["status"] == 0 and post["smagorinsky"]["status"] == 0
+    assert post["mlp"]["u"] < post["smagorinsky"]["u"], post
+    assert post["mlp"]["theta"] <= 1.05 * post["smagorinsky"]["theta"], post
