@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liberf_b200.so")
 SOURCES = ["kernels.cu", "terrain.cu", "api.cu", "noalloc.cu", "mlp.cu", "closure.cu", "plotfile.cu", "checkpoint.cu"]
-HEADERS = ["common.cuh", "kernels.cuh", "tcgen05.cuh", "mlp.cuh", "amrex_io.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "tiles.cuh", "tcgen05.cuh", "mlp.cuh", "amrex_io.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -376,7 +376,7 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                              Sst, Acur, B.Fcons, B.Fmz, B.ter, B.cA, B.cInvB, B.cCB, B.cP, B.cQ,
                                              B.avz, SUM.cons, SUM.mz));
         }
-        TIMED(7, launch_ter_post<R>(P, st, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut, B.tke,
+        TIMED(7, launch_ter_post<R>(P, st, c->tkz.ter_post, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext, nrk < 2 ? 1 : 0, B.mut, B.tke,
                                     B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1], Vnew[2]));
         a = 1 - a;
     }
@@ -653,6 +653,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     make_params(c);
     if (c->mixed) tiled_setup<float>(c->P, &c->tkz);
     else tiled_setup<double>(c->P, &c->tkz);
+    c->tkz.ter_post = !cfg->use_terrain ? 0 : (c->mixed ? ter_post_kz<float>(c->P) : ter_post_kz<double>(c->P));
     c->lag_parity_per_step = substeps_per_step(c->cfg) & 1;
     // shared-memory tiles of the vertical kernels: TX columns x all levels
     {
@@ -1219,7 +1220,7 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
     if ((rc = pack4(c, S_scratch, 0, nullptr, B.avx, B.avy, B.avz))) return rc;
     // stage state and primitives: those of the preceding slow_rhs_pre
     if (c->P.ter)
-        launch_ter_post<double>(c->P, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.tke,
+        launch_ter_post<double>(c->P, c->stream, c->tkz.ter_post, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.tke,
                                 B.ter, B.avx, B.avy, B.avz, c->vel[1][0], c->vel[1][1], c->vel[1][2]);
     else
     launch_post<double>(c->P, c->tkz, c->stream, slow_dt, OLD, c->S[2], SUM, NEW, B.aux[0], B.aux[1], 0, B.mut, B.tke,

@@ -92,6 +92,7 @@ struct TerBuf {
 constexpr int TTX = 32, TTY = 8;
 struct TiledKz {
     int cell, mom, post;
+    int ter_post;   // the terrain post pass (terrain contexts)
 };
 
 // erf_b200_create's configuration checks (api.cu): ERF_B200_OK or an error code.
@@ -200,8 +201,12 @@ void launch_ter_fast_vert(const Params& P, cudaStream_t st, int tx, size_t smem,
                           const R* cP, const R* cQ, R* avz, double* out_cons, double* out_mz);
 void ter_vert_shape(int nz, int* tx, size_t* smem);
 template <class R>
-void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
-                     StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,
-                     TerBuf<R> T, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn);
+void launch_ter_post(const Params& P, cudaStream_t st, int kz, double slow_dt, StateBuf Sold, StateBuf Sst,
+                     StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
+                     TkeBuf<R> tke, TerBuf<R> T, const R* avx, const R* avy, const R* avz, double* un, double* vn,
+                     double* wn);
+// Levels per block of the tiled terrain post pass (from the occupancy API).
+template <class R>
+int ter_post_kz(const Params& P);
 
 }  // namespace erfb

@@ -28,6 +28,7 @@
 #include <cfloat>
 
 #include "kernels.cuh"
+#include "tiles.cuh"
 
 namespace erfb {
 namespace {
@@ -37,7 +38,7 @@ namespace {
 // natural register counts these kernels are latency-bound at 3-5 blocks.
 #define TER_MINB_SLOW_CELL 4
 #define TER_MINB_STRAIN 8
-#define TER_MINB_POST 8
+#define TER_MINB_POST 4   // the tiled post pass: 256-thread blocks
 #define TER_MINB_SLOW_MOM 8
 #define TER_MINB_STRESS 8
 
@@ -1443,109 +1444,160 @@ __global__ void __launch_bounds__(1024) k_ter_fast_vert(Params P, double dtau, d
 // round trips, w on the ground and the lid from Omega = 0 of the new u, v;
 // the next stage's primitives.
 // ---------------------------------------------------------------------------
-template <class R>
-__global__ void __launch_bounds__(128, TER_MINB_POST) k_ter_post(Params P, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum, StateBuf Snew,
-                           StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* __restrict__ mut,
-                           TkeBuf<R> tke, TerBuf<R> T, const R* __restrict__ avx, const R* __restrict__ avy,
-                           const R* __restrict__ avz, double* __restrict__ un, double* __restrict__ vn,
-                           double* __restrict__ wn) {
+template <class R, int DH, int DV, int MH, int MV, int NS>
+__global__ void __launch_bounds__(TTX * TTY, TER_MINB_POST) k_ter_post(Params P, int kz, double slow_dt, StateBuf Sold,
+                                                                       StateBuf Sst, StateBuf Ssum, StateBuf Snew,
+                                                                       StageAux<R> Acur, StageAux<R> Anext,
+                                                                       int make_next, const R* __restrict__ mut,
+                                                                       TkeBuf<R> tke, TerBuf<R> T,
+                                                                       const R* __restrict__ avx,
+                                                                       const R* __restrict__ avy,
+                                                                       const R* __restrict__ avz, double* __restrict__ un,
+                                                                       double* __restrict__ vn, double* __restrict__ wn) {
+    __shared__ FluxTile<R> sh[NS];
+    __shared__ Plane<R> pl[NS];
     const Geo& g = P.g;
-    int i, j, k;
-    if (!cell_ij(g, i, j, k)) return;
     const int nz = g.nz;
     const int64_t N = g.ncell;
-    int64_t c = cidx(g, i, j, k);
+    const int i = blockIdx.x * TTX + threadIdx.x, j = blockIdx.y * TTY + threadIdx.y;
+    const bool ok = i < g.nx && j < g.ny;
+    const int k0 = blockIdx.z * kz, k1 = min(k0 + kz, g.nz);
     const bool dd = P.les == ERF_LES_DEARDORFF;
-    const double Jc = detJ_at(P, i, j, k);
-    auto AX = [&](int ii) { return double(avx[cidx(g, wrap(ii, g.nx), j, k)]); };
-    auto AY = [&](int jj) { return double(avy[cidx(g, i, wrap(jj, g.ny), k)]); };
-    auto AZ = [&](int kk) { return double(avz[cidx(g, i, j, kk)]); };
     // slow variables: the passive scalar, the moisture species, then (Deardorff) rho*KE
     const int nscal = P.moist ? 1 + (P.ncomp - ERF_RHOQ1_COMP) : 1;
     const int nslow = nscal + (dd ? 1 : 0);
-    for (int q = 0; q < nslow; ++q) {
-        const bool ke = q >= nscal, species = q > 0 && q < nscal;
-        const int n = q == 0 ? ERF_RHOSCALAR_COMP : (ke ? ERF_RHOKE_COMP : ERF_RHOQ1_COMP + q - 1);
-        const R* phi = Acur.prim + (int64_t)(n - 1) * N;
-        auto ph = [&](int ii, int jj, int kk) { return ccw(phi, g, ii, jj, kk); };
-        const int ht = species ? P.moi_h : P.dry_h, vt = species ? P.moi_v : P.dry_v;
-        const double hf = species ? P.f_moi_h : P.f_dry_h, vf = species ? P.f_moi_v : P.f_dry_v;
-        double fxl = AX(i), fxh = AX(i + 1), fyl = AY(j), fyh = AY(j + 1), fzl = AZ(k), fzh = AZ(k + 1);
-        double tx_l = fxl * interp_dir(0, i, j, k, ph, ht, fxl, hf), tx_h = fxh * interp_dir(0, i + 1, j, k, ph, ht, fxh, hf);
-        double ty_l = fyl * interp_dir(1, i, j, k, ph, ht, fyl, hf), ty_h = fyh * interp_dir(1, i, j + 1, k, ph, ht, fyh, hf);
-        double tz_l = fzl * interp_dir(2, i, j, k, ph, vt, fzl, vf), tz_h = fzh * interp_dir(2, i, j, k + 1, ph, vt, fzh, vf);
-        double invdetJ = 1. / Jc;
-        double r = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
-        if (P.use_diff) {
-            // raw x / y fluxes precomputed for the scalar and KE; the species' formed here
-            DiffT<R> D{P, Sst.cons, phi, mut, nullptr, ke ? 0.0 : P.alphaC_eff, ke ? P.invSigmaK : P.invSc,
-                       species ? nullptr : T.fx[ke ? 1 : 0], species ? nullptr : T.fy[ke ? 1 : 0]};
-            double rlo, rhi;
-            r -= D.div(i, j, k, rlo, rhi);
-        }
-        if (ke) {
-            r += P.g_over_theta0 * double(tke.hfz[c]);
-            r += 2.0 * double(mut[c]) * double(tke.smn[c]);
-            r -= double(tke.diss[c]);
-        }
-        double v_ = Sold.cons[n * N + c] + slow_dt * r;
-        Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, species ? 0.0 : 2.220446049250313e-16);
-    }
-    Snew.cons[c] = Ssum.cons[c];
-    Snew.cons[N + c] = Ssum.cons[N + c];
-    if (!dd) Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
-    Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
-    double rho = Ssum.cons[c];
-    // horizontal momenta through the two round trips; velocity u2
-    auto u2f = [&](int ii, int jj, int kk) {
-        if (kk < 0 || kk >= nz) {
-            if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
-            kk = kk < 0 ? 0 : nz - 1;
-        }
-        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
-        int64_t e = cidx(g, ii, jj, kk);
-        double rs = Ssum.cons[e] + Ssum.cons[cidx(g, wrap(ii - 1, g.nx), jj, kk)];
-        double m = Ssum.mx[e];
-        double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
-        return (m * 2.0) / rs;
+    R zl[NS], zh[NS];
+    double dz_lo[NS];   // diffusive z flux through the cell's bottom face, carried up the column
+#pragma unroll
+    for (int q = 0; q < NS; ++q) { zl[q] = zh[q] = R(0); dz_lo[q] = 0.0; }
+    const TileEdge edge = tile_edge(g);
+    auto comp_of = [&](int q) {
+        return q == 0 ? ERF_RHOSCALAR_COMP : (q < nscal ? ERF_RHOQ1_COMP + q - 1 : ERF_RHOKE_COMP);
     };
-    auto v2f = [&](int ii, int jj, int kk) {
-        if (kk < 0 || kk >= nz) {
-            if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
-            kk = kk < 0 ? 0 : nz - 1;
+    auto slow_phi = [&](int q) { return Acur.prim + (int64_t)(comp_of(q) - 1) * N; };
+#pragma unroll
+    for (int q = 0; q < NS; ++q)
+        if (q < nslow) load_plane(g, pl[q], slow_phi(q), k0);
+    for (int k = k0; k < k1; ++k) {
+        plane_wait();
+        __syncthreads();
+        // advective fluxes with the average (area-weighted, contravariant) momenta
+        if (ok) {
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                if (q >= nslow) break;
+                if (q == 0 || q >= nscal)
+                    tile_put<DH, DV>(g, sh[q], pl[q], slow_phi(q), avx, avy, avz, P.dry_h, P.dry_v, R(P.f_dry_h),
+                                     R(P.f_dry_v), i, j, k, k == k0, zl[q], zh[q]);
+                else
+                    tile_put<MH, MV>(g, sh[q], pl[q], slow_phi(q), avx, avy, avz, P.moi_h, P.moi_v, R(P.f_moi_h),
+                                     R(P.f_moi_v), i, j, k, k == k0, zl[q], zh[q]);
+            }
         }
-        ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
-        int64_t e = cidx(g, ii, jj, kk);
-        double rs = Ssum.cons[e] + Ssum.cons[cidx(g, ii, wrap(jj - 1, g.ny), kk)];
-        double m = Ssum.my[e];
-        double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
-        return (m * 2.0) / rs;
-    };
-    {
-        double rs = rho + Ssum.cons[cidx(g, wrap(i - 1, g.nx), j, k)];
-        double u2 = u2f(i, j, k);
-        Snew.mx[c] = (u2 * 0.5) * rs; un[c] = u2;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            if (q >= nslow) break;
+            if (q == 0 || q >= nscal)
+                tile_put_edge<DH>(g, edge, sh[q], pl[q], avx, avy, P.dry_h, R(P.f_dry_h), k);
+            else
+                tile_put_edge<MH>(g, edge, sh[q], pl[q], avx, avy, P.moi_h, R(P.f_moi_h), k);
+        }
+        __syncthreads();
+        if (k + 1 < k1) {   // next level's planes arrive during the update below
+#pragma unroll
+            for (int q = 0; q < NS; ++q)
+                if (q < nslow) load_plane(g, pl[q], slow_phi(q), k + 1);
+        }
+        if (!ok) continue;   // the next level's first barrier orders the reuse of sh
+        const int64_t c = cidx(g, i, j, k);
+        const double invdetJ = 1. / detJ_at(P, i, j, k);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            if (q >= nslow) break;
+            const bool ke = q >= nscal, species = q > 0 && q < nscal;
+            const int n = comp_of(q);
+            // -div over detJ; (-S) invdetJ equals the reference's -invdetJ S bit for bit
+            double r = double(tile_div(g, sh[q], zl[q], zh[q])) * invdetJ;
+            zl[q] = zh[q];
+            if (P.use_diff) {
+                // DiffT::div with the z-face flux carried from the level below:
+                // raw x / y fluxes precomputed for the scalar and KE, the species' formed here
+                const R* phi = slow_phi(q);
+                DiffT<R> D{P, Sst.cons, phi, mut, nullptr, ke ? 0.0 : P.alphaC_eff, ke ? P.invSigmaK : P.invSc,
+                           species ? nullptr : T.fx[ke ? 1 : 0], species ? nullptr : T.fy[ke ? 1 : 0]};
+                double raw;
+                double fxl = D.xr(i, j, k) * hzeta_I(P, i, j, k), fxh = D.xr(i + 1, j, k) * hzeta_I(P, i + 1, j, k);
+                double fyl = D.yr(i, j, k) * hzeta_J(P, i, j, k), fyh = D.yr(i, j + 1, k) * hzeta_J(P, i, j + 1, k);
+                double fzl = (k == k0) ? D.zflux(i, j, k, raw) : dz_lo[q];
+                double fzh = D.zflux(i, j, k + 1, raw);
+                dz_lo[q] = fzh;
+                double sd = (fxh - fxl) * g.dxi * 1.0 + (fyh - fyl) * g.dyi * 1.0 + (fzh - fzl) * g.dzi;
+                r -= sd / detJ_at(P, i, j, k);
+            }
+            if (ke) {
+                r += P.g_over_theta0 * double(tke.hfz[c]);
+                r += 2.0 * double(mut[c]) * double(tke.smn[c]);
+                r -= double(tke.diss[c]);
+            }
+            double v_ = Sold.cons[n * N + c] + slow_dt * r;
+            Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, species ? 0.0 : 2.220446049250313e-16);
+        }
+        Snew.cons[c] = Ssum.cons[c];
+        Snew.cons[N + c] = Ssum.cons[N + c];
+        if (!dd) Snew.cons[2 * N + c] = Sst.cons[2 * N + c];
+        Snew.cons[3 * N + c] = Sst.cons[3 * N + c];
+        double rho = Ssum.cons[c];
+        // horizontal momenta through the two round trips; velocity u2
+        auto u2f = [&](int ii, int jj, int kk) {
+            if (kk < 0 || kk >= nz) {
+                if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
+                kk = kk < 0 ? 0 : nz - 1;
+            }
+            ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+            int64_t e = cidx(g, ii, jj, kk);
+            double rs = Ssum.cons[e] + Ssum.cons[cidx(g, wrap(ii - 1, g.nx), jj, kk)];
+            double m = Ssum.mx[e];
+            double u1 = (m * 2.0) / rs; m = (u1 * 0.5) * rs;
+            return (m * 2.0) / rs;
+        };
+        auto v2f = [&](int ii, int jj, int kk) {
+            if (kk < 0 || kk >= nz) {
+                if ((kk < 0 && g.zlo_noslip) || (kk >= nz && g.zhi_noslip)) return 0.0;
+                kk = kk < 0 ? 0 : nz - 1;
+            }
+            ii = wrap(ii, g.nx); jj = wrap(jj, g.ny);
+            int64_t e = cidx(g, ii, jj, kk);
+            double rs = Ssum.cons[e] + Ssum.cons[cidx(g, ii, wrap(jj - 1, g.ny), kk)];
+            double m = Ssum.my[e];
+            double v1 = (m * 2.0) / rs; m = (v1 * 0.5) * rs;
+            return (m * 2.0) / rs;
+        };
+        {
+            double rs = rho + Ssum.cons[cidx(g, wrap(i - 1, g.nx), j, k)];
+            double u2 = u2f(i, j, k);
+            Snew.mx[c] = (u2 * 0.5) * rs; un[c] = u2;
+        }
+        {
+            double rs = rho + Ssum.cons[cidx(g, i, wrap(j - 1, g.ny), k)];
+            double v2 = v2f(i, j, k);
+            Snew.my[c] = (v2 * 0.5) * rs; vn[c] = v2;
+        }
+        if (k == 0) {
+            double wb = w_from_omega(P, i, j, 0, 0.0, u2f, v2f);
+            Snew.mz[c] = (wb * 0.5) * (rho + rho); wn[c] = wb;
+        } else {
+            double rs = rho + Ssum.cons[c - g.sk];
+            double m = Ssum.mz[c];
+            double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
+            double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
+            Snew.mz[c] = m; wn[c] = w2;
+        }
+        if (k == nz - 1) {
+            double wt = w_from_omega(P, i, j, nz, 0.0, u2f, v2f);
+            Snew.mz[c + g.sk] = (wt * 0.5) * (rho + rho); wn[c + g.sk] = wt;
+        }
+        if (make_next) stage_aux_ter<R>(P, Snew.cons, Anext, c, k);
     }
-    {
-        double rs = rho + Ssum.cons[cidx(g, i, wrap(j - 1, g.ny), k)];
-        double v2 = v2f(i, j, k);
-        Snew.my[c] = (v2 * 0.5) * rs; vn[c] = v2;
-    }
-    if (k == 0) {
-        double wb = w_from_omega(P, i, j, 0, 0.0, u2f, v2f);
-        Snew.mz[c] = (wb * 0.5) * (rho + rho); wn[c] = wb;
-    } else {
-        double rs = rho + Ssum.cons[c - g.sk];
-        double m = Ssum.mz[c];
-        double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
-        double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
-        Snew.mz[c] = m; wn[c] = w2;
-    }
-    if (k == nz - 1) {
-        double wt = w_from_omega(P, i, j, nz, 0.0, u2f, v2f);
-        Snew.mz[c + g.sk] = (wt * 0.5) * (rho + rho); wn[c + g.sk] = wt;
-    }
-    if (make_next) stage_aux_ter<R>(P, Snew.cons, Anext, c, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -1615,10 +1667,29 @@ void ter_vert_shape(int nz, int* tx, size_t* smem) {
         cudaFuncSetAttribute(k_ter_fast_vert<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     }
 }
+namespace {
+// The tiled post pass per scheme: dry scalars (and KE) and moisture
+// species compile-time Upwind5 / WENO5 where the configuration has them,
+// the run-time dispatch otherwise; NS = 2 holds the scalar and KE of a dry
+// state, 5 the scalar, three species and KE.
 template <class R>
-void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, StateBuf Sst, StateBuf Ssum,
-                     StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut, TkeBuf<R> tke,
-                     TerBuf<R> T, const R* avx, const R* avy, const R* avz, double* un, double* vn, double* wn) {
+using TerPostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, StateBuf, StageAux<R>, StageAux<R>, int,
+                          const R*, TkeBuf<R>, TerBuf<R>, const R*, const R*, const R*, double*, double*, double*);
+constexpr int TU5 = ERF_ADV_UPWIND_5TH, TW5 = ERF_ADV_WENO_5;
+template <class R>
+TerPostK<R> ter_post_kernel(const Params& P) {
+    const bool du = P.dry_h == TU5 && P.dry_v == TU5, mw = P.moi_h == TW5 && P.moi_v == TW5;
+    if (!P.moist) return du ? k_ter_post<R, TU5, TU5, -1, -1, 2> : k_ter_post<R, -1, -1, -1, -1, 2>;
+    if (du && mw) return k_ter_post<R, TU5, TU5, TW5, TW5, 5>;
+    return k_ter_post<R, -1, -1, -1, -1, 5>;
+}
+}  // namespace
+
+template <class R>
+void launch_ter_post(const Params& P, cudaStream_t st, int kz, double slow_dt, StateBuf Sold, StateBuf Sst,
+                     StateBuf Ssum, StateBuf Snew, StageAux<R> Acur, StageAux<R> Anext, int make_next, const R* mut,
+                     TkeBuf<R> tke, TerBuf<R> T, const R* avx, const R* avy, const R* avz, double* un, double* vn,
+                     double* wn) {
     if (P.use_diff) {
         const int64_t N = P.g.ncell;
         const bool dd = P.les == ERF_LES_DEARDORFF;
@@ -1627,8 +1698,13 @@ void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf 
             T.fy[0], dd ? Acur.prim + (int64_t)(ERF_RHOKE_COMP - 1) * N : nullptr, 0.0, P.invSigmaK, T.fx[1],
             T.fy[1]);
     }
-    k_ter_post<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, slow_dt, Sold, Sst, Ssum, Snew, Acur, Anext,
-                                                                 make_next, mut, tke, T, avx, avy, avz, un, vn, wn);
+    ter_post_kernel<R>(P)<<<tile_grid(P.g, kz), dim3(TTX, TTY, 1), 0, st>>>(P, kz, slow_dt, Sold, Sst, Ssum, Snew,
+                                                                            Acur, Anext, make_next, mut, tke, T, avx,
+                                                                            avy, avz, un, vn, wn);
+}
+template <class R>
+int ter_post_kz(const Params& P) {
+    return pick_kz(ter_post_kernel<R>(P), P.g);
 }
 
 #define ERFB_TER_INSTANTIATE(R)                                                                                     \
@@ -1648,9 +1724,10 @@ void launch_ter_post(const Params& P, cudaStream_t st, double slow_dt, StateBuf 
     template void launch_ter_fast_vert<R>(const Params&, cudaStream_t, int, size_t, double, double, double, double, \
                                           StateBuf, int, StateBuf, StageAux<R>, const R*, const R*, TerBuf<R>,       \
                                           const R*, const R*, const R*, const R*, const R*, R*, double*, double*);   \
-    template void launch_ter_post<R>(const Params&, cudaStream_t, double, StateBuf, StateBuf, StateBuf, StateBuf,    \
-                                     StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, TerBuf<R>, const R*,        \
-                                     const R*, const R*, double*, double*, double*);
+    template void launch_ter_post<R>(const Params&, cudaStream_t, int, double, StateBuf, StateBuf, StateBuf,         \
+                                     StateBuf, StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, TerBuf<R>,        \
+                                     const R*, const R*, const R*, double*, double*, double*);                       \
+    template int ter_post_kz<R>(const Params&);
 
 ERFB_TER_INSTANTIATE(double)
 ERFB_TER_INSTANTIATE(float)
