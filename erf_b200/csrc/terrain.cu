@@ -41,6 +41,7 @@ namespace {
 #define TER_MINB_POST 4   // the tiled post pass: 256-thread blocks
 #define TER_MINB_SLOW_MOM 8
 #define TER_MINB_STRESS 8
+constexpr int TU5 = ERF_ADV_UPWIND_5TH, TW5 = ERF_ADV_WENO_5;   // compile-time scheme codes
 
 // ---------------------------------------------------------------------------
 // Metric terms (Utils/ERF_TerrainMetrics.H:33-395), same operand order.
@@ -848,19 +849,20 @@ __device__ __forceinline__ double omega_mom(const Params& P, StateBuf S, const d
     return omega_from_w(P, i, j, k, rw, MX, MY);
 }
 
-// Face interpolation of a cell field along x / y / z with run-time scheme
-// (the stencil's unused entries are zero); upw the advecting flux.
-template <class FP>
+// Face interpolation of a cell field along x / y / z (the stencil's unused
+// entries are zero); upw the advecting flux.  TS >= 0 fixes the scheme at
+// compile time, TS < 0 takes it from `type` at run time (same arithmetic).
+template <int TS, class FP>
 __device__ __forceinline__ double interp_dir(int dir, int i, int j, int k, FP phi, int type, double upw, double frac) {
     double s[6];
-    const int w = stencil_width(type);
+    const int w = width_of<TS>(type);
 #pragma unroll
     for (int m = 0; m < 6; ++m) {
         int off = m - 3;
         bool used = (off >= -w && off <= w - 1);
         s[m] = used ? phi(i + (dir == 0 ? off : 0), j + (dir == 1 ? off : 0), k + (dir == 2 ? off : 0)) : 0.0;
     }
-    return interp_rt<double>(type, s, upw, frac);
+    return interp_of<TS, double>(type, s, upw, frac);
 }
 }  // namespace
 
@@ -895,7 +897,7 @@ __global__ void k_ter_rawflux(Params P, const double* __restrict__ rho, const R*
 // ay likewise, az = 1) over detJ, the average momenta, theta advection with
 // the dycore scheme, DiffusionSrcForState_T and hfx_z.
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, int HT, int VT>
 __global__ void __launch_bounds__(128, TER_MINB_SLOW_CELL) k_ter_slow_cell(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
                                 const double* __restrict__ v, const R* __restrict__ mut, TkeBuf<R> tke, TerBuf<R> T,
                                 R* __restrict__ Fcons, R* __restrict__ avx, R* __restrict__ avy, R* __restrict__ avz) {
@@ -922,9 +924,9 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_CELL) k_ter_slow_cell(Param
     auto th = [&](int ii, int jj, int kk) { return ccw(A.prim, g, ii, jj, kk); };
     const int ht = P.dyc_h, vt = P.dyc_v;
     const double hf = P.f_dyc_h, vf = P.f_dyc_v;
-    double tx_l = fxl * interp_dir(0, i, j, k, th, ht, fxl, hf), tx_h = fxh * interp_dir(0, i + 1, j, k, th, ht, fxh, hf);
-    double ty_l = fyl * interp_dir(1, i, j, k, th, ht, fyl, hf), ty_h = fyh * interp_dir(1, i, j + 1, k, th, ht, fyh, hf);
-    double tz_l = fzl * interp_dir(2, i, j, k, th, vt, fzl, vf), tz_h = fzh * interp_dir(2, i, j, k + 1, th, vt, fzh, vf);
+    double tx_l = fxl * interp_dir<HT>(0, i, j, k, th, ht, fxl, hf), tx_h = fxh * interp_dir<HT>(0, i + 1, j, k, th, ht, fxh, hf);
+    double ty_l = fyl * interp_dir<HT>(1, i, j, k, th, ht, fyl, hf), ty_h = fyh * interp_dir<HT>(1, i, j + 1, k, th, ht, fyh, hf);
+    double tz_l = fzl * interp_dir<VT>(2, i, j, k, th, vt, fzl, vf), tz_h = fzh * interp_dir<VT>(2, i, j, k + 1, th, vt, fzh, vf);
     double invdetJ = 1. / Jc;
     double frt = -invdetJ * 1.0 * ((tx_h - tx_l) * g.dxi + (ty_h - ty_l) * g.dyi + (tz_h - tz_l) * g.dzi);
     if (P.use_diff) {
@@ -950,7 +952,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_CELL) k_ter_slow_cell(Param
 // and (k >= 1) z faces at (i,j,k).  Omega is the stage's, left in avz by
 // k_ter_slow_cell.
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, int HT, int VT>
 __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params P, StateBuf S, StageAux<R> A, const double* __restrict__ u,
                                const double* __restrict__ v, const double* __restrict__ w, const R* __restrict__ t11,
                                const R* __restrict__ t22, const R* __restrict__ t33, const R* __restrict__ t12,
@@ -991,12 +993,12 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             src = -src / (0.5 * (Jt(i, j, k) + Jt(i - 1, j, k)));
         } else {
             double a, xh, xl, yh, yl, zh, zl;
-            a = 0.5 * (RU(i + 1, j, k) * 1.0 + RU(i, j, k) * 1.0); xh = a * interp_dir(0, i + 1, j, k, U, ht, a, hf) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i + 1, j, k));
-            a = 0.5 * (RU(i - 1, j, k) * 1.0 + RU(i, j, k) * 1.0); xl = a * interp_dir(0, i, j, k, U, ht, a, hf) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i - 1, j, k));
-            a = 0.5 * (RV(i, j + 1, k) * 1.0 + RV(i - 1, j + 1, k) * 1.0); yh = a * interp_dir(1, i, j + 1, k, U, ht, a, hf) * hzeta_EK(P, i, j + 1, k);
-            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i - 1, j, k) * 1.0); yl = a * interp_dir(1, i, j, k, U, ht, a, hf) * hzeta_EK(P, i, j, k);
-            a = 0.5 * (Om(i, j, k + 1) + Om(i - 1, j, k + 1)) * 0.5 * (az + az); zh = a * interp_dir(2, i, j, k + 1, U, vt, a, vf);
-            a = 0.5 * (Om(i, j, k) + Om(i - 1, j, k)) * 0.5 * (az + az); zl = a * interp_dir(2, i, j, k, U, vt, a, vf);
+            a = 0.5 * (RU(i + 1, j, k) * 1.0 + RU(i, j, k) * 1.0); xh = a * interp_dir<HT>(0, i + 1, j, k, U, ht, a, hf) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i + 1, j, k));
+            a = 0.5 * (RU(i - 1, j, k) * 1.0 + RU(i, j, k) * 1.0); xl = a * interp_dir<HT>(0, i, j, k, U, ht, a, hf) * 0.5 * (hzeta_I(P, i, j, k) + hzeta_I(P, i - 1, j, k));
+            a = 0.5 * (RV(i, j + 1, k) * 1.0 + RV(i - 1, j + 1, k) * 1.0); yh = a * interp_dir<HT>(1, i, j + 1, k, U, ht, a, hf) * hzeta_EK(P, i, j + 1, k);
+            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i - 1, j, k) * 1.0); yl = a * interp_dir<HT>(1, i, j, k, U, ht, a, hf) * hzeta_EK(P, i, j, k);
+            a = 0.5 * (Om(i, j, k + 1) + Om(i - 1, j, k + 1)) * 0.5 * (az + az); zh = a * interp_dir<VT>(2, i, j, k + 1, U, vt, a, vf);
+            a = 0.5 * (Om(i, j, k) + Om(i - 1, j, k)) * 0.5 * (az + az); zl = a * interp_dir<VT>(2, i, j, k, U, vt, a, vf);
             src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
             src /= 0.5 * (Jt(i, j, k) + Jt(i - 1, j, k));
             src = -src;
@@ -1042,12 +1044,12 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             src = -src / (0.5 * (Jt(i, j, k) + Jt(i, j - 1, k)));
         } else {
             double a, xh, xl, yh, yl, zh, zl;
-            a = 0.5 * (RU(i + 1, j, k) * 1.0 + RU(i + 1, j - 1, k) * 1.0); xh = a * interp_dir(0, i + 1, j, k, V, ht, a, hf) * hzeta_EK(P, i + 1, j, k);
-            a = 0.5 * (RU(i, j, k) * 1.0 + RU(i, j - 1, k) * 1.0); xl = a * interp_dir(0, i, j, k, V, ht, a, hf) * hzeta_EK(P, i, j, k);
-            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i, j + 1, k) * 1.0); yh = a * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j + 1, k)) * interp_dir(1, i, j + 1, k, V, ht, a, hf);
-            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i, j - 1, k) * 1.0); yl = a * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j - 1, k)) * interp_dir(1, i, j, k, V, ht, a, hf);
-            a = 0.5 * (Om(i, j, k + 1) + Om(i, j - 1, k + 1)) * 0.5 * (az + az); zh = a * interp_dir(2, i, j, k + 1, V, vt, a, vf);
-            a = 0.5 * (Om(i, j, k) + Om(i, j - 1, k)) * 0.5 * (az + az); zl = a * interp_dir(2, i, j, k, V, vt, a, vf);
+            a = 0.5 * (RU(i + 1, j, k) * 1.0 + RU(i + 1, j - 1, k) * 1.0); xh = a * interp_dir<HT>(0, i + 1, j, k, V, ht, a, hf) * hzeta_EK(P, i + 1, j, k);
+            a = 0.5 * (RU(i, j, k) * 1.0 + RU(i, j - 1, k) * 1.0); xl = a * interp_dir<HT>(0, i, j, k, V, ht, a, hf) * hzeta_EK(P, i, j, k);
+            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i, j + 1, k) * 1.0); yh = a * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j + 1, k)) * interp_dir<HT>(1, i, j + 1, k, V, ht, a, hf);
+            a = 0.5 * (RV(i, j, k) * 1.0 + RV(i, j - 1, k) * 1.0); yl = a * 0.5 * (hzeta_J(P, i, j, k) + hzeta_J(P, i, j - 1, k)) * interp_dir<HT>(1, i, j, k, V, ht, a, hf);
+            a = 0.5 * (Om(i, j, k + 1) + Om(i, j - 1, k + 1)) * 0.5 * (az + az); zh = a * interp_dir<VT>(2, i, j, k + 1, V, vt, a, vf);
+            a = 0.5 * (Om(i, j, k) + Om(i, j - 1, k)) * 0.5 * (az + az); zl = a * interp_dir<VT>(2, i, j, k, V, vt, a, vf);
             src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
             src /= 0.5 * (Jt(i, j, k) + Jt(i, j - 1, k));
             src = -src;
@@ -1099,10 +1101,10 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             src = -src / (0.5 * (Jt(i, j, k) + Jt(i, j, k - 1)));
         } else {
             double a, xh, xl, yh, yl, zh, zl;
-            a = 0.5 * (RU(i + 1, j, k) + RU(i + 1, j, k - 1)) * 1.0; xh = a * interp_dir(0, i + 1, j, k, W, ht, a, hf) * hzeta_EJ(P, i + 1, j, k);
-            a = 0.5 * (RU(i, j, k) + RU(i, j, k - 1)) * 1.0; xl = a * interp_dir(0, i, j, k, W, ht, a, hf) * hzeta_EJ(P, i, j, k);
-            a = 0.5 * (RV(i, j + 1, k) + RV(i, j + 1, k - 1)) * 1.0; yh = a * interp_dir(1, i, j + 1, k, W, ht, a, hf) * hzeta_EI(P, i, j + 1, k);
-            a = 0.5 * (RV(i, j, k) + RV(i, j, k - 1)) * 1.0; yl = a * interp_dir(1, i, j, k, W, ht, a, hf) * hzeta_EI(P, i, j, k);
+            a = 0.5 * (RU(i + 1, j, k) + RU(i + 1, j, k - 1)) * 1.0; xh = a * interp_dir<HT>(0, i + 1, j, k, W, ht, a, hf) * hzeta_EJ(P, i + 1, j, k);
+            a = 0.5 * (RU(i, j, k) + RU(i, j, k - 1)) * 1.0; xl = a * interp_dir<HT>(0, i, j, k, W, ht, a, hf) * hzeta_EJ(P, i, j, k);
+            a = 0.5 * (RV(i, j + 1, k) + RV(i, j + 1, k - 1)) * 1.0; yh = a * interp_dir<HT>(1, i, j + 1, k, W, ht, a, hf) * hzeta_EI(P, i, j + 1, k);
+            a = 0.5 * (RV(i, j, k) + RV(i, j, k - 1)) * 1.0; yl = a * interp_dir<HT>(1, i, j, k, W, ht, a, hf) * hzeta_EI(P, i, j, k);
             auto iZall = [&](int kk, double upw, double frac, int type) {
                 int gt = (type == ERF_ADV_UPWIND_5TH || type == ERF_ADV_CENTERED_6TH) ? ERF_ADV_UPWIND_5TH
                          : (type == ERF_ADV_CENTERED_2ND ? ERF_ADV_CENTERED_2ND : ERF_ADV_UPWIND_3RD);
@@ -1120,14 +1122,14 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
             else if (k == hi_z_face - 2 || k == lo_z_face + 1) {
                 if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) ih = iZall(k + 1, Oh, 0, ERF_ADV_CENTERED_4TH);
                 else ih = iZall(k + 1, Oh, vf, vt);
-            } else ih = interp_dir(2, i, j, k + 1, W, vt, Oh, vf);
+            } else ih = interp_dir<VT>(2, i, j, k + 1, W, vt, Oh, vf);
             zh = Oh * ih;
             double Ol = 0.25 * (Om(i, j, k) + Om(i, j, k - 1)) * (az + az);
             if (k == lo_z_face + 1) il = iZall(k, Ol, 0, ERF_ADV_CENTERED_2ND);
             else if (k == lo_z_face + 2 || k == hi_z_face - 1) {
                 if (vt != ERF_ADV_CENTERED_2ND && vt != ERF_ADV_UPWIND_3RD) il = iZall(k, Ol, 0, ERF_ADV_CENTERED_4TH);
                 else il = iZall(k, Ol, vf, vt);
-            } else il = interp_dir(2, i, j, k, W, vt, Ol, vf);
+            } else il = interp_dir<VT>(2, i, j, k, W, vt, Ol, vf);
             zl = Ol * il;
             src = (xh - xl) * dxi * 1.0 + (yh - yl) * dyi * 1.0 + (zh - zl) * dzi;
             double denom = 0.5 * (Jt(i, j, k) + Jt(i, j, k - 1));
@@ -1624,15 +1626,17 @@ void launch_ter_slow_cell(const Params& P, cudaStream_t st, StateBuf S, StageAux
         k_ter_rawflux<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S.cons, mut, A.prim, P.alphaT_eff, P.invPr,
                                                                         T.fx[0], T.fy[0], nullptr, 0.0, 0.0, nullptr,
                                                                         nullptr);
-    k_ter_slow_cell<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S, A, u, v, mut, tke, T, Fcons, avx, avy,
-                                                                      avz);
+    const bool u5 = P.dyc_h == TU5 && P.dyc_v == TU5;
+    (u5 ? k_ter_slow_cell<R, TU5, TU5> : k_ter_slow_cell<R, -1, -1>)<<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(
+        P, S, A, u, v, mut, tke, T, Fcons, avx, avy, avz);
 }
 template <class R>
 void launch_ter_slow_mom(const Params& P, cudaStream_t st, StateBuf S, StageAux<R> A, const double* u,
                          const double* v, const double* w, const R* t11, const R* t22, const R* t33, const R* t12,
                          const R* t13, const R* t23, TerBuf<R> T, const R* Om, R* Fmx, R* Fmy, R* Fmz) {
-    k_ter_slow_mom<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, S, A, u, v, w, t11, t22, t33, t12, t13, t23, T,
-                                                                     Om, Fmx, Fmy, Fmz);
+    const bool u5 = P.dyc_h == TU5 && P.dyc_v == TU5;
+    (u5 ? k_ter_slow_mom<R, TU5, TU5> : k_ter_slow_mom<R, -1, -1>)<<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(
+        P, S, A, u, v, w, t11, t22, t33, t12, t13, t23, T, Om, Fmx, Fmy, Fmz);
 }
 template <class R>
 void launch_ter_fast_h(const Params& P, cudaStream_t st, int step, double dtau, double facinv, StateBuf Sprev,
@@ -1675,7 +1679,6 @@ namespace {
 template <class R>
 using TerPostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, StateBuf, StageAux<R>, StageAux<R>, int,
                           const R*, TkeBuf<R>, TerBuf<R>, const R*, const R*, const R*, double*, double*, double*);
-constexpr int TU5 = ERF_ADV_UPWIND_5TH, TW5 = ERF_ADV_WENO_5;
 template <class R>
 TerPostK<R> ter_post_kernel(const Params& P) {
     const bool du = P.dry_h == TU5 && P.dry_v == TU5, mw = P.moi_h == TW5 && P.moi_v == TW5;
