@@ -11,7 +11,9 @@
 //              network forward on the tensor cores (mlp::forward_cta) and
 //              writes rho * (deviatoric stress, heat flux).  Cells outside
 //              the envelope get the Smagorinsky stress and heat flux
-//              (nu_t = (Cs Delta)^2 |S|, Pr_t) instead.
+//              (nu_t = (Cs Delta)^2 |S|, Pr_t) instead, and cells within
+//              ENV_MARGIN of its edge a linear blend of the two, so that
+//              the closure is continuous in the state.
 //   k_closure_edges  averages the cell-centred off-diagonal stresses to the
 //              xy / xz / yz edges where the momentum divergence reads them.
 //
@@ -29,6 +31,10 @@
 namespace erfb {
 
 using namespace erfb::mlp;
+
+// Share of each feature's training range, at either end, across which the
+// network hands over to Smagorinsky.
+constexpr float ENV_MARGIN = 0.05f;
 
 template <class R>
 __device__ __forceinline__ void closure_features(const Geo& g, const double* __restrict__ u,
@@ -113,14 +119,22 @@ __global__ void __launch_bounds__(ROWS) k_closure(Params P, ClosureNet net, cons
         const bool live = c < g.ncell;
         float f[NIN], xn[NIN];
         bool fb = !live;
+        // weight of the network: 1 well inside the training envelope, falling
+        // linearly to 0 across the outer ENV_MARGIN of each feature's range,
+        // so that the closure is continuous where it hands over to Smagorinsky
+        float wgt = 1.0f;
         if (live) {
             int k = (int)(c / g.sk), rem = (int)(c - (int64_t)k * g.sk);
             int j = rem / g.nx, i = rem - j * g.nx;
             closure_features<R>(g, u, v, w, theta, delta, i, j, k, f);
             for (int q = 0; q < NIN; ++q) {
-                fb = fb || !(f[q] >= sE[q] && f[q] <= sE[NIN + q]);
+                const float lo = sE[q], hi = sE[NIN + q], m = ENV_MARGIN * (hi - lo);
+                const float d = fminf(f[q] - lo, hi - f[q]);
+                if (m > 0.0f) wgt = fminf(wgt, fmaxf(0.0f, fminf(1.0f, d / m)));
+                else if (!(d >= 0.0f)) wgt = 0.0f;
                 xn[q] = (f[q] - sN[q]) / sN[NIN + q];
             }
+            fb = !(wgt > 0.0f);
         }
         if (fb)
             for (int q = 0; q < NIN; ++q) xn[q] = 0.0f;
@@ -133,6 +147,11 @@ __global__ void __launch_bounds__(ROWS) k_closure(Params P, ClosureNet net, cons
             ++nfb;
         } else {
             for (int q = 0; q < NOUT; ++q) o[q] = y[q] * sN[2 * NIN + NOUT + q] + sN[2 * NIN + q];
+            if (wgt < 1.0f) {
+                float os[NOUT];
+                smagorinsky_closure(f, csd2, invPr, os);
+                for (int q = 0; q < NOUT; ++q) o[q] = wgt * o[q] + (1.0f - wgt) * os[q];
+            }
         }
         const R rho = R(cons[c]);
         t11[c] = rho * R(o[0]); t22[c] = rho * R(o[1]); t33[c] = rho * R(o[2]);
