@@ -353,7 +353,7 @@ def main(argv=None):
     import argparse
     import time
     ap = argparse.ArgumentParser()
-    ap.add_argument("--fine", type=int, nargs=3, default=[256, 256, 64])
+    ap.add_argument("--fine", type=int, nargs=3, default=[512, 512, 128])
     ap.add_argument("--factor", type=int, default=4)
     ap.add_argument("--spinup", type=int, default=400)
     ap.add_argument("--snapshots", type=int, default=4)
