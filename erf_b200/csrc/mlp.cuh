@@ -44,6 +44,19 @@ __device__ __forceinline__ float gelu(float z) {
     const float h = 0.5f * z;
     return fmaf(h, t, h);
 }
+// Bias plus GELU of two values with the paired FP32 instructions of sm_100
+// (one instruction per operation for both lanes, each lane rounded as the
+// scalar operation above, so the values are the same as gelu(z + b)).
+__device__ __forceinline__ float2 bias_gelu2(float2 z, float2 b) {
+    const float2 CA = make_float2(GELU_C * GELU_A, GELU_C * GELU_A), C = make_float2(GELU_C, GELU_C);
+    const float2 half = make_float2(0.5f, 0.5f);
+    z = __fadd2_rn(z, b);
+    const float2 u = __fmul2_rn(z, z);
+    const float2 a = __fmul2_rn(z, __ffma2_rn(CA, u, C));
+    const float2 t = make_float2(tanh_fast(a.x), tanh_fast(a.y));
+    const float2 h = __fmul2_rn(half, z);
+    return __ffma2_rn(h, t, h);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
     float t = tanh_fast(GELU_C * (z + GELU_A * z * z * z));
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * GELU_C * (1.0f + 3.0f * GELU_A * z * z);
@@ -84,7 +97,11 @@ __device__ __forceinline__ bool forward_cta(const unsigned char* sW, unsigned ch
         const float* b = sB + layer * HID;
         if (layer < 3) {
 #pragma unroll
-            for (int q = 0; q < HID; ++q) z[q] = gelu(z[q] + b[q]);
+            for (int q = 0; q < HID; q += 2) {
+                const float2 r = bias_gelu2(make_float2(z[q], z[q + 1]), make_float2(b[q], b[q + 1]));
+                z[q] = r.x;
+                z[q + 1] = r.y;
+            }
             put_row(sH, HID, t, z, HID);
         } else {
             for (int q = 0; q < NOUTP; ++q) y[q] = z[q] + b[q];
