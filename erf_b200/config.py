@@ -25,6 +25,7 @@ MOIST_NONE, MOIST_KESSLER, MOIST_KESSLER_NORAIN = 0, 1, 2
 BC_NO_SLIP_WALL, BC_SLIP_WALL, BC_PERIODIC, BC_MOST = 5, 6, 7, 8
 PREC_FP64, PREC_MIXED = 0, 1
 SUBSTEP_IMPLICIT, SUBSTEP_NONE = 0, 1
+TERRAIN_STATIC, TERRAIN_MOVING = 0, 1
 # conserved components (Source/ERF_IndexDefines.H:36-43)
 RHO_COMP, RHOTHETA_COMP, RHOKE_COMP, RHOQKE_COMP, RHOSCALAR_COMP, RHOQ1_COMP = 0, 1, 2, 3, 4, 5
 
@@ -60,8 +61,10 @@ class ErfConfig(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("use_terrain", ctypes.c_int),
         ("substepping_type", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("terrain_type", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
         ("most_z0", ctypes.c_double), ("most_zref", ctypes.c_double),
+        ("mt_ampl", ctypes.c_double), ("mt_wavelength", ctypes.c_double),
     ]
 
     def copy(self) -> "ErfConfig":
@@ -123,6 +126,8 @@ def defaults() -> ErfConfig:
     c.precision = PREC_FP64
     c.most_z0 = 0.1      # ABLMost z0_const
     c.most_zref = 0.0    # 0: half the lowest cell (MOSTAverage's default)
+    c.terrain_type = TERRAIN_STATIC
+    c.mt_ampl, c.mt_wavelength = 0.0, 100.0
     return c
 
 
@@ -168,6 +173,13 @@ def from_inputs(keys: dict) -> ErfConfig:
             c.mri_ratio = int(g(k))
     if g("buoyancy_type") is not None:
         c.buoyancy_type = int(g("buoyancy_type"))
+    if g("use_terrain") is not None:
+        c.use_terrain = 1 if str(g("use_terrain")).lower() in ("1", "true") else 0
+    tt = g("terrain_type")
+    if tt is not None:
+        c.terrain_type = {"Static": TERRAIN_STATIC, "Moving": TERRAIN_MOVING}[str(tt).strip('"')]
+    if keys.get("prob.Ampl") is not None:
+        c.mt_ampl = float(keys["prob.Ampl"])
     st = g("substepping_type")
     if st is not None:
         c.substepping_type = {"None": SUBSTEP_NONE, "Implicit": SUBSTEP_IMPLICIT}[str(st).strip('"')]

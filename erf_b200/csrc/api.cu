@@ -78,6 +78,16 @@ struct erf_b200_ctx {
     double *r0, *p0, *pi0, *th0;   // nz+2 values, or (nz+2) planes with terrain
     double *znd = nullptr, *detJ = nullptr, *zcc = nullptr;   // static terrain
     double* met = nullptr;                                    // its metric tables
+    // moving terrain: the grids at the step's old time (z[0] = znd, with
+    // met / detJ / zcc) and at the stage's source (z[1], with met1 / detJ1 /
+    // zcc1) and new (z[2]) times; z_t; the step's old base state; the clock
+    struct MovingTerrain {
+        double* z[3];
+        double *met1, *detJ1, *zcc1;
+        double* zt;
+        double *r0o, *p0o;
+        double* time;
+    } mt{};
     int ter_tx = 0;                                           // k_ter_fast_vert columns per block
     size_t ter_smem = 0;                                      // and its shared memory
     bool ter_set = false;
@@ -159,7 +169,10 @@ int validate(const erf_b200_config* c) {
     if (!adv_supported(c->dycore_horiz_adv) || !adv_supported(c->dycore_vert_adv)) return ERF_B200_ECONFIG;
     if (c->dycore_horiz_adv == ERF_ADV_WENO_3 || c->dycore_horiz_adv == ERF_ADV_WENO_5) return ERF_B200_ECONFIG;
     if (c->dycore_vert_adv == ERF_ADV_WENO_3 || c->dycore_vert_adv == ERF_ADV_WENO_5) return ERF_B200_ECONFIG;
-    if (c->dycore_horiz_adv == ERF_ADV_CENTERED_2ND && c->dycore_vert_adv == ERF_ADV_CENTERED_2ND) return ERF_B200_ECONFIG;
+    // Centered_2nd in both directions takes AdvectionSrcForMom's simplified
+    // form (ERF_AdvectionSrcForMom.cpp:95-110, 205-215), built on the terrain path
+    if (!c->use_terrain && c->dycore_horiz_adv == ERF_ADV_CENTERED_2ND && c->dycore_vert_adv == ERF_ADV_CENTERED_2ND)
+        return ERF_B200_ECONFIG;
     if (!adv_supported(c->dryscal_horiz_adv) || !adv_supported(c->dryscal_vert_adv)) return ERF_B200_ECONFIG;
     if (!adv_supported(c->moistscal_horiz_adv) || !adv_supported(c->moistscal_vert_adv)) return ERF_B200_ECONFIG;
     if (c->les_type != ERF_LES_NONE && c->les_type != ERF_LES_SMAGORINSKY && c->les_type != ERF_LES_DEARDORFF &&
@@ -169,6 +182,20 @@ int validate(const erf_b200_config* c) {
         return ERF_B200_ECONFIG;
     if (c->les_type == ERF_LES_MLP && c->molec_diff_type != ERF_MOLEC_NONE) return ERF_B200_ECONFIG;
     if (c->use_terrain != 0 && c->use_terrain != 1) return ERF_B200_ECONFIG;
+    if (c->terrain_type != ERF_TERRAIN_STATIC && c->terrain_type != ERF_TERRAIN_MOVING) return ERF_B200_ECONFIG;
+    if (c->terrain_type == ERF_TERRAIN_MOVING) {
+        // moving terrain: the reference's MovingTerrain setting -- dry,
+        // Centered_2nd dycore (asserted by slow_rhs_fun_pre), no diffusion,
+        // buoyancy type 1, slip walls, one update per RK stage
+        if (!c->use_terrain || c->substepping_type != ERF_SUBSTEP_NONE) return ERF_B200_ECONFIG;
+        if (c->moisture != ERF_MOIST_NONE || c->les_type != ERF_LES_NONE || c->molec_diff_type != ERF_MOLEC_NONE)
+            return ERF_B200_ECONFIG;
+        if (c->dycore_horiz_adv != ERF_ADV_CENTERED_2ND || c->dycore_vert_adv != ERF_ADV_CENTERED_2ND)
+            return ERF_B200_ECONFIG;
+        if (c->buoyancy_type != 1 || c->zlo_bc != ERF_BC_SLIP_WALL || c->zhi_bc != ERF_BC_SLIP_WALL)
+            return ERF_B200_ECONFIG;
+        if (!(c->mt_wavelength > 0.0) || !(std::fabs(c->mt_ampl) < 0.5 * c->nz * c->dz)) return ERF_B200_ECONFIG;
+    }
     if (c->use_terrain) {
         // terrain path: LES closure (or no diffusion), explicit closures only;
         // with moisture, buoyancy type 1 (total density against the 3-D base state)
@@ -220,6 +247,16 @@ void make_params(erf_b200_ctx* c) {
     P.znd = c->znd;
     P.detJ = c->detJ;
     P.met = c->met;
+    P.mt_zt = nullptr;
+    P.mt_znew = nullptr;
+    {
+        const double PI = 3.14159265358979323846264338327950288;
+        P.mt_ampl = f.mt_ampl;
+        P.mt_kp = f.mt_wavelength > 0.0 ? 2.0 * PI / f.mt_wavelength : 0.0;
+        P.mt_om = std::sqrt(9.81 * P.mt_kp);   // deep-water gravity wave, CONST_GRAV
+        P.mt_dx = f.dx;
+        P.mt_dz = f.dz;
+    }
     // Deardorff constants (ERF_ComputeTurbulentViscosity.cpp:129-142) and the
     // buoyancy factor of the TKE source (ERF_DiffusionSrcForState_N.cpp:681-697)
     P.Delta = DeltaMsf;
@@ -386,11 +423,71 @@ void enqueue_step_ter(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     }
 }
 
+// One step over moving terrain without acoustic substepping
+// (MRISplitIntegrator::advance with the moving-terrain branches of
+// slow_rhs_fun_pre, no_substep_fun and slow_rhs_fun_post, then
+// post_timestep).  The grid at the step's old time and its tables serve the
+// step prologue and the slow-variable pass; each stage regenerates the grid
+// at its source time (tables for the slow right-hand side) and at its new
+// time, forms z_t, updates the base state after the slow right-hand side
+// and applies the detJ-weighted stage update.  Every launch reads the
+// device clock, so the captured graph replays for any step.
+template <class R>
+void enqueue_step_mt(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
+    Params Po = c->P;
+    Po.mt_zt = c->mt.zt;
+    Po.mt_znew = c->mt.z[2];
+    Params Ps = Po;
+    Ps.znd = c->mt.z[1];
+    Ps.met = c->mt.met1;
+    Ps.detJ = c->mt.detJ1;
+    const double dt = c->cfg.dt;
+    cudaStream_t st = c->stream;
+    const size_t nb = (size_t)(c->cfg.nz + 2) * c->cfg.nx * c->cfg.ny * sizeof(double);
+    StateBuf OLD = c->S[p], N0 = c->S[1 - p], N1 = c->S[2], SUM = c->S[3];
+    double** Vold = c->vel[p];
+    double** Vnew = c->vel[1 - p];
+    launch_mt_grid(Po, st, c->mt.time, dt, 0, c->mt.z[0]);
+    launch_ter_metrics(Po, st, c->detJ, c->zcc);
+    cudaMemcpyAsync(c->mt.r0o, c->r0, nb, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(c->mt.p0o, c->p0, nb, cudaMemcpyDeviceToDevice, st);
+    TIMED(0, launch_ter_step_begin<R>(Po, st, OLD.cons, Vold[0], Vold[1], Vold[2], OLD, Vnew[0], Vnew[1], Vnew[2],
+                                      B.aux[0], B.mut, B.tke));
+    StateBuf outs[3] = {N0, N1, N0};
+    StateBuf stage[3] = {OLD, outs[0], outs[1]};
+    int a = 0;
+    for (int nrk = 0; nrk < 3; ++nrk) {
+        StateBuf Sst = stage[nrk], Snew = outs[nrk];
+        StageAux<R> Acur = B.aux[a], Anext = B.aux[1 - a];
+        int nsub; double dtau, slow_dt;
+        stage_schedule(c->cfg, nrk, nsub, dtau, slow_dt);
+        const int ts_src = nrk, ts_new = nrk + 1;   // T, T + dt/3, T + dt/2, T + dt
+        launch_mt_grid(Po, st, c->mt.time, dt, ts_src, c->mt.z[1]);
+        launch_mt_grid(Po, st, c->mt.time, dt, ts_new, c->mt.z[2]);
+        launch_ter_metrics(Ps, st, c->mt.detJ1, c->mt.zcc1);
+        launch_mt_zt(Po, st, c->mt.z[0], c->mt.z[2], c->mt.time, dt, ts_new, c->mt.zt);
+        TIMED(2, launch_ter_slow_cell<R>(Ps, st, Sst, Acur, Vnew[0], Vnew[1], B.mut, B.tke, B.ter, B.Fcons, B.avx,
+                                         B.avy, B.avz));
+        TIMED(4, launch_ter_slow_mom<R>(Ps, st, Sst, Acur, Vnew[0], Vnew[1], Vnew[2], B.t11, B.t22, B.t33, B.t12,
+                                        B.t13, B.t23, B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz));
+        launch_mt_base_state(Po, st, c->mt.r0o, c->mt.p0o, c->mt.z[0], c->mt.z[1], c->mt.z[2], c->mt.time, dt,
+                             ts_new, c->r0, c->p0);
+        TIMED(10, launch_mt_no_substep<R>(Po, st, nsub * dtau, OLD, B.Fcons, B.Fmx, B.Fmy, B.Fmz, c->mt.z[0],
+                                          c->mt.z[2], SUM));
+        TIMED(7, launch_ter_post<R>(Po, st, c->tkz.ter_post, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext,
+                                    nrk < 2 ? 1 : 0, B.mut, B.tke, B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1],
+                                    Vnew[2]));
+        a = 1 - a;
+    }
+    launch_mt_advance_time(st, c->mt.time, dt);
+}
+
 // Enqueue one full step with parity p (state slot p is the old state).
 template <class R>
 void enqueue_step_t(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     if (c->P.ter) {
-        enqueue_step_ter<R>(c, B, p, T);
+        if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) enqueue_step_mt<R>(c, B, p, T);
+        else enqueue_step_ter<R>(c, B, p, T);
         return;
     }
     const Params& P = c->P;
@@ -580,6 +677,9 @@ int erf_b200_config_defaults(erf_b200_config* cfg) {
     cfg->force_stage1_single_substep = 1;
     cfg->most_z0 = 0.1;
     cfg->most_zref = 0.0;
+    cfg->terrain_type = ERF_TERRAIN_STATIC;
+    cfg->mt_ampl = 0.0;
+    cfg->mt_wavelength = 100.0;
     cfg->ncomp = 5;
     cfg->dycore_horiz_adv = cfg->dycore_vert_adv = ERF_ADV_UPWIND_3RD;
     cfg->dryscal_horiz_adv = cfg->dryscal_vert_adv = ERF_ADV_UPWIND_3RD;
@@ -643,6 +743,15 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
         const size_t sk = (size_t)cfg->nx * cfg->ny;
         A(&c->znd, (size_t)(cfg->nz + 3) * sk); A(&c->detJ, N); A(&c->zcc, (size_t)(cfg->nz + 1) * sk);
         A(&c->met, (size_t)TER_NMET * NZF);
+        if (cfg->terrain_type == ERF_TERRAIN_MOVING) {
+            c->mt.z[0] = c->znd;
+            A(&c->mt.z[1], (size_t)(cfg->nz + 3) * sk); A(&c->mt.z[2], (size_t)(cfg->nz + 3) * sk);
+            A(&c->mt.met1, (size_t)TER_NMET * NZF); A(&c->mt.detJ1, N); A(&c->mt.zcc1, (size_t)(cfg->nz + 1) * sk);
+            A(&c->mt.zt, NZF);
+            A(&c->mt.r0o, (size_t)(cfg->nz + 2) * sk); A(&c->mt.p0o, (size_t)(cfg->nz + 2) * sk);
+            A(&c->mt.time, 1);
+            if (rc == ERF_B200_OK) cudaMemsetAsync(c->mt.time, 0, sizeof(double), c->stream);
+        }
     }
     if (rc == ERF_B200_OK) {
         void* q = nullptr;
@@ -651,6 +760,8 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     }
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     make_params(c);
+    // a moving grid is generated by the step itself
+    if (cfg->use_terrain && cfg->terrain_type == ERF_TERRAIN_MOVING) c->ter_set = true;
     if (c->mixed) tiled_setup<float>(c->P, &c->tkz);
     else tiled_setup<double>(c->P, &c->tkz);
     c->tkz.ter_post = !cfg->use_terrain ? 0 : (c->mixed ? ter_post_kz<float>(c->P) : ter_post_kz<double>(c->P));
@@ -763,6 +874,7 @@ int erf_b200_set_base_state(erf_b200_ctx* c, const double* rho0, const double* p
 // and detJ / z_cc formed on the GPU (make_J, make_zcc).
 int erf_b200_set_terrain(erf_b200_ctx* c, const double* z_nd) {
     if (!c || !z_nd || !c->cfg.use_terrain) return ERF_B200_EINVAL;
+    if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) return ERF_B200_EINVAL;   // the grid is generated
     const int nx = c->cfg.nx, ny = c->cfg.ny, nz = c->cfg.nz;
     const size_t nn = (size_t)(nx + 1) * (ny + 1) * (nz + 1), sk = (size_t)nx * ny;
     std::vector<double> h(nn), z((size_t)(nz + 3) * sk);
@@ -793,6 +905,40 @@ int erf_b200_set_terrain(erf_b200_ctx* c, const double* z_nd) {
     for (double v : J)
         if (!(v > 0.0)) return ERF_B200_EINVAL;   // folded or inverted cells
     c->ter_set = true;
+    return ERF_B200_OK;
+}
+
+// Moving terrain: set the device clock (the old time of the next step).
+int erf_b200_set_time(erf_b200_ctx* c, double time) {
+    if (!c || c->cfg.terrain_type != ERF_TERRAIN_MOVING || !c->cfg.use_terrain) return ERF_B200_EINVAL;
+    CK(cudaMemcpyAsync(c->mt.time, &time, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ERF_B200_OK;
+}
+
+// Moving terrain: the clock, the grid at that time ((nz+1)(ny+1)(nx+1)
+// nodes, i fastest; node nx / ny repeat node 0) and the evolved base state
+// (rho0, p0: (nz+2) planes of nx*ny) into host memory; NULL skips an output.
+int erf_b200_moving_terrain_state(erf_b200_ctx* c, double* time, double* z_nd, double* rho0, double* p0) {
+    if (!c || c->cfg.terrain_type != ERF_TERRAIN_MOVING || !c->cfg.use_terrain) return ERF_B200_EINVAL;
+    const int nx = c->cfg.nx, ny = c->cfg.ny, nz = c->cfg.nz;
+    const size_t sk = (size_t)nx * ny;
+    if (z_nd) {
+        Params Po = c->P;
+        launch_mt_grid(Po, c->stream, c->mt.time, c->cfg.dt, 0, c->mt.z[1]);
+        CK(cudaGetLastError());
+        std::vector<double> z((size_t)(nz + 3) * sk);
+        CK(cudaMemcpyAsync(z.data(), c->mt.z[1], z.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k <= nz; ++k)
+            for (int j = 0; j <= ny; ++j)
+                for (int i = 0; i <= nx; ++i)
+                    z_nd[((size_t)k * (ny + 1) + j) * (nx + 1) + i] = z[(size_t)(k + 1) * sk + (size_t)(j % ny) * nx + (i % nx)];
+    }
+    if (time) CK(cudaMemcpyAsync(time, c->mt.time, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (rho0) CK(cudaMemcpyAsync(rho0, c->r0, (size_t)(nz + 2) * sk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (p0) CK(cudaMemcpyAsync(p0, c->p0, (size_t)(nz + 2) * sk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return ERF_B200_OK;
 }
 
@@ -1010,6 +1156,7 @@ int erf_b200_turbulent_viscosity(erf_b200_ctx* c, const erf_b200_fab* xvel, cons
                                  const erf_b200_fab* zvel, const erf_b200_fab* cons) {
     if (!c || c->mixed || !c->base_set) return ERF_B200_EINVAL;
     if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) return ERF_B200_EINVAL;   // fused step only
     const Geo& g = c->g;
     if (!fab_ok(cons, 0, g, c->cfg.ncomp) || !fab_ok(xvel, 1, g, 1) || !fab_ok(yvel, 2, g, 1) || !fab_ok(zvel, 3, g, 1))
         return ERF_B200_EINVAL;
@@ -1050,6 +1197,7 @@ int erf_b200_slow_rhs_pre(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b2
     (void)slow_dt;
     if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
     if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) return ERF_B200_EINVAL;   // fused step only
     if (c->P.most && !c->most_set) return ERF_B200_EBADSTATE;
     if (c->P.les == ERF_LES_MLP && !c->net) return ERF_B200_EBADSTATE;
     const Geo& g = c->g;
@@ -1100,6 +1248,7 @@ int erf_b200_make_fast_coeffs(erf_b200_ctx* c, const erf_b200_fab* fast_coeffs, 
                               double dtau) {
     if (!c || c->mixed || !c->base_set || !fast_coeffs) return ERF_B200_EINVAL;
     if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) return ERF_B200_EINVAL;   // fused step only
     const Geo& g = c->g;
     if (!fab4_ok(S_stage, g, c->cfg.ncomp) || !fab_ok(fast_coeffs, 3, g, 5)) return ERF_B200_EINVAL;
     StateBuf Sst = c->S[2];
@@ -1125,6 +1274,7 @@ int fast_rhs_pass(erf_b200_ctx* c, bool terrain, int step, int nrk, const erf_b2
     if (!c || c->mixed || !c->base_set || step < 0 || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
     if (terrain != (c->P.ter != 0)) return ERF_B200_ECONFIG;   // _N without terrain, _T with it
     if (terrain && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) return ERF_B200_EINVAL;   // fused step only
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
     if (!fab4_ok(S_slow_rhs, g, 2) || !fab4_ok(S_prev, g, 2) || !fab4_ok(S_stage, g, nc) || !fab4_ok(S_data, g, 2) ||
@@ -1208,6 +1358,7 @@ int erf_b200_slow_rhs_post(erf_b200_ctx* c, int nrk, double slow_dt, const erf_b
     (void)S_rhs;
     if (!c || c->mixed || !c->base_set || nrk < 0 || nrk > 2) return ERF_B200_EINVAL;
     if (c->P.ter && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (c->cfg.terrain_type == ERF_TERRAIN_MOVING) return ERF_B200_EINVAL;   // fused step only
     const Geo& g = c->g;
     const int nc = c->cfg.ncomp;
     if (!fab4_ok(S_old, g, nc) || !fab4_ok(S_new, g, nc) || !fab4_ok(S_data, g, nc) || !fab4_ok(S_scratch, g, 1))

@@ -34,6 +34,13 @@ struct Params {
     const double* znd;
     const double* detJ;
     const double* met;          // metric tables (terrain.cu), TER_NMET planes of nzf
+    // moving terrain (terrain_type Moving; null pointers otherwise): z_t on
+    // the z faces ((nz+1) planes of nx*ny), the nodes at the stage's new time
+    // (detJ_new of the slow-variable update), and the surface wave
+    // h = mt_ampl sin(mt_kp x - mt_om t) on x = i mt_dx, levels k mt_dz
+    const double* mt_zt;
+    const double* mt_znew;
+    double mt_ampl, mt_kp, mt_om, mt_dx, mt_dz;
     // MOST ground (Moeng stress, adiabatic): the level of the reference
     // height, the step's plane means {u, v, |U|, u*} (most_avg, device), the
     // eddy viscosity (R = double or float by most_mut_f32) for eta
@@ -172,6 +179,18 @@ void launch_post(const Params& P, const TiledKz& t, cudaStream_t st, double slow
 
 // Static terrain (terrain.cu): metrics, base state and the _T passes.
 void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* zcc);
+// Moving terrain (terrain.cu).  tdev: the step's old time on the device;
+// tsel 0..3 picks T, T + dt/3, T + dt/2, T + dt.
+void launch_mt_grid(const Params& P, cudaStream_t st, const double* tdev, double dt, int tsel, double* z);
+void launch_mt_zt(const Params& P, cudaStream_t st, const double* zo, const double* zn, const double* tdev,
+                  double dt, int tsel_new, double* zt);
+void launch_mt_base_state(const Params& P, cudaStream_t st, const double* r0o, const double* p0o, const double* zo,
+                          const double* zs, const double* zn, const double* tdev, double dt, int tsel_new,
+                          double* r0n, double* p0n);
+template <class R>
+void launch_mt_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons,
+                          const R* Fmx, const R* Fmy, const R* Fmz, const double* zo, const double* zn, StateBuf Ssum);
+void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt);
 void launch_ter_base_state(const Params& P, cudaStream_t st, const double* zcc, const double* th3, const double* qv3,
                            double th_s, double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0);
 template <class R>

@@ -299,6 +299,188 @@ void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* 
 }
 
 // ---------------------------------------------------------------------------
+// Moving terrain (terrain_type Moving), without acoustic substepping.  The
+// grid is regenerated on the device at every geometry time of the stage
+// (the step's old time, the stage's source and new times) from the device
+// copy of the step's old time, so that the step graph replays unchanged.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mt_time_at(double T, double dt, int tsel) {
+    return tsel == 0 ? T : (tsel == 1 ? T + dt / 3.0 : (tsel == 2 ? T + dt / 2.0 : T + dt));
+}
+// node (i,j,k) of a grid in the znd layout ((nz+3) planes, lateral periodic)
+__device__ __forceinline__ double znode(const double* z, const Geo& g, int i, int j, int k) {
+    return __ldg(z + (int64_t)(k + 1) * g.sk + (int64_t)wrap(j, g.ny) * g.nx + wrap(i, g.nx));
+}
+// make_J of one cell from the nodes (Utils/ERF_TerrainMetrics.cpp:583-640);
+// k = -1 takes level 0 (the grid's ghost level mirrors the first cell)
+__device__ __forceinline__ double mt_detj(const double* z, const Geo& g, int i, int j, int k) {
+    if (k < 0) k = 0;
+    auto Z = [&](int a, int b, int c) { return znode(z, g, a, b, c); };
+    return .25 * g.dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1)
+                          - Z(i, j, k) - Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
+}
+
+// Problem::init_custom_terrain of the travelling wave
+// (Exec/DevTests/MovingTerrain/ERF_prob.cpp:147-200) and init_terrain_grid
+// with terrain_smoothing = 2 (Utils/ERF_TerrainMetrics.cpp:501-536, 320-333):
+// z(k) = z_k + (1 - z_k / z_top)^3 h over z_k = k dz, z(0) = h,
+// z(-1) = 2 h - z(1), z(nz+1) = 2 z(nz) - z(nz-1).  One thread per column.
+__global__ void k_mt_grid(Params P, const double* __restrict__ tdev, double dt, int tsel, double* __restrict__ z) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const double t = mt_time_at(*tdev, dt, tsel);
+    const double x = i * P.mt_dx;
+    const double hs = P.mt_ampl * sin(P.mt_kp * x - P.mt_om * t);
+    const int nz = g.nz;
+    const double ztop = nz * P.mt_dz;
+    double* col = z + (int64_t)j * g.nx + i;
+    double zk1 = 0.0, zkm1 = 0.0, zk = hs;
+    for (int k = 0; k <= nz; ++k) {
+        const double zl = k * P.mt_dz;
+        double v = zl + pow(1. - zl / ztop, 3.0) * hs;
+        if (k == 0) v = hs;
+        col[(int64_t)(k + 1) * g.sk] = v;
+        if (k == 1) zk1 = v;
+        if (k == nz - 1) zkm1 = v;
+        if (k == nz) zk = v;
+    }
+    col[0] = 2.0 * hs - zk1;
+    col[(int64_t)(nz + 2) * g.sk] = 2.0 * zk - zkm1;
+}
+void launch_mt_grid(const Params& P, cudaStream_t st, const double* tdev, double dt, int tsel, double* z) {
+    k_mt_grid<<<ter_grid(P.g, 1), ter_block(), 0, st>>>(P, tdev, dt, tsel, z);
+}
+
+// z_t of the stage (ERF_TI_slow_rhs_fun.H:84-107): (z_new - z_old) / slow_dt
+// averaged over the four nodes of each z face, slow_dt = new stage time - T.
+__global__ void k_mt_zt(Params P, const double* __restrict__ zo, const double* __restrict__ zn,
+                        const double* __restrict__ tdev, double dt, int tsel_new, double* __restrict__ zt) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const double T = *tdev;
+    const double inv_dt = 1. / (mt_time_at(T, dt, tsel_new) - T);
+    auto N = [&](int a, int b) { return znode(zn, g, a, b, k); };
+    auto O = [&](int a, int b) { return znode(zo, g, a, b, k); };
+    zt[cidx(g, i, j, k)] = 0.25 * inv_dt * (N(i + 1, j + 1) - O(i + 1, j + 1) + N(i, j + 1) - O(i, j + 1)
+                                            + N(i + 1, j) - O(i + 1, j) + N(i, j) - O(i, j));
+}
+void launch_mt_zt(const Params& P, cudaStream_t st, const double* zo, const double* zn, const double* tdev,
+                  double dt, int tsel_new, double* zt) {
+    k_mt_zt<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, zo, zn, tdev, dt, tsel_new, zt);
+}
+
+// The base-state update of a moving-terrain stage (ERF_TI_slow_rhs_fun.H:149-210):
+// rho_0 and (rho theta)_0 advanced from the step's old base state by the
+// vertical flux -z_t (face averages of the previous stage's new base state),
+// detJ-weighted old -> source -> new; p_0 from (rho theta)_0.  One thread
+// per column walks up the levels, keeping the level below (already
+// overwritten) in registers; the ghost levels are not updated.
+__global__ void k_mt_base_state(Params P, const double* __restrict__ r0o, const double* __restrict__ p0o,
+                                const double* __restrict__ zo, const double* __restrict__ zs,
+                                const double* __restrict__ zn, const double* __restrict__ tdev, double dt,
+                                int tsel_new, double* __restrict__ r0n, double* __restrict__ p0n) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const double T = *tdev;
+    const double dt_base = mt_time_at(T, dt, tsel_new) - T;
+    const double* zt = P.mt_zt;
+    auto at = [&](int k) { return (int64_t)(k + 1) * g.sk + (int64_t)j * g.nx + i; };
+    double r_m = r0n[at(-1)], rt_m = eos_rt_given_p(p0n[at(-1)]);
+    double r_c = r0n[at(0)], rt_c = eos_rt_given_p(p0n[at(0)]);
+    for (int k = 0; k < g.nz; ++k) {
+        const double r_p = r0n[at(k + 1)], rt_p = eos_rt_given_p(p0n[at(k + 1)]);
+        const double zl = zt[cidx(g, i, j, k)], zh = zt[cidx(g, i, j, k + 1)];
+        double fr_lo = -zl * 0.5 * (r_c + r_m);
+        double fr_hi = -zh * 0.5 * (r_c + r_p);
+        double frt_lo = fr_lo * 0.5 * (rt_c / r_c + rt_m / r_m);
+        double frt_hi = fr_hi * 0.5 * (rt_c / r_c + rt_p / r_p);
+        const double Js = mt_detj(zs, g, i, j, k), Jo = mt_detj(zo, g, i, j, k), Jn = mt_detj(zn, g, i, j, k);
+        double invdetJ = 1.0 / Js;
+        double src_r = -invdetJ * (fr_hi - fr_lo) * g.dzi;
+        double src_rt = -invdetJ * (frt_hi - frt_lo) * g.dzi;
+        double rho0_new = Jo * r0o[at(k)] + dt_base * Js * src_r;
+        double rt0_new = Jo * eos_rt_given_p(p0o[at(k)]) + dt_base * Js * src_rt;
+        r0n[at(k)] = rho0_new / Jn;
+        rt0_new /= Jn;
+        p0n[at(k)] = eos_p(rt0_new, 0.0);
+        r_m = r_c; rt_m = rt_c; r_c = r_p; rt_c = rt_p;
+    }
+}
+void launch_mt_base_state(const Params& P, cudaStream_t st, const double* r0o, const double* p0o, const double* zo,
+                          const double* zs, const double* zn, const double* tdev, double dt, int tsel_new,
+                          double* r0n, double* p0n) {
+    k_mt_base_state<<<ter_grid(P.g, 1), ter_block(), 0, st>>>(P, r0o, p0o, zo, zs, zn, tdev, dt, tsel_new, r0n, p0n);
+}
+
+// no_substep_fun for moving terrain (TimeIntegration/ERF_TI_no_substep_fun.H:54-109),
+// part 1: rho and rho theta detJ-weighted old -> new, the horizontal
+// momenta with h_zeta of their faces (the slow right-hand sides already
+// carry the source geometry's factors).
+__device__ __forceinline__ double mt_hzI(const double* z, const Geo& g, int i, int j, int k) {
+    return 0.5 * g.dzi * (znode(z, g, i, j, k + 1) + znode(z, g, i, j + 1, k + 1) - znode(z, g, i, j, k) - znode(z, g, i, j + 1, k));
+}
+__device__ __forceinline__ double mt_hzJ(const double* z, const Geo& g, int i, int j, int k) {
+    return 0.5 * g.dzi * (znode(z, g, i, j, k + 1) + znode(z, g, i + 1, j, k + 1) - znode(z, g, i, j, k) - znode(z, g, i + 1, j, k));
+}
+template <class R>
+__global__ void k_mt_no_substep_h(Params P, double slow_dt, StateBuf Sold, const R* __restrict__ Fcons,
+                                  const R* __restrict__ Fmx, const R* __restrict__ Fmy, const double* __restrict__ zo,
+                                  const double* __restrict__ zn, StateBuf Ssum) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int64_t c = cidx(g, i, j, k), N = g.ncell;
+    const double Jo = mt_detj(zo, g, i, j, k), Jn = mt_detj(zn, g, i, j, k);
+    for (int n = 0; n < 2; ++n) {
+        double v = Jo * Sold.cons[n * N + c] + slow_dt * double(Fcons[n * N + c]);
+        Ssum.cons[n * N + c] = v / Jn;
+    }
+    Ssum.mx[c] = (mt_hzI(zo, g, i, j, k) * Sold.mx[c] + slow_dt * double(Fmx[c])) / mt_hzI(zn, g, i, j, k);
+    Ssum.my[c] = (mt_hzJ(zo, g, i, j, k) * Sold.my[c] + slow_dt * double(Fmy[c])) / mt_hzJ(zn, g, i, j, k);
+}
+// part 2: rho w with the face detJ; on the moving ground W from Omega =
+// rho z_t on the new grid with the new horizontal momenta.
+template <class R>
+__global__ void k_mt_no_substep_w(Params P, double slow_dt, StateBuf Sold, const R* __restrict__ Fmz,
+                                  const double* __restrict__ zo, const double* __restrict__ zn, StateBuf Ssum) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int64_t c = cidx(g, i, j, k);
+    if (k == 0) {
+        Params Pn = P;
+        Pn.znd = zn;
+        auto MX = [&](int a, int b, int kk) { return Ssum.mx[cidx(g, wrap(a, g.nx), wrap(b, g.ny), kk)]; };
+        auto MY = [&](int a, int b, int kk) { return Ssum.my[cidx(g, wrap(a, g.nx), wrap(b, g.ny), kk)]; };
+        double mx = zlo_xi_fn(Pn, i, j, 0), my = zlo_eta_fn(Pn, i, j, 0), u, v;
+        zface_uv(i, j, 0, MX, MY, u, v);
+        const double rho_on_face = Ssum.cons[c];
+        Ssum.mz[c] = rho_on_face * P.mt_zt[c] + mx * u + my * v;
+    } else {
+        double ko = 0.5 * (mt_detj(zo, g, i, j, k) + mt_detj(zo, g, i, j, k - 1));
+        double kn = 0.5 * (mt_detj(zn, g, i, j, k) + mt_detj(zn, g, i, j, k - 1));
+        Ssum.mz[c] = (ko * Sold.mz[c] + slow_dt * double(Fmz[c])) / kn;
+    }
+}
+template <class R>
+void launch_mt_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons,
+                          const R* Fmx, const R* Fmy, const R* Fmz, const double* zo, const double* zn, StateBuf Ssum) {
+    k_mt_no_substep_h<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, slow_dt, Sold, Fcons, Fmx, Fmy, zo, zn, Ssum);
+    k_mt_no_substep_w<R><<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, slow_dt, Sold, Fmz, zo, zn, Ssum);
+}
+template void launch_mt_no_substep<double>(const Params&, cudaStream_t, double, StateBuf, const double*, const double*,
+                                           const double*, const double*, const double*, const double*, StateBuf);
+template void launch_mt_no_substep<float>(const Params&, cudaStream_t, double, StateBuf, const float*, const float*,
+                                          const float*, const float*, const double*, const double*, StateBuf);
+
+// post_timestep's clock (ERF.cpp:547-559 with t_new = t_old + dt)
+__global__ void k_mt_advance_time(double* t, double dt) { *t = *t + dt; }
+void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt) { k_mt_advance_time<<<1, 1, 0, st>>>(tdev, dt); }
+
+// ---------------------------------------------------------------------------
 // Base state over the terrain, one thread per column: calc_rho_p Newton
 // integration from p_sfc at z = 0 through the column's cell centres
 // (ERF_InputSoundingData.H:176-256), then erf_enforce_hse with terrain
@@ -547,11 +729,14 @@ __global__ void k_ter_step_begin(Params P, const double* __restrict__ cons, cons
         double m0 = (vo[c] * 0.5) * rs, v1 = (m0 * 2.0) / rs;
         S.my[c] = (v1 * 0.5) * rs; vn[c] = v1;
     }
-    if (k == 0) {
+    if (k == 0 && !P.mt_zt) {
         double wb = w_from_omega(P, i, j, 0, 0.0, urt, vrt);
         S.mz[c] = (wb * 0.5) * (rho + rho); wn[c] = wb;
     } else {
-        double rs = rho + cons[c - g.sk];
+        // (a moving ground keeps its w: the moving-terrain branch of
+        // impose_vertical_zvel_bcs sets nothing; rho below the ground is
+        // the foextrap ghost)
+        double rs = rho + (k == 0 ? rho : cons[c - g.sk]);
         double m0 = (wo[c] * 0.5) * rs, w1 = (m0 * 2.0) / rs;
         S.mz[c] = (w1 * 0.5) * rs; wn[c] = w1;
     }
@@ -846,7 +1031,13 @@ __device__ __forceinline__ double omega_mom(const Params& P, StateBuf S, const d
         return tvel(v, g, ii, jj, g.nz) * 0.5 * rs;
     };
     double rw = S.mz[cidx(g, wrap(i, g.nx), wrap(j, g.ny), k)];
-    return omega_from_w(P, i, j, k, rw, MX, MY);
+    double om = omega_from_w(P, i, j, k, rw, MX, MY);
+    if (P.mt_zt && k < g.nz) {   // the grid's own motion (ERF_slow_rhs_pre.cpp:389-398); z_t = 0 at the lid
+        const int ii = wrap(i, g.nx), jj = wrap(j, g.ny);
+        const double rho_at_face = 0.5 * (S.cons[cidx(g, ii, jj, k)] + S.cons[cidx(g, ii, jj, k - 1)]);
+        om -= rho_at_face * P.mt_zt[cidx(g, ii, jj, k)];
+    }
+    return om;
 }
 
 // Face interpolation of a cell field along x / y / z (the stencil's unused
@@ -939,6 +1130,10 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_CELL) k_ter_slow_cell(Param
             if (k == nz - 1) tke.hfz[c + g.sk] = R(rhi);
         }
     }
+    if (P.mt_zt) {   // moving terrain: the rho and rho theta RHS carry detJ (ERF_slow_rhs_pre.cpp:528-535)
+        frho *= Jc;
+        frt *= Jc;
+    }
     Fcons[c] = R(frho);
     Fcons[N + c] = R(frt);
 }
@@ -1028,6 +1223,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
         }
         xsrc += 0.5 * (S.cons[c] + S.cons[cidx(g, wrap(i - 1, g.nx), j, k)]) * P.geo0;
         r += (-gpx - 0.0) / (1.0 + moist_q(P, A.prim, c, cidx(g, wrap(i - 1, g.nx), j, k))) + xsrc;
+        if (P.mt_zt) r *= hzeta_I(P, i, j, k);   // moving terrain (ERF_slow_rhs_pre.cpp:633-636)
         Fmx[c] = R(r);
     }
     // ---------------- y-momentum at face (i,j,k)
@@ -1078,6 +1274,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
         }
         ysrc += 0.5 * (S.cons[c] + S.cons[cidx(g, i, wrap(j - 1, g.ny), k)]) * P.geo1;
         r += (-gpy - 0.0) / (1.0 + moist_q(P, A.prim, c, cidx(g, i, wrap(j - 1, g.ny), k))) + ysrc;
+        if (P.mt_zt) r *= hzeta_J(P, i, j, k);   // :681-684
         Fmy[c] = R(r);
     }
     // ---------------- z-momentum at face (i,j,k), 1 <= k <= nz-1
@@ -1174,6 +1371,7 @@ __global__ void __launch_bounds__(128, TER_MINB_SLOW_MOM) k_ter_slow_mom(Params 
         }
         zsrc += 0.5 * (S.cons[c] + S.cons[c - g.sk]) * P.geo2;
         r += (zsrc - gpz - 0.0) / (1.0 + moist_q(P, A.prim, c, c - g.sk));
+        if (P.mt_zt) r *= 0.5 * (Jt(i, j, k) + Jt(i, j, k - 1));   // :741-743
         Fmz[c] = R(r);
         if (k == nz - 1) Fmz[c + g.sk] = R(0);
     }
@@ -1446,7 +1644,7 @@ __global__ void __launch_bounds__(1024) k_ter_fast_vert(Params P, double dtau, d
 // round trips, w on the ground and the lid from Omega = 0 of the new u, v;
 // the next stage's primitives.
 // ---------------------------------------------------------------------------
-template <class R, int DH, int DV, int MH, int MV, int NS>
+template <class R, int DH, int DV, int MH, int MV, int NS, bool MT = false>
 __global__ void __launch_bounds__(TTX * TTY, TER_MINB_POST) k_ter_post(Params P, int kz, double slow_dt, StateBuf Sold,
                                                                        StateBuf Sst, StateBuf Ssum, StateBuf Snew,
                                                                        StageAux<R> Acur, StageAux<R> Anext,
@@ -1541,6 +1739,15 @@ __global__ void __launch_bounds__(TTX * TTY, TER_MINB_POST) k_ter_post(Params P,
                 r += 2.0 * double(mut[c]) * double(tke.smn[c]);
                 r -= double(tke.diss[c]);
             }
+            if (MT) {
+                // moving terrain (ERF_slow_rhs_post.cpp:467-478): detJ-weighted
+                // old -> new; only rho KE is clamped
+                const double Jo = detJ_at(P, i, j, k), Jn = mt_detj(P.mt_znew, g, i, j, k);
+                double tv = Jo * Sold.cons[n * N + c] + slow_dt * Jo * r;
+                tv /= Jn;
+                Snew.cons[n * N + c] = ke ? fmax(tv, 2.220446049250313e-16) : tv;
+                continue;
+            }
             double v_ = Sold.cons[n * N + c] + slow_dt * r;
             Snew.cons[n * N + c] = (q == 0) ? v_ : fmax(v_, species ? 0.0 : 2.220446049250313e-16);
         }
@@ -1584,11 +1791,12 @@ __global__ void __launch_bounds__(TTX * TTY, TER_MINB_POST) k_ter_post(Params P,
             double v2 = v2f(i, j, k);
             Snew.my[c] = (v2 * 0.5) * rs; vn[c] = v2;
         }
-        if (k == 0) {
+        if (k == 0 && !MT) {
             double wb = w_from_omega(P, i, j, 0, 0.0, u2f, v2f);
             Snew.mz[c] = (wb * 0.5) * (rho + rho); wn[c] = wb;
         } else {
-            double rs = rho + Ssum.cons[c - g.sk];
+            // (on a moving ground the w of the update, through the two round trips)
+            double rs = rho + (k == 0 ? rho : Ssum.cons[c - g.sk]);
             double m = Ssum.mz[c];
             double w1 = (m * 2.0) / rs; m = (w1 * 0.5) * rs;
             double w2 = (m * 2.0) / rs; m = (w2 * 0.5) * rs;
@@ -1682,6 +1890,7 @@ using TerPostK = void (*)(Params, int, double, StateBuf, StateBuf, StateBuf, Sta
 template <class R>
 TerPostK<R> ter_post_kernel(const Params& P) {
     const bool du = P.dry_h == TU5 && P.dry_v == TU5, mw = P.moi_h == TW5 && P.moi_v == TW5;
+    if (P.mt_znew) return k_ter_post<R, -1, -1, -1, -1, 2, true>;   // moving terrain: dry
     if (!P.moist) return du ? k_ter_post<R, TU5, TU5, -1, -1, 2> : k_ter_post<R, -1, -1, -1, -1, 2>;
     if (du && mw) return k_ter_post<R, TU5, TU5, TW5, TW5, 5>;
     return k_ter_post<R, -1, -1, -1, -1, 5>;

@@ -36,7 +36,7 @@ EXPORTS = [
     "erf_b200_last_cuda_error", "erf_b200_set_terrain", "erf_b200_make_base_state_terrain",
     "erf_b200_fast_rhs_T", "erf_b200_write_plotfile", "erf_b200_write_checkpoint", "erf_b200_read_checkpoint",
     "erf_b200_selftest_bounded_wait", "erf_b200_no_substep", "erf_b200_most_update_fluxes",
-    "erf_b200_ensemble_abort", "erf_b200_ensemble_steps",
+    "erf_b200_ensemble_abort", "erf_b200_ensemble_steps", "erf_b200_set_time", "erf_b200_moving_terrain_state",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs", "no_substep"]
@@ -73,6 +73,8 @@ def load_library():
                                            dp, dp, dp, dp]
     L.erf_b200_set_base_state.argtypes = [vp, dp, dp, dp, dp]
     L.erf_b200_set_terrain.argtypes = [vp, dp]
+    L.erf_b200_set_time.argtypes = [vp, ctypes.c_double]
+    L.erf_b200_moving_terrain_state.argtypes = [vp, dp, dp, dp, dp]
     L.erf_b200_make_base_state_terrain.argtypes = [vp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                    dp, dp, dp, dp]
     fabp = ctypes.POINTER(ErfFab)
@@ -234,6 +236,21 @@ class Dycore:
         cfg = self.cfg
         assert z.shape == (cfg.nz + 1, cfg.ny + 1, cfg.nx + 1)
         _check(self.lib.erf_b200_set_terrain(self._ctx, z.ctypes.data), "set_terrain")
+
+    def set_time(self, t: float):
+        """Moving terrain: the device clock (the old time of the next step)."""
+        _check(self.lib.erf_b200_set_time(self._ctx, float(t)), "set_time")
+
+    def moving_terrain_state(self):
+        """Moving terrain: (time, z_nd [nz+1][ny+1][nx+1], rho0, p0 ((nz+2)*ny*nx))."""
+        cfg = self.cfg
+        t = np.zeros(1)
+        z = np.zeros((cfg.nz + 1, cfg.ny + 1, cfg.nx + 1))
+        r0 = np.zeros((cfg.nz + 2) * cfg.ny * cfg.nx)
+        p0 = np.zeros((cfg.nz + 2) * cfg.ny * cfg.nx)
+        _check(self.lib.erf_b200_moving_terrain_state(self._ctx, t.ctypes.data, z.ctypes.data, r0.ctypes.data,
+                                                      p0.ctypes.data), "moving_terrain_state")
+        return float(t[0]), z, r0, p0
 
     def make_base_state_terrain(self, case):
         """Base state over the terrain on the GPU: 4 arrays of (nz+2)*ny*nx."""

@@ -123,6 +123,10 @@ typedef struct erf_b200_fab {
 #define ERF_SUBSTEP_IMPLICIT 0
 #define ERF_SUBSTEP_NONE     1
 
+/* terrain_type */
+#define ERF_TERRAIN_STATIC 0
+#define ERF_TERRAIN_MOVING 1
+
 typedef struct erf_b200_config {
     /* grid: one box covering the domain, periodic in x and y */
     int    nx, ny, nz;
@@ -170,12 +174,24 @@ typedef struct erf_b200_config {
      * with the whole slow right-hand side, MRISplitIntegrator::set_no_substep,
      * TimeIntegration/ERF_MRI.H:177-180, 255-324; mri_ratio is then unused) */
     int    substepping_type;
-    int    reserved[5];
+    /* SolverChoice::terrain_type with use_terrain: ERF_TERRAIN_STATIC
+     * (z_phys_nd installed by erf_b200_set_terrain) or ERF_TERRAIN_MOVING:
+     * the library regenerates the grid at every geometry time from the
+     * travelling surface wave h(x, t) = mt_ampl sin(k x - omega t),
+     * k = 2 pi / mt_wavelength, omega = sqrt(g k) (the surface of
+     * Exec/DevTests/MovingTerrain/ERF_prob.cpp:147-200) smoothed upward with
+     * Sullivan's factor (1 - z/z_top)^3 (terrain_smoothing = 2,
+     * Utils/ERF_TerrainMetrics.cpp:501-536) over the uniform levels k dz */
+    int    terrain_type;
+    int    reserved[4];
     /* MOST surface layer for zlo_bc ERF_BC_MOST (ABLMost, erf.most.*): the
      * roughness length z0 and the reference height zref (moved to the
      * centre of the cell level that contains it, as MOSTAverage does); Moeng
      * stress, adiabatic surface, plane averages */
     double most_z0, most_zref;
+    /* moving terrain (terrain_type ERF_TERRAIN_MOVING): wave amplitude and
+     * wavelength in metres (prob.Ampl; the wavelength is 100 m upstream) */
+    double mt_ampl, mt_wavelength;
 } erf_b200_config;
 
 /* Opaque context: owns all integrator scratch (S_sum, S_scratch, F_slow,
@@ -242,6 +258,23 @@ int erf_b200_set_terrain(erf_b200_ctx* ctx, const double* z_nd);
  * planes (plane k+1 for level k), the layout erf_b200_set_base_state expects
  * with terrain.  Replaces calc_rho_p + ERF::erf_enforce_hse with terrain
  * (Initialization/ERF_init1d.cpp:152-241). */
+/* Moving terrain (terrain_type ERF_TERRAIN_MOVING).  The grid is not
+ * installed but generated by every step at the geometry times the
+ * reference's moving-terrain path asks for (slow_rhs_fun_pre,
+ * TimeIntegration/ERF_TI_slow_rhs_fun.H:55-107: the step's old time and each
+ * RK stage's source and new times), from a device clock that each step
+ * advances by dt (post_timestep, ERF.cpp:547-559).  The base state set by
+ * erf_b200_set_base_state is the initial one and evolves with the grid.
+ *   erf_b200_set_time: the clock (the old time of the next step; 0 after
+ *     create);
+ *   erf_b200_moving_terrain_state: the clock, the grid at that time
+ *     ((nz+1)(ny+1)(nx+1) nodes, i fastest; node nx / ny repeat node 0) and
+ *     the evolved base density and pressure ((nz+2) planes of nx*ny, plane
+ *     k+1 for level k) into host memory; NULL skips an output.
+ * Both return ERF_B200_EINVAL for a context without moving terrain. */
+int erf_b200_set_time(erf_b200_ctx* ctx, double time);
+int erf_b200_moving_terrain_state(erf_b200_ctx* ctx, double* time, double* z_nd, double* rho0, double* p0);
+
 int erf_b200_make_base_state_terrain(erf_b200_ctx* ctx, const double* theta3, const double* qv3,
                                      double theta_sfc, double qv_sfc, double p_sfc,
                                      double* rho0, double* p0, double* pi0, double* th0);

@@ -165,6 +165,28 @@ def terrain_metrics(cfg, z_nd):
     return detJ, zcc, ax, ay
 
 
+def advance_moving_terrain(cfg, time0, base, cons, u, v, w, nsteps):
+    """Advance copies of the dense state over moving terrain (no acoustic
+    substepping) by nsteps from time0.  Returns (cons, u, v, w, z_nd, rho0,
+    p0): the state, the grid at the final time and the evolved base state."""
+    L = lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.oracle_advance_moving_terrain.argtypes = [ctypes.c_void_p, ctypes.c_double, dp, dp, dp, dp, dp, dp, dp, dp,
+                                                ctypes.c_int, dp, dp, dp]
+    L.oracle_advance_moving_terrain.restype = ctypes.c_int
+    cons, u, v, w = (np.ascontiguousarray(a, dtype=np.float64).copy() for a in (cons, u, v, w))
+    r0, p0, pi0, th0 = (np.ascontiguousarray(a, dtype=np.float64) for a in base)
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    z = np.zeros((nz + 1, ny + 1, nx + 1))
+    r0o = np.zeros((nz + 2) * ny * nx)
+    p0o = np.zeros((nz + 2) * ny * nx)
+    rc = L.oracle_advance_moving_terrain(ctypes.byref(cfg), float(time0), _p(r0), _p(p0), _p(pi0), _p(th0),
+                                         _p(cons), _p(u), _p(v), _p(w), int(nsteps), _p(z), _p(r0o), _p(p0o))
+    if rc != 0:
+        raise RuntimeError("oracle_advance_moving_terrain failed: %d" % rc)
+    return cons, u, v, w, z, r0o, p0o
+
+
 def advance_terrain(cfg, z_nd, base, cons, u, v, w, nsteps):
     """Advance copies of the dense state over terrain by nsteps."""
     L = lib()

@@ -963,6 +963,9 @@ struct Oracle {
             if (!terrain) Om(i, j, k) = S.mz(i, j, k);
             else if (k <= 0) Om(i, j, k) = 0.;
             else if (k >= nz + 1) Om(i, j, k) = S.mz(i, j, k);
+            else if (moving)   // the grid's own motion subtracted (rho at the face as in MomentumToVelocity)
+                Om(i, j, k) = omega_from_w(i, j, k, S.mz(i, j, k), S.mx, S.my)
+                              - 0.5 * (cd(i, j, k, 0) + cd(i, j, k - 1, 0)) * zt(i, j, k);
             else Om(i, j, k) = omega_from_w(i, j, k, S.mz(i, j, k), S.mx, S.my);
         });
         // AdvectionSrcForRho (Advection/ERF_AdvectionSrcForState.cpp:30-93)
@@ -981,7 +984,14 @@ struct Oracle {
             if (terrain) diffusion_state_T(1, 1, cd, prim, R.cons);
             else diffusion_state(1, 1, cd, prim, R.cons, mut);
         }
-        // cc_src is zero for the supported configurations
+        // cc_src is zero for the supported configurations; with moving
+        // terrain the rho and rho theta right-hand sides carry detJ
+        // (ERF_slow_rhs_pre.cpp:528-535)
+        if (moving)
+            loop(valid(CC), [&](int i, int j, int k) {
+                R.cons(i, j, k, 0) *= detJ(i, j, k);
+                R.cons(i, j, k, 1) *= detJ(i, j, k);
+            });
         if (terrain) {
             advect_mom_T(R, S, V, Om);
             if (use_diff) diffusion_mom_T(R, t11, t22, t33, t12, t13, t21, t23, t31, t32);
@@ -1126,6 +1136,7 @@ struct Oracle {
             double q = 0.0;
             if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i - 1, j, k, 4) + prim(i, j, k, 5) + prim(i - 1, j, k, 5));
             R.mx(i, j, k) += (-gpx - 0.0) / (1.0 + q) + xsrc(i, j, k);
+            if (moving) R.mx(i, j, k) *= hzeta_I(i, j, k);   // ERF_slow_rhs_pre.cpp:633-636
         });
         loop(tby, [&](int i, int j, int k) {
             double gpy = dxInv[1] * (pp(i, j, k) - pp(i, j - 1, k));
@@ -1140,6 +1151,7 @@ struct Oracle {
             double q = 0.0;
             if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i, j - 1, k, 4) + prim(i, j, k, 5) + prim(i, j - 1, k, 5));
             R.my(i, j, k) += (-gpy - 0.0) / (1.0 + q) + ysrc(i, j, k);
+            if (moving) R.my(i, j, k) *= hzeta_J(i, j, k);   // :681-684
         });
         loop(tbz, [&](int i, int j, int k) {
             double mz = terrain ? hzeta_K(i, j, k) : 1.0;
@@ -1147,6 +1159,7 @@ struct Oracle {
             double q = 0.0;
             if (use_moisture) q = 0.5 * (prim(i, j, k, 4) + prim(i, j, k - 1, 4) + prim(i, j, k, 5) + prim(i, j, k - 1, 5));
             R.mz(i, j, k) += (zsrc(i, j, k) - gpz - 0.0) / (1.0 + q);
+            if (moving) R.mz(i, j, k) *= 0.5 * (detJ(i, j, k) + detJ(i, j, k - 1));   // :741-743
         });
     }
 
@@ -1340,6 +1353,23 @@ struct Oracle {
         int nq = ncomp - ERF_RHOQ1_COMP;
         if (use_moisture && nq > 0)
             do_var(ERF_RHOQ1_COMP, nq, c.moistscal_horiz_adv, c.moistscal_vert_adv, c.moistscal_horiz_upw_frac, c.moistscal_vert_upw_frac);
+        if (moving) {
+            // ERF_slow_rhs_post.cpp:467-478: detJ-weighted from the old
+            // geometry to the new one; only rho KE (and rho QKE) are clamped
+            loop(valid(CC), [&](int i, int j, int k) {
+                auto upd = [&](int n) {
+                    double tv = detJ(i, j, k) * Sold.cons(i, j, k, n) + dt * detJ(i, j, k) * R.cons(i, j, k, n);
+                    Sd.cons(i, j, k, n) = tv / g_new.detJ(i, j, k);
+                };
+                if (dd) {
+                    upd(ERF_RHOKE_COMP);
+                    Sd.cons(i, j, k, ERF_RHOKE_COMP) = std::max(Sd.cons(i, j, k, ERF_RHOKE_COMP), std::numeric_limits<double>::epsilon());
+                }
+                upd(ERF_RHOSCALAR_COMP);
+                if (use_moisture)
+                    for (int m = ERF_RHOQ1_COMP; m < ncomp; ++m) upd(m);
+            });
+        } else
         loop(valid(CC), [&](int i, int j, int k) {
             if (dd) {
                 int n = ERF_RHOKE_COMP;
@@ -1618,6 +1648,12 @@ struct Oracle {
                 znd(i, j, -1) = 2.0 * znd(i, j, 0) - znd(i, j, 1);
                 znd(i, j, nz + 1) = 2.0 * znd(i, j, nz) - znd(i, j, nz - 1);
             }
+        make_metrics();
+    }
+
+    // make_J, make_areas, make_zcc (Utils/ERF_TerrainMetrics.cpp:583-715)
+    // from the nodes in znd.
+    void make_metrics() {
         int lc[3] = {-2, -2, -1}, hc[3] = {nx + 1, ny + 1, nz};
         detJ.define(lc, hc, 1, 1.0); zcc.define(lc, hc, 1);
         int lx[3] = {-2, -2, -1}, hx[3] = {nx + 2, ny + 1, nz};
@@ -1721,6 +1757,163 @@ struct Oracle {
                         (*f[a])(i, j, k) = src[a][(size_t)(k + 1) * nx * ny + (size_t)js * nx + is];
                     }
         }
+    }
+
+    // ==================================================================
+    // Moving terrain (terrain_type Moving), no acoustic substepping.
+    // The grid is regenerated from the travelling surface wave at every
+    // geometry time the reference asks for; the base state evolves by the
+    // vertical flux that the moving grid induces.
+    // ==================================================================
+    bool moving = false;
+    double time = 0.0;                   // t_old of the step being taken
+    struct Geo { Fab znd, detJ, axA, ayA, zcc; };
+    Geo g_old, g_src, g_new;
+    Fab r0o, p0o;                        // base_state at the start of the step (r0f / p0f: base_state_new)
+    Fab zt;                              // z_t_rk on the z faces
+
+    void save_geo(Geo& g) const { g.znd = znd; g.detJ = detJ; g.axA = axA; g.ayA = ayA; g.zcc = zcc; }
+    void load_geo(const Geo& g) { znd = g.znd; detJ = g.detJ; axA = g.axA; ayA = g.ayA; zcc = g.zcc; }
+
+    // Problem::init_custom_terrain (Exec/DevTests/MovingTerrain/ERF_prob.cpp:147-200):
+    // the surface h = Ampl sin(kp x - omega t), kp = 2 pi / wavelength,
+    // omega = sqrt(g kp); then init_terrain_grid with terrain_smoothing = 2
+    // (Utils/ERF_TerrainMetrics.cpp:89-209, 501-536): over the uniform levels
+    // z_k = k dz, z(k) = z_k + (1 - z_k / z_top)^3 h, z(-1) = 2 h - z(1);
+    // lateral ghosts are the periodic images (FillBoundary), z(nz+1) the
+    // linear extrapolation.
+    void mt_grid(double t) {
+        const double PI = 3.14159265358979323846264338327950288;
+        const double kp = 2.0 * PI / c.mt_wavelength, om = std::sqrt(CONST_GRAV * kp);
+        const double ztop = nz * c.dz;
+        int l[3] = {-3, -3, -1}, h[3] = {nx + 3, ny + 3, nz + 1};
+        znd.define(l, h, 1);
+        for (int j = 0; j <= ny; ++j)
+            for (int i = 0; i <= nx; ++i) {
+                const double x = i * c.dx;
+                const double hs = c.mt_ampl * std::sin(kp * x - om * t);
+                for (int k = 0; k <= nz; ++k) {
+                    const double zl = k * c.dz;
+                    znd(i, j, k) = zl + std::pow(1. - zl / ztop, 3.0) * hs;
+                }
+                znd(i, j, 0) = hs;
+                znd(i, j, -1) = 2.0 * hs - znd(i, j, 1);
+            }
+        auto wrapn = [](int i, int n) { while (i < 0) i += n; while (i > n) i -= n; return i; };
+        for (int k = -1; k <= nz; ++k)
+            for (int j = l[1]; j <= h[1]; ++j)
+                for (int i = l[0]; i <= h[0]; ++i) {
+                    if (i >= 0 && i <= nx && j >= 0 && j <= ny) continue;
+                    int is = (i >= 0 && i <= nx) ? i : wrapn(i, nx);
+                    int js = (j >= 0 && j <= ny) ? j : wrapn(j, ny);
+                    if (is == nx && !(i >= 0 && i <= nx)) is = 0;
+                    if (js == ny && !(j >= 0 && j <= ny)) js = 0;
+                    znd(i, j, k) = znd(is, js, k);
+                }
+        for (int j = l[1]; j <= h[1]; ++j)
+            for (int i = l[0]; i <= h[0]; ++i) znd(i, j, nz + 1) = 2.0 * znd(i, j, nz) - znd(i, j, nz - 1);
+        make_metrics();
+    }
+
+    // slow_rhs_fun_pre, moving terrain (TimeIntegration/ERF_TI_slow_rhs_fun.H:55-107):
+    // the geometry at the step's old time, at the stage's source time and
+    // at the stage's new time, and z_t = (z_new - z_old) / slow_dt averaged
+    // over the four nodes of each z face, on the faces grown by one laterally.
+    void mt_stage_geometry(double t_old, double t_src, double t_new, double slow_dt) {
+        mt_grid(t_old); save_geo(g_old);
+        mt_grid(t_src); save_geo(g_src);
+        mt_grid(t_new); save_geo(g_new);
+        const double inv_dt = 1. / slow_dt;
+        const Fab &zn = g_new.znd, &zo = g_old.znd;
+        int l[3] = {-2, -2, 0}, h[3] = {nx + 1, ny + 1, nz};
+        zt.define(l, h, 1);
+        for (int k = 0; k <= nz; ++k)
+            for (int j = -1; j <= ny; ++j)
+                for (int i = -1; i <= nx; ++i)
+                    zt(i, j, k) = 0.25 * inv_dt * (zn(i + 1, j + 1, k) - zo(i + 1, j + 1, k) + zn(i, j + 1, k) - zo(i, j + 1, k)
+                                                   + zn(i + 1, j, k) - zo(i + 1, j, k) + zn(i, j, k) - zo(i, j, k));
+    }
+
+    // The base-state update of slow_rhs_fun_pre for moving terrain
+    // (ERF_TI_slow_rhs_fun.H:149-210): rho_0 and (rho theta)_0 advanced in
+    // flux form by the vertical flux -z_t (face average), detJ-weighted from
+    // the step's old base state, and p_0 re-made from (rho theta)_0.  Run
+    // after the stage's slow right-hand side, which used the base state of
+    // the previous stage.
+    void mt_base_state(double dt_base) {
+        Fab rt0, rt0n, r0t;
+        int l[3] = {-2, -2, -1}, h[3] = {nx + 1, ny + 1, nz};
+        rt0.define(l, h, 1); rt0n.define(l, h, 1); r0t.define(l, h, 1);
+        for (int k = -1; k <= nz; ++k)
+            for (int j = -1; j <= ny; ++j)
+                for (int i = -1; i <= nx; ++i) {
+                    rt0(i, j, k) = getRhoThetagivenP(p0o(i, j, k));
+                    rt0n(i, j, k) = getRhoThetagivenP(p0f(i, j, k));
+                    r0t(i, j, k) = r0f(i, j, k);
+                }
+        for (int k = 0; k < nz; ++k)
+            for (int j = -1; j <= ny; ++j)
+                for (int i = -1; i <= nx; ++i) {
+                    double fr_lo = -zt(i, j, k) * 0.5 * (r0t(i, j, k) + r0t(i, j, k - 1));
+                    double fr_hi = -zt(i, j, k + 1) * 0.5 * (r0t(i, j, k) + r0t(i, j, k + 1));
+                    double frt_lo = fr_lo * 0.5 * (rt0n(i, j, k) / r0t(i, j, k) + rt0n(i, j, k - 1) / r0t(i, j, k - 1));
+                    double frt_hi = fr_hi * 0.5 * (rt0n(i, j, k) / r0t(i, j, k) + rt0n(i, j, k + 1) / r0t(i, j, k + 1));
+                    double invdetJ = 1.0 / g_src.detJ(i, j, k);
+                    double src_r = -invdetJ * (fr_hi - fr_lo) * dxInv[2];
+                    double src_rt = -invdetJ * (frt_hi - frt_lo) * dxInv[2];
+                    double rho0_new = g_old.detJ(i, j, k) * r0o(i, j, k) + dt_base * g_src.detJ(i, j, k) * src_r;
+                    double rt0_new = g_old.detJ(i, j, k) * rt0(i, j, k) + dt_base * g_src.detJ(i, j, k) * src_rt;
+                    r0f(i, j, k) = rho0_new / g_new.detJ(i, j, k);
+                    rt0_new /= g_new.detJ(i, j, k);
+                    p0f(i, j, k) = getPgivenRTh(rt0_new);
+                }
+        // FillBoundary: lateral ghosts from the periodic images
+        for (int k = 0; k < nz; ++k)
+            for (int j = l[1]; j <= h[1]; ++j)
+                for (int i = l[0]; i <= h[0]; ++i) {
+                    if (i >= 0 && i < nx && j >= 0 && j < ny) continue;
+                    int is = ((i % nx) + nx) % nx, js = ((j % ny) + ny) % ny;
+                    r0f(i, j, k) = r0f(is, js, k);
+                    p0f(i, j, k) = p0f(is, js, k);
+                }
+    }
+
+    // no_substep_fun for moving terrain (TimeIntegration/ERF_TI_no_substep_fun.H:54-109):
+    // rho and rho theta advanced detJ-weighted (the slow right-hand side
+    // already carries the source geometry's detJ), the horizontal momenta
+    // with h_zeta at the faces, rho w with the face detJ; at the moving
+    // ground rho w follows the ground: W from Omega = rho z_t on the new grid.
+    void no_substep_mt(State& Ssum, const State& Sold, const State& F, double slow_dt) {
+        const Fab &dJo = g_old.detJ, &dJn = g_new.detJ, &Zo = g_old.znd, &Zn = g_new.znd;
+        auto hzI = [&](const Fab& Zf, int i, int j, int k) {
+            return 0.5 * dxInv[2] * (Zf(i, j, k + 1) + Zf(i, j + 1, k + 1) - Zf(i, j, k) - Zf(i, j + 1, k));
+        };
+        auto hzJ = [&](const Fab& Zf, int i, int j, int k) {
+            return 0.5 * dxInv[2] * (Zf(i, j, k + 1) + Zf(i + 1, j, k + 1) - Zf(i, j, k) - Zf(i + 1, j, k));
+        };
+        loop(valid(CC), [&](int i, int j, int k) {
+            for (int n = 0; n < 2; ++n) {
+                Ssum.cons(i, j, k, n) = dJo(i, j, k) * Sold.cons(i, j, k, n) + slow_dt * F.cons(i, j, k, n);
+                Ssum.cons(i, j, k, n) /= dJn(i, j, k);
+            }
+        });
+        loop(valid(XF), [&](int i, int j, int k) {
+            Ssum.mx(i, j, k) = (hzI(Zo, i, j, k) * Sold.mx(i, j, k) + slow_dt * F.mx(i, j, k)) / hzI(Zn, i, j, k);
+        });
+        loop(valid(YF), [&](int i, int j, int k) {
+            Ssum.my(i, j, k) = (hzJ(Zo, i, j, k) * Sold.my(i, j, k) + slow_dt * F.my(i, j, k)) / hzJ(Zn, i, j, k);
+        });
+        load_geo(g_new);
+        loop(valid(ZF), [&](int i, int j, int k) {
+            if (k == 0) {
+                double rho_on_face = Ssum.cons(i, j, k, 0);
+                Ssum.mz(i, j, k) = w_from_omega(i, j, k, rho_on_face * zt(i, j, k), Ssum.mx, Ssum.my);
+            } else {
+                double ko = 0.5 * (dJo(i, j, k) + dJo(i, j, k - 1));
+                double kn = 0.5 * (dJn(i, j, k) + dJn(i, j, k - 1));
+                Ssum.mz(i, j, k) = (ko * Sold.mz(i, j, k) + slow_dt * F.mz(i, j, k)) / kn;
+            }
+        });
     }
 
     // ComputeStrain_T (Diffusion/ERF_ComputeStrain_T.cpp:28-507): z-wall
@@ -2233,7 +2426,9 @@ struct Oracle {
         Bx b = grow(valid(ZF), ng, ng, 0);
         for (int j = b.lo[1]; j <= b.hi[1]; ++j)
             for (int i = b.lo[0]; i <= b.hi[0]; ++i) {
-                w(i, j, 0) = w_from_omega(i, j, 0, 0.0, u, v);
+                // a moving ground keeps the w of the update (the moving-terrain
+                // branch of impose_vertical_zvel_bcs sets nothing)
+                if (!moving) w(i, j, 0) = w_from_omega(i, j, 0, 0.0, u, v);
                 w(i, j, nz) = w_from_omega(i, j, nz, 0.0, u, v);
             }
     }
@@ -2387,6 +2582,7 @@ struct Oracle {
         else physbcs_w(vel_state.w, ngv);
         // S_old = {cons, V2M(old velocities)}
         S_old.cons.copy_from(Sc);
+        if (moving) { r0o = r0f; p0o = p0f; }   // base_state == base_state_new at the step's start
         // turbulent viscosity from the old velocities (strain + Smagorinsky)
         tock(5);
         if (use_turb) turbulent_viscosity(vel_state, S_old.cons, mut);
@@ -2418,6 +2614,24 @@ struct Oracle {
             double slow_dt = (nrk == 0 ? dt / 3.0 : (nrk == 1 ? dt / 2.0 : dt));
             if (nrk > 0) cons_to_prim(S_new.cons, ngc, prim, pi_stage);
             tock(5);
+            if (moving) {
+                // ERF_MRI.H:245-320 with the moving-terrain branches of
+                // slow_rhs_fun_pre / no_substep_fun / slow_rhs_fun_post; the
+                // stage times and slow_dt = new stage time - old step time
+                double t_so = nrk == 0 ? time : (nrk == 1 ? time + dt / 3.0 : time + dt / 2.0);
+                double t_sn = nrk == 0 ? time + dt / 3.0 : (nrk == 1 ? time + dt / 2.0 : time + dt);
+                double sdt = t_sn - time;
+                mt_stage_geometry(time, t_so, t_sn, sdt);
+                load_geo(g_src);
+                slow_rhs_pre(nrk, sdt, F_slow, S_new, S_scr, Vnew);
+                mt_base_state(sdt);
+                no_substep_mt(S_sum, S_old, F_slow, nsub * dtau);
+                load_geo(g_old);
+                apply_bcs(S_sum, Vnew, ngc, ngv, true, false);
+                slow_rhs_post(nrk, sdt, F_slow, S_old, S_new, S_sum, S_scr);
+                apply_bcs(S_new, Vnew, ngc, ngv, false, false);
+                continue;
+            }
             slow_rhs_pre(nrk, slow_dt, F_slow, S_new, S_scr, Vnew);
             tock(1);
             double inv_fac = 1.0 / (double)nsub;
@@ -2436,6 +2650,9 @@ struct Oracle {
             apply_bcs(S_new, Vnew, ngc, ngv, false, false);
             tock(3);
         }
+        // post_timestep (ERF.cpp:547-559): the new geometry and base state
+        // become the old ones
+        if (moving) { load_geo(g_new); time += dt; }
         // new state: cons of S_new, velocities from the last post_update
         Sc.copy_from(S_new.cons);
         vel_state.u.copy_from(Vnew.u); vel_state.v.copy_from(Vnew.v); vel_state.w.copy_from(Vnew.w);
@@ -2639,6 +2856,49 @@ int oracle_advance_terrain(const erf_b200_config* cfg, const double* z_nd, const
     store_box(o->vel_state.u, u, nx + 1, ny, nz);
     store_box(o->vel_state.v, v, nx, ny + 1, nz);
     store_box(o->vel_state.w, w, nx, ny, nz + 1);
+    return 0;
+}
+
+// Moving terrain without acoustic substepping: the grid is generated from
+// cfg's surface wave at time0 and at every geometry time after it; rho0 ..
+// th0 are the initial base state ((nz+2) planes of ny*nx).  On return
+// z_nd ((nz+1)(ny+1)(nx+1) valid nodes) holds the grid at the final time and
+// rho0_out / p0_out ((nz+2) planes) the evolved base state.
+int oracle_advance_moving_terrain(const erf_b200_config* cfg, double time0, const double* rho0, const double* p0,
+                                  const double* pi0, const double* th0, double* cons, double* u, double* v,
+                                  double* w, int nsteps, double* z_nd, double* rho0_out, double* p0_out) {
+    if (!cfg->use_terrain || cfg->terrain_type != ERF_TERRAIN_MOVING || cfg->substepping_type != ERF_SUBSTEP_NONE)
+        return 1;
+    std::unique_ptr<Oracle> o(new Oracle(*cfg));
+    int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
+    o->terrain = true;
+    o->moving = true;
+    o->time = time0;
+    o->mt_grid(time0);
+    o->set_base_terrain(rho0, p0, pi0, th0);
+    o->init_storage();
+    o->alloc(o->cons_state, CC, o->ngc, o->ncomp);
+    o->alloc_vel(o->vel_state);
+    load_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    load_box(o->vel_state.u, u, nx + 1, ny, nz);
+    load_box(o->vel_state.v, v, nx, ny + 1, nz);
+    load_box(o->vel_state.w, w, nx, ny, nz + 1);
+    for (int s = 0; s < nsteps; ++s) o->step(cfg->dt);
+    store_cc(o->cons_state, cons, nx, ny, nz, o->ncomp);
+    store_box(o->vel_state.u, u, nx + 1, ny, nz);
+    store_box(o->vel_state.v, v, nx, ny + 1, nz);
+    store_box(o->vel_state.w, w, nx, ny, nz + 1);
+    if (z_nd)
+        for (int k = 0; k <= nz; ++k)
+            for (int j = 0; j <= ny; ++j)
+                for (int i = 0; i <= nx; ++i) z_nd[((size_t)k * (ny + 1) + j) * (nx + 1) + i] = o->znd(i, j, k);
+    for (int k = -1; k <= nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                size_t q = (size_t)(k + 1) * nx * ny + (size_t)j * nx + i;
+                if (rho0_out) rho0_out[q] = o->r0f(i, j, k);
+                if (p0_out) p0_out[q] = o->p0f(i, j, k);
+            }
     return 0;
 }
 

@@ -75,3 +75,25 @@ def read_plotfile_minmax(path):
     vals = [np.array([float(x) for x in r.split(",") if x], dtype=np.float64) for r in rows]
     assert len(vals) == 2 and all(v.size == nvar for v in vals), rows
     return {"names": names, "time": time, "min": vals[0], "max": vals[1]}
+
+
+def read_plotfile_minmax_boxes(path):
+    """Names, time, the boxes and the per-FAB, per-component min / max of a
+    plotfile whose FAB data is not stored: Level_0/Cell_H lists the boxes
+    ((lo) (hi) (type)), then nfab rows of minima and nfab rows of maxima."""
+    import re
+    with open(os.path.join(path, "Header")) as fh:
+        lines = [ln.rstrip("\n") for ln in fh]
+    nvar = int(lines[1])
+    names = lines[2:2 + nvar]
+    time = float(lines[2 + nvar + 1])
+    with open(os.path.join(path, "Level_0", "Cell_H")) as fh:
+        text = fh.read()
+    boxes = [[[int(a) for a in lo.split(",")], [int(a) for a in hi.split(",")]]
+             for lo, hi in re.findall(r"\(\(([-\d,]+)\) \(([-\d,]+)\) \([-\d,]+\)\)", text)]
+    ch = [ln.strip() for ln in text.splitlines()]
+    rows = [ln for ln in ch if ln.count(",") >= nvar and not ln.startswith("FabOnDisk")]
+    vals = np.array([[float(x) for x in r.split(",") if x] for r in rows], dtype=np.float64)
+    nfab = len(boxes)
+    assert vals.shape == (2 * nfab, nvar), (vals.shape, nfab)
+    return {"names": names, "time": time, "boxes": np.array(boxes), "min": vals[:nfab], "max": vals[nfab:]}

@@ -137,3 +137,48 @@ def test_create_accepts_most_config(lib):
     assert rc in (0, 2)
     if rc == 0:
         lib.erf_b200_destroy(ctx)
+
+
+@pytest.mark.parametrize("change", ["static_flag", "substeps", "moist", "les", "molec", "upwind", "buoyancy",
+                                    "noslip", "wavelength", "bad_type"])
+def test_create_rejects_unsupported_moving_terrain(lib, change):
+    """Moving terrain is accepted as the reference's MovingTerrain problem
+    runs it: dry, no diffusion, Centered_2nd dycore, buoyancy type 1, slip
+    walls, one update per RK stage; the rest is refused before any CUDA call."""
+    from erf_b200 import terrain as T
+    c = T.moving_terrain(nx=8, ny=4, nz=10).cfg
+    if change == "static_flag":
+        c.use_terrain = 0
+    elif change == "substeps":
+        c.substepping_type = C.SUBSTEP_IMPLICIT
+    elif change == "moist":
+        c.moisture, c.ncomp = C.MOIST_KESSLER, 8
+    elif change == "les":
+        c.les_type = C.LES_SMAGORINSKY
+    elif change == "molec":
+        c.molec_diff_type = C.MOLEC_CONSTANT
+    elif change == "upwind":
+        c.dycore_horiz_adv = C.UPWIND_3RD
+    elif change == "buoyancy":
+        c.buoyancy_type = 2
+    elif change == "noslip":
+        c.zlo_bc = C.BC_NO_SLIP_WALL
+    elif change == "wavelength":
+        c.mt_wavelength = 0.0
+    elif change == "bad_type":
+        c.terrain_type = 2
+    ctx = ctypes.c_void_p()
+    lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
+    assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
+
+
+def test_create_accepts_moving_terrain_config(lib):
+    from erf_b200 import terrain as T
+    c = T.moving_terrain(nx=8, ny=4, nz=10).cfg
+    ctx = ctypes.c_void_p()
+    lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
+    lib.erf_b200_destroy.argtypes = [ctypes.c_void_p]
+    rc = lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None)
+    assert rc in (0, 2)
+    if rc == 0:
+        lib.erf_b200_destroy(ctx)

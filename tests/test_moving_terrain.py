@@ -1,0 +1,107 @@
+"""Moving terrain (terrain_type Moving) without acoustic substepping: the
+oracle pinned to the reference's gold MovingTerrain_nosub
+(Tests/test_files/MovingTerrain_nosub/MovingTerrain_nosub.i with
+Exec/DevTests/MovingTerrain/ERF_prob.cpp; only the plotfile's header is kept
+upstream, so the per-box min / max of Level_0/Cell_H), and the case
+builder's own pieces (grid, base state, initial wave).
+
+The gold's z_velocity is matched to 1.1e-8 relative, every other field to
+<= 1e-12: the ground-face w of the reference run differs from the one
+W-from-Omega gives on the new grid by about 2e-8 relative while the momenta
+and the density (which that w feeds) agree to round-off, so the tolerance
+of that one field is 2e-8.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from erf_b200 import terrain as T
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def plot_fields_mt(cfg, cons, u, v, w, z_nd, rho0, p0):
+    """The plotfile variables of the gold (IO/ERF_Plotfile.cpp): cell-centred
+    velocities, pressure and theta from the dry EOS, the base state, z at
+    the cell centres and detJ of the final grid."""
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    z = z_nd
+    dzi = 1.0 / cfg.dz
+    detJ = 0.25 * dzi * (z[1:, :-1, :-1] + z[1:, :-1, 1:] + z[1:, 1:, :-1] + z[1:, 1:, 1:]
+                         - z[:-1, :-1, :-1] - z[:-1, :-1, 1:] - z[:-1, 1:, :-1] - z[:-1, 1:, 1:])
+    pres = 1.0e5 * (287.0 * cons[1] / 1.0e5) ** 1.4
+    return {"density": cons[0], "x_velocity": 0.5 * (u[:, :, :-1] + u[:, :, 1:]),
+            "y_velocity": 0.5 * (v[:, :-1] + v[:, 1:]), "z_velocity": 0.5 * (w[:-1] + w[1:]),
+            "pressure": pres, "theta": cons[1] / cons[0],
+            "pres_hse": p0.reshape(nz + 2, ny, nx)[1:nz + 1], "dens_hse": rho0.reshape(nz + 2, ny, nx)[1:nz + 1],
+            "z_phys": T.cell_heights(z), "detJ": detJ}
+
+
+def gold_box_errors(gold, f):
+    """Per (box, field, min / max): |got - gold| / max(1, |gold|)."""
+    out = {}
+    for b, (lo, hi) in enumerate(gold["boxes"]):
+        sl = np.s_[:, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
+        for q, nm in enumerate(gold["names"]):
+            a = f[str(nm)][sl]
+            for tag, val, ref in (("min", a.min(), gold["vmin"][b, q]), ("max", a.max(), gold["vmax"][b, q])):
+                out[(b, str(nm), tag)] = abs(val - ref) / max(1.0, abs(ref))
+    return out
+
+
+def test_case_builder_grid_and_base_state():
+    case = T.moving_terrain()
+    cfg = case.cfg
+    z = case.z_nd
+    # the surface is the wave at t = 0, the lid flat at z_top
+    x = np.arange(cfg.nx + 1) * cfg.dx
+    np.testing.assert_allclose(z[0, 0], 0.16 * np.sin(2 * math.pi / 100.0 * x), rtol=0, atol=1e-15)
+    assert np.all(z[-1] == cfg.nz * cfg.dz)
+    # hydrostatic: the enforce_hse recursion holds exactly, and theta is 300
+    r0, p0 = (b.reshape(cfg.nz + 2, cfg.ny, cfg.nx) for b in case.base[:2])
+    zc = T.cell_heights(np.concatenate([z, (2 * z[-1] - z[-2])[None]], axis=0))
+    lhs = p0[2:] - p0[1:-1]
+    rhs = -(zc[1:] - zc[:-1]) * 0.5 * (r0[2:] + r0[1:-1]) * 9.81
+    np.testing.assert_allclose(lhs, rhs, rtol=1e-12)
+    th0 = case.base[3].reshape(cfg.nz + 2, cfg.ny, cfg.nx)[1:-1]
+    np.testing.assert_allclose(th0, 300.0, rtol=1e-7)
+
+
+def test_oracle_reproduces_moving_terrain_nosub_gold():
+    case = T.moving_terrain()
+    cfg = case.cfg
+    gold = np.load(os.path.join(HERE, "golden", "MovingTerrain_nosub_minmax.npz"))
+    assert abs(float(gold["time"]) - case.steps * cfg.dt) < 1e-12
+    cons, u, v, w = case.build_state()
+    out = oracle.advance_moving_terrain(cfg, 0.0, case.base, cons, u, v, w, case.steps)
+    f = plot_fields_mt(cfg, *out)
+    errs = gold_box_errors(gold, f)
+    worst = {}
+    for (b, nm, tag), e in errs.items():
+        worst[nm] = max(worst.get(nm, 0.0), e)
+    print(worst)
+    for nm, e in worst.items():
+        tol = 2e-8 if nm == "z_velocity" else 2e-10
+        assert e <= tol, (nm, e)
+    # the wave moved: the final grid is the surface at t = 0.1 s
+    kp = 2 * math.pi / 100.0
+    om = math.sqrt(9.81 * kp)
+    x = np.arange(cfg.nx + 1) * cfg.dx
+    np.testing.assert_allclose(out[4][0, 0], 0.16 * np.sin(kp * x - om * 0.1), rtol=0, atol=1e-14)
+
+
+def test_oracle_moving_terrain_restart_is_seamless():
+    """Two calls of 3 steps from the returned state, time and base state
+    equal one call of 6 steps (the geometry depends on time only)."""
+    case = T.moving_terrain(nx=10, ny=2, nz=20, Lx=50.0, Ly=10.0, H=100.0, ampl=0.3, wavelength=50.0)
+    cfg = case.cfg
+    st = case.build_state()
+    a = oracle.advance_moving_terrain(cfg, 0.0, case.base, *st, 6)
+    b1 = oracle.advance_moving_terrain(cfg, 0.0, case.base, *st, 3)
+    base_mid = [b1[5], b1[6], case.base[2], case.base[3]]
+    b2 = oracle.advance_moving_terrain(cfg, 3 * cfg.dt, base_mid, *b1[:4], 3)
+    for x, y in zip(a, b2):
+        np.testing.assert_allclose(x, y, rtol=1e-13, atol=1e-15)
