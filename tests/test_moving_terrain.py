@@ -5,11 +5,14 @@ Exec/DevTests/MovingTerrain/ERF_prob.cpp; only the plotfile's header is kept
 upstream, so the per-box min / max of Level_0/Cell_H), and the case
 builder's own pieces (grid, base state, initial wave).
 
-The gold's z_velocity is matched to 1.1e-8 relative, every other field to
-<= 1e-12: the ground-face w of the reference run differs from the one
-W-from-Omega gives on the new grid by about 2e-8 relative while the momenta
-and the density (which that w feeds) agree to round-off, so the tolerance
-of that one field is 2e-8.
+Each min / max is compared as |got - gold| / max(1, |gold|) (the
+fcompare-style bound 2e-10 of Tests/CMakeLists.txt:3-4).  Every field
+meets it to <= 1e-13 except z_velocity, off by 1.1e-9 (1.1e-8 of its
+0.1 m/s extremes, which sit in the first cell above the moving ground):
+the ground-face w of the reference run differs from the one W-from-Omega
+gives on the new grid by about 2e-8 relative while the momenta and the
+density (which that w feeds) agree to round-off; that one field is held
+to 3e-9.
 """
 import math
 import os
@@ -84,7 +87,7 @@ def test_oracle_reproduces_moving_terrain_nosub_gold():
         worst[nm] = max(worst.get(nm, 0.0), e)
     print(worst)
     for nm, e in worst.items():
-        tol = 2e-8 if nm == "z_velocity" else 2e-10
+        tol = 3e-9 if nm == "z_velocity" else 2e-10
         assert e <= tol, (nm, e)
     # the wave moved: the final grid is the surface at t = 0.1 s
     kp = 2 * math.pi / 100.0

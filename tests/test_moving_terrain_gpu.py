@@ -5,7 +5,8 @@ MovingTerrain_nosub (per-box min / max of the final plotfile).
 Bars: relative L2 <= 1e-10 per field after 20 steps against the oracle
 (v, which is round-off around zero in this 2-D wave, by its absolute
 difference), the evolved base state and the final grid likewise; the gold
-as the oracle meets it (z_velocity 2e-8, the rest 2e-10); a run split over
+as the oracle meets it (z_velocity 3e-9, the rest 2e-10, as
+|got - gold| / max(1, |gold|)); a run split over
 two calls equal to one call (the device clock carries the time); the mixed
 form within 1e-3 of FP64.
 """
@@ -79,7 +80,7 @@ def test_moving_terrain_matches_oracle_and_gold():
         worst[nm] = max(worst.get(nm, 0.0), e)
     print("vs gold:", worst)
     for nm, e in worst.items():
-        assert e <= (2e-8 if nm == "z_velocity" else 2e-10), (nm, e)
+        assert e <= (3e-9 if nm == "z_velocity" else 2e-10), (nm, e)
 
 
 def test_moving_terrain_split_run_equals_one_run():
