@@ -62,7 +62,8 @@ class ErfConfig(ctypes.Structure):
         ("use_terrain", ctypes.c_int),
         ("substepping_type", ctypes.c_int),
         ("terrain_type", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("no_lagged_delta_rt", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
         ("most_z0", ctypes.c_double), ("most_zref", ctypes.c_double),
         ("mt_ampl", ctypes.c_double), ("mt_wavelength", ctypes.c_double),
     ]
@@ -178,6 +179,8 @@ def from_inputs(keys: dict) -> ErfConfig:
     tt = g("terrain_type")
     if tt is not None:
         c.terrain_type = {"Static": TERRAIN_STATIC, "Moving": TERRAIN_MOVING}[str(tt).strip('"')]
+    if g("use_lagged_delta_rt") is not None:
+        c.no_lagged_delta_rt = 0 if str(g("use_lagged_delta_rt")).lower() in ("1", "true") else 1
     if keys.get("prob.Ampl") is not None:
         c.mt_ampl = float(keys["prob.Ampl"])
     st = g("substepping_type")

@@ -354,7 +354,7 @@ def moving_terrain(nx=40, ny=8, nz=79, Lx=200.0, Ly=40.0, H=400.0, ampl=0.16, wa
     200 m x 40 m x 400 m, periodic x / y, slip walls, Centered_2nd everywhere,
     no diffusion, gravity with buoyancy type 1, moving terrain with Sullivan
     smoothing, Ampl 0.16 m.  Without substepping dt = 0.005 s for 20 steps;
-    with it dt = 0.1 s, ratio 20, 10 steps."""
+    with it dt = 0.1 s, ratio 20, 10 steps, use_lagged_delta_rt = false."""
     c = C.defaults()
     c.nx, c.ny, c.nz = nx, ny, nz
     c.dx, c.dy, c.dz = Lx / nx, Ly / ny, H / nz
@@ -372,6 +372,7 @@ def moving_terrain(nx=40, ny=8, nz=79, Lx=200.0, Ly=40.0, H=400.0, ampl=0.16, wa
     if substeps:
         c.substepping_type = C.SUBSTEP_IMPLICIT
         c.dt, c.mri_ratio = (0.1 if dt is None else dt), 20
+        c.no_lagged_delta_rt = 1       # erf.use_lagged_delta_rt = false
         nsteps = 10 if steps is None else steps
         name = "MovingTerrain_sub"
     else:

@@ -183,7 +183,13 @@ typedef struct erf_b200_config {
      * Sullivan's factor (1 - z/z_top)^3 (terrain_smoothing = 2,
      * Utils/ERF_TerrainMetrics.cpp:501-536) over the uniform levels k dz */
     int    terrain_type;
-    int    reserved[4];
+    /* SolverChoice::use_lagged_delta_rt = false (1 here; 0 keeps the
+     * reference default, true): the acoustic substeps over moving terrain
+     * then extrapolate d(rho theta) without the lagged correction
+     * (ERF_fast_rhs_MT.cpp:197-210); the reference allows it for moving
+     * terrain only (ERF_DataStruct.H:389) */
+    int    no_lagged_delta_rt;
+    int    reserved[3];
     /* MOST surface layer for zlo_bc ERF_BC_MOST (ABLMost, erf.most.*): the
      * roughness length z0 and the reference height zref (moved to the
      * centre of the cell level that contains it, as MOSTAverage does); Moeng

@@ -1533,7 +1533,19 @@ struct Oracle {
     double P0(int i, int j, int k) const { return terrain ? p0f(i, j, k) : p0[k + 1]; }
     double PI0(int i, int j, int k) const { return terrain ? pi0f(i, j, k) : pi0[k + 1]; }
 
-    double Z(int i, int j, int k) const { return znd(i, j, k); }
+    // the nodes the metric terms read: the current grid, or another one for
+    // the length of an on() call (moving terrain mixes several grids); per
+    // thread, since on() runs inside the OpenMP loops
+    static inline thread_local const Fab* zsel = nullptr;
+    double Z(int i, int j, int k) const { return zsel ? (*zsel)(i, j, k) : znd(i, j, k); }
+    template <class F>
+    double on(const Fab& zf, F f) {
+        const Fab* s = zsel;
+        zsel = &zf;
+        double r = f();
+        zsel = s;
+        return r;
+    }
     double hzeta_cc(int i, int j, int k) const {
         return 0.25 * dxInv[2] * (Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k + 1) + Z(i, j, k + 1) + Z(i, j + 1, k + 1)
                                   - Z(i + 1, j, k) - Z(i + 1, j + 1, k) - Z(i, j, k) - Z(i, j + 1, k));
@@ -1913,6 +1925,172 @@ struct Oracle {
                 double kn = 0.5 * (dJn(i, j, k) + dJn(i, j, k - 1));
                 Ssum.mz(i, j, k) = (ko * Sold.mz(i, j, k) + slow_dt * F.mz(i, j, k)) / kn;
             }
+        });
+    }
+
+    // erf_fast_rhs_MT (TimeIntegration/ERF_fast_rhs_MT.cpp:48-626): one
+    // acoustic substep over moving terrain.  Go / Gn: the grids at the
+    // substep's old and new times, Gs: the stage's (source) grid; zt: z_t of
+    // the stage, zpt: the substep's z_t less it.  The horizontal momenta are
+    // advanced h_zeta-weighted, rho w through the column solve on the
+    // perturbation of Omega, rho and rho theta detJ-weighted old -> new.
+    void fast_rhs_MT(int step, const State& Rs, const State& Sprev_in, const State& Sst, State& Sd, State& Scr,
+                     const Geo& Go, const Geo& Gn, const Geo& Gs, const Fab& zpt, double dtau, double beta_s,
+                     double facinv) {
+        State Sprev; alloc_state(Sprev); copy_state(Sprev, Sprev_in);
+        const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s), beta_d = 0.1;
+        const double dxi = dxInv[0], dyi = dxInv[1], dzi = dxInv[2];
+        const bool lagged = c.no_lagged_delta_rt == 0;
+        const Fab &dJo = Go.detJ, &dJn = Gn.detJ, &dJs = Gs.detJ;
+        Fab extrap, trhs, om;
+        alloc(extrap, CC, 1, 1); alloc(trhs, CC, 0, 2); alloc(om, ZF, 0, 1);
+        Fab& lag = Scr.cons;
+        Fab& cur = Sd.cons;
+        loop(grow(valid(CC), 1, 1, 1), [&](int i, int j, int k) {
+            if (step == 0) {
+                cur(i, j, k, 0) = Sprev.cons(i, j, k, 0);
+                cur(i, j, k, 1) = Sprev.cons(i, j, k, 1);
+                double d = cur(i, j, k, 1) - Sst.cons(i, j, k, 1);
+                extrap(i, j, k) = d;
+                lag(i, j, k, 1) = d;
+            } else if (lagged) {
+                double d = cur(i, j, k, 1) - Sst.cons(i, j, k, 1);
+                extrap(i, j, k) = d + beta_d * (d - lag(i, j, k, 1));
+                lag(i, j, k, 1) = d;
+            } else {
+                extrap(i, j, k) = cur(i, j, k, 1) - Sst.cons(i, j, k, 1);
+            }
+        });
+        // horizontal momenta, h_zeta-weighted on the old grid
+        loop(valid(XF), [&](int i, int j, int k) {
+            double hxi = on(Go.znd, [&] { return hxi_I(i, j, k); }), hz = on(Go.znd, [&] { return hzeta_I(i, j, k); });
+            double gp_xi = (extrap(i, j, k) - extrap(i - 1, j, k)) * dxi;
+            double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k) - extrap(i, j, k))
+                                      : 0.25 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k - 1) - extrap(i, j, k - 1));
+            double gpx = hz * gp_xi - hxi * gp_zeta;
+            gpx *= 1.0;
+            double pi_c = 0.5 * (pi_stage(i - 1, j, k) + pi_stage(i, j, k));
+            double f = -Gamma_ * R_d * pi_c * gpx;
+            Sd.mx(i, j, k) = hz * Sprev.mx(i, j, k) + dtau * f + dtau * Rs.mx(i, j, k);
+        });
+        loop(valid(YF), [&](int i, int j, int k) {
+            double het = on(Go.znd, [&] { return heta_J(i, j, k); }), hz = on(Go.znd, [&] { return hzeta_J(i, j, k); });
+            double gp_eta = (extrap(i, j, k) - extrap(i, j - 1, k)) * dyi;
+            double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k) - extrap(i, j - 1, k))
+                                      : 0.25 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k - 1) - extrap(i, j - 1, k - 1));
+            double gpy = hz * gp_eta - het * gp_zeta;
+            gpy *= 1.0;
+            double pi_c = 0.5 * (pi_stage(i, j - 1, k) + pi_stage(i, j, k));
+            double f = -Gamma_ * R_d * pi_c * gpy;
+            Sd.my(i, j, k) = hz * Sprev.my(i, j, k) + dtau * f + dtau * Rs.my(i, j, k);
+        });
+        // horizontal fluxes of rho and rho theta: the weighted momenta less
+        // the stage's on the stage grid
+        loop(valid(CC), [&](int i, int j, int k) {
+            double hxl = on(Gs.znd, [&] { return hzeta_I(i, j, k); }), hxh = on(Gs.znd, [&] { return hzeta_I(i + 1, j, k); });
+            double hyl = on(Gs.znd, [&] { return hzeta_J(i, j, k); }), hyh = on(Gs.znd, [&] { return hzeta_J(i, j + 1, k); });
+            double xl = Sd.mx(i, j, k) - Sst.mx(i, j, k) * hxl, xh = Sd.mx(i + 1, j, k) - Sst.mx(i + 1, j, k) * hxh;
+            double yl = Sd.my(i, j, k) - Sst.my(i, j, k) * hyl, yh = Sd.my(i, j + 1, k) - Sst.my(i, j + 1, k) * hyh;
+            trhs(i, j, k, 0) = (xh - xl) * dxi + (yh - yl) * dyi;
+            trhs(i, j, k, 1) = ((xh * (prim(i, j, k, 0) + prim(i + 1, j, k, 0)) - xl * (prim(i, j, k, 0) + prim(i - 1, j, k, 0))) * dxi +
+                                (yh * (prim(i, j, k, 0) + prim(i, j + 1, k, 0)) - yl * (prim(i, j, k, 0) + prim(i, j - 1, k, 0))) * dyi) * 0.5;
+        });
+        // Omega'' of the previous substep on the old grid.  After the first
+        // substep the reference passes one state as both the previous and the
+        // new one, so the horizontal momenta read here are this substep's
+        // (h_zeta-weighted, not yet divided); rho w is still the previous one.
+        const Fab& pmx = step == 0 ? Sprev.mx : Sd.mx;
+        const Fab& pmy = step == 0 ? Sprev.my : Sd.my;
+        loop(valid(ZF), [&](int i, int j, int k) {
+            if (k == 0) om(i, j, k) = 0.;
+            else if (k == nz) om(i, j, k) = Sprev.mz(i, j, k) - Sst.mz(i, j, k) - zpt(i, j, k);
+            else {
+                double a = on(Go.znd, [&] { return omega_from_w(i, j, k, Sprev.mz(i, j, k), pmx, pmy); });
+                double b = on(Go.znd, [&] { return omega_from_w(i, j, k, Sst.mz(i, j, k), Sst.mx, Sst.my); });
+                om(i, j, k) = (a - b) - zpt(i, j, k);
+            }
+        });
+        Fab& avx = Scr.mx; Fab& avy = Scr.my; Fab& avz = Scr.mz;
+        loop(valid(XF), [&](int i, int j, int k) {
+            Sd.mx(i, j, k) /= on(Gn.znd, [&] { return hzeta_I(i, j, k); });
+            avx(i, j, k) += facinv * (Sd.mx(i, j, k) - Sst.mx(i, j, k));
+        });
+        loop(valid(YF), [&](int i, int j, int k) {
+            Sd.my(i, j, k) /= on(Gn.znd, [&] { return hzeta_J(i, j, k); });
+            avy(i, j, k) += facinv * (Sd.my(i, j, k) - Sst.my(i, j, k));
+        });
+        // the column system for the perturbation of Omega
+        const double halfg = std::abs(0.5 * -c.gravity);
+        const Fab& fc = fast_coeffs;
+        Fab RHS, soln; alloc(RHS, ZF, 0, 1); alloc(soln, ZF, 0, 1);
+        Bx bs = valid(CC); bs.lo[2] = 1; bs.hi[2] = nz - 1;
+        loop(bs, [&](int i, int j, int k) {
+            double Jo = 0.5 * (dJo(i, j, k) + dJo(i, j, k - 1));
+            double Jn = 0.5 * (dJn(i, j, k) + dJn(i, j, k - 1));
+            double Js = 0.5 * (dJs(i, j, k) + dJs(i, j, k - 1));
+            double cP = fc(i, j, k, 3), cQ = fc(i, j, k, 4);
+            double tlo = 0.5 * (prim(i, j, k - 2, 0) + prim(i, j, k - 1, 0));
+            double tmid = 0.5 * (prim(i, j, k - 1, 0) + prim(i, j, k, 0));
+            double thi = 0.5 * (prim(i, j, k, 0) + prim(i, j, k + 1, 0));
+            double R0t = cP * cur(i, j, k, 1) * Jo + cQ * cur(i, j, k - 1, 1) * Jo
+                         - cP * Sst.cons(i, j, k, 1) * Js - cQ * Sst.cons(i, j, k - 1, 1) * Js
+                         - halfg * (cur(i, j, k, 0) + cur(i, j, k - 1, 0)) * Jo
+                         + halfg * (Sst.cons(i, j, k, 0) + Sst.cons(i, j, k - 1, 0)) * Js;
+            double R1t = -halfg * (Rs.cons(i, j, k, 0) + Rs.cons(i, j, k - 1, 0))
+                         + (cP * Rs.cons(i, j, k, 1) + cQ * Rs.cons(i, j, k - 1, 1));
+            double Okp1 = om(i, j, k + 1), Ok = om(i, j, k), Okm1 = om(i, j, k - 1);
+            R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + trhs(i, j, k, 0) + trhs(i, j, k - 1, 0));
+            R1t += -(cP * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + trhs(i, j, k, 1)) +
+                     cQ * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + trhs(i, j, k - 1, 1)));
+            RHS(i, j, k) = Jo * Sprev.mz(i, j, k) - Js * Sst.mz(i, j, k) + dtau * (Rs.mz(i, j, k) + R0t + dtau * beta_2 * R1t);
+            double un = on(Gn.znd, [&] { return omega_from_w(i, j, k, 0., Sd.mx, Sd.my); });
+            double us = on(Gs.znd, [&] { return omega_from_w(i, j, k, 0., Sst.mx, Sst.my); });
+            double UppVpp = Jn * un - Js * us;
+            RHS(i, j, k) += UppVpp;
+        });
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                double rho_on_bdy = 0.5 * (Sprev.cons(i, j, 0, 0) + Sprev.cons(i, j, -1, 0));
+                RHS(i, j, 0) = rho_on_bdy * zpt(i, j, 0);
+                soln(i, j, 0) = RHS(i, j, 0) * fc(i, j, 0, 1);
+                RHS(i, j, nz) = 0.0;
+                for (int k = 1; k <= nz; ++k) soln(i, j, k) = (RHS(i, j, k) - fc(i, j, k, 0) * soln(i, j, k - 1)) * fc(i, j, k, 1);
+                for (int k = nz - 1; k >= 0; --k) soln(i, j, k) -= (fc(i, j, k, 2) * fc(i, j, k, 1)) * soln(i, j, k + 1);
+                Sd.mz(i, j, nz) = Sst.mz(i, j, nz) + soln(i, j, nz);
+            }
+        // the new rho w; on the moving ground W from Omega = rho (z_t + z_t'')
+        Bx bw = valid(ZF); bw.hi[2] = nz - 1;
+        loop(bw, [&](int i, int j, int k) {
+            double rho_on_face = 0.5 * (cur(i, j, k, 0) + cur(i, j, k - 1, 0));
+            if (k == 0) {
+                Sd.mz(i, j, k) = on(Gn.znd, [&] { return w_from_omega(i, j, k, rho_on_face * (zt(i, j, k) + zpt(i, j, k)), Sd.mx, Sd.my); });
+                soln(i, j, k) = 0.;
+            } else {
+                double wn = on(Gn.znd, [&] { return w_from_omega(i, j, k, 0.0, Sd.mx, Sd.my); });
+                double ws = on(Gs.znd, [&] { return w_from_omega(i, j, k, 0.0, Sst.mx, Sst.my); });
+                double wpp = soln(i, j, k) + (wn - ws);
+                double Jo = 0.5 * (dJo(i, j, k) + dJo(i, j, k - 1));
+                double Jn = 0.5 * (dJn(i, j, k) + dJn(i, j, k - 1));
+                Sd.mz(i, j, k) = Jo * (Sst.mz(i, j, k) + wpp);
+                Sd.mz(i, j, k) /= Jn;
+                double a = on(Gn.znd, [&] { return omega_from_w(i, j, k, Sd.mz(i, j, k), Sd.mx, Sd.my); });
+                double b = on(Gs.znd, [&] { return omega_from_w(i, j, k, Sst.mz(i, j, k), Sst.mx, Sst.my); });
+                soln(i, j, k) = a - b;
+                soln(i, j, k) -= rho_on_face * zpt(i, j, k);
+            }
+        });
+        // rho and rho theta, detJ-weighted old -> new
+        loop(valid(CC), [&](int i, int j, int k) {
+            double zl = beta_2 * soln(i, j, k) + beta_1 * om(i, j, k);
+            double zh = beta_2 * soln(i, j, k + 1) + beta_1 * om(i, j, k + 1);
+            avz(i, j, k) += facinv * zl / (1.0 * 1.0);
+            if (k == nz - 1) avz(i, j, k + 1) += facinv * zh / (1.0 * 1.0);
+            double frho = -(trhs(i, j, k, 0) + (zh - zl) * dzi);
+            double tr = dJo(i, j, k) * cur(i, j, k, 0) + dtau * (Rs.cons(i, j, k, 0) + frho);
+            cur(i, j, k, 0) = tr / dJn(i, j, k);
+            double frt = -(trhs(i, j, k, 1) + 0.5 * (zh * (prim(i, j, k, 0) + prim(i, j, k + 1, 0)) - zl * (prim(i, j, k, 0) + prim(i, j, k - 1, 0))) * dzi);
+            double tt = dJo(i, j, k) * cur(i, j, k, 1) + dtau * (Rs.cons(i, j, k, 1) + frt);
+            cur(i, j, k, 1) = tt / dJn(i, j, k);
         });
     }
 
@@ -2625,9 +2803,41 @@ struct Oracle {
                 load_geo(g_src);
                 slow_rhs_pre(nrk, sdt, F_slow, S_new, S_scr, Vnew);
                 mt_base_state(sdt);
-                no_substep_mt(S_sum, S_old, F_slow, nsub * dtau);
-                load_geo(g_old);
-                apply_bcs(S_sum, Vnew, ngc, ngv, true, false);
+                if (nosub) {
+                    no_substep_mt(S_sum, S_old, F_slow, nsub * dtau);
+                    load_geo(g_old);
+                    apply_bcs(S_sum, Vnew, ngc, ngv, true, false);
+                } else {
+                    // fast_rhs_fun, moving terrain (ERF_TI_fast_rhs_fun.H:47-118):
+                    // per substep the grids at its old and new times, z_t'' = the
+                    // substep's z_t less the stage's, the fast coefficients on the
+                    // old grid with the step's old base state, then the boundary
+                    // fill on the old grid; the level keeps the last substep's
+                    // old grid and the new grid is the last substep's new one.
+                    Geo g_stg = g_src, g_so, g_sn;
+                    Fab zpt; zpt.define(zt.lo, zt.hi, 1);
+                    for (int ks = 0; ks < nsub; ++ks) {
+                        mt_grid(time + ks * dtau); save_geo(g_so);
+                        mt_grid(time + (ks + 1) * dtau); save_geo(g_sn);
+                        const double inv_dt = 1. / dtau;
+                        for (int k = 0; k <= nz; ++k)
+                            for (int j = -1; j <= ny; ++j)
+                                for (int i = -1; i <= nx; ++i) {
+                                    const Fab &zn = g_sn.znd, &zo = g_so.znd;
+                                    zpt(i, j, k) = 0.25 * inv_dt * (zn(i + 1, j + 1, k) - zo(i + 1, j + 1, k) + zn(i, j + 1, k) - zo(i, j + 1, k)
+                                                                    + zn(i + 1, j, k) - zo(i + 1, j, k) + zn(i, j, k) - zo(i, j, k));
+                                    zpt(i, j, k) -= zt(i, j, k);
+                                }
+                        load_geo(g_so);
+                        std::swap(r0f, r0o);   // make_fast_coeffs reads base_state, not base_state_new
+                        make_fast_coeffs(S_new, dtau, beta_s);
+                        std::swap(r0f, r0o);
+                        fast_rhs_MT(ks, F_slow, ks == 0 ? S_old : S_sum, S_new, S_sum, S_scr, g_so, g_sn, g_stg, zpt,
+                                    dtau, beta_s, 1.0 / (double)nsub);
+                        apply_bcs(S_sum, Vnew, 1, 1, true, false);
+                    }
+                    g_new = g_sn;
+                }
                 slow_rhs_post(nrk, sdt, F_slow, S_old, S_new, S_sum, S_scr);
                 apply_bcs(S_new, Vnew, ngc, ngv, false, false);
                 continue;
@@ -2859,7 +3069,7 @@ int oracle_advance_terrain(const erf_b200_config* cfg, const double* z_nd, const
     return 0;
 }
 
-// Moving terrain without acoustic substepping: the grid is generated from
+// Moving terrain (with or without acoustic substepping): the grid is generated from
 // cfg's surface wave at time0 and at every geometry time after it; rho0 ..
 // th0 are the initial base state ((nz+2) planes of ny*nx).  On return
 // z_nd ((nz+1)(ny+1)(nx+1) valid nodes) holds the grid at the final time and
@@ -2867,8 +3077,7 @@ int oracle_advance_terrain(const erf_b200_config* cfg, const double* z_nd, const
 int oracle_advance_moving_terrain(const erf_b200_config* cfg, double time0, const double* rho0, const double* p0,
                                   const double* pi0, const double* th0, double* cons, double* u, double* v,
                                   double* w, int nsteps, double* z_nd, double* rho0_out, double* p0_out) {
-    if (!cfg->use_terrain || cfg->terrain_type != ERF_TERRAIN_MOVING || cfg->substepping_type != ERF_SUBSTEP_NONE)
-        return 1;
+    if (!cfg->use_terrain || cfg->terrain_type != ERF_TERRAIN_MOVING) return 1;
     std::unique_ptr<Oracle> o(new Oracle(*cfg));
     int nz = cfg->nz, nx = cfg->nx, ny = cfg->ny;
     o->terrain = true;

@@ -108,3 +108,20 @@ def test_oracle_moving_terrain_restart_is_seamless():
     b2 = oracle.advance_moving_terrain(cfg, 3 * cfg.dt, base_mid, *b1[:4], 3)
     for x, y in zip(a, b2):
         np.testing.assert_allclose(x, y, rtol=1e-13, atol=1e-15)
+
+
+def test_oracle_reproduces_moving_terrain_sub_gold():
+    """Tests/test_files/MovingTerrain_sub/MovingTerrain_sub.i: 10 steps of
+    0.1 s, 20 acoustic substeps (erf_fast_rhs_MT), use_lagged_delta_rt =
+    false; every field of the gold to <= 1e-11."""
+    case = T.moving_terrain(substeps=True)
+    cfg = case.cfg
+    gold = np.load(os.path.join(HERE, "golden", "MovingTerrain_sub_minmax.npz"))
+    assert abs(float(gold["time"]) - case.steps * cfg.dt) < 1e-12
+    out = oracle.advance_moving_terrain(cfg, 0.0, case.base, *case.build_state(), case.steps)
+    worst = {}
+    for (b, nm, tag), e in gold_box_errors(gold, plot_fields_mt(cfg, *out)).items():
+        worst[nm] = max(worst.get(nm, 0.0), e)
+    print(worst)
+    for nm, e in worst.items():
+        assert e <= 2e-10, (nm, e)
