@@ -82,11 +82,12 @@ struct erf_b200_ctx {
     // met / detJ / zcc) and at the stage's source (z[1], with met1 / detJ1 /
     // zcc1) and new (z[2]) times; z_t; the step's old base state; the clock
     struct MovingTerrain {
-        double* z[3];
+        double* z[5];                  // + the substep's old and new grids
         double *met1, *detJ1, *zcc1;
         double* zt;
         double *r0o, *p0o;
         double* time;
+        double *detJso, *zpt, *trhs, *om;   // acoustic substeps
     } mt{};
     int ter_tx = 0;                                           // k_ter_fast_vert columns per block
     size_t ter_smem = 0;                                      // and its shared memory
@@ -186,8 +187,10 @@ int validate(const erf_b200_config* c) {
     if (c->terrain_type == ERF_TERRAIN_MOVING) {
         // moving terrain: the reference's MovingTerrain setting -- dry,
         // Centered_2nd dycore (asserted by slow_rhs_fun_pre), no diffusion,
-        // buoyancy type 1, slip walls, one update per RK stage
-        if (!c->use_terrain || c->substepping_type != ERF_SUBSTEP_NONE) return ERF_B200_ECONFIG;
+        // buoyancy type 1, slip walls; with acoustic substepping up to 512
+        // levels (the column kernel's local solution)
+        if (!c->use_terrain) return ERF_B200_ECONFIG;
+        if (c->substepping_type == ERF_SUBSTEP_IMPLICIT && c->nz > 512) return ERF_B200_ECONFIG;
         if (c->moisture != ERF_MOIST_NONE || c->les_type != ERF_LES_NONE || c->molec_diff_type != ERF_MOLEC_NONE)
             return ERF_B200_ECONFIG;
         if (c->dycore_horiz_adv != ERF_ADV_CENTERED_2ND || c->dycore_vert_adv != ERF_ADV_CENTERED_2ND)
@@ -195,6 +198,8 @@ int validate(const erf_b200_config* c) {
         if (c->buoyancy_type != 1 || c->zlo_bc != ERF_BC_SLIP_WALL || c->zhi_bc != ERF_BC_SLIP_WALL)
             return ERF_B200_ECONFIG;
         if (!(c->mt_wavelength > 0.0) || !(std::fabs(c->mt_ampl) < 0.5 * c->nz * c->dz)) return ERF_B200_ECONFIG;
+    } else if (c->no_lagged_delta_rt) {
+        return ERF_B200_ECONFIG;   // the reference allows it for moving terrain only (ERF_DataStruct.H:389)
     }
     if (c->use_terrain) {
         // terrain path: LES closure (or no diffusion), explicit closures only;
@@ -437,6 +442,7 @@ void enqueue_step_mt(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
     Params Po = c->P;
     Po.mt_zt = c->mt.zt;
     Po.mt_znew = c->mt.z[2];
+    const bool nosub = no_substepping(c->cfg);
     Params Ps = Po;
     Ps.znd = c->mt.z[1];
     Ps.met = c->mt.met1;
@@ -472,9 +478,42 @@ void enqueue_step_mt(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                         B.t13, B.t23, B.ter, B.avz, B.Fmx, B.Fmy, B.Fmz));
         launch_mt_base_state(Po, st, c->mt.r0o, c->mt.p0o, c->mt.z[0], c->mt.z[1], c->mt.z[2], c->mt.time, dt,
                              ts_new, c->r0, c->p0);
-        TIMED(10, launch_mt_no_substep<R>(Po, st, nsub * dtau, OLD, B.Fcons, B.Fmx, B.Fmy, B.Fmz, c->mt.z[0],
-                                          c->mt.z[2], SUM));
-        TIMED(7, launch_ter_post<R>(Po, st, c->tkz.ter_post, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext,
+        Params Pp = Po;   // the slow-variable pass: the level's grid when it runs
+        if (nosub) {
+            TIMED(10, launch_mt_no_substep<R>(Po, st, nsub * dtau, OLD, B.Fcons, B.Fmx, B.Fmy, B.Fmz, c->mt.z[0],
+                                              c->mt.z[2], SUM));
+        } else {
+            // fast_rhs_fun, moving terrain (ERF_TI_fast_rhs_fun.H:47-118): per
+            // substep the grids at its old and new times, z_t'', the fast
+            // coefficients on the old grid with the step's old base state;
+            // the level keeps the last substep's old grid and its new one
+            // serves the slow-variable update
+            const double beta_s = 0.1;
+            const double D = dtau * dtau * (0.5 * (1.0 + beta_s)) * (0.5 * (1.0 + beta_s)) * c->g.dzi;
+            dim3 tg((c->g.nx + c->tile_tx - 1) / c->tile_tx, c->g.ny, 1), tcb(c->tile_tx, c->coef_warps, 1);
+            Params Pf = Po;
+            Pf.detJ = c->mt.detJso;
+            Pf.r0 = c->mt.r0o;
+            int lp = 0;
+            for (int ks = 0; ks < nsub; ++ks) {
+                launch_mt_grid_sub(Po, st, c->mt.time, dtau, ks, c->mt.z[3]);
+                launch_mt_grid_sub(Po, st, c->mt.time, dtau, ks + 1, c->mt.z[4]);
+                launch_mt_zpt(Po, st, c->mt.z[3], c->mt.z[4], dtau, c->mt.zpt);
+                launch_mt_detj(Po, st, c->mt.z[3], c->mt.detJso);
+                TIMED(9, launch_fast_coef<R>(Pf, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP,
+                                             B.cQ));
+                TIMED(6, launch_mt_fast<R>(Po, st, ks, c->cfg.no_lagged_delta_rt ? 0 : 1, dtau, beta_s,
+                                           1.0 / (double)nsub, ks == 0 ? OLD : SUM, Sst, Acur, B.Fcons, B.Fmx, B.Fmy,
+                                           B.Fmz, B.lag[lp], B.lag[1 - lp], B.cA, B.cInvB, B.cCB, B.cP, B.cQ,
+                                           c->mt.z[3], c->mt.z[4], c->mt.z[1], c->mt.zpt, c->mt.trhs, c->mt.om,
+                                           B.avx, B.avy, B.avz, SUM, ks == nsub - 1 ? 1 : 0));
+                lp ^= 1;
+            }
+            Pp.znd = c->mt.z[3];
+            Pp.detJ = c->mt.detJso;
+            Pp.mt_znew = c->mt.z[4];
+        }
+        TIMED(7, launch_ter_post<R>(Pp, st, c->tkz.ter_post, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext,
                                     nrk < 2 ? 1 : 0, B.mut, B.tke, B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1],
                                     Vnew[2]));
         a = 1 - a;
@@ -751,6 +790,10 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
             A(&c->mt.r0o, (size_t)(cfg->nz + 2) * sk); A(&c->mt.p0o, (size_t)(cfg->nz + 2) * sk);
             A(&c->mt.time, 1);
             if (rc == ERF_B200_OK) cudaMemsetAsync(c->mt.time, 0, sizeof(double), c->stream);
+            if (cfg->substepping_type == ERF_SUBSTEP_IMPLICIT) {
+                A(&c->mt.z[3], (size_t)(cfg->nz + 3) * sk); A(&c->mt.z[4], (size_t)(cfg->nz + 3) * sk);
+                A(&c->mt.detJso, N); A(&c->mt.zpt, NZF); A(&c->mt.trhs, 2 * N); A(&c->mt.om, NZF);
+            }
         }
     }
     if (rc == ERF_B200_OK) {

@@ -191,6 +191,18 @@ template <class R>
 void launch_mt_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons,
                           const R* Fmx, const R* Fmy, const R* Fmz, const double* zo, const double* zn, StateBuf Ssum);
 void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt);
+// acoustic substeps over moving terrain: the grid at T + ks dtau, z_t'' of
+// the substep, detJ of a grid, and one substep (last: no boundary fill after
+// it, the slow-variable pass does that)
+void launch_mt_grid_sub(const Params& P, cudaStream_t st, const double* tdev, double dtau, int ks, double* z);
+void launch_mt_zpt(const Params& P, cudaStream_t st, const double* zo, const double* zn, double dtau, double* zpt);
+void launch_mt_detj(const Params& P, cudaStream_t st, const double* z, double* detJ);
+template <class R>
+void launch_mt_fast(const Params& P, cudaStream_t st, int step, int lagged, double dtau, double beta_s, double facinv,
+                    StateBuf Sprev, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmx, const R* Fmy,
+                    const R* Fmz, const R* lag_in, R* lag_out, const R* cA, const R* cInvB, const R* cCB, const R* cP,
+                    const R* cQ, const double* zo, const double* zn, const double* zs, const double* zpt,
+                    double* trhs, double* om, R* avx, R* avy, R* avz, StateBuf Ssum, int last);
 void launch_ter_base_state(const Params& P, cudaStream_t st, const double* zcc, const double* th3, const double* qv3,
                            double th_s, double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0);
 template <class R>

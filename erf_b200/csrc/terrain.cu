@@ -329,7 +329,8 @@ __global__ void k_mt_grid(Params P, const double* __restrict__ tdev, double dt, 
     const Geo& g = P.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.nx || j >= g.ny) return;
-    const double t = mt_time_at(*tdev, dt, tsel);
+    // tsel >= 0: a stage point; tsel < 0: substep -1 - tsel of length dt, T + ks dt
+    const double t = tsel >= 0 ? mt_time_at(*tdev, dt, tsel) : *tdev + (-1 - tsel) * dt;
     const double x = i * P.mt_dx;
     const double hs = P.mt_ampl * sin(P.mt_kp * x - P.mt_om * t);
     const int nz = g.nz;
@@ -475,6 +476,325 @@ template void launch_mt_no_substep<double>(const Params&, cudaStream_t, double, 
                                            const double*, const double*, const double*, const double*, StateBuf);
 template void launch_mt_no_substep<float>(const Params&, cudaStream_t, double, StateBuf, const float*, const float*,
                                           const float*, const float*, const double*, const double*, StateBuf);
+
+// ---------------------------------------------------------------------------
+// Acoustic substeps over moving terrain (erf_fast_rhs_MT,
+// TimeIntegration/ERF_fast_rhs_MT.cpp:48-626).  zo / zn: the grids at the
+// substep's old and new times, zs: the stage's; zpt: the substep's z_t less
+// the stage's.  The new state's horizontal momenta are formed h_zeta-weighted
+// in place, read that way by the flux and Omega'' kernels, then divided by
+// the new grid's h_zeta; one thread per column solves for Omega'' and
+// updates rho w, rho and rho theta.
+// ---------------------------------------------------------------------------
+constexpr int MT_NZMAX = 512;   // levels of the column kernel's local solution
+
+__device__ __forceinline__ void mt_slopes(const double* z, const Geo& g, int i, int j, int k, double& sx, double& sy) {
+    sx = 0.5 * g.dxi * (znode(z, g, i + 1, j + 1, k) + znode(z, g, i + 1, j, k) - znode(z, g, i, j + 1, k) - znode(z, g, i, j, k));
+    sy = 0.5 * g.dyi * (znode(z, g, i + 1, j + 1, k) + znode(z, g, i, j + 1, k) - znode(z, g, i + 1, j, k) - znode(z, g, i, j, k));
+}
+__device__ __forceinline__ double mt_hxI(const double* z, const Geo& g, int i, int j, int k) {
+    auto Z = [&](int a, int b, int c) { return znode(z, g, a, b, c); };
+    return 0.125 * g.dxi * (Z(i + 1, j, k) + Z(i + 1, j, k + 1) + Z(i + 1, j + 1, k) + Z(i + 1, j + 1, k + 1)
+                            - Z(i - 1, j, k) - Z(i - 1, j, k + 1) - Z(i - 1, j + 1, k) - Z(i - 1, j + 1, k + 1));
+}
+__device__ __forceinline__ double mt_hetaJ(const double* z, const Geo& g, int i, int j, int k) {
+    auto Z = [&](int a, int b, int c) { return znode(z, g, a, b, c); };
+    return 0.125 * g.dyi * (Z(i, j + 1, k) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k) + Z(i + 1, j + 1, k + 1)
+                            - Z(i, j - 1, k) - Z(i, j - 1, k + 1) - Z(i + 1, j - 1, k) - Z(i + 1, j - 1, k + 1));
+}
+// OmegaFromW of face (i,j,k) on grid z, horizontal momenta mx / my
+__device__ __forceinline__ double mt_omega(const double* z, const Geo& g, int i, int j, int k, double w,
+                                           const double* mx, const double* my) {
+    auto U = [&](int a, int b, int c) { return mx[cidx(g, wrap(a, g.nx), wrap(b, g.ny), c)]; };
+    auto V = [&](int a, int b, int c) { return my[cidx(g, wrap(a, g.nx), wrap(b, g.ny), c)]; };
+    double sx, sy, u, v;
+    mt_slopes(z, g, i, j, k, sx, sy);
+    zface_uv(i, j, k, U, V, u, v);
+    return w - sx * u - sy * v;
+}
+__device__ __forceinline__ double mt_wfrom(const double* z, const Geo& g, int i, int j, int k, double om,
+                                           const double* mx, const double* my) {
+    auto U = [&](int a, int b, int c) { return mx[cidx(g, wrap(a, g.nx), wrap(b, g.ny), c)]; };
+    auto V = [&](int a, int b, int c) { return my[cidx(g, wrap(a, g.nx), wrap(b, g.ny), c)]; };
+    double sx, sy, u, v;
+    mt_slopes(z, g, i, j, k, sx, sy);
+    zface_uv(i, j, k, U, V, u, v);
+    return om + sx * u + sy * v;
+}
+
+// the substep's z_t less the stage's (ERF_TI_fast_rhs_fun.H:66-90)
+__global__ void k_mt_zpt(Params P, const double* __restrict__ zo, const double* __restrict__ zn, double inv_dt,
+                         double* __restrict__ zpt) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    auto N = [&](int a, int b) { return znode(zn, g, a, b, k); };
+    auto O = [&](int a, int b) { return znode(zo, g, a, b, k); };
+    const int64_t f = cidx(g, i, j, k);
+    double v = 0.25 * inv_dt * (N(i + 1, j + 1) - O(i + 1, j + 1) + N(i, j + 1) - O(i, j + 1) + N(i + 1, j) - O(i + 1, j) + N(i, j) - O(i, j));
+    zpt[f] = v - P.mt_zt[f];
+}
+// detJ of a grid's cells (make_J)
+__global__ void k_mt_detj(Params P, const double* __restrict__ z, double* __restrict__ detJ) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    detJ[cidx(g, i, j, k)] = mt_detj(z, g, i, j, k);
+}
+
+// x / y momenta of the substep, h_zeta-weighted on the old grid
+// (ERF_fast_rhs_MT.cpp:197-273); d(rho theta) extrapolated with or without
+// the lagged correction; the new lag.
+template <class R>
+__global__ void k_mt_fast_h(Params P, int step, int lagged, double dtau, StateBuf Sprev, StateBuf Sst, StageAux<R> A,
+                            const R* __restrict__ Fmx, const R* __restrict__ Fmy, const R* __restrict__ lag_in,
+                            R* __restrict__ lag_out, const double* __restrict__ zo, StateBuf Ssum) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    const int im = wrap(i - 1, g.nx), jm = wrap(j - 1, g.ny);
+    const int64_t c = cidx(g, i, j, k), cxm = cidx(g, im, j, k), cym = cidx(g, i, jm, k);
+    const double beta_d = 0.1, dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
+    auto extrap = [&](int ii, int jj, int kk) {
+        int64_t e = cidx(g, wrap(ii, g.nx), wrap(jj, g.ny), clampk(kk, nz));
+        double d = Sprev.cons[N + e] - Sst.cons[N + e];
+        if (step == 0 || !lagged) return d;
+        return d + beta_d * (d - double(lag_in[e]));
+    };
+    if (step == 0 || lagged) lag_out[c] = R(Sprev.cons[N + c] - Sst.cons[N + c]);
+    double mx, my;
+    {
+        double hxi = mt_hxI(zo, g, i, j, k), hz = mt_hzI(zo, g, i, j, k);
+        double gp_xi = (extrap(i, j, k) - extrap(i - 1, j, k)) * dxi;
+        double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k) - extrap(i, j, k))
+                                  : 0.25 * dzi * (extrap(i - 1, j, k + 1) + extrap(i, j, k + 1) - extrap(i - 1, j, k - 1) - extrap(i, j, k - 1));
+        double gpx = hz * gp_xi - hxi * gp_zeta;
+        gpx *= 1.0;
+        double pi_c = 0.5 * (double(A.pi[cxm]) + double(A.pi[c]));
+        double f = -Gamma_ * R_d * pi_c * gpx;
+        mx = hz * Sprev.mx[c] + dtau * f + dtau * double(Fmx[c]);
+    }
+    {
+        double het = mt_hetaJ(zo, g, i, j, k), hz = mt_hzJ(zo, g, i, j, k);
+        double gp_eta = (extrap(i, j, k) - extrap(i, j - 1, k)) * dyi;
+        double gp_zeta = (k == 0) ? 0.5 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k) - extrap(i, j - 1, k))
+                                  : 0.25 * dzi * (extrap(i, j, k + 1) + extrap(i, j - 1, k + 1) - extrap(i, j, k - 1) - extrap(i, j - 1, k - 1));
+        double gpy = hz * gp_eta - het * gp_zeta;
+        gpy *= 1.0;
+        double pi_c = 0.5 * (double(A.pi[cym]) + double(A.pi[c]));
+        double f = -Gamma_ * R_d * pi_c * gpy;
+        my = hz * Sprev.my[c] + dtau * f + dtau * double(Fmy[c]);
+    }
+    Ssum.mx[c] = mx;
+    Ssum.my[c] = my;
+}
+
+// horizontal fluxes of rho and rho theta (the weighted momenta less the
+// stage's on the stage grid) and Omega'' of the previous substep on the old
+// grid (ERF_fast_rhs_MT.cpp:283-340).  After the first substep the previous
+// and new states are one, so Omega'' reads the weighted momenta, as the
+// reference's aliased arrays do.
+template <class R>
+__global__ void k_mt_fast_flux(Params P, StateBuf Sprev, StateBuf Sst, StageAux<R> A, StateBuf Ssum,
+                               const double* __restrict__ zo, const double* __restrict__ zs,
+                               const double* __restrict__ zpt, double* __restrict__ trhs, double* __restrict__ om) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell, f = cidx(g, i, j, k);
+    if (k < nz) {
+        const int ip = wrap(i + 1, g.nx), im = wrap(i - 1, g.nx), jp = wrap(j + 1, g.ny), jm = wrap(j - 1, g.ny);
+        const int64_t cxp = cidx(g, ip, j, k), cyp = cidx(g, i, jp, k);
+        double xl = Ssum.mx[f] - Sst.mx[f] * mt_hzI(zs, g, i, j, k), xh = Ssum.mx[cxp] - Sst.mx[cxp] * mt_hzI(zs, g, i + 1, j, k);
+        double yl = Ssum.my[f] - Sst.my[f] * mt_hzJ(zs, g, i, j, k), yh = Ssum.my[cyp] - Sst.my[cyp] * mt_hzJ(zs, g, i, j + 1, k);
+        auto th = [&](int a, int b) { return double(A.prim[cidx(g, a, b, k)]); };
+        const double t0 = th(i, j);
+        trhs[f] = (xh - xl) * g.dxi + (yh - yl) * g.dyi;
+        trhs[N + f] = ((xh * (t0 + th(ip, j)) - xl * (t0 + th(im, j))) * g.dxi +
+                       (yh * (t0 + th(i, jp)) - yl * (t0 + th(i, jm))) * g.dyi) * 0.5;
+    }
+    double o;
+    if (k == 0) o = 0.;
+    else if (k == nz) o = Sprev.mz[f] - Sst.mz[f] - zpt[f];
+    else {
+        double a = mt_omega(zo, g, i, j, k, Sprev.mz[f], Sprev.mx, Sprev.my);
+        double b = mt_omega(zo, g, i, j, k, Sst.mz[f], Sst.mx, Sst.my);
+        o = (a - b) - zpt[f];
+    }
+    om[f] = o;
+}
+
+// the horizontal momenta divided by the new grid's h_zeta; their average
+template <class R>
+__global__ void k_mt_fast_div(Params P, double facinv, StateBuf Sst, const double* __restrict__ zn, StateBuf Ssum,
+                              R* __restrict__ avx, R* __restrict__ avy) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int64_t c = cidx(g, i, j, k);
+    double mx = Ssum.mx[c] / mt_hzI(zn, g, i, j, k);
+    double my = Ssum.my[c] / mt_hzJ(zn, g, i, j, k);
+    Ssum.mx[c] = mx;
+    Ssum.my[c] = my;
+    avx[c] += R(facinv * (mx - Sst.mx[c]));
+    avy[c] += R(facinv * (my - Sst.my[c]));
+}
+
+// One column per thread (ERF_fast_rhs_MT.cpp:375-600): the right-hand side
+// of the Omega'' system (old / new / stage face detJ, the stage's
+// coefficients made on the substep's old grid), the Thomas sweep, rho w on
+// the lid; then rho w from Omega'' (on the moving ground W from Omega =
+// rho (z_t + z_t'')), the vertical fluxes, the average contravariant
+// momentum, and rho / rho theta detJ-weighted old -> new.
+template <class R>
+__global__ void k_mt_fast_col(Params P, double dtau, double beta_1, double beta_2, double facinv, StateBuf Sprev,
+                              StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons, const R* __restrict__ Fmz,
+                              const R* __restrict__ cA, const R* __restrict__ cInvB, const R* __restrict__ cCB,
+                              const R* __restrict__ cP, const R* __restrict__ cQ, const double* __restrict__ zo,
+                              const double* __restrict__ zn, const double* __restrict__ zs,
+                              const double* __restrict__ zpt, const double* __restrict__ om,
+                              const double* __restrict__ trhs, R* __restrict__ avz, StateBuf Ssum) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    const double dzi = g.dzi;
+    const double halfg = fabs(0.5 * -P.gravity);
+    double soln[MT_NZMAX + 1];
+    auto C = [&](int k) { return cidx(g, i, j, k); };
+    auto th = [&](int k) { return double(A.prim[C(clampk(k, nz))]); };
+    auto fJ = [&](const double* z, int k) { return 0.5 * (mt_detj(z, g, i, j, k) + mt_detj(z, g, i, j, k - 1)); };
+    // ground row
+    {
+        const double rho_on_bdy = 0.5 * (Sprev.cons[C(0)] + Sprev.cons[C(0)]);
+        soln[0] = (rho_on_bdy * zpt[C(0)]) * double(cInvB[C(0)]);
+    }
+    for (int k = 1; k < nz; ++k) {
+        const double Jo = fJ(zo, k), Jn = fJ(zn, k), Js = fJ(zs, k);
+        const double cp = double(cP[C(k)]), cq = double(cQ[C(k)]);
+        const double tlo = 0.5 * (th(k - 2) + th(k - 1)), tmid = 0.5 * (th(k - 1) + th(k)), thi = 0.5 * (th(k) + th(k + 1));
+        const int64_t a = C(k), b = C(k - 1);
+        double R0t = cp * Sprev.cons[N + a] * Jo + cq * Sprev.cons[N + b] * Jo
+                     - cp * Sst.cons[N + a] * Js - cq * Sst.cons[N + b] * Js
+                     - halfg * (Sprev.cons[a] + Sprev.cons[b]) * Jo
+                     + halfg * (Sst.cons[a] + Sst.cons[b]) * Js;
+        double R1t = -halfg * (double(Fcons[a]) + double(Fcons[b])) + (cp * double(Fcons[N + a]) + cq * double(Fcons[N + b]));
+        const double Okp1 = om[C(k + 1)], Ok = om[a], Okm1 = om[b];
+        R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + trhs[a] + trhs[b]);
+        R1t += -(cp * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + trhs[N + a]) +
+                 cq * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + trhs[N + b]));
+        double rhs = Jo * Sprev.mz[a] - Js * Sst.mz[a] + dtau * (double(Fmz[a]) + R0t + dtau * beta_2 * R1t);
+        double un = mt_omega(zn, g, i, j, k, 0., Ssum.mx, Ssum.my);
+        double us = mt_omega(zs, g, i, j, k, 0., Sst.mx, Sst.my);
+        rhs += Jn * un - Js * us;
+        soln[k] = (rhs - double(cA[a]) * soln[k - 1]) * double(cInvB[a]);
+    }
+    soln[nz] = (0.0 - double(cA[C(nz)]) * soln[nz - 1]) * double(cInvB[C(nz)]);
+    for (int k = nz - 1; k >= 0; --k) soln[k] = soln[k] - double(cCB[C(k)]) * soln[k + 1];
+    Ssum.mz[C(nz)] = Sst.mz[C(nz)] + soln[nz];
+    // rho w from Omega''
+    for (int k = 0; k < nz; ++k) {
+        const int64_t a = C(k);
+        const double rho_on_face = 0.5 * (Sprev.cons[a] + Sprev.cons[C(k > 0 ? k - 1 : 0)]);
+        if (k == 0) {
+            Ssum.mz[a] = mt_wfrom(zn, g, i, j, 0, rho_on_face * (P.mt_zt[a] + zpt[a]), Ssum.mx, Ssum.my);
+            soln[0] = 0.;
+        } else {
+            double wn = mt_wfrom(zn, g, i, j, k, 0.0, Ssum.mx, Ssum.my);
+            double ws = mt_wfrom(zs, g, i, j, k, 0.0, Sst.mx, Sst.my);
+            double wpp = soln[k] + (wn - ws);
+            double m = fJ(zo, k) * (Sst.mz[a] + wpp);
+            m /= fJ(zn, k);
+            Ssum.mz[a] = m;
+            double o1 = mt_omega(zn, g, i, j, k, m, Ssum.mx, Ssum.my);
+            double o2 = mt_omega(zs, g, i, j, k, Sst.mz[a], Sst.mx, Sst.my);
+            soln[k] = o1 - o2;
+            soln[k] -= rho_on_face * zpt[a];
+        }
+    }
+    // rho and rho theta
+    for (int k = 0; k < nz; ++k) {
+        const int64_t a = C(k);
+        double zl = beta_2 * soln[k] + beta_1 * om[a];
+        double zh = beta_2 * soln[k + 1] + beta_1 * om[C(k + 1)];
+        avz[a] += R(facinv * zl / (1.0 * 1.0));
+        if (k == nz - 1) avz[C(k + 1)] += R(facinv * zh / (1.0 * 1.0));
+        const double Jo = mt_detj(zo, g, i, j, k), Jn = mt_detj(zn, g, i, j, k);
+        double frho = -(trhs[a] + (zh - zl) * dzi);
+        double tr = Jo * Sprev.cons[a] + dtau * (double(Fcons[a]) + frho);
+        double frt = -(trhs[N + a] + 0.5 * (zh * (th(k) + th(k + 1)) - zl * (th(k) + th(k - 1))) * dzi);
+        double tt = Jo * Sprev.cons[N + a] + dtau * (double(Fcons[N + a]) + frt);
+        Ssum.cons[a] = tr / Jn;
+        Ssum.cons[N + a] = tt / Jn;
+    }
+}
+
+// the boundary fill after a substep (apply_bcs, fast variables): the
+// momenta through M -> V -> M with the walls' density ghosts; w on the flat
+// lid from Omega = 0, the moving ground untouched but round-tripped
+__global__ void k_mt_fast_bc(Params P, StateBuf Ssum) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int nz = g.nz;
+    const int64_t f = cidx(g, i, j, k);
+    if (k < nz) {
+        double rs = Ssum.cons[f] + Ssum.cons[cidx(g, wrap(i - 1, g.nx), j, k)];
+        double u = (Ssum.mx[f] * 2.0) / rs;
+        Ssum.mx[f] = (u * 0.5) * rs;
+        rs = Ssum.cons[f] + Ssum.cons[cidx(g, i, wrap(j - 1, g.ny), k)];
+        double v = (Ssum.my[f] * 2.0) / rs;
+        Ssum.my[f] = (v * 0.5) * rs;
+    }
+    if (k == nz) {
+        Ssum.mz[f] = 0.0;   // W from Omega = 0 on the flat lid
+    } else {
+        double rs = Ssum.cons[f] + Ssum.cons[k > 0 ? f - g.sk : f];
+        double w = (Ssum.mz[f] * 2.0) / rs;
+        Ssum.mz[f] = (w * 0.5) * rs;
+    }
+}
+
+void launch_mt_grid_sub(const Params& P, cudaStream_t st, const double* tdev, double dtau, int ks, double* z) {
+    k_mt_grid<<<ter_grid(P.g, 1), ter_block(), 0, st>>>(P, tdev, dtau, -1 - ks, z);
+}
+void launch_mt_zpt(const Params& P, cudaStream_t st, const double* zo, const double* zn, double dtau, double* zpt) {
+    k_mt_zpt<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, zo, zn, 1. / dtau, zpt);
+}
+void launch_mt_detj(const Params& P, cudaStream_t st, const double* z, double* detJ) {
+    k_mt_detj<<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, z, detJ);
+}
+template <class R>
+void launch_mt_fast(const Params& P, cudaStream_t st, int step, int lagged, double dtau, double beta_s, double facinv,
+                    StateBuf Sprev, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmx, const R* Fmy,
+                    const R* Fmz, const R* lag_in, R* lag_out, const R* cA, const R* cInvB, const R* cCB, const R* cP,
+                    const R* cQ, const double* zo, const double* zn, const double* zs, const double* zpt,
+                    double* trhs, double* om, R* avx, R* avy, R* avz, StateBuf Ssum, int last) {
+    const Geo& g = P.g;
+    const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
+    k_mt_fast_h<R><<<ter_grid(g, g.nz), ter_block(), 0, st>>>(P, step, lagged, dtau, Sprev, Sst, A, Fmx, Fmy, lag_in,
+                                                              lag_out, zo, Ssum);
+    k_mt_fast_flux<R><<<ter_grid(g, g.nz + 1), ter_block(), 0, st>>>(P, Sprev, Sst, A, Ssum, zo, zs, zpt, trhs, om);
+    k_mt_fast_div<R><<<ter_grid(g, g.nz), ter_block(), 0, st>>>(P, facinv, Sst, zn, Ssum, avx, avy);
+    k_mt_fast_col<R><<<ter_grid(g, 1), ter_block(), 0, st>>>(P, dtau, beta_1, beta_2, facinv, Sprev, Sst, A, Fcons, Fmz,
+                                                            cA, cInvB, cCB, cP, cQ, zo, zn, zs, zpt, om, trhs, avz,
+                                                            Ssum);
+    if (!last) k_mt_fast_bc<<<ter_grid(g, g.nz + 1), ter_block(), 0, st>>>(P, Ssum);
+}
+template void launch_mt_fast<double>(const Params&, cudaStream_t, int, int, double, double, double, StateBuf, StateBuf,
+                                     StageAux<double>, const double*, const double*, const double*, const double*,
+                                     const double*, double*, const double*, const double*, const double*,
+                                     const double*, const double*, const double*, const double*, const double*,
+                                     const double*, double*, double*, double*, double*, double*, StateBuf, int);
+template void launch_mt_fast<float>(const Params&, cudaStream_t, int, int, double, double, double, StateBuf, StateBuf,
+                                    StageAux<float>, const float*, const float*, const float*, const float*,
+                                    const float*, float*, const float*, const float*, const float*, const float*,
+                                    const float*, const double*, const double*, const double*, const double*, double*,
+                                    double*, float*, float*, float*, StateBuf, int);
 
 // post_timestep's clock (ERF.cpp:547-559 with t_new = t_old + dt)
 __global__ void k_mt_advance_time(double* t, double dt) { *t = *t + dt; }

@@ -139,18 +139,24 @@ def test_create_accepts_most_config(lib):
         lib.erf_b200_destroy(ctx)
 
 
-@pytest.mark.parametrize("change", ["static_flag", "substeps", "moist", "les", "molec", "upwind", "buoyancy",
-                                    "noslip", "wavelength", "bad_type"])
+@pytest.mark.parametrize("change", ["static_flag", "tall_substepped", "moist", "les", "molec", "upwind", "buoyancy",
+                                    "noslip", "wavelength", "bad_type", "unlagged_static"])
 def test_create_rejects_unsupported_moving_terrain(lib, change):
-    """Moving terrain is accepted as the reference's MovingTerrain problem
-    runs it: dry, no diffusion, Centered_2nd dycore, buoyancy type 1, slip
-    walls, one update per RK stage; the rest is refused before any CUDA call."""
+    """Moving terrain is accepted as the reference's MovingTerrain problems
+    run it: dry, no diffusion, Centered_2nd dycore, buoyancy type 1, slip
+    walls, with or without acoustic substepping (up to 512 levels with);
+    use_lagged_delta_rt = false only there; the rest is refused before any
+    CUDA call."""
     from erf_b200 import terrain as T
     c = T.moving_terrain(nx=8, ny=4, nz=10).cfg
     if change == "static_flag":
         c.use_terrain = 0
-    elif change == "substeps":
+    elif change == "tall_substepped":
         c.substepping_type = C.SUBSTEP_IMPLICIT
+        c.nz = 513
+    elif change == "unlagged_static":
+        c = C.defaults()
+        c.no_lagged_delta_rt = 1
     elif change == "moist":
         c.moisture, c.ncomp = C.MOIST_KESSLER, 8
     elif change == "les":
@@ -172,9 +178,10 @@ def test_create_rejects_unsupported_moving_terrain(lib, change):
     assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
 
 
-def test_create_accepts_moving_terrain_config(lib):
+@pytest.mark.parametrize("substeps", [False, True])
+def test_create_accepts_moving_terrain_config(lib, substeps):
     from erf_b200 import terrain as T
-    c = T.moving_terrain(nx=8, ny=4, nz=10).cfg
+    c = T.moving_terrain(nx=8, ny=4, nz=10, substeps=substeps).cfg
     ctx = ctypes.c_void_p()
     lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
     lib.erf_b200_destroy.argtypes = [ctypes.c_void_p]

@@ -141,3 +141,51 @@ def test_moving_terrain_entry_points_refuse_other_contexts():
     with pytest.raises(ErfError):
         dy.set_time(1.0)
     dy.close()
+
+
+def test_moving_terrain_substeps_match_oracle_and_gold():
+    """MovingTerrain_sub: 10 steps of 0.1 s with 20 acoustic substeps over
+    the moving grid (erf_fast_rhs_MT), use_lagged_delta_rt = false."""
+    case = T.moving_terrain(substeps=True)
+    cfg = case.cfg
+    got, t, z, r0, p0, status = _gpu(case, case.steps)
+    assert status == 0
+    ref = oracle.advance_moving_terrain(cfg, 0.0, case.base, *case.build_state(), case.steps)
+    errs = _errors(got, ref[:4])
+    errs["rho0"] = rel_l2(r0, ref[5])
+    errs["p0"] = rel_l2(p0, ref[6])
+    vdiff = float(np.max(np.abs(got[2] - ref[2])))
+    print("moving terrain, substeps, 40x8x79, 10 steps, GPU vs oracle:", errs, "max |dv|", vdiff)
+    bad = {k: e for k, e in errs.items() if not e <= TOL}
+    assert not bad, errs
+    assert vdiff <= 1e-15
+    gold = np.load(os.path.join(HERE, "golden", "MovingTerrain_sub_minmax.npz"))
+    worst = {}
+    for (b, nm, tag), e in gold_box_errors(gold, plot_fields_mt(cfg, *got, z, r0, p0)).items():
+        worst[nm] = max(worst.get(nm, 0.0), e)
+    print("vs gold:", worst)
+    for nm, e in worst.items():
+        assert e <= 2e-10, (nm, e)
+
+
+@pytest.mark.parametrize("lagged", [True, False])
+def test_moving_terrain_substeps_steeper_wave(lagged):
+    """A steeper, shorter wave, 6 substeps per step, with and without the
+    lagged d(rho theta) correction; and the mixed form against FP64."""
+    case = T.moving_terrain(nx=24, ny=4, nz=30, Lx=120.0, Ly=20.0, H=150.0, ampl=0.5, wavelength=60.0,
+                            substeps=True, dt=0.05, steps=8)
+    case.cfg.mri_ratio = 6
+    case.cfg.no_lagged_delta_rt = 0 if lagged else 1
+    got, t, z, r0, p0, status = _gpu(case, case.steps)
+    assert status == 0
+    ref = oracle.advance_moving_terrain(case.cfg, 0.0, case.base, *case.build_state(), case.steps)
+    errs = _errors(got, ref[:4])
+    errs["rho0"] = rel_l2(r0, ref[5])
+    print("substeps, 24x4x30, lagged", lagged, errs)
+    bad = {k: e for k, e in errs.items() if not e <= TOL}
+    assert not bad, errs
+    mixed = _gpu(case, case.steps, precision=C.PREC_MIXED)
+    assert mixed[5] == 0
+    em = _errors(mixed[0], got)
+    print("  mixed vs FP64:", em)
+    assert all(e <= 1e-3 for e in em.values()), em
