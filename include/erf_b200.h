@@ -181,7 +181,8 @@ typedef struct erf_b200_config {
      * k = 2 pi / mt_wavelength, omega = sqrt(g k) (the surface of
      * Exec/DevTests/MovingTerrain/ERF_prob.cpp:147-200) smoothed upward with
      * Sullivan's factor (1 - z/z_top)^3 (terrain_smoothing = 2,
-     * Utils/ERF_TerrainMetrics.cpp:501-536) over the uniform levels k dz */
+     * Utils/ERF_TerrainMetrics.cpp:501-536) over the uniform levels k dz;
+     * with or without acoustic substepping (erf_fast_rhs_MT) */
     int    terrain_type;
     /* SolverChoice::use_lagged_delta_rt = false (1 here; 0 keeps the
      * reference default, true): the acoustic substeps over moving terrain
