@@ -7,8 +7,18 @@
 #include <new>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kernels.cuh"
 #include "mlp.cuh"
+
+// NVTX range for the length of a scope (an entry point or a step's launch)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 namespace erfb {
 __global__ void k_kessler(Params P, double* cons, double dtn, double dz);
@@ -92,6 +102,8 @@ struct erf_b200_ctx {
     int ter_tx = 0;                                           // k_ter_fast_vert columns per block
     size_t ter_smem = 0;                                      // and its shared memory
     bool ter_set = false;
+    int last = -1;               // state slot of the latest state (erf_b200_diagnostics)
+    double* diag = nullptr;      // its scratch (partials, result)
     double *h_stage;          // device staging buffers for the host-array entry point
     int* status;
     bool base_set = false;
@@ -351,11 +363,18 @@ struct LaunchTimer {
     }
     void done() { cudaEventRecord(ev[used - 1], st); }
 };
+// NVTX range names of the pass slots (the tracing tools' timeline; the
+// calls cost a pointer test when no tool is attached)
+static const char* const kPassName[] = {"step_begin", "stress", "slow_cell", "plane_avg", "slow_mom",
+                                        "fast_horizontal", "fast_column", "slow_post", "kessler", "fast_coeffs",
+                                        "no_substep"};
 #define TIMED(slotid, launch)                 \
     do {                                      \
+        nvtxRangePushA(kPassName[slotid]);    \
         if (T) T->mark(slotid);               \
         launch;                               \
         if (T) T->done();                     \
+        nvtxRangePop();                       \
     } while (0)
 
 // One full step over static terrain: the same stage / substep schedule with
@@ -951,6 +970,32 @@ int erf_b200_set_terrain(erf_b200_ctx* c, const double* z_nd) {
     return ERF_B200_OK;
 }
 
+// Diagnostics of the latest state (the resident one, or the one the last
+// erf_b200_advance left): out[0] the mass (integral of rho over the
+// physical volume, dx dy dz detJ per cell), out[1] the integral of rho
+// theta, out[2] max |w|.  Synchronises the stream.
+int erf_b200_diagnostics(erf_b200_ctx* c, double* out) {
+    if (!c || !out) return ERF_B200_EINVAL;
+    const int p = c->cur >= 0 ? c->cur : c->last;
+    if (p < 0) return ERF_B200_EBADSTATE;
+    if (c->cfg.use_terrain && !c->ter_set) return ERF_B200_EBADSTATE;
+    if (!c->diag) {
+        int rc = dalloc(c, &c->diag, (size_t)diagnostics_scratch_doubles());
+        if (rc) return rc;
+    }
+    const double* zg = nullptr;
+    if (c->cfg.use_terrain && c->cfg.terrain_type == ERF_TERRAIN_MOVING) {   // the grid at the clock's time
+        launch_mt_grid(c->P, c->stream, c->mt.time, c->cfg.dt, 0, c->mt.z[1]);
+        zg = c->mt.z[1];
+    }
+    double* res = c->diag + diagnostics_scratch_doubles() - 3;
+    launch_diagnostics(c->P, c->stream, c->S[p].cons, c->vel[p][2], zg, c->diag, res);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ERF_B200_OK;
+}
+
 // Moving terrain: set the device clock (the old time of the next step).
 int erf_b200_set_time(erf_b200_ctx* c, double time) {
     if (!c || c->cfg.terrain_type != ERF_TERRAIN_MOVING || !c->cfg.use_terrain) return ERF_B200_EINVAL;
@@ -1011,8 +1056,15 @@ int erf_b200_advance(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b200_f
     if ((rc = pack(c, zvel, 3, 1, c->vel[0][2]))) return rc;
     if (!c->graph[0] || !c->graph[1]) return ERF_B200_EBADSTATE;   // learned closure not attached
     c->cur = -1;
-    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph[s & 1], c->stream));
+    {
+        NvtxRange r("erf_b200_advance");
+        for (int s = 0; s < nsteps; ++s) {
+            NvtxRange rs("step");
+            CK(cudaGraphLaunch(c->graph[s & 1], c->stream));
+        }
+    }
     int p = nsteps & 1;
+    c->last = p;
     if ((rc = unpack(c, cons, 0, c->cfg.ncomp, c->S[p].cons))) return rc;
     if ((rc = unpack(c, xvel, 1, 1, c->vel[p][0]))) return rc;
     if ((rc = unpack(c, yvel, 2, 1, c->vel[p][1]))) return rc;
@@ -1515,6 +1567,7 @@ int erf_b200_load_state(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b20
         (rc = pack(c, zvel, 3, 1, c->vel[0][2])))
         return rc;
     c->cur = 0;
+    c->last = 0;
     return cuda_fail(cudaGetLastError());
 }
 
@@ -1536,10 +1589,13 @@ int erf_b200_store_state(erf_b200_ctx* c, const erf_b200_fab* cons, const erf_b2
 int erf_b200_advance_resident(erf_b200_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return ERF_B200_EINVAL;
     if (c->cur < 0 || !c->graph[0] || !c->graph[1]) return ERF_B200_EBADSTATE;
+    NvtxRange r("erf_b200_advance_resident");
     for (int s = 0; s < nsteps; ++s) {
+        NvtxRange rs("step");
         CK(cudaGraphLaunch(c->graph[c->cur], c->stream));
         c->cur ^= 1;
     }
+    c->last = c->cur;
     return ERF_B200_OK;
 }
 

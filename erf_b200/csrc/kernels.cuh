@@ -191,6 +191,12 @@ template <class R>
 void launch_mt_no_substep(const Params& P, cudaStream_t st, double slow_dt, StateBuf Sold, const R* Fcons,
                           const R* Fmx, const R* Fmy, const R* Fmz, const double* zo, const double* zn, StateBuf Ssum);
 void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt);
+// step diagnostics (terrain.cu): out = {mass, integral of rho theta, max |w|};
+// zgrid: moving terrain's nodes (NULL: P.detJ with terrain, 1 without);
+// part: diagnostics_scratch_doubles() - 3 values
+void launch_diagnostics(const Params& P, cudaStream_t st, const double* cons, const double* w, const double* zgrid,
+                        double* part, double* out);
+int diagnostics_scratch_doubles();
 // acoustic substeps over moving terrain: the grid at T + ks dtau, z_t'' of
 // the substep, detJ of a grid, and one substep (last: no boundary fill after
 // it, the slow-variable pass does that)

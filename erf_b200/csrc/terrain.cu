@@ -796,6 +796,64 @@ template void launch_mt_fast<float>(const Params&, cudaStream_t, int, int, doubl
                                     const float*, const double*, const double*, const double*, const double*, double*,
                                     double*, float*, float*, float*, StateBuf, int);
 
+// ---------------------------------------------------------------------------
+// Step diagnostics of a resident state (sum_integrated_quantities /
+// volWgtSumMF, IO/ERF_WriteScalarProfiles.cpp:14-60, 378-420): the
+// integrals of rho and rho theta over the physical volume (dx dy dz detJ per
+// cell; detJ from P.detJ with static terrain, from the nodes of zgrid with
+// moving terrain, 1 without terrain) and max |w| over the z faces.
+// Fixed-order two-pass reduction, so the result does not depend on
+// scheduling.
+// ---------------------------------------------------------------------------
+constexpr int DIAG_BLOCKS = 592, DIAG_THREADS = 256;
+__global__ void __launch_bounds__(DIAG_THREADS) k_diag_partial(Params P, const double* __restrict__ cons,
+                                                               const double* __restrict__ w,
+                                                               const double* __restrict__ zgrid,
+                                                               double* __restrict__ part) {
+    const Geo& g = P.g;
+    __shared__ double sm[3][DIAG_THREADS];
+    double m = 0.0, rt = 0.0, wm = 0.0;
+    const int64_t N = g.ncell, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += stride) {
+        double J = 1.0;
+        if (zgrid) {
+            const int k = (int)(c / g.sk), r = (int)(c - (int64_t)k * g.sk), j = r / g.nx, i = r - j * g.nx;
+            J = mt_detj(zgrid, g, i, j, k);
+        } else if (P.ter) {
+            J = P.detJ[c];
+        }
+        m += cons[c] * J;
+        rt += cons[N + c] * J;
+    }
+    for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < g.nzf; f += stride) wm = fmax(wm, fabs(w[f]));
+    sm[0][threadIdx.x] = m; sm[1][threadIdx.x] = rt; sm[2][threadIdx.x] = wm;
+    __syncthreads();
+    for (int h = DIAG_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            sm[0][threadIdx.x] += sm[0][threadIdx.x + h];
+            sm[1][threadIdx.x] += sm[1][threadIdx.x + h];
+            sm[2][threadIdx.x] = fmax(sm[2][threadIdx.x], sm[2][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = sm[0][0]; part[3 * blockIdx.x + 1] = sm[1][0]; part[3 * blockIdx.x + 2] = sm[2][0];
+    }
+}
+__global__ void k_diag_final(Params P, const double* __restrict__ part, int nb, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double m = 0.0, rt = 0.0, wm = 0.0;
+    for (int b = 0; b < nb; ++b) { m += part[3 * b]; rt += part[3 * b + 1]; wm = fmax(wm, part[3 * b + 2]); }
+    const double vol = 1.0 / (P.g.dxi * P.g.dyi * P.g.dzi);
+    out[0] = m * vol; out[1] = rt * vol; out[2] = wm;
+}
+void launch_diagnostics(const Params& P, cudaStream_t st, const double* cons, const double* w, const double* zgrid,
+                        double* part, double* out) {
+    k_diag_partial<<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(P, cons, w, zgrid, part);
+    k_diag_final<<<1, 32, 0, st>>>(P, part, DIAG_BLOCKS, out);
+}
+int diagnostics_scratch_doubles() { return 3 * DIAG_BLOCKS + 3; }
+
 // post_timestep's clock (ERF.cpp:547-559 with t_new = t_old + dt)
 __global__ void k_mt_advance_time(double* t, double dt) { *t = *t + dt; }
 void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt) { k_mt_advance_time<<<1, 1, 0, st>>>(tdev, dt); }

@@ -37,6 +37,7 @@ EXPORTS = [
     "erf_b200_fast_rhs_T", "erf_b200_write_plotfile", "erf_b200_write_checkpoint", "erf_b200_read_checkpoint",
     "erf_b200_selftest_bounded_wait", "erf_b200_no_substep", "erf_b200_most_update_fluxes",
     "erf_b200_ensemble_abort", "erf_b200_ensemble_steps", "erf_b200_set_time", "erf_b200_moving_terrain_state",
+    "erf_b200_diagnostics",
 ]
 KERNEL_SLOTS = ["step_begin", "stress", "slow_cell", "plane_avg", "slow_mom", "fast_horizontal", "fast_column",
                 "slow_post", "kessler", "fast_coeffs", "no_substep"]
@@ -75,6 +76,7 @@ def load_library():
     L.erf_b200_set_terrain.argtypes = [vp, dp]
     L.erf_b200_set_time.argtypes = [vp, ctypes.c_double]
     L.erf_b200_moving_terrain_state.argtypes = [vp, dp, dp, dp, dp]
+    L.erf_b200_diagnostics.argtypes = [vp, dp]
     L.erf_b200_make_base_state_terrain.argtypes = [vp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                    dp, dp, dp, dp]
     fabp = ctypes.POINTER(ErfFab)
@@ -236,6 +238,13 @@ class Dycore:
         cfg = self.cfg
         assert z.shape == (cfg.nz + 1, cfg.ny + 1, cfg.nx + 1)
         _check(self.lib.erf_b200_set_terrain(self._ctx, z.ctypes.data), "set_terrain")
+
+    def diagnostics(self) -> dict:
+        """Mass and rho-theta integrals (dx dy dz detJ per cell) and max |w|
+        of the latest state (a device reduction; synchronises)."""
+        out = np.zeros(3)
+        _check(self.lib.erf_b200_diagnostics(self._ctx, out.ctypes.data), "diagnostics")
+        return {"mass": float(out[0]), "rhotheta": float(out[1]), "max_w": float(out[2])}
 
     def set_time(self, t: float):
         """Moving terrain: the device clock (the old time of the next step)."""

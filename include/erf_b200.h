@@ -280,6 +280,15 @@ int erf_b200_set_terrain(erf_b200_ctx* ctx, const double* z_nd);
  *     k+1 for level k) into host memory; NULL skips an output.
  * Both return ERF_B200_EINVAL for a context without moving terrain. */
 int erf_b200_set_time(erf_b200_ctx* ctx, double time);
+
+/* Step diagnostics of the latest state (the resident one after
+ * erf_b200_load_state / erf_b200_advance_resident, or the one the last
+ * erf_b200_advance returned): out[0] the mass, the integral of rho over the
+ * physical volume (dx dy dz detJ per cell: ERF's sum_interval mass check,
+ * sum_integrated_quantities / volWgtSumMF, IO/ERF_WriteScalarProfiles.cpp:
+ * 14-60, 378-420), out[1] the integral of rho theta, out[2] max |w|.  A
+ * fixed-order reduction on the device; synchronises the stream. */
+int erf_b200_diagnostics(erf_b200_ctx* ctx, double* out);
 int erf_b200_moving_terrain_state(erf_b200_ctx* ctx, double* time, double* z_nd, double* rho0, double* p0);
 
 int erf_b200_make_base_state_terrain(erf_b200_ctx* ctx, const double* theta3, const double* qv3,
