@@ -2,6 +2,13 @@
 
     python -m erf_b200.build            # incremental
     python -m erf_b200.build --force    # rebuild everything
+    python -m erf_b200.build --bounds   # the bounds-checked variant
+
+The bounds-checked variant liberf_b200_bounds.so is the same code compiled
+with -DERF_B200_BOUNDS=1: every global index formed by cidx is checked
+against its array and a stray one sets ERF_B200_EBOUNDS instead of
+touching memory outside the array (the stand-in for a memory checker).
+Select it for a process with ERF_B200_LIB=<path>.
 """
 from __future__ import annotations
 
@@ -14,6 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liberf_b200.so")
+OBJ_BOUNDS = os.path.join(HERE, "_build_bounds")
+LIB_BOUNDS = os.path.join(HERE, "liberf_b200_bounds.so")
 SOURCES = ["kernels.cu", "terrain.cu", "api.cu", "noalloc.cu", "mlp.cu", "closure.cu", "plotfile.cu", "checkpoint.cu"]
 HEADERS = ["common.cuh", "kernels.cuh", "tiles.cuh", "tcgen05.cuh", "mlp.cuh", "amrex_io.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -29,7 +38,10 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, bounds: bool = False) -> str:
+    OBJ = OBJ_BOUNDS if bounds else globals()["OBJ"]
+    LIB = LIB_BOUNDS if bounds else globals()["LIB"]
+    flags = FLAGS + (["-DERF_B200_BOUNDS=1"] if bounds else [])
     os.makedirs(OBJ, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "erf_b200.h")]
     objs = [os.path.join(OBJ, s.replace(".cu", ".o")) for s in SOURCES]
@@ -37,7 +49,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     def compile_one(job):
         s, obj = job
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, s), "-o", obj]
+        cmd = [NVCC, *ARCH, *flags, "-c", os.path.join(CSRC, s), "-o", obj]
         out = subprocess.run(cmd, capture_output=True, text=True)
         with open(os.path.join(OBJ, s + ".log"), "w") as fh:
             fh.write(" ".join(cmd) + "\n" + out.stdout + out.stderr)
@@ -59,4 +71,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, bounds="--bounds" in sys.argv))

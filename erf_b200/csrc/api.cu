@@ -245,6 +245,9 @@ void make_params(erf_b200_ctx* c) {
     g.dxi = 1.0 / f.dx; g.dyi = 1.0 / f.dy; g.dzi = 1.0 / f.dz;
     g.zlo_noslip = f.zlo_bc == ERF_BC_NO_SLIP_WALL;
     g.zhi_noslip = f.zhi_bc == ERF_BC_NO_SLIP_WALL;
+#ifdef ERF_B200_BOUNDS
+    g.oob = c->status;
+#endif
     Params& P = c->P;
     P.g = g;
     P.ncomp = f.ncomp; P.nprim = f.ncomp - 1;
@@ -896,6 +899,7 @@ int erf_b200_get_status(erf_b200_ctx* c) {
     int h = 0;
     CK(cudaMemcpy(&h, c->status, sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemset(c->status, 0, sizeof(int)));
+    if (h & ST_BOUNDS) return ERF_B200_EBOUNDS;
     if (h & ST_TIMEOUT) return ERF_B200_ETIMEOUT;
     if (h & ST_NAN) return ERF_B200_ENAN;
     if (h & ST_BADSTATE) return ERF_B200_EBADSTATE;

@@ -25,6 +25,7 @@ constexpr double Rd_on_Rv = R_d / R_v;
 constexpr int ST_BADSTATE = 1;
 constexpr int ST_NAN = 2;
 constexpr int ST_TIMEOUT = 4;   // a bounded tensor-core wait ran out
+constexpr int ST_BOUNDS = 8;    // bounds-checked build: an index left its array
 
 // ---------------------------------------------------------------------------
 // Equation of state (reference: Source/Utils/ERF_EOS.H:42-151).  Same
@@ -247,6 +248,9 @@ struct Geo {
     int64_t nzf;       // nx*ny*(nz+1)
     double dxi, dyi, dzi;
     int zlo_noslip, zhi_noslip;
+#ifdef ERF_B200_BOUNDS
+    int* oob = nullptr;   // status word the bounds checks OR ST_BOUNDS into
+#endif
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
@@ -259,7 +263,18 @@ __device__ __forceinline__ int wrap_far(int i, int n) {
     return i;
 }
 __device__ __forceinline__ int clampk(int k, int nz) { return k < 0 ? 0 : (k >= nz ? nz - 1 : k); }
+// Linear index of (i, j, k).  In the bounds-checked build
+// (-DERF_B200_BOUNDS=1) an index outside i in [0, nx), j in [0, ny),
+// k in [0, nz] (the z-face arrays have nz+1 levels) sets ST_BOUNDS in the
+// status word and is replaced by element 0, so the access stays inside the
+// array and the run goes on (no trap).
 __device__ __forceinline__ int64_t cidx(const Geo& g, int i, int j, int k) {
+#ifdef ERF_B200_BOUNDS
+    if ((unsigned)i >= (unsigned)g.nx || (unsigned)j >= (unsigned)g.ny || (unsigned)k > (unsigned)g.nz) {
+        if (g.oob) atomicOr(g.oob, ST_BOUNDS);
+        return 0;
+    }
+#endif
     return (int64_t)i + (int64_t)g.nx * j + g.sk * k;
 }
 

@@ -15,11 +15,13 @@ import numpy as np
 from . import config as C
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liberf_b200.so")
+# ERF_B200_LIB selects another build of the library for this process (the
+# bounds-checked liberf_b200_bounds.so); the default is the in-tree build
+LIB_PATH = os.environ.get("ERF_B200_LIB", os.path.join(_HERE, "liberf_b200.so"))
 _lib = None
 
 ERRORS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "EBADSTATE", 5: "ENAN", 6: "EPIVOT",
-          7: "ETIMEOUT", 8: "ECONFIG", 9: "EABORTED"}
+          7: "ETIMEOUT", 8: "ECONFIG", 9: "EABORTED", 10: "EBOUNDS"}
 EABORTED = 9
 
 EXPORTS = [

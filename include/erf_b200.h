@@ -45,6 +45,8 @@ extern "C" {
 #define ERF_B200_ETIMEOUT         7   /* a bounded device wait ran out          */
 #define ERF_B200_ECONFIG          8   /* configuration rejected                 */
 #define ERF_B200_EABORTED         9   /* an ensemble run was stopped by its abort word */
+#define ERF_B200_EBOUNDS         10   /* bounds-checked build (liberf_b200_bounds.so):
+                                         a kernel formed an index outside its array */
 
 /* ----------------------------------------------------------------------------
  * Enumerations: numeric values match the reference's enums so that a caller
