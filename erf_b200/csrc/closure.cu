@@ -83,7 +83,10 @@ __device__ __forceinline__ void smagorinsky_closure(const float* f, float csd2, 
 }
 
 template <class R>
-__global__ void __launch_bounds__(ROWS) k_closure(Params P, ClosureNet net, const double* __restrict__ cons,
+// Five CTAs per SM: the register cap (96, no spills) lets one CTA's features
+// and GELU overlap the others' MMA waits (124 registers and 4 CTAs without it;
+// 1.170 -> 1.150 ms per mixed learned step on the coarse ABL, same results).
+__global__ void __launch_bounds__(ROWS, 5) k_closure(Params P, ClosureNet net, const double* __restrict__ cons,
                                                   const double* __restrict__ u, const double* __restrict__ v,
                                                   const double* __restrict__ w, const R* __restrict__ theta,
                                                   R* __restrict__ t11, R* __restrict__ t22, R* __restrict__ t33,
