@@ -189,3 +189,35 @@ def test_moving_terrain_substeps_steeper_wave(lagged):
     em = _errors(mixed[0], got)
     print("  mixed vs FP64:", em)
     assert all(e <= 1e-3 for e in em.values()), em
+
+
+def test_moving_terrain_plotfile_matches_gold_header(tmp_path):
+    """End to end: the GPU's MovingTerrain_sub result written as an AMReX
+    plotfile by the library's writer (with the evolved base state and the
+    final grid) carries, for every variable of the gold, the same range as
+    the reference's own gold plotfile header (its four boxes taken
+    together), within the fcompare-style bound."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from plotfile import read_plotfile_minmax
+    from erf_b200.plotfile import write_plotfile
+    case = T.moving_terrain(substeps=True)
+    cfg = case.cfg
+    got, t, z, r0, p0, status = _gpu(case, case.steps)
+    assert status == 0
+    path = str(tmp_path / "plt00010")
+    base = [r0, p0, case.base[2], case.base[3]]
+    write_plotfile(cfg, path, *got, base=base, z_nd=z, time=t, step=case.steps)
+    ours = read_plotfile_minmax(path)
+    gold = np.load(os.path.join(HERE, "golden", "MovingTerrain_sub_minmax.npz"))
+    assert abs(ours["time"] - float(gold["time"])) < 1e-12
+    names = list(ours["names"])
+    worst = {}
+    for q, nm in enumerate(gold["names"]):
+        nm = str(nm)
+        a = names.index(nm)
+        lo, hi = gold["vmin"][:, q].min(), gold["vmax"][:, q].max()
+        e = max(abs(ours["min"][a] - lo) / max(1.0, abs(lo)), abs(ours["max"][a] - hi) / max(1.0, abs(hi)))
+        worst[nm] = e
+    print("plotfile vs gold header:", worst)
+    assert all(e <= 2e-10 for e in worst.values()), worst
