@@ -195,6 +195,25 @@ def abl_most(nx=64, ny=64, nz=64, seed=0, les="smagorinsky", z0=0.1, zref=0.0) -
     return case
 
 
+def abl_most_moist(nx=64, ny=64, nz=64, seed=0, les="smagorinsky", z0=0.1, zref=0.0) -> Case:
+    """abl_most with Kessler moisture (rain included): water vapour falling
+    off from 12 g/kg at the ground with a 1.5 km scale height, moist scalars
+    advected with WENO5, buoyancy type 2 (the temperature-perturbation form
+    about the moist base state's plane averages).  The adiabatic (Moeng) MOST
+    ground applies no moisture flux, as the reference's only computes one for
+    its CUSTOM flux type (BoundaryConditions/ERF_ABLMost.cpp:413-433)."""
+    case = abl_most(nx=nx, ny=ny, nz=nz, seed=seed, les=les, z0=z0, zref=zref)
+    c = case.cfg
+    c.ncomp, c.moisture = 8, C.MOIST_KESSLER
+    c.moistscal_horiz_adv = c.moistscal_vert_adv = C.WENO_5
+    c.buoyancy_type = 2
+    z = (np.arange(nz) + 0.5) * c.dz
+    case.qv_cc = 0.012 * np.exp(-z / 1500.0)
+    case.qv_sfc = 0.012
+    case.name = "abl_most_moist_" + les
+    return case
+
+
 def moist_bubble(nx=128, ny=128, nz=80, seed=1) -> Case:
     c = C.defaults()
     c.nx, c.ny, c.nz = nx, ny, nz

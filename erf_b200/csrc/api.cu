@@ -167,9 +167,11 @@ int validate(const erf_b200_config* c) {
         return ERF_B200_ECONFIG;
     if (c->zhi_bc != ERF_BC_NO_SLIP_WALL && c->zhi_bc != ERF_BC_SLIP_WALL) return ERF_B200_ECONFIG;
     if (c->zlo_bc == ERF_BC_MOST) {
-        // MOST ground: flat, dry, under an eddy-viscosity closure (eta of the
-        // ghost rule), z0 below the snapped reference height
-        if (c->use_terrain || c->moisture != ERF_MOIST_NONE) return ERF_B200_ECONFIG;
+        // MOST ground: flat, under an eddy-viscosity closure (eta of the ghost
+        // rule), z0 below the snapped reference height; with moisture the
+        // adiabatic ground adds no moisture flux (the reference computes one
+        // for its CUSTOM flux type only, ERF_ABLMost.cpp:413-433)
+        if (c->use_terrain) return ERF_B200_ECONFIG;
         if (c->les_type != ERF_LES_SMAGORINSKY && c->les_type != ERF_LES_DEARDORFF) return ERF_B200_ECONFIG;
         if (!(c->most_z0 > 0.0) || !(c->most_zref >= 0.0) || !(c->most_zref < c->nz * c->dz)) return ERF_B200_ECONFIG;
         int k;

@@ -92,12 +92,12 @@ def test_create_rejects_bad_config_without_gpu(lib):
     assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
 
 
-@pytest.mark.parametrize("change", ["terrain", "no_closure", "mlp", "moist", "z0_above_zref", "zref_outside",
+@pytest.mark.parametrize("change", ["terrain", "no_closure", "mlp", "z0_above_zref", "zref_outside",
                                     "most_lid"])
 def test_create_rejects_unsupported_most_config(lib, change):
-    """A MOST ground is accepted flat, dry and under Smagorinsky or
-    Deardorff, with z0 below the snapped reference height, and only as the
-    lower boundary; the rest is refused before any CUDA call."""
+    """A MOST ground is accepted flat and under Smagorinsky or Deardorff,
+    with z0 below the snapped reference height, and only as the lower
+    boundary; the rest is refused before any CUDA call."""
     c = C.defaults()
     c.zlo_bc = C.BC_MOST
     c.les_type = C.LES_SMAGORINSKY
@@ -109,8 +109,6 @@ def test_create_rejects_unsupported_most_config(lib, change):
     elif change == "mlp":
         c.les_type = C.LES_MLP
         c.molec_diff_type = C.MOLEC_NONE
-    elif change == "moist":
-        c.moisture, c.ncomp = C.MOIST_KESSLER, 8
     elif change == "z0_above_zref":
         c.most_z0 = 0.5 * c.dz + 1.0   # above the first cell centre
         c.most_zref = 0.0
@@ -123,13 +121,17 @@ def test_create_rejects_unsupported_most_config(lib, change):
     assert lib.erf_b200_create(ctypes.byref(ctx), ctypes.byref(c), None) == 8  # ERF_B200_ECONFIG
 
 
-def test_create_accepts_most_config(lib):
-    """The supported MOST ground passes validation (without a GPU the create
-    call then fails at its first CUDA call, ERF_B200_ECUDA)."""
+@pytest.mark.parametrize("moist", [False, True])
+def test_create_accepts_most_config(lib, moist):
+    """The supported MOST ground passes validation, dry or with Kessler
+    moisture (without a GPU the create call then fails at its first CUDA
+    call, ERF_B200_ECUDA)."""
     c = C.defaults()
     c.zlo_bc = C.BC_MOST
     c.les_type = C.LES_DEARDORFF
     c.most_z0, c.most_zref = 0.1, 8.0
+    if moist:
+        c.moisture, c.ncomp = C.MOIST_KESSLER, 8
     ctx = ctypes.c_void_p()
     lib.erf_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p]
     lib.erf_b200_destroy.argtypes = [ctypes.c_void_p]

@@ -10,7 +10,9 @@ adiabatic, implicit MOST: BoundaryConditions/ERF_ABLMost.cpp:11-142 and
     reference height at the first cell centre, Deardorff with it at the
     second; with and without acoustic substepping);
   * the mixed form over the MOST ground within its budget (1e-2 after 100
-    steps), as the other mixed-form cases.
+    steps), as the other mixed-form cases;
+  * a moist (Kessler, buoyancy type 2) ABL over the MOST ground against the
+    oracle, Smagorinsky and Deardorff.
 """
 import os
 
@@ -94,3 +96,17 @@ def test_most_mixed_within_budget():
     print("mixed abl_most 24x20x16, 100 steps:", err)
     assert st == 0
     assert all(e <= 1e-2 for e in err.values()), err
+
+
+@pytest.mark.parametrize("les,zref", [("smagorinsky", 0.0), ("deardorff", 80.0)])
+def test_moist_most_matches_oracle(les, zref):
+    """The MOST ground under a moist (Kessler) ABL with buoyancy type 2: the
+    adiabatic ground adds no moisture flux, so the moist dycore runs over the
+    dry MOST rule; 10 steps, every field <= 1e-10 against the oracle."""
+    case = cases.abl_most_moist(nx=24, ny=20, nz=16, les=les, zref=zref)
+    errs, st, got, init = _run_both(case, 10)
+    print("moist MOST", les, zref, errs)
+    assert st == 0
+    bad = {k: v for k, v in errs.items() if not v <= TOL}
+    assert not bad, errs
+    assert got[1][0].mean() < init[1][0].mean()
