@@ -392,6 +392,44 @@ def terrain_arm(args, C, Dycore, stream, n_err=100):
     return out
 
 
+def moving_terrain_arm(args, C, Dycore, stream):
+    """Moving terrain: the reference's MovingTerrain physics (Sullivan grid
+    under a travelling surface wave, Centered_2nd, buoyancy type 1) at the
+    gold size (40 x 8 x 79, with 20 acoustic substeps per step) and on a
+    larger periodic grid with and without substeps; graph replay on a
+    device-resident state, plain FP64.  Each step regenerates the grid on
+    the device at every geometry time."""
+    import torch
+    from erf_b200 import terrain as T
+    runs = {
+        "gold_size_substeps": T.moving_terrain(substeps=True),
+        "large_substeps": T.moving_terrain(nx=512, ny=128, nz=79, Lx=2560.0, Ly=640.0, substeps=True),
+        "large_no_substep": T.moving_terrain(nx=512, ny=128, nz=79, Lx=2560.0, Ly=640.0),
+    }
+    out = {"workload": "moving terrain (MovingTerrain physics): 40x8x79 and 512x128x79 cells, dx=dy=5 m, "
+                       "400 m deep, 0.16 m wave of 100 m; dt 0.1 s with 20 substeps / dt 0.005 s without"}
+    for name, case in runs.items():
+        cfg = case.cfg
+        n_cells = cfg.nx * cfg.ny * cfg.nz
+        dy = Dycore(cfg, stream=stream.cuda_stream)
+        dy.set_base_state(case.base)
+        dy.load_state(*case.build_state())
+        dy.advance_resident(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dy.advance_resident(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        d = dy.diagnostics()
+        out[name] = {"cells": n_cells, "value": n_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                     "substeps_per_step": (cfg.mri_ratio if cfg.substepping_type == C.SUBSTEP_IMPLICIT else 0),
+                     "status": dy.status(), "mass": d["mass"]}
+        dy.close()
+    return out
+
+
 def cpu_baseline_run(case_fn, nx, ny, nz, nsteps):
     """Time the FP64 CPU oracle on a bounded sample of the workload; returns
     cell-steps/s, seconds, cores and the seconds of each pass."""
@@ -468,7 +506,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="moist_bubble", choices=sorted(cases.CASES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble", "terrain"],
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed", "learned", "ensemble", "terrain",
+                                                       "moving_terrain"],
                     help="precision forms to time (the JSON line needs both; single forms are for profiling)")
     ap.add_argument("--terrain-size", default="256x256x96",
                     help="cells of the terrain ABL (nx x ny x nz); smaller only for profiling")
@@ -671,6 +710,13 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return 0
+    if args.form == "moving_terrain":
+        if rank == 0:
+            print(json.dumps({"form": "moving_terrain", "moving_terrain": moving_terrain_arm(args, C, Dycore, stream)}),
+                  flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     if args.form == "learned":
         if rank == 0:
             print(json.dumps({"form": "learned", "learned": learned_arm(measure, form_error, C)}), flush=True)
@@ -706,6 +752,7 @@ def main():
     from erf_b200.dycore import Ensemble
     ensemble = ensemble_arm(args, C, Dycore, Ensemble, stream) if rank == 0 else None
     terrain_res = terrain_arm(args, C, Dycore, stream) if rank == 0 else None
+    mt_res = moving_terrain_arm(args, C, Dycore, stream) if rank == 0 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -743,6 +790,7 @@ def main():
             "learned": learned,
             "ensemble": ensemble,
             "terrain": terrain_res,
+            "moving_terrain": mt_res,
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clock_samples),
             "gpu_launches": plain["launches"],

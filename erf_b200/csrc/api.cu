@@ -97,7 +97,7 @@ struct erf_b200_ctx {
         double* zt;
         double *r0o, *p0o;
         double* time;
-        double *detJso, *zpt, *trhs, *om;   // acoustic substeps
+        double *detJso, *zpt, *trhs, *om, *soln;   // acoustic substeps
     } mt{};
     int ter_tx = 0;                                           // k_ter_fast_vert columns per block
     size_t ter_smem = 0;                                      // and its shared memory
@@ -201,10 +201,8 @@ int validate(const erf_b200_config* c) {
     if (c->terrain_type == ERF_TERRAIN_MOVING) {
         // moving terrain: the reference's MovingTerrain setting -- dry,
         // Centered_2nd dycore (asserted by slow_rhs_fun_pre), no diffusion,
-        // buoyancy type 1, slip walls; with acoustic substepping up to 512
-        // levels (the column kernel's local solution)
+        // buoyancy type 1, slip walls
         if (!c->use_terrain) return ERF_B200_ECONFIG;
-        if (c->substepping_type == ERF_SUBSTEP_IMPLICIT && c->nz > 512) return ERF_B200_ECONFIG;
         if (c->moisture != ERF_MOIST_NONE || c->les_type != ERF_LES_NONE || c->molec_diff_type != ERF_MOLEC_NONE)
             return ERF_B200_ECONFIG;
         if (c->dycore_horiz_adv != ERF_ADV_CENTERED_2ND || c->dycore_vert_adv != ERF_ADV_CENTERED_2ND)
@@ -530,7 +528,7 @@ void enqueue_step_mt(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
                                            1.0 / (double)nsub, ks == 0 ? OLD : SUM, Sst, Acur, B.Fcons, B.Fmx, B.Fmy,
                                            B.Fmz, B.lag[lp], B.lag[1 - lp], B.cA, B.cInvB, B.cCB, B.cP, B.cQ,
                                            c->mt.z[3], c->mt.z[4], c->mt.z[1], c->mt.zpt, c->mt.trhs, c->mt.om,
-                                           B.avx, B.avy, B.avz, SUM, ks == nsub - 1 ? 1 : 0));
+                                           c->mt.soln, B.avx, B.avy, B.avz, SUM, ks == nsub - 1 ? 1 : 0));
                 lp ^= 1;
             }
             Pp.znd = c->mt.z[3];
@@ -817,6 +815,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
             if (cfg->substepping_type == ERF_SUBSTEP_IMPLICIT) {
                 A(&c->mt.z[3], (size_t)(cfg->nz + 3) * sk); A(&c->mt.z[4], (size_t)(cfg->nz + 3) * sk);
                 A(&c->mt.detJso, N); A(&c->mt.zpt, NZF); A(&c->mt.trhs, 2 * N); A(&c->mt.om, NZF);
+                A(&c->mt.soln, NZF);
             }
         }
     }

@@ -208,7 +208,7 @@ void launch_mt_fast(const Params& P, cudaStream_t st, int step, int lagged, doub
                     StateBuf Sprev, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmx, const R* Fmy,
                     const R* Fmz, const R* lag_in, R* lag_out, const R* cA, const R* cInvB, const R* cCB, const R* cP,
                     const R* cQ, const double* zo, const double* zn, const double* zs, const double* zpt,
-                    double* trhs, double* om, R* avx, R* avy, R* avz, StateBuf Ssum, int last);
+                    double* trhs, double* om, double* soln, R* avx, R* avy, R* avz, StateBuf Ssum, int last);
 void launch_ter_base_state(const Params& P, cudaStream_t st, const double* zcc, const double* th3, const double* qv3,
                            double th_s, double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0);
 template <class R>

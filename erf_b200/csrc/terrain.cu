@@ -486,7 +486,6 @@ template void launch_mt_no_substep<float>(const Params&, cudaStream_t, double, S
 // the new grid's h_zeta; one thread per column solves for Omega'' and
 // updates rho w, rho and rho theta.
 // ---------------------------------------------------------------------------
-constexpr int MT_NZMAX = 512;   // levels of the column kernel's local solution
 
 __device__ __forceinline__ void mt_slopes(const double* z, const Geo& g, int i, int j, int k, double& sx, double& sy) {
     sx = 0.5 * g.dxi * (znode(z, g, i + 1, j + 1, k) + znode(z, g, i + 1, j, k) - znode(z, g, i, j + 1, k) - znode(z, g, i, j, k));
@@ -643,94 +642,129 @@ __global__ void k_mt_fast_div(Params P, double facinv, StateBuf Sst, const doubl
     avy[c] += R(facinv * (my - Sst.my[c]));
 }
 
-// One column per thread (ERF_fast_rhs_MT.cpp:375-600): the right-hand side
-// of the Omega'' system (old / new / stage face detJ, the stage's
-// coefficients made on the substep's old grid), the Thomas sweep, rho w on
-// the lid; then rho w from Omega'' (on the moving ground W from Omega =
-// rho (z_t + z_t'')), the vertical fluxes, the average contravariant
-// momentum, and rho / rho theta detJ-weighted old -> new.
+// The Omega'' column system (ERF_fast_rhs_MT.cpp:375-600) in four kernels:
+// its right-hand side (one thread per z face: the old / new / stage face
+// detJ, the stage's coefficients made on the substep's old grid), the
+// Thomas sweep (one thread per column, the only serial part), rho w from
+// Omega'' with the ground at W from Omega = rho (z_t + z_t'') (one thread
+// per face), then the vertical fluxes, the average contravariant momentum
+// and rho / rho theta detJ-weighted old -> new (one thread per cell).
+// soln: the right-hand side, then the solution, then the new Omega''.
 template <class R>
-__global__ void k_mt_fast_col(Params P, double dtau, double beta_1, double beta_2, double facinv, StateBuf Sprev,
-                              StateBuf Sst, StageAux<R> A, const R* __restrict__ Fcons, const R* __restrict__ Fmz,
-                              const R* __restrict__ cA, const R* __restrict__ cInvB, const R* __restrict__ cCB,
-                              const R* __restrict__ cP, const R* __restrict__ cQ, const double* __restrict__ zo,
-                              const double* __restrict__ zn, const double* __restrict__ zs,
-                              const double* __restrict__ zpt, const double* __restrict__ om,
-                              const double* __restrict__ trhs, R* __restrict__ avz, StateBuf Ssum) {
+__global__ void k_mt_col_rhs(Params P, double dtau, double beta_1, double beta_2, StateBuf Sprev, StateBuf Sst,
+                             StageAux<R> A, const R* __restrict__ Fcons, const R* __restrict__ Fmz,
+                             const R* __restrict__ cP, const R* __restrict__ cQ, const double* __restrict__ zo,
+                             const double* __restrict__ zn, const double* __restrict__ zs,
+                             const double* __restrict__ zpt, const double* __restrict__ om,
+                             const double* __restrict__ trhs, StateBuf Ssum, double* __restrict__ soln) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k > g.nz) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell;
+    auto C = [&](int kk) { return cidx(g, i, j, kk); };
+    const int64_t a = C(k);
+    if (k == 0) {
+        const double rho_on_bdy = 0.5 * (Sprev.cons[a] + Sprev.cons[a]);
+        soln[a] = rho_on_bdy * zpt[a];
+        return;
+    }
+    if (k == nz) {
+        soln[a] = 0.0;
+        return;
+    }
+    const double dzi = g.dzi, halfg = fabs(0.5 * -P.gravity);
+    auto th = [&](int kk) { return double(A.prim[C(clampk(kk, nz))]); };
+    auto fJ = [&](const double* z) { return 0.5 * (mt_detj(z, g, i, j, k) + mt_detj(z, g, i, j, k - 1)); };
+    const double Jo = fJ(zo), Jn = fJ(zn), Js = fJ(zs);
+    const double cp = double(cP[a]), cq = double(cQ[a]);
+    const double tlo = 0.5 * (th(k - 2) + th(k - 1)), tmid = 0.5 * (th(k - 1) + th(k)), thi = 0.5 * (th(k) + th(k + 1));
+    const int64_t b = C(k - 1);
+    double R0t = cp * Sprev.cons[N + a] * Jo + cq * Sprev.cons[N + b] * Jo
+                 - cp * Sst.cons[N + a] * Js - cq * Sst.cons[N + b] * Js
+                 - halfg * (Sprev.cons[a] + Sprev.cons[b]) * Jo
+                 + halfg * (Sst.cons[a] + Sst.cons[b]) * Js;
+    double R1t = -halfg * (double(Fcons[a]) + double(Fcons[b])) + (cp * double(Fcons[N + a]) + cq * double(Fcons[N + b]));
+    const double Okp1 = om[C(k + 1)], Ok = om[a], Okm1 = om[b];
+    R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + trhs[a] + trhs[b]);
+    R1t += -(cp * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + trhs[N + a]) +
+             cq * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + trhs[N + b]));
+    double rhs = Jo * Sprev.mz[a] - Js * Sst.mz[a] + dtau * (double(Fmz[a]) + R0t + dtau * beta_2 * R1t);
+    double un = mt_omega(zn, g, i, j, k, 0., Ssum.mx, Ssum.my);
+    double us = mt_omega(zs, g, i, j, k, 0., Sst.mx, Sst.my);
+    rhs += Jn * un - Js * us;
+    soln[a] = rhs;
+}
+template <class R>
+__global__ void k_mt_col_sweep(Params P, StateBuf Sst, const R* __restrict__ cA, const R* __restrict__ cInvB,
+                               const R* __restrict__ cCB, StateBuf Ssum, double* __restrict__ soln) {
     const Geo& g = P.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.nx || j >= g.ny) return;
     const int nz = g.nz;
-    const int64_t N = g.ncell;
-    const double dzi = g.dzi;
-    const double halfg = fabs(0.5 * -P.gravity);
-    double soln[MT_NZMAX + 1];
-    auto C = [&](int k) { return cidx(g, i, j, k); };
-    auto th = [&](int k) { return double(A.prim[C(clampk(k, nz))]); };
-    auto fJ = [&](const double* z, int k) { return 0.5 * (mt_detj(z, g, i, j, k) + mt_detj(z, g, i, j, k - 1)); };
-    // ground row
-    {
-        const double rho_on_bdy = 0.5 * (Sprev.cons[C(0)] + Sprev.cons[C(0)]);
-        soln[0] = (rho_on_bdy * zpt[C(0)]) * double(cInvB[C(0)]);
+    auto C = [&](int kk) { return cidx(g, i, j, kk); };
+    double s = soln[C(0)] * double(cInvB[C(0)]);
+    soln[C(0)] = s;
+    for (int k = 1; k <= nz; ++k) {
+        s = (soln[C(k)] - double(cA[C(k)]) * s) * double(cInvB[C(k)]);
+        soln[C(k)] = s;
     }
-    for (int k = 1; k < nz; ++k) {
-        const double Jo = fJ(zo, k), Jn = fJ(zn, k), Js = fJ(zs, k);
-        const double cp = double(cP[C(k)]), cq = double(cQ[C(k)]);
-        const double tlo = 0.5 * (th(k - 2) + th(k - 1)), tmid = 0.5 * (th(k - 1) + th(k)), thi = 0.5 * (th(k) + th(k + 1));
-        const int64_t a = C(k), b = C(k - 1);
-        double R0t = cp * Sprev.cons[N + a] * Jo + cq * Sprev.cons[N + b] * Jo
-                     - cp * Sst.cons[N + a] * Js - cq * Sst.cons[N + b] * Js
-                     - halfg * (Sprev.cons[a] + Sprev.cons[b]) * Jo
-                     + halfg * (Sst.cons[a] + Sst.cons[b]) * Js;
-        double R1t = -halfg * (double(Fcons[a]) + double(Fcons[b])) + (cp * double(Fcons[N + a]) + cq * double(Fcons[N + b]));
-        const double Okp1 = om[C(k + 1)], Ok = om[a], Okm1 = om[b];
-        R1t += (halfg) * (beta_1 * dzi * (Okp1 - Okm1) + trhs[a] + trhs[b]);
-        R1t += -(cp * (beta_1 * dzi * (Okp1 * thi - Ok * tmid) + trhs[N + a]) +
-                 cq * (beta_1 * dzi * (Ok * tmid - Okm1 * tlo) + trhs[N + b]));
-        double rhs = Jo * Sprev.mz[a] - Js * Sst.mz[a] + dtau * (double(Fmz[a]) + R0t + dtau * beta_2 * R1t);
-        double un = mt_omega(zn, g, i, j, k, 0., Ssum.mx, Ssum.my);
-        double us = mt_omega(zs, g, i, j, k, 0., Sst.mx, Sst.my);
-        rhs += Jn * un - Js * us;
-        soln[k] = (rhs - double(cA[a]) * soln[k - 1]) * double(cInvB[a]);
+    Ssum.mz[C(nz)] = Sst.mz[C(nz)] + s;
+    for (int k = nz - 1; k >= 0; --k) {
+        s = soln[C(k)] - double(cCB[C(k)]) * s;
+        soln[C(k)] = s;
     }
-    soln[nz] = (0.0 - double(cA[C(nz)]) * soln[nz - 1]) * double(cInvB[C(nz)]);
-    for (int k = nz - 1; k >= 0; --k) soln[k] = soln[k] - double(cCB[C(k)]) * soln[k + 1];
-    Ssum.mz[C(nz)] = Sst.mz[C(nz)] + soln[nz];
-    // rho w from Omega''
-    for (int k = 0; k < nz; ++k) {
-        const int64_t a = C(k);
-        const double rho_on_face = 0.5 * (Sprev.cons[a] + Sprev.cons[C(k > 0 ? k - 1 : 0)]);
-        if (k == 0) {
-            Ssum.mz[a] = mt_wfrom(zn, g, i, j, 0, rho_on_face * (P.mt_zt[a] + zpt[a]), Ssum.mx, Ssum.my);
-            soln[0] = 0.;
-        } else {
-            double wn = mt_wfrom(zn, g, i, j, k, 0.0, Ssum.mx, Ssum.my);
-            double ws = mt_wfrom(zs, g, i, j, k, 0.0, Sst.mx, Sst.my);
-            double wpp = soln[k] + (wn - ws);
-            double m = fJ(zo, k) * (Sst.mz[a] + wpp);
-            m /= fJ(zn, k);
-            Ssum.mz[a] = m;
-            double o1 = mt_omega(zn, g, i, j, k, m, Ssum.mx, Ssum.my);
-            double o2 = mt_omega(zs, g, i, j, k, Sst.mz[a], Sst.mx, Sst.my);
-            soln[k] = o1 - o2;
-            soln[k] -= rho_on_face * zpt[a];
-        }
+}
+template <class R>
+__global__ void k_mt_col_w(Params P, StateBuf Sprev, StateBuf Sst, const double* __restrict__ zo,
+                           const double* __restrict__ zn, const double* __restrict__ zs,
+                           const double* __restrict__ zpt, StateBuf Ssum, double* __restrict__ soln) {
+    const Geo& g = P.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const int64_t a = cidx(g, i, j, k);
+    const double rho_on_face = 0.5 * (Sprev.cons[a] + Sprev.cons[cidx(g, i, j, k > 0 ? k - 1 : 0)]);
+    if (k == 0) {
+        Ssum.mz[a] = mt_wfrom(zn, g, i, j, 0, rho_on_face * (P.mt_zt[a] + zpt[a]), Ssum.mx, Ssum.my);
+        soln[a] = 0.;
+        return;
     }
-    // rho and rho theta
-    for (int k = 0; k < nz; ++k) {
-        const int64_t a = C(k);
-        double zl = beta_2 * soln[k] + beta_1 * om[a];
-        double zh = beta_2 * soln[k + 1] + beta_1 * om[C(k + 1)];
-        avz[a] += R(facinv * zl / (1.0 * 1.0));
-        if (k == nz - 1) avz[C(k + 1)] += R(facinv * zh / (1.0 * 1.0));
-        const double Jo = mt_detj(zo, g, i, j, k), Jn = mt_detj(zn, g, i, j, k);
-        double frho = -(trhs[a] + (zh - zl) * dzi);
-        double tr = Jo * Sprev.cons[a] + dtau * (double(Fcons[a]) + frho);
-        double frt = -(trhs[N + a] + 0.5 * (zh * (th(k) + th(k + 1)) - zl * (th(k) + th(k - 1))) * dzi);
-        double tt = Jo * Sprev.cons[N + a] + dtau * (double(Fcons[N + a]) + frt);
-        Ssum.cons[a] = tr / Jn;
-        Ssum.cons[N + a] = tt / Jn;
-    }
+    auto fJ = [&](const double* z) { return 0.5 * (mt_detj(z, g, i, j, k) + mt_detj(z, g, i, j, k - 1)); };
+    double wn = mt_wfrom(zn, g, i, j, k, 0.0, Ssum.mx, Ssum.my);
+    double ws = mt_wfrom(zs, g, i, j, k, 0.0, Sst.mx, Sst.my);
+    double wpp = soln[a] + (wn - ws);
+    double m = fJ(zo) * (Sst.mz[a] + wpp);
+    m /= fJ(zn);
+    Ssum.mz[a] = m;
+    double o1 = mt_omega(zn, g, i, j, k, m, Ssum.mx, Ssum.my);
+    double o2 = mt_omega(zs, g, i, j, k, Sst.mz[a], Sst.mx, Sst.my);
+    double sv = o1 - o2;
+    sv -= rho_on_face * zpt[a];
+    soln[a] = sv;
+}
+template <class R>
+__global__ void k_mt_col_cons(Params P, double dtau, double beta_1, double beta_2, double facinv, StateBuf Sprev,
+                              StageAux<R> A, const R* __restrict__ Fcons, const double* __restrict__ zo,
+                              const double* __restrict__ zn, const double* __restrict__ om,
+                              const double* __restrict__ trhs, const double* __restrict__ soln,
+                              R* __restrict__ avz, StateBuf Ssum) {
+    const Geo& g = P.g;
+    int i, j, k;
+    if (!cell_ij(g, i, j, k)) return;
+    const int nz = g.nz;
+    const int64_t N = g.ncell, a = cidx(g, i, j, k), ah = cidx(g, i, j, k + 1);
+    auto th = [&](int kk) { return double(A.prim[cidx(g, i, j, clampk(kk, nz))]); };
+    double zl = beta_2 * soln[a] + beta_1 * om[a];
+    double zh = beta_2 * soln[ah] + beta_1 * om[ah];
+    avz[a] += R(facinv * zl / (1.0 * 1.0));
+    if (k == nz - 1) avz[ah] += R(facinv * zh / (1.0 * 1.0));
+    const double Jo = mt_detj(zo, g, i, j, k), Jn = mt_detj(zn, g, i, j, k);
+    double frho = -(trhs[a] + (zh - zl) * g.dzi);
+    double tr = Jo * Sprev.cons[a] + dtau * (double(Fcons[a]) + frho);
+    double frt = -(trhs[N + a] + 0.5 * (zh * (th(k) + th(k + 1)) - zl * (th(k) + th(k - 1))) * g.dzi);
+    double tt = Jo * Sprev.cons[N + a] + dtau * (double(Fcons[N + a]) + frt);
+    Ssum.cons[a] = tr / Jn;
+    Ssum.cons[N + a] = tt / Jn;
 }
 
 // the boundary fill after a substep (apply_bcs, fast variables): the
@@ -773,28 +807,31 @@ void launch_mt_fast(const Params& P, cudaStream_t st, int step, int lagged, doub
                     StateBuf Sprev, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmx, const R* Fmy,
                     const R* Fmz, const R* lag_in, R* lag_out, const R* cA, const R* cInvB, const R* cCB, const R* cP,
                     const R* cQ, const double* zo, const double* zn, const double* zs, const double* zpt,
-                    double* trhs, double* om, R* avx, R* avy, R* avz, StateBuf Ssum, int last) {
+                    double* trhs, double* om, double* soln, R* avx, R* avy, R* avz, StateBuf Ssum, int last) {
     const Geo& g = P.g;
     const double beta_1 = 0.5 * (1.0 - beta_s), beta_2 = 0.5 * (1.0 + beta_s);
     k_mt_fast_h<R><<<ter_grid(g, g.nz), ter_block(), 0, st>>>(P, step, lagged, dtau, Sprev, Sst, A, Fmx, Fmy, lag_in,
                                                               lag_out, zo, Ssum);
     k_mt_fast_flux<R><<<ter_grid(g, g.nz + 1), ter_block(), 0, st>>>(P, Sprev, Sst, A, Ssum, zo, zs, zpt, trhs, om);
     k_mt_fast_div<R><<<ter_grid(g, g.nz), ter_block(), 0, st>>>(P, facinv, Sst, zn, Ssum, avx, avy);
-    k_mt_fast_col<R><<<ter_grid(g, 1), ter_block(), 0, st>>>(P, dtau, beta_1, beta_2, facinv, Sprev, Sst, A, Fcons, Fmz,
-                                                            cA, cInvB, cCB, cP, cQ, zo, zn, zs, zpt, om, trhs, avz,
-                                                            Ssum);
+    k_mt_col_rhs<R><<<ter_grid(g, g.nz + 1), ter_block(), 0, st>>>(P, dtau, beta_1, beta_2, Sprev, Sst, A, Fcons, Fmz,
+                                                                  cP, cQ, zo, zn, zs, zpt, om, trhs, Ssum, soln);
+    k_mt_col_sweep<R><<<ter_grid(g, 1), ter_block(), 0, st>>>(P, Sst, cA, cInvB, cCB, Ssum, soln);
+    k_mt_col_w<R><<<ter_grid(g, g.nz), ter_block(), 0, st>>>(P, Sprev, Sst, zo, zn, zs, zpt, Ssum, soln);
+    k_mt_col_cons<R><<<ter_grid(g, g.nz), ter_block(), 0, st>>>(P, dtau, beta_1, beta_2, facinv, Sprev, A, Fcons, zo, zn,
+                                                                om, trhs, soln, avz, Ssum);
     if (!last) k_mt_fast_bc<<<ter_grid(g, g.nz + 1), ter_block(), 0, st>>>(P, Ssum);
 }
 template void launch_mt_fast<double>(const Params&, cudaStream_t, int, int, double, double, double, StateBuf, StateBuf,
                                      StageAux<double>, const double*, const double*, const double*, const double*,
                                      const double*, double*, const double*, const double*, const double*,
                                      const double*, const double*, const double*, const double*, const double*,
-                                     const double*, double*, double*, double*, double*, double*, StateBuf, int);
+                                     const double*, double*, double*, double*, double*, double*, double*, StateBuf, int);
 template void launch_mt_fast<float>(const Params&, cudaStream_t, int, int, double, double, double, StateBuf, StateBuf,
                                     StageAux<float>, const float*, const float*, const float*, const float*,
                                     const float*, float*, const float*, const float*, const float*, const float*,
                                     const float*, const double*, const double*, const double*, const double*, double*,
-                                    double*, float*, float*, float*, StateBuf, int);
+                                    double*, double*, float*, float*, float*, StateBuf, int);
 
 // ---------------------------------------------------------------------------
 // Step diagnostics of a resident state (sum_integrated_quantities /

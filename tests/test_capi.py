@@ -141,21 +141,18 @@ def test_create_accepts_most_config(lib, moist):
         lib.erf_b200_destroy(ctx)
 
 
-@pytest.mark.parametrize("change", ["static_flag", "tall_substepped", "moist", "les", "molec", "upwind", "buoyancy",
+@pytest.mark.parametrize("change", ["static_flag", "moist", "les", "molec", "upwind", "buoyancy",
                                     "noslip", "wavelength", "bad_type", "unlagged_static"])
 def test_create_rejects_unsupported_moving_terrain(lib, change):
     """Moving terrain is accepted as the reference's MovingTerrain problems
     run it: dry, no diffusion, Centered_2nd dycore, buoyancy type 1, slip
-    walls, with or without acoustic substepping (up to 512 levels with);
-    use_lagged_delta_rt = false only there; the rest is refused before any
+    walls, with or without acoustic substepping; use_lagged_delta_rt =
+    false only there; the rest is refused before any
     CUDA call."""
     from erf_b200 import terrain as T
     c = T.moving_terrain(nx=8, ny=4, nz=10).cfg
     if change == "static_flag":
         c.use_terrain = 0
-    elif change == "tall_substepped":
-        c.substepping_type = C.SUBSTEP_IMPLICIT
-        c.nz = 513
     elif change == "unlagged_static":
         c = C.defaults()
         c.no_lagged_delta_rt = 1
