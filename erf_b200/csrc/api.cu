@@ -98,6 +98,7 @@ struct erf_b200_ctx {
         double *r0o, *p0o;
         double* time;
         double *detJso, *zpt, *trhs, *om, *soln;   // acoustic substeps
+        double* fac;                              // Sullivan's factor per level
     } mt{};
     int ter_tx = 0;                                           // k_ter_fast_vert columns per block
     size_t ter_smem = 0;                                      // and its shared memory
@@ -269,6 +270,7 @@ void make_params(erf_b200_ctx* c) {
     P.met = c->met;
     P.mt_zt = nullptr;
     P.mt_znew = nullptr;
+    P.mt_fac = c->mt.fac;
     {
         const double PI = 3.14159265358979323846264338327950288;
         P.mt_ampl = f.mt_ampl;
@@ -517,23 +519,26 @@ void enqueue_step_mt(erf_b200_ctx* c, Bulk<R>& B, int p, LaunchTimer* T) {
             Pf.detJ = c->mt.detJso;
             Pf.r0 = c->mt.r0o;
             int lp = 0;
+            // the substep grids alternate: a substep's new grid is the next one's old grid
+            double *zso = c->mt.z[3], *zsn = c->mt.z[4];
+            launch_mt_grid_sub(Po, st, c->mt.time, dtau, 0, zso);
             for (int ks = 0; ks < nsub; ++ks) {
-                launch_mt_grid_sub(Po, st, c->mt.time, dtau, ks, c->mt.z[3]);
-                launch_mt_grid_sub(Po, st, c->mt.time, dtau, ks + 1, c->mt.z[4]);
-                launch_mt_zpt(Po, st, c->mt.z[3], c->mt.z[4], dtau, c->mt.zpt);
-                launch_mt_detj(Po, st, c->mt.z[3], c->mt.detJso);
+                if (ks > 0) std::swap(zso, zsn);
+                launch_mt_grid_sub(Po, st, c->mt.time, dtau, ks + 1, zsn);
+                launch_mt_zpt(Po, st, zso, zsn, dtau, c->mt.zpt);
+                launch_mt_detj(Po, st, zso, c->mt.detJso);
                 TIMED(9, launch_fast_coef<R>(Pf, st, tg, tcb, c->coef_smem, D, Sst, Acur, B.cA, B.cInvB, B.cCB, B.cP,
                                              B.cQ));
                 TIMED(6, launch_mt_fast<R>(Po, st, ks, c->cfg.no_lagged_delta_rt ? 0 : 1, dtau, beta_s,
                                            1.0 / (double)nsub, ks == 0 ? OLD : SUM, Sst, Acur, B.Fcons, B.Fmx, B.Fmy,
                                            B.Fmz, B.lag[lp], B.lag[1 - lp], B.cA, B.cInvB, B.cCB, B.cP, B.cQ,
-                                           c->mt.z[3], c->mt.z[4], c->mt.z[1], c->mt.zpt, c->mt.trhs, c->mt.om,
+                                           zso, zsn, c->mt.z[1], c->mt.zpt, c->mt.trhs, c->mt.om,
                                            c->mt.soln, B.avx, B.avy, B.avz, SUM, ks == nsub - 1 ? 1 : 0));
                 lp ^= 1;
             }
-            Pp.znd = c->mt.z[3];
+            Pp.znd = zso;
             Pp.detJ = c->mt.detJso;
-            Pp.mt_znew = c->mt.z[4];
+            Pp.mt_znew = zsn;
         }
         TIMED(7, launch_ter_post<R>(Pp, st, c->tkz.ter_post, slow_dt, OLD, Sst, SUM, Snew, Acur, Anext,
                                     nrk < 2 ? 1 : 0, B.mut, B.tke, B.ter, B.avx, B.avy, B.avz, Vnew[0], Vnew[1],
@@ -811,6 +816,7 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
             A(&c->mt.zt, NZF);
             A(&c->mt.r0o, (size_t)(cfg->nz + 2) * sk); A(&c->mt.p0o, (size_t)(cfg->nz + 2) * sk);
             A(&c->mt.time, 1);
+            A(&c->mt.fac, (size_t)cfg->nz + 1);
             if (rc == ERF_B200_OK) cudaMemsetAsync(c->mt.time, 0, sizeof(double), c->stream);
             if (cfg->substepping_type == ERF_SUBSTEP_IMPLICIT) {
                 A(&c->mt.z[3], (size_t)(cfg->nz + 3) * sk); A(&c->mt.z[4], (size_t)(cfg->nz + 3) * sk);
@@ -827,7 +833,20 @@ int erf_b200_create(erf_b200_ctx** out, const erf_b200_config* cfg, void* stream
     if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
     make_params(c);
     // a moving grid is generated by the step itself
-    if (cfg->use_terrain && cfg->terrain_type == ERF_TERRAIN_MOVING) c->ter_set = true;
+    if (cfg->use_terrain && cfg->terrain_type == ERF_TERRAIN_MOVING) {
+        c->ter_set = true;
+        // Sullivan's factor (1 - z_k / z_top)^3 of each level, formed on the
+        // host with the C library's pow as init_which_terrain_grid's is
+        std::vector<double> fac((size_t)cfg->nz + 1);
+        const double ztop = cfg->nz * cfg->dz;
+        for (int k = 0; k <= cfg->nz; ++k) {
+            const double zl = k * cfg->dz;
+            fac[k] = std::pow(1. - zl / ztop, 3.0);
+        }
+        if (cudaMemcpy(c->mt.fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = ERF_B200_ECUDA;
+        if (rc != ERF_B200_OK) { erf_b200_destroy(c); return rc; }
+    }
     if (c->mixed) tiled_setup<float>(c->P, &c->tkz);
     else tiled_setup<double>(c->P, &c->tkz);
     c->tkz.ter_post = !cfg->use_terrain ? 0 : (c->mixed ? ter_post_kz<float>(c->P) : ter_post_kz<double>(c->P));

@@ -40,6 +40,7 @@ struct Params {
     // h = mt_ampl sin(mt_kp x - mt_om t) on x = i mt_dx, levels k mt_dz
     const double* mt_zt;
     const double* mt_znew;
+    const double* mt_fac;       // Sullivan's factor of each level (nz+1)
     double mt_ampl, mt_kp, mt_om, mt_dx, mt_dz;
     // MOST ground (Moeng stress, adiabatic): the level of the reference
     // height, the step's plane means {u, v, |U|, u*} (most_avg, device), the

@@ -332,14 +332,16 @@ __global__ void k_mt_grid(Params P, const double* __restrict__ tdev, double dt, 
     // tsel >= 0: a stage point; tsel < 0: substep -1 - tsel of length dt, T + ks dt
     const double t = tsel >= 0 ? mt_time_at(*tdev, dt, tsel) : *tdev + (-1 - tsel) * dt;
     const double x = i * P.mt_dx;
-    const double hs = P.mt_ampl * sin(P.mt_kp * x - P.mt_om * t);
+    // products and sums rounded one at a time, as the host C++ of the
+    // reference forms them (no fused multiply-add): the grid's node heights
+    // enter z_t through differences over a substep, which magnify any change
+    const double hs = __dmul_rn(P.mt_ampl, sin(__dsub_rn(__dmul_rn(P.mt_kp, x), __dmul_rn(P.mt_om, t))));
     const int nz = g.nz;
-    const double ztop = nz * P.mt_dz;
     double* col = z + (int64_t)j * g.nx + i;
     double zk1 = 0.0, zkm1 = 0.0, zk = hs;
     for (int k = 0; k <= nz; ++k) {
         const double zl = k * P.mt_dz;
-        double v = zl + pow(1. - zl / ztop, 3.0) * hs;
+        double v = __dadd_rn(zl, __dmul_rn(P.mt_fac[k], hs));
         if (k == 0) v = hs;
         col[(int64_t)(k + 1) * g.sk] = v;
         if (k == 1) zk1 = v;
