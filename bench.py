@@ -634,13 +634,20 @@ def main():
         dominant = max(kern, key=lambda k: kern[k]["total_ms"])
         dk = kern[dominant]
         form = "mixed" if precision == C.PREC_MIXED else "fp64"
-        traffic = None
+        # DRAM bytes per launch of the dominant kernel from the committed ncu
+        # capture (dram__bytes_read.sum + dram__bytes_write.sum); the capture
+        # names the library build it measured, reported beside the figure
+        traffic, traffic_src = None, None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             with open(tpath) as fh:
-                traffic = json.load(fh).get(f"{args.case}/{form}", {}).get(dominant)
+                tj = json.load(fh)
+            traffic = tj.get(f"{args.case}/{form}", {}).get(dominant)
+            if traffic is not None:
+                traffic_src = {k: tj.get(k) for k in ("captured", "library_sha16", "command")}
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm, "unit": "GB/s",
-                    "frac": dk["gbs"] / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                    "frac": dk["gbs"] / hbm, "traffic": traffic, "traffic_source": traffic_src,
+                    "peak_kind": peak_kind,
                     "algo_bytes_per_launch": dk["algo_bytes"], "ms_per_launch": dk["ms_per_launch"]}
         step_bytes = sum(bpc[k] * n_cells * (kern[k]["launches"] / args.steps) for k in kern)
         roof_cells = hbm * 1e9 / (step_bytes / n_cells)
