@@ -23,7 +23,11 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liberf_b200.so")
 OBJ_BOUNDS = os.path.join(HERE, "_build_bounds")
 LIB_BOUNDS = os.path.join(HERE, "liberf_b200_bounds.so")
-SOURCES = ["kernels.cu", "terrain.cu", "api.cu", "noalloc.cu", "mlp.cu", "closure.cu", "plotfile.cu", "checkpoint.cu"]
+# the two terrain halves take longest, so they start first
+SOURCES = ["terrain.cu", "terrain_f32.cu", "kernels.cu", "api.cu", "noalloc.cu", "mlp.cu", "closure.cu", "plotfile.cu",
+           "checkpoint.cu"]
+# sources a translation unit includes besides the headers
+INCLUDED = {"terrain_f32.cu": ["terrain.cu"]}
 HEADERS = ["common.cuh", "kernels.cuh", "tiles.cuh", "tcgen05.cuh", "mlp.cuh", "amrex_io.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -45,7 +49,7 @@ def build(force: bool = False, verbose: bool = False, bounds: bool = False) -> s
     os.makedirs(OBJ, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "erf_b200.h")]
     objs = [os.path.join(OBJ, s.replace(".cu", ".o")) for s in SOURCES]
-    todo = [(s, o) for s, o in zip(SOURCES, objs) if force or _stale(o, [os.path.join(CSRC, s)] + hdrs)]
+    todo = [(s, o) for s, o in zip(SOURCES, objs) if force or _stale(o, [os.path.join(CSRC, d) for d in [s] + INCLUDED.get(s, [])] + hdrs)]
 
     def compile_one(job):
         s, obj = job

@@ -30,6 +30,15 @@
 #include "kernels.cuh"
 #include "tiles.cuh"
 
+// The library compiles this file twice so that the two halves build side by
+// side: as terrain.cu (ERFB_TER_F32 0: every non-template definition and the
+// FP64 instantiations) and through terrain_f32.cu (ERFB_TER_F32 1: the FP32
+// instantiations only).  Kernels that are not templates are static, so each
+// half may hold its own copy of those it launches.
+#ifndef ERFB_TER_F32
+#define ERFB_TER_F32 0
+#endif
+
 namespace erfb {
 namespace {
 
@@ -253,7 +262,7 @@ dim3 ter_grid(const Geo& g, int nk) { return dim3((g.nx + 31) / 32, (g.ny + 3) /
 // Metrics: detJ per cell and z at cell centres (levels 0..nz, the top one
 // from the extrapolated node level).
 // ---------------------------------------------------------------------------
-__global__ void k_ter_metrics(Params P, double* __restrict__ detJ, double* __restrict__ zcc) {
+static __global__ void k_ter_metrics(Params P, double* __restrict__ detJ, double* __restrict__ zcc) {
     const Geo& g = P.g;
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -265,7 +274,7 @@ __global__ void k_ter_metrics(Params P, double* __restrict__ detJ, double* __res
                                     + Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1));
 }
 // The metric tables (k in [0, nz] for every plane)
-__global__ void k_ter_met_tables(Params P, double* __restrict__ met) {
+static __global__ void k_ter_met_tables(Params P, double* __restrict__ met) {
     const Geo& g = P.g;
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -293,10 +302,12 @@ __global__ void k_ter_met_tables(Params P, double* __restrict__ met) {
     m[MT_HXI_EI * s] = hxi_EI_fn(P, i, j, k);
     m[MT_HETA_EI * s] = heta_EI_fn(P, i, j, k);
 }
+#if !ERFB_TER_F32
 void launch_ter_metrics(const Params& P, cudaStream_t st, double* detJ, double* zcc) {
     k_ter_metrics<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, detJ, zcc);
     k_ter_met_tables<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, const_cast<double*>(P.met));
 }
+#endif
 
 // ---------------------------------------------------------------------------
 // Moving terrain (terrain_type Moving), without acoustic substepping.  The
@@ -325,7 +336,7 @@ __device__ __forceinline__ double mt_detj(const double* z, const Geo& g, int i, 
 // with terrain_smoothing = 2 (Utils/ERF_TerrainMetrics.cpp:501-536, 320-333):
 // z(k) = z_k + (1 - z_k / z_top)^3 h over z_k = k dz, z(0) = h,
 // z(-1) = 2 h - z(1), z(nz+1) = 2 z(nz) - z(nz-1).  One thread per column.
-__global__ void k_mt_grid(Params P, const double* __restrict__ tdev, double dt, int tsel, double* __restrict__ z) {
+static __global__ void k_mt_grid(Params P, const double* __restrict__ tdev, double dt, int tsel, double* __restrict__ z) {
     const Geo& g = P.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.nx || j >= g.ny) return;
@@ -351,13 +362,15 @@ __global__ void k_mt_grid(Params P, const double* __restrict__ tdev, double dt, 
     col[0] = 2.0 * hs - zk1;
     col[(int64_t)(nz + 2) * g.sk] = 2.0 * zk - zkm1;
 }
+#if !ERFB_TER_F32
 void launch_mt_grid(const Params& P, cudaStream_t st, const double* tdev, double dt, int tsel, double* z) {
     k_mt_grid<<<ter_grid(P.g, 1), ter_block(), 0, st>>>(P, tdev, dt, tsel, z);
 }
+#endif
 
 // z_t of the stage (ERF_TI_slow_rhs_fun.H:84-107): (z_new - z_old) / slow_dt
 // averaged over the four nodes of each z face, slow_dt = new stage time - T.
-__global__ void k_mt_zt(Params P, const double* __restrict__ zo, const double* __restrict__ zn,
+static __global__ void k_mt_zt(Params P, const double* __restrict__ zo, const double* __restrict__ zn,
                         const double* __restrict__ tdev, double dt, int tsel_new, double* __restrict__ zt) {
     const Geo& g = P.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
@@ -369,10 +382,12 @@ __global__ void k_mt_zt(Params P, const double* __restrict__ zo, const double* _
     zt[cidx(g, i, j, k)] = 0.25 * inv_dt * (N(i + 1, j + 1) - O(i + 1, j + 1) + N(i, j + 1) - O(i, j + 1)
                                             + N(i + 1, j) - O(i + 1, j) + N(i, j) - O(i, j));
 }
+#if !ERFB_TER_F32
 void launch_mt_zt(const Params& P, cudaStream_t st, const double* zo, const double* zn, const double* tdev,
                   double dt, int tsel_new, double* zt) {
     k_mt_zt<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, zo, zn, tdev, dt, tsel_new, zt);
 }
+#endif
 
 // The base-state update of a moving-terrain stage (ERF_TI_slow_rhs_fun.H:149-210):
 // rho_0 and (rho theta)_0 advanced from the step's old base state by the
@@ -380,7 +395,7 @@ void launch_mt_zt(const Params& P, cudaStream_t st, const double* zo, const doub
 // detJ-weighted old -> source -> new; p_0 from (rho theta)_0.  One thread
 // per column walks up the levels, keeping the level below (already
 // overwritten) in registers; the ghost levels are not updated.
-__global__ void k_mt_base_state(Params P, const double* __restrict__ r0o, const double* __restrict__ p0o,
+static __global__ void k_mt_base_state(Params P, const double* __restrict__ r0o, const double* __restrict__ p0o,
                                 const double* __restrict__ zo, const double* __restrict__ zs,
                                 const double* __restrict__ zn, const double* __restrict__ tdev, double dt,
                                 int tsel_new, double* __restrict__ r0n, double* __restrict__ p0n) {
@@ -412,11 +427,13 @@ __global__ void k_mt_base_state(Params P, const double* __restrict__ r0o, const 
         r_m = r_c; rt_m = rt_c; r_c = r_p; rt_c = rt_p;
     }
 }
+#if !ERFB_TER_F32
 void launch_mt_base_state(const Params& P, cudaStream_t st, const double* r0o, const double* p0o, const double* zo,
                           const double* zs, const double* zn, const double* tdev, double dt, int tsel_new,
                           double* r0n, double* p0n) {
     k_mt_base_state<<<ter_grid(P.g, 1), ter_block(), 0, st>>>(P, r0o, p0o, zo, zs, zn, tdev, dt, tsel_new, r0n, p0n);
 }
+#endif
 
 // no_substep_fun for moving terrain (TimeIntegration/ERF_TI_no_substep_fun.H:54-109),
 // part 1: rho and rho theta detJ-weighted old -> new, the horizontal
@@ -474,10 +491,13 @@ void launch_mt_no_substep(const Params& P, cudaStream_t st, double slow_dt, Stat
     k_mt_no_substep_h<R><<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, slow_dt, Sold, Fcons, Fmx, Fmy, zo, zn, Ssum);
     k_mt_no_substep_w<R><<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, slow_dt, Sold, Fmz, zo, zn, Ssum);
 }
+#if !ERFB_TER_F32
 template void launch_mt_no_substep<double>(const Params&, cudaStream_t, double, StateBuf, const double*, const double*,
                                            const double*, const double*, const double*, const double*, StateBuf);
+#else
 template void launch_mt_no_substep<float>(const Params&, cudaStream_t, double, StateBuf, const float*, const float*,
                                           const float*, const float*, const double*, const double*, StateBuf);
+#endif
 
 // ---------------------------------------------------------------------------
 // Acoustic substeps over moving terrain (erf_fast_rhs_MT,
@@ -524,7 +544,7 @@ __device__ __forceinline__ double mt_wfrom(const double* z, const Geo& g, int i,
 }
 
 // the substep's z_t less the stage's (ERF_TI_fast_rhs_fun.H:66-90)
-__global__ void k_mt_zpt(Params P, const double* __restrict__ zo, const double* __restrict__ zn, double inv_dt,
+static __global__ void k_mt_zpt(Params P, const double* __restrict__ zo, const double* __restrict__ zn, double inv_dt,
                          double* __restrict__ zpt) {
     const Geo& g = P.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
@@ -536,7 +556,7 @@ __global__ void k_mt_zpt(Params P, const double* __restrict__ zo, const double* 
     zpt[f] = v - P.mt_zt[f];
 }
 // detJ of a grid's cells (make_J)
-__global__ void k_mt_detj(Params P, const double* __restrict__ z, double* __restrict__ detJ) {
+static __global__ void k_mt_detj(Params P, const double* __restrict__ z, double* __restrict__ detJ) {
     const Geo& g = P.g;
     int i, j, k;
     if (!cell_ij(g, i, j, k)) return;
@@ -772,7 +792,7 @@ __global__ void k_mt_col_cons(Params P, double dtau, double beta_1, double beta_
 // the boundary fill after a substep (apply_bcs, fast variables): the
 // momenta through M -> V -> M with the walls' density ghosts; w on the flat
 // lid from Omega = 0, the moving ground untouched but round-tripped
-__global__ void k_mt_fast_bc(Params P, StateBuf Ssum) {
+static __global__ void k_mt_fast_bc(Params P, StateBuf Ssum) {
     const Geo& g = P.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -795,15 +815,21 @@ __global__ void k_mt_fast_bc(Params P, StateBuf Ssum) {
     }
 }
 
+#if !ERFB_TER_F32
 void launch_mt_grid_sub(const Params& P, cudaStream_t st, const double* tdev, double dtau, int ks, double* z) {
     k_mt_grid<<<ter_grid(P.g, 1), ter_block(), 0, st>>>(P, tdev, dtau, -1 - ks, z);
 }
+#endif
+#if !ERFB_TER_F32
 void launch_mt_zpt(const Params& P, cudaStream_t st, const double* zo, const double* zn, double dtau, double* zpt) {
     k_mt_zpt<<<ter_grid(P.g, P.g.nz + 1), ter_block(), 0, st>>>(P, zo, zn, 1. / dtau, zpt);
 }
+#endif
+#if !ERFB_TER_F32
 void launch_mt_detj(const Params& P, cudaStream_t st, const double* z, double* detJ) {
     k_mt_detj<<<ter_grid(P.g, P.g.nz), ter_block(), 0, st>>>(P, z, detJ);
 }
+#endif
 template <class R>
 void launch_mt_fast(const Params& P, cudaStream_t st, int step, int lagged, double dtau, double beta_s, double facinv,
                     StateBuf Sprev, StateBuf Sst, StageAux<R> A, const R* Fcons, const R* Fmx, const R* Fmy,
@@ -824,16 +850,19 @@ void launch_mt_fast(const Params& P, cudaStream_t st, int step, int lagged, doub
                                                                 om, trhs, soln, avz, Ssum);
     if (!last) k_mt_fast_bc<<<ter_grid(g, g.nz + 1), ter_block(), 0, st>>>(P, Ssum);
 }
+#if !ERFB_TER_F32
 template void launch_mt_fast<double>(const Params&, cudaStream_t, int, int, double, double, double, StateBuf, StateBuf,
                                      StageAux<double>, const double*, const double*, const double*, const double*,
                                      const double*, double*, const double*, const double*, const double*,
                                      const double*, const double*, const double*, const double*, const double*,
                                      const double*, double*, double*, double*, double*, double*, double*, StateBuf, int);
+#else
 template void launch_mt_fast<float>(const Params&, cudaStream_t, int, int, double, double, double, StateBuf, StateBuf,
                                     StageAux<float>, const float*, const float*, const float*, const float*,
                                     const float*, float*, const float*, const float*, const float*, const float*,
                                     const float*, const double*, const double*, const double*, const double*, double*,
                                     double*, double*, float*, float*, float*, StateBuf, int);
+#endif
 
 // ---------------------------------------------------------------------------
 // Step diagnostics of a resident state (sum_integrated_quantities /
@@ -845,7 +874,7 @@ template void launch_mt_fast<float>(const Params&, cudaStream_t, int, int, doubl
 // scheduling.
 // ---------------------------------------------------------------------------
 constexpr int DIAG_BLOCKS = 592, DIAG_THREADS = 256;
-__global__ void __launch_bounds__(DIAG_THREADS) k_diag_partial(Params P, const double* __restrict__ cons,
+static __global__ void __launch_bounds__(DIAG_THREADS) k_diag_partial(Params P, const double* __restrict__ cons,
                                                                const double* __restrict__ w,
                                                                const double* __restrict__ zgrid,
                                                                double* __restrict__ part) {
@@ -879,23 +908,29 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_diag_partial(Params P, const d
         part[3 * blockIdx.x] = sm[0][0]; part[3 * blockIdx.x + 1] = sm[1][0]; part[3 * blockIdx.x + 2] = sm[2][0];
     }
 }
-__global__ void k_diag_final(Params P, const double* __restrict__ part, int nb, double* __restrict__ out) {
+static __global__ void k_diag_final(Params P, const double* __restrict__ part, int nb, double* __restrict__ out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double m = 0.0, rt = 0.0, wm = 0.0;
     for (int b = 0; b < nb; ++b) { m += part[3 * b]; rt += part[3 * b + 1]; wm = fmax(wm, part[3 * b + 2]); }
     const double vol = 1.0 / (P.g.dxi * P.g.dyi * P.g.dzi);
     out[0] = m * vol; out[1] = rt * vol; out[2] = wm;
 }
+#if !ERFB_TER_F32
 void launch_diagnostics(const Params& P, cudaStream_t st, const double* cons, const double* w, const double* zgrid,
                         double* part, double* out) {
     k_diag_partial<<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(P, cons, w, zgrid, part);
     k_diag_final<<<1, 32, 0, st>>>(P, part, DIAG_BLOCKS, out);
 }
+#endif
+#if !ERFB_TER_F32
 int diagnostics_scratch_doubles() { return 3 * DIAG_BLOCKS + 3; }
+#endif
 
 // post_timestep's clock (ERF.cpp:547-559 with t_new = t_old + dt)
-__global__ void k_mt_advance_time(double* t, double dt) { *t = *t + dt; }
+static __global__ void k_mt_advance_time(double* t, double dt) { *t = *t + dt; }
+#if !ERFB_TER_F32
 void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt) { k_mt_advance_time<<<1, 1, 0, st>>>(tdev, dt); }
+#endif
 
 // ---------------------------------------------------------------------------
 // Base state over the terrain, one thread per column: calc_rho_p Newton
@@ -903,7 +938,7 @@ void launch_mt_advance_time(cudaStream_t st, double* tdev, double dt) { k_mt_adv
 // (ERF_InputSoundingData.H:176-256), then erf_enforce_hse with terrain
 // (ERF_init1d.cpp:152-241).  Output (nz+2) planes, plane k+1 for level k.
 // ---------------------------------------------------------------------------
-__global__ void k_ter_base_state(Params P, const double* __restrict__ zcc, const double* __restrict__ th3,
+static __global__ void k_ter_base_state(Params P, const double* __restrict__ zcc, const double* __restrict__ th3,
                                  const double* __restrict__ qv3, double th_s, double qv_s, double p_s,
                                  double* __restrict__ rho0, double* __restrict__ p0o, double* __restrict__ pi0o,
                                  double* __restrict__ th0o) {
@@ -966,11 +1001,13 @@ __global__ void k_ter_base_state(Params P, const double* __restrict__ zcc, const
         put(kk, pprev);
     }
 }
+#if !ERFB_TER_F32
 void launch_ter_base_state(const Params& P, cudaStream_t st, const double* zcc, const double* th3, const double* qv3,
                            double th_s, double qv_s, double p_s, double* rho0, double* p0, double* pi0, double* th0) {
     dim3 b(32, 4, 1), gr((P.g.nx + 31) / 32, (P.g.ny + 3) / 4, 1);
     k_ter_base_state<<<gr, b, 0, st>>>(P, zcc, th3, qv3, th_s, qv_s, p_s, rho0, p0, pi0, th0);
 }
+#endif
 
 
 namespace {
@@ -2283,6 +2320,12 @@ void launch_ter_fast_vert(const Params& P, cudaStream_t st, int tx, size_t smem,
 }
 // Columns per block of k_ter_fast_vert (the widest power of two up to 32 whose
 // FP64 column arrays fit) and its shared memory; 0 columns if none fits.
+template <class R>
+void ter_vert_attr(size_t smem) {
+    cudaFuncSetAttribute(k_ter_fast_vert<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+#if !ERFB_TER_F32
+extern template void ter_vert_attr<float>(size_t);
 void ter_vert_shape(int nz, int* tx, size_t* smem) {
     int dev = 0, maxopt = 0;
     cudaGetDevice(&dev);
@@ -2292,10 +2335,11 @@ void ter_vert_shape(int nz, int* tx, size_t* smem) {
     *tx = t;
     *smem = t >= 1 ? (size_t)(7 * nz + 5) * t * sizeof(double) : 0;
     if (t >= 1) {
-        cudaFuncSetAttribute(k_ter_fast_vert<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
-        cudaFuncSetAttribute(k_ter_fast_vert<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+        ter_vert_attr<double>(*smem);
+        ter_vert_attr<float>(*smem);
     }
 }
+#endif
 namespace {
 // The tiled post pass per scheme: dry scalars (and KE) and moisture
 // species compile-time Upwind5 / WENO5 where the configuration has them,
@@ -2356,10 +2400,14 @@ int ter_post_kz(const Params& P) {
     template void launch_ter_post<R>(const Params&, cudaStream_t, int, double, StateBuf, StateBuf, StateBuf,         \
                                      StateBuf, StageAux<R>, StageAux<R>, int, const R*, TkeBuf<R>, TerBuf<R>,        \
                                      const R*, const R*, const R*, double*, double*, double*);                       \
-    template int ter_post_kz<R>(const Params&);
+    template int ter_post_kz<R>(const Params&);                                                                      \
+    template void ter_vert_attr<R>(size_t);
 
+#if !ERFB_TER_F32
 ERFB_TER_INSTANTIATE(double)
+#else
 ERFB_TER_INSTANTIATE(float)
+#endif
 #undef ERFB_TER_INSTANTIATE
 
 }  // namespace erfb
